@@ -1,0 +1,109 @@
+/* include/rphys_ext.h -- extensions to the v1 ABI. No v1 symbol changes; everything here is a
+ * new export with the rphys_ext_ / rphys_batch_ prefix.
+ *
+ * The reference configures a world through its Rust World API, which the v1 C ABI does not
+ * expose (the FFI ignores caller mass and friction: crates/riftphys-ffi/src/lib.rs:544-557,
+ * 724-728). The setters below restate those World methods one for one so C hosts and the
+ * benchmark scenes can reach them. Inspection calls return the step's intermediate products
+ * (pair list, culled manifolds with their solver level, statistics) for parity checking.
+ */
+#pragma once
+
+#include "riftphys_c.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RPHYS_SHAPE_SPHERE  0u
+#define RPHYS_SHAPE_BOX     1u
+#define RPHYS_SHAPE_CAPSULE 2u
+
+/* One body with one collider at its centre. Mass properties come from
+ * MassProps::from_{sphere,box,capsule}_density(dims, density) (riftphys-geom/src/mass.rs:75-145). */
+typedef struct RPhysBodyDescEx {
+    RPhysIsometry pose;
+    RPhysVelocity vel;
+    uint32_t shape;        /* RPHYS_SHAPE_* */
+    float dims[3];         /* sphere: r; box: hx, hy, hz; capsule: r, half_height */
+    float density;         /* kg/m^3, dynamic bodies only */
+    RPhysBodyType body_type;
+    uint32_t material_id;  /* riftphys-materials MaterialId ordinal (0 = Default, 4 = Grit) */
+    uint32_t sleep_allowed;/* World::set_body_sleep_allowed (world.rs:565-570) */
+} RPhysBodyDescEx;
+
+/* World::add_body + World::add_collider (riftphys-world/src/world/world.rs:595-622). Bodies get
+ * consecutive 1-based ids; *out_first_id receives the first. */
+RPhysResult rphys_ext_add_bodies(RPhysWorld* world, const RPhysBodyDescEx* descs, uint32_t n,
+                                 uint32_t* out_first_id);
+
+/* Contact properties for a material pair, either order (World::set_pair_props,
+ * world.rs:975-979). Compliant (stiffness > 0) and patch-friction pairs are not supported. */
+typedef struct RPhysPairProps { float mu_s, mu_k, restitution, stribeck_v; } RPhysPairProps;
+RPhysResult rphys_ext_set_pair_props(RPhysWorld* world, uint32_t mat_a, uint32_t mat_b,
+                                     const RPhysPairProps* props);
+
+/* World::set_solver_iterations (world.rs:994-996): each is clamped to at least 1. */
+RPhysResult rphys_ext_set_solver_iterations(RPhysWorld* world, uint32_t velocity, uint32_t position);
+
+/* World::set_gravity (world.rs:560-563). */
+RPhysResult rphys_ext_set_gravity(RPhysWorld* world, RPhysVec3 g);
+
+/* HeightField::from_heights (riftphys-terrain/src/terrain.rs:24-50) from f32 samples, row-major
+ * with x fastest (nx * nz values); replaces any terrain the world had. */
+RPhysResult rphys_ext_set_heightfield_f32(RPhysWorld* world, uint32_t nx, uint32_t nz,
+                                          float cell_x, float cell_z, float origin_x, float origin_z,
+                                          const float* heights, uint32_t material_id);
+
+/* Velocity-solve termination. tolerance <= 0: the reference's fixed iteration count. tolerance > 0:
+ * sweep until the residual (largest |delta impulse| / effective mass over all rows in a sweep,
+ * m/s) is <= tolerance, at most max_sweeps sweeps. */
+RPhysResult rphys_ext_set_residual_mode(RPhysWorld* world, float tolerance, uint32_t max_sweeps);
+
+/* Runs n ticks of dt (each one World::step) with a single completion wait at the end. */
+RPhysResult rphys_ext_step_n(RPhysWorld* world, float dt, uint32_t n);
+
+#define RPHYS_STATERR_NONFINITE_AABB  1u   /* an AABB with a non-finite bound beyond min.x */
+#define RPHYS_STATERR_CAPACITY        2u   /* a per-step buffer overflowed; results invalid */
+#define RPHYS_STATERR_WAIT_TIMEOUT    4u   /* a bounded device wait gave up */
+
+typedef struct RPhysStepStats {
+    uint32_t pairs;          /* broadphase pairs (StepStats::pairs_tested) */
+    uint32_t contacts;       /* culled contact points (StepStats::contacts) */
+    uint32_t islands;        /* StepStats::islands */
+    uint32_t levels;         /* contact levels of the solve schedule */
+    uint32_t max_batch;      /* largest level (World::last_max_batch().0) */
+    uint32_t warm_matched;   /* contacts started warm (World::warm_matched) */
+    uint32_t sweeps;         /* velocity sweeps run in the last tick */
+    uint32_t bounce_skipped; /* rows that would take the W6 bounce passes (solved inelastic here) */
+    uint32_t warm_entries;   /* entries in the warm-start cache (World::warm_contacts) */
+    uint32_t sleeping;       /* bodies asleep (World::num_sleeping) */
+    uint32_t error_flags;    /* RPHYS_STATERR_* */
+    float residual;          /* residual of the last velocity sweep (m/s) */
+} RPhysStepStats;
+RPhysResult rphys_ext_get_stats(const RPhysWorld* world, RPhysStepStats* out);
+
+/* Last tick's broadphase pairs as (i, j) collider indices, i < j, ascending. */
+RPhysResult rphys_ext_get_pairs(const RPhysWorld* world, uint32_t* out_ij, uint32_t cap_pairs,
+                                uint32_t* out_count);
+
+/* Last tick's culled, oriented contacts in solve order, with their solver level
+ * (0xFFFFFFFF: no movable body, not scheduled). */
+typedef struct RPhysContactRecord {
+    uint32_t a_collider, b_collider;   /* b = 0xFFFFFFFF for terrain */
+    RPhysVec3 point, normal;
+    float depth, impulse;
+    uint32_t level;
+    uint32_t pad;
+} RPhysContactRecord;
+RPhysResult rphys_ext_get_contact_records(const RPhysWorld* world, RPhysContactRecord* out,
+                                          uint32_t cap, uint32_t* out_count);
+
+/* Raw state of bodies [first, first + count) (internal 0-based indices): 13 floats each,
+ * pos xyz, rot xyzw, lin xyz, ang xyz. */
+RPhysResult rphys_ext_get_body_states(const RPhysWorld* world, uint32_t first, uint32_t count,
+                                      float* out13);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,550 @@
+// oracle/oracle_capi.cpp -- TEST INFRASTRUCTURE (the oracle). The reference's C ABI
+// (crates/riftphys-ffi/src/lib.rs) over the CPU restatement in oracle_world.cpp, exporting the
+// same rphys_* symbols as the product library so one test suite drives both. Validation order,
+// error codes, thread-local messages and deterministic out-param defaults follow lib.rs.
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "../include/rphys_ext.h"
+#include "oracle_world.h"
+
+using namespace orc;
+using om::V3;
+using om::Q4;
+
+static thread_local std::string g_err;
+static thread_local bool g_has_err = false;
+static void clear_err() { g_has_err = false; g_err.clear(); }
+static RPhysResult fail(RPhysResult code, const std::string& m) { g_err = m; g_has_err = true; return code; }
+
+struct RPhysWorld {
+  std::mutex mu;
+  World w;
+  uint32_t bodies_created = 0, colliders_created = 0, max_bodies, max_colliders;
+  RPhysWorld(uint32_t mb, uint32_t mc) : w(mb), max_bodies(mb), max_colliders(mc) {}
+};
+struct RPhysWorldSnapshot { Snapshot s; };
+
+static V3 v(const RPhysVec3& a) { return V3{a.x, a.y, a.z}; }
+static Q4 q(const RPhysQuat& a) { return Q4{a.x, a.y, a.z, a.w}; }
+static bool fin3(const RPhysVec3& a) { return std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z); }
+static bool fin_iso(const RPhysIsometry& p) {
+  return fin3(p.pos) && std::isfinite(p.rot.x) && std::isfinite(p.rot.y) && std::isfinite(p.rot.z) && std::isfinite(p.rot.w);
+}
+static bool fin_vel(const RPhysVelocity& a) { return fin3(a.lin) && fin3(a.ang); }
+static bool fin_mat(const RPhysMaterial& m) {
+  return std::isfinite(m.mu_static) && std::isfinite(m.mu_dynamic) && std::isfinite(m.restitution);
+}
+
+// checked_live_body_id (lib.rs:373-409)
+static RPhysResult live_id(RPhysWorld* W, uint32_t id, const char* ctx, uint32_t* out) {
+  if (id == 0) return fail(RPHYS_ERR_INVALID_ID, std::string(ctx) + ": body_id == 0 (invalid)");
+  if (id == RPHYS_TERRAIN_BODY_ID) return fail(RPHYS_ERR_INVALID_ID, std::string(ctx) + ": body_id is terrain sentinel (not a real body)");
+  uint32_t raw = id - 1;
+  if (raw >= W->bodies_created) return fail(RPHYS_ERR_INVALID_ID, std::string(ctx) + ": body_id out of range");
+  if (!(raw < W->w.alive.size() && W->w.alive[raw])) return fail(RPHYS_ERR_INVALID_ID, std::string(ctx) + ": body_id not found (removed)");
+  *out = raw;
+  return RPHYS_OK;
+}
+static RPhysResult add_common(RPhysWorld* W, const char* ctx, const RPhysIsometry& pose, const RPhysVelocity& vel,
+                              uint32_t shape, const float dims[3], float density, bool dynamic, uint32_t mat,
+                              bool sleep_allowed, uint32_t* out_id) {
+  if (W->bodies_created + 1ull > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, std::string(ctx) + ": body capacity exceeded");
+  if (W->colliders_created + 1ull > W->max_colliders) return fail(RPHYS_ERR_CAPACITY, std::string(ctx) + ": collider capacity exceeded");
+  float im = 0; V3 inertia{0, 0, 0};
+  if (dynamic) mass_from_density(shape, dims, density, &im, &inertia);
+  Shape s{shape, dims[0], dims[1], dims[2], V3{0, 0, 0}, V3{0, 0, 0}, V3{0, 0, 0}};
+  if (shape == SH_SPHERE) { s.b = 0; s.c = 0; }
+  if (shape == SH_CAPSULE) { s.c = 0; }
+  uint32_t id = W->w.add_body(Iso{v(pose.pos), q(pose.rot)}, v(vel.lin), v(vel.ang), im, inertia, dynamic);
+  if (id != W->bodies_created) return fail(RPHYS_ERR_INTERNAL, std::string(ctx) + ": internal body id reuse/skip");
+  W->bodies_created++;
+  W->w.add_collider(id, s, mat);
+  W->colliders_created++;
+  if (!sleep_allowed) { W->w.sleep_allowed[id] = 0; W->w.wake(id); }
+  *out_id = id + 1;
+  return RPHYS_OK;
+}
+
+extern "C" {
+
+uint32_t rphys_get_abi_version(void) { return RPHYS_ABI_VERSION; }
+const char* rphys_get_build_id(void) { return "riftphys_ffi-oracle-0.1.0"; }
+const char* rphys_last_error_message(void) { return g_has_err ? g_err.c_str() : nullptr; }
+
+RPhysResult rphys_last_error_copy(char* dst, uint32_t cap, uint32_t* out_len) {
+  uint32_t len = g_has_err ? (uint32_t)g_err.size() : 0;
+  if (out_len) *out_len = len;
+  if (cap == 0) return RPHYS_OK;
+  if (!dst) return RPHYS_ERR_NULL;
+  uint32_t n = len < cap - 1 ? len : cap - 1;
+  if (n) std::memcpy(dst, g_err.data(), n);
+  dst[n] = 0;
+  return RPHYS_OK;
+}
+
+RPhysWorld* rphys_world_create(uint32_t max_bodies, uint32_t max_colliders) {
+  clear_err();
+  try { return new RPhysWorld(max_bodies, max_colliders); } catch (...) { fail(RPHYS_ERR_INTERNAL, "panic in rphys_world_create"); return nullptr; }
+}
+void rphys_world_destroy(RPhysWorld* w) { delete w; }
+
+RPhysResult rphys_world_set_epoch(RPhysWorld* W, uint64_t e) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_world_set_epoch: world is null");
+  std::lock_guard<std::mutex> g(W->mu); W->w.epoch = e; return RPHYS_OK;
+}
+RPhysResult rphys_world_set_rng_seed(RPhysWorld* W, uint64_t s) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_world_set_rng_seed: world is null");
+  std::lock_guard<std::mutex> g(W->mu); W->w.rng = s | 1ull; return RPHYS_OK;
+}
+
+RPhysResult rphys_add_capsule_body(RPhysWorld* W, const RPhysCapsuleBodyDesc* d, uint32_t* out) {
+  clear_err();
+  const char* ctx = "rphys_add_capsule_body";
+  if (out) *out = 0;
+  if (!W || !d || !out) return fail(RPHYS_ERR_NULL, std::string(ctx) + ": null arg");
+  if (!fin_iso(d->pose)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": pose contains NaN/Inf");
+  if (!fin_vel(d->vel)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": vel contains NaN/Inf");
+  if (!fin_mat(d->material)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": material contains NaN/Inf");
+  if (!(std::isfinite(d->radius) && d->radius > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": radius must be finite and > 0");
+  if (!(std::isfinite(d->half_height) && d->half_height >= 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": half_height must be finite and >= 0");
+  if (d->body_type > 1) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": invalid body_type");
+  if (d->body_type == 1 && !(std::isfinite(d->mass) && d->mass > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": dynamic body mass must be finite and > 0");
+  std::lock_guard<std::mutex> g(W->mu);
+  float dims[3] = {d->radius, d->half_height, 0};
+  return add_common(W, ctx, d->pose, d->vel, SH_CAPSULE, dims, 1500.0f, d->body_type == 1, 0, true, out);
+}
+RPhysResult rphys_add_box_body(RPhysWorld* W, const RPhysBoxBodyDesc* d, uint32_t* out) {
+  clear_err();
+  const char* ctx = "rphys_add_box_body";
+  if (out) *out = 0;
+  if (!W || !d || !out) return fail(RPHYS_ERR_NULL, std::string(ctx) + ": null arg");
+  if (!fin_iso(d->pose)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": pose contains NaN/Inf");
+  if (!fin_vel(d->vel)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": vel contains NaN/Inf");
+  if (!fin_mat(d->material)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": material contains NaN/Inf");
+  if (!(std::isfinite(d->hx) && d->hx > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": hx must be finite and > 0");
+  if (!(std::isfinite(d->hy) && d->hy > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": hy must be finite and > 0");
+  if (!(std::isfinite(d->hz) && d->hz > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": hz must be finite and > 0");
+  if (d->body_type > 1) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": invalid body_type");
+  if (d->body_type == 1 && !(std::isfinite(d->mass) && d->mass > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": dynamic body mass must be finite and > 0");
+  std::lock_guard<std::mutex> g(W->mu);
+  float dims[3] = {d->hx, d->hy, d->hz};
+  return add_common(W, ctx, d->pose, d->vel, SH_BOX, dims, 1500.0f, d->body_type == 1, 0, true, out);
+}
+RPhysResult rphys_add_sphere_body(RPhysWorld* W, const RPhysSphereBodyDesc* d, uint32_t* out) {
+  clear_err();
+  const char* ctx = "rphys_add_sphere_body";
+  if (out) *out = 0;
+  if (!W || !d || !out) return fail(RPHYS_ERR_NULL, std::string(ctx) + ": null arg");
+  if (!fin_iso(d->pose)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": pose contains NaN/Inf");
+  if (!fin_vel(d->vel)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": vel contains NaN/Inf");
+  if (!fin_mat(d->material)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": material contains NaN/Inf");
+  if (!(std::isfinite(d->radius) && d->radius > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": radius must be finite and > 0");
+  if (d->body_type > 1) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": invalid body_type");
+  if (d->body_type == 1 && !(std::isfinite(d->mass) && d->mass > 0)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": dynamic body mass must be finite and > 0");
+  std::lock_guard<std::mutex> g(W->mu);
+  float dims[3] = {d->radius, 0, 0};
+  return add_common(W, ctx, d->pose, d->vel, SH_SPHERE, dims, 1500.0f, d->body_type == 1, 0, true, out);
+}
+RPhysResult rphys_body_remove(RPhysWorld* W, uint32_t id) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_body_remove: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  uint32_t b; RPhysResult r = live_id(W, id, "rphys_body_remove", &b);
+  if (r) return r;
+  if (!W->w.remove_body(b)) return fail(RPHYS_ERR_INTERNAL, "rphys_body_remove: internal remove failed");
+  return RPHYS_OK;
+}
+RPhysResult rphys_body_get_pose(const RPhysWorld* Wc, uint32_t id, RPhysIsometry* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_body_get_pose: out_pose is null");
+  *out = RPhysIsometry{{0, 0, 0}, {0, 0, 0, 1}};
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_body_get_pose: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  uint32_t b; RPhysResult r = live_id(W, id, "rphys_body_get_pose", &b);
+  if (r) return r;
+  V3 p = W->w.pos[b]; Q4 o = W->w.rot[b];
+  *out = RPhysIsometry{{p.x, p.y, p.z}, {o.x, o.y, o.z, o.w}};
+  return RPHYS_OK;
+}
+RPhysResult rphys_body_set_pose(RPhysWorld* W, uint32_t id, const RPhysIsometry* p) {
+  clear_err();
+  if (!W || !p) return fail(RPHYS_ERR_NULL, "rphys_body_set_pose: null arg");
+  if (!fin_iso(*p)) return fail(RPHYS_ERR_BAD_ARG, "rphys_body_set_pose: pose contains NaN/Inf");
+  std::lock_guard<std::mutex> g(W->mu);
+  uint32_t b; RPhysResult r = live_id(W, id, "rphys_body_set_pose", &b);
+  if (r) return r;
+  W->w.set_body_pose(b, Iso{v(p->pos), q(p->rot)});
+  return RPHYS_OK;
+}
+RPhysResult rphys_body_get_velocity(const RPhysWorld* Wc, uint32_t id, RPhysVelocity* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_body_get_velocity: out_vel is null");
+  *out = RPhysVelocity{{0, 0, 0}, {0, 0, 0}};
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_body_get_velocity: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  uint32_t b; RPhysResult r = live_id(W, id, "rphys_body_get_velocity", &b);
+  if (r) return r;
+  V3 l = W->w.lin[b], a = W->w.ang[b];
+  *out = RPhysVelocity{{l.x, l.y, l.z}, {a.x, a.y, a.z}};
+  return RPHYS_OK;
+}
+RPhysResult rphys_body_set_velocity(RPhysWorld* W, uint32_t id, const RPhysVelocity* vel) {
+  clear_err();
+  if (!W || !vel) return fail(RPHYS_ERR_NULL, "rphys_body_set_velocity: null arg");
+  if (!fin_vel(*vel)) return fail(RPHYS_ERR_BAD_ARG, "rphys_body_set_velocity: velocity contains NaN/Inf");
+  std::lock_guard<std::mutex> g(W->mu);
+  uint32_t b; RPhysResult r = live_id(W, id, "rphys_body_set_velocity", &b);
+  if (r) return r;
+  W->w.set_body_vel(b, v(vel->lin), v(vel->ang));
+  return RPHYS_OK;
+}
+RPhysResult rphys_body_apply_impulse(RPhysWorld* W, uint32_t id, RPhysVec3 imp) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_body_apply_impulse: world is null");
+  if (!fin3(imp)) return fail(RPHYS_ERR_BAD_ARG, "rphys_body_apply_impulse: impulse contains NaN/Inf");
+  std::lock_guard<std::mutex> g(W->mu);
+  uint32_t b; RPhysResult r = live_id(W, id, "rphys_body_apply_impulse", &b);
+  if (r) return r;
+  W->w.apply_impulse_world(b, v(imp));
+  return RPHYS_OK;
+}
+
+RPhysResult rphys_world_step_ex(RPhysWorld* W, const RPhysStepParams* p) {
+  clear_err();
+  if (!W || !p) return fail(RPHYS_ERR_NULL, "rphys_world_step_ex: null arg");
+  if (p->size_bytes < sizeof(RPhysStepParams)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: size_bytes too small");
+  if (!std::isfinite(p->dt)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: dt is not finite");
+  if (p->dt < 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: dt is negative");
+  if (p->substeps == 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: substeps == 0");
+  std::lock_guard<std::mutex> g(W->mu);
+  float sub = p->dt / (float)p->substeps;
+  if (!std::isfinite(sub)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: sub_dt is not finite");
+  for (uint32_t i = 0; i < p->substeps; ++i) W->w.step(sub);
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_step(RPhysWorld* W, float dt) {
+  RPhysStepParams p{(uint32_t)sizeof(RPhysStepParams), 0, 1, 0, dt};
+  return rphys_world_step_ex(W, &p);
+}
+RPhysResult rphys_world_tick_index(const RPhysWorld* Wc, uint64_t* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_tick_index: out_tick is null");
+  *out = 0;
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_world_tick_index: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  *out = W->w.tick;
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_num_bodies(const RPhysWorld* Wc, uint32_t* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_num_bodies: out_num is null");
+  *out = 0;
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_world_num_bodies: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  *out = W->w.num_bodies();
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_get_step_hash(const RPhysWorld* Wc, RPhysHash32* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_get_step_hash: out_hash is null");
+  std::memset(out, 0, sizeof(*out));
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_world_get_step_hash: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.step_hash(out->bytes);
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_step_and_hash(RPhysWorld* W, float dt, RPhysHash32* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_step_and_hash: out_hash is null");
+  std::memset(out, 0, sizeof(*out));
+  RPhysResult r = rphys_world_step(W, dt);
+  if (r) return r;
+  return rphys_world_get_step_hash(W, out);
+}
+
+static RPhysResult set_hf(RPhysWorld* W, uint32_t nx, uint32_t nz, float cx, float cz, float ox, float oz,
+                          std::vector<float> h, uint32_t mat) {
+  // HeightField::from_heights (terrain.rs:24-50)
+  HeightField hf;
+  hf.nx = nx; hf.nz = nz;
+  hf.sx = (std::isfinite(cx) && cx > 0) ? om::q6(cx) : 1.0f;
+  hf.sz = (std::isfinite(cz) && cz > 0) ? om::q6(cz) : 1.0f;
+  hf.ox = ox; hf.oz = oz;
+  float mn = INFINITY, mx = -INFINITY;
+  for (auto& x : h) { float val = std::isfinite(x) ? x : 0.0f; x = om::q6(val); mn = om::rmin(mn, x); mx = om::rmax(mx, x); }
+  hf.min_y = om::q6(mn); hf.max_y = om::q6(mx);
+  hf.h = std::move(h);
+  hf.mat = mat;
+  W->w.hf = std::move(hf);
+  W->w.has_hf = true;
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_set_heightfield_i16(RPhysWorld* W, const RPhysHeightfieldDesc* d, float ox, float oz, float yoff) {
+  clear_err();
+  if (!W || !d) return fail(RPHYS_ERR_NULL, "rphys_world_set_heightfield_i16: null arg");
+  if (d->size_bytes < sizeof(RPhysHeightfieldDesc)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: size_bytes too small");
+  if (d->width == 0 || d->height == 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: width/height == 0");
+  if (d->row_stride != 0 && d->row_stride < d->width) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: row_stride must be >= width");
+  if (!d->heights) return fail(RPHYS_ERR_NULL, "rphys_world_set_heightfield_i16: heights is null");
+  if (!(std::isfinite(d->cell_size_x) && std::isfinite(d->cell_size_z) && d->cell_size_x > 0 && d->cell_size_z > 0))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: bad cell sizes");
+  uint32_t stride = d->row_stride == 0 ? d->width : d->row_stride;
+  std::vector<float> h;
+  h.reserve((size_t)d->width * d->height);
+  for (uint32_t r = 0; r < d->height; ++r)
+    for (uint32_t c = 0; c < d->width; ++c)
+      h.push_back(((float)d->heights[(size_t)r * stride + c] * d->height_scale + d->height_offset) + yoff);
+  std::lock_guard<std::mutex> g(W->mu);
+  return set_hf(W, d->width, d->height, d->cell_size_x, d->cell_size_z, ox, oz, std::move(h), 4);
+}
+RPhysResult rphys_world_set_heightfield_raw32_square(RPhysWorld* W, const uint8_t* bytes, uint32_t n, float wx, float wz,
+                                                     float ox, float oz, float yoff) {
+  clear_err();
+  if (!W || !bytes) return fail(RPHYS_ERR_NULL, "rphys_world_set_heightfield_raw32_square: null arg");
+  if (n < 4) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_raw32_square: bytes_len too small to form a grid");
+  size_t cnt = n / 4;
+  size_t dim = (size_t)std::sqrt((double)cnt);
+  if (dim * dim != cnt) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_raw32_square: byte length is not a square number of f32s");
+  float cx = wx / om::rmax((float)dim - 1.0f, 1.0f), cz = wz / om::rmax((float)dim - 1.0f, 1.0f);
+  std::vector<float> h(cnt);
+  for (size_t i = 0; i < cnt; ++i) { float x; std::memcpy(&x, bytes + 4 * i, 4); h[i] = x + yoff; }
+  std::lock_guard<std::mutex> g(W->mu);
+  return set_hf(W, (uint32_t)dim, (uint32_t)dim, cx, cz, ox, oz, std::move(h), 4);
+}
+RPhysResult rphys_world_clear_heightfield(RPhysWorld* W) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_world_clear_heightfield: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.has_hf = false;
+  W->w.hf = HeightField{};
+  return RPHYS_OK;
+}
+
+RPhysResult rphys_world_get_contacts(const RPhysWorld* Wc, RPhysContactEvent* out, uint32_t cap, uint32_t* out_count) {
+  clear_err();
+  if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_world_get_contacts: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  auto& cs = W->w.last_frame_contacts;
+  *out_count = (uint32_t)cs.size();
+  if (!out) return RPHYS_OK;
+  uint32_t n = (uint32_t)cs.size() < cap ? (uint32_t)cs.size() : cap;
+  for (uint32_t i = 0; i < n; ++i) {
+    const Contact& c = cs[i];
+    RPhysContactEvent e;
+    e.body_id_a = W->w.colliders[c.a_collider].body + 1;
+    e.body_id_b = c.b_collider == kTerrain ? RPHYS_TERRAIN_BODY_ID : W->w.colliders[c.b_collider].body + 1;
+    e.position = RPhysVec3{c.point.x, c.point.y, c.point.z};
+    e.normal = RPhysVec3{c.normal.x, c.normal.y, c.normal.z};
+    e.impulse = c.impulse;
+    out[i] = e;
+  }
+  return RPHYS_OK;
+}
+
+RPhysWorldSnapshot* rphys_world_snapshot_create(const RPhysWorld* Wc) {
+  clear_err();
+  if (!Wc) { fail(RPHYS_ERR_NULL, "rphys_world_snapshot_create: world is null"); return nullptr; }
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  auto* s = new RPhysWorldSnapshot();
+  World& w = W->w;
+  s->s.tick = w.tick;
+  for (uint32_t i = 0; i < w.num_bodies(); ++i) {
+    if (w.alive[i]) { s->s.poses.push_back(Iso{w.pos[i], w.rot[i]}); s->s.lin.push_back(w.lin[i]); s->s.ang.push_back(w.ang[i]); }
+    else { s->s.poses.push_back(Iso{V3{0, 0, 0}, Q4{0, 0, 0, 1}}); s->s.lin.push_back(V3{0, 0, 0}); s->s.ang.push_back(V3{0, 0, 0}); }
+  }
+  s->s.carried = w.carried_state();
+  return s;
+}
+RPhysResult rphys_world_snapshot_restore(RPhysWorld* W, const RPhysWorldSnapshot* s) {
+  clear_err();
+  if (!W || !s) return fail(RPHYS_ERR_NULL, "rphys_world_snapshot_restore: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  World& w = W->w;
+  w.tick = s->s.tick;
+  for (uint32_t i = 0; i < s->s.poses.size(); ++i) {
+    if (i < w.alive.size() && w.alive[i] && i < w.num_bodies()) {
+      w.set_body_pose(i, s->s.poses[i]);
+      w.set_body_vel(i, s->s.lin[i], s->s.ang[i]);
+    }
+  }
+  w.restore_carried_state(s->s.carried);
+  return RPHYS_OK;
+}
+void rphys_world_snapshot_free(RPhysWorldSnapshot* s) { delete s; }
+
+// ---------------------------------------------------------------- extensions
+RPhysResult rphys_ext_add_bodies(RPhysWorld* W, const RPhysBodyDescEx* d, uint32_t n, uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_bodies: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  if ((uint64_t)W->bodies_created + n > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_add_bodies: body capacity exceeded");
+  if ((uint64_t)W->colliders_created + n > W->max_colliders) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_add_bodies: collider capacity exceeded");
+  for (uint32_t i = 0; i < n; ++i) {
+    const RPhysBodyDescEx& e = d[i];
+    if (!fin_iso(e.pose) || !fin_vel(e.vel)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: pose/vel contains NaN/Inf");
+    if (e.shape > 2 || e.body_type > 1 || !material_known(e.material_id)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: bad shape/body_type/material");
+    int nd = e.shape == 0 ? 1 : (e.shape == 1 ? 3 : 1);
+    for (int k = 0; k < nd; ++k) if (!(std::isfinite(e.dims[k]) && e.dims[k] > 0)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: dims must be finite and > 0");
+    if (e.shape == 2 && !(std::isfinite(e.dims[1]) && e.dims[1] >= 0)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: half_height must be finite and >= 0");
+    if (e.body_type == 1 && !(std::isfinite(e.density) && e.density > 0)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: density must be finite and > 0");
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    const RPhysBodyDescEx& e = d[i];
+    uint32_t id;
+    RPhysResult r = add_common(W, "rphys_ext_add_bodies", e.pose, e.vel, e.shape, e.dims, e.density, e.body_type == 1,
+                               e.material_id, e.sleep_allowed != 0, &id);
+    if (r) return r;
+    if (i == 0) *out_first = id;
+  }
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_pair_props(RPhysWorld* W, uint32_t a, uint32_t b, const RPhysPairProps* p) {
+  clear_err();
+  if (!W || !p) return fail(RPHYS_ERR_NULL, "rphys_ext_set_pair_props: null arg");
+  if (!material_known(a) || !material_known(b)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_pair_props: unknown material");
+  if (!(std::isfinite(p->mu_s) && std::isfinite(p->mu_k) && std::isfinite(p->restitution) && std::isfinite(p->stribeck_v)))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_pair_props: non-finite property");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.set_pair_props(a, b, PairProps{p->mu_s, p->mu_k, p->restitution, p->stribeck_v, 0.0f});
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_solver_iterations(RPhysWorld* W, uint32_t v_it, uint32_t p_it) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_solver_iterations: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.iters_v = v_it < 1 ? 1 : v_it;
+  W->w.iters_p = p_it < 1 ? 1 : p_it;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_gravity(RPhysWorld* W, RPhysVec3 g3) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_gravity: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.gravity = v(g3);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_heightfield_f32(RPhysWorld* W, uint32_t nx, uint32_t nz, float cx, float cz, float ox, float oz,
+                                          const float* h, uint32_t mat) {
+  clear_err();
+  if (!W || !h) return fail(RPHYS_ERR_NULL, "rphys_ext_set_heightfield_f32: null arg");
+  if (nx == 0 || nz == 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_heightfield_f32: nx/nz == 0");
+  if (!material_known(mat)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_heightfield_f32: unknown material");
+  std::vector<float> hh(h, h + (size_t)nx * nz);
+  std::lock_guard<std::mutex> g(W->mu);
+  return set_hf(W, nx, nz, cx, cz, ox, oz, std::move(hh), mat);
+}
+RPhysResult rphys_ext_set_residual_mode(RPhysWorld* W, float tol, uint32_t max_sweeps) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_residual_mode: world is null");
+  if (!std::isfinite(tol)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_residual_mode: tolerance not finite");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.res_tol = tol; W->w.res_max = max_sweeps;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_step_n(RPhysWorld* W, float dt, uint32_t n) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_step_n: world is null");
+  if (!std::isfinite(dt) || dt < 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_step_n: bad dt");
+  std::lock_guard<std::mutex> g(W->mu);
+  for (uint32_t i = 0; i < n; ++i) W->w.step(dt);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
+  clear_err();
+  if (!Wc || !o) return fail(RPHYS_ERR_NULL, "rphys_ext_get_stats: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  const Stats& s = W->w.stats;
+  std::memset(o, 0, sizeof(*o));
+  o->pairs = s.pairs; o->contacts = s.contacts; o->islands = s.islands; o->levels = s.levels;
+  o->max_batch = s.max_batch; o->warm_matched = s.warm_matched; o->sweeps = s.sweeps;
+  o->bounce_skipped = s.bounce_skipped; o->residual = s.residual;
+  uint32_t we = 0;
+  for (auto& kv : W->w.warm) we += (uint32_t)kv.second.size();
+  o->warm_entries = we;
+  o->sleeping = W->w.num_sleeping();
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_pairs(const RPhysWorld* Wc, uint32_t* out, uint32_t cap, uint32_t* out_count) {
+  clear_err();
+  if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_ext_get_pairs: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  auto& p = W->w.last_pairs;
+  *out_count = (uint32_t)p.size();
+  if (!out) return RPHYS_OK;
+  for (uint32_t i = 0; i < p.size() && i < cap; ++i) { out[2 * i] = p[i].first; out[2 * i + 1] = p[i].second; }
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_contact_records(const RPhysWorld* Wc, RPhysContactRecord* out, uint32_t cap, uint32_t* out_count) {
+  clear_err();
+  if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_ext_get_contact_records: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  auto& cs = W->w.last_frame_contacts;
+  *out_count = (uint32_t)cs.size();
+  if (!out) return RPHYS_OK;
+  for (uint32_t i = 0; i < cs.size() && i < cap; ++i) {
+    const Contact& c = cs[i];
+    RPhysContactRecord r;
+    r.a_collider = c.a_collider; r.b_collider = c.b_collider;
+    r.point = RPhysVec3{c.point.x, c.point.y, c.point.z};
+    r.normal = RPhysVec3{c.normal.x, c.normal.y, c.normal.z};
+    r.depth = c.depth; r.impulse = c.impulse;
+    r.level = i < W->w.last_levels.size() ? W->w.last_levels[i] : 0xFFFFFFFFu;
+    r.pad = 0;
+    out[i] = r;
+  }
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_body_states(const RPhysWorld* Wc, uint32_t first, uint32_t count, float* out) {
+  clear_err();
+  if (!Wc || (!out && count)) return fail(RPHYS_ERR_NULL, "rphys_ext_get_body_states: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  World& w = W->w;
+  if ((uint64_t)first + count > w.num_bodies()) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_get_body_states: range out of bounds");
+  for (uint32_t k = 0; k < count; ++k) {
+    uint32_t i = first + k;
+    float* o = out + 13 * (size_t)k;
+    o[0] = w.pos[i].x; o[1] = w.pos[i].y; o[2] = w.pos[i].z;
+    o[3] = w.rot[i].x; o[4] = w.rot[i].y; o[5] = w.rot[i].z; o[6] = w.rot[i].w;
+    o[7] = w.lin[i].x; o[8] = w.lin[i].y; o[9] = w.lin[i].z;
+    o[10] = w.ang[i].x; o[11] = w.ang[i].y; o[12] = w.ang[i].z;
+  }
+  return RPHYS_OK;
+}
+
+// Oracle-only: CPU threads for the timed baseline (narrowphase and level batches, order-preserving).
+RPhysResult rphys_oracle_set_threads(RPhysWorld* W, int threads) {
+  if (!W) return RPHYS_ERR_NULL;
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.threads = threads < 1 ? 1 : threads;
+  return RPHYS_OK;
+}
+// Oracle-only: BLAKE3 of a byte buffer (known-answer tests).
+void rphys_oracle_blake3(const uint8_t* data, size_t n, uint8_t out[32]);
+
+}  // extern "C"
+
+#include "blake3_spec.h"
+extern "C" void rphys_oracle_blake3(const uint8_t* data, size_t n, uint8_t out[32]) {
+  b3::Hasher h;
+  h.update(data, n);
+  h.finalize(out);
+}

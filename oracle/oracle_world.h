@@ -1,0 +1,146 @@
+// oracle/oracle_world.h -- TEST INFRASTRUCTURE (the oracle): a CPU restatement of the
+// reference's per-tick rigid-body step, World::step (riftphys-world/src/world/step.rs:40-542)
+// and everything it calls at the configured feature set: sphere / box / capsule colliders with
+// no offset, a static ground body, a HeightField environment, rigid contacts, warm starting,
+// sleeping, the BLAKE3 tick hash. Only tests/, __graft_entry__.smoke() and bench.py's
+// cpu_baseline leg use it; the product (riftphys-rust_b200/) never links it.
+//
+// Not restated (no configuration reaches them, or the C ABI cannot): joints, compliant and
+// patch-friction pairs, collider offsets, players, accel components, pending epoch swaps. The
+// W6 bounce passes (solver.rs:1047-1241) are detected and counted, and the rows that would take
+// them are left as the inelastic solve produced them (the same rule the GPU path follows).
+#pragma once
+#include <cstdint>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "om.h"
+
+namespace orc {
+using om::M3;
+using om::Q4;
+using om::V3;
+
+enum : uint32_t { SH_SPHERE = 0, SH_BOX = 1, SH_CAPSULE = 2, SH_TRIANGLE = 3 };
+static const uint32_t kTerrain = 0xFFFFFFFFu;  // TERRAIN_CI (world.rs:26)
+
+struct Shape { uint32_t kind; float a, b, c; V3 ta, tb, tc; };
+struct Aabb { V3 min, max; };
+struct Iso { V3 pos; Q4 rot; };
+struct Collider { uint32_t body; Shape shape; Aabb aabb; uint32_t mat; };
+struct Contact {
+  uint32_t a_collider, b_collider;
+  V3 point, normal;
+  float depth;
+  int32_t env_mat;  // -1: None
+  float impulse;
+};
+struct PairProps { float mu_s, mu_k, restitution, stribeck_v, stiffness; };
+using WarmKey = std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>;
+struct WarmContact { V3 la; float jn; V3 jt; };
+
+struct HeightField {
+  uint32_t nx = 0, nz = 0;
+  float sx = 1, sz = 1, ox = 0, oz = 0;
+  std::vector<float> h;
+  float min_y = 0, max_y = 0;
+  uint32_t mat = 4;
+};
+
+struct CarriedState {
+  std::map<WarmKey, std::vector<WarmContact>> warm;
+  std::vector<V3> last_lin_vel;
+  std::vector<uint8_t> awake;
+  std::vector<uint16_t> sleep_ticks;
+};
+
+struct Snapshot {
+  uint64_t tick;
+  std::vector<Iso> poses;
+  std::vector<V3> lin, ang;
+  CarriedState carried;
+};
+
+struct Stats {
+  uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
+  uint32_t sweeps = 0, bounce_skipped = 0;
+  float residual = 0;
+};
+
+struct World {
+  V3 gravity{0.0f, -9.81f, 0.0f};
+  uint64_t epoch = 0;
+  uint64_t rng = 0xC0FFEEull | 1ull;
+  // Bodies SoA (riftphys-dynamics/src/dynamics.rs:38-46)
+  std::vector<V3> pos;
+  std::vector<Q4> rot;
+  std::vector<V3> lin, ang;
+  std::vector<float> inv_mass;
+  std::vector<uint8_t> dyn;
+  std::vector<M3> inv_I;
+  std::vector<Collider> colliders;
+  // SleepManager (sleep.rs:5-13): sized to the world's capacity at creation
+  std::vector<uint8_t> awake, sleep_allowed;
+  std::vector<uint16_t> sleep_ticks;
+  std::vector<uint8_t> alive;
+  std::vector<V3> last_lin_vel;
+  std::map<WarmKey, std::vector<WarmContact>> warm;
+  uint32_t iters_v = 20, iters_p = 20;
+  std::vector<std::pair<std::pair<uint32_t, uint32_t>, PairProps>> overrides;
+  bool has_hf = false;
+  HeightField hf;
+  uint64_t tick = 0;
+  std::vector<Contact> last_frame_contacts;
+  std::vector<std::pair<uint32_t, uint32_t>> last_pairs;
+  std::vector<uint32_t> last_levels;  // per last_frame_contacts entry
+  Stats stats;
+  float res_tol = 0.0f;
+  uint32_t res_max = 0;
+  int threads = 1;  // >1: narrowphase and level batches on OpenMP (order-preserving)
+
+  explicit World(uint32_t capacity);
+  uint32_t num_bodies() const { return (uint32_t)pos.size(); }
+
+  // dynamics.rs
+  M3 inv_inertia_world(uint32_t i) const;
+  void set_pose(uint32_t i, const Iso& p);
+  void set_vel(uint32_t i, V3 l, V3 a);
+  void apply_impulse(uint32_t i, V3 j);
+  void apply_angular_impulse(uint32_t i, V3 tau);
+  // world.rs
+  uint32_t add_body(const Iso& pose, V3 lin, V3 ang, float inv_mass_in, V3 inertia_diag,
+                    bool dynamic);
+  void add_collider(uint32_t body, const Shape& s, uint32_t mat);
+  void set_body_pose(uint32_t id, const Iso& p);
+  void set_body_vel(uint32_t id, V3 l, V3 a);
+  void wake(uint32_t id);
+  void apply_impulse_world(uint32_t id, V3 j);
+  bool remove_body(uint32_t id);
+  void drop_warm_of(uint32_t b);
+  PairProps pair_props(uint32_t a, uint32_t b) const;
+  void set_pair_props(uint32_t a, uint32_t b, const PairProps& p);
+  void update_colliders_aabb();
+  CarriedState carried_state() const;
+  void restore_carried_state(const CarriedState& s);
+  // step.rs / provenance.rs
+  void step(float dt);
+  void step_hash(uint8_t out[32]) const;
+  uint32_t num_sleeping() const;
+};
+
+Aabb aabb_of(const Shape& s, const Iso& xf);
+
+// Narrowphase (riftphys-collision/src/narrowphase.rs), exposed for unit tests.
+struct CP { V3 position, normal; float penetration; };
+struct Manifold { V3 normal; CP pts[4]; int len = 0; };
+bool collide_shapes(const Shape& a, const Iso& xa, const Shape& b, const Iso& xb, float cd, Manifold* out);
+
+// MassProps::from_*_density (riftphys-geom/src/mass.rs:75-145): inv_mass and inertia diagonal.
+bool mass_from_density(uint32_t shape, const float dims[3], float density, float* inv_mass, V3* inertia);
+// Material table and pair mixing (riftphys-materials/src/materials.rs:97-101,278-305)
+PairProps table_pair_props(uint32_t a, uint32_t b);
+bool material_known(uint32_t id);
+
+}  // namespace orc

@@ -1,0 +1,361 @@
+"""riftphys-rust_b200: Python bindings of the RiftPhys C ABI (v1 + extensions).
+
+The product is ``build/librphys_gpu.so`` in this directory: the reference's C ABI
+(crates/riftphys-ffi/src/riftphys_c.h) implemented by C++ host code over hand-written sm_100a
+CUDA kernels. This module only declares the ctypes signatures of that ABI, mirroring the
+reference's FFI one entry point per function, and gives a thin ``World`` wrapper with the same
+names, argument meanings and error codes (an ``RPhysError`` carries the code and the
+thread-local message, as ``rphys_last_error_message`` does in crates/riftphys-ffi/src/lib.rs).
+
+``load_product()`` loads the CUDA library and raises if it is missing: there is no CPU
+fallback on the product path.
+"""
+import ctypes
+import os
+from ctypes import (POINTER, Structure, byref, c_char, c_char_p, c_float, c_int,
+                    c_uint8, c_uint32, c_uint64, c_void_p)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PRODUCT_LIB = os.path.join(HERE, "build", "librphys_gpu.so")
+
+RPHYS_OK = 0
+RPHYS_ERR_NULL = 1
+RPHYS_ERR_INVALID_ID = 2
+RPHYS_ERR_CAPACITY = 3
+RPHYS_ERR_BAD_ARG = 4
+RPHYS_ERR_INTERNAL = 0x80000000
+RPHYS_TERRAIN_BODY_ID = 0xFFFFFFFF
+RPHYS_BODY_STATIC = 0
+RPHYS_BODY_DYNAMIC = 1
+SHAPE_SPHERE, SHAPE_BOX, SHAPE_CAPSULE = 0, 1, 2
+
+
+class Vec3(Structure):
+    _fields_ = [("x", c_float), ("y", c_float), ("z", c_float)]
+
+
+class Quat(Structure):
+    _fields_ = [("x", c_float), ("y", c_float), ("z", c_float), ("w", c_float)]
+
+
+class Isometry(Structure):
+    _fields_ = [("pos", Vec3), ("rot", Quat)]
+
+
+class Velocity(Structure):
+    _fields_ = [("lin", Vec3), ("ang", Vec3)]
+
+
+class Material(Structure):
+    _fields_ = [("mu_static", c_float), ("mu_dynamic", c_float), ("restitution", c_float)]
+
+
+class CapsuleBodyDesc(Structure):
+    _fields_ = [("pose", Isometry), ("vel", Velocity), ("radius", c_float), ("half_height", c_float),
+                ("mass", c_float), ("body_type", c_uint32), ("material", Material), ("user_tag", c_uint32)]
+
+
+class BoxBodyDesc(Structure):
+    _fields_ = [("pose", Isometry), ("vel", Velocity), ("hx", c_float), ("hy", c_float), ("hz", c_float),
+                ("mass", c_float), ("body_type", c_uint32), ("material", Material), ("user_tag", c_uint32)]
+
+
+class SphereBodyDesc(Structure):
+    _fields_ = [("pose", Isometry), ("vel", Velocity), ("radius", c_float), ("mass", c_float),
+                ("body_type", c_uint32), ("material", Material), ("user_tag", c_uint32)]
+
+
+class Hash32(Structure):
+    _fields_ = [("bytes", c_uint8 * 32)]
+
+
+class StepParams(Structure):
+    _fields_ = [("size_bytes", c_uint32), ("flags", c_uint32), ("substeps", c_uint32),
+                ("solver_iters", c_uint32), ("dt", c_float)]
+
+
+class ContactEvent(Structure):
+    _fields_ = [("body_id_a", c_uint32), ("body_id_b", c_uint32), ("position", Vec3), ("normal", Vec3),
+                ("impulse", c_float)]
+
+
+class HeightfieldDesc(Structure):
+    _fields_ = [("size_bytes", c_uint32), ("flags", c_uint32), ("width", c_uint32), ("height", c_uint32),
+                ("row_stride", c_uint32), ("cell_size_x", c_float), ("cell_size_z", c_float),
+                ("height_scale", c_float), ("height_offset", c_float), ("heights", c_void_p)]
+
+
+class BodyDescEx(Structure):
+    _fields_ = [("pose", Isometry), ("vel", Velocity), ("shape", c_uint32), ("dims", c_float * 3),
+                ("density", c_float), ("body_type", c_uint32), ("material_id", c_uint32),
+                ("sleep_allowed", c_uint32)]
+
+
+class PairProps(Structure):
+    _fields_ = [("mu_s", c_float), ("mu_k", c_float), ("restitution", c_float), ("stribeck_v", c_float)]
+
+
+class StepStats(Structure):
+    _fields_ = [(n, c_uint32) for n in ("pairs", "contacts", "islands", "levels", "max_batch", "warm_matched",
+                                        "sweeps", "bounce_skipped", "warm_entries", "sleeping", "error_flags")] + \
+               [("residual", c_float)]
+
+
+class ContactRecord(Structure):
+    _fields_ = [("a_collider", c_uint32), ("b_collider", c_uint32), ("point", Vec3), ("normal", Vec3),
+                ("depth", c_float), ("impulse", c_float), ("level", c_uint32), ("pad", c_uint32)]
+
+
+# (name, restype, argtypes) of every entry point declared in include/riftphys_c.h and include/rphys_ext.h
+ABI = [
+    ("rphys_get_abi_version", c_uint32, []),
+    ("rphys_get_build_id", c_char_p, []),
+    ("rphys_last_error_message", c_char_p, []),
+    ("rphys_last_error_copy", c_uint32, [c_char_p, c_uint32, POINTER(c_uint32)]),
+    ("rphys_world_create", c_void_p, [c_uint32, c_uint32]),
+    ("rphys_world_destroy", None, [c_void_p]),
+    ("rphys_world_set_epoch", c_uint32, [c_void_p, c_uint64]),
+    ("rphys_world_set_rng_seed", c_uint32, [c_void_p, c_uint64]),
+    ("rphys_add_capsule_body", c_uint32, [c_void_p, POINTER(CapsuleBodyDesc), POINTER(c_uint32)]),
+    ("rphys_add_box_body", c_uint32, [c_void_p, POINTER(BoxBodyDesc), POINTER(c_uint32)]),
+    ("rphys_add_sphere_body", c_uint32, [c_void_p, POINTER(SphereBodyDesc), POINTER(c_uint32)]),
+    ("rphys_body_remove", c_uint32, [c_void_p, c_uint32]),
+    ("rphys_body_get_pose", c_uint32, [c_void_p, c_uint32, POINTER(Isometry)]),
+    ("rphys_body_set_pose", c_uint32, [c_void_p, c_uint32, POINTER(Isometry)]),
+    ("rphys_body_get_velocity", c_uint32, [c_void_p, c_uint32, POINTER(Velocity)]),
+    ("rphys_body_set_velocity", c_uint32, [c_void_p, c_uint32, POINTER(Velocity)]),
+    ("rphys_body_apply_impulse", c_uint32, [c_void_p, c_uint32, Vec3]),
+    ("rphys_world_step_ex", c_uint32, [c_void_p, POINTER(StepParams)]),
+    ("rphys_world_step", c_uint32, [c_void_p, c_float]),
+    ("rphys_world_tick_index", c_uint32, [c_void_p, POINTER(c_uint64)]),
+    ("rphys_world_num_bodies", c_uint32, [c_void_p, POINTER(c_uint32)]),
+    ("rphys_world_get_step_hash", c_uint32, [c_void_p, POINTER(Hash32)]),
+    ("rphys_world_step_and_hash", c_uint32, [c_void_p, c_float, POINTER(Hash32)]),
+    ("rphys_world_set_heightfield_i16", c_uint32, [c_void_p, POINTER(HeightfieldDesc), c_float, c_float, c_float]),
+    ("rphys_world_set_heightfield_raw32_square", c_uint32,
+     [c_void_p, c_void_p, c_uint32, c_float, c_float, c_float, c_float, c_float]),
+    ("rphys_world_clear_heightfield", c_uint32, [c_void_p]),
+    ("rphys_world_get_contacts", c_uint32, [c_void_p, POINTER(ContactEvent), c_uint32, POINTER(c_uint32)]),
+    ("rphys_world_snapshot_create", c_void_p, [c_void_p]),
+    ("rphys_world_snapshot_restore", c_uint32, [c_void_p, c_void_p]),
+    ("rphys_world_snapshot_free", None, [c_void_p]),
+    ("rphys_ext_add_bodies", c_uint32, [c_void_p, POINTER(BodyDescEx), c_uint32, POINTER(c_uint32)]),
+    ("rphys_ext_set_pair_props", c_uint32, [c_void_p, c_uint32, c_uint32, POINTER(PairProps)]),
+    ("rphys_ext_set_solver_iterations", c_uint32, [c_void_p, c_uint32, c_uint32]),
+    ("rphys_ext_set_gravity", c_uint32, [c_void_p, Vec3]),
+    ("rphys_ext_set_heightfield_f32", c_uint32,
+     [c_void_p, c_uint32, c_uint32, c_float, c_float, c_float, c_float, c_void_p, c_uint32]),
+    ("rphys_ext_set_residual_mode", c_uint32, [c_void_p, c_float, c_uint32]),
+    ("rphys_ext_step_n", c_uint32, [c_void_p, c_float, c_uint32]),
+    ("rphys_ext_get_stats", c_uint32, [c_void_p, POINTER(StepStats)]),
+    ("rphys_ext_get_pairs", c_uint32, [c_void_p, c_void_p, c_uint32, POINTER(c_uint32)]),
+    ("rphys_ext_get_contact_records", c_uint32, [c_void_p, POINTER(ContactRecord), c_uint32, POINTER(c_uint32)]),
+    ("rphys_ext_get_body_states", c_uint32, [c_void_p, c_uint32, c_uint32, c_void_p]),
+]
+
+
+class RPhysError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rphys error {code:#x}: {msg}")
+        self.code = code
+        self.msg = msg
+
+
+class Lib:
+    """A loaded library exporting the RiftPhys C ABI (the CUDA product, or a test oracle)."""
+
+    def __init__(self, path):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"RiftPhys library not built: {path}")
+        self.path = path
+        self.dll = ctypes.CDLL(path)
+        for name, res, args in ABI:
+            f = getattr(self.dll, name)
+            f.restype = res
+            f.argtypes = args
+        self.extra = {}
+
+    def call(self, name, *args):
+        r = getattr(self.dll, name)(*args)
+        if r != RPHYS_OK:
+            msg = self.dll.rphys_last_error_message()
+            raise RPhysError(r, msg.decode() if msg else "")
+        return r
+
+    def world(self, max_bodies=1024, max_colliders=2048):
+        return World(self, max_bodies, max_colliders)
+
+
+def load_product():
+    """The CUDA library. Raises if it was not built: the product has no CPU fallback."""
+    return Lib(PRODUCT_LIB)
+
+
+def iso(x=0.0, y=0.0, z=0.0, q=(0.0, 0.0, 0.0, 1.0)):
+    return Isometry(Vec3(x, y, z), Quat(*q))
+
+
+def vel(lin=(0.0, 0.0, 0.0), ang=(0.0, 0.0, 0.0)):
+    return Velocity(Vec3(*lin), Vec3(*ang))
+
+
+class World:
+    """Owns one RPhysWorld handle of a Lib."""
+
+    def __init__(self, lib, max_bodies=1024, max_colliders=2048):
+        self.lib = lib
+        self.h = lib.dll.rphys_world_create(max_bodies, max_colliders)
+        if not self.h:
+            msg = lib.dll.rphys_last_error_message()
+            raise RPhysError(RPHYS_ERR_INTERNAL, msg.decode() if msg else "create failed")
+
+    def close(self):
+        if self.h:
+            self.lib.dll.rphys_world_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def c(self, name, *args):
+        return self.lib.call(name, self.h, *args)
+
+    # ---- v1
+    def add_box(self, pos, he, dynamic=True, mass=1.0, q=(0, 0, 0, 1), v=(0, 0, 0), w=(0, 0, 0)):
+        d = BoxBodyDesc(iso(*pos, q=q), vel(v, w), he[0], he[1], he[2], mass,
+                        RPHYS_BODY_DYNAMIC if dynamic else RPHYS_BODY_STATIC, Material(0.9, 0.7, 0.0), 0)
+        out = c_uint32(0)
+        self.c("rphys_add_box_body", byref(d), byref(out))
+        return out.value
+
+    def add_sphere(self, pos, r, dynamic=True, mass=1.0, v=(0, 0, 0)):
+        d = SphereBodyDesc(iso(*pos), vel(v), r, mass, RPHYS_BODY_DYNAMIC if dynamic else RPHYS_BODY_STATIC,
+                           Material(0.9, 0.7, 0.0), 0)
+        out = c_uint32(0)
+        self.c("rphys_add_sphere_body", byref(d), byref(out))
+        return out.value
+
+    def add_capsule(self, pos, r, hh, dynamic=True, mass=1.0, q=(0, 0, 0, 1)):
+        d = CapsuleBodyDesc(iso(*pos, q=q), vel(), r, hh, mass, RPHYS_BODY_DYNAMIC if dynamic else RPHYS_BODY_STATIC,
+                            Material(0.9, 0.7, 0.0), 0)
+        out = c_uint32(0)
+        self.c("rphys_add_capsule_body", byref(d), byref(out))
+        return out.value
+
+    def step(self, dt, substeps=1):
+        p = StepParams(ctypes.sizeof(StepParams), 0, substeps, 0, dt)
+        self.c("rphys_world_step_ex", byref(p))
+
+    def step_hash(self, dt):
+        h = Hash32()
+        self.c("rphys_world_step_and_hash", c_float(dt), byref(h))
+        return bytes(h.bytes)
+
+    def hash(self):
+        h = Hash32()
+        self.c("rphys_world_get_step_hash", byref(h))
+        return bytes(h.bytes)
+
+    def pose(self, bid):
+        p = Isometry()
+        self.c("rphys_body_get_pose", bid, byref(p))
+        return (p.pos.x, p.pos.y, p.pos.z), (p.rot.x, p.rot.y, p.rot.z, p.rot.w)
+
+    def velocity(self, bid):
+        v = Velocity()
+        self.c("rphys_body_get_velocity", bid, byref(v))
+        return (v.lin.x, v.lin.y, v.lin.z), (v.ang.x, v.ang.y, v.ang.z)
+
+    def tick(self):
+        t = c_uint64(0)
+        self.c("rphys_world_tick_index", byref(t))
+        return t.value
+
+    def num_bodies(self):
+        n = c_uint32(0)
+        self.c("rphys_world_num_bodies", byref(n))
+        return n.value
+
+    def snapshot(self):
+        s = self.lib.dll.rphys_world_snapshot_create(self.h)
+        if not s:
+            raise RPhysError(RPHYS_ERR_INTERNAL, "snapshot_create failed")
+        return s
+
+    def restore(self, snap):
+        self.c("rphys_world_snapshot_restore", c_void_p(snap))
+
+    def free_snapshot(self, snap):
+        self.lib.dll.rphys_world_snapshot_free(c_void_p(snap))
+
+    def apply_impulse(self, bid, j):
+        self.c("rphys_body_apply_impulse", bid, Vec3(*j))
+
+    def contacts(self):
+        n = c_uint32(0)
+        self.c("rphys_world_get_contacts", None, 0, byref(n))
+        buf = (ContactEvent * max(1, n.value))()
+        self.c("rphys_world_get_contacts", buf, n.value, byref(n))
+        return list(buf)[: n.value]
+
+    # ---- extensions
+    def add_bodies(self, descs):
+        arr = (BodyDescEx * len(descs))(*descs)
+        out = c_uint32(0)
+        self.c("rphys_ext_add_bodies", arr, len(descs), byref(out))
+        return out.value
+
+    def set_pair_props(self, a, b, mu_s, mu_k, restitution, stribeck_v):
+        p = PairProps(mu_s, mu_k, restitution, stribeck_v)
+        self.c("rphys_ext_set_pair_props", a, b, byref(p))
+
+    def set_iterations(self, v, p):
+        self.c("rphys_ext_set_solver_iterations", v, p)
+
+    def set_gravity(self, g):
+        self.c("rphys_ext_set_gravity", Vec3(*g))
+
+    def set_heightfield(self, heights, nx, nz, cell_x, cell_z, origin_x, origin_z, material=4):
+        import numpy as np
+        h = np.ascontiguousarray(heights, dtype=np.float32)
+        assert h.size == nx * nz
+        self.c("rphys_ext_set_heightfield_f32", nx, nz, c_float(cell_x), c_float(cell_z), c_float(origin_x),
+               c_float(origin_z), h.ctypes.data_as(c_void_p), material)
+
+    def set_residual_mode(self, tol, max_sweeps):
+        self.c("rphys_ext_set_residual_mode", c_float(tol), max_sweeps)
+
+    def step_n(self, dt, n):
+        self.c("rphys_ext_step_n", c_float(dt), n)
+
+    def stats(self):
+        s = StepStats()
+        self.c("rphys_ext_get_stats", byref(s))
+        return {f: getattr(s, f) for f, _ in StepStats._fields_}
+
+    def pairs(self):
+        import numpy as np
+        n = c_uint32(0)
+        self.c("rphys_ext_get_pairs", None, 0, byref(n))
+        buf = np.zeros((max(1, n.value), 2), dtype=np.uint32)
+        self.c("rphys_ext_get_pairs", buf.ctypes.data_as(c_void_p), n.value, byref(n))
+        return buf[: n.value]
+
+    def contact_records(self):
+        n = c_uint32(0)
+        self.c("rphys_ext_get_contact_records", None, 0, byref(n))
+        buf = (ContactRecord * max(1, n.value))()
+        self.c("rphys_ext_get_contact_records", buf, n.value, byref(n))
+        return list(buf)[: n.value]
+
+    def body_states(self, first=0, count=None):
+        import numpy as np
+        if count is None:
+            count = self.num_bodies() - first
+        out = np.zeros((count, 13), dtype=np.float32)
+        if count:
+            self.c("rphys_ext_get_body_states", first, count, out.ctypes.data_as(c_void_p))
+        return out
