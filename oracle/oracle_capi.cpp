@@ -548,3 +548,23 @@ extern "C" void rphys_oracle_blake3(const uint8_t* data, size_t n, uint8_t out[3
   h.update(data, n);
   h.finalize(out);
 }
+
+// Oracle-only: collide_shapes on two posed shapes (narrowphase unit tests). shape: 0 sphere,
+// 1 box, 2 capsule; dims as RPhysBodyDescEx; pose7 = pos xyz, rot xyzw. Writes up to 4 points as
+// (position xyz, normal xyz, penetration) into out7x4; returns the point count (0: no contact).
+extern "C" int rphys_oracle_collide(uint32_t sa, const float* da, const float* pa, uint32_t sb, const float* db,
+                                    const float* pb, float cd, float* out) {
+  Shape A{sa, da[0], da[1], da[2], V3{0, 0, 0}, V3{0, 0, 0}, V3{0, 0, 0}};
+  Shape B{sb, db[0], db[1], db[2], V3{0, 0, 0}, V3{0, 0, 0}, V3{0, 0, 0}};
+  Iso xa{V3{pa[0], pa[1], pa[2]}, Q4{pa[3], pa[4], pa[5], pa[6]}};
+  Iso xb{V3{pb[0], pb[1], pb[2]}, Q4{pb[3], pb[4], pb[5], pb[6]}};
+  Manifold m;
+  if (!collide_shapes(A, xa, B, xb, cd, &m)) return 0;
+  for (int k = 0; k < m.len; ++k) {
+    float* o = out + 7 * k;
+    o[0] = m.pts[k].position.x; o[1] = m.pts[k].position.y; o[2] = m.pts[k].position.z;
+    o[3] = m.pts[k].normal.x; o[4] = m.pts[k].normal.y; o[5] = m.pts[k].normal.z;
+    o[6] = m.pts[k].penetration;
+  }
+  return m.len;
+}

@@ -1,0 +1,596 @@
+// capi.cu -- the drop-in boundary: the reference's C ABI v1 (crates/riftphys-ffi/src/lib.rs,
+// riftphys_c.h) and the rphys_ext_ extensions, over the GPU world. Each call validates its
+// arguments in the reference's order, clears and sets the thread-local error message, writes
+// the deterministic default to out-params first, takes the world's mutex, and converts any C++
+// or CUDA failure into RPHYS_ERR_INTERNAL (the reference's ffi_guard, lib.rs:97-106).
+// step_ex synchronises before returning, so every getter sees the finished tick.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "../../include/rphys_ext.h"
+#include "world_gpu.h"
+
+using rp::WorldGpu;
+
+static thread_local std::string g_err;
+static thread_local bool g_has_err = false;
+static void clear_err() { g_has_err = false; g_err.clear(); }
+static RPhysResult fail(RPhysResult code, const std::string& m) { g_err = m; g_has_err = true; return code; }
+
+struct RPhysWorld {
+  std::mutex mu;
+  std::unique_ptr<WorldGpu> w;
+  uint32_t bodies_created = 0, colliders_created = 0, max_bodies, max_colliders;
+  // contacts of the last tick, as the reference's last_frame_contacts (step.rs:384)
+  RPhysWorld(uint32_t mb, uint32_t mc) : w(new WorldGpu(mb, mc)), max_bodies(mb), max_colliders(mc) {}
+};
+struct RPhysWorldSnapshot { rp::SnapshotGpu* s; };
+
+template <class F>
+static RPhysResult guard(const char* ctx, F f) {
+  try {
+    return f();
+  } catch (const std::exception& e) {
+    return fail(RPHYS_ERR_INTERNAL, std::string(ctx) + ": " + e.what());
+  } catch (...) {
+    return fail(RPHYS_ERR_INTERNAL, std::string(ctx) + ": internal failure");
+  }
+}
+static bool fin3(const RPhysVec3& a) { return std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z); }
+static bool fin_iso(const RPhysIsometry& p) {
+  return fin3(p.pos) && std::isfinite(p.rot.x) && std::isfinite(p.rot.y) && std::isfinite(p.rot.z) && std::isfinite(p.rot.w);
+}
+static bool fin_vel(const RPhysVelocity& a) { return fin3(a.lin) && fin3(a.ang); }
+static bool fin_mat(const RPhysMaterial& m) {
+  return std::isfinite(m.mu_static) && std::isfinite(m.mu_dynamic) && std::isfinite(m.restitution);
+}
+// checked_live_body_id (lib.rs:373-409)
+static RPhysResult live_id(RPhysWorld* W, uint32_t id, const std::string& ctx, uint32_t* out) {
+  if (id == 0) return fail(RPHYS_ERR_INVALID_ID, ctx + ": body_id == 0 (invalid)");
+  if (id == RPHYS_TERRAIN_BODY_ID) return fail(RPHYS_ERR_INVALID_ID, ctx + ": body_id is terrain sentinel (not a real body)");
+  uint32_t raw = id - 1;
+  if (raw >= W->bodies_created) return fail(RPHYS_ERR_INVALID_ID, ctx + ": body_id out of range");
+  if (!W->w->alive(raw)) return fail(RPHYS_ERR_INVALID_ID, ctx + ": body_id not found (removed)");
+  *out = raw;
+  return RPHYS_OK;
+}
+static void pose7(const RPhysIsometry& p, float o[7]) {
+  o[0] = p.pos.x; o[1] = p.pos.y; o[2] = p.pos.z; o[3] = p.rot.x; o[4] = p.rot.y; o[5] = p.rot.z; o[6] = p.rot.w;
+}
+static void vel6(const RPhysVelocity& v, float o[6]) {
+  o[0] = v.lin.x; o[1] = v.lin.y; o[2] = v.lin.z; o[3] = v.ang.x; o[4] = v.ang.y; o[5] = v.ang.z;
+}
+static RPhysResult add_one(RPhysWorld* W, const std::string& ctx, const RPhysIsometry& pose, const RPhysVelocity& vel,
+                           uint32_t shape, const float dims[3], float density, bool dynamic, uint32_t mat, bool sleep_ok,
+                           uint32_t* out) {
+  if (W->bodies_created + 1ull > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, ctx + ": body capacity exceeded");
+  if (W->colliders_created + 1ull > W->max_colliders) return fail(RPHYS_ERR_CAPACITY, ctx + ": collider capacity exceeded");
+  float im = 0, in[3] = {0, 0, 0};
+  if (dynamic) rp::mass_from_density(shape, dims, density, &im, in);
+  float p[7], v[6];
+  pose7(pose, p); vel6(vel, v);
+  uint32_t id = W->w->add_body(p, v, shape, dims, im, in, dynamic, mat, sleep_ok);
+  if (id != W->bodies_created) return fail(RPHYS_ERR_INTERNAL, ctx + ": internal body id reuse/skip");
+  W->bodies_created++;
+  W->colliders_created++;
+  *out = id + 1;
+  return RPHYS_OK;
+}
+#define LOCK std::lock_guard<std::mutex> lk(W->mu)
+
+extern "C" {
+
+uint32_t rphys_get_abi_version(void) { return RPHYS_ABI_VERSION; }
+const char* rphys_get_build_id(void) { return "riftphys_ffi-b200-0.1.0"; }
+const char* rphys_last_error_message(void) { return g_has_err ? g_err.c_str() : nullptr; }
+RPhysResult rphys_last_error_copy(char* dst, uint32_t cap, uint32_t* out_len) {
+  uint32_t len = g_has_err ? (uint32_t)g_err.size() : 0;
+  if (out_len) *out_len = len;
+  if (cap == 0) return RPHYS_OK;
+  if (!dst) return RPHYS_ERR_NULL;
+  uint32_t n = len < cap - 1 ? len : cap - 1;
+  if (n) std::memcpy(dst, g_err.data(), n);
+  dst[n] = 0;
+  return RPHYS_OK;
+}
+
+RPhysWorld* rphys_world_create(uint32_t max_bodies, uint32_t max_colliders) {
+  clear_err();
+  try {
+    return new RPhysWorld(max_bodies, max_colliders);
+  } catch (const std::exception& e) {
+    fail(RPHYS_ERR_INTERNAL, std::string("rphys_world_create: ") + e.what());
+    return nullptr;
+  }
+}
+void rphys_world_destroy(RPhysWorld* w) {
+  try { delete w; } catch (...) {}
+}
+RPhysResult rphys_world_set_epoch(RPhysWorld* W, uint64_t e) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_world_set_epoch: world is null");
+  LOCK; W->w->set_epoch(e); return RPHYS_OK;
+}
+RPhysResult rphys_world_set_rng_seed(RPhysWorld* W, uint64_t s) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_world_set_rng_seed: world is null");
+  LOCK; W->w->set_rng_state(s | 1ull); return RPHYS_OK;  // XorShift64::new (rng.rs:7-9)
+}
+
+#define BODY_PRELUDE(NAME)                                                                                   \
+  clear_err();                                                                                               \
+  const std::string ctx = NAME;                                                                              \
+  if (out) *out = 0;                                                                                         \
+  if (!W || !d || !out) return fail(RPHYS_ERR_NULL, ctx + ": null arg");                                     \
+  if (!fin_iso(d->pose)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": pose contains NaN/Inf");                    \
+  if (!fin_vel(d->vel)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": vel contains NaN/Inf");                      \
+  if (!fin_mat(d->material)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": material contains NaN/Inf");
+#define BODY_TYPE_CHECK                                                                                        \
+  if (d->body_type > 1) return fail(RPHYS_ERR_BAD_ARG, ctx + ": invalid body_type");                           \
+  if (d->body_type == 1 && !(std::isfinite(d->mass) && d->mass > 0))                                           \
+    return fail(RPHYS_ERR_BAD_ARG, ctx + ": dynamic body mass must be finite and > 0");
+
+// Dynamic FFI bodies get MaterialId::Default's density, 1500 kg/m^3, whatever the caller's mass
+// (lib.rs:724-728; materials.rs:362), and keep material Default (mat_from_ffi, lib.rs:544-557).
+RPhysResult rphys_add_capsule_body(RPhysWorld* W, const RPhysCapsuleBodyDesc* d, uint32_t* out) {
+  BODY_PRELUDE("rphys_add_capsule_body")
+  if (!(std::isfinite(d->radius) && d->radius > 0)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": radius must be finite and > 0");
+  if (!(std::isfinite(d->half_height) && d->half_height >= 0)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": half_height must be finite and >= 0");
+  BODY_TYPE_CHECK
+  return guard(ctx.c_str(), [&]() {
+    LOCK;
+    float dims[3] = {d->radius, d->half_height, 0};
+    return add_one(W, ctx, d->pose, d->vel, RPHYS_SHAPE_CAPSULE, dims, 1500.0f, d->body_type == 1, 0, true, out);
+  });
+}
+RPhysResult rphys_add_box_body(RPhysWorld* W, const RPhysBoxBodyDesc* d, uint32_t* out) {
+  BODY_PRELUDE("rphys_add_box_body")
+  if (!(std::isfinite(d->hx) && d->hx > 0)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": hx must be finite and > 0");
+  if (!(std::isfinite(d->hy) && d->hy > 0)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": hy must be finite and > 0");
+  if (!(std::isfinite(d->hz) && d->hz > 0)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": hz must be finite and > 0");
+  BODY_TYPE_CHECK
+  return guard(ctx.c_str(), [&]() {
+    LOCK;
+    float dims[3] = {d->hx, d->hy, d->hz};
+    return add_one(W, ctx, d->pose, d->vel, RPHYS_SHAPE_BOX, dims, 1500.0f, d->body_type == 1, 0, true, out);
+  });
+}
+RPhysResult rphys_add_sphere_body(RPhysWorld* W, const RPhysSphereBodyDesc* d, uint32_t* out) {
+  BODY_PRELUDE("rphys_add_sphere_body")
+  if (!(std::isfinite(d->radius) && d->radius > 0)) return fail(RPHYS_ERR_BAD_ARG, ctx + ": radius must be finite and > 0");
+  BODY_TYPE_CHECK
+  return guard(ctx.c_str(), [&]() {
+    LOCK;
+    float dims[3] = {d->radius, 0, 0};
+    return add_one(W, ctx, d->pose, d->vel, RPHYS_SHAPE_SPHERE, dims, 1500.0f, d->body_type == 1, 0, true, out);
+  });
+}
+RPhysResult rphys_body_remove(RPhysWorld* W, uint32_t id) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_body_remove: world is null");
+  return guard("rphys_body_remove", [&]() {
+    LOCK;
+    uint32_t b;
+    RPhysResult r = live_id(W, id, "rphys_body_remove", &b);
+    if (r) return r;
+    if (!W->w->remove_body(b)) return fail(RPHYS_ERR_INTERNAL, "rphys_body_remove: internal remove failed");
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_body_get_pose(const RPhysWorld* Wc, uint32_t id, RPhysIsometry* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_body_get_pose: out_pose is null");
+  *out = RPhysIsometry{{0, 0, 0}, {0, 0, 0, 1}};
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_body_get_pose: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_body_get_pose", [&]() {
+    LOCK;
+    uint32_t b;
+    RPhysResult r = live_id(W, id, "rphys_body_get_pose", &b);
+    if (r) return r;
+    float p[7];
+    W->w->get_body_pose(b, p);
+    *out = RPhysIsometry{{p[0], p[1], p[2]}, {p[3], p[4], p[5], p[6]}};
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_body_set_pose(RPhysWorld* W, uint32_t id, const RPhysIsometry* p) {
+  clear_err();
+  if (!W || !p) return fail(RPHYS_ERR_NULL, "rphys_body_set_pose: null arg");
+  if (!fin_iso(*p)) return fail(RPHYS_ERR_BAD_ARG, "rphys_body_set_pose: pose contains NaN/Inf");
+  return guard("rphys_body_set_pose", [&]() {
+    LOCK;
+    uint32_t b;
+    RPhysResult r = live_id(W, id, "rphys_body_set_pose", &b);
+    if (r) return r;
+    float q[7];
+    pose7(*p, q);
+    W->w->set_body_pose(b, q);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_body_get_velocity(const RPhysWorld* Wc, uint32_t id, RPhysVelocity* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_body_get_velocity: out_vel is null");
+  *out = RPhysVelocity{{0, 0, 0}, {0, 0, 0}};
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_body_get_velocity: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_body_get_velocity", [&]() {
+    LOCK;
+    uint32_t b;
+    RPhysResult r = live_id(W, id, "rphys_body_get_velocity", &b);
+    if (r) return r;
+    float v[6];
+    W->w->get_body_vel(b, v);
+    *out = RPhysVelocity{{v[0], v[1], v[2]}, {v[3], v[4], v[5]}};
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_body_set_velocity(RPhysWorld* W, uint32_t id, const RPhysVelocity* vel) {
+  clear_err();
+  if (!W || !vel) return fail(RPHYS_ERR_NULL, "rphys_body_set_velocity: null arg");
+  if (!fin_vel(*vel)) return fail(RPHYS_ERR_BAD_ARG, "rphys_body_set_velocity: velocity contains NaN/Inf");
+  return guard("rphys_body_set_velocity", [&]() {
+    LOCK;
+    uint32_t b;
+    RPhysResult r = live_id(W, id, "rphys_body_set_velocity", &b);
+    if (r) return r;
+    float v[6];
+    vel6(*vel, v);
+    W->w->set_body_vel(b, v);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_body_apply_impulse(RPhysWorld* W, uint32_t id, RPhysVec3 imp) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_body_apply_impulse: world is null");
+  if (!fin3(imp)) return fail(RPHYS_ERR_BAD_ARG, "rphys_body_apply_impulse: impulse contains NaN/Inf");
+  return guard("rphys_body_apply_impulse", [&]() {
+    LOCK;
+    uint32_t b;
+    RPhysResult r = live_id(W, id, "rphys_body_apply_impulse", &b);
+    if (r) return r;
+    float j[3] = {imp.x, imp.y, imp.z};
+    W->w->apply_impulse(b, j);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+
+RPhysResult rphys_world_step_ex(RPhysWorld* W, const RPhysStepParams* p) {
+  clear_err();
+  if (!W || !p) return fail(RPHYS_ERR_NULL, "rphys_world_step_ex: null arg");
+  if (p->size_bytes < sizeof(RPhysStepParams)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: size_bytes too small");
+  if (!std::isfinite(p->dt)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: dt is not finite");
+  if (p->dt < 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: dt is negative");
+  if (p->substeps == 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: substeps == 0");
+  return guard("rphys_world_step_ex", [&]() {
+    LOCK;
+    float sub = p->dt / (float)p->substeps;
+    if (!std::isfinite(sub)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_step_ex: sub_dt is not finite");
+    for (uint32_t i = 0; i < p->substeps; ++i) W->w->step(sub);  // solver_iters and flags ignored (lib.rs:1147-1148)
+    W->w->synchronize();
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_world_step(RPhysWorld* W, float dt) {
+  RPhysStepParams p{(uint32_t)sizeof(RPhysStepParams), 0, 1, 0, dt};
+  return rphys_world_step_ex(W, &p);
+}
+RPhysResult rphys_world_tick_index(const RPhysWorld* Wc, uint64_t* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_tick_index: out_tick is null");
+  *out = 0;
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_world_tick_index: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  LOCK;
+  *out = W->w->tick();
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_num_bodies(const RPhysWorld* Wc, uint32_t* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_num_bodies: out_num is null");
+  *out = 0;
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_world_num_bodies: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  LOCK;
+  *out = W->w->num_bodies();
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_get_step_hash(const RPhysWorld* Wc, RPhysHash32* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_get_step_hash: out_hash is null");
+  std::memset(out, 0, sizeof(*out));
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_world_get_step_hash: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_world_get_step_hash", [&]() {
+    LOCK;
+    W->w->step_hash(out->bytes);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_world_step_and_hash(RPhysWorld* W, float dt, RPhysHash32* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_step_and_hash: out_hash is null");
+  std::memset(out, 0, sizeof(*out));
+  RPhysResult r = rphys_world_step(W, dt);
+  if (r) return r;
+  return rphys_world_get_step_hash(W, out);
+}
+
+// HeightField::from_heights (terrain.rs:24-50): cell sizes and heights quantised to 1e-6.
+static RPhysResult set_hf(RPhysWorld* W, uint32_t nx, uint32_t nz, float cx, float cz, float ox, float oz,
+                          std::vector<float> h, uint32_t mat) {
+  float sx = (std::isfinite(cx) && cx > 0) ? rp::q6(cx) : 1.0f;
+  float sz = (std::isfinite(cz) && cz > 0) ? rp::q6(cz) : 1.0f;
+  float mn = INFINITY, mx = -INFINITY;
+  for (auto& x : h) {
+    float v = std::isfinite(x) ? x : 0.0f;
+    x = rp::q6(v);
+    mn = rp::rmin(mn, x);
+    mx = rp::rmax(mx, x);
+  }
+  W->w->set_heightfield(nx, nz, sx, sz, ox, oz, h, rp::q6(mn), rp::q6(mx), mat);
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_set_heightfield_i16(RPhysWorld* W, const RPhysHeightfieldDesc* d, float ox, float oz, float yoff) {
+  clear_err();
+  if (!W || !d) return fail(RPHYS_ERR_NULL, "rphys_world_set_heightfield_i16: null arg");
+  if (d->size_bytes < sizeof(RPhysHeightfieldDesc)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: size_bytes too small");
+  if (d->width == 0 || d->height == 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: width/height == 0");
+  if (d->row_stride != 0 && d->row_stride < d->width) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: row_stride must be >= width");
+  if (!d->heights) return fail(RPHYS_ERR_NULL, "rphys_world_set_heightfield_i16: heights is null");
+  if (!(std::isfinite(d->cell_size_x) && std::isfinite(d->cell_size_z) && d->cell_size_x > 0 && d->cell_size_z > 0))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_i16: bad cell sizes");
+  uint32_t stride = d->row_stride == 0 ? d->width : d->row_stride;
+  std::vector<float> h;
+  h.reserve((size_t)d->width * d->height);
+  for (uint32_t r = 0; r < d->height; ++r)
+    for (uint32_t c = 0; c < d->width; ++c)
+      h.push_back(((float)d->heights[(size_t)r * stride + c] * d->height_scale + d->height_offset) + yoff);
+  return guard("rphys_world_set_heightfield_i16", [&]() {
+    LOCK;
+    return set_hf(W, d->width, d->height, d->cell_size_x, d->cell_size_z, ox, oz, std::move(h), 4);
+  });
+}
+RPhysResult rphys_world_set_heightfield_raw32_square(RPhysWorld* W, const uint8_t* bytes, uint32_t n, float wx, float wz,
+                                                     float ox, float oz, float yoff) {
+  clear_err();
+  if (!W || !bytes) return fail(RPHYS_ERR_NULL, "rphys_world_set_heightfield_raw32_square: null arg");
+  if (n < 4) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_raw32_square: bytes_len too small to form a grid");
+  size_t cnt = n / 4;
+  size_t dim = (size_t)std::sqrt((double)cnt);
+  if (dim * dim != cnt) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_set_heightfield_raw32_square: byte length is not a square number of f32s");
+  float cx = wx / rp::rmax((float)dim - 1.0f, 1.0f), cz = wz / rp::rmax((float)dim - 1.0f, 1.0f);
+  std::vector<float> h(cnt);
+  for (size_t i = 0; i < cnt; ++i) { float x; std::memcpy(&x, bytes + 4 * i, 4); h[i] = x + yoff; }
+  return guard("rphys_world_set_heightfield_raw32_square", [&]() {
+    LOCK;
+    return set_hf(W, (uint32_t)dim, (uint32_t)dim, cx, cz, ox, oz, std::move(h), 4);
+  });
+}
+RPhysResult rphys_world_clear_heightfield(RPhysWorld* W) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_world_clear_heightfield: world is null");
+  LOCK;
+  W->w->clear_heightfield();
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_get_contacts(const RPhysWorld* Wc, RPhysContactEvent* out, uint32_t cap, uint32_t* out_count) {
+  clear_err();
+  if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_world_get_contacts: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_world_get_contacts", [&]() {
+    LOCK;
+    std::vector<WorldGpu::ContactOut> cs;
+    W->w->get_contacts(cs);
+    *out_count = (uint32_t)cs.size();
+    if (!out) return (RPhysResult)RPHYS_OK;
+    uint32_t n = (uint32_t)cs.size() < cap ? (uint32_t)cs.size() : cap;
+    for (uint32_t i = 0; i < n; ++i) {
+      const auto& c = cs[i];
+      RPhysContactEvent e;
+      e.body_id_a = W->w->body_of_collider(c.a) + 1;
+      e.body_id_b = c.b == 0xFFFFFFFFu ? RPHYS_TERRAIN_BODY_ID : W->w->body_of_collider(c.b) + 1;
+      e.position = RPhysVec3{c.p[0], c.p[1], c.p[2]};
+      e.normal = RPhysVec3{c.n[0], c.n[1], c.n[2]};
+      e.impulse = c.impulse;
+      out[i] = e;
+    }
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysWorldSnapshot* rphys_world_snapshot_create(const RPhysWorld* Wc) {
+  clear_err();
+  if (!Wc) { fail(RPHYS_ERR_NULL, "rphys_world_snapshot_create: world is null"); return nullptr; }
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  try {
+    LOCK;
+    return new RPhysWorldSnapshot{W->w->snapshot_create()};
+  } catch (const std::exception& e) {
+    fail(RPHYS_ERR_INTERNAL, std::string("rphys_world_snapshot_create: ") + e.what());
+    return nullptr;
+  }
+}
+RPhysResult rphys_world_snapshot_restore(RPhysWorld* W, const RPhysWorldSnapshot* s) {
+  clear_err();
+  if (!W || !s) return fail(RPHYS_ERR_NULL, "rphys_world_snapshot_restore: null arg");
+  return guard("rphys_world_snapshot_restore", [&]() {
+    LOCK;
+    W->w->snapshot_restore(s->s);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+void rphys_world_snapshot_free(RPhysWorldSnapshot* s) {
+  if (!s) return;
+  try { WorldGpu::snapshot_free(s->s); } catch (...) {}
+  delete s;
+}
+
+// ---------------------------------------------------------------- extensions
+RPhysResult rphys_ext_add_bodies(RPhysWorld* W, const RPhysBodyDescEx* d, uint32_t n, uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_bodies: null arg");
+  for (uint32_t i = 0; i < n; ++i) {
+    const RPhysBodyDescEx& e = d[i];
+    if (!fin_iso(e.pose) || !fin_vel(e.vel)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: pose/vel contains NaN/Inf");
+    if (e.shape > 2 || e.body_type > 1 || !rp::material_known(e.material_id))
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: bad shape/body_type/material");
+    int nd = e.shape == 0 ? 1 : (e.shape == 1 ? 3 : 1);
+    for (int k = 0; k < nd; ++k)
+      if (!(std::isfinite(e.dims[k]) && e.dims[k] > 0)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: dims must be finite and > 0");
+    if (e.shape == 2 && !(std::isfinite(e.dims[1]) && e.dims[1] >= 0))
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: half_height must be finite and >= 0");
+    if (e.body_type == 1 && !(std::isfinite(e.density) && e.density > 0))
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: density must be finite and > 0");
+  }
+  return guard("rphys_ext_add_bodies", [&]() {
+    LOCK;
+    if ((uint64_t)W->bodies_created + n > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_add_bodies: body capacity exceeded");
+    if ((uint64_t)W->colliders_created + n > W->max_colliders) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_add_bodies: collider capacity exceeded");
+    if (n == 0) return (RPhysResult)RPHYS_OK;
+    std::vector<float> p7(7 * (size_t)n), v6(6 * (size_t)n), dims(3 * (size_t)n), im(n), in3(3 * (size_t)n);
+    std::vector<uint32_t> sh(n), mat(n);
+    std::vector<uint8_t> dyn(n), sok(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      const RPhysBodyDescEx& e = d[i];
+      pose7(e.pose, &p7[7 * (size_t)i]);
+      vel6(e.vel, &v6[6 * (size_t)i]);
+      float dd[3] = {e.dims[0], e.shape == 0 ? 0.0f : e.dims[1], e.shape == 1 ? e.dims[2] : 0.0f};
+      std::memcpy(&dims[3 * (size_t)i], dd, 12);
+      sh[i] = e.shape; mat[i] = e.material_id; dyn[i] = e.body_type == 1; sok[i] = e.sleep_allowed != 0;
+      im[i] = 0; in3[3 * i] = in3[3 * i + 1] = in3[3 * i + 2] = 0;
+      if (dyn[i]) rp::mass_from_density(e.shape, dd, e.density, &im[i], &in3[3 * (size_t)i]);
+    }
+    uint32_t first = W->w->num_bodies();
+    W->w->add_bodies_bulk(n, p7.data(), v6.data(), sh.data(), dims.data(), im.data(), in3.data(), dyn.data(), mat.data(),
+                          sok.data());
+    W->bodies_created += n;
+    W->colliders_created += n;
+    *out_first = first + 1;
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_set_pair_props(RPhysWorld* W, uint32_t a, uint32_t b, const RPhysPairProps* p) {
+  clear_err();
+  if (!W || !p) return fail(RPHYS_ERR_NULL, "rphys_ext_set_pair_props: null arg");
+  if (!rp::material_known(a) || !rp::material_known(b)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_pair_props: unknown material");
+  if (!(std::isfinite(p->mu_s) && std::isfinite(p->mu_k) && std::isfinite(p->restitution) && std::isfinite(p->stribeck_v)))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_pair_props: non-finite property");
+  return guard("rphys_ext_set_pair_props", [&]() {
+    LOCK;
+    W->w->set_pair_props(a, b, rp::PairPropsHost{p->mu_s, p->mu_k, p->restitution, p->stribeck_v, 0.0f});
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_set_solver_iterations(RPhysWorld* W, uint32_t v, uint32_t p) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_solver_iterations: world is null");
+  LOCK;
+  W->w->set_solver_iterations(v, p);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_gravity(RPhysWorld* W, RPhysVec3 g) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_gravity: world is null");
+  LOCK;
+  W->w->set_gravity(rp::mk3(g.x, g.y, g.z));
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_heightfield_f32(RPhysWorld* W, uint32_t nx, uint32_t nz, float cx, float cz, float ox, float oz,
+                                          const float* h, uint32_t mat) {
+  clear_err();
+  if (!W || !h) return fail(RPHYS_ERR_NULL, "rphys_ext_set_heightfield_f32: null arg");
+  if (nx == 0 || nz == 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_heightfield_f32: nx/nz == 0");
+  if (!rp::material_known(mat)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_heightfield_f32: unknown material");
+  std::vector<float> hh(h, h + (size_t)nx * nz);
+  return guard("rphys_ext_set_heightfield_f32", [&]() {
+    LOCK;
+    return set_hf(W, nx, nz, cx, cz, ox, oz, std::move(hh), mat);
+  });
+}
+RPhysResult rphys_ext_set_residual_mode(RPhysWorld* W, float tol, uint32_t max_sweeps) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_residual_mode: world is null");
+  if (!std::isfinite(tol)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_residual_mode: tolerance not finite");
+  LOCK;
+  W->w->set_residual_mode(tol, max_sweeps);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_step_n(RPhysWorld* W, float dt, uint32_t n) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_step_n: world is null");
+  if (!std::isfinite(dt) || dt < 0) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_step_n: bad dt");
+  return guard("rphys_ext_step_n", [&]() {
+    LOCK;
+    for (uint32_t i = 0; i < n; ++i) W->w->step(dt);
+    W->w->synchronize();
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
+  clear_err();
+  if (!Wc || !o) return fail(RPHYS_ERR_NULL, "rphys_ext_get_stats: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_get_stats", [&]() {
+    LOCK;
+    const rp::StepStatsHost& s = W->w->stats();
+    o->pairs = s.pairs; o->contacts = s.contacts; o->islands = s.islands; o->levels = s.levels;
+    o->max_batch = s.max_batch; o->warm_matched = s.warm_matched; o->sweeps = s.sweeps;
+    o->bounce_skipped = s.bounce_skipped; o->warm_entries = s.warm_entries; o->sleeping = s.sleeping;
+    o->error_flags = s.error_flags; o->residual = s.residual;
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_get_pairs(const RPhysWorld* Wc, uint32_t* out, uint32_t cap, uint32_t* out_count) {
+  clear_err();
+  if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_ext_get_pairs: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_get_pairs", [&]() {
+    LOCK;
+    std::vector<uint64_t> p;
+    W->w->get_pairs(p);
+    *out_count = (uint32_t)p.size();
+    if (!out) return (RPhysResult)RPHYS_OK;
+    for (uint32_t i = 0; i < p.size() && i < cap; ++i) { out[2 * i] = (uint32_t)(p[i] >> 32); out[2 * i + 1] = (uint32_t)p[i]; }
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_get_contact_records(const RPhysWorld* Wc, RPhysContactRecord* out, uint32_t cap, uint32_t* out_count) {
+  clear_err();
+  if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_ext_get_contact_records: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_get_contact_records", [&]() {
+    LOCK;
+    std::vector<WorldGpu::ContactOut> cs;
+    W->w->get_contacts(cs);
+    *out_count = (uint32_t)cs.size();
+    if (!out) return (RPhysResult)RPHYS_OK;
+    for (uint32_t i = 0; i < cs.size() && i < cap; ++i) {
+      const auto& c = cs[i];
+      RPhysContactRecord r;
+      r.a_collider = c.a; r.b_collider = c.b;
+      r.point = RPhysVec3{c.p[0], c.p[1], c.p[2]};
+      r.normal = RPhysVec3{c.n[0], c.n[1], c.n[2]};
+      r.depth = c.depth; r.impulse = c.impulse; r.level = c.level; r.pad = 0;
+      out[i] = r;
+    }
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_get_body_states(const RPhysWorld* Wc, uint32_t first, uint32_t count, float* out) {
+  clear_err();
+  if (!Wc || (!out && count)) return fail(RPHYS_ERR_NULL, "rphys_ext_get_body_states: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_get_body_states", [&]() {
+    LOCK;
+    if ((uint64_t)first + count > W->w->num_bodies()) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_get_body_states: range out of bounds");
+    W->w->get_body_states(first, count, out);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+
+}  // extern "C"

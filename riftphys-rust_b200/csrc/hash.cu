@@ -1,0 +1,227 @@
+// hash.cu -- World::step_hash (riftphys-world/src/world/provenance.rs:6-24 and hash_carried,
+// world.rs:882-909) on the GPU: the byte stream is written in place by one thread per record,
+// then hashed with BLAKE3 (`blake3` crate 1.8.2, Cargo.lock:267-269; algorithm from the published
+// BLAKE3 specification): one thread compresses each 1 KiB chunk, then parent nodes are merged
+// pairwise, level by level -- the left-complete tree the specification defines (an odd last node
+// moves up a level unchanged). BLAKE3 is integer-ALU work (32-bit add / xor / rotate).
+//
+// Stream layout: epoch u64 | rng state u64 | BLAKE3("") (the empty schedule digest) |
+//   per body: index u32, pos xyz, rot xyzw, lin xyz, ang xyz (canonical f32 bits) |
+//   warm keys u64 | per key: 4 x u32, count u32, per entry la xyz, jn, jt xyz |
+//   warm patches u64 0 | warm joints u64 0 | rotors u64 0 |
+//   last_lin_vel count u64 + xyz each | awake count u64 + u8 each | sleep ticks count u64 + u16 each.
+#include <cstring>
+
+#include "step_internal.cuh"
+
+namespace rp {
+
+__constant__ uint32_t c_iv[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
+                                 0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
+
+__device__ __forceinline__ uint32_t rotr(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
+#define B3G(a, b, c, d, x, y)        \
+  a = a + b + x; d = rotr(d ^ a, 16); \
+  c = c + d; b = rotr(b ^ c, 12);     \
+  a = a + b + y; d = rotr(d ^ a, 8);  \
+  c = c + d; b = rotr(b ^ c, 7);
+
+// The compression function: 7 rounds, message words permuted between rounds by the
+// specification's fixed permutation (2, 6, 3, 10, 7, 0, 4, 13, 1, 11, 12, 5, 9, 14, 15, 8).
+__device__ void b3_compress(const uint32_t cv[8], const uint32_t blk[16], uint64_t counter, uint32_t blen,
+                            uint32_t flags, uint32_t out[8]) {
+  uint32_t s0 = cv[0], s1 = cv[1], s2 = cv[2], s3 = cv[3], s4 = cv[4], s5 = cv[5], s6 = cv[6], s7 = cv[7];
+  uint32_t s8 = c_iv[0], s9 = c_iv[1], s10 = c_iv[2], s11 = c_iv[3];
+  uint32_t s12 = (uint32_t)counter, s13 = (uint32_t)(counter >> 32), s14 = blen, s15 = flags;
+  uint32_t m[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) m[i] = blk[i];
+#pragma unroll
+  for (int r = 0; r < 7; ++r) {
+    B3G(s0, s4, s8, s12, m[0], m[1]);
+    B3G(s1, s5, s9, s13, m[2], m[3]);
+    B3G(s2, s6, s10, s14, m[4], m[5]);
+    B3G(s3, s7, s11, s15, m[6], m[7]);
+    B3G(s0, s5, s10, s15, m[8], m[9]);
+    B3G(s1, s6, s11, s12, m[10], m[11]);
+    B3G(s2, s7, s8, s13, m[12], m[13]);
+    B3G(s3, s4, s9, s14, m[14], m[15]);
+    if (r < 6) {
+      uint32_t t[16] = {m[2], m[6], m[3], m[10], m[7], m[0], m[4], m[13], m[1], m[11], m[12], m[5], m[9], m[14], m[15], m[8]};
+#pragma unroll
+      for (int i = 0; i < 16; ++i) m[i] = t[i];
+    }
+  }
+  out[0] = s0 ^ s8; out[1] = s1 ^ s9; out[2] = s2 ^ s10; out[3] = s3 ^ s11;
+  out[4] = s4 ^ s12; out[5] = s5 ^ s13; out[6] = s6 ^ s14; out[7] = s7 ^ s15;
+}
+enum : uint32_t { CHUNK_START = 1, CHUNK_END = 2, PARENT = 4, ROOT = 8 };
+
+// One thread per 1024-byte chunk: its chaining value; a single-chunk input is finalised as root.
+__global__ void k_b3_chunks(const uint8_t* __restrict__ data, uint64_t len, uint32_t nch, uint32_t* cvs, uint32_t* root) {
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  uint64_t base = (uint64_t)c * 1024;
+  uint64_t clen = len - base < 1024 ? len - base : 1024;
+  uint32_t nblocks = clen == 0 ? 1 : (uint32_t)((clen + 63) / 64);
+  uint32_t cv[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) cv[i] = c_iv[i];
+  for (uint32_t b = 0; b < nblocks; ++b) {
+    uint32_t blk[16];
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(data + base + 64 * (uint64_t)b);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) blk[i] = w[i];  // zero-padded past len (little-endian words)
+    uint32_t blen = b + 1 == nblocks ? (uint32_t)(clen - 64 * (uint64_t)b) : 64u;
+    uint32_t flags = (b == 0 ? CHUNK_START : 0u) | (b + 1 == nblocks ? CHUNK_END : 0u);
+    if (nch == 1 && b + 1 == nblocks) flags |= ROOT;
+    uint32_t o[8];
+    b3_compress(cv, blk, c, blen, flags, o);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) cv[i] = o[i];
+  }
+  if (nch == 1) {
+    for (int i = 0; i < 8; ++i) root[i] = cv[i];
+  } else {
+    for (int i = 0; i < 8; ++i) cvs[8 * c + i] = cv[i];
+  }
+}
+// One tree level: node t of the next level is parent(2t, 2t+1), or node 2t carried up.
+__global__ void k_b3_parents(uint32_t n_in, const uint32_t* __restrict__ in, uint32_t* out, uint32_t* root) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t n_out = (n_in + 1) / 2;
+  if (t >= n_out) return;
+  if (2 * t + 1 < n_in) {
+    uint32_t blk[16];
+    for (int i = 0; i < 8; ++i) { blk[i] = in[16 * t + i]; blk[8 + i] = in[16 * t + 8 + i]; }
+    uint32_t cv[8];
+    for (int i = 0; i < 8; ++i) cv[i] = c_iv[i];
+    uint32_t o[8];
+    b3_compress(cv, blk, 0, 64, PARENT | (n_in == 2 ? ROOT : 0u), o);
+    uint32_t* dst = n_in == 2 ? root : out + 8 * t;
+    for (int i = 0; i < 8; ++i) dst[i] = o[i];
+  } else {
+    for (int i = 0; i < 8; ++i) out[8 * t + i] = in[16 * t + i];
+  }
+}
+
+// ---- stream writers
+__device__ __forceinline__ void put32(uint8_t* p, uint32_t v) {
+  p[0] = (uint8_t)v; p[1] = (uint8_t)(v >> 8); p[2] = (uint8_t)(v >> 16); p[3] = (uint8_t)(v >> 24);
+}
+__device__ __forceinline__ void put64(uint8_t* p, uint64_t v) { put32(p, (uint32_t)v); put32(p + 4, (uint32_t)(v >> 32)); }
+__global__ void k_h_bodies(uint32_t nb, const float4* __restrict__ pos, const float4* __restrict__ rot,
+                           const float4* __restrict__ lin, const float4* __restrict__ ang, uint8_t* out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  uint8_t* p = out + 56 * (size_t)i;
+  float4 a = pos[i], q = rot[i], l = lin[i], w = ang[i];
+  put32(p, i);
+  put32(p + 4, canon_bits(a.x)); put32(p + 8, canon_bits(a.y)); put32(p + 12, canon_bits(a.z));
+  put32(p + 16, canon_bits(q.x)); put32(p + 20, canon_bits(q.y)); put32(p + 24, canon_bits(q.z)); put32(p + 28, canon_bits(q.w));
+  put32(p + 32, canon_bits(l.x)); put32(p + 36, canon_bits(l.y)); put32(p + 40, canon_bits(l.z));
+  put32(p + 44, canon_bits(w.x)); put32(p + 48, canon_bits(w.y)); put32(p + 52, canon_bits(w.z));
+}
+__global__ void k_h_warm_flags(uint32_t n, const uint4* __restrict__ k, uint32_t* flag) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  bool first = e == 0;
+  if (!first) { uint4 a = k[e], b = k[e - 1]; first = !(a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w); }
+  flag[e] = first ? 1u : 0u;
+}
+// Entry e of group g sits after g+1 group headers (20 bytes) and e entries (28 bytes).
+__global__ void k_h_warm(uint32_t n, const uint4* __restrict__ k, const float4* __restrict__ wa,
+                         const float4* __restrict__ wb, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ gs,
+                         uint8_t* out) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  uint32_t g = gs[e] + flag[e] - 1;
+  if (flag[e]) {
+    uint32_t cnt = 1;
+    while (e + cnt < n && !flag[e + cnt]) cnt++;
+    uint8_t* h = out + 20 * (size_t)g + 28 * (size_t)e;
+    uint4 key = k[e];
+    put32(h, key.x); put32(h + 4, key.y); put32(h + 8, key.z); put32(h + 12, key.w); put32(h + 16, cnt);
+  }
+  uint8_t* p = out + 20 * (size_t)(g + 1) + 28 * (size_t)e;
+  float4 a = wa[e], b = wb[e];
+  put32(p, canon_bits(a.x)); put32(p + 4, canon_bits(a.y)); put32(p + 8, canon_bits(a.z));
+  put32(p + 12, canon_bits(a.w));
+  put32(p + 16, canon_bits(b.x)); put32(p + 20, canon_bits(b.y)); put32(p + 24, canon_bits(b.z));
+}
+__global__ void k_h_tail(uint32_t nb, uint32_t cap, const float4* __restrict__ last, const uint8_t* __restrict__ awake,
+                         const uint16_t* __restrict__ ticks, uint8_t* out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  // [u64 nb][12 nb][u64 cap][cap][u64 cap][2 cap]
+  if (i == 0) put64(out, nb);
+  if (i < nb) {
+    float4 v = last[i];
+    uint8_t* p = out + 8 + 12 * (size_t)i;
+    put32(p, canon_bits(v.x)); put32(p + 4, canon_bits(v.y)); put32(p + 8, canon_bits(v.z));
+  }
+  uint8_t* a = out + 8 + 12 * (size_t)nb;
+  if (i == 0) put64(a, cap);
+  if (i < cap) a[8 + i] = awake[i];
+  uint8_t* t = a + 8 + cap;
+  if (i == 0) put64(t, cap);
+  if (i < cap) { uint16_t v = ticks[i]; t[8 + 2 * i] = (uint8_t)v; t[9 + 2 * i] = (uint8_t)(v >> 8); }
+}
+
+void WorldGpu::step_hash(uint8_t out32[32]) {
+  Scratch& S = *s_;
+  cudaStream_t st = stream_;
+  const int T = 256;
+  uint32_t cap = cap_b_ > nb_ ? cap_b_ : nb_;
+  // number of distinct warm keys
+  S.woff.ensure(n_warm + 1); S.wpos.ensure(n_warm + 1);
+  uint32_t nkeys = 0;
+  if (n_warm) {
+    k_h_warm_flags<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, S.woff.p);
+    nkeys = exclusive_scan_total(S, S.woff.p, S.wpos.p, n_warm, st);
+  }
+  uint64_t off_bodies = 48;
+  uint64_t off_warm = off_bodies + 56ull * nb_;
+  uint64_t off_tail = off_warm + 8 + 20ull * nkeys + 28ull * n_warm + 24;
+  uint64_t len = off_tail + 8 + 12ull * nb_ + 8 + cap + 8 + 2ull * cap;
+  uint32_t nch = (uint32_t)((len + 1023) / 1024);
+  S.hbuf.ensure((size_t)nch * 1024 + 64);
+  RP_CUDA(cudaMemsetAsync(S.hbuf.p, 0, (size_t)nch * 1024 + 64, st));
+  uint8_t head[48];
+  auto p64 = [&](uint8_t* p, uint64_t v) { for (int i = 0; i < 8; ++i) p[i] = (uint8_t)(v >> (8 * i)); };
+  p64(head, epoch_);
+  p64(head + 8, rng_);
+  static const uint8_t kEmpty[32] = {0xaf, 0x13, 0x49, 0xb9, 0xf5, 0xf9, 0xa1, 0xa6, 0xa0, 0x40, 0x4d,
+                                     0xea, 0x36, 0xdc, 0xc9, 0x49, 0x9b, 0xcb, 0x25, 0xc9, 0xad, 0xc1,
+                                     0x12, 0xb7, 0xcc, 0x9a, 0x93, 0xca, 0xe4, 0x1f, 0x32, 0x62};
+  std::memcpy(head + 16, kEmpty, 32);
+  RP_CUDA(cudaMemcpyAsync(S.hbuf.p, head, 48, cudaMemcpyHostToDevice, st));
+  if (nb_) k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, S.hbuf.p + off_bodies);
+  uint8_t wcount[8];
+  p64(wcount, nkeys);
+  RP_CUDA(cudaMemcpyAsync(S.hbuf.p + off_warm, wcount, 8, cudaMemcpyHostToDevice, st));
+  if (n_warm)
+    k_h_warm<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, warm_a.p, warm_b.p, S.woff.p, S.wpos.p,
+                                                  S.hbuf.p + off_warm + 8);
+  // the three zero-length maps are already zero bytes
+  uint32_t nt = cap > nb_ ? cap : nb_;
+  k_h_tail<<<(nt + T) / T, T, 0, st>>>(nb_, cap, last_lin.p, awake.p, sleep_ticks.p, S.hbuf.p + off_tail);
+  S.hcv.ensure(16 * (size_t)nch + 16);
+  uint32_t* root = S.hcv.p;
+  uint32_t* a = S.hcv.p + 8;
+  uint32_t* b = S.hcv.p + 8 + 8 * (size_t)nch;
+  k_b3_chunks<<<(nch + 127) / 128, 128, 0, st>>>(S.hbuf.p, len, nch, a, root);
+  uint32_t n = nch;
+  while (n > 1) {
+    uint32_t n_out = (n + 1) / 2;
+    k_b3_parents<<<(n_out + 127) / 128, 128, 0, st>>>(n, a, b, root);
+    std::swap(a, b);
+    n = n_out;
+  }
+  uint32_t r[8];
+  RP_CUDA(cudaMemcpyAsync(r, root, 32, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < 8; ++i)
+    for (int k = 0; k < 4; ++k) out32[4 * i + k] = (uint8_t)(r[i] >> (8 * k));
+}
+
+}  // namespace rp

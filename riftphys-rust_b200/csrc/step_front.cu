@@ -1,0 +1,465 @@
+// step_front.cu -- stages 1 and 2 of the tick on the GPU: forces, AABBs and swept AABBs,
+// the sweep-and-prune broadphase, pair and terrain narrowphase, contact culling and orientation.
+// Reference: riftphys-world/src/world/step.rs:53-150, 499-542; broadphase.rs:29-99;
+// narrowphase.rs; terrain.rs:300-358.
+#include <cub/cub.cuh>
+
+#include "rp_narrow.cuh"
+#include "step_internal.cuh"
+
+namespace rp {
+
+// ------------------------------------------------------------------ stage 1
+// Stage 1 forces (step.rs:55-68): snapshot the start-of-step velocities; v += q6(g) dt for
+// dynamic awake bodies (grav_eval Uniform, gravity.rs:79-87). One thread per body.
+__global__ void k_forces(int nb, const float4* lin, const float4* __restrict__ ang,
+                         float4* lin_out, float4* pre_lin, float4* pre_ang,
+                         const uint8_t* __restrict__ dyn, const uint8_t* __restrict__ awake, f3 g, float dt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  float4 l = lin[i];
+  pre_lin[i] = l;
+  pre_ang[i] = ang[i];
+  if (!dyn[i] || !awake[i]) return;
+  f3 nl = xyz(l) + g * dt;
+  if (vfin(nl)) lin_out[i] = f4(fin_v(nl), l.w);  // Bodies::set_vel (dynamics.rs:141-145)
+}
+
+// aabb_of (shape.rs:7-56) with Aabb::new's 1e-6 quantisation (aabb.rs:21-26)
+__device__ __forceinline__ void aabb_of(uint32_t kind, float4 d, f3 p, q4 q, f3* mn, f3* mx) {
+  f3 he;
+  if (kind == SH_SPHERE) he = splat(fabsf(d.x));
+  else if (kind == SH_BOX) {
+    m3 r = mfrom_quat(q);
+    m3 ar = mcols(vabs(r.c0), vabs(r.c1), vabs(r.c2));
+    he = mvec(ar, mk3(fabsf(d.x), fabsf(d.y), fabsf(d.z)));
+  } else {
+    f3 axis = qrot(q, mk3(0, 1, 0)) * fabsf(d.y);
+    he = vabs(axis) + splat(fabsf(d.x));
+  }
+  f3 a = p - he, b = p + he;
+  a = mk3(qf32(a.x), qf32(a.y), qf32(a.z));
+  b = mk3(qf32(b.x), qf32(b.y), qf32(b.z));
+  *mn = vmin(a, b);
+  *mx = vmax(a, b);
+}
+
+// update_colliders_aabb (world.rs:793-798) + the swept, margin-inflated box (step.rs:75-81):
+// s = 0.05 + (|v| + |w| reach) dt, reach = half the AABB diagonal (world.rs:97-100).
+// Also classifies each collider for the broadphase (broadphase.rs:36-47): 0 = skipped
+// (non-finite min.x), 1 = in the grid, 2 = oversized (> 5 cells on an axis).
+__global__ void k_aabbs(int ncol, const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ ckind,
+                        const float4* __restrict__ cdims, const float4* __restrict__ pos, const float4* __restrict__ rot,
+                        const float4* __restrict__ lin, const float4* __restrict__ ang, float dt,
+                        float4* amin, float4* amax, float4* smin, float4* smax, float* sweep,
+                        uint32_t* sap_flag, uint32_t* over_flag, uint32_t* err) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  uint32_t b = cbody[c];
+  f3 mn, mx;
+  aabb_of(ckind[c], cdims[c], xyz(pos[b]), asq(rot[b]), &mn, &mx);
+  amin[c] = f4(mn);
+  amax[c] = f4(mx);
+  float reach = 0.5f * len(mx - mn);
+  float s = 0.05f + (len(xyz(lin[b])) + len(xyz(ang[b])) * reach) * dt;
+  sweep[c] = s;
+  f3 a = mn - splat(s), z = mx + splat(s);
+  smin[c] = f4(a);
+  smax[c] = f4(z);
+  uint32_t cls = 0;
+  if (fin(a.x)) {
+    float dx = z.x - a.x, dy = z.y - a.y, dz = z.z - a.z;
+    const float lim = 2.5f * 5.0f;
+    if (dx > lim || dy > lim || dz > lim) cls = 2;
+    else {
+      cls = 1;
+      if (!(fin(a.y) && fin(a.z) && fin(z.x) && fin(z.y) && fin(z.z))) atomicOr(err, 1u);
+    }
+  }
+  sap_flag[c] = cls == 1;
+  over_flag[c] = cls == 2;
+}
+
+// ------------------------------------------------------------------ broadphase
+__device__ __forceinline__ bool overlaps4(float4 amn, float4 amx, float4 bmn, float4 bmx) {
+  return !(amx.x < bmn.x || amn.x > bmx.x || amx.y < bmn.y || amn.y > bmx.y || amx.z < bmn.z || amn.z > bmx.z);
+}
+__device__ __forceinline__ uint32_t sortable(float f) {
+  uint32_t u = fbits(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__global__ void k_sap_keys(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ smin, uint32_t* keys) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) keys[k] = sortable(smin[ids[k]].x);
+}
+__global__ void k_gather_minx(int n, const uint32_t* __restrict__ order, const float4* __restrict__ smin, float* minx) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) minx[k] = smin[order[k]].x;
+}
+// Sweep along x over the sorted in-grid colliders: every overlapping pair once, counted by the
+// earlier of the two in sort order. The set equals the grid's (broadphase.rs:49-81): two
+// finite AABBs that overlap share the cell of any point of their intersection.
+template <bool EMIT>
+__global__ void k_sap_sweep(int n, const uint32_t* __restrict__ order, const float* __restrict__ minx,
+                            const float4* __restrict__ smin, const float4* __restrict__ smax,
+                            uint32_t* cnt, const uint32_t* __restrict__ off, unsigned long long* out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  uint32_t i = order[p];
+  float4 imn = smin[i], imx = smax[i];
+  uint32_t c = 0, o = EMIT ? off[p] : 0;
+  for (int q = p + 1; q < n; ++q) {
+    if (minx[q] > imx.x) break;
+    uint32_t j = order[q];
+    if (overlaps4(imn, imx, smin[j], smax[j])) {
+      if (EMIT) {
+        uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
+        out[o + c] = ((unsigned long long)lo << 32) | hi;
+      }
+      c++;
+    }
+  }
+  if (!EMIT) cnt[p] = c;
+}
+// Oversized colliders against every collider (broadphase.rs:83-92), one thread per collider.
+template <bool EMIT>
+__global__ void k_oversized(int ncol, int nover, const uint32_t* __restrict__ over, const float4* __restrict__ smin,
+                            const float4* __restrict__ smax, uint32_t* cnt, const uint32_t* __restrict__ off,
+                            unsigned long long* out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  float4 cmn = smin[c], cmx = smax[c];
+  uint32_t k = 0, o = EMIT ? off[c] : 0;
+  for (int t = 0; t < nover; ++t) {
+    uint32_t b = over[t];
+    if (b == (uint32_t)c) continue;
+    if (overlaps4(smin[b], smax[b], cmn, cmx)) {
+      if (EMIT) {
+        uint32_t lo = b < (uint32_t)c ? b : c, hi = b < (uint32_t)c ? c : b;
+        out[o + k] = ((unsigned long long)lo << 32) | hi;
+      }
+      k++;
+    }
+  }
+  if (!EMIT) cnt[c] = k;
+}
+__global__ void k_unique_flags(int n, const unsigned long long* __restrict__ a, uint8_t* flag) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) flag[k] = (k == 0 || a[k] != a[k - 1]) ? 1 : 0;
+}
+
+// ------------------------------------------------------------------ narrowphase
+// One thread per broadphase pair (step.rs:97-113): contact distance reach = s_i + s_j - 0.05;
+// depth = penetration - reach + 0.05. Up to 4 points in fixed slots.
+__global__ void k_narrow_pairs(int np, const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ cbody,
+                               const uint32_t* __restrict__ ckind, const float4* __restrict__ cdims,
+                               const float4* __restrict__ pos, const float4* __restrict__ rot,
+                               const float* __restrict__ sweep, float4* out_pt, float4* out_n, uint32_t* out_cnt) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  unsigned long long key = pairs[p];
+  uint32_t i = (uint32_t)(key >> 32), j = (uint32_t)key;
+  uint32_t ba = cbody[i], bb = cbody[j];
+  uint32_t cnt = 0;
+  if (ba != bb) {
+    float reach = sweep[i] + sweep[j] - 0.05f;
+    float4 da = cdims[i], db = cdims[j];
+    Shape sa; sa.kind = ckind[i]; sa.a = da.x; sa.b = da.y; sa.c = da.z;
+    Shape sb; sb.kind = ckind[j]; sb.a = db.x; sb.b = db.y; sb.c = db.z;
+    Iso xa; xa.pos = xyz(pos[ba]); xa.rot = asq(rot[ba]);
+    Iso xb; xb.pos = xyz(pos[bb]); xb.rot = asq(rot[bb]);
+    Manifold m;
+    if (collide_pair(sa, xa, sb, xb, reach, &m)) {
+      for (int k = 0; k < m.len; ++k) {
+        out_pt[4 * p + k] = f4(m.pts[k].position, (m.pts[k].penetration - reach) + 0.05f);
+        out_n[4 * p + k] = f4(m.pts[k].normal);
+      }
+      cnt = m.len;
+    }
+  }
+  out_cnt[p] = cnt;
+}
+
+// HeightField::query_aabb (terrain.rs:300-358): the cell window of an AABB.
+__device__ __forceinline__ long sat_i32(float f) {
+  if (isnan(f)) return 0;
+  if (f >= 2147483647.0f) return 2147483647L;
+  if (f <= -2147483648.0f) return -2147483648L;
+  return (long)f;
+}
+__device__ __forceinline__ bool hf_window(const HFView& hf, f3 mn, f3 mx, int* gx0, int* gx1, int* gz0, int* gz1) {
+  int nx = (int)hf.nx, nz = (int)hf.nz;
+  if (nx < 2 || nz < 2) return false;
+  float lminx = mn.x - hf.ox, lmaxx = mx.x - hf.ox, lminz = mn.z - hf.oz, lmaxz = mx.z - hf.oz;
+  long a = sat_i32(floorf(lminx / hf.sx)) - 1, b = sat_i32(ceilf(lmaxx / hf.sx)) + 1;
+  long c = sat_i32(floorf(lminz / hf.sz)) - 1, d = sat_i32(ceilf(lmaxz / hf.sz)) + 1;
+  *gx0 = (int)(a < 0 ? 0 : (a > nx - 2 ? nx - 2 : a));
+  *gx1 = (int)(b < 0 ? 0 : (b > nx - 2 ? nx - 2 : b));
+  *gz0 = (int)(c < 0 ? 0 : (c > nz - 2 ? nz - 2 : c));
+  *gz1 = (int)(d < 0 ? 0 : (d > nz - 2 ? nz - 2 : d));
+  if (mn.y > hf.max_y + 1.0f || mx.y < hf.min_y - 1.0f) return false;
+  return true;
+}
+__device__ __forceinline__ Tri hf_tri(const HFView& hf, int gx, int gz, int which) {
+  float h00 = hf.h[(size_t)gx + (size_t)gz * hf.nx], h10 = hf.h[(size_t)(gx + 1) + (size_t)gz * hf.nx];
+  float h01 = hf.h[(size_t)gx + (size_t)(gz + 1) * hf.nx], h11 = hf.h[(size_t)(gx + 1) + (size_t)(gz + 1) * hf.nx];
+  float x0 = (float)gx * hf.sx + hf.ox, x1 = x0 + hf.sx;
+  float z0 = (float)gz * hf.sz + hf.oz, z1 = z0 + hf.sz;
+  Tri t;
+  if (which == 0) { t.a = mk3(x0, h00, z0); t.b = mk3(x0, h01, z1); t.c = mk3(x1, h10, z0); }
+  else { t.a = mk3(x1, h10, z0); t.b = mk3(x0, h01, z1); t.c = mk3(x1, h11, z1); }
+  return t;
+}
+
+// Terrain contacts of one collider (step.rs:121-141) culled to its bucket of at most 4
+// (cull_and_orient_contacts, step.rs:508-530): the raw points in query order (gz outer, gx inner,
+// two triangles per cell, manifold order) are streamed; with more than 4, boxes keep
+// reduce_to_4 of all points on the deepest point's normal, spheres and capsules the 4 deepest
+// by 1e-6 key, earlier first on ties. reduce_to_4's four argmax passes re-run the query.
+__global__ void k_terrain(int ncol, HFView hf, const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ ckind,
+                          const float4* __restrict__ cdims, const float4* __restrict__ pos, const float4* __restrict__ rot,
+                          const float* __restrict__ sweep, const float4* __restrict__ amin, const float4* __restrict__ amax,
+                          float4* out_pt, float4* out_n, uint32_t* out_cnt) {
+  int ci = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= ncol) return;
+  uint32_t b = cbody[ci];
+  int gx0, gx1, gz0, gz1;
+  out_cnt[ci] = 0;
+  if (!hf_window(hf, xyz(amin[ci]), xyz(amax[ci]), &gx0, &gx1, &gz0, &gz1)) return;
+  float4 d = cdims[ci];
+  Shape s; s.kind = ckind[ci]; s.a = d.x; s.b = d.y; s.c = d.z;
+  Iso x; x.pos = xyz(pos[b]); x.rot = asq(rot[b]);
+  float cd = sweep[ci];
+  // pass 0: count, first 4 raw, top-4 by key (stable) for spheres/capsules, argmax depth for boxes
+  int total = 0;
+  float4 first_pt[4], first_n[4];
+  float4 top_pt[4], top_n[4]; long long top_k[4]; int ntop = 0;
+  long long best0 = LLONG_MIN; f3 p0 = mk3(0, 0, 0), nd = mk3(0, 0, 0);
+  for (int gz = gz0; gz <= gz1; ++gz)
+    for (int gx = gx0; gx <= gx1; ++gx)
+      for (int w = 0; w < 2; ++w) {
+        Tri t = hf_tri(hf, gx, gz, w);
+        Manifold m;
+        if (!collide_tri(s, x, t, cd, &m)) continue;
+        for (int k = 0; k < m.len; ++k) {
+          float depth = (m.pts[k].penetration - cd) + 0.05f;
+          float4 P = f4(m.pts[k].position, depth), N = f4(m.pts[k].normal);
+          if (total < 4) { first_pt[total] = P; first_n[total] = N; }
+          long long key = sort_key6(depth);
+          if (s.kind == SH_BOX) {
+            if (key > best0) { best0 = key; p0 = m.pts[k].position; nd = m.pts[k].normal; }
+          } else {
+            // insert into the descending top-4, after equal keys (stable)
+            int at = ntop;
+            while (at > 0 && top_k[at - 1] < key) at--;
+            if (at < 4) {
+              int last = ntop < 4 ? ntop : 3;
+              for (int q = last; q > at; --q) { top_k[q] = top_k[q - 1]; top_pt[q] = top_pt[q - 1]; top_n[q] = top_n[q - 1]; }
+              top_k[at] = key; top_pt[at] = P; top_n[at] = N;
+              if (ntop < 4) ntop++;
+            }
+          }
+          total++;
+        }
+      }
+  if (total <= 4) {
+    for (int k = 0; k < total; ++k) { out_pt[4 * ci + k] = first_pt[k]; out_n[4 * ci + k] = first_n[k]; }
+    out_cnt[ci] = total;
+    return;
+  }
+  if (s.kind != SH_BOX) {
+    for (int k = 0; k < 4; ++k) { out_pt[4 * ci + k] = top_pt[k]; out_n[4 * ci + k] = top_n[k]; }
+    out_cnt[ci] = 4;
+    return;
+  }
+  // boxes: reduce_to_4 (narrowphase.rs:312-338) over all raw points, normal = deepest point's
+  float4 selp[4], seln[4]; int nsel = 0;
+  long long bk; int bi, idx;
+  f3 p1 = mk3(0, 0, 0), e = mk3(0, 0, 0); float s2 = 0.0f;
+  for (int pass = 0; pass < 4; ++pass) {
+    bk = LLONG_MIN; bi = 0; idx = 0;
+    float bv = -INFINITY; float4 bp = make_float4(0, 0, 0, 0), bn = make_float4(0, 0, 0, 0);
+    for (int gz = gz0; gz <= gz1; ++gz)
+      for (int gx = gx0; gx <= gx1; ++gx)
+        for (int w = 0; w < 2; ++w) {
+          Tri t = hf_tri(hf, gx, gz, w);
+          Manifold m;
+          if (!collide_tri(s, x, t, cd, &m)) continue;
+          for (int k = 0; k < m.len; ++k) {
+            f3 pt = m.pts[k].position;
+            float depth = (m.pts[k].penetration - cd) + 0.05f;
+            float v;
+            if (pass == 0) v = depth;
+            else if (pass == 1) v = len2(pt - p0);
+            else if (pass == 2) v = fabsf(dot(cross(pt - p0, e), nd));
+            else v = -dot(cross(pt - p0, e), nd) * s2;
+            long long key = sort_key6(v);
+            if (key > bk) { bk = key; bi = idx; bv = v; bp = f4(pt, depth); bn = f4(m.pts[k].normal); }
+            idx++;
+          }
+        }
+    if (pass == 0) { selp[nsel] = bp; seln[nsel] = bn; nsel++; p0 = xyz(bp); continue; }
+    if (pass == 1) {
+      if (!(bv > 1.0e-12f)) break;
+      selp[nsel] = bp; seln[nsel] = bn; nsel++; p1 = xyz(bp); e = p1 - p0; continue;
+    }
+    if (pass == 2) {
+      if (!(bv > 1.0e-12f)) break;
+      selp[nsel] = bp; seln[nsel] = bn; nsel++;
+      s2 = signum(dot(cross(xyz(bp) - p0, e), nd));
+      continue;
+    }
+    if (bv > 1.0e-12f) { selp[nsel] = bp; seln[nsel] = bn; nsel++; }
+  }
+  for (int k = 0; k < nsel; ++k) { out_pt[4 * ci + k] = selp[k]; out_n[4 * ci + k] = seln[k]; }
+  out_cnt[ci] = nsel;
+}
+
+// First pair index whose collider i is >= c, for every c in [0, ncol]: pair buckets of
+// collider c precede its terrain bucket in the BTreeMap order (step.rs:500-505).
+__global__ void k_pair_starts(int ncol, int np, const unsigned long long* __restrict__ pairs, uint32_t* pstart) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ncol) return;
+  unsigned long long key = (unsigned long long)c << 32;
+  int lo = 0, hi = np;
+  while (lo < hi) { int mid = (lo + hi) >> 1; if (pairs[mid] < key) lo = mid + 1; else hi = mid; }
+  pstart[c] = lo;
+}
+// Bucket counts in merged key order: pair p at p + i, terrain bucket of c at c + pstart[c+1].
+__global__ void k_bucket_counts(int np, int ncol, const unsigned long long* __restrict__ pairs,
+                                const uint32_t* __restrict__ pcnt, const uint32_t* __restrict__ tcnt,
+                                const uint32_t* __restrict__ pstart, uint32_t* bcnt) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < np) { uint32_t i = (uint32_t)(pairs[k] >> 32); bcnt[k + i] = pcnt[k]; }
+  else if (k < np + ncol) { int c = k - np; bcnt[c + pstart[c + 1]] = tcnt ? tcnt[c] : 0; }
+}
+// Scatter the culled contacts into solve order and orient pair normals from A's collider
+// centre toward B's (step.rs:532-540).
+__global__ void k_scatter_contacts(int np, int ncol, const unsigned long long* __restrict__ pairs,
+                                   const uint32_t* __restrict__ pcnt, const float4* __restrict__ ppt,
+                                   const float4* __restrict__ pn, const uint32_t* __restrict__ tcnt,
+                                   const float4* __restrict__ tpt, const float4* __restrict__ tn,
+                                   const uint32_t* __restrict__ pstart, const uint32_t* __restrict__ boff,
+                                   const uint32_t* __restrict__ cbody, const float4* __restrict__ pos,
+                                   uint32_t* c_a, uint32_t* c_b, float4* c_pt, float4* c_n) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < np) {
+    uint32_t i = (uint32_t)(pairs[k] >> 32), j = (uint32_t)pairs[k];
+    uint32_t o = boff[k + i], n = pcnt[k];
+    f3 pa = xyz(pos[cbody[i]]), pb = xyz(pos[cbody[j]]);
+    for (uint32_t q = 0; q < n; ++q) {
+      float4 nn = pn[4 * k + q];
+      f3 nv = xyz(nn);
+      if (dot(nv, pb - pa) < 0.0f) nv = -nv;
+      c_a[o + q] = i; c_b[o + q] = j;
+      c_pt[o + q] = ppt[4 * k + q];
+      c_n[o + q] = f4(nv, 0.0f);
+    }
+  } else if (k < np + ncol) {
+    int c = k - np;
+    if (!tcnt) return;
+    uint32_t o = boff[c + pstart[c + 1]], n = tcnt[c];
+    for (uint32_t q = 0; q < n; ++q) {
+      c_a[o + q] = c; c_b[o + q] = 0xFFFFFFFFu;
+      c_pt[o + q] = tpt[4 * c + q];
+      float4 nn = tn[4 * c + q];
+      c_n[o + q] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host driver
+void run_front(WorldGpu& W, StepCtx& ctx) {
+  auto& S = *W.s_;
+  cudaStream_t st = W.stream();
+  const int nb = (int)W.num_bodies(), ncol = (int)W.num_colliders();
+  const int T = 256;
+  // stage 1
+  if (nb > 0)
+    k_forces<<<(nb + T - 1) / T, T, 0, st>>>(nb, W.lin.p, W.ang.p, W.lin.p, S.pre_lin.p, S.pre_ang.p, W.dyn.p,
+                                              W.awake.p, ctx.g, ctx.dt);
+  // stage 2: AABBs, sweep, classification
+  S.amin.ensure(ncol); S.amax.ensure(ncol); S.smin.ensure(ncol); S.smax.ensure(ncol); S.sweep.ensure(ncol);
+  S.u32a.ensure(ncol + 1); S.u32b.ensure(ncol + 1);
+  if (ncol > 0)
+    k_aabbs<<<(ncol + T - 1) / T, T, 0, st>>>(ncol, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, W.lin.p,
+                                               W.ang.p, ctx.dt, S.amin.p, S.amax.p, S.smin.p, S.smax.p, S.sweep.p,
+                                               S.u32a.p, S.u32b.p, W.d_stats.p + STAT_ERR);
+  // broadphase: in-grid colliders sorted along x, oversized list
+  S.sap_ids.ensure(ncol + 1); S.over_ids.ensure(ncol + 1); S.counts.ensure(4);
+  uint32_t n_sap = 0, n_over = 0;
+  if (ncol > 0) {
+    select_flagged_iota(S, ncol, S.u32a.p, S.sap_ids.p, S.counts.p + 0, st);
+    select_flagged_iota(S, ncol, S.u32b.p, S.over_ids.p, S.counts.p + 1, st);
+    uint32_t hc[2];
+    cudaMemcpyAsync(hc, S.counts.p, 8, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    n_sap = hc[0]; n_over = hc[1];
+  }
+  S.sap_key.ensure(n_sap + 1); S.sap_key2.ensure(n_sap + 1); S.sap_ord.ensure(n_sap + 1); S.minx.ensure(n_sap + 1);
+  S.sap_cnt.ensure(n_sap + 1); S.sap_off.ensure(n_sap + 1);
+  S.ov_cnt.ensure(ncol + 1); S.ov_off.ensure(ncol + 1);
+  uint32_t n_sap_pairs = 0, n_ov_pairs = 0;
+  if (n_sap > 0) {
+    k_sap_keys<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.sap_key.p);
+    sort_pairs_u32(S, S.sap_key.p, S.sap_key2.p, S.sap_ids.p, S.sap_ord.p, n_sap, 0, 32, st);
+    k_gather_minx<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.smin.p, S.minx.p);
+    k_sap_sweep<false><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, S.sap_cnt.p,
+                                                           nullptr, nullptr);
+    n_sap_pairs = exclusive_scan_total(S, S.sap_cnt.p, S.sap_off.p, n_sap, st);
+  }
+  if (n_over > 0 && ncol > 0) {
+    k_oversized<false><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, S.ov_cnt.p,
+                                                          nullptr, nullptr);
+    n_ov_pairs = exclusive_scan_total(S, S.ov_cnt.p, S.ov_off.p, ncol, st);
+  }
+  uint32_t n_raw = n_sap_pairs + n_ov_pairs;
+  S.pairs.ensure(n_raw + 1); S.pairs2.ensure(n_raw + 1); S.flag8.ensure(n_raw + 1);
+  if (n_sap_pairs > 0)
+    k_sap_sweep<true><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, nullptr,
+                                                          S.sap_off.p, S.pairs2.p);
+  if (n_ov_pairs > 0)
+    k_oversized<true><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, nullptr,
+                                                         S.ov_off.p, S.pairs2.p + n_sap_pairs);
+  uint32_t np = 0;
+  if (n_raw > 0) {
+    sort_keys_u64(S, S.pairs2.p, S.pairs.p, n_raw, st);  // -> S.pairs
+    k_unique_flags<<<(n_raw + T - 1) / T, T, 0, st>>>(n_raw, S.pairs.p, S.flag8.p);
+    np = select_flagged_u64(S, S.pairs.p, S.flag8.p, S.pairs2.p, n_raw, st);
+    cudaMemcpyAsync(S.pairs.p, S.pairs2.p, sizeof(unsigned long long) * np, cudaMemcpyDeviceToDevice, st);
+  }
+  ctx.np = np;
+  W.n_pairs = np;
+  // narrowphase over pairs
+  S.p_pt.ensure(4 * (size_t)np + 4); S.p_n.ensure(4 * (size_t)np + 4); S.p_cnt.ensure(np + 1);
+  if (np > 0)
+    k_narrow_pairs<<<(np + 127) / 128, 128, 0, st>>>(np, S.pairs.p, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p,
+                                                    W.rot.p, S.sweep.p, S.p_pt.p, S.p_n.p, S.p_cnt.p);
+  // terrain
+  S.t_pt.ensure(4 * (size_t)ncol + 4); S.t_n.ensure(4 * (size_t)ncol + 4); S.t_cnt.ensure(ncol + 1);
+  bool terrain = ctx.hf.h != nullptr;
+  if (terrain && ncol > 0)
+    k_terrain<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, ctx.hf, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p,
+                                                 W.rot.p, S.sweep.p, S.amin.p, S.amax.p, S.t_pt.p, S.t_n.p, S.t_cnt.p);
+  // merge buckets in key order, scan, scatter
+  S.pstart.ensure(ncol + 2);
+  k_pair_starts<<<(ncol + 1 + T - 1) / T, T, 0, st>>>(ncol, np, S.pairs.p, S.pstart.p);
+  uint32_t nbk = np + ncol;
+  S.bcnt.ensure(nbk + 1); S.boff.ensure(nbk + 1);
+  uint32_t nc = 0;
+  if (nbk > 0) {
+    k_bucket_counts<<<(nbk + T - 1) / T, T, 0, st>>>(np, ncol, S.pairs.p, S.p_cnt.p, terrain ? S.t_cnt.p : nullptr,
+                                                    S.pstart.p, S.bcnt.p);
+    nc = exclusive_scan_total(S, S.bcnt.p, S.boff.p, nbk, st);
+  }
+  ctx.nc = nc;
+  W.n_contacts = nc;
+  S.c_a.ensure(nc + 1); S.c_b.ensure(nc + 1); S.c_pt.ensure(nc + 1); S.c_n.ensure(nc + 1);
+  if (nc > 0)
+    k_scatter_contacts<<<(nbk + T - 1) / T, T, 0, st>>>(np, ncol, S.pairs.p, S.p_cnt.p, S.p_pt.p, S.p_n.p,
+                                                       terrain ? S.t_cnt.p : nullptr, S.t_pt.p, S.t_n.p, S.pstart.p,
+                                                       S.boff.p, W.col_body.p, W.pos.p, S.c_a.p, S.c_b.p, S.c_pt.p,
+                                                       S.c_n.p);
+}
+
+}  // namespace rp

@@ -1,0 +1,125 @@
+// step_internal.cuh -- per-tick scratch buffers, the tick context, and the small set of
+// device-wide primitives (radix sort, scan, select) the pipeline uses.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "world_gpu.h"
+
+namespace rp {
+
+#define RP_CUDA(x)                                                                      \
+  do {                                                                                  \
+    cudaError_t e__ = (x);                                                              \
+    if (e__ != cudaSuccess)                                                             \
+      throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e__) + \
+                               " at " __FILE__ ":" + std::to_string(__LINE__));         \
+  } while (0)
+
+// d_stats slots
+enum : int {
+  STAT_ERR = 0,          // RPHYS_STATERR_* bits
+  STAT_WARM_MATCHED = 1,
+  STAT_BOUNCE = 2,
+  STAT_SWEEPS = 3,       // max sweeps over islands
+  STAT_RESID = 4,        // f32 bits of the max residual (non-negative: integer max is order-free)
+  STAT_SLEEPING = 5,
+  STAT_LEVELS = 6,
+  STAT_MAXBATCH = 7,
+  STAT_NISL = 8,
+  STAT_COUNT = 16
+};
+
+template <class T>
+void DBuf<T>::ensure(size_t n) {
+  if (n <= cap) return;
+  if (p) cudaFree(p);
+  size_t c = n < 16 ? 16 : n + n / 4;
+  RP_CUDA(cudaMalloc(&p, c * sizeof(T)));
+  cap = c;
+}
+template <class T>
+void DBuf<T>::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+}
+
+struct WorldGpu::Scratch {
+  // per body
+  DBuf<float4> pre_lin, pre_ang, orig_pos, orig_rot, pred_pos, pred_rot, split_l, split_a;
+  DBuf<float> Iw;
+  DBuf<uint8_t> constrained, loaded, ballistic, touching;
+  DBuf<uint32_t> uf, uf2, body_level, isl_of_root, root_mark;
+  // per collider
+  DBuf<float4> amin, amax, smin, smax;
+  DBuf<float> sweep;
+  DBuf<uint32_t> u32a, u32b, sap_ids, over_ids, sap_key, sap_key2, sap_ord, sap_cnt, sap_off, ov_cnt, ov_off, counts;
+  DBuf<float> minx;
+  // pairs and narrowphase
+  DBuf<unsigned long long> pairs, pairs2;
+  DBuf<uint8_t> flag8;
+  DBuf<float4> p_pt, p_n, t_pt, t_n;
+  DBuf<uint32_t> p_cnt, t_cnt, pstart, bcnt, boff;
+  // contacts
+  DBuf<uint32_t> c_a, c_b;
+  DBuf<float4> c_pt, c_n;  // c_pt.w = depth, c_n.w = impulse
+  // rows (solver.rs:47-87 ContactConstraint, the fields the configured path reads)
+  DBuf<uint2> r_ab;
+  DBuf<uint32_t> r_flags;
+  DBuf<float2> r_inv;
+  DBuf<float4> r_ra, r_rb, r_n, r_t1, r_t2, r_mu, r_la;
+  DBuf<float> acc_jn;
+  DBuf<float2> acc_jt;
+  DBuf<int> wm_idx;
+  // schedules
+  DBuf<uint32_t> row_isl, row_isl2, rows_sched, rows_sched2, isl_start, isl_cnt, level, lvl_cnt, lvl_off,
+      lvl_start, ord_main, ord_vs, ord_ps, lvl_off_vs, lvl_start_vs, lvl_off_ps, lvl_start_ps, nlev, nlev_vs, nlev_ps,
+      tmp32, tmp32b;
+  DBuf<unsigned long long> key64, key64b;
+  DBuf<uint32_t> lvl_hist, row_level;
+  // position pass
+  DBuf<float4> pc_la, pc_lb;
+  // warm cache build
+  DBuf<uint8_t> wflag;
+  DBuf<uint32_t> woff, wpos;
+  // hash
+  DBuf<uint8_t> hbuf;
+  DBuf<uint32_t> hcv;
+  // primitives' temporary storage
+  DBuf<uint8_t> cub_tmp;
+};
+
+// The heightfield as the terrain kernel reads it (HeightField, terrain.rs:13-21); h == nullptr: none.
+struct HFView { const float* h; uint32_t nx, nz; float sx, sz, ox, oz, min_y, max_y; };
+
+struct StepCtx {
+  float dt;
+  f3 g, up;
+  uint32_t np = 0, nc = 0, nisl = 0, nref_isl = 0, nsched = 0;
+  HFView hf{nullptr, 0, 0, 1, 1, 0, 0, 0, 0};
+  uint32_t hf_mat = 4;
+};
+
+// ---- primitives (step_prims.cu)
+void select_flagged_iota(WorldGpu::Scratch& S, int n, const uint32_t* flags, uint32_t* out, uint32_t* d_count,
+                         cudaStream_t st);
+uint32_t select_flagged_u64(WorldGpu::Scratch& S, const unsigned long long* in, const uint8_t* flags,
+                            unsigned long long* out, uint32_t n, cudaStream_t st);
+uint32_t select_flagged_u32(WorldGpu::Scratch& S, const uint32_t* in, const uint8_t* flags, uint32_t* out,
+                            uint32_t n, cudaStream_t st);
+void sort_pairs_u32(WorldGpu::Scratch& S, const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout,
+                    uint32_t n, int bit0, int bit1, cudaStream_t st);
+void sort_pairs_u64(WorldGpu::Scratch& S, const unsigned long long* kin, unsigned long long* kout, const uint32_t* vin,
+                    uint32_t* vout, uint32_t n, int bit0, int bit1, cudaStream_t st);
+void sort_keys_u64(WorldGpu::Scratch& S, const unsigned long long* kin, unsigned long long* kout, uint32_t n,
+                   cudaStream_t st);
+uint32_t exclusive_scan_total(WorldGpu::Scratch& S, const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t st);
+void exclusive_scan(WorldGpu::Scratch& S, const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t st);
+
+void run_front(WorldGpu& W, StepCtx& ctx);
+void run_solve(WorldGpu& W, StepCtx& ctx);
+
+}  // namespace rp

@@ -1,0 +1,1025 @@
+// step_solve.cu -- stages 3 to 7 of the tick on the GPU.
+//
+// Exactness argument. The reference solves contacts in level batches (solver.rs:621-642): a row's
+// level is one more than the last level of any awake dynamic body it writes, so the rows of one
+// level write disjoint bodies and batch order reproduces the serial Gauss-Seidel order bit for
+// bit (solver.rs:15-18). Every other order-dependent pass over contacts touches the same bodies
+// the same way -- warm-start application (:717-762), the ballistic test (step.rs:180-206), the
+// position projection (step.rs:447-497) -- so it runs on the same schedule; the two shock passes
+// (solver.rs:964-993, step.rs:450-456) sort rows by height first and get their own schedule.
+// Rows split into islands (connected through awake dynamic bodies); one warp owns an island and
+// walks its levels with __syncwarp between them, so no two warps ever touch the same body.
+#include <cub/cub.cuh>
+
+#include "step_internal.cuh"
+
+namespace rp {
+
+namespace {
+const int T = 256;
+inline int nblk(uint32_t n, int t = T) { return (int)((n + t - 1) / t); }
+}  // namespace
+
+// row flag bits
+enum : uint32_t { RF_TERRAIN = 1, RF_TOI = 4, RF_WA = 8, RF_WB = 16 };
+
+__device__ __forceinline__ m3 ld_m3(const float* p, uint32_t i) {
+  const float* q = p + 9 * (size_t)i;
+  return mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
+}
+__device__ __forceinline__ void st_m3(float* p, uint32_t i, const m3& m) {
+  float* q = p + 9 * (size_t)i;
+  q[0] = m.c0.x; q[1] = m.c0.y; q[2] = m.c0.z; q[3] = m.c1.x; q[4] = m.c1.y; q[5] = m.c1.z;
+  q[6] = m.c2.x; q[7] = m.c2.y; q[8] = m.c2.z;
+}
+
+// ------------------------------------------------------------------ islands (islands.rs:27-93)
+__device__ __forceinline__ uint32_t uf_find(uint32_t* p, uint32_t x) {
+  volatile uint32_t* vp = p;
+  while (true) {
+    uint32_t px = vp[x];
+    if (px == x) return x;
+    uint32_t ppx = vp[px];
+    if (ppx != px) atomicCAS(&p[x], px, ppx);  // path halving
+    x = px;
+  }
+}
+// Union by hooking the larger root under the smaller: each component's root is its least body.
+__device__ __forceinline__ void uf_union(uint32_t* p, uint32_t a, uint32_t b) {
+  while (true) {
+    uint32_t ra = uf_find(p, a), rb = uf_find(p, b);
+    if (ra == rb) return;
+    if (ra > rb) { uint32_t t = ra; ra = rb; rb = t; }
+    if (atomicCAS(&p[rb], rb, ra) == rb) return;
+  }
+}
+__global__ void k_iota(uint32_t n, uint32_t* p) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = i;
+}
+// mode 0: the reference's islands (bodies with inv_mass > 0, asleep or not, islands.rs:266-287);
+// mode 1: solve islands (bodies an impulse can move: awake and dynamic).
+__global__ void k_union_contacts(uint32_t nc, int mode, const uint32_t* __restrict__ c_a, const uint32_t* __restrict__ c_b,
+                                 const uint32_t* __restrict__ cbody, const float* __restrict__ inv_mass,
+                                 const uint8_t* __restrict__ awake, uint32_t* parent) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc || c_b[k] == 0xFFFFFFFFu) return;
+  uint32_t a = cbody[c_a[k]], b = cbody[c_b[k]];
+  bool da = inv_mass[a] > 0.0f, db = inv_mass[b] > 0.0f;
+  if (mode == 1) { da = da && awake[a]; db = db && awake[b]; }
+  if (da && db) uf_union(parent, a, b);
+}
+// route_to_island (islands.rs:316-345): the root each contact lands in, marked.
+__global__ void k_ref_island_marks(uint32_t nc, const uint32_t* __restrict__ c_a, const uint32_t* __restrict__ c_b,
+                                   const uint32_t* __restrict__ cbody, const float* __restrict__ inv_mass,
+                                   uint32_t* parent, uint32_t* mark) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  uint32_t a = cbody[c_a[k]];
+  bool da = inv_mass[a] > 0.0f, db = false;
+  uint32_t b = 0;
+  if (c_b[k] != 0xFFFFFFFFu) { b = cbody[c_b[k]]; db = inv_mass[b] > 0.0f; }
+  if (!da && !db) return;
+  mark[uf_find(parent, da ? a : b)] = 1;
+}
+
+// ------------------------------------------------------------------ rows
+// World inverse inertia per body, R I^-1 R^T (dynamics.rs:158-163), once per tick: rotations
+// don't change during the velocity solve, so every apply_angular_impulse reads the same matrix.
+__global__ void k_world_inertia(uint32_t nb, const float4* __restrict__ rot, const float* __restrict__ inv_mass,
+                                const float* __restrict__ inv_I, float* Iw) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  m3 m = inv_mass[i] == 0.0f ? mzero() : world_inertia(asq(rot[i]), ld_m3(inv_I, i));
+  st_m3(Iw, i, m);
+}
+
+__device__ __forceinline__ float eff_mass(float ia, float ib, const m3& IA, const m3& IB, f3 ra, f3 rb, f3 d) {
+  f3 ca = cross(ra, d), cb = cross(rb, d);
+  float k = ((ia + ib) + dot(ca, mvec(IA, ca))) + dot(cb, mvec(IB, cb));
+  return k > 1.0e-9f ? 1.0f / k : 0.0f;
+}
+// orthonormal_basis (riftphys-world/src/world/geom.rs:30-38)
+__device__ __forceinline__ void orthonormal_basis(f3 n, f3* t1, f3* t2) {
+  float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+  f3 base = (ax <= ay && ax <= az) ? mk3(1, 0, 0) : (ay <= az ? mk3(0, 1, 0) : mk3(0, 0, 1));
+  *t1 = normalize_or_zero(cross(base, n));
+  *t2 = cross(n, *t1);
+}
+
+struct RowsV {
+  uint2* ab; uint32_t* flags; float2* inv; float4 *ra, *rb, *n, *t1, *t2, *mu, *la;
+};
+struct BodiesV {
+  float4 *pos, *rot, *lin, *ang;
+  const float* inv_mass; const float* Iw; const float* inv_I; const uint8_t* awake; const uint8_t* dyn;
+};
+
+// Constraint pre-processing (solver.rs:494-590), one thread per contact. Also the anchors in
+// body A's frame (solver.rs:728-731) and the island of each row that has a movable body.
+__global__ void k_build_rows(uint32_t nc, float dt, const uint32_t* __restrict__ c_a, const uint32_t* __restrict__ c_b,
+                             const float4* __restrict__ c_pt, const float4* __restrict__ c_n,
+                             const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ cmat, uint32_t hf_mat,
+                             const float* __restrict__ ptab, BodiesV B, const float4* __restrict__ pre_lin,
+                             const float4* __restrict__ pre_ang, RowsV R, float* acc_jn, float2* acc_jt,
+                             const uint32_t* __restrict__ uf, uint32_t* row_root) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  bool terrain = c_b[k] == 0xFFFFFFFFu;
+  uint32_t ai = cbody[c_a[k]], bi = terrain ? 0 : cbody[c_b[k]];
+  bool a_aw = B.awake[ai] != 0, b_aw = terrain ? false : B.awake[bi] != 0;
+  float inv_a = a_aw ? B.inv_mass[ai] : 0.0f, inv_b = b_aw ? B.inv_mass[bi] : 0.0f;
+  m3 IA = inv_a > 0.0f ? ld_m3(B.Iw, ai) : mzero();
+  m3 IB = inv_b > 0.0f ? ld_m3(B.Iw, bi) : mzero();
+  uint32_t ma = cmat[c_a[k]], mb = terrain ? hf_mat : cmat[c_b[k]];
+  const float* pp = ptab + 5 * (ma * 14 + mb);
+  float4 cp = c_pt[k], cn = c_n[k];
+  f3 point = xyz(cp), n = xyz(cn);
+  f3 t1, t2;
+  orthonormal_basis(n, &t1, &t2);
+  f3 pa = xyz(B.pos[ai]);
+  f3 ra = point - pa;
+  f3 rb = terrain ? mk3(0, 0, 0) : point - xyz(B.pos[bi]);
+  float m_n = eff_mass(inv_a, inv_b, IA, IB, ra, rb, n);
+  float m_t1 = eff_mass(inv_a, inv_b, IA, IB, ra, rb, t1);
+  float m_t2 = eff_mass(inv_a, inv_b, IA, IB, ra, rb, t2);
+  float mu_s = pp[0], mu_k = pp[1], rest = pp[2], sv = rmax(pp[3], 1.0e-4f);
+  float pen = cp.w - 0.05f;
+  float bias = pen > 0.0f ? rmin(rmax(pen - 0.005f, 0.0f) * (0.05f / dt), 2.0f) : pen / dt;
+  // approach at mid-step (:538-544) and the restitution target (:569-588)
+  f3 val = xyz(pre_lin[ai]), vaa = xyz(pre_ang[ai]);
+  f3 vbl = terrain ? mk3(0, 0, 0) : xyz(pre_lin[bi]), vba = terrain ? mk3(0, 0, 0) : xyz(pre_ang[bi]);
+  float v_pre = dot((vbl + cross(vba, rb)) - (val + cross(vaa, ra)), n);
+  f3 va = xyz(B.lin[ai]) + cross(xyz(B.ang[ai]), ra);
+  f3 vb = terrain ? mk3(0, 0, 0) : xyz(B.lin[bi]) + cross(xyz(B.ang[bi]), rb);
+  float v_rel_n = 0.5f * (v_pre + dot(vb - va, n));
+  float rbias = 0.0f;
+  uint32_t flags = terrain ? RF_TERRAIN : 0u;
+  if (v_rel_n < -1.0f) { rbias = (-rest) * v_rel_n; flags |= RF_TOI; }  // no body is jointed
+  bool wa = inv_a > 0.0f, wb = !terrain && inv_b > 0.0f;
+  if (wa) flags |= RF_WA;
+  if (wb) flags |= RF_WB;
+  R.ab[k] = make_uint2(ai, bi);
+  R.flags[k] = flags;
+  R.inv[k] = make_float2(inv_a, inv_b);
+  R.ra[k] = f4(ra, m_n);
+  R.rb[k] = f4(rb, m_t1);
+  R.n[k] = f4(n, m_t2);
+  R.t1[k] = f4(t1, bias);
+  R.t2[k] = f4(t2, rbias);
+  R.mu[k] = make_float4(mu_s, mu_k, sv, 0.0f);
+  R.la[k] = f4(qrot(qconj(asq(B.rot[ai])), point - pa));
+  acc_jn[k] = 0.0f;
+  acc_jt[k] = make_float2(0.0f, 0.0f);
+  row_root[k] = (wa || wb) ? uf_find(const_cast<uint32_t*>(uf), wa ? ai : bi) : 0xFFFFFFFFu;
+}
+
+// ------------------------------------------------------------------ row math shared by passes
+struct Row {
+  uint32_t ai, bi, flags;
+  float inv_a, inv_b;
+  f3 ra, rb, n, t1, t2;
+  float m_n, m_t1, m_t2, mu_s, mu_k, sv, bias, rbias;
+};
+__device__ __forceinline__ Row ld_row(const RowsV& R, uint32_t k) {
+  Row r;
+  uint2 ab = R.ab[k];
+  r.ai = ab.x; r.bi = ab.y; r.flags = R.flags[k];
+  float2 iv = R.inv[k]; r.inv_a = iv.x; r.inv_b = iv.y;
+  float4 a = R.ra[k], b = R.rb[k], n = R.n[k], t1 = R.t1[k], t2 = R.t2[k], mu = R.mu[k];
+  r.ra = xyz(a); r.m_n = a.w; r.rb = xyz(b); r.m_t1 = b.w; r.n = xyz(n); r.m_t2 = n.w;
+  r.t1 = xyz(t1); r.bias = t1.w; r.t2 = xyz(t2); r.rbias = t2.w;
+  r.mu_s = mu.x; r.mu_k = mu.y; r.sv = mu.z;
+  return r;
+}
+__device__ __forceinline__ f3 rel_vel(const BodiesV& B, const Row& r) {
+  f3 va = xyz(B.lin[r.ai]) + cross(xyz(B.ang[r.ai]), r.ra);
+  f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : xyz(B.lin[r.bi]) + cross(xyz(B.ang[r.bi]), r.rb);
+  return vb - va;
+}
+// Bodies::apply_impulse / apply_angular_impulse (dynamics.rs:193-205) with the tick's R I^-1 R^T
+__device__ __forceinline__ void body_impulse(const BodiesV& B, uint32_t i, f3 j, f3 tau) {
+  float im = B.inv_mass[i];
+  if (im > 0.0f && vfin(j)) { float4 l = B.lin[i]; B.lin[i] = f4(fin_v(xyz(l) + j * im), l.w); }
+  if (B.inv_mass[i] > 0.0f && vfin(tau)) {
+    f3 dw = mvec(ld_m3(B.Iw, i), tau);
+    float4 a = B.ang[i];
+    B.ang[i] = f4(fin_v(xyz(a) + dw), a.w);
+  }
+}
+// apply_contact_impulse (solver.rs:455-464)
+__device__ __forceinline__ void contact_impulse(const BodiesV& B, const Row& r, f3 j) {
+  if (r.inv_a > 0.0f) { f3 nj = -j; body_impulse(B, r.ai, nj, cross(r.ra, nj)); }
+  if (r.inv_b > 0.0f) body_impulse(B, r.bi, j, cross(r.rb, j));
+}
+__device__ __forceinline__ float mu_dynamic(const Row& r, float slip) {  // solver.rs:429-431
+  float t = slip / r.sv;
+  return r.mu_k + (r.mu_s - r.mu_k) * exp_rp(-(t * t));
+}
+// Warm start of one matched row (solver.rs:749-760)
+__device__ __forceinline__ void warm_apply(const BodiesV& B, const Row& r, uint32_t k, float4 ea, float4 eb,
+                                           float* acc_jn, float2* acc_jt) {
+  float jn = ea.w;
+  f3 jt = xyz(eb);
+  acc_jn[k] = jn;
+  f3 imp = r.n * jn;
+  f3 v = rel_vel(B, r);
+  float a = dot(v, r.t1), b = dot(v, r.t2);
+  float mu = mu_dynamic(r, sqrtf(a * a + b * b));
+  f3 t = clamp_length_max(mk3(dot(jt, r.t1), dot(jt, r.t2), 0.0f), mu * jn);
+  acc_jt[k] = make_float2(t.x, t.y);
+  imp = imp + ((r.t1 * t.x) + (r.t2 * t.y));
+  contact_impulse(B, r, imp);
+}
+// One Gauss-Seidel update of a contact row (solver.rs:857-878); returns the row's residual.
+__device__ __forceinline__ float pgs_row(const BodiesV& B, const Row& r, uint32_t k, float* acc_jn, float2* acc_jt) {
+  float v_rel_n = dot(rel_vel(B, r), r.n);
+  float jn_raw = (r.bias - v_rel_n) * r.m_n;
+  float old_jn = acc_jn[k];
+  float new_jn = rmax(old_jn + jn_raw, 0.0f);
+  acc_jn[k] = new_jn;
+  contact_impulse(B, r, r.n * (new_jn - old_jn));
+  f3 vf = rel_vel(B, r);
+  float vt1 = dot(vf, r.t1), vt2 = dot(vf, r.t2);
+  float slip = sqrtf(vt1 * vt1 + vt2 * vt2);
+  float mu = mu_dynamic(r, slip);
+  float2 ot = acc_jt[k];
+  f3 old_t = mk3(ot.x, ot.y, 0.0f);
+  f3 new_t = clamp_length_max(old_t - mk3(vt1 * r.m_t1, vt2 * r.m_t2, 0.0f), mu * new_jn);
+  acc_jt[k] = make_float2(new_t.x, new_t.y);
+  f3 d = new_t - old_t;
+  contact_impulse(B, r, (r.t1 * d.x) + (r.t2 * d.y));
+  float res = 0.0f;
+  if (r.m_n > 0.0f) res = rmax(res, fabsf(new_jn - old_jn) / r.m_n);
+  if (r.m_t1 > 0.0f) res = rmax(res, fabsf(d.x) / r.m_t1);
+  if (r.m_t2 > 0.0f) res = rmax(res, fabsf(d.y) / r.m_t2);
+  return res;
+}
+
+// ------------------------------------------------------------------ warm matching
+// Keys (solver.rs:720-726): (body A, body B or u32::MAX, ordinal A, ordinal B); every body has
+// one collider, so both ordinals are 0.
+__device__ __forceinline__ uint4 row_key(uint32_t a, bool terrain, uint32_t b) {
+  return terrain ? make_uint4(a, 0xFFFFFFFFu, 0u, 0u) : make_uint4(a, b, 0u, 0u);
+}
+__device__ __forceinline__ bool key_lt(uint4 a, uint4 b) {
+  if (a.x != b.x) return a.x < b.x;
+  if (a.y != b.y) return a.y < b.y;
+  if (a.z != b.z) return a.z < b.z;
+  return a.w < b.w;
+}
+__device__ __forceinline__ bool key_eq(uint4 a, uint4 b) { return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w; }
+__device__ __forceinline__ uint32_t key_lower_bound(const uint4* keys, uint32_t n, uint4 k) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) { uint32_t mid = (lo + hi) >> 1; if (key_lt(keys[mid], k)) lo = mid + 1; else hi = mid; }
+  return lo;
+}
+// One thread per run of contacts sharing a key: the nearest unused cached anchor within 1 cm,
+// lowest index on ties (solver.rs:733-748). Records the entry index per contact (-1: cold).
+__global__ void k_warm_match(uint32_t nc, const uint2* __restrict__ ab, const uint32_t* __restrict__ flags,
+                             const float4* __restrict__ la, const uint4* __restrict__ wkey, const float4* __restrict__ wa,
+                             uint32_t nw, int* wm_idx, uint32_t* n_matched, uint32_t* err) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  uint2 x = ab[k];
+  uint4 key = row_key(x.x, flags[k] & RF_TERRAIN, x.y);
+  if (k > 0) {
+    uint2 y = ab[k - 1];
+    if (key_eq(row_key(y.x, flags[k - 1] & RF_TERRAIN, y.y), key)) return;  // not the run's first
+  }
+  uint32_t e0 = key_lower_bound(wkey, nw, key), e1 = e0;
+  while (e1 < nw && key_eq(wkey[e1], key)) e1++;
+  unsigned long long used = 0ull;
+  if (e1 - e0 > 64) { atomicOr(err, 2u); e1 = e0 + 64; }
+  const float tol2 = 0.01f * 0.01f;
+  uint32_t matched = 0;
+  for (uint32_t c = k; c < nc; ++c) {
+    if (c > k) {
+      uint2 z = ab[c];
+      if (!key_eq(row_key(z.x, flags[c] & RF_TERRAIN, z.y), key)) break;
+    }
+    f3 anchor = xyz(la[c]);
+    int best = -1; float bd = 0.0f;
+    for (uint32_t e = e0; e < e1; ++e) {
+      if (used & (1ull << (e - e0))) continue;
+      float d = len2(xyz(wa[e]) - anchor);
+      if (d <= tol2 && (best < 0 || d < bd)) { best = (int)e; bd = d; }
+    }
+    if (best >= 0) { used |= 1ull << (best - (int)e0); matched++; }
+    wm_idx[c] = best;
+  }
+  if (matched) atomicAdd(n_matched, matched);
+}
+// Matched rows with no movable body: their impulses are set, nothing moves (solver.rs:749-760).
+__global__ void k_warm_unscheduled(uint32_t nc, RowsV R, BodiesV B, const int* __restrict__ wm_idx,
+                                   const float4* __restrict__ wa, const float4* __restrict__ wb, float* acc_jn,
+                                   float2* acc_jt) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  uint32_t f = R.flags[k];
+  if (f & (RF_WA | RF_WB)) return;
+  int e = wm_idx[k];
+  if (e < 0) return;
+  Row r = ld_row(R, k);
+  warm_apply(B, r, k, wa[e], wb[e], acc_jn, acc_jt);
+}
+
+// ------------------------------------------------------------------ schedules
+// Rows of one island in the serial order `ord_in`; greedy levels as solver.rs:625-642, one
+// thread per island walking its rows in order. body_level entries of the island's bodies are
+// reset first, so islands never interfere.
+__global__ void k_levels(uint32_t nisl, const uint32_t* __restrict__ isl_start, const uint32_t* __restrict__ isl_cnt,
+                         const uint32_t* __restrict__ ord_in, const uint2* __restrict__ ab,
+                         const uint32_t* __restrict__ flags, uint32_t* body_level, unsigned long long* key_out,
+                         uint32_t* nlev, uint32_t* row_level) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nisl) return;
+  uint32_t s0 = isl_start[i], s1 = s0 + isl_cnt[i];
+  for (uint32_t s = s0; s < s1; ++s) {
+    uint32_t r = ord_in[s];
+    uint2 x = ab[r];
+    uint32_t f = flags[r];
+    if (f & RF_WA) body_level[x.x] = 0;
+    if (f & RF_WB) body_level[x.y] = 0;
+  }
+  uint32_t maxl = 0;
+  for (uint32_t s = s0; s < s1; ++s) {
+    uint32_t r = ord_in[s];
+    uint2 x = ab[r];
+    uint32_t f = flags[r];
+    uint32_t la = (f & RF_WA) ? body_level[x.x] : 0, lb = (f & RF_WB) ? body_level[x.y] : 0;
+    uint32_t t = la > lb ? la : lb;
+    if (f & RF_WA) body_level[x.x] = t + 1;
+    if (f & RF_WB) body_level[x.y] = t + 1;
+    key_out[s] = ((unsigned long long)i << 32) | t;
+    if (row_level) row_level[r] = t;
+    if (t + 1 > maxl) maxl = t + 1;
+  }
+  nlev[i] = maxl;
+}
+__global__ void k_plus1(uint32_t n, const uint32_t* __restrict__ a, uint32_t* b) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i] + 1;
+}
+// Level start positions per island (+ a sentinel at the island's end), and the global
+// per-level histogram (solver.rs:684-687's last_max_batch).
+__global__ void k_level_starts(uint32_t n, const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ lvl_off,
+                               const uint32_t* __restrict__ nlev, const uint32_t* __restrict__ isl_start,
+                               const uint32_t* __restrict__ isl_cnt, uint32_t* lvl_start, uint32_t* hist) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  unsigned long long k = keys[s];
+  uint32_t isl = (uint32_t)(k >> 32), L = (uint32_t)k;
+  if (s == 0 || keys[s - 1] != k) lvl_start[lvl_off[isl] + L] = s;
+  if (s == isl_start[isl]) lvl_start[lvl_off[isl] + nlev[isl]] = isl_start[isl] + isl_cnt[isl];
+  if (hist) atomicAdd(&hist[L], 1u);
+}
+__global__ void k_gather_u32(uint32_t n, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ src, uint32_t* dst) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[idx[i]];
+}
+
+struct Sched { uint32_t* ord; uint32_t* lvl_off; uint32_t* lvl_start; uint32_t* nlev; };
+
+// ------------------------------------------------------------------ island passes (warp per island)
+__device__ __forceinline__ float warp_max(float v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// Warm start application, then the velocity sweeps (solver.rs:717-915).
+__global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* acc_jn, float2* acc_jt,
+                            const int* __restrict__ wm_idx, const float4* __restrict__ wa, const float4* __restrict__ wb,
+                            int iters, float tol, uint32_t* stats) {
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nisl) return;
+  uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+  for (uint32_t L = 0; L < nl; ++L) {
+    uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+    for (uint32_t s = s0 + lane; s < s1; s += 32) {
+      uint32_t k = S.ord[s];
+      int e = wm_idx[k];
+      if (e >= 0) { Row r = ld_row(R, k); warm_apply(B, r, k, wa[e], wb[e], acc_jn, acc_jt); }
+    }
+    __syncwarp();
+  }
+  int it = 0;
+  float resid = 0.0f;
+  while (it < iters) {
+    resid = 0.0f;
+    for (uint32_t L = 0; L < nl; ++L) {
+      uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+      for (uint32_t s = s0 + lane; s < s1; s += 32) {
+        uint32_t k = S.ord[s];
+        Row r = ld_row(R, k);
+        resid = rmax(resid, pgs_row(B, r, k, acc_jn, acc_jt));
+      }
+      __syncwarp();
+    }
+    it++;
+    resid = warp_max(resid);
+    if (tol > 0.0f && resid <= tol) break;
+  }
+  if (lane == 0) {
+    atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
+    atomicMax(&stats[STAT_RESID], fbits(resid));
+  }
+}
+// Shock propagation (solver.rs:964-993): rows in (1e-6 height key, index) order, the lower body
+// of a two-body row frozen for its update.
+__global__ void k_vel_shock(uint32_t nisl, Sched S, RowsV R, BodiesV B, f3 up, float* acc_jn) {
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nisl) return;
+  uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+  for (uint32_t L = 0; L < nl; ++L) {
+    uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+    for (uint32_t s = s0 + lane; s < s1; s += 32) {
+      uint32_t k = S.ord[s];
+      Row r = ld_row(R, k);
+      m3 IA = r.inv_a > 0.0f ? ld_m3(B.Iw, r.ai) : mzero();
+      m3 IB = r.inv_b > 0.0f ? ld_m3(B.Iw, r.bi) : mzero();
+      if (r.inv_a > 0.0f && r.inv_b > 0.0f) {
+        if (dot(xyz(B.pos[r.ai]), up) < dot(xyz(B.pos[r.bi]), up)) { r.inv_a = 0.0f; IA = mzero(); }
+        else { r.inv_b = 0.0f; IB = mzero(); }
+        r.m_n = eff_mass(r.inv_a, r.inv_b, IA, IB, r.ra, r.rb, r.n);
+      }
+      float v = dot(rel_vel(B, r), r.n);
+      float old = acc_jn[k];
+      float nw = rmax(old + (r.bias - v) * r.m_n, 0.0f);
+      acc_jn[k] = nw;
+      contact_impulse(B, r, r.n * (nw - old));
+    }
+    __syncwarp();
+  }
+}
+// Shock keys (1e-6 units of the lower body's height; terrain rows -inf) as order-preserving u64.
+__global__ void k_shock_keys(uint32_t n, const uint32_t* __restrict__ rows, const uint2* __restrict__ ab,
+                             const uint32_t* __restrict__ flags, const float4* __restrict__ pos, f3 up,
+                             unsigned long long* keys) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t k = rows[i];
+  uint2 x = ab[k];
+  float h = (flags[k] & RF_TERRAIN) ? -INFINITY : rmin(dot(xyz(pos[x.x]), up), dot(xyz(pos[x.y]), up));
+  long long s = sort_key6(h);
+  keys[i] = (unsigned long long)s ^ 0x8000000000000000ull;
+}
+
+// Contact load flags (solver.rs:1248-1256), impulse write-back (:1268-1270), W6 rows counted.
+__global__ void k_after_solve(uint32_t nc, RowsV R, const float* __restrict__ acc_jn, const float2* __restrict__ acc_jt,
+                              uint8_t* loaded, float4* c_n, uint32_t* stats) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  uint2 x = R.ab[k];
+  uint32_t f = R.flags[k];
+  float jn = acc_jn[k];
+  float2 jt = acc_jt[k];
+  if (jn > 0.0f || jt.x != 0.0f || jt.y != 0.0f) {
+    loaded[x.x] = 1;
+    if (!(f & RF_TERRAIN)) loaded[x.y] = 1;
+  }
+  c_n[k].w = jn;
+  if ((f & RF_TOI) && R.t2[k].w > 0.0f && jn > 0.0f) atomicAdd(&stats[STAT_BOUNCE], 1u);
+}
+
+// ------------------------------------------------------------------ warm cache rebuild
+// solver.rs:917-944: the rows' impulses as the sweeps left them, keyed, in contact order; then
+// the old entries of pairs where neither body is awake and dynamic (and still alive).
+__global__ void k_warm_new_flags(uint32_t nc, RowsV R, const float* __restrict__ acc_jn, const float2* __restrict__ acc_jt,
+                                 uint32_t* flag) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  float2 t = acc_jt[k];
+  f3 jt = (xyz(R.t1[k]) * t.x) + (xyz(R.t2[k]) * t.y);
+  flag[k] = (acc_jn[k] == 0.0f && vzero(jt)) ? 0u : 1u;
+}
+__global__ void k_warm_new_write(uint32_t nc, RowsV R, const float* __restrict__ acc_jn, const float2* __restrict__ acc_jt,
+                                 const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off,
+                                 const uint32_t* __restrict__ okept_cnt_ptr, const uint4* __restrict__ okey, uint32_t n_okept,
+                                 uint4* nk, float4* na, float4* nbv) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc || !flag[k]) return;
+  uint2 x = R.ab[k];
+  uint4 key = row_key(x.x, R.flags[k] & RF_TERRAIN, x.y);
+  float2 t = acc_jt[k];
+  f3 jt = (xyz(R.t1[k]) * t.x) + (xyz(R.t2[k]) * t.y);
+  uint32_t pos = off[k] + key_lower_bound(okey, n_okept, key);
+  nk[pos] = key;
+  na[pos] = f4(xyz(R.la[k]), acc_jn[k]);
+  nbv[pos] = f4(jt);
+  (void)okept_cnt_ptr;
+}
+__device__ __forceinline__ bool idle_body(uint32_t b, const uint8_t* alive, const uint8_t* dyn, const uint8_t* awake, uint32_t nb) {
+  if (b == 0xFFFFFFFFu) return true;
+  if (b >= nb || !alive[b]) return false;
+  return !dyn[b] || !awake[b];
+}
+__global__ void k_warm_old_flags(uint32_t nw, const uint4* __restrict__ wk, const uint4* __restrict__ newk, uint32_t n_new,
+                                 const uint8_t* __restrict__ alive, const uint8_t* __restrict__ dyn,
+                                 const uint8_t* __restrict__ awake, uint32_t nb, uint8_t* flag) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nw) return;
+  uint4 k = wk[e];
+  bool keep = idle_body(k.x, alive, dyn, awake, nb) && idle_body(k.y, alive, dyn, awake, nb);
+  if (keep) {
+    uint32_t p = key_lower_bound(newk, n_new, k);
+    if (p < n_new && key_eq(newk[p], k)) keep = false;
+  }
+  flag[e] = keep ? 1 : 0;
+}
+
+// ------------------------------------------------------------------ stage 4: ballistic + integration
+__global__ void k_constrained(uint32_t nc, const uint32_t* __restrict__ c_a, const uint32_t* __restrict__ c_b,
+                              const uint32_t* __restrict__ cbody, uint8_t* constrained) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  constrained[cbody[c_a[k]]] = 1;
+  if (c_b[k] != 0xFFFFFFFFu) constrained[cbody[c_b[k]]] = 1;
+}
+__global__ void k_ballistic_init(uint32_t nb, const uint8_t* __restrict__ constrained, const uint8_t* __restrict__ loaded,
+                                 uint8_t* ballistic) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nb) ballistic[i] = (!constrained[i] || !loaded[i]) ? 1 : 0;
+}
+// step.rs:180-206 per contact, on the solve schedule. Flags of bodies that can't move are read
+// at their initial value and never written: for those last_lin_vel equals the velocity, so
+// their averaged motion equals their velocity, and their flag changes no movable body's outcome.
+__global__ void k_ballistic(uint32_t nisl, Sched S, RowsV R, BodiesV B, const float4* __restrict__ c_pt,
+                            const float4* __restrict__ c_n, const float4* __restrict__ last_lin, float dt,
+                            uint8_t* ballistic) {
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nisl) return;
+  uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+  for (uint32_t L = 0; L < nl; ++L) {
+    uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+    for (uint32_t s = s0 + lane; s < s1; s += 32) {
+      uint32_t k = S.ord[s];
+      uint2 x = R.ab[k];
+      uint32_t f = R.flags[k];
+      bool hb = !(f & RF_TERRAIN);
+      uint32_t a = x.x, b = x.y;
+      bool ba = ballistic[a] != 0, bb = hb ? ballistic[b] != 0 : false;
+      if (!ba && (!hb || !bb)) continue;
+      f3 point = xyz(c_pt[k]), n = xyz(c_n[k]);
+      f3 la = ba ? (xyz(last_lin[a]) + xyz(B.lin[a])) * 0.5f : xyz(B.lin[a]);
+      f3 wa = xyz(B.ang[a]);
+      f3 ra = point - xyz(B.pos[a]);
+      f3 lb = mk3(0, 0, 0), wb = mk3(0, 0, 0), rb = mk3(0, 0, 0);
+      if (hb) { lb = bb ? (xyz(last_lin[b]) + xyz(B.lin[b])) * 0.5f : xyz(B.lin[b]); wb = xyz(B.ang[b]); rb = point - xyz(B.pos[b]); }
+      float approach = dot((lb + cross(wb, rb)) - (la + cross(wa, ra)), n);
+      f3 vbl = hb ? xyz(B.lin[b]) : mk3(0, 0, 0), vba = hb ? xyz(B.ang[b]) : mk3(0, 0, 0);
+      float v_end = dot((vbl + cross(vba, rb)) - (xyz(B.lin[a]) + cross(xyz(B.ang[a]), ra)), n);
+      float s0v = -(c_pt[k].w - 0.05f);
+      if (s0v + (2.0f * v_end) * dt < 0.0f || s0v + approach * dt < 0.0f) {
+        if (f & RF_WA) ballistic[a] = 0;
+        if (f & RF_WB) ballistic[b] = 0;
+      }
+    }
+    __syncwarp();
+  }
+}
+// Position integration with the gyroscopic midpoint turn (step.rs:208-280), one thread per body.
+__global__ void k_integrate(uint32_t nb, BodiesV B, const uint8_t* __restrict__ ballistic,
+                            const float4* __restrict__ last_lin, float dt, float4* orig_pos, float4* orig_rot,
+                            float4* pred_pos, float4* pred_rot) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  float4 P = B.pos[i], Q = B.rot[i];
+  orig_pos[i] = P; orig_rot[i] = Q;
+  pred_pos[i] = P; pred_rot[i] = Q;
+  if (!B.dyn[i] || !B.awake[i]) return;
+  f3 pos = xyz(P); q4 rot = asq(Q);
+  float4 L = B.lin[i], A = B.ang[i];
+  f3 vl = xyz(L), va = xyz(A);
+  pos = pos + vl * dt;
+  if (ballistic[i]) pos = pos + (xyz(last_lin[i]) - vl) * (0.5f * dt);
+  if (len2(va) > 0.0f) {
+    m3 l = B.inv_mass[i] == 0.0f ? mzero() : world_inertia(rot, ld_m3(B.inv_I, i));
+    float det = mdet(l);
+    bool has_m = fin(det) && fabsf(det) > 1.0e-20f;
+    f3 m = has_m ? mvec(minverse(l), va) : mk3(0, 0, 0);
+    q4 start = rot;
+    // turn(q, w, h) = normalize(from_axis_angle(w / |w|, |w| h) * q), or q for |w|^2 <= 1e-18
+    {
+      f3 w = va;
+      if (!(len2(w) <= 1.0e-18f)) rot = qnormalize(qmul(qfrom_axis_angle(normalize(w), len(w) * dt), start));
+    }
+    if (has_m) {
+      m3 il = B.inv_mass[i] == 0.0f ? mzero() : ld_m3(B.inv_I, i);
+      float mean = ((il.c0.x + il.c1.y) + il.c2.z) / 3.0f;
+      m3 dev = msub(il, mdiag(splat(mean)));
+      bool principal = len(cross(m, va)) < (1.0e-5f * len(m)) * len(va);
+      float gain = principal ? 0.0f : (dt * rmax(rmax(len(dev.c0), len(dev.c1)), len(dev.c2))) * len(m);
+      float cq = ceilf(gain / 0.5f);
+      long long nn = isnan(cq) ? 0 : (cq <= 0.0f ? 0 : (cq >= 1.0e18f ? 1000000000000000000LL : (long long)cq));
+      int n = (int)(nn < 1 ? 1 : (nn > 256 ? 256 : nn));
+      float h = dt / (float)n;
+      q4 q = start;
+      f3 w = va;
+      for (int s = 0; s < n; ++s) {
+        q4 q0 = q;
+        q = len2(w) <= 1.0e-18f ? q0 : qnormalize(qmul(qfrom_axis_angle(normalize(w), len(w) * h), q0));
+        f3 we = mvec(world_inertia(q, il), m);
+        for (int r = 0; r < 2; ++r) {
+          f3 wm = (w + we) * 0.5f;
+          q = len2(wm) <= 1.0e-18f ? q0 : qnormalize(qmul(qfrom_axis_angle(normalize(wm), len(wm) * h), q0));
+          we = mvec(world_inertia(q, il), m);
+        }
+        w = we;
+      }
+      rot = q;
+      va = w;
+      if (vfin(vl)) B.lin[i] = f4(fin_v(vl), L.w);  // Bodies::set_vel
+      if (vfin(va)) B.ang[i] = f4(fin_v(va), A.w);
+    }
+  }
+  // Bodies::set_pose (dynamics.rs:130-134)
+  if (vfin(pos)) P = f4(fin_v(pos), P.w);
+  if (qfin(rot)) Q = f4q(fin_q(rot));
+  B.pos[i] = P; B.rot[i] = Q;
+  pred_pos[i] = P; pred_rot[i] = Q;
+}
+
+// ------------------------------------------------------------------ stage 5: position pass
+// pos_contacts (step.rs:423-443): body-local anchors at the start-of-step poses. Row k's A anchor
+// is R.la (the warm-start anchor, the same expression); B's is computed here.
+__global__ void k_pos_anchors(uint32_t nc, RowsV R, const float4* __restrict__ c_pt, const float4* __restrict__ orig_pos,
+                              const float4* __restrict__ orig_rot, float4* lb) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  uint32_t f = R.flags[k];
+  if (f & RF_TERRAIN) { lb[k] = make_float4(0, 0, 0, 0); return; }
+  uint32_t b = R.ab[k].y;
+  lb[k] = f4(qrot(qconj(asq(orig_rot[b])), xyz(c_pt[k]) - xyz(orig_pos[b])));
+}
+// One projection of contact k (step.rs:457-496).
+__device__ __forceinline__ void project_one(const BodiesV& B, const RowsV& R, uint32_t k, bool shock, f3 up,
+                                            const float4* __restrict__ c_pt, const float4* __restrict__ c_n,
+                                            const float4* __restrict__ lbv, float4* split_l, float4* split_a) {
+  uint2 x = R.ab[k];
+  uint32_t f = R.flags[k];
+  bool hb = !(f & RF_TERRAIN);
+  uint32_t a = x.x, b = x.y;
+  bool am = B.inv_mass[a] > 0.0f && B.awake[a];
+  bool bm = hb && B.inv_mass[b] > 0.0f && B.awake[b];
+  if (shock && am && bm) {
+    float ha = dot(xyz(B.pos[a]), up), hbb = dot(xyz(B.pos[b]), up);
+    if (ha < hbb) am = false; else bm = false;
+  }
+  f3 n = xyz(c_n[k]);
+  float4 cp = c_pt[k];
+  float pen0 = cp.w - 0.05f;
+  f3 pa_pos = xyz(B.pos[a]); q4 pa_rot = asq(B.rot[a]);
+  f3 wa = pa_pos + qrot(pa_rot, xyz(R.la[k]));
+  f3 pb_pos = mk3(0, 0, 0); q4 pb_rot = qident();
+  f3 wb;
+  if (hb) { pb_pos = xyz(B.pos[b]); pb_rot = asq(B.rot[b]); wb = pb_pos + qrot(pb_rot, xyz(lbv[k])); }
+  else wb = xyz(cp);
+  float pen = pen0 - dot(wb - wa, n);
+  float err = pen - 0.005f;
+  if (err <= 0.0f) return;
+  f3 ra = wa - pa_pos;
+  f3 rb = hb ? wb - pb_pos : mk3(0, 0, 0);
+  float ima = am ? B.inv_mass[a] : 0.0f;
+  m3 iia = am ? world_inertia(pa_rot, ld_m3(B.inv_I, a)) : mzero();
+  float imb = (hb && bm) ? B.inv_mass[b] : 0.0f;
+  m3 iib = (hb && bm) ? world_inertia(pb_rot, ld_m3(B.inv_I, b)) : mzero();
+  f3 ca = cross(ra, n), cb = cross(rb, n);
+  float w = ((ima + imb) + dot(ca, mvec(iia, ca))) + dot(cb, mvec(iib, cb));
+  if (w <= 1.0e-9f) return;
+  float lambda = err / w;
+  // move_body (step.rs:484-491)
+  auto move_body = [&](uint32_t id, f3 ppos, q4 prot, float im, const m3& ii, f3 r, f3 j) {
+    f3 dth = mvec(ii, cross(r, j));
+    float4 sl = split_l[id], sa = split_a[id];
+    split_l[id] = f4(xyz(sl) + j * im);
+    split_a[id] = f4(xyz(sa) + dth);
+    q4 dq = qscale(qmul(mkq(dth.x, dth.y, dth.z, 0.0f), prot), 0.5f);
+    q4 nr = qnormalize(mkq(prot.x + dq.x, prot.y + dq.y, prot.z + dq.z, prot.w + dq.w));
+    f3 np = ppos + j * im;
+    float4 P = B.pos[id];
+    if (vfin(np)) B.pos[id] = f4(fin_v(np), P.w);
+    if (qfin(nr)) B.rot[id] = f4q(fin_q(nr));
+  };
+  if (am) move_body(a, pa_pos, pa_rot, ima, iia, ra, (-n) * lambda);
+  if (hb && bm) move_body(b, pb_pos, pb_rot, imb, iib, rb, n * lambda);
+}
+__global__ void k_pos_iterations(uint32_t nisl, Sched S, RowsV R, BodiesV B, int iters, int shock, f3 up,
+                                 const float4* __restrict__ c_pt, const float4* __restrict__ c_n,
+                                 const float4* __restrict__ lbv, float4* split_l, float4* split_a) {
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nisl) return;
+  uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+  for (int it = 0; it < iters; ++it) {
+    for (uint32_t L = 0; L < nl; ++L) {
+      uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+      for (uint32_t s = s0 + lane; s < s1; s += 32)
+        project_one(B, R, S.ord[s], shock != 0, up, c_pt, c_n, lbv, split_l, split_a);
+      __syncwarp();
+    }
+  }
+}
+
+// ------------------------------------------------------------------ stages 6 and 7
+__global__ void k_touching(uint32_t nc, const uint32_t* __restrict__ c_a, const uint32_t* __restrict__ c_b,
+                           const float4* __restrict__ c_pt, const uint32_t* __restrict__ cbody, uint8_t* touching) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc || c_b[k] != 0xFFFFFFFFu) return;
+  if (c_pt[k].w - 0.05f > -0.005f) touching[cbody[c_a[k]]] = 1;  // no compliant pairs
+}
+// Velocity from corrections (step.rs:316-376), last velocities (:378-379), sleep (sleep.rs:59-80).
+__global__ void k_stage6(uint32_t nb, BodiesV B, const float4* __restrict__ orig_pos, const float4* __restrict__ pred_pos,
+                         const float4* __restrict__ pred_rot, const float4* __restrict__ split_l,
+                         const float4* __restrict__ split_a, const uint8_t* __restrict__ touching, float dt,
+                         float4* last_lin, uint8_t* awake, uint16_t* sleep_ticks, const uint8_t* __restrict__ sleep_allowed,
+                         uint32_t* stats) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nb) return;
+  float4 L = B.lin[i], A = B.ang[i];
+  if (B.dyn[i] && awake[i]) {
+    f3 vl = xyz(L), va = xyz(A);
+    float4 P = B.pos[i];
+    f3 np = xyz(P);
+    q4 nr = asq(B.rot[i]);
+    f3 d_lin = (np - xyz(pred_pos[i])) - xyz(split_l[i]);
+    if (!vzero(d_lin)) vl = vl + d_lin / dt;
+    if (touching[i] && vl.y < 0.0f) {
+      vl.y = 0.0f;
+      np.y = orig_pos[i].y;
+      if (vfin(np)) B.pos[i] = f4(fin_v(np), P.w);
+      if (qfin(nr)) B.rot[i] = f4q(fin_q(nr));
+    }
+    q4 pr = asq(pred_rot[i]);
+    if (!qeq(nr, pr)) {
+      q4 dq = qmul(nr, qconj(pr));
+      f3 d_ang = mk3(dq.x, dq.y, dq.z) * 2.0f;
+      if (dq.w < 0.0f) d_ang = -d_ang;
+      va = va + (d_ang - xyz(split_a[i])) / dt;
+    }
+    if (vfin(vl)) L = f4(fin_v(vl), L.w);
+    if (vfin(va)) A = f4(fin_v(va), A.w);
+    B.lin[i] = L; B.ang[i] = A;
+  }
+  last_lin[i] = L;
+  if (sleep_allowed[i] && awake[i] && B.dyn[i]) {
+    if (len2(xyz(L)) < 0.01f && len2(xyz(A)) < 0.01f) {
+      uint16_t t = (uint16_t)(sleep_ticks[i] + 1);
+      sleep_ticks[i] = t;
+      if (t > 30) awake[i] = 0;
+    } else {
+      sleep_ticks[i] = 0;
+    }
+  }
+}
+__global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, uint32_t* stats) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t v = (i < n && awake[i] == 0) ? 1u : 0u;
+  v = __reduce_add_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(&stats[STAT_SLEEPING], v);
+}
+
+// ------------------------------------------------------------------ small helpers
+__global__ void k_flag_sched(uint32_t n, const uint32_t* __restrict__ root, uint8_t* fl) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) fl[k] = root[k] != 0xFFFFFFFFu;
+}
+__global__ void k_run_starts(uint32_t n, const uint32_t* __restrict__ roots, uint32_t* start_flag) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) start_flag[s] = (s == 0 || roots[s] != roots[s - 1]) ? 1u : 0u;
+}
+__global__ void k_island_starts(uint32_t n, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pos,
+                                uint32_t* isl_start) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n && flag[s]) isl_start[pos[s]] = s;
+}
+__global__ void k_island_counts(uint32_t nisl, uint32_t n, const uint32_t* __restrict__ isl_start, uint32_t* isl_cnt) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nisl) isl_cnt[i] = (i + 1 < nisl ? isl_start[i + 1] : n) - isl_start[i];
+}
+__global__ void k_warm_merge_kept(uint32_t n, const uint4* __restrict__ kk, const float4* __restrict__ ka,
+                                  const float4* __restrict__ kb, const uint4* __restrict__ newk, uint32_t n_new, uint4* ok,
+                                  float4* oa, float4* ob) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint32_t p = j + key_lower_bound(newk, n_new, kk[j]);
+  ok[p] = kk[j]; oa[p] = ka[j]; ob[p] = kb[j];
+}
+
+// ------------------------------------------------------------------ host driver
+static void build_schedule(WorldGpu::Scratch& S, uint32_t nsched, uint32_t nisl, const uint32_t* ord_in,
+                           const uint32_t* isl_start, const uint32_t* isl_cnt, uint32_t* ord_out, DBuf<uint32_t>& lvl_off,
+                           DBuf<uint32_t>& lvl_start, DBuf<uint32_t>& nlev, uint32_t* hist, uint32_t* row_level,
+                           cudaStream_t st) {
+  nlev.ensure(nisl + 1);
+  lvl_off.ensure(nisl + 1);
+  S.key64.ensure(nsched + 1); S.key64b.ensure(nsched + 1);
+  k_levels<<<nblk(nisl, 128), 128, 0, st>>>(nisl, isl_start, isl_cnt, ord_in, S.r_ab.p, S.r_flags.p, S.body_level.p,
+                                            S.key64.p, nlev.p, row_level);
+  sort_pairs_u64(S, S.key64.p, S.key64b.p, ord_in, ord_out, nsched, 0, 64, st);
+  S.tmp32.ensure(nisl + 1);
+  k_plus1<<<nblk(nisl), T, 0, st>>>(nisl, nlev.p, S.tmp32.p);
+  uint32_t total = exclusive_scan_total(S, S.tmp32.p, lvl_off.p, nisl, st);
+  lvl_start.ensure(total + 1);
+  k_level_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.key64b.p, lvl_off.p, nlev.p, isl_start, isl_cnt, lvl_start.p,
+                                             hist);
+}
+
+void run_solve(WorldGpu& W, StepCtx& ctx) {
+  auto& S = *W.s_;
+  cudaStream_t st = W.stream();
+  const uint32_t nb = W.num_bodies(), nc = ctx.nc;
+  uint32_t* stats = W.d_stats.p;
+  S.constrained.ensure(nb + 1); S.loaded.ensure(nb + 1); S.ballistic.ensure(nb + 1); S.touching.ensure(nb + 1);
+  S.uf.ensure(nb + 1); S.uf2.ensure(nb + 1); S.body_level.ensure(nb + 1); S.root_mark.ensure(nb + 1);
+  S.Iw.ensure(9 * (size_t)nb + 9);
+  S.orig_pos.ensure(nb + 1); S.orig_rot.ensure(nb + 1); S.pred_pos.ensure(nb + 1); S.pred_rot.ensure(nb + 1);
+  S.split_l.ensure(nb + 1); S.split_a.ensure(nb + 1);
+  RP_CUDA(cudaMemsetAsync(S.loaded.p, 0, nb + 1, st));
+  RP_CUDA(cudaMemsetAsync(S.constrained.p, 0, nb + 1, st));
+  RP_CUDA(cudaMemsetAsync(S.touching.p, 0, nb + 1, st));
+  RP_CUDA(cudaMemsetAsync(S.split_l.p, 0, sizeof(float4) * (nb + 1), st));
+  RP_CUDA(cudaMemsetAsync(S.split_a.p, 0, sizeof(float4) * (nb + 1), st));
+  BodiesV B{W.pos.p, W.rot.p, W.lin.p, W.ang.p, W.inv_mass.p, S.Iw.p, W.inv_I.p, W.awake.p, W.dyn.p};
+  RowsV R{S.r_ab.p, S.r_flags.p, S.r_inv.p, S.r_ra.p, S.r_rb.p, S.r_n.p, S.r_t1.p, S.r_t2.p, S.r_mu.p, S.r_la.p};
+  ctx.nisl = 0;
+  // ---- the reference's islands: their count, and whether the solve runs (step.rs:146-150)
+  uint32_t nref = 0;
+  if (nc > 0 && nb > 0) {
+    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf2.p);
+    RP_CUDA(cudaMemsetAsync(S.root_mark.p, 0, sizeof(uint32_t) * nb, st));
+    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 0, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf2.p);
+    k_ref_island_marks<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, S.uf2.p, S.root_mark.p);
+    S.tmp32.ensure(nb + 1);
+    nref = exclusive_scan_total(S, S.root_mark.p, S.tmp32.p, nb, st);
+  }
+  ctx.nref_isl = nref;
+  W.st_.islands = nref;
+  S.row_level.ensure(nc + 1);
+  RP_CUDA(cudaMemsetAsync(S.row_level.p, 0xFF, sizeof(uint32_t) * (nc + 1), st));
+  W.levels_valid_ = true;
+  if (nref > 0) {
+    // ---- rows
+    k_world_inertia<<<nblk(nb), T, 0, st>>>(nb, W.rot.p, W.inv_mass.p, W.inv_I.p, S.Iw.p);
+    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf.p);
+    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 1, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf.p);
+    S.r_ab.ensure(nc); S.r_flags.ensure(nc); S.r_inv.ensure(nc); S.r_ra.ensure(nc); S.r_rb.ensure(nc); S.r_n.ensure(nc);
+    S.r_t1.ensure(nc); S.r_t2.ensure(nc); S.r_mu.ensure(nc); S.r_la.ensure(nc); S.acc_jn.ensure(nc); S.acc_jt.ensure(nc);
+    S.wm_idx.ensure(nc); S.row_isl.ensure(nc + 1); S.row_isl2.ensure(nc + 1);
+    R = RowsV{S.r_ab.p, S.r_flags.p, S.r_inv.p, S.r_ra.p, S.r_rb.p, S.r_n.p, S.r_t1.p, S.r_t2.p, S.r_mu.p, S.r_la.p};
+    k_build_rows<<<nblk(nc), T, 0, st>>>(nc, ctx.dt, S.c_a.p, S.c_b.p, S.c_pt.p, S.c_n.p, W.col_body.p, W.col_mat.p,
+                                         ctx.hf_mat, W.pair_table.p, B, S.pre_lin.p, S.pre_ang.p, R, S.acc_jn.p,
+                                         S.acc_jt.p, S.uf.p, S.row_isl.p);
+    // ---- solve islands: roots of scheduled rows -> dense island ids, rows grouped by island
+    S.flag8.ensure(nc + 1); S.rows_sched.ensure(nc + 1); S.rows_sched2.ensure(nc + 1);
+    S.tmp32.ensure(nc + 1); S.tmp32b.ensure(nc + 1);
+    uint32_t nsched = 0;
+    k_flag_sched<<<nblk(nc), T, 0, st>>>(nc, S.row_isl.p, S.flag8.p);
+    {
+      cub::CountingInputIterator<uint32_t> it0(0);
+      size_t bytes = 0;
+      S.counts.ensure(4);
+      RP_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it0, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nc, st));
+      S.cub_tmp.ensure(bytes + 16);
+      RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, it0, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nc, st));
+      RP_CUDA(cudaMemcpyAsync(&nsched, S.counts.p + 3, 4, cudaMemcpyDeviceToHost, st));
+      RP_CUDA(cudaStreamSynchronize(st));
+    }
+    ctx.nsched = nsched;
+    uint32_t nisl = 0;
+    S.isl_start.ensure(nsched + 1); S.isl_cnt.ensure(nsched + 1);
+    S.ord_main.ensure(nsched + 1); S.ord_vs.ensure(nsched + 1); S.ord_ps.ensure(nsched + 1);
+    if (nsched > 0) {
+      // island root per scheduled row; sorting (root, row) makes each island's rows contiguous, in order
+      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.row_isl.p, S.tmp32.p);
+      sort_pairs_u32(S, S.tmp32.p, S.tmp32b.p, S.rows_sched.p, S.rows_sched2.p, nsched, 0, 32, st);
+      S.woff.ensure(nsched + 1); S.wpos.ensure(nsched + 1);
+      k_run_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32b.p, S.woff.p);
+      nisl = exclusive_scan_total(S, S.woff.p, S.wpos.p, nsched, st);
+      k_island_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.woff.p, S.wpos.p, S.isl_start.p);
+      k_island_counts<<<nblk(nisl), T, 0, st>>>(nisl, nsched, S.isl_start.p, S.isl_cnt.p);
+      ctx.nisl = nisl;
+      // ---- main schedule (row order within each island)
+      S.lvl_hist.ensure(nsched + 1);
+      RP_CUDA(cudaMemsetAsync(S.lvl_hist.p, 0, sizeof(uint32_t) * (nsched + 1), st));
+      build_schedule(S, nsched, nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_main.p, S.lvl_off, S.lvl_start,
+                     S.nlev, S.lvl_hist.p, S.row_level.p, st);
+      // levels / max batch (solver.rs:684-687)
+      {
+        size_t bytes = 0;
+        RP_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.nlev.p, stats + STAT_LEVELS, nisl, st));
+        S.cub_tmp.ensure(bytes + 16);
+        RP_CUDA(cub::DeviceReduce::Max(S.cub_tmp.p, bytes, S.nlev.p, stats + STAT_LEVELS, nisl, st));
+        bytes = 0;
+        RP_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.lvl_hist.p, stats + STAT_MAXBATCH, nsched, st));
+        S.cub_tmp.ensure(bytes + 16);
+        RP_CUDA(cub::DeviceReduce::Max(S.cub_tmp.p, bytes, S.lvl_hist.p, stats + STAT_MAXBATCH, nsched, st));
+      }
+    }
+    Sched SM{S.ord_main.p, S.lvl_off.p, S.lvl_start.p, S.nlev.p};
+    // ---- warm start matching (solver.rs:717-762)
+    k_warm_match<<<nblk(nc), T, 0, st>>>(nc, S.r_ab.p, S.r_flags.p, S.r_la.p, W.warm_key.p, W.warm_a.p, W.n_warm,
+                                         S.wm_idx.p, stats + STAT_WARM_MATCHED, stats + STAT_ERR);
+    k_warm_unscheduled<<<nblk(nc), T, 0, st>>>(nc, R, B, S.wm_idx.p, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p);
+    // ---- warm application + velocity sweeps
+    const bool resid_mode = W.res_tol_ > 0.0f;
+    int iters = (int)(resid_mode ? (W.res_max_ > 0 ? W.res_max_ : W.iters_v_) : W.iters_v_);
+    if (nisl > 0)
+      k_vel_solve<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p, W.warm_a.p,
+                                                        W.warm_b.p, iters, resid_mode ? W.res_tol_ : 0.0f, stats);
+    // ---- warm-start cache for the next tick (solver.rs:917-944)
+    {
+      S.woff.ensure(nc + 1); S.wpos.ensure(nc + 1);
+      k_warm_new_flags<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.wpos.p);
+      uint32_t n_new = exclusive_scan_total(S, S.wpos.p, S.woff.p, nc, st);
+      // new keys alone first (positions without the old-kept offsets), to test old entries against
+      W.warm_key2.ensure(n_new + W.n_warm + 1); W.warm_a2.ensure(n_new + W.n_warm + 1); W.warm_b2.ensure(n_new + W.n_warm + 1);
+      k_warm_new_write<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.wpos.p, S.woff.p, nullptr, nullptr, 0,
+                                               W.warm_key2.p, W.warm_a2.p, W.warm_b2.p);
+      uint32_t n_kept = 0;
+      S.wflag.ensure(W.n_warm + 1);
+      DBuf<uint4> kept_k; DBuf<float4> kept_a, kept_b;
+      if (W.n_warm > 0) {
+        k_warm_old_flags<<<nblk(W.n_warm), T, 0, st>>>(W.n_warm, W.warm_key.p, W.warm_key2.p, n_new, W.alive_d.p, W.dyn.p,
+                                                       W.awake.p, nb, S.wflag.p);
+        kept_k.ensure(W.n_warm + 1); kept_a.ensure(W.n_warm + 1); kept_b.ensure(W.n_warm + 1);
+        size_t bytes = 0;
+        S.counts.ensure(4);
+        RP_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, W.warm_key.p, S.wflag.p, kept_k.p, S.counts.p + 3, W.n_warm, st));
+        S.cub_tmp.ensure(bytes + 16);
+        RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, W.warm_key.p, S.wflag.p, kept_k.p, S.counts.p + 3, W.n_warm, st));
+        RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, W.warm_a.p, S.wflag.p, kept_a.p, S.counts.p + 3, W.n_warm, st));
+        RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, W.warm_b.p, S.wflag.p, kept_b.p, S.counts.p + 3, W.n_warm, st));
+        RP_CUDA(cudaMemcpyAsync(&n_kept, S.counts.p + 3, 4, cudaMemcpyDeviceToHost, st));
+        RP_CUDA(cudaStreamSynchronize(st));
+      }
+      if (n_kept == 0) {
+        std::swap(W.warm_key.p, W.warm_key2.p); std::swap(W.warm_key.cap, W.warm_key2.cap);
+        std::swap(W.warm_a.p, W.warm_a2.p); std::swap(W.warm_a.cap, W.warm_a2.cap);
+        std::swap(W.warm_b.p, W.warm_b2.p); std::swap(W.warm_b.cap, W.warm_b2.cap);
+        W.n_warm = n_new;
+      } else {
+        // merge: new entry k at off[k] + #kept below its key; kept entry j at j + #new below its key
+        W.warm_key.ensure(n_new + n_kept + 1); W.warm_a.ensure(n_new + n_kept + 1); W.warm_b.ensure(n_new + n_kept + 1);
+        k_warm_new_write<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.wpos.p, S.woff.p, nullptr, kept_k.p,
+                                                 n_kept, W.warm_key.p, W.warm_a.p, W.warm_b.p);
+        k_warm_merge_kept<<<nblk(n_kept), T, 0, st>>>(n_kept, kept_k.p, kept_a.p, kept_b.p, W.warm_key2.p, n_new, W.warm_key.p,
+                                        W.warm_a.p, W.warm_b.p);
+        W.n_warm = n_new + n_kept;
+        RP_CUDA(cudaStreamSynchronize(st));
+      }
+    }
+    // ---- shock propagation (solver.rs:964-993)
+    if (nisl > 0) {
+      k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p);
+      sort_pairs_u64(S, S.key64.p, S.key64b.p, S.rows_sched.p, S.tmp32.p, nsched, 0, 64, st);  // by height key, stable
+      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p);      // their roots
+      sort_pairs_u32(S, S.tmp32b.p, S.woff.p, S.tmp32.p, S.rows_sched2.p, nsched, 0, 32, st);   // by island, stable
+      build_schedule(S, nsched, nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_vs.p, S.lvl_off_vs,
+                     S.lvl_start_vs, S.nlev_vs, nullptr, nullptr, st);
+      Sched SV{S.ord_vs.p, S.lvl_off_vs.p, S.lvl_start_vs.p, S.nlev_vs.p};
+      k_vel_shock<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, SV, R, B, ctx.up, S.acc_jn.p);
+    }
+    k_after_solve<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.loaded.p, S.c_n.p, stats);
+  }
+  // ---- stage 4
+  if (nc > 0) k_constrained<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, S.constrained.p);
+  if (nb > 0) k_ballistic_init<<<nblk(nb), T, 0, st>>>(nb, S.constrained.p, S.loaded.p, S.ballistic.p);
+  Sched SM{S.ord_main.p, S.lvl_off.p, S.lvl_start.p, S.nlev.p};
+  if (ctx.nisl > 0)
+    k_ballistic<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SM, R, B, S.c_pt.p, S.c_n.p, W.last_lin.p, ctx.dt,
+                                                          S.ballistic.p);
+  if (nb > 0)
+    k_integrate<<<nblk(nb, 128), 128, 0, st>>>(nb, B, S.ballistic.p, W.last_lin.p, ctx.dt, S.orig_pos.p, S.orig_rot.p,
+                                               S.pred_pos.p, S.pred_rot.p);
+  // ---- stage 5: position pass (step.rs:284-309); its contacts are the scheduled rows
+  if (ctx.nisl > 0) {
+    S.pc_lb.ensure(nc + 1);
+    k_pos_anchors<<<nblk(nc), T, 0, st>>>(nc, R, S.c_pt.p, S.orig_pos.p, S.orig_rot.p, S.pc_lb.p);
+    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SM, R, B, (int)W.iters_p_, 0, ctx.up, S.c_pt.p,
+                                                               S.c_n.p, S.pc_lb.p, S.split_l.p, S.split_a.p);
+    // shock projection in (height key, index) order at the poses the iterations left
+    uint32_t nsched = ctx.nsched;
+    k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p);
+    sort_pairs_u64(S, S.key64.p, S.key64b.p, S.rows_sched.p, S.tmp32.p, nsched, 0, 64, st);
+    k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p);
+    sort_pairs_u32(S, S.tmp32b.p, S.woff.p, S.tmp32.p, S.rows_sched2.p, nsched, 0, 32, st);
+    build_schedule(S, nsched, ctx.nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_ps.p, S.lvl_off_ps,
+                   S.lvl_start_ps, S.nlev_ps, nullptr, nullptr, st);
+    Sched SP{S.ord_ps.p, S.lvl_off_ps.p, S.lvl_start_ps.p, S.nlev_ps.p};
+    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SP, R, B, 1, 1, ctx.up, S.c_pt.p, S.c_n.p,
+                                                               S.pc_lb.p, S.split_l.p, S.split_a.p);
+  }
+  // ---- stages 6 and 7
+  if (nc > 0) k_touching<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, S.c_pt.p, W.col_body.p, S.touching.p);
+  if (nb > 0)
+    k_stage6<<<nblk(nb), T, 0, st>>>(nb, B, S.orig_pos.p, S.pred_pos.p, S.pred_rot.p, S.split_l.p, S.split_a.p,
+                                     S.touching.p, ctx.dt, W.last_lin.p, W.awake.p, W.sleep_ticks.p, W.sleep_allowed.p,
+                                     stats);
+  uint32_t ncap = W.capacity() > nb ? W.capacity() : nb;
+  k_count_sleeping<<<nblk(ncap), T, 0, st>>>(ncap, W.awake.p, stats);
+}
+
+}  // namespace rp

@@ -1,0 +1,162 @@
+// world_gpu.h -- the device-resident world behind the C ABI, and the per-tick pipeline that
+// replaces World::step (riftphys-world/src/world/step.rs:40-420) on one B200.
+//
+// HBM layout (structure of arrays, 16-byte rows for 128-bit loads):
+//   bodies     pos/rot/lin/ang/last_lin float4, inv_mass f32, inv_I 9 x f32 (column-major),
+//              dyn/awake/sleep_allowed/alive u8, sleep_ticks u16 -- allocated at the world's
+//              body capacity; sleep arrays are hashed at that length, as the reference sizes
+//              SleepManager by capacity (sleep.rs:15-27).
+//   colliders  body u32, kind u32, mat u32, dims float4 (one collider per body, body order).
+//   warm cache sorted by key (uint4: body A, body B or 0xFFFFFFFF, ordinal A, ordinal B);
+//              la+jn float4, jt float4 per entry, entries of one key contiguous in contact order.
+//   per tick   pairs (u64 (i << 32 | j)), contacts (SoA), rows (SoA), schedules (u32 arrays).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "rp_math.cuh"
+
+namespace rp {
+
+struct StepStatsHost {
+  uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
+  uint32_t sweeps = 0, bounce_skipped = 0, warm_entries = 0, sleeping = 0, error_flags = 0;
+  float residual = 0.0f;
+};
+
+struct PairPropsHost { float mu_s, mu_k, restitution, stribeck_v, stiffness; };
+
+// A device array that only grows.
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t n);
+  void release();
+  ~DBuf() { release(); }
+};
+
+struct SnapshotGpu;
+
+class WorldGpu {
+ public:
+  WorldGpu(uint32_t max_bodies, uint32_t max_colliders);
+  ~WorldGpu();
+
+  // ---- configuration and body management (world.rs)
+  uint32_t num_bodies() const { return nb_; }
+  uint32_t num_colliders() const { return ncol_; }
+  uint32_t capacity() const { return cap_b_; }
+  bool alive(uint32_t id) const { return id < nb_ && h_alive_[id] != 0; }
+  // World::add_body + add_collider; shape/dims/material as RPhysBodyDescEx. Returns the index.
+  uint32_t add_body(const float pose[7], const float vel[6], uint32_t shape, const float dims[3],
+                    float inv_mass, const float inertia_diag[3], bool dynamic, uint32_t mat,
+                    bool sleep_allowed);
+  void add_bodies_bulk(uint32_t n, const float* pose7, const float* vel6, const uint32_t* shape,
+                       const float* dims3, const float* inv_mass, const float* inertia3,
+                       const uint8_t* dynamic, const uint32_t* mat, const uint8_t* sleep_allowed);
+  bool remove_body(uint32_t id);
+  void set_body_pose(uint32_t id, const float pose[7]);
+  void set_body_vel(uint32_t id, const float vel[6]);
+  void apply_impulse(uint32_t id, const float j[3]);
+  void get_body_pose(uint32_t id, float pose[7]);
+  void get_body_vel(uint32_t id, float vel[6]);
+  void get_body_states(uint32_t first, uint32_t count, float* out13);
+  void set_pair_props(uint32_t a, uint32_t b, const PairPropsHost& p);
+  void set_solver_iterations(uint32_t v, uint32_t p) { iters_v_ = v < 1 ? 1 : v; iters_p_ = p < 1 ? 1 : p; }
+  void set_gravity(f3 g) { gravity_ = g; }
+  void set_residual_mode(float tol, uint32_t max_sweeps) { res_tol_ = tol; res_max_ = max_sweeps; }
+  void set_heightfield(uint32_t nx, uint32_t nz, float sx, float sz, float ox, float oz,
+                       const std::vector<float>& q6_heights, float min_y, float max_y, uint32_t mat);
+  void clear_heightfield();
+  void set_epoch(uint64_t e) { epoch_ = e; }
+  void set_rng_state(uint64_t s) { rng_ = s; }
+  uint64_t tick() const { return tick_; }
+
+  // ---- the tick
+  void step(float dt);      // World::step, asynchronous on the world's stream
+  void synchronize();       // waits for the stream; raises on a device error
+  void step_hash(uint8_t out[32]);
+
+  // ---- inspection
+  const StepStatsHost& stats();
+  void get_pairs(std::vector<uint64_t>& out);
+  struct ContactOut { uint32_t a, b; float p[3], n[3]; float depth, impulse; uint32_t level; };
+  void get_contacts(std::vector<ContactOut>& out);
+  uint32_t body_of_collider(uint32_t c) const { return h_col_body_[c]; }
+
+  // ---- rollback
+  SnapshotGpu* snapshot_create();
+  void snapshot_restore(const SnapshotGpu* s);
+  static void snapshot_free(SnapshotGpu* s);
+
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  void upload_pair_table();
+  void drop_warm_of(uint32_t b);
+  void filter_warm(int mode, uint32_t body);  // mode 0: drop body, 1: keep alive keys only
+  uint32_t read_u32(const uint32_t* dptr);
+
+  // capacities and counts
+  uint32_t cap_b_, cap_c_, nb_ = 0, ncol_ = 0;
+  cudaStream_t stream_ = nullptr;
+  // host mirrors of static data
+  std::vector<uint8_t> h_alive_;
+  std::vector<uint32_t> h_col_body_, h_col_kind_, h_col_mat_;
+  std::vector<float> h_col_dims_;
+  std::vector<std::pair<std::pair<uint32_t, uint32_t>, PairPropsHost>> overrides_;
+  f3 gravity_ = mk3(0.0f, -9.81f, 0.0f);
+  uint64_t epoch_ = 0, rng_ = 0xC0FFEEull | 1ull, tick_ = 0;
+  // heightfield
+  bool has_hf_ = false;
+  uint32_t hf_nx_ = 0, hf_nz_ = 0, hf_mat_ = 4;
+  float hf_sx_ = 1, hf_sz_ = 1, hf_ox_ = 0, hf_oz_ = 0, hf_min_ = 0, hf_max_ = 0;
+  DBuf<float> hf_h_;
+
+ public:
+  // solver configuration and device state (read by the pipeline in the .cu files)
+  uint32_t iters_v_ = 20, iters_p_ = 20;
+  float res_tol_ = 0.0f;
+  uint32_t res_max_ = 0;
+  DBuf<float4> pos, rot, lin, ang, last_lin;
+  DBuf<float> inv_mass, inv_I;
+  DBuf<uint8_t> dyn, awake, sleep_allowed, alive_d;
+  DBuf<uint16_t> sleep_ticks;
+  DBuf<uint32_t> col_body, col_kind, col_mat;
+  DBuf<float4> col_dims;
+  DBuf<float> pair_table;  // 14 x 14 x 5
+  // warm cache
+  DBuf<uint4> warm_key, warm_key2;
+  DBuf<float4> warm_a, warm_b, warm_a2, warm_b2;  // a: la.xyz + jn, b: jt.xyz
+  uint32_t n_warm = 0;
+  // per-tick products kept for inspection
+  uint32_t n_pairs = 0, n_contacts = 0;
+  StepStatsHost st_;
+  bool stats_dirty_ = false;
+  bool levels_valid_ = false;
+  struct Scratch;
+  Scratch* s_ = nullptr;
+  DBuf<uint32_t> d_stats;  // device-side counters
+};
+
+struct SnapshotGpu {
+  uint64_t tick;
+  uint32_t nb, cap, n_warm;
+  DBuf<float4> pos, rot, lin, ang, last_lin;
+  DBuf<uint8_t> awake;
+  DBuf<uint16_t> ticks;
+  DBuf<uint4> wk;
+  DBuf<float4> wa, wb;
+};
+
+// MassProps::from_*_density (riftphys-geom/src/mass.rs:75-145); host side.
+bool mass_from_density(uint32_t shape, const float dims[3], float density, float* inv_mass, float inertia[3]);
+// pair_props with the built-in table (riftphys-materials/src/materials.rs:250-305)
+PairPropsHost table_pair_props(uint32_t a, uint32_t b);
+bool material_known(uint32_t id);
+
+}  // namespace rp

@@ -1,0 +1,136 @@
+"""Seeded synthetic scenes for the benchmark configurations and the parity tests.
+
+All randomness comes from a project-written splitmix64 generator, so the same seed gives the same
+f32 inputs on every machine; the scenes are built through the C ABI of whichever library the
+``World`` wraps (the CUDA product or the CPU restatement used as a checker).
+
+box_drop      1,000 boxes (half-extent 0.5 m, 1 kg, mu 0.5, e 0) on a 10x10x10 grid at 1.1 m pitch,
+              jitter U[-0.05, 0.05] m, yaw U[0, 2 pi), bottom layer 1 m above a static 50x0.5x50 ground
+              box, dt 1/60, 8 velocity and 8 position iterations.
+terrain       bodies (40% spheres r U[0.2,0.6], 30% capsules r U[0.15,0.4] hh U[0.3,0.8], 30% boxes
+              he U[0.2,0.7], density 1000) at uniform positions in a square of side `area` x [0, 60] m,
+              lifted above the terrain, velocities N(0,1) per axis, falling onto a heightfield
+              h = 6 sin(x/37) cos(z/53) + 2 valuenoise(x/8, z/8), 1 m spacing; dt 1/60, 20 iterations.
+"""
+import math
+
+import numpy as np
+
+MASK64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    def __init__(self, seed):
+        self.s = seed & MASK64
+
+    def next_u64(self):
+        self.s = (self.s + 0x9E3779B97F4A7C15) & MASK64
+        z = self.s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+        return z ^ (z >> 31)
+
+    def uniform(self, lo=0.0, hi=1.0):
+        return lo + (hi - lo) * ((self.next_u64() >> 11) * (1.0 / (1 << 53)))
+
+    def normal(self):
+        u1 = max(self.uniform(), 1e-300)
+        u2 = self.uniform()
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+
+def _yaw_quat(theta):
+    return (0.0, math.sin(theta * 0.5), 0.0, math.cos(theta * 0.5))
+
+
+def _rand_quat(rng):
+    # uniform random rotation (Shoemake)
+    u1, u2, u3 = rng.uniform(), rng.uniform(), rng.uniform()
+    a, b = math.sqrt(1 - u1), math.sqrt(u1)
+    return (a * math.sin(2 * math.pi * u2), a * math.cos(2 * math.pi * u2),
+            b * math.sin(2 * math.pi * u3), b * math.cos(2 * math.pi * u3))
+
+
+def box_drop(rp, w, n_side=10, pitch=1.1, seed=1, iterations=(8, 8), sleep_allowed=True):
+    """Builds the box-drop scene into World ``w``; returns (dt, body count)."""
+    rng = SplitMix64(seed)
+    w.set_pair_props(0, 0, 0.5, 0.5, 0.0, 0.08)
+    w.set_iterations(*iterations)
+    descs = [rp.BodyDescEx(rp.iso(0.0, -0.5, 0.0), rp.vel(), rp.SHAPE_BOX, (50.0, 0.5, 50.0), 0.0,
+                           rp.RPHYS_BODY_STATIC, 0, 1)]
+    off = (n_side - 1) * 0.5
+    for iy in range(n_side):
+        for iz in range(n_side):
+            for ix in range(n_side):
+                x = (ix - off) * pitch + rng.uniform(-0.05, 0.05)
+                y = 1.0 + 0.5 + iy * pitch + rng.uniform(-0.05, 0.05)
+                z = (iz - off) * pitch + rng.uniform(-0.05, 0.05)
+                q = _yaw_quat(rng.uniform(0.0, 2.0 * math.pi))
+                # MassProps::from_box_density(he, 1 / (8 * 0.125)): 1 kg
+                descs.append(rp.BodyDescEx(rp.iso(x, y, z, q=q), rp.vel(), rp.SHAPE_BOX, (0.5, 0.5, 0.5), 1.0,
+                                           rp.RPHYS_BODY_DYNAMIC, 0, 1 if sleep_allowed else 0))
+    w.add_bodies(descs)
+    return 1.0 / 60.0, len(descs)
+
+
+def value_noise(x, z, seed):
+    """Seeded lattice value noise with smoothstep bilinear interpolation (numpy, vectorised)."""
+    xi, zi = np.floor(x).astype(np.int64), np.floor(z).astype(np.int64)
+    fx, fz = x - xi, z - zi
+
+    def lat(ix, iz):
+        with np.errstate(over="ignore"):
+            h = (ix.astype(np.uint64) * np.uint64(0x27D4EB2F165667C5)
+                 + iz.astype(np.uint64) * np.uint64(0x165667B19E3779F9)
+                 + np.uint64((seed * 0x9E3779B97F4A7C15) & MASK64))
+            h ^= h >> np.uint64(29)
+            h = h * np.uint64(0xBF58476D1CE4E5B9)
+            h ^= h >> np.uint64(32)
+        return (h >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+
+    sx, sz = fx * fx * (3 - 2 * fx), fz * fz * (3 - 2 * fz)
+    a, b = lat(xi, zi), lat(xi + 1, zi)
+    c, d = lat(xi, zi + 1), lat(xi + 1, zi + 1)
+    return (a * (1 - sx) + b * sx) * (1 - sz) + (c * (1 - sx) + d * sx) * sz
+
+
+def heightfield(n=512, spacing=1.0, seed=7):
+    origin = -0.5 * (n - 1) * spacing
+    g = origin + spacing * np.arange(n, dtype=np.float64)
+    X, Z = np.meshgrid(g, g, indexing="xy")  # row-major, x fastest
+    h = 6.0 * np.sin(X / 37.0) * np.cos(Z / 53.0) + 2.0 * value_noise(X / 8.0, Z / 8.0, seed)
+    return h.astype(np.float32), origin
+
+
+def terrain(rp, w, n_bodies=100_000, hf_n=512, area=400.0, seed=2, iterations=(20, 20)):
+    """Builds the mixed-shape terrain scene into World ``w``; returns (dt, body count)."""
+    rng = SplitMix64(seed)
+    h, origin = heightfield(hf_n, 1.0, seed)
+    w.set_heightfield(h, hf_n, hf_n, 1.0, 1.0, origin, origin, material=4)  # Grit, as the FFI's terrain
+    # restitution 0 on every pair the scene uses; friction from the material table
+    w.set_pair_props(0, 0, 0.6, 0.5, 0.0, 0.08)
+    w.set_pair_props(0, 4, 0.883176, 0.724569, 0.0, 0.1)
+    w.set_iterations(*iterations)
+    hmax = float(h.max())
+    descs = []
+    half = 0.5 * area
+    for _ in range(n_bodies):
+        kind = rng.uniform()
+        if kind < 0.4:
+            shape, dims, bound = rp.SHAPE_SPHERE, (rng.uniform(0.2, 0.6), 0.0, 0.0), None
+            bound = dims[0]
+        elif kind < 0.7:
+            r, hh = rng.uniform(0.15, 0.4), rng.uniform(0.3, 0.8)
+            shape, dims, bound = rp.SHAPE_CAPSULE, (r, hh, 0.0), r + hh
+        else:
+            he = (rng.uniform(0.2, 0.7), rng.uniform(0.2, 0.7), rng.uniform(0.2, 0.7))
+            shape, dims, bound = rp.SHAPE_BOX, he, math.sqrt(he[0] ** 2 + he[1] ** 2 + he[2] ** 2)
+        x, z = rng.uniform(-half, half), rng.uniform(-half, half)
+        y = rng.uniform(0.0, 60.0)
+        # lift above the local terrain (the heightfield's maximum bounds it from above)
+        y = max(y, hmax + bound + 0.1)
+        q = _rand_quat(rng)
+        v = (rng.normal(), rng.normal(), rng.normal())
+        descs.append(rp.BodyDescEx(rp.iso(x, y, z, q=q), rp.vel(v), shape, dims, 1000.0, rp.RPHYS_BODY_DYNAMIC, 0, 1))
+    w.add_bodies(descs)
+    return 1.0 / 60.0, len(descs)
