@@ -1,0 +1,294 @@
+"""Benchmark: body-ticks/s of the rigid-body tick at PGS residual <= 1e-4 on one B200.
+
+Workload (default ``--config terrain``): 100,000 bodies (40% spheres, 30% capsules, 30% boxes,
+density 1000) falling onto a 512x512 heightfield (1 m spacing), dt 1/60, 20 iterations; the
+velocity solve sweeps until its residual (largest |delta impulse| / effective mass over all rows,
+m/s) is <= 1e-4, at most 80 sweeps. Seeded synthetic scene (no dataset). A "step" is one tick of
+the whole world. The scene is first advanced ``--settle`` ticks (untimed) so the timed ticks sit
+in the contact-rich part of the 600-tick run; then W warm-up ticks, then exactly K timed ticks,
+bracketed by a barrier + device synchronize, timed with CUDA events recorded on the world's own
+stream. ``--config box_drop`` is the 1,000-box drop (8 iterations).
+
+value   whole-job body-ticks/s (bodies x K summed over ranks / max over ranks of the timed span).
+e2e     the same metric through the C ABI's rphys_world_step_ex with the tick's state read back to
+        host memory (rphys_ext_get_body_states: pos, rot, lin, ang) every tick, timed on the host.
+roofline  the stage with the most device time in a separate profiled pass (CUDA events around each
+        stage on the world's stream): its algorithmic bytes per launch / its mean duration, against
+        the measured HBM copy bandwidth in MEASURED_PEAKS.json.
+cpu_baseline  the CPU restatement of the reference step (C++, OpenMP) on a bounded sample of the
+        same workload: a 50x50 m patch at the same body density and shape mix, settled, then timed.
+
+Multi-GPU: a single world does not shard (its contacts couple every body), so N ranks run N
+independent replicas (one per GPU, scaling "weak"); no collective touches the data path.
+``--impl reference`` times the CPU reference restatement instead (rank 0 only).
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def _import_pkg():
+    import importlib.util
+    pkg = os.path.join(ROOT, "riftphys-rust_b200")
+    if "riftphys_rust_b200" in sys.modules:
+        return sys.modules["riftphys_rust_b200"]
+    spec = importlib.util.spec_from_file_location("riftphys_rust_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["riftphys_rust_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+rp = _import_pkg()
+import riftphys_rust_b200.scenes as scenes  # noqa: E402
+
+TOL = 1.0e-4
+# algorithmic bytes per unit of each stage (counted once per required HBM read or write)
+BYTES = {
+    "forces": ("bodies", 24), "aabb_sweep": ("colliders", 92), "integrate": ("bodies", 152),
+    "vel_solve": ("row_sweeps", 280), "pos_iter": ("pos_row_sweeps", 152), "narrow_pairs": ("pairs", 88 + 4 * 28),
+    "stage6": ("bodies", 120),
+}
+
+
+def build_scene(lib, config, n_bodies=None, area=None, hf_n=None):
+    if config == "box_drop":
+        w = lib.world(1024, 1024)
+        dt, n = scenes.box_drop(rp, w, n_side=10)
+        return w, dt, n, "box_drop: 1,000 boxes (he 0.5 m, 1 kg) on a static 50x0.5x50 ground box, dt 1/60, 8+8 iters"
+    n_bodies = n_bodies or 100_000
+    w = lib.world(n_bodies + 16, n_bodies + 16)
+    dt, n = scenes.terrain(rp, w, n_bodies=n_bodies, hf_n=hf_n or 512, area=area or 400.0)
+    return w, dt, n, (f"terrain: {n} bodies (40% spheres, 30% capsules, 30% boxes, 1000 kg/m^3) on a "
+                      f"{hf_n or 512}^2 heightfield at 1 m spacing, dt 1/60, 20 iters")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index, self.samples, self.proc = index, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 6:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        mx = max(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[2 + k]})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons}
+
+
+def peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def oracle_path():
+    p = os.path.join(ROOT, "oracle", "build", "liboracle_rphys.so")
+    if not os.path.exists(p):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    return p
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference step, all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import ctypes
+    lib = rp.Lib(oracle_path())
+    lib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    threads = os.cpu_count() or 1
+    ticks = max(1, args.steps)
+    value, sample = cpu_sample_with(lib, ticks, threads)
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": "body-ticks/s",
+                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                      "scaling": "weak", "dtype": "f32", "data": "synthetic",
+                      "config": {"workload": args.config, "sample": sample},
+                      "cpu_baseline": {"value": value, "unit": "body-ticks/s", "cores": threads, "kind": "port",
+                                       "sample": sample},
+                      "e2e": {"value": value, "unit": "body-ticks/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def cpu_sample_with(lib, ticks, threads, settle=240):
+    n = int(round(100_000 * (50.0 / 400.0) ** 2))
+    w = lib.world(n + 16, n + 16)
+    dt, nb = scenes.terrain(rp, w, n_bodies=n, hf_n=64, area=50.0)
+    w.set_residual_mode(TOL, 80)
+    lib.dll.rphys_oracle_set_threads(w.h, threads)
+    w.step_n(dt, settle)
+    t0 = time.perf_counter()
+    w.step_n(dt, ticks)
+    el = time.perf_counter() - t0
+    return nb * ticks / el, (f"{nb}-body 50x50 m patch of the 100k-body terrain workload (same density and shape "
+                             f"mix, 64^2 heightfield), ticks {settle + 1}-{settle + ticks}, residual mode, "
+                             f"{threads} threads")
+
+
+METRIC = "body-ticks/s at PGS residual <=1e-4"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--settle", type=int, default=240)
+    ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop"])
+    ap.add_argument("--mode", default="residual", choices=["residual", "fixed"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--bodies", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-ticks", type=int, default=5)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world_size > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    lib = rp.load_product()
+    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies)
+    if args.mode == "residual":
+        w.set_residual_mode(TOL, 4 * (8 if args.config == "box_drop" else 20))
+    # settle into the contact regime, then warm up
+    if args.settle:
+        w.step_n(dt, args.settle)
+    for _ in range(args.warmup):
+        w.step_n(dt, 1)
+    stream = torch.cuda.ExternalStream(w.stream_handle())
+    launches0 = lib.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0.record(stream)
+    w.step_n(dt, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = lib.launch_count() - launches0
+    if world_size > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    st = w.stats()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world_size > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = nb * args.steps * world_size / (ms_max / 1000.0)
+
+    # e2e: the drop-in C-ABI call with the tick's state read back to host memory every tick
+    import numpy as np
+    host = np.empty((nb, 13), dtype=np.float32)
+    e2e_ticks = max(3, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(e2e_ticks):
+        w.step(dt)
+        w.c("rphys_ext_get_body_states", 0, nb, host.ctypes.data_as(ctypes.c_void_p))
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": nb * e2e_ticks / e2e_s, "unit": "body-ticks/s", "h2d_bytes_per_step": 0,
+           "d2h_bytes_per_step": 64 * nb}
+
+    # roofline: the stage with the most device time, in a separate profiled pass
+    w.profile(True)
+    units = {"bodies": 0, "colliders": 0, "row_sweeps": 0, "pos_row_sweeps": 0, "pairs": 0}
+    for _ in range(args.profile_ticks):
+        w.step_n(dt, 1)
+        s = w.stats()
+        units["bodies"] += nb
+        units["colliders"] += nb
+        units["row_sweeps"] += s["row_sweeps"]
+        units["pos_row_sweeps"] += s["rows_scheduled"] * (8 if args.config == "box_drop" else 20)
+        units["pairs"] += s["pairs"]
+    prof = w.profile_read()
+    w.profile(False)
+    total_ms = sum(v[0] for v in prof.values())
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = peak_hbm()
+    stage, (stage_ms, stage_calls) = top
+    roof = {"kernel": stage, "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_source": peak_kind,
+            "traffic": None, "share_of_tick": stage_ms / total_ms if total_ms else None}
+    if stage in BYTES and stage_calls:
+        unit, per = BYTES[stage]
+        bytes_per_launch = per * units[unit] / stage_calls
+        achieved = bytes_per_launch / (stage_ms / stage_calls / 1000.0) / 1e9
+        roof.update({"achieved": achieved, "frac": achieved / peak, "bytes_per_launch": bytes_per_launch,
+                     "ms_per_launch": stage_ms / stage_calls})
+    else:
+        roof.update({"achieved": None, "frac": None, "ms_per_launch": stage_ms / max(1, stage_calls)})
+    stages = {k: round(v[0] / max(1, v[1]), 4) for k, v in prof.items() if v[1]}
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline and args.config == "terrain":
+        import ctypes
+        olib = rp.Lib(oracle_path())
+        olib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        threads = os.cpu_count() or 1
+        v, sample = cpu_sample_with(olib, 10, threads)
+        cpu = {"value": v, "unit": "body-ticks/s", "cores": threads, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "body-ticks/s", "n_gpus": world_size, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": desc, "settle_ticks": args.settle, "mode": args.mode, "tolerance": TOL,
+                           "parallelism": f"replicas{world_size}", "l2": "inputs larger than L2" if nb > 50000 else
+                           "working set within L2", "sweeps_last_tick": st["sweeps"],
+                           "residual_last_tick": st["residual"], "rows_last_tick": st["rows_scheduled"],
+                           "contacts_last_tick": st["contacts"], "islands_last_tick": st["islands"]},
+                "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": launches, "stage_ms": stages}
+        print(json.dumps(line), flush=True)
+    w.close()
+    if world_size > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -80,6 +80,8 @@ typedef struct RPhysStepStats {
     uint32_t sleeping;       /* bodies asleep (World::num_sleeping) */
     uint32_t error_flags;    /* RPHYS_STATERR_* */
     float residual;          /* residual of the last velocity sweep (m/s) */
+    uint32_t row_sweeps;     /* velocity row updates run in the last tick (rows x sweeps) */
+    uint32_t rows_scheduled; /* contact rows with a movable body in the last tick */
 } RPhysStepStats;
 RPhysResult rphys_ext_get_stats(const RPhysWorld* world, RPhysStepStats* out);
 
@@ -103,6 +105,22 @@ RPhysResult rphys_ext_get_contact_records(const RPhysWorld* world, RPhysContactR
  * pos xyz, rot xyzw, lin xyz, ang xyz. */
 RPhysResult rphys_ext_get_body_states(const RPhysWorld* world, uint32_t first, uint32_t count,
                                       float* out13);
+
+/* Per-stage timing with CUDA events recorded on the world's stream around each stage of the tick
+ * (on: also waits for each tick to finish). read: totals in ms and tick counts since enabling;
+ * returns the number of stages; names from rphys_ext_profile_stage_name. */
+RPhysResult rphys_ext_profile_enable(RPhysWorld* world, uint32_t on);
+RPhysResult rphys_ext_profile_read(const RPhysWorld* world, double* ms, uint64_t* ticks, uint32_t cap,
+                                   uint32_t* out_stages);
+const char* rphys_ext_profile_stage_name(uint32_t stage);
+
+/* The CUDA stream every kernel of this world runs on (a cudaStream_t), for callers that time or
+ * order their own work against the tick. 0 from a library without a device. */
+RPhysResult rphys_ext_stream_handle(const RPhysWorld* world, uint64_t* out_stream);
+
+/* Device kernels this library has launched since it was loaded (all worlds): every launch site
+ * counts its kernels, and each device-wide sort, scan or select counts the kernels it runs. */
+RPhysResult rphys_ext_launch_count(uint64_t* out_launches);
 
 #ifdef __cplusplus
 }

@@ -474,6 +474,7 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
   o->pairs = s.pairs; o->contacts = s.contacts; o->islands = s.islands; o->levels = s.levels;
   o->max_batch = s.max_batch; o->warm_matched = s.warm_matched; o->sweeps = s.sweeps;
   o->bounce_skipped = s.bounce_skipped; o->residual = s.residual;
+  o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
   uint32_t we = 0;
   for (auto& kv : W->w.warm) we += (uint32_t)kv.second.size();
   o->warm_entries = we;
@@ -527,6 +528,25 @@ RPhysResult rphys_ext_get_body_states(const RPhysWorld* Wc, uint32_t first, uint
     o[7] = w.lin[i].x; o[8] = w.lin[i].y; o[9] = w.lin[i].z;
     o[10] = w.ang[i].x; o[11] = w.ang[i].y; o[12] = w.ang[i].z;
   }
+  return RPHYS_OK;
+}
+
+RPhysResult rphys_ext_profile_enable(RPhysWorld* W, uint32_t) { return W ? RPHYS_OK : RPHYS_ERR_NULL; }
+RPhysResult rphys_ext_profile_read(const RPhysWorld* W, double*, uint64_t*, uint32_t, uint32_t* n) {
+  if (!W || !n) return RPHYS_ERR_NULL;
+  *n = 0;
+  return RPHYS_OK;
+}
+const char* rphys_ext_profile_stage_name(uint32_t) { return nullptr; }
+RPhysResult rphys_ext_stream_handle(const RPhysWorld* W, uint64_t* out) {
+  if (!W || !out) return RPHYS_ERR_NULL;
+  *out = 0;
+  return RPHYS_OK;
+}
+
+RPhysResult rphys_ext_launch_count(uint64_t* out) {
+  if (!out) return RPHYS_ERR_NULL;
+  *out = 0;
   return RPHYS_OK;
 }
 

@@ -1109,6 +1109,12 @@ void World::step(float dt) {
       if (residual_mode && resid <= res_tol) break;
     }
     stats.sweeps = sweeps;
+    {
+      uint32_t ns = 0;
+      for (auto& b : batches) ns += (uint32_t)b.size();
+      stats.rows_scheduled = ns;
+      stats.row_sweeps = ns * sweeps;
+    }
     stats.residual = resid;
     // warm-start cache (:917-944)
     std::map<WarmKey, std::vector<WarmContact>> nw;

@@ -98,7 +98,7 @@ class PairProps(Structure):
 class StepStats(Structure):
     _fields_ = [(n, c_uint32) for n in ("pairs", "contacts", "islands", "levels", "max_batch", "warm_matched",
                                         "sweeps", "bounce_skipped", "warm_entries", "sleeping", "error_flags")] + \
-               [("residual", c_float)]
+               [("residual", c_float), ("row_sweeps", c_uint32), ("rows_scheduled", c_uint32)]
 
 
 class ContactRecord(Structure):
@@ -151,6 +151,11 @@ ABI = [
     ("rphys_ext_get_pairs", c_uint32, [c_void_p, c_void_p, c_uint32, POINTER(c_uint32)]),
     ("rphys_ext_get_contact_records", c_uint32, [c_void_p, POINTER(ContactRecord), c_uint32, POINTER(c_uint32)]),
     ("rphys_ext_get_body_states", c_uint32, [c_void_p, c_uint32, c_uint32, c_void_p]),
+    ("rphys_ext_profile_enable", c_uint32, [c_void_p, c_uint32]),
+    ("rphys_ext_profile_read", c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, POINTER(c_uint32)]),
+    ("rphys_ext_profile_stage_name", c_char_p, [c_uint32]),
+    ("rphys_ext_stream_handle", c_uint32, [c_void_p, POINTER(c_uint64)]),
+    ("rphys_ext_launch_count", c_uint32, [POINTER(c_uint64)]),
 ]
 
 
@@ -181,6 +186,11 @@ class Lib:
             msg = self.dll.rphys_last_error_message()
             raise RPhysError(r, msg.decode() if msg else "")
         return r
+
+    def launch_count(self):
+        n = c_uint64(0)
+        self.call("rphys_ext_launch_count", byref(n))
+        return n.value
 
     def world(self, max_bodies=1024, max_colliders=2048):
         return World(self, max_bodies, max_colliders)
@@ -350,6 +360,24 @@ class World:
         buf = (ContactRecord * max(1, n.value))()
         self.c("rphys_ext_get_contact_records", buf, n.value, byref(n))
         return list(buf)[: n.value]
+
+    def stream_handle(self):
+        s = c_uint64(0)
+        self.c("rphys_ext_stream_handle", byref(s))
+        return s.value
+
+    def profile(self, on=True):
+        self.c("rphys_ext_profile_enable", 1 if on else 0)
+
+    def profile_read(self):
+        """{stage: (total ms, ticks)} since profiling was enabled (CUDA library only)."""
+        import numpy as np
+        ms = np.zeros(64, dtype=np.float64)
+        ticks = np.zeros(64, dtype=np.uint64)
+        n = c_uint32(0)
+        self.c("rphys_ext_profile_read", ms.ctypes.data_as(c_void_p), ticks.ctypes.data_as(c_void_p), 64, byref(n))
+        names = [self.lib.dll.rphys_ext_profile_stage_name(i).decode() for i in range(n.value)]
+        return {names[i]: (float(ms[i]), int(ticks[i])) for i in range(n.value)}
 
     def body_states(self, first=0, count=None):
         import numpy as np

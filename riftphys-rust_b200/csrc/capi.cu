@@ -14,6 +14,9 @@
 #include "world_gpu.h"
 
 using rp::WorldGpu;
+namespace rp {
+extern unsigned long long g_launches;
+}
 
 static thread_local std::string g_err;
 static thread_local bool g_has_err = false;
@@ -542,6 +545,7 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
     o->max_batch = s.max_batch; o->warm_matched = s.warm_matched; o->sweeps = s.sweeps;
     o->bounce_skipped = s.bounce_skipped; o->warm_entries = s.warm_entries; o->sleeping = s.sleeping;
     o->error_flags = s.error_flags; o->residual = s.residual;
+    o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
     return (RPhysResult)RPHYS_OK;
   });
 }
@@ -591,6 +595,44 @@ RPhysResult rphys_ext_get_body_states(const RPhysWorld* Wc, uint32_t first, uint
     W->w->get_body_states(first, count, out);
     return (RPhysResult)RPHYS_OK;
   });
+}
+
+RPhysResult rphys_ext_profile_enable(RPhysWorld* W, uint32_t on) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_profile_enable: world is null");
+  LOCK;
+  W->w->profile_enable(on != 0);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_profile_read(const RPhysWorld* Wc, double* ms, uint64_t* ticks, uint32_t cap, uint32_t* out_n) {
+  clear_err();
+  if (!Wc || !out_n) return fail(RPHYS_ERR_NULL, "rphys_ext_profile_read: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  LOCK;
+  std::vector<double> m(64);
+  std::vector<uint64_t> c(64);
+  int n = W->w->profile_read(m.data(), c.data(), 64);
+  *out_n = (uint32_t)n;
+  for (int i = 0; i < n && (uint32_t)i < cap; ++i) {
+    if (ms) ms[i] = m[i];
+    if (ticks) ticks[i] = c[i];
+  }
+  return RPHYS_OK;
+}
+const char* rphys_ext_profile_stage_name(uint32_t stage) { return WorldGpu::phase_name((int)stage); }
+
+RPhysResult rphys_ext_stream_handle(const RPhysWorld* Wc, uint64_t* out) {
+  clear_err();
+  if (!Wc || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_stream_handle: null arg");
+  *out = (uint64_t)(uintptr_t)Wc->w->stream();
+  return RPHYS_OK;
+}
+
+RPhysResult rphys_ext_launch_count(uint64_t* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_ext_launch_count: null arg");
+  *out = rp::g_launches;
+  return RPHYS_OK;
 }
 
 }  // extern "C"

@@ -176,7 +176,7 @@ void WorldGpu::step_hash(uint8_t out32[32]) {
   S.woff.ensure(n_warm + 1); S.wpos.ensure(n_warm + 1);
   uint32_t nkeys = 0;
   if (n_warm) {
-    k_h_warm_flags<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, S.woff.p);
+    k_h_warm_flags<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, S.woff.p); RP_COUNT_LAUNCH(1);
     nkeys = exclusive_scan_total(S, S.woff.p, S.wpos.p, n_warm, st);
   }
   uint64_t off_bodies = 48;
@@ -195,25 +195,25 @@ void WorldGpu::step_hash(uint8_t out32[32]) {
                                      0x12, 0xb7, 0xcc, 0x9a, 0x93, 0xca, 0xe4, 0x1f, 0x32, 0x62};
   std::memcpy(head + 16, kEmpty, 32);
   RP_CUDA(cudaMemcpyAsync(S.hbuf.p, head, 48, cudaMemcpyHostToDevice, st));
-  if (nb_) k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, S.hbuf.p + off_bodies);
+  if (nb_) k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, S.hbuf.p + off_bodies); RP_COUNT_LAUNCH(1);
   uint8_t wcount[8];
   p64(wcount, nkeys);
   RP_CUDA(cudaMemcpyAsync(S.hbuf.p + off_warm, wcount, 8, cudaMemcpyHostToDevice, st));
   if (n_warm)
     k_h_warm<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, warm_a.p, warm_b.p, S.woff.p, S.wpos.p,
-                                                  S.hbuf.p + off_warm + 8);
+                                                  S.hbuf.p + off_warm + 8); RP_COUNT_LAUNCH(1);
   // the three zero-length maps are already zero bytes
   uint32_t nt = cap > nb_ ? cap : nb_;
-  k_h_tail<<<(nt + T) / T, T, 0, st>>>(nb_, cap, last_lin.p, awake.p, sleep_ticks.p, S.hbuf.p + off_tail);
+  k_h_tail<<<(nt + T) / T, T, 0, st>>>(nb_, cap, last_lin.p, awake.p, sleep_ticks.p, S.hbuf.p + off_tail); RP_COUNT_LAUNCH(1);
   S.hcv.ensure(16 * (size_t)nch + 16);
   uint32_t* root = S.hcv.p;
   uint32_t* a = S.hcv.p + 8;
   uint32_t* b = S.hcv.p + 8 + 8 * (size_t)nch;
-  k_b3_chunks<<<(nch + 127) / 128, 128, 0, st>>>(S.hbuf.p, len, nch, a, root);
+  k_b3_chunks<<<(nch + 127) / 128, 128, 0, st>>>(S.hbuf.p, len, nch, a, root); RP_COUNT_LAUNCH(1);
   uint32_t n = nch;
   while (n > 1) {
     uint32_t n_out = (n + 1) / 2;
-    k_b3_parents<<<(n_out + 127) / 128, 128, 0, st>>>(n, a, b, root);
+    k_b3_parents<<<(n_out + 127) / 128, 128, 0, st>>>(n, a, b, root); RP_COUNT_LAUNCH(1);
     std::swap(a, b);
     n = n_out;
   }

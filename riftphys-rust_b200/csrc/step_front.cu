@@ -374,17 +374,23 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   cudaStream_t st = W.stream();
   const int nb = (int)W.num_bodies(), ncol = (int)W.num_colliders();
   const int T = 256;
+  auto& P = S.prof;
   // stage 1
+  P.begin(PH_FORCES, st);
   if (nb > 0)
     k_forces<<<(nb + T - 1) / T, T, 0, st>>>(nb, W.lin.p, W.ang.p, W.lin.p, S.pre_lin.p, S.pre_ang.p, W.dyn.p,
-                                              W.awake.p, ctx.g, ctx.dt);
+                                              W.awake.p, ctx.g, ctx.dt); RP_COUNT_LAUNCH(1);
+  P.end(PH_FORCES, st);
+  P.begin(PH_AABB, st);
   // stage 2: AABBs, sweep, classification
   S.amin.ensure(ncol); S.amax.ensure(ncol); S.smin.ensure(ncol); S.smax.ensure(ncol); S.sweep.ensure(ncol);
   S.u32a.ensure(ncol + 1); S.u32b.ensure(ncol + 1);
   if (ncol > 0)
     k_aabbs<<<(ncol + T - 1) / T, T, 0, st>>>(ncol, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, W.lin.p,
                                                W.ang.p, ctx.dt, S.amin.p, S.amax.p, S.smin.p, S.smax.p, S.sweep.p,
-                                               S.u32a.p, S.u32b.p, W.d_stats.p + STAT_ERR);
+                                               S.u32a.p, S.u32b.p, W.d_stats.p + STAT_ERR); RP_COUNT_LAUNCH(1);
+  P.end(PH_AABB, st);
+  P.begin(PH_BROAD, st);
   // broadphase: in-grid colliders sorted along x, oversized list
   S.sap_ids.ensure(ncol + 1); S.over_ids.ensure(ncol + 1); S.counts.ensure(4);
   uint32_t n_sap = 0, n_over = 0;
@@ -401,55 +407,61 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   S.ov_cnt.ensure(ncol + 1); S.ov_off.ensure(ncol + 1);
   uint32_t n_sap_pairs = 0, n_ov_pairs = 0;
   if (n_sap > 0) {
-    k_sap_keys<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.sap_key.p);
+    k_sap_keys<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.sap_key.p); RP_COUNT_LAUNCH(1);
     sort_pairs_u32(S, S.sap_key.p, S.sap_key2.p, S.sap_ids.p, S.sap_ord.p, n_sap, 0, 32, st);
-    k_gather_minx<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.smin.p, S.minx.p);
+    k_gather_minx<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.smin.p, S.minx.p); RP_COUNT_LAUNCH(1);
     k_sap_sweep<false><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, S.sap_cnt.p,
-                                                           nullptr, nullptr);
+                                                           nullptr, nullptr); RP_COUNT_LAUNCH(1);
     n_sap_pairs = exclusive_scan_total(S, S.sap_cnt.p, S.sap_off.p, n_sap, st);
   }
   if (n_over > 0 && ncol > 0) {
     k_oversized<false><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, S.ov_cnt.p,
-                                                          nullptr, nullptr);
+                                                          nullptr, nullptr); RP_COUNT_LAUNCH(1);
     n_ov_pairs = exclusive_scan_total(S, S.ov_cnt.p, S.ov_off.p, ncol, st);
   }
   uint32_t n_raw = n_sap_pairs + n_ov_pairs;
   S.pairs.ensure(n_raw + 1); S.pairs2.ensure(n_raw + 1); S.flag8.ensure(n_raw + 1);
   if (n_sap_pairs > 0)
     k_sap_sweep<true><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, nullptr,
-                                                          S.sap_off.p, S.pairs2.p);
+                                                          S.sap_off.p, S.pairs2.p); RP_COUNT_LAUNCH(1);
   if (n_ov_pairs > 0)
     k_oversized<true><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, nullptr,
-                                                         S.ov_off.p, S.pairs2.p + n_sap_pairs);
+                                                         S.ov_off.p, S.pairs2.p + n_sap_pairs); RP_COUNT_LAUNCH(1);
   uint32_t np = 0;
   if (n_raw > 0) {
     sort_keys_u64(S, S.pairs2.p, S.pairs.p, n_raw, st);  // -> S.pairs
-    k_unique_flags<<<(n_raw + T - 1) / T, T, 0, st>>>(n_raw, S.pairs.p, S.flag8.p);
+    k_unique_flags<<<(n_raw + T - 1) / T, T, 0, st>>>(n_raw, S.pairs.p, S.flag8.p); RP_COUNT_LAUNCH(1);
     np = select_flagged_u64(S, S.pairs.p, S.flag8.p, S.pairs2.p, n_raw, st);
     cudaMemcpyAsync(S.pairs.p, S.pairs2.p, sizeof(unsigned long long) * np, cudaMemcpyDeviceToDevice, st);
   }
   ctx.np = np;
   W.n_pairs = np;
+  P.end(PH_BROAD, st);
+  P.begin(PH_NARROW, st);
   // narrowphase over pairs
   S.p_pt.ensure(4 * (size_t)np + 4); S.p_n.ensure(4 * (size_t)np + 4); S.p_cnt.ensure(np + 1);
   if (np > 0)
     k_narrow_pairs<<<(np + 127) / 128, 128, 0, st>>>(np, S.pairs.p, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p,
-                                                    W.rot.p, S.sweep.p, S.p_pt.p, S.p_n.p, S.p_cnt.p);
+                                                    W.rot.p, S.sweep.p, S.p_pt.p, S.p_n.p, S.p_cnt.p); RP_COUNT_LAUNCH(1);
+  P.end(PH_NARROW, st);
+  P.begin(PH_TERRAIN, st);
   // terrain
   S.t_pt.ensure(4 * (size_t)ncol + 4); S.t_n.ensure(4 * (size_t)ncol + 4); S.t_cnt.ensure(ncol + 1);
   bool terrain = ctx.hf.h != nullptr;
   if (terrain && ncol > 0)
     k_terrain<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, ctx.hf, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p,
-                                                 W.rot.p, S.sweep.p, S.amin.p, S.amax.p, S.t_pt.p, S.t_n.p, S.t_cnt.p);
+                                                 W.rot.p, S.sweep.p, S.amin.p, S.amax.p, S.t_pt.p, S.t_n.p, S.t_cnt.p); RP_COUNT_LAUNCH(1);
+  P.end(PH_TERRAIN, st);
+  P.begin(PH_CONTACTS, st);
   // merge buckets in key order, scan, scatter
   S.pstart.ensure(ncol + 2);
-  k_pair_starts<<<(ncol + 1 + T - 1) / T, T, 0, st>>>(ncol, np, S.pairs.p, S.pstart.p);
+  k_pair_starts<<<(ncol + 1 + T - 1) / T, T, 0, st>>>(ncol, np, S.pairs.p, S.pstart.p); RP_COUNT_LAUNCH(1);
   uint32_t nbk = np + ncol;
   S.bcnt.ensure(nbk + 1); S.boff.ensure(nbk + 1);
   uint32_t nc = 0;
   if (nbk > 0) {
     k_bucket_counts<<<(nbk + T - 1) / T, T, 0, st>>>(np, ncol, S.pairs.p, S.p_cnt.p, terrain ? S.t_cnt.p : nullptr,
-                                                    S.pstart.p, S.bcnt.p);
+                                                    S.pstart.p, S.bcnt.p); RP_COUNT_LAUNCH(1);
     nc = exclusive_scan_total(S, S.bcnt.p, S.boff.p, nbk, st);
   }
   ctx.nc = nc;
@@ -459,7 +471,8 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
     k_scatter_contacts<<<(nbk + T - 1) / T, T, 0, st>>>(np, ncol, S.pairs.p, S.p_cnt.p, S.p_pt.p, S.p_n.p,
                                                        terrain ? S.t_cnt.p : nullptr, S.t_pt.p, S.t_n.p, S.pstart.p,
                                                        S.boff.p, W.col_body.p, W.pos.p, S.c_a.p, S.c_b.p, S.c_pt.p,
-                                                       S.c_n.p);
+                                                       S.c_n.p); RP_COUNT_LAUNCH(1);
+  P.end(PH_CONTACTS, st);
 }
 
 }  // namespace rp

@@ -18,6 +18,11 @@ namespace rp {
                                " at " __FILE__ ":" + std::to_string(__LINE__));         \
   } while (0)
 
+// Kernel launches issued by this library (exact: every launch site adds its count; each
+// device-wide sort / scan / select adds the kernels it runs).
+extern unsigned long long g_launches;
+#define RP_COUNT_LAUNCH(n) (::rp::g_launches += (n))
+
 // d_stats slots
 enum : int {
   STAT_ERR = 0,          // RPHYS_STATERR_* bits
@@ -29,7 +34,49 @@ enum : int {
   STAT_LEVELS = 6,
   STAT_MAXBATCH = 7,
   STAT_NISL = 8,
+  STAT_ROWSWEEPS = 9,    // velocity row updates this tick (rows x sweeps, summed over islands)
   STAT_COUNT = 16
+};
+
+
+
+// Stages timed with CUDA events on the world's stream when profiling is on.
+enum Phase : int {
+  PH_FORCES = 0, PH_AABB, PH_BROAD, PH_NARROW, PH_TERRAIN, PH_CONTACTS, PH_ISLANDS, PH_ROWS, PH_SCHED,
+  PH_WARM_MATCH, PH_VEL_SOLVE, PH_WARM_CACHE, PH_VEL_SHOCK, PH_BALLISTIC, PH_INTEGRATE, PH_POS_ITER,
+  PH_POS_SHOCK, PH_STAGE6, PH_COUNT
+};
+static const char* const kPhaseNames[PH_COUNT] = {
+    "forces", "aabb_sweep", "broadphase", "narrow_pairs", "terrain", "contacts", "islands", "rows", "schedule",
+    "warm_match", "vel_solve", "warm_cache", "vel_shock", "ballistic", "integrate", "pos_iter", "pos_shock", "stage6"};
+
+struct Profiler {
+  bool on = false;
+  cudaEvent_t ev[PH_COUNT][2] = {};
+  bool used[PH_COUNT] = {};
+  double ms[PH_COUNT] = {};
+  uint64_t calls[PH_COUNT] = {};
+  void begin(int p, cudaStream_t st) {
+    if (!on) return;
+    if (!ev[p][0]) { cudaEventCreate(&ev[p][0]); cudaEventCreate(&ev[p][1]); }
+    cudaEventRecord(ev[p][0], st);
+  }
+  void end(int p, cudaStream_t st) {
+    if (!on) return;
+    cudaEventRecord(ev[p][1], st);
+    used[p] = true;
+  }
+  // after the stream is idle: fold this tick's events into the totals
+  void collect() {
+    if (!on) return;
+    for (int p = 0; p < PH_COUNT; ++p) {
+      if (!used[p]) continue;
+      float t = 0.0f;
+      if (cudaEventElapsedTime(&t, ev[p][0], ev[p][1]) == cudaSuccess) { ms[p] += t; calls[p] += 1; }
+      used[p] = false;
+    }
+  }
+  void reset() { for (int p = 0; p < PH_COUNT; ++p) { ms[p] = 0; calls[p] = 0; used[p] = false; } }
 };
 
 template <class T>
@@ -90,6 +137,9 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> hcv;
   // primitives' temporary storage
   DBuf<uint8_t> cub_tmp;
+  DBuf<uint4> kept_k;
+  DBuf<float4> kept_a, kept_b;
+  Profiler prof;
 };
 
 // The heightfield as the terrain kernel reads it (HeightField, terrain.rs:13-21); h == nullptr: none.

@@ -6,6 +6,8 @@
 
 namespace rp {
 
+unsigned long long g_launches = 0;
+
 namespace {
 template <class F>
 void with_tmp(WorldGpu::Scratch& S, F f) {
@@ -22,6 +24,7 @@ void select_flagged_iota(WorldGpu::Scratch& S, int n, const uint32_t* flags, uin
   with_tmp(S, [&](void* t, size_t& b) {
     RP_CUDA(cub::DeviceSelect::Flagged(t, b, it, flags, out, d_count, n, st));
   });
+  RP_COUNT_LAUNCH(2);
 }
 
 uint32_t select_flagged_u64(WorldGpu::Scratch& S, const unsigned long long* in, const uint8_t* flags,
@@ -30,6 +33,7 @@ uint32_t select_flagged_u64(WorldGpu::Scratch& S, const unsigned long long* in, 
   with_tmp(S, [&](void* t, size_t& b) {
     RP_CUDA(cub::DeviceSelect::Flagged(t, b, in, flags, out, S.counts.p + 2, n, st));
   });
+  RP_COUNT_LAUNCH(2);
   uint32_t c = 0;
   RP_CUDA(cudaMemcpyAsync(&c, S.counts.p + 2, 4, cudaMemcpyDeviceToHost, st));
   RP_CUDA(cudaStreamSynchronize(st));
@@ -42,6 +46,7 @@ uint32_t select_flagged_u32(WorldGpu::Scratch& S, const uint32_t* in, const uint
   with_tmp(S, [&](void* t, size_t& b) {
     RP_CUDA(cub::DeviceSelect::Flagged(t, b, in, flags, out, S.counts.p + 3, n, st));
   });
+  RP_COUNT_LAUNCH(2);
   uint32_t c = 0;
   RP_CUDA(cudaMemcpyAsync(&c, S.counts.p + 3, 4, cudaMemcpyDeviceToHost, st));
   RP_CUDA(cudaStreamSynchronize(st));
@@ -54,6 +59,7 @@ void sort_pairs_u32(WorldGpu::Scratch& S, const uint32_t* kin, uint32_t* kout, c
   with_tmp(S, [&](void* t, size_t& b) {
     RP_CUDA(cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int)n, bit0, bit1, st));
   });
+  RP_COUNT_LAUNCH(1 + (bit1 - bit0 + 7) / 8);
 }
 
 void sort_pairs_u64(WorldGpu::Scratch& S, const unsigned long long* kin, unsigned long long* kout, const uint32_t* vin,
@@ -62,6 +68,7 @@ void sort_pairs_u64(WorldGpu::Scratch& S, const unsigned long long* kin, unsigne
   with_tmp(S, [&](void* t, size_t& b) {
     RP_CUDA(cub::DeviceRadixSort::SortPairs(t, b, kin, kout, vin, vout, (int)n, bit0, bit1, st));
   });
+  RP_COUNT_LAUNCH(1 + (bit1 - bit0 + 7) / 8);
 }
 
 void sort_keys_u64(WorldGpu::Scratch& S, const unsigned long long* kin, unsigned long long* kout, uint32_t n,
@@ -70,6 +77,7 @@ void sort_keys_u64(WorldGpu::Scratch& S, const unsigned long long* kin, unsigned
   with_tmp(S, [&](void* t, size_t& b) {
     RP_CUDA(cub::DeviceRadixSort::SortKeys(t, b, kin, kout, (int)n, 0, 64, st));
   });
+  RP_COUNT_LAUNCH(9);
 }
 
 void exclusive_scan(WorldGpu::Scratch& S, const uint32_t* in, uint32_t* out, uint32_t n, cudaStream_t st) {
@@ -77,6 +85,7 @@ void exclusive_scan(WorldGpu::Scratch& S, const uint32_t* in, uint32_t* out, uin
   with_tmp(S, [&](void* t, size_t& b) {
     RP_CUDA(cub::DeviceScan::ExclusiveSum(t, b, in, out, (int)n, st));
   });
+  RP_COUNT_LAUNCH(2);
 }
 
 // Exclusive sum of in[0, n) into out; returns the total (one device-to-host read).

@@ -421,6 +421,7 @@ __global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* a
     if (tol > 0.0f && resid <= tol) break;
   }
   if (lane == 0) {
+    atomicAdd(&stats[STAT_ROWSWEEPS], (S.lvl_start[off + nl] - S.lvl_start[off]) * (uint32_t)it);
     atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
     atomicMax(&stats[STAT_RESID], fbits(resid));
   }
@@ -817,14 +818,14 @@ static void build_schedule(WorldGpu::Scratch& S, uint32_t nsched, uint32_t nisl,
   lvl_off.ensure(nisl + 1);
   S.key64.ensure(nsched + 1); S.key64b.ensure(nsched + 1);
   k_levels<<<nblk(nisl, 128), 128, 0, st>>>(nisl, isl_start, isl_cnt, ord_in, S.r_ab.p, S.r_flags.p, S.body_level.p,
-                                            S.key64.p, nlev.p, row_level);
+                                            S.key64.p, nlev.p, row_level); RP_COUNT_LAUNCH(1);
   sort_pairs_u64(S, S.key64.p, S.key64b.p, ord_in, ord_out, nsched, 0, 64, st);
   S.tmp32.ensure(nisl + 1);
-  k_plus1<<<nblk(nisl), T, 0, st>>>(nisl, nlev.p, S.tmp32.p);
+  k_plus1<<<nblk(nisl), T, 0, st>>>(nisl, nlev.p, S.tmp32.p); RP_COUNT_LAUNCH(1);
   uint32_t total = exclusive_scan_total(S, S.tmp32.p, lvl_off.p, nisl, st);
   lvl_start.ensure(total + 1);
   k_level_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.key64b.p, lvl_off.p, nlev.p, isl_start, isl_cnt, lvl_start.p,
-                                             hist);
+                                             hist); RP_COUNT_LAUNCH(1);
 }
 
 void run_solve(WorldGpu& W, StepCtx& ctx) {
@@ -845,13 +846,15 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   BodiesV B{W.pos.p, W.rot.p, W.lin.p, W.ang.p, W.inv_mass.p, S.Iw.p, W.inv_I.p, W.awake.p, W.dyn.p};
   RowsV R{S.r_ab.p, S.r_flags.p, S.r_inv.p, S.r_ra.p, S.r_rb.p, S.r_n.p, S.r_t1.p, S.r_t2.p, S.r_mu.p, S.r_la.p};
   ctx.nisl = 0;
+  auto& P = S.prof;
+  P.begin(PH_ISLANDS, st);
   // ---- the reference's islands: their count, and whether the solve runs (step.rs:146-150)
   uint32_t nref = 0;
   if (nc > 0 && nb > 0) {
-    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf2.p);
+    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf2.p); RP_COUNT_LAUNCH(1);
     RP_CUDA(cudaMemsetAsync(S.root_mark.p, 0, sizeof(uint32_t) * nb, st));
-    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 0, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf2.p);
-    k_ref_island_marks<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, S.uf2.p, S.root_mark.p);
+    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 0, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf2.p); RP_COUNT_LAUNCH(1);
+    k_ref_island_marks<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, S.uf2.p, S.root_mark.p); RP_COUNT_LAUNCH(1);
     S.tmp32.ensure(nb + 1);
     nref = exclusive_scan_total(S, S.root_mark.p, S.tmp32.p, nb, st);
   }
@@ -860,23 +863,27 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   S.row_level.ensure(nc + 1);
   RP_CUDA(cudaMemsetAsync(S.row_level.p, 0xFF, sizeof(uint32_t) * (nc + 1), st));
   W.levels_valid_ = true;
+  P.end(PH_ISLANDS, st);
   if (nref > 0) {
     // ---- rows
-    k_world_inertia<<<nblk(nb), T, 0, st>>>(nb, W.rot.p, W.inv_mass.p, W.inv_I.p, S.Iw.p);
-    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf.p);
-    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 1, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf.p);
+    P.begin(PH_ROWS, st);
+    k_world_inertia<<<nblk(nb), T, 0, st>>>(nb, W.rot.p, W.inv_mass.p, W.inv_I.p, S.Iw.p); RP_COUNT_LAUNCH(1);
+    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf.p); RP_COUNT_LAUNCH(1);
+    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 1, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf.p); RP_COUNT_LAUNCH(1);
     S.r_ab.ensure(nc); S.r_flags.ensure(nc); S.r_inv.ensure(nc); S.r_ra.ensure(nc); S.r_rb.ensure(nc); S.r_n.ensure(nc);
     S.r_t1.ensure(nc); S.r_t2.ensure(nc); S.r_mu.ensure(nc); S.r_la.ensure(nc); S.acc_jn.ensure(nc); S.acc_jt.ensure(nc);
     S.wm_idx.ensure(nc); S.row_isl.ensure(nc + 1); S.row_isl2.ensure(nc + 1);
     R = RowsV{S.r_ab.p, S.r_flags.p, S.r_inv.p, S.r_ra.p, S.r_rb.p, S.r_n.p, S.r_t1.p, S.r_t2.p, S.r_mu.p, S.r_la.p};
     k_build_rows<<<nblk(nc), T, 0, st>>>(nc, ctx.dt, S.c_a.p, S.c_b.p, S.c_pt.p, S.c_n.p, W.col_body.p, W.col_mat.p,
                                          ctx.hf_mat, W.pair_table.p, B, S.pre_lin.p, S.pre_ang.p, R, S.acc_jn.p,
-                                         S.acc_jt.p, S.uf.p, S.row_isl.p);
+                                         S.acc_jt.p, S.uf.p, S.row_isl.p); RP_COUNT_LAUNCH(1);
+    P.end(PH_ROWS, st);
+    P.begin(PH_SCHED, st);
     // ---- solve islands: roots of scheduled rows -> dense island ids, rows grouped by island
     S.flag8.ensure(nc + 1); S.rows_sched.ensure(nc + 1); S.rows_sched2.ensure(nc + 1);
     S.tmp32.ensure(nc + 1); S.tmp32b.ensure(nc + 1);
     uint32_t nsched = 0;
-    k_flag_sched<<<nblk(nc), T, 0, st>>>(nc, S.row_isl.p, S.flag8.p);
+    k_flag_sched<<<nblk(nc), T, 0, st>>>(nc, S.row_isl.p, S.flag8.p); RP_COUNT_LAUNCH(1);
     {
       cub::CountingInputIterator<uint32_t> it0(0);
       size_t bytes = 0;
@@ -884,6 +891,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it0, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nc, st));
       S.cub_tmp.ensure(bytes + 16);
       RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, it0, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nc, st));
+      RP_COUNT_LAUNCH(2);
       RP_CUDA(cudaMemcpyAsync(&nsched, S.counts.p + 3, 4, cudaMemcpyDeviceToHost, st));
       RP_CUDA(cudaStreamSynchronize(st));
     }
@@ -893,13 +901,13 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     S.ord_main.ensure(nsched + 1); S.ord_vs.ensure(nsched + 1); S.ord_ps.ensure(nsched + 1);
     if (nsched > 0) {
       // island root per scheduled row; sorting (root, row) makes each island's rows contiguous, in order
-      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.row_isl.p, S.tmp32.p);
+      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.row_isl.p, S.tmp32.p); RP_COUNT_LAUNCH(1);
       sort_pairs_u32(S, S.tmp32.p, S.tmp32b.p, S.rows_sched.p, S.rows_sched2.p, nsched, 0, 32, st);
       S.woff.ensure(nsched + 1); S.wpos.ensure(nsched + 1);
-      k_run_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32b.p, S.woff.p);
+      k_run_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32b.p, S.woff.p); RP_COUNT_LAUNCH(1);
       nisl = exclusive_scan_total(S, S.woff.p, S.wpos.p, nsched, st);
-      k_island_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.woff.p, S.wpos.p, S.isl_start.p);
-      k_island_counts<<<nblk(nisl), T, 0, st>>>(nisl, nsched, S.isl_start.p, S.isl_cnt.p);
+      k_island_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.woff.p, S.wpos.p, S.isl_start.p); RP_COUNT_LAUNCH(1);
+      k_island_counts<<<nblk(nisl), T, 0, st>>>(nisl, nsched, S.isl_start.p, S.isl_cnt.p); RP_COUNT_LAUNCH(1);
       ctx.nisl = nisl;
       // ---- main schedule (row order within each island)
       S.lvl_hist.ensure(nsched + 1);
@@ -912,46 +920,59 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
         RP_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.nlev.p, stats + STAT_LEVELS, nisl, st));
         S.cub_tmp.ensure(bytes + 16);
         RP_CUDA(cub::DeviceReduce::Max(S.cub_tmp.p, bytes, S.nlev.p, stats + STAT_LEVELS, nisl, st));
+        RP_COUNT_LAUNCH(2);
         bytes = 0;
         RP_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.lvl_hist.p, stats + STAT_MAXBATCH, nsched, st));
         S.cub_tmp.ensure(bytes + 16);
         RP_CUDA(cub::DeviceReduce::Max(S.cub_tmp.p, bytes, S.lvl_hist.p, stats + STAT_MAXBATCH, nsched, st));
+        RP_COUNT_LAUNCH(2);
       }
     }
+    P.end(PH_SCHED, st);
     Sched SM{S.ord_main.p, S.lvl_off.p, S.lvl_start.p, S.nlev.p};
+    P.begin(PH_WARM_MATCH, st);
     // ---- warm start matching (solver.rs:717-762)
     k_warm_match<<<nblk(nc), T, 0, st>>>(nc, S.r_ab.p, S.r_flags.p, S.r_la.p, W.warm_key.p, W.warm_a.p, W.n_warm,
-                                         S.wm_idx.p, stats + STAT_WARM_MATCHED, stats + STAT_ERR);
-    k_warm_unscheduled<<<nblk(nc), T, 0, st>>>(nc, R, B, S.wm_idx.p, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p);
+                                         S.wm_idx.p, stats + STAT_WARM_MATCHED, stats + STAT_ERR); RP_COUNT_LAUNCH(1);
+    k_warm_unscheduled<<<nblk(nc), T, 0, st>>>(nc, R, B, S.wm_idx.p, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p); RP_COUNT_LAUNCH(1);
+    P.end(PH_WARM_MATCH, st);
+    P.begin(PH_VEL_SOLVE, st);
     // ---- warm application + velocity sweeps
     const bool resid_mode = W.res_tol_ > 0.0f;
     int iters = (int)(resid_mode ? (W.res_max_ > 0 ? W.res_max_ : W.iters_v_) : W.iters_v_);
     if (nisl > 0)
       k_vel_solve<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p, W.warm_a.p,
-                                                        W.warm_b.p, iters, resid_mode ? W.res_tol_ : 0.0f, stats);
+                                                        W.warm_b.p, iters, resid_mode ? W.res_tol_ : 0.0f, stats); RP_COUNT_LAUNCH(1);
+    P.end(PH_VEL_SOLVE, st);
+    P.begin(PH_WARM_CACHE, st);
     // ---- warm-start cache for the next tick (solver.rs:917-944)
     {
       S.woff.ensure(nc + 1); S.wpos.ensure(nc + 1);
-      k_warm_new_flags<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.wpos.p);
+      k_warm_new_flags<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.wpos.p); RP_COUNT_LAUNCH(1);
       uint32_t n_new = exclusive_scan_total(S, S.wpos.p, S.woff.p, nc, st);
       // new keys alone first (positions without the old-kept offsets), to test old entries against
       W.warm_key2.ensure(n_new + W.n_warm + 1); W.warm_a2.ensure(n_new + W.n_warm + 1); W.warm_b2.ensure(n_new + W.n_warm + 1);
       k_warm_new_write<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.wpos.p, S.woff.p, nullptr, nullptr, 0,
-                                               W.warm_key2.p, W.warm_a2.p, W.warm_b2.p);
+                                               W.warm_key2.p, W.warm_a2.p, W.warm_b2.p); RP_COUNT_LAUNCH(1);
       uint32_t n_kept = 0;
       S.wflag.ensure(W.n_warm + 1);
-      DBuf<uint4> kept_k; DBuf<float4> kept_a, kept_b;
+      DBuf<uint4>& kept_k = S.kept_k;
+      DBuf<float4>& kept_a = S.kept_a;
+      DBuf<float4>& kept_b = S.kept_b;
       if (W.n_warm > 0) {
         k_warm_old_flags<<<nblk(W.n_warm), T, 0, st>>>(W.n_warm, W.warm_key.p, W.warm_key2.p, n_new, W.alive_d.p, W.dyn.p,
-                                                       W.awake.p, nb, S.wflag.p);
+                                                       W.awake.p, nb, S.wflag.p); RP_COUNT_LAUNCH(1);
         kept_k.ensure(W.n_warm + 1); kept_a.ensure(W.n_warm + 1); kept_b.ensure(W.n_warm + 1);
         size_t bytes = 0;
         S.counts.ensure(4);
         RP_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, W.warm_key.p, S.wflag.p, kept_k.p, S.counts.p + 3, W.n_warm, st));
         S.cub_tmp.ensure(bytes + 16);
         RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, W.warm_key.p, S.wflag.p, kept_k.p, S.counts.p + 3, W.n_warm, st));
+        RP_COUNT_LAUNCH(2);
         RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, W.warm_a.p, S.wflag.p, kept_a.p, S.counts.p + 3, W.n_warm, st));
+        RP_COUNT_LAUNCH(2);
         RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, W.warm_b.p, S.wflag.p, kept_b.p, S.counts.p + 3, W.n_warm, st));
+        RP_COUNT_LAUNCH(2);
         RP_CUDA(cudaMemcpyAsync(&n_kept, S.counts.p + 3, 4, cudaMemcpyDeviceToHost, st));
         RP_CUDA(cudaStreamSynchronize(st));
       }
@@ -964,62 +985,75 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
         // merge: new entry k at off[k] + #kept below its key; kept entry j at j + #new below its key
         W.warm_key.ensure(n_new + n_kept + 1); W.warm_a.ensure(n_new + n_kept + 1); W.warm_b.ensure(n_new + n_kept + 1);
         k_warm_new_write<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.wpos.p, S.woff.p, nullptr, kept_k.p,
-                                                 n_kept, W.warm_key.p, W.warm_a.p, W.warm_b.p);
+                                                 n_kept, W.warm_key.p, W.warm_a.p, W.warm_b.p); RP_COUNT_LAUNCH(1);
         k_warm_merge_kept<<<nblk(n_kept), T, 0, st>>>(n_kept, kept_k.p, kept_a.p, kept_b.p, W.warm_key2.p, n_new, W.warm_key.p,
-                                        W.warm_a.p, W.warm_b.p);
+                                        W.warm_a.p, W.warm_b.p); RP_COUNT_LAUNCH(1);
         W.n_warm = n_new + n_kept;
         RP_CUDA(cudaStreamSynchronize(st));
       }
     }
+    P.end(PH_WARM_CACHE, st);
+    P.begin(PH_VEL_SHOCK, st);
     // ---- shock propagation (solver.rs:964-993)
     if (nisl > 0) {
-      k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p);
+      k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p); RP_COUNT_LAUNCH(1);
       sort_pairs_u64(S, S.key64.p, S.key64b.p, S.rows_sched.p, S.tmp32.p, nsched, 0, 64, st);  // by height key, stable
-      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p);      // their roots
+      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p); RP_COUNT_LAUNCH(1);      // their roots
       sort_pairs_u32(S, S.tmp32b.p, S.woff.p, S.tmp32.p, S.rows_sched2.p, nsched, 0, 32, st);   // by island, stable
       build_schedule(S, nsched, nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_vs.p, S.lvl_off_vs,
                      S.lvl_start_vs, S.nlev_vs, nullptr, nullptr, st);
       Sched SV{S.ord_vs.p, S.lvl_off_vs.p, S.lvl_start_vs.p, S.nlev_vs.p};
-      k_vel_shock<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, SV, R, B, ctx.up, S.acc_jn.p);
+      k_vel_shock<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, SV, R, B, ctx.up, S.acc_jn.p); RP_COUNT_LAUNCH(1);
     }
-    k_after_solve<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.loaded.p, S.c_n.p, stats);
+    P.end(PH_VEL_SHOCK, st);
+    k_after_solve<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.loaded.p, S.c_n.p, stats); RP_COUNT_LAUNCH(1);
   }
   // ---- stage 4
-  if (nc > 0) k_constrained<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, S.constrained.p);
-  if (nb > 0) k_ballistic_init<<<nblk(nb), T, 0, st>>>(nb, S.constrained.p, S.loaded.p, S.ballistic.p);
+  P.begin(PH_BALLISTIC, st);
+  if (nc > 0) k_constrained<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, S.constrained.p); RP_COUNT_LAUNCH(1);
+  if (nb > 0) k_ballistic_init<<<nblk(nb), T, 0, st>>>(nb, S.constrained.p, S.loaded.p, S.ballistic.p); RP_COUNT_LAUNCH(1);
   Sched SM{S.ord_main.p, S.lvl_off.p, S.lvl_start.p, S.nlev.p};
   if (ctx.nisl > 0)
     k_ballistic<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SM, R, B, S.c_pt.p, S.c_n.p, W.last_lin.p, ctx.dt,
-                                                          S.ballistic.p);
+                                                          S.ballistic.p); RP_COUNT_LAUNCH(1);
+  P.end(PH_BALLISTIC, st);
+  P.begin(PH_INTEGRATE, st);
   if (nb > 0)
     k_integrate<<<nblk(nb, 128), 128, 0, st>>>(nb, B, S.ballistic.p, W.last_lin.p, ctx.dt, S.orig_pos.p, S.orig_rot.p,
-                                               S.pred_pos.p, S.pred_rot.p);
+                                               S.pred_pos.p, S.pred_rot.p); RP_COUNT_LAUNCH(1);
+  P.end(PH_INTEGRATE, st);
   // ---- stage 5: position pass (step.rs:284-309); its contacts are the scheduled rows
   if (ctx.nisl > 0) {
+    P.begin(PH_POS_ITER, st);
     S.pc_lb.ensure(nc + 1);
-    k_pos_anchors<<<nblk(nc), T, 0, st>>>(nc, R, S.c_pt.p, S.orig_pos.p, S.orig_rot.p, S.pc_lb.p);
+    k_pos_anchors<<<nblk(nc), T, 0, st>>>(nc, R, S.c_pt.p, S.orig_pos.p, S.orig_rot.p, S.pc_lb.p); RP_COUNT_LAUNCH(1);
     k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SM, R, B, (int)W.iters_p_, 0, ctx.up, S.c_pt.p,
-                                                               S.c_n.p, S.pc_lb.p, S.split_l.p, S.split_a.p);
+                                                               S.c_n.p, S.pc_lb.p, S.split_l.p, S.split_a.p); RP_COUNT_LAUNCH(1);
+    P.end(PH_POS_ITER, st);
+    P.begin(PH_POS_SHOCK, st);
     // shock projection in (height key, index) order at the poses the iterations left
     uint32_t nsched = ctx.nsched;
-    k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p);
+    k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p); RP_COUNT_LAUNCH(1);
     sort_pairs_u64(S, S.key64.p, S.key64b.p, S.rows_sched.p, S.tmp32.p, nsched, 0, 64, st);
-    k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p);
+    k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p); RP_COUNT_LAUNCH(1);
     sort_pairs_u32(S, S.tmp32b.p, S.woff.p, S.tmp32.p, S.rows_sched2.p, nsched, 0, 32, st);
     build_schedule(S, nsched, ctx.nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_ps.p, S.lvl_off_ps,
                    S.lvl_start_ps, S.nlev_ps, nullptr, nullptr, st);
     Sched SP{S.ord_ps.p, S.lvl_off_ps.p, S.lvl_start_ps.p, S.nlev_ps.p};
     k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SP, R, B, 1, 1, ctx.up, S.c_pt.p, S.c_n.p,
-                                                               S.pc_lb.p, S.split_l.p, S.split_a.p);
+                                                               S.pc_lb.p, S.split_l.p, S.split_a.p); RP_COUNT_LAUNCH(1);
+    P.end(PH_POS_SHOCK, st);
   }
   // ---- stages 6 and 7
-  if (nc > 0) k_touching<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, S.c_pt.p, W.col_body.p, S.touching.p);
+  P.begin(PH_STAGE6, st);
+  if (nc > 0) k_touching<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, S.c_pt.p, W.col_body.p, S.touching.p); RP_COUNT_LAUNCH(1);
   if (nb > 0)
     k_stage6<<<nblk(nb), T, 0, st>>>(nb, B, S.orig_pos.p, S.pred_pos.p, S.pred_rot.p, S.split_l.p, S.split_a.p,
                                      S.touching.p, ctx.dt, W.last_lin.p, W.awake.p, W.sleep_ticks.p, W.sleep_allowed.p,
-                                     stats);
+                                     stats); RP_COUNT_LAUNCH(1);
   uint32_t ncap = W.capacity() > nb ? W.capacity() : nb;
-  k_count_sleeping<<<nblk(ncap), T, 0, st>>>(ncap, W.awake.p, stats);
+  k_count_sleeping<<<nblk(ncap), T, 0, st>>>(ncap, W.awake.p, stats); RP_COUNT_LAUNCH(1);
+  P.end(PH_STAGE6, st);
 }
 
 }  // namespace rp

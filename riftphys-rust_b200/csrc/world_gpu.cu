@@ -235,7 +235,7 @@ uint32_t WorldGpu::add_body(const float pose[7], const float vel[6], uint32_t sh
   body_init(pose, vel, im_in, inertia, dynamic, &P, &Q, &L, &A, &im, &ii, &d, &last);
   uint32_t id = nb_++;
   k_set_body<<<1, 1, 0, stream_>>>(id, P, Q, L, A, im, ii, d, sleep_ok ? 1 : 0, pos.p, rot.p, lin.p, ang.p, last_lin.p,
-                                   inv_mass.p, inv_I.p, dyn.p, awake.p, sleep_allowed.p, sleep_ticks.p, alive_d.p, last);
+                                   inv_mass.p, inv_I.p, dyn.p, awake.p, sleep_allowed.p, sleep_ticks.p, alive_d.p, last); RP_COUNT_LAUNCH(1);
   h_alive_.push_back(1);
   uint32_t c = ncol_++;
   h_col_body_.push_back(id); h_col_kind_.push_back(shape); h_col_mat_.push_back(mat);
@@ -298,15 +298,18 @@ void WorldGpu::filter_warm(int mode, uint32_t body) {
   const int T = 256;
   Scratch& S = *s_;
   S.wflag.ensure(n_warm + 1);
-  k_warm_filter<<<(n_warm + T - 1) / T, T, 0, stream_>>>(n_warm, warm_key.p, mode, body, alive_d.p, nb_, S.wflag.p);
+  k_warm_filter<<<(n_warm + T - 1) / T, T, 0, stream_>>>(n_warm, warm_key.p, mode, body, alive_d.p, nb_, S.wflag.p); RP_COUNT_LAUNCH(1);
   warm_key2.ensure(n_warm + 1); warm_a2.ensure(n_warm + 1); warm_b2.ensure(n_warm + 1);
   S.counts.ensure(4);
   size_t bytes = 0;
   RP_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, warm_key.p, S.wflag.p, warm_key2.p, S.counts.p, n_warm, stream_));
   S.cub_tmp.ensure(bytes + 16);
   RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, warm_key.p, S.wflag.p, warm_key2.p, S.counts.p, n_warm, stream_));
+  RP_COUNT_LAUNCH(2);
   RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, warm_a.p, S.wflag.p, warm_a2.p, S.counts.p, n_warm, stream_));
+  RP_COUNT_LAUNCH(2);
   RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, warm_b.p, S.wflag.p, warm_b2.p, S.counts.p, n_warm, stream_));
+  RP_COUNT_LAUNCH(2);
   uint32_t n = 0;
   RP_CUDA(cudaMemcpyAsync(&n, S.counts.p, 4, cudaMemcpyDeviceToHost, stream_));
   RP_CUDA(cudaStreamSynchronize(stream_));
@@ -320,7 +323,7 @@ void WorldGpu::drop_warm_of(uint32_t b) { filter_warm(0, b); }
 bool WorldGpu::remove_body(uint32_t id) {  // World::remove_body (world.rs:696-713)
   if (id >= nb_ || !h_alive_[id]) return false;
   h_alive_[id] = 0;
-  k_deactivate<<<1, 1, 0, stream_>>>(id, lin.p, ang.p, inv_mass.p, inv_I.p, dyn.p, alive_d.p);
+  k_deactivate<<<1, 1, 0, stream_>>>(id, lin.p, ang.p, inv_mass.p, inv_I.p, dyn.p, alive_d.p); RP_COUNT_LAUNCH(1);
   // colliders.retain(|c| c.body != id): later colliders shift down by one
   std::vector<uint32_t> keep;
   for (uint32_t c = 0; c < ncol_; ++c) if (h_col_body_[c] != id) keep.push_back(c);
@@ -345,16 +348,16 @@ bool WorldGpu::remove_body(uint32_t id) {  // World::remove_body (world.rs:696-7
 }
 void WorldGpu::set_body_pose(uint32_t id, const float p[7]) {  // world.rs:501-513
   drop_warm_of(id);
-  k_set_pose<<<1, 1, 0, stream_>>>(id, make_float4(p[0], p[1], p[2], 0), make_float4(p[3], p[4], p[5], p[6]), pos.p, rot.p);
+  k_set_pose<<<1, 1, 0, stream_>>>(id, make_float4(p[0], p[1], p[2], 0), make_float4(p[3], p[4], p[5], p[6]), pos.p, rot.p); RP_COUNT_LAUNCH(1);
   RP_CUDA(cudaStreamSynchronize(stream_));
 }
 void WorldGpu::set_body_vel(uint32_t id, const float v[6]) {
   k_set_vel<<<1, 1, 0, stream_>>>(id, make_float4(v[0], v[1], v[2], 0), make_float4(v[3], v[4], v[5], 0), lin.p, ang.p,
-                                  last_lin.p);
+                                  last_lin.p); RP_COUNT_LAUNCH(1);
   RP_CUDA(cudaStreamSynchronize(stream_));
 }
 void WorldGpu::apply_impulse(uint32_t id, const float j[3]) {
-  k_apply_impulse<<<1, 1, 0, stream_>>>(id, make_float4(j[0], j[1], j[2], 0), lin.p, inv_mass.p, awake.p, sleep_ticks.p);
+  k_apply_impulse<<<1, 1, 0, stream_>>>(id, make_float4(j[0], j[1], j[2], 0), lin.p, inv_mass.p, awake.p, sleep_ticks.p); RP_COUNT_LAUNCH(1);
   RP_CUDA(cudaStreamSynchronize(stream_));
 }
 void WorldGpu::get_body_pose(uint32_t id, float out[7]) {
@@ -411,8 +414,23 @@ void WorldGpu::step(float dt) {
   st_.pairs = ctx.np;
   st_.contacts = ctx.nc;
   st_.islands = ctx.nref_isl;
+  st_.rows_scheduled = ctx.nsched;
   stats_dirty_ = true;
+  if (s_->prof.on) {
+    RP_CUDA(cudaStreamSynchronize(stream_));
+    s_->prof.collect();
+  }
 }
+void WorldGpu::profile_enable(bool on) {
+  s_->prof.on = on;
+  s_->prof.reset();
+}
+int WorldGpu::profile_read(double* ms, uint64_t* calls, int cap) {
+  int n = PH_COUNT < cap ? PH_COUNT : cap;
+  for (int p = 0; p < n; ++p) { ms[p] = s_->prof.ms[p]; calls[p] = s_->prof.calls[p]; }
+  return PH_COUNT;
+}
+const char* WorldGpu::phase_name(int p) { return (p >= 0 && p < PH_COUNT) ? kPhaseNames[p] : nullptr; }
 void WorldGpu::synchronize() {
   RP_CUDA(cudaStreamSynchronize(stream_));
   RP_CUDA(cudaGetLastError());
@@ -430,6 +448,7 @@ const StepStatsHost& WorldGpu::stats() {
     st_.sleeping = h[STAT_SLEEPING];
     st_.levels = h[STAT_LEVELS];
     st_.max_batch = h[STAT_MAXBATCH];
+    st_.row_sweeps = h[STAT_ROWSWEEPS];
     stats_dirty_ = false;
   }
   st_.warm_entries = n_warm;
@@ -488,7 +507,7 @@ void WorldGpu::snapshot_restore(const SnapshotGpu* s) {  // lib.rs:1754-1793 + r
   const int T = 256;
   if (n)
     k_restore_bodies<<<(n + T - 1) / T, T, 0, stream_>>>(n, s->pos.p, s->rot.p, s->lin.p, s->ang.p, s->last_lin.p,
-                                                          alive_d.p, pos.p, rot.p, lin.p, ang.p, last_lin.p);
+                                                          alive_d.p, pos.p, rot.p, lin.p, ang.p, last_lin.p); RP_COUNT_LAUNCH(1);
   uint32_t ncap = s->cap < (cap_b_ > nb_ ? cap_b_ : nb_) ? s->cap : (cap_b_ > nb_ ? cap_b_ : nb_);
   if (ncap) {
     RP_CUDA(cudaMemcpyAsync(awake.p, s->awake.p, ncap, cudaMemcpyDeviceToDevice, stream_));

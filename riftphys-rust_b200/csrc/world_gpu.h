@@ -25,6 +25,7 @@ struct StepStatsHost {
   uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
   uint32_t sweeps = 0, bounce_skipped = 0, warm_entries = 0, sleeping = 0, error_flags = 0;
   float residual = 0.0f;
+  uint32_t row_sweeps = 0, rows_scheduled = 0;
 };
 
 struct PairPropsHost { float mu_s, mu_k, restitution, stribeck_v, stiffness; };
@@ -94,6 +95,10 @@ class WorldGpu {
   static void snapshot_free(SnapshotGpu* s);
 
   cudaStream_t stream() const { return stream_; }
+  // per-stage CUDA-event timing (totals since the last reset)
+  void profile_enable(bool on);
+  int profile_read(double* ms, uint64_t* calls, int cap);
+  static const char* phase_name(int p);
 
  private:
   void upload_pair_table();
