@@ -131,7 +131,6 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import ctypes
     lib = rp.Lib(oracle_path())
     lib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
     threads = os.cpu_count() or 1
@@ -195,8 +194,10 @@ def main():
     if args.mode == "residual":
         w.set_residual_mode(TOL, 4 * (8 if args.config == "box_drop" else 20))
     # settle into the contact regime, then warm up
+    t_settle = time.perf_counter()
     if args.settle:
         w.step_n(dt, args.settle)
+    print(f"[bench] {nb} bodies, settle {args.settle} ticks in {time.perf_counter() - t_settle:.2f}s", file=sys.stderr)
     for _ in range(args.warmup):
         w.step_n(dt, 1)
     stream = torch.cuda.ExternalStream(w.stream_handle())
@@ -248,6 +249,8 @@ def main():
         units["pairs"] += s["pairs"]
     prof = w.profile_read()
     w.profile(False)
+    for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0]):
+        print(f"[bench] stage {k:14s} {v[0] / max(1, v[1]):9.4f} ms/tick", file=sys.stderr)
     total_ms = sum(v[0] for v in prof.values())
     top = max(prof.items(), key=lambda kv: kv[1][0])
     peak, peak_kind = peak_hbm()
@@ -266,7 +269,6 @@ def main():
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu_baseline and args.config == "terrain":
-        import ctypes
         olib = rp.Lib(oracle_path())
         olib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
         threads = os.cpu_count() or 1
