@@ -107,7 +107,7 @@ class ClockSampler:
         sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
         mx = max(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if "Active" in s[2 + k]})
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[2 + k].strip() == "Active"})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons}
 
 

@@ -211,108 +211,131 @@ __device__ __forceinline__ Tri hf_tri(const HFView& hf, int gx, int gz, int whic
   return t;
 }
 
-// Terrain contacts of one collider (step.rs:121-141) culled to its bucket of at most 4
-// (cull_and_orient_contacts, step.rs:508-530): the raw points in query order (gz outer, gx inner,
-// two triangles per cell, manifold order) are streamed; with more than 4, boxes keep
-// reduce_to_4 of all points on the deepest point's normal, spheres and capsules the 4 deepest
-// by 1e-6 key, earlier first on ties. reduce_to_4's four argmax passes re-run the query.
-__global__ void k_terrain(int ncol, HFView hf, const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ ckind,
-                          const float4* __restrict__ cdims, const float4* __restrict__ pos, const float4* __restrict__ rot,
-                          const float* __restrict__ sweep, const float4* __restrict__ amin, const float4* __restrict__ amax,
-                          float4* out_pt, float4* out_n, uint32_t* out_cnt) {
+// Terrain contacts (step.rs:121-141) in three steps, so the triangle narrowphase runs one work
+// item per (collider, heightfield cell) instead of one thread per collider:
+//   k_terrain_windows  each collider's cell window (HeightField::query_aabb) and its cell count;
+//   k_terrain_items    per cell: both triangles through collide_shapes, count (EMIT=false) or
+//                      write (EMIT=true) the raw points in query order (gz outer, gx inner,
+//                      triangle 1 then 2, manifold order);
+//   k_terrain_cull     per collider: cull_and_orient_contacts' bucket rule (step.rs:508-530): up to 4
+//                      raw points kept as they are; more: boxes keep reduce_to_4 on the deepest
+//                      point's normal, spheres and capsules the 4 deepest by 1e-6 key, earlier first.
+__global__ void k_terrain_windows(int ncol, HFView hf, const float4* __restrict__ amin, const float4* __restrict__ amax,
+                                  int4* win, uint32_t* ncell) {
   int ci = blockIdx.x * blockDim.x + threadIdx.x;
   if (ci >= ncol) return;
-  uint32_t b = cbody[ci];
   int gx0, gx1, gz0, gz1;
-  out_cnt[ci] = 0;
-  if (!hf_window(hf, xyz(amin[ci]), xyz(amax[ci]), &gx0, &gx1, &gz0, &gz1)) return;
+  if (!hf_window(hf, xyz(amin[ci]), xyz(amax[ci]), &gx0, &gx1, &gz0, &gz1)) { ncell[ci] = 0; win[ci] = make_int4(0, 0, 0, 0); return; }
+  int wx = gx1 - gx0 + 1, wz = gz1 - gz0 + 1;
+  if (wx <= 0 || wz <= 0) { ncell[ci] = 0; win[ci] = make_int4(0, 0, 0, 0); return; }
+  win[ci] = make_int4(gx0, gz0, wx, wz);
+  ncell[ci] = (uint32_t)wx * (uint32_t)wz;
+}
+__device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* a, uint32_t n, uint32_t v) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) { uint32_t mid = (lo + hi) >> 1; if (a[mid] <= v) lo = mid + 1; else hi = mid; }
+  return lo;
+}
+template <bool EMIT>
+__global__ void k_terrain_items(uint32_t nitems, int ncol, HFView hf, const uint32_t* __restrict__ cell_off,
+                                const int4* __restrict__ win, const uint32_t* __restrict__ cbody,
+                                const uint32_t* __restrict__ ckind, const float4* __restrict__ cdims,
+                                const float4* __restrict__ pos, const float4* __restrict__ rot,
+                                const float* __restrict__ sweep, uint32_t* cnt, const uint32_t* __restrict__ cand_off,
+                                float4* cand_p, float4* cand_n) {
+  uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= nitems) return;
+  uint32_t ci = upper_bound_u32(cell_off, (uint32_t)ncol, it) - 1;  // cell_off: exclusive scan of cell counts
+  uint32_t q = it - cell_off[ci];
+  int4 w = win[ci];
+  int gx = w.x + (int)(q % (uint32_t)w.z);
+  int gz = w.y + (int)(q / (uint32_t)w.z);
+  uint32_t b = cbody[ci];
   float4 d = cdims[ci];
-  Shape s; s.kind = ckind[ci]; s.a = d.x; s.b = d.y; s.c = d.z;
+  Shape sh; sh.kind = ckind[ci]; sh.a = d.x; sh.b = d.y; sh.c = d.z;
   Iso x; x.pos = xyz(pos[b]); x.rot = asq(rot[b]);
   float cd = sweep[ci];
-  // pass 0: count, first 4 raw, top-4 by key (stable) for spheres/capsules, argmax depth for boxes
-  int total = 0;
-  float4 first_pt[4], first_n[4];
-  float4 top_pt[4], top_n[4]; long long top_k[4]; int ntop = 0;
-  long long best0 = LLONG_MIN; f3 p0 = mk3(0, 0, 0), nd = mk3(0, 0, 0);
-  for (int gz = gz0; gz <= gz1; ++gz)
-    for (int gx = gx0; gx <= gx1; ++gx)
-      for (int w = 0; w < 2; ++w) {
-        Tri t = hf_tri(hf, gx, gz, w);
-        Manifold m;
-        if (!collide_tri(s, x, t, cd, &m)) continue;
-        for (int k = 0; k < m.len; ++k) {
-          float depth = (m.pts[k].penetration - cd) + 0.05f;
-          float4 P = f4(m.pts[k].position, depth), N = f4(m.pts[k].normal);
-          if (total < 4) { first_pt[total] = P; first_n[total] = N; }
-          long long key = sort_key6(depth);
-          if (s.kind == SH_BOX) {
-            if (key > best0) { best0 = key; p0 = m.pts[k].position; nd = m.pts[k].normal; }
-          } else {
-            // insert into the descending top-4, after equal keys (stable)
-            int at = ntop;
-            while (at > 0 && top_k[at - 1] < key) at--;
-            if (at < 4) {
-              int last = ntop < 4 ? ntop : 3;
-              for (int q = last; q > at; --q) { top_k[q] = top_k[q - 1]; top_pt[q] = top_pt[q - 1]; top_n[q] = top_n[q - 1]; }
-              top_k[at] = key; top_pt[at] = P; top_n[at] = N;
-              if (ntop < 4) ntop++;
-            }
-          }
-          total++;
-        }
+  uint32_t n = 0, o = EMIT ? cand_off[it] : 0;
+  for (int tri = 0; tri < 2; ++tri) {
+    Tri t = hf_tri(hf, gx, gz, tri);
+    Manifold m;
+    if (!collide_tri(sh, x, t, cd, &m)) continue;
+    for (int k = 0; k < m.len; ++k) {
+      if (EMIT) {
+        cand_p[o + n] = f4(m.pts[k].position, (m.pts[k].penetration - cd) + 0.05f);
+        cand_n[o + n] = f4(m.pts[k].normal);
       }
+      n++;
+    }
+  }
+  if (!EMIT) cnt[it] = n;
+}
+__global__ void k_terrain_cull(int ncol, const uint32_t* __restrict__ ckind, const uint32_t* __restrict__ cell_off,
+                               const uint32_t* __restrict__ ncell, const uint32_t* __restrict__ cand_off, uint32_t nitems,
+                               uint32_t ncand, const float4* __restrict__ cand_p, const float4* __restrict__ cand_n,
+                               float4* out_pt, float4* out_n, uint32_t* out_cnt) {
+  int ci = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= ncol) return;
+  uint32_t i0 = cell_off[ci], i1 = i0 + ncell[ci];
+  uint32_t c0 = i0 < nitems ? cand_off[i0] : ncand, c1 = i1 < nitems ? cand_off[i1] : ncand;
+  uint32_t total = c1 - c0;
   if (total <= 4) {
-    for (int k = 0; k < total; ++k) { out_pt[4 * ci + k] = first_pt[k]; out_n[4 * ci + k] = first_n[k]; }
+    for (uint32_t k = 0; k < total; ++k) { out_pt[4 * ci + k] = cand_p[c0 + k]; out_n[4 * ci + k] = cand_n[c0 + k]; }
     out_cnt[ci] = total;
     return;
   }
-  if (s.kind != SH_BOX) {
-    for (int k = 0; k < 4; ++k) { out_pt[4 * ci + k] = top_pt[k]; out_n[4 * ci + k] = top_n[k]; }
+  if (ckind[ci] != SH_BOX) {
+    // the 4 deepest by 1e-6 key, earlier first on ties (a stable sort by Reverse(key), truncated)
+    long long tk[4]; uint32_t ti[4]; int nt = 0;
+    for (uint32_t c = c0; c < c1; ++c) {
+      long long key = sort_key6(cand_p[c].w);
+      int at = nt;
+      while (at > 0 && tk[at - 1] < key) at--;
+      if (at < 4) {
+        int last = nt < 4 ? nt : 3;
+        for (int j = last; j > at; --j) { tk[j] = tk[j - 1]; ti[j] = ti[j - 1]; }
+        tk[at] = key; ti[at] = c;
+        if (nt < 4) nt++;
+      }
+    }
+    for (int k = 0; k < 4; ++k) { out_pt[4 * ci + k] = cand_p[ti[k]]; out_n[4 * ci + k] = cand_n[ti[k]]; }
     out_cnt[ci] = 4;
     return;
   }
-  // boxes: reduce_to_4 (narrowphase.rs:312-338) over all raw points, normal = deepest point's
-  float4 selp[4], seln[4]; int nsel = 0;
-  long long bk; int bi, idx;
-  f3 p1 = mk3(0, 0, 0), e = mk3(0, 0, 0); float s2 = 0.0f;
-  for (int pass = 0; pass < 4; ++pass) {
-    bk = LLONG_MIN; bi = 0; idx = 0;
-    float bv = -INFINITY; float4 bp = make_float4(0, 0, 0, 0), bn = make_float4(0, 0, 0, 0);
-    for (int gz = gz0; gz <= gz1; ++gz)
-      for (int gx = gx0; gx <= gx1; ++gx)
-        for (int w = 0; w < 2; ++w) {
-          Tri t = hf_tri(hf, gx, gz, w);
-          Manifold m;
-          if (!collide_tri(s, x, t, cd, &m)) continue;
-          for (int k = 0; k < m.len; ++k) {
-            f3 pt = m.pts[k].position;
-            float depth = (m.pts[k].penetration - cd) + 0.05f;
-            float v;
-            if (pass == 0) v = depth;
-            else if (pass == 1) v = len2(pt - p0);
-            else if (pass == 2) v = fabsf(dot(cross(pt - p0, e), nd));
-            else v = -dot(cross(pt - p0, e), nd) * s2;
-            long long key = sort_key6(v);
-            if (key > bk) { bk = key; bi = idx; bv = v; bp = f4(pt, depth); bn = f4(m.pts[k].normal); }
-            idx++;
-          }
-        }
-    if (pass == 0) { selp[nsel] = bp; seln[nsel] = bn; nsel++; p0 = xyz(bp); continue; }
-    if (pass == 1) {
-      if (!(bv > 1.0e-12f)) break;
-      selp[nsel] = bp; seln[nsel] = bn; nsel++; p1 = xyz(bp); e = p1 - p0; continue;
+  // boxes: reduce_to_4 (narrowphase.rs:312-338) on the deepest point's normal (lowest index on ties)
+  auto argmax = [&](int pass, f3 p0, f3 e, f3 nd, float s2, uint32_t* bi, float* bv) {
+    long long bk = LLONG_MIN; *bi = c0; *bv = -INFINITY;
+    for (uint32_t c = c0; c < c1; ++c) {
+      float4 P = cand_p[c];
+      f3 pt = xyz(P);
+      float v;
+      if (pass == 0) v = P.w;
+      else if (pass == 1) v = len2(pt - p0);
+      else if (pass == 2) v = fabsf(dot(cross(pt - p0, e), nd));
+      else v = -dot(cross(pt - p0, e), nd) * s2;
+      long long key = sort_key6(v);
+      if (key > bk) { bk = key; *bi = c; *bv = v; }
     }
-    if (pass == 2) {
-      if (!(bv > 1.0e-12f)) break;
-      selp[nsel] = bp; seln[nsel] = bn; nsel++;
-      s2 = signum(dot(cross(xyz(bp) - p0, e), nd));
-      continue;
+  };
+  uint32_t sel[4]; int ns = 0;
+  uint32_t i; float v;
+  argmax(0, mk3(0, 0, 0), mk3(0, 0, 0), mk3(0, 0, 0), 0.0f, &i, &v);
+  f3 p0 = xyz(cand_p[i]), nd = xyz(cand_n[i]);
+  sel[ns++] = i;
+  argmax(1, p0, mk3(0, 0, 0), nd, 0.0f, &i, &v);
+  if (v > 1.0e-12f) {
+    sel[ns++] = i;
+    f3 e = xyz(cand_p[i]) - p0;
+    argmax(2, p0, e, nd, 0.0f, &i, &v);
+    if (v > 1.0e-12f) {
+      sel[ns++] = i;
+      float s2 = signum(dot(cross(xyz(cand_p[i]) - p0, e), nd));
+      argmax(3, p0, e, nd, s2, &i, &v);
+      if (v > 1.0e-12f) sel[ns++] = i;
     }
-    if (bv > 1.0e-12f) { selp[nsel] = bp; seln[nsel] = bn; nsel++; }
   }
-  for (int k = 0; k < nsel; ++k) { out_pt[4 * ci + k] = selp[k]; out_n[4 * ci + k] = seln[k]; }
-  out_cnt[ci] = nsel;
+  for (int k = 0; k < ns; ++k) { out_pt[4 * ci + k] = cand_p[sel[k]]; out_n[4 * ci + k] = cand_n[sel[k]]; }
+  out_cnt[ci] = ns;
 }
 
 // First pair index whose collider i is >= c, for every c in [0, ncol]: pair buckets of
@@ -448,9 +471,26 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   // terrain
   S.t_pt.ensure(4 * (size_t)ncol + 4); S.t_n.ensure(4 * (size_t)ncol + 4); S.t_cnt.ensure(ncol + 1);
   bool terrain = ctx.hf.h != nullptr;
-  if (terrain && ncol > 0)
-    k_terrain<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, ctx.hf, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p,
-                                                 W.rot.p, S.sweep.p, S.amin.p, S.amax.p, S.t_pt.p, S.t_n.p, S.t_cnt.p); RP_COUNT_LAUNCH(1);
+  if (terrain && ncol > 0) {
+    S.t_win.ensure(ncol + 1); S.t_ncell.ensure(ncol + 1); S.t_celloff.ensure(ncol + 1);
+    k_terrain_windows<<<(ncol + T - 1) / T, T, 0, st>>>(ncol, ctx.hf, S.amin.p, S.amax.p, S.t_win.p, S.t_ncell.p); RP_COUNT_LAUNCH(1);
+    uint32_t nitems = exclusive_scan_total(S, S.t_ncell.p, S.t_celloff.p, ncol, st);
+    uint32_t ncand = 0;
+    S.t_icnt.ensure(nitems + 1); S.t_ioff.ensure(nitems + 1);
+    if (nitems > 0) {
+      k_terrain_items<false><<<(nitems + 127) / 128, 128, 0, st>>>(nitems, ncol, ctx.hf, S.t_celloff.p, S.t_win.p, W.col_body.p,
+                                                                  W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, S.sweep.p,
+                                                                  S.t_icnt.p, nullptr, nullptr, nullptr); RP_COUNT_LAUNCH(1);
+      ncand = exclusive_scan_total(S, S.t_icnt.p, S.t_ioff.p, nitems, st);
+    }
+    S.t_cp.ensure(ncand + 1); S.t_cn.ensure(ncand + 1);
+    if (ncand > 0)
+      k_terrain_items<true><<<(nitems + 127) / 128, 128, 0, st>>>(nitems, ncol, ctx.hf, S.t_celloff.p, S.t_win.p, W.col_body.p,
+                                                                 W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, S.sweep.p,
+                                                                 nullptr, S.t_ioff.p, S.t_cp.p, S.t_cn.p); RP_COUNT_LAUNCH(1);
+    k_terrain_cull<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, W.col_kind.p, S.t_celloff.p, S.t_ncell.p, S.t_ioff.p, nitems,
+                                                      ncand, S.t_cp.p, S.t_cn.p, S.t_pt.p, S.t_n.p, S.t_cnt.p); RP_COUNT_LAUNCH(1);
+  }
   P.end(PH_TERRAIN, st);
   P.begin(PH_CONTACTS, st);
   // merge buckets in key order, scan, scatter

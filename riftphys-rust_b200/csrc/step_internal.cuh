@@ -20,8 +20,16 @@ namespace rp {
 
 // Kernel launches issued by this library (exact: every launch site adds its count; each
 // device-wide sort / scan / select adds the kernels it runs).
+// Counting also checks the launch: a bad configuration is reported at its own line instead of
+// surfacing later as the "last error" of an unrelated call.
 extern unsigned long long g_launches;
-#define RP_COUNT_LAUNCH(n) (::rp::g_launches += (n))
+inline void count_launch(unsigned n, const char* file, int line) {
+  g_launches += n;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e) + " at " + file + ":" + std::to_string(line));
+}
+#define RP_COUNT_LAUNCH(n) ::rp::count_launch((n), __FILE__, __LINE__)
 
 // d_stats slots
 enum : int {
@@ -110,6 +118,9 @@ struct WorldGpu::Scratch {
   DBuf<uint8_t> flag8;
   DBuf<float4> p_pt, p_n, t_pt, t_n;
   DBuf<uint32_t> p_cnt, t_cnt, pstart, bcnt, boff;
+  DBuf<int4> t_win;
+  DBuf<uint32_t> t_ncell, t_celloff, t_icnt, t_ioff;
+  DBuf<float4> t_cp, t_cn;
   // contacts
   DBuf<uint32_t> c_a, c_b;
   DBuf<float4> c_pt, c_n;  // c_pt.w = depth, c_n.w = impulse
@@ -127,6 +138,18 @@ struct WorldGpu::Scratch {
       tmp32, tmp32b;
   DBuf<unsigned long long> key64, key64b;
   DBuf<uint32_t> lvl_hist, row_level;
+  DBuf<uint32_t> lv_key, lv_key2, lv_val, lv_val2, lv_pred, lv_level, lv_np1;  // parallel level schedule
+  // solve groups (islands packed for one CTA each) and their shared-memory residents
+  DBuf<uint32_t> g_small_rows, g_small_pre, g_big, g_big_pre, g_of_isl, g_key, g_key2, g_start, g_cnt, g_class,
+      body_grp, gb_key, gb_key2, gb_list, gb_tmp, gb_start, gb_cnt, body_local;
+  // rows in schedule order (coalesced per level) for the shared-memory solve
+  DBuf<uint2> s_loc;                      // local body index of A / B (0xFFFFFFFF: cannot move)
+  DBuf<uint32_t> s_flags;
+  DBuf<float2> s_inv;
+  DBuf<float4> s_ra, s_rb, s_n, s_t1, s_t2, s_mu, s_va, s_vb, s_wa, s_wb;
+  DBuf<float> s_jn;
+  DBuf<float2> s_jt;
+  DBuf<int> s_wm;
   // position pass
   DBuf<float4> pc_la, pc_lb;
   // warm cache build

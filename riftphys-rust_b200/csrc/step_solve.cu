@@ -17,7 +17,8 @@ namespace rp {
 
 namespace {
 const int T = 256;
-inline int nblk(uint32_t n, int t = T) { return (int)((n + t - 1) / t); }
+// at least one block: every kernel returns early past its n, and a zero grid is a launch error
+inline int nblk(uint32_t n, int t = T) { return n ? (int)((n + t - 1) / t) : 1; }
 }  // namespace
 
 // row flag bits
@@ -325,37 +326,72 @@ __global__ void k_warm_unscheduled(uint32_t nc, RowsV R, BodiesV B, const int* _
 }
 
 // ------------------------------------------------------------------ schedules
-// Rows of one island in the serial order `ord_in`; greedy levels as solver.rs:625-642, one
-// thread per island walking its rows in order. body_level entries of the island's bodies are
-// reset first, so islands never interfere.
-__global__ void k_levels(uint32_t nisl, const uint32_t* __restrict__ isl_start, const uint32_t* __restrict__ isl_cnt,
-                         const uint32_t* __restrict__ ord_in, const uint2* __restrict__ ab,
-                         const uint32_t* __restrict__ flags, uint32_t* body_level, unsigned long long* key_out,
-                         uint32_t* nlev, uint32_t* row_level) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nisl) return;
-  uint32_t s0 = isl_start[i], s1 = s0 + isl_cnt[i];
-  for (uint32_t s = s0; s < s1; ++s) {
-    uint32_t r = ord_in[s];
-    uint2 x = ab[r];
-    uint32_t f = flags[r];
-    if (f & RF_WA) body_level[x.x] = 0;
-    if (f & RF_WB) body_level[x.y] = 0;
+// Greedy level schedule (solver.rs:621-642) in parallel. In the serial order `ord_in`, a row's
+// level is one more than the level of the previous row writing any of its bodies (0 if none):
+// level(s) = max over its predecessors p of level(p) + 1. Predecessors come from a stable sort of
+// (body, position) entries; the levels are then the fixed point of that recurrence on the
+// predecessor DAG, reached by monotone relaxation from 0 (after k passes every row whose longest
+// predecessor chain has length <= k is exact; an acyclic graph converges in depth + 1 passes).
+// Each row is one position s in ord_in; positions of one island are contiguous.
+__global__ void k_level_entries(uint32_t n, const uint32_t* __restrict__ ord_in, const uint2* __restrict__ ab,
+                                const uint32_t* __restrict__ flags, uint32_t* key, uint32_t* val) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t r = ord_in[s];
+  uint2 x = ab[r];
+  uint32_t f = flags[r];
+  key[2 * s] = (f & RF_WA) ? x.x : 0xFFFFFFFFu;
+  key[2 * s + 1] = (f & RF_WB) ? x.y : 0xFFFFFFFFu;
+  val[2 * s] = 2 * s;
+  val[2 * s + 1] = 2 * s + 1;
+}
+// entries sorted by body (stable): the previous entry of the same body is the predecessor
+__global__ void k_level_preds(uint32_t m, const uint32_t* __restrict__ key, const uint32_t* __restrict__ val,
+                              uint32_t* pred) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m) return;
+  uint32_t b = key[e];
+  if (b == 0xFFFFFFFFu) return;
+  pred[val[e]] = (e > 0 && key[e - 1] == b) ? (val[e - 1] >> 1) : 0xFFFFFFFFu;
+}
+// One warp per island: lanes own contiguous chunks of the island's positions and sweep them in
+// order (so chains inside a chunk settle in one pass) until a pass changes nothing.
+__global__ void k_level_relax(uint32_t nisl, const uint32_t* __restrict__ isl_start, const uint32_t* __restrict__ isl_cnt,
+                              const uint32_t* __restrict__ ord_in, const uint32_t* __restrict__ pred, uint32_t* level,
+                              unsigned long long* key_out, uint32_t* nlev, uint32_t* row_level, uint32_t* err) {
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t lane = threadIdx.x & 31;
+  if (warp >= nisl) return;
+  uint32_t s0 = isl_start[warp], n = isl_cnt[warp];
+  uint32_t chunk = (n + 31) / 32;
+  uint32_t a = s0 + lane * chunk, z = a + chunk;
+  if (z > s0 + n) z = s0 + n;
+  for (uint32_t s = a; s < z; ++s) level[s] = 0;
+  __syncwarp();
+  volatile uint32_t* vl = level;
+  uint32_t passes = 0;
+  while (true) {
+    bool changed = false;
+    for (uint32_t s = a; s < z; ++s) {
+      uint32_t p0 = pred[2 * s], p1 = pred[2 * s + 1];
+      uint32_t L = 0;
+      if (p0 != 0xFFFFFFFFu) { uint32_t v = vl[p0] + 1; if (v > L) L = v; }
+      if (p1 != 0xFFFFFFFFu) { uint32_t v = vl[p1] + 1; if (v > L) L = v; }
+      if (L != vl[s]) { vl[s] = L; changed = true; }
+    }
+    __syncwarp();
+    if (!__any_sync(0xffffffffu, changed)) break;
+    if (++passes > n + 2) { if (lane == 0) atomicOr(err, 4u); break; }  // cannot happen on a DAG
   }
-  uint32_t maxl = 0;
-  for (uint32_t s = s0; s < s1; ++s) {
-    uint32_t r = ord_in[s];
-    uint2 x = ab[r];
-    uint32_t f = flags[r];
-    uint32_t la = (f & RF_WA) ? body_level[x.x] : 0, lb = (f & RF_WB) ? body_level[x.y] : 0;
-    uint32_t t = la > lb ? la : lb;
-    if (f & RF_WA) body_level[x.x] = t + 1;
-    if (f & RF_WB) body_level[x.y] = t + 1;
-    key_out[s] = ((unsigned long long)i << 32) | t;
-    if (row_level) row_level[r] = t;
-    if (t + 1 > maxl) maxl = t + 1;
+  uint32_t mx = 0;
+  for (uint32_t s = a; s < z; ++s) {
+    uint32_t L = vl[s];
+    key_out[s] = ((unsigned long long)warp << 32) | L;
+    if (row_level) row_level[ord_in[s]] = L;
+    if (L + 1 > mx) mx = L + 1;
   }
-  nlev[i] = maxl;
+  for (int o = 16; o > 0; o >>= 1) { uint32_t t = __shfl_xor_sync(0xffffffffu, mx, o); if (t > mx) mx = t; }
+  if (lane == 0) nlev[warp] = mx;
 }
 __global__ void k_plus1(uint32_t n, const uint32_t* __restrict__ a, uint32_t* b) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -389,10 +425,10 @@ __device__ __forceinline__ float warp_max(float v) {
 // Warm start application, then the velocity sweeps (solver.rs:717-915).
 __global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* acc_jn, float2* acc_jt,
                             const int* __restrict__ wm_idx, const float4* __restrict__ wa, const float4* __restrict__ wb,
-                            int iters, float tol, uint32_t* stats) {
+                            int iters, float tol, uint32_t* stats, const uint32_t* __restrict__ g_class) {
   uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (warp >= nisl) return;
+  if (warp >= nisl || g_class[warp] != 2u) return;
   uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
   for (uint32_t L = 0; L < nl; ++L) {
     uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
@@ -782,7 +818,260 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
   if ((threadIdx.x & 31) == 0 && v) atomicAdd(&stats[STAT_SLEEPING], v);
 }
 
+// ------------------------------------------------------------------ solve groups
+// Small islands (at most GROUP_ROWS rows) are packed, in island order, into groups of about
+// GROUP_ROWS rows (by the prefix sum of their row counts); bigger islands form a group alone.
+// Islands are independent, so any interleaving of their rows is a valid serial order: a group
+// is scheduled and solved exactly like one island. One CTA solves one group with the bodies it
+// moves held in shared memory.
+#define GROUP_ROWS 256u
+#define SMALL_BODIES 640u   // shared-memory bodies of a 128-thread CTA (72 B each)
+#define BIG_BODIES 2800u    // shared-memory bodies of a 512-thread CTA
+__global__ void k_group_flags(uint32_t nisl, const uint32_t* __restrict__ isl_cnt, uint32_t* small_rows, uint32_t* big) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nisl) return;
+  bool small = isl_cnt[i] <= GROUP_ROWS;
+  small_rows[i] = small ? isl_cnt[i] : 0u;
+  big[i] = small ? 0u : 1u;
+}
+__global__ void k_group_of_isl(uint32_t nisl, const uint32_t* __restrict__ isl_cnt, const uint32_t* __restrict__ small_pre,
+                               const uint32_t* __restrict__ big_pre, uint32_t g_small, uint32_t* g_of_isl) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nisl) return;
+  g_of_isl[i] = isl_cnt[i] <= GROUP_ROWS ? small_pre[i] / GROUP_ROWS : g_small + big_pre[i];
+}
+// group key of each position of the island-sorted row order (island id = run index)
+__global__ void k_group_keys(uint32_t n, const uint32_t* __restrict__ run_flag, const uint32_t* __restrict__ run_pre,
+                             const uint32_t* __restrict__ g_of_isl, uint32_t* key) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) key[s] = g_of_isl[run_pre[s] + run_flag[s] - 1];
+}
+__global__ void k_group_ranges(uint32_t n, const uint32_t* __restrict__ key, uint32_t* start, uint32_t* cnt) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t g = key[s];
+  if (s == 0 || key[s - 1] != g) start[g] = s;
+  atomicAdd(&cnt[g], 1u);
+}
+// the group of every body a scheduled row moves (all rows of a body lie in one island)
+__global__ void k_body_groups(uint32_t n, const uint32_t* __restrict__ ord, const uint32_t* __restrict__ key,
+                              const uint2* __restrict__ ab, const uint32_t* __restrict__ flags, uint32_t* body_grp) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t r = ord[s], g = key[s], f = flags[r];
+  uint2 x = ab[r];
+  if (f & RF_WA) body_grp[x.x] = g;
+  if (f & RF_WB) body_grp[x.y] = g;
+}
+__global__ void k_flag_grouped(uint32_t nb, const uint32_t* __restrict__ body_grp, uint32_t* flag) {
+  uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nb) flag[b] = body_grp[b] != 0xFFFFFFFFu;
+}
+__global__ void k_body_local(uint32_t n, const uint32_t* __restrict__ gkey, const uint32_t* __restrict__ blist,
+                             uint32_t* gb_start, uint32_t* gb_cnt, uint32_t* body_local) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  uint32_t g = gkey[p];
+  if (p == 0 || gkey[p - 1] != g) gb_start[g] = p;
+  atomicAdd(&gb_cnt[g], 1u);
+}
+__global__ void k_body_local2(uint32_t n, const uint32_t* __restrict__ gkey, const uint32_t* __restrict__ blist,
+                              const uint32_t* __restrict__ gb_start, uint32_t* body_local) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) body_local[blist[p]] = p - gb_start[gkey[p]];
+}
+__global__ void k_group_class(uint32_t ng, const uint32_t* __restrict__ gb_cnt, uint32_t* cls) {
+  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  uint32_t nbg = gb_cnt[g];
+  cls[g] = nbg <= SMALL_BODIES ? 0u : (nbg <= BIG_BODIES ? 1u : 2u);
+}
+struct SRowsV {
+  uint2* loc; uint32_t* flags; float2* inv; float4 *ra, *rb, *n, *t1, *t2, *mu, *va, *vb; float* jn; float2* jt; int* wm;
+};
+// Rows in schedule order, with local body indices and the constant velocity of a side that
+// cannot move (a static or sleeping body's velocity at the contact; zero for terrain).
+__global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, RowsV R, BodiesV B,
+                               const uint32_t* __restrict__ body_local, const int* __restrict__ wm_idx, SRowsV O) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t r = ord[s];
+  uint2 x = R.ab[r];
+  uint32_t f = R.flags[r];
+  float4 ra = R.ra[r], rb = R.rb[r];
+  O.loc[s] = make_uint2((f & RF_WA) ? body_local[x.x] : 0xFFFFFFFFu, (f & RF_WB) ? body_local[x.y] : 0xFFFFFFFFu);
+  O.flags[s] = f;
+  O.inv[s] = R.inv[r];
+  O.ra[s] = ra; O.rb[s] = rb; O.n[s] = R.n[r]; O.t1[s] = R.t1[r]; O.t2[s] = R.t2[r]; O.mu[s] = R.mu[r];
+  f3 va = mk3(0, 0, 0), vb = mk3(0, 0, 0);
+  if (!(f & RF_WA)) va = xyz(B.lin[x.x]) + cross(xyz(B.ang[x.x]), xyz(ra));
+  if (!(f & RF_TERRAIN) && !(f & RF_WB)) vb = xyz(B.lin[x.y]) + cross(xyz(B.ang[x.y]), xyz(rb));
+  O.va[s] = f4(va);
+  O.vb[s] = f4(vb);
+  O.jn[s] = 0.0f;
+  O.jt[s] = make_float2(0.0f, 0.0f);
+  O.wm[s] = wm_idx[r];
+}
+
+// Shared-memory body state of one group
+struct SBodies { float4* lin; float4* ang; float* Iw; float* im; };
+struct SRow {
+  uint32_t la, lb, flags;
+  float inv_a, inv_b;
+  f3 ra, rb, n, t1, t2, va, vb;
+  float m_n, m_t1, m_t2, mu_s, mu_k, sv, bias;
+};
+__device__ __forceinline__ SRow ld_srow(const SRowsV& R, uint32_t s) {
+  SRow r;
+  uint2 l = R.loc[s]; r.la = l.x; r.lb = l.y; r.flags = R.flags[s];
+  float2 iv = R.inv[s]; r.inv_a = iv.x; r.inv_b = iv.y;
+  float4 a = R.ra[s], b = R.rb[s], n = R.n[s], t1 = R.t1[s], t2 = R.t2[s], mu = R.mu[s];
+  r.ra = xyz(a); r.m_n = a.w; r.rb = xyz(b); r.m_t1 = b.w; r.n = xyz(n); r.m_t2 = n.w;
+  r.t1 = xyz(t1); r.bias = t1.w; r.t2 = xyz(t2);
+  r.mu_s = mu.x; r.mu_k = mu.y; r.sv = mu.z;
+  r.va = xyz(R.va[s]); r.vb = xyz(R.vb[s]);
+  return r;
+}
+__device__ __forceinline__ f3 rel_vel_s(const SBodies& B, const SRow& r) {
+  f3 va = r.la != 0xFFFFFFFFu ? xyz(B.lin[r.la]) + cross(xyz(B.ang[r.la]), r.ra) : r.va;
+  f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : (r.lb != 0xFFFFFFFFu ? xyz(B.lin[r.lb]) + cross(xyz(B.ang[r.lb]), r.rb) : r.vb);
+  return vb - va;
+}
+__device__ __forceinline__ void body_impulse_s(const SBodies& B, uint32_t l, f3 j, f3 tau) {
+  float im = B.im[l];
+  if (im > 0.0f && vfin(j)) { float4 v = B.lin[l]; B.lin[l] = f4(fin_v(xyz(v) + j * im), v.w); }
+  if (im > 0.0f && vfin(tau)) {
+    const float* q = B.Iw + 9 * l;
+    m3 Iw = mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
+    f3 dw = mvec(Iw, tau);
+    float4 a = B.ang[l];
+    B.ang[l] = f4(fin_v(xyz(a) + dw), a.w);
+  }
+}
+__device__ __forceinline__ void contact_impulse_s(const SBodies& B, const SRow& r, f3 j) {
+  if (r.inv_a > 0.0f) { f3 nj = -j; body_impulse_s(B, r.la, nj, cross(r.ra, nj)); }
+  if (r.inv_b > 0.0f) body_impulse_s(B, r.lb, j, cross(r.rb, j));
+}
+__device__ __forceinline__ float mu_dynamic_s(const SRow& r, float slip) {
+  float t = slip / r.sv;
+  return r.mu_k + (r.mu_s - r.mu_k) * exp_rp(-(t * t));
+}
+__device__ __forceinline__ void warm_apply_s(const SBodies& B, const SRow& r, uint32_t s, float4 ea, float4 eb,
+                                             float* jn_arr, float2* jt_arr) {
+  float jn = ea.w;
+  f3 jt = xyz(eb);
+  jn_arr[s] = jn;
+  f3 imp = r.n * jn;
+  f3 v = rel_vel_s(B, r);
+  float a = dot(v, r.t1), b = dot(v, r.t2);
+  float mu = mu_dynamic_s(r, sqrtf(a * a + b * b));
+  f3 t = clamp_length_max(mk3(dot(jt, r.t1), dot(jt, r.t2), 0.0f), mu * jn);
+  jt_arr[s] = make_float2(t.x, t.y);
+  imp = imp + ((r.t1 * t.x) + (r.t2 * t.y));
+  contact_impulse_s(B, r, imp);
+}
+__device__ __forceinline__ float pgs_row_s(const SBodies& B, const SRow& r, uint32_t s, float* jn_arr, float2* jt_arr) {
+  float v_rel_n = dot(rel_vel_s(B, r), r.n);
+  float jn_raw = (r.bias - v_rel_n) * r.m_n;
+  float old_jn = jn_arr[s];
+  float new_jn = rmax(old_jn + jn_raw, 0.0f);
+  jn_arr[s] = new_jn;
+  contact_impulse_s(B, r, r.n * (new_jn - old_jn));
+  f3 vf = rel_vel_s(B, r);
+  float vt1 = dot(vf, r.t1), vt2 = dot(vf, r.t2);
+  float slip = sqrtf(vt1 * vt1 + vt2 * vt2);
+  float mu = mu_dynamic_s(r, slip);
+  float2 ot = jt_arr[s];
+  f3 old_t = mk3(ot.x, ot.y, 0.0f);
+  f3 new_t = clamp_length_max(old_t - mk3(vt1 * r.m_t1, vt2 * r.m_t2, 0.0f), mu * new_jn);
+  jt_arr[s] = make_float2(new_t.x, new_t.y);
+  f3 d = new_t - old_t;
+  contact_impulse_s(B, r, (r.t1 * d.x) + (r.t2 * d.y));
+  float res = 0.0f;
+  if (r.m_n > 0.0f) res = rmax(res, fabsf(new_jn - old_jn) / r.m_n);
+  if (r.m_t1 > 0.0f) res = rmax(res, fabsf(d.x) / r.m_t1);
+  if (r.m_t2 > 0.0f) res = rmax(res, fabsf(d.y) / r.m_t2);
+  return res;
+}
+// Warm start application and the velocity sweeps of one group (solver.rs:717-915), bodies in
+// shared memory, rows streamed from the schedule-ordered arrays; __syncthreads between levels.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t ng, uint32_t want_class, const uint32_t* __restrict__ g_class,
+                                                       const uint32_t* __restrict__ gb_start, const uint32_t* __restrict__ gb_cnt,
+                                                       const uint32_t* __restrict__ gb_list, Sched S, SRowsV R, BodiesV G,
+                                                       const float4* __restrict__ wa, const float4* __restrict__ wb,
+                                                       float* acc_jn, float2* acc_jt, int iters, float tol, uint32_t* stats) {
+  uint32_t g = blockIdx.x;
+  if (g >= ng || g_class[g] != want_class) return;
+  extern __shared__ float4 smem[];
+  uint32_t nbg = gb_cnt[g], b0 = gb_start[g];
+  SBodies B;
+  B.lin = smem;
+  B.ang = smem + nbg;
+  B.Iw = reinterpret_cast<float*>(smem + 2 * nbg);
+  B.im = B.Iw + 9 * nbg;
+  for (uint32_t i = threadIdx.x; i < nbg; i += NT) {
+    uint32_t b = gb_list[b0 + i];
+    B.lin[i] = G.lin[b];
+    B.ang[i] = G.ang[b];
+    for (int k = 0; k < 9; ++k) B.Iw[9 * i + k] = G.Iw[9 * (size_t)b + k];
+    B.im[i] = G.inv_mass[b];
+  }
+  __syncthreads();
+  uint32_t off = S.lvl_off[g], nl = S.nlev[g];
+  for (uint32_t L = 0; L < nl; ++L) {
+    uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+    for (uint32_t s = s0 + threadIdx.x; s < s1; s += NT) {
+      int e = R.wm[s];
+      if (e >= 0) { SRow r = ld_srow(R, s); warm_apply_s(B, r, s, wa[e], wb[e], R.jn, R.jt); }
+    }
+    __syncthreads();
+  }
+  __shared__ float red[NT / 32];
+  int it = 0;
+  float resid = 0.0f;
+  while (it < iters) {
+    float rr = 0.0f;
+    for (uint32_t L = 0; L < nl; ++L) {
+      uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+      for (uint32_t s = s0 + threadIdx.x; s < s1; s += NT) {
+        SRow r = ld_srow(R, s);
+        rr = rmax(rr, pgs_row_s(B, r, s, R.jn, R.jt));
+      }
+      __syncthreads();
+    }
+    it++;
+    for (int o = 16; o > 0; o >>= 1) rr = fmaxf(rr, __shfl_xor_sync(0xffffffffu, rr, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rr;
+    __syncthreads();
+    resid = 0.0f;
+    for (int w = 0; w < NT / 32; ++w) resid = fmaxf(resid, red[w]);
+    __syncthreads();
+    if (tol > 0.0f && resid <= tol) break;
+  }
+  for (uint32_t i = threadIdx.x; i < nbg; i += NT) {
+    uint32_t b = gb_list[b0 + i];
+    G.lin[b] = B.lin[i];
+    G.ang[b] = B.ang[i];
+  }
+  uint32_t s_begin = S.lvl_start[off], s_end = nl ? S.lvl_start[off + nl] : s_begin;
+  for (uint32_t s = s_begin + threadIdx.x; s < s_end; s += NT) {
+    uint32_t r = S.ord[s];
+    acc_jn[r] = R.jn[s];
+    acc_jt[r] = R.jt[s];
+  }
+  if (threadIdx.x == 0 && nl) {
+    atomicAdd(&stats[STAT_ROWSWEEPS], (s_end - s_begin) * (uint32_t)it);
+    atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
+    atomicMax(&stats[STAT_RESID], fbits(resid));
+  }
+}
+
 // ------------------------------------------------------------------ small helpers
+__global__ void k_scatter_u32(uint32_t n, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ src, uint32_t* dst) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[idx[i]] = src[i];
+}
 __global__ void k_flag_sched(uint32_t n, const uint32_t* __restrict__ root, uint8_t* fl) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) fl[k] = root[k] != 0xFFFFFFFFu;
@@ -810,19 +1099,27 @@ __global__ void k_warm_merge_kept(uint32_t n, const uint4* __restrict__ kk, cons
 }
 
 // ------------------------------------------------------------------ host driver
-static void build_schedule(WorldGpu::Scratch& S, uint32_t nsched, uint32_t nisl, const uint32_t* ord_in,
+static void build_schedule(WorldGpu::Scratch& S, uint32_t* W_err, uint32_t nsched, uint32_t nisl, const uint32_t* ord_in,
                            const uint32_t* isl_start, const uint32_t* isl_cnt, uint32_t* ord_out, DBuf<uint32_t>& lvl_off,
                            DBuf<uint32_t>& lvl_start, DBuf<uint32_t>& nlev, uint32_t* hist, uint32_t* row_level,
                            cudaStream_t st) {
   nlev.ensure(nisl + 1);
   lvl_off.ensure(nisl + 1);
   S.key64.ensure(nsched + 1); S.key64b.ensure(nsched + 1);
-  k_levels<<<nblk(nisl, 128), 128, 0, st>>>(nisl, isl_start, isl_cnt, ord_in, S.r_ab.p, S.r_flags.p, S.body_level.p,
-                                            S.key64.p, nlev.p, row_level); RP_COUNT_LAUNCH(1);
+  // predecessors, then levels (see k_level_entries)
+  S.lv_key.ensure(2 * (size_t)nsched + 2); S.lv_key2.ensure(2 * (size_t)nsched + 2);
+  S.lv_val.ensure(2 * (size_t)nsched + 2); S.lv_val2.ensure(2 * (size_t)nsched + 2);
+  S.lv_pred.ensure(2 * (size_t)nsched + 2); S.lv_level.ensure(nsched + 1);
+  k_level_entries<<<nblk(nsched), T, 0, st>>>(nsched, ord_in, S.r_ab.p, S.r_flags.p, S.lv_key.p, S.lv_val.p); RP_COUNT_LAUNCH(1);
+  sort_pairs_u32(S, S.lv_key.p, S.lv_key2.p, S.lv_val.p, S.lv_val2.p, 2 * nsched, 0, 32, st);
+  RP_CUDA(cudaMemsetAsync(S.lv_pred.p, 0xFF, sizeof(uint32_t) * 2 * (size_t)nsched, st));
+  k_level_preds<<<nblk(2 * nsched), T, 0, st>>>(2 * nsched, S.lv_key2.p, S.lv_val2.p, S.lv_pred.p); RP_COUNT_LAUNCH(1);
+  k_level_relax<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, isl_start, isl_cnt, ord_in, S.lv_pred.p, S.lv_level.p,
+                                                      S.key64.p, nlev.p, row_level, W_err); RP_COUNT_LAUNCH(1);
   sort_pairs_u64(S, S.key64.p, S.key64b.p, ord_in, ord_out, nsched, 0, 64, st);
-  S.tmp32.ensure(nisl + 1);
-  k_plus1<<<nblk(nisl), T, 0, st>>>(nisl, nlev.p, S.tmp32.p); RP_COUNT_LAUNCH(1);
-  uint32_t total = exclusive_scan_total(S, S.tmp32.p, lvl_off.p, nisl, st);
+  S.lv_np1.ensure(nisl + 1);
+  k_plus1<<<nblk(nisl), T, 0, st>>>(nisl, nlev.p, S.lv_np1.p); RP_COUNT_LAUNCH(1);
+  uint32_t total = exclusive_scan_total(S, S.lv_np1.p, lvl_off.p, nisl, st);
   lvl_start.ensure(total + 1);
   k_level_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.key64b.p, lvl_off.p, nlev.p, isl_start, isl_cnt, lvl_start.p,
                                              hist); RP_COUNT_LAUNCH(1);
@@ -896,7 +1193,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cudaStreamSynchronize(st));
     }
     ctx.nsched = nsched;
-    uint32_t nisl = 0;
+    uint32_t nisl = 0, ng = 0;
     S.isl_start.ensure(nsched + 1); S.isl_cnt.ensure(nsched + 1);
     S.ord_main.ensure(nsched + 1); S.ord_vs.ensure(nsched + 1); S.ord_ps.ensure(nsched + 1);
     if (nsched > 0) {
@@ -908,18 +1205,55 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       nisl = exclusive_scan_total(S, S.woff.p, S.wpos.p, nsched, st);
       k_island_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.woff.p, S.wpos.p, S.isl_start.p); RP_COUNT_LAUNCH(1);
       k_island_counts<<<nblk(nisl), T, 0, st>>>(nisl, nsched, S.isl_start.p, S.isl_cnt.p); RP_COUNT_LAUNCH(1);
-      ctx.nisl = nisl;
-      // ---- main schedule (row order within each island)
+      // ---- solve groups: small islands packed by the prefix sum of their rows, big ones alone
+      S.g_small_rows.ensure(nisl + 1); S.g_small_pre.ensure(nisl + 1); S.g_big.ensure(nisl + 1);
+      S.g_big_pre.ensure(nisl + 1); S.g_of_isl.ensure(nisl + 1);
+      k_group_flags<<<nblk(nisl), T, 0, st>>>(nisl, S.isl_cnt.p, S.g_small_rows.p, S.g_big.p); RP_COUNT_LAUNCH(1);
+      uint32_t small_total = exclusive_scan_total(S, S.g_small_rows.p, S.g_small_pre.p, nisl, st);
+      uint32_t nbig = exclusive_scan_total(S, S.g_big.p, S.g_big_pre.p, nisl, st);
+      uint32_t g_small = small_total ? (small_total - 1) / GROUP_ROWS + 1 : 0;
+      ng = g_small + nbig;
+      k_group_of_isl<<<nblk(nisl), T, 0, st>>>(nisl, S.isl_cnt.p, S.g_small_pre.p, S.g_big_pre.p, g_small, S.g_of_isl.p); RP_COUNT_LAUNCH(1);
+      S.g_key.ensure(nsched + 1); S.g_key2.ensure(nsched + 1);
+      k_group_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.woff.p, S.wpos.p, S.g_of_isl.p, S.g_key.p); RP_COUNT_LAUNCH(1);
+      int gbits = 1;
+      while ((1u << gbits) < ng + 1 && gbits < 32) gbits++;
+      sort_pairs_u32(S, S.g_key.p, S.g_key2.p, S.rows_sched2.p, S.tmp32.p, nsched, 0, gbits, st);  // rows by group, stable
+      S.g_start.ensure(ng + 1); S.g_cnt.ensure(ng + 1); S.g_class.ensure(ng + 1);
+      RP_CUDA(cudaMemsetAsync(S.g_start.p, 0, sizeof(uint32_t) * (ng + 1), st));
+      RP_CUDA(cudaMemsetAsync(S.g_cnt.p, 0, sizeof(uint32_t) * (ng + 1), st));
+      k_group_ranges<<<nblk(nsched), T, 0, st>>>(nsched, S.g_key2.p, S.g_start.p, S.g_cnt.p); RP_COUNT_LAUNCH(1);
+      S.row_isl2.ensure(nc + 1);
+      k_scatter_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.row_isl2.p); RP_COUNT_LAUNCH(1);  // group of each row
+      ctx.nisl = ng;
+      // ---- main schedule (row order within each group)
       S.lvl_hist.ensure(nsched + 1);
       RP_CUDA(cudaMemsetAsync(S.lvl_hist.p, 0, sizeof(uint32_t) * (nsched + 1), st));
-      build_schedule(S, nsched, nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_main.p, S.lvl_off, S.lvl_start,
+      build_schedule(S, stats + STAT_ERR, nsched, ng, S.tmp32.p, S.g_start.p, S.g_cnt.p, S.ord_main.p, S.lvl_off, S.lvl_start,
                      S.nlev, S.lvl_hist.p, S.row_level.p, st);
+      // ---- the bodies each group moves, with their index inside the group
+      S.body_grp.ensure(nb + 1); S.gb_tmp.ensure(nb + 1); S.gb_key.ensure(nb + 1); S.gb_key2.ensure(nb + 1);
+      S.gb_list.ensure(nb + 1); S.gb_start.ensure(ng + 1); S.gb_cnt.ensure(ng + 1); S.body_local.ensure(nb + 1);
+      RP_CUDA(cudaMemsetAsync(S.body_grp.p, 0xFF, sizeof(uint32_t) * (nb + 1), st));
+      k_body_groups<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.r_ab.p, S.r_flags.p, S.body_grp.p); RP_COUNT_LAUNCH(1);
+      k_flag_grouped<<<nblk(nb), T, 0, st>>>(nb, S.body_grp.p, S.gb_key.p); RP_COUNT_LAUNCH(1);
+      select_flagged_iota(S, nb, S.gb_key.p, S.gb_tmp.p, S.counts.p + 0, st);
+      uint32_t ngb = 0;
+      RP_CUDA(cudaMemcpyAsync(&ngb, S.counts.p + 0, 4, cudaMemcpyDeviceToHost, st));
+      RP_CUDA(cudaStreamSynchronize(st));
+      k_gather_u32<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_tmp.p, S.body_grp.p, S.gb_key.p); RP_COUNT_LAUNCH(1);
+      sort_pairs_u32(S, S.gb_key.p, S.gb_key2.p, S.gb_tmp.p, S.gb_list.p, ngb, 0, gbits, st);
+      RP_CUDA(cudaMemsetAsync(S.gb_start.p, 0, sizeof(uint32_t) * (ng + 1), st));
+      RP_CUDA(cudaMemsetAsync(S.gb_cnt.p, 0, sizeof(uint32_t) * (ng + 1), st));
+      k_body_local<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.gb_cnt.p, S.body_local.p); RP_COUNT_LAUNCH(1);
+      k_body_local2<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.body_local.p); RP_COUNT_LAUNCH(1);
+      k_group_class<<<nblk(ng), T, 0, st>>>(ng, S.gb_cnt.p, S.g_class.p); RP_COUNT_LAUNCH(1);
       // levels / max batch (solver.rs:684-687)
       {
         size_t bytes = 0;
-        RP_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.nlev.p, stats + STAT_LEVELS, nisl, st));
+        RP_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.nlev.p, stats + STAT_LEVELS, ng, st));
         S.cub_tmp.ensure(bytes + 16);
-        RP_CUDA(cub::DeviceReduce::Max(S.cub_tmp.p, bytes, S.nlev.p, stats + STAT_LEVELS, nisl, st));
+        RP_CUDA(cub::DeviceReduce::Max(S.cub_tmp.p, bytes, S.nlev.p, stats + STAT_LEVELS, ng, st));
         RP_COUNT_LAUNCH(2);
         bytes = 0;
         RP_CUDA(cub::DeviceReduce::Max(nullptr, bytes, S.lvl_hist.p, stats + STAT_MAXBATCH, nsched, st));
@@ -940,9 +1274,31 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     // ---- warm application + velocity sweeps
     const bool resid_mode = W.res_tol_ > 0.0f;
     int iters = (int)(resid_mode ? (W.res_max_ > 0 ? W.res_max_ : W.iters_v_) : W.iters_v_);
-    if (nisl > 0)
-      k_vel_solve<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p, W.warm_a.p,
-                                                        W.warm_b.p, iters, resid_mode ? W.res_tol_ : 0.0f, stats); RP_COUNT_LAUNCH(1);
+    if (ng > 0) {
+      // rows in schedule order, then one CTA per group (bodies in shared memory); groups moving more
+      // bodies than a CTA holds run on the warp kernel over global memory
+      S.s_loc.ensure(nsched + 1); S.s_flags.ensure(nsched + 1); S.s_inv.ensure(nsched + 1); S.s_ra.ensure(nsched + 1);
+      S.s_rb.ensure(nsched + 1); S.s_n.ensure(nsched + 1); S.s_t1.ensure(nsched + 1); S.s_t2.ensure(nsched + 1);
+      S.s_mu.ensure(nsched + 1); S.s_va.ensure(nsched + 1); S.s_vb.ensure(nsched + 1); S.s_jn.ensure(nsched + 1);
+      S.s_jt.ensure(nsched + 1); S.s_wm.ensure(nsched + 1);
+      SRowsV SR{S.s_loc.p, S.s_flags.p, S.s_inv.p, S.s_ra.p, S.s_rb.p, S.s_n.p, S.s_t1.p, S.s_t2.p, S.s_mu.p, S.s_va.p,
+                S.s_vb.p, S.s_jn.p, S.s_jt.p, S.s_wm.p};
+      k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, SR); RP_COUNT_LAUNCH(1);
+      const float tol = resid_mode ? W.res_tol_ : 0.0f;
+      k_vel_solve_smem<128><<<ng, 128, SMALL_BODIES * 72, st>>>(ng, 0u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
+                                                                SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p,
+                                                                iters, tol, stats); RP_COUNT_LAUNCH(1);
+      static bool big_attr = false;
+      if (!big_attr) {
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_smem<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, BIG_BODIES * 72));
+        big_attr = true;
+      }
+      k_vel_solve_smem<512><<<ng, 512, BIG_BODIES * 72, st>>>(ng, 1u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
+                                                              SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p,
+                                                              iters, tol, stats); RP_COUNT_LAUNCH(1);
+      k_vel_solve<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p, W.warm_a.p,
+                                                      W.warm_b.p, iters, tol, stats, S.g_class.p); RP_COUNT_LAUNCH(1);
+    }
     P.end(PH_VEL_SOLVE, st);
     P.begin(PH_WARM_CACHE, st);
     // ---- warm-start cache for the next tick (solver.rs:917-944)
@@ -995,15 +1351,15 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     P.end(PH_WARM_CACHE, st);
     P.begin(PH_VEL_SHOCK, st);
     // ---- shock propagation (solver.rs:964-993)
-    if (nisl > 0) {
+    if (ng > 0) {
       k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p); RP_COUNT_LAUNCH(1);
       sort_pairs_u64(S, S.key64.p, S.key64b.p, S.rows_sched.p, S.tmp32.p, nsched, 0, 64, st);  // by height key, stable
-      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p); RP_COUNT_LAUNCH(1);      // their roots
-      sort_pairs_u32(S, S.tmp32b.p, S.woff.p, S.tmp32.p, S.rows_sched2.p, nsched, 0, 32, st);   // by island, stable
-      build_schedule(S, nsched, nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_vs.p, S.lvl_off_vs,
+      k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl2.p, S.tmp32b.p); RP_COUNT_LAUNCH(1);     // their groups
+      sort_pairs_u32(S, S.tmp32b.p, S.woff.p, S.tmp32.p, S.rows_sched2.p, nsched, 0, 32, st);   // by group, stable
+      build_schedule(S, stats + STAT_ERR, nsched, ng, S.rows_sched2.p, S.g_start.p, S.g_cnt.p, S.ord_vs.p, S.lvl_off_vs,
                      S.lvl_start_vs, S.nlev_vs, nullptr, nullptr, st);
       Sched SV{S.ord_vs.p, S.lvl_off_vs.p, S.lvl_start_vs.p, S.nlev_vs.p};
-      k_vel_shock<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, SV, R, B, ctx.up, S.acc_jn.p); RP_COUNT_LAUNCH(1);
+      k_vel_shock<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, SV, R, B, ctx.up, S.acc_jn.p); RP_COUNT_LAUNCH(1);
     }
     P.end(PH_VEL_SHOCK, st);
     k_after_solve<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.loaded.p, S.c_n.p, stats); RP_COUNT_LAUNCH(1);
@@ -1035,9 +1391,9 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     uint32_t nsched = ctx.nsched;
     k_shock_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched.p, S.r_ab.p, S.r_flags.p, W.pos.p, ctx.up, S.key64.p); RP_COUNT_LAUNCH(1);
     sort_pairs_u64(S, S.key64.p, S.key64b.p, S.rows_sched.p, S.tmp32.p, nsched, 0, 64, st);
-    k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl.p, S.tmp32b.p); RP_COUNT_LAUNCH(1);
+    k_gather_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.row_isl2.p, S.tmp32b.p); RP_COUNT_LAUNCH(1);
     sort_pairs_u32(S, S.tmp32b.p, S.woff.p, S.tmp32.p, S.rows_sched2.p, nsched, 0, 32, st);
-    build_schedule(S, nsched, ctx.nisl, S.rows_sched2.p, S.isl_start.p, S.isl_cnt.p, S.ord_ps.p, S.lvl_off_ps,
+    build_schedule(S, stats + STAT_ERR, nsched, ctx.nisl, S.rows_sched2.p, S.g_start.p, S.g_cnt.p, S.ord_ps.p, S.lvl_off_ps,
                    S.lvl_start_ps, S.nlev_ps, nullptr, nullptr, st);
     Sched SP{S.ord_ps.p, S.lvl_off_ps.p, S.lvl_start_ps.p, S.nlev_ps.p};
     k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SP, R, B, 1, 1, ctx.up, S.c_pt.p, S.c_n.p,
