@@ -265,6 +265,11 @@ RPhysResult rphys_world_get_step_hash(const RPhysWorld* Wc, RPhysHash32* out) {
   W->w.step_hash(out->bytes);
   return RPHYS_OK;
 }
+// The CPU restatement allocates as it likes; this entry point only mirrors the CUDA library's
+// symbol so both load through the same bindings, and returns the same digest.
+RPhysResult rphys_ext_world_step_hash_noalloc(const RPhysWorld* Wc, RPhysHash32* out) {
+  return rphys_world_get_step_hash(Wc, out);
+}
 RPhysResult rphys_world_step_and_hash(RPhysWorld* W, float dt, RPhysHash32* out) {
   clear_err();
   if (!out) return fail(RPHYS_ERR_NULL, "rphys_world_step_and_hash: out_hash is null");

@@ -156,6 +156,7 @@ ABI = [
     ("rphys_ext_profile_stage_name", c_char_p, [c_uint32]),
     ("rphys_ext_stream_handle", c_uint32, [c_void_p, POINTER(c_uint64)]),
     ("rphys_ext_launch_count", c_uint32, [POINTER(c_uint64)]),
+    ("rphys_ext_world_step_hash_noalloc", c_uint32, [c_void_p, POINTER(Hash32)]),
 ]
 
 
@@ -267,6 +268,12 @@ class World:
     def hash(self):
         h = Hash32()
         self.c("rphys_world_get_step_hash", byref(h))
+        return bytes(h.bytes)
+
+    def hash_noalloc(self):
+        """The tick hash through the allocation-free entry point (same digest as hash())."""
+        h = Hash32()
+        self.c("rphys_ext_world_step_hash_noalloc", byref(h))
         return bytes(h.bytes)
 
     def pose(self, bid):

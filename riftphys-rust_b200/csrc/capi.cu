@@ -6,6 +6,7 @@
 // step_ex synchronises before returning, so every getter sees the finished tick.
 #include <cmath>
 #include <cstring>
+#include <stdexcept>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -311,6 +312,22 @@ RPhysResult rphys_world_get_step_hash(const RPhysWorld* Wc, RPhysHash32* out) {
   return guard("rphys_world_get_step_hash", [&]() {
     LOCK;
     W->w->step_hash(out->bytes);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_world_step_hash_noalloc(const RPhysWorld* Wc, RPhysHash32* out) {
+  clear_err();
+  if (!out) return fail(RPHYS_ERR_NULL, "rphys_ext_world_step_hash_noalloc: out_hash is null");
+  std::memset(out, 0, sizeof(*out));
+  if (!Wc) return fail(RPHYS_ERR_NULL, "rphys_ext_world_step_hash_noalloc: world is null");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_world_step_hash_noalloc", [&]() {
+    LOCK;
+    try {
+      W->w->step_hash_noalloc(out->bytes);
+    } catch (const std::length_error& e) {
+      return fail(RPHYS_ERR_CAPACITY, std::string("rphys_ext_world_step_hash_noalloc: ") + e.what());
+    }
     return (RPhysResult)RPHYS_OK;
   });
 }

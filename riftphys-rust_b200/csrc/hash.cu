@@ -11,6 +11,10 @@
 //   warm patches u64 0 | warm joints u64 0 | rotors u64 0 |
 //   last_lin_vel count u64 + xyz each | awake count u64 + u8 each | sleep ticks count u64 + u16 each.
 #include <cstring>
+#include <mutex>
+#include <stdexcept>
+
+#include <cub/device/device_scan.cuh>
 
 #include "step_internal.cuh"
 
@@ -210,6 +214,118 @@ void WorldGpu::step_hash(uint8_t out32[32]) {
   uint32_t* a = S.hcv.p + 8;
   uint32_t* b = S.hcv.p + 8 + 8 * (size_t)nch;
   k_b3_chunks<<<(nch + 127) / 128, 128, 0, st>>>(S.hbuf.p, len, nch, a, root); RP_COUNT_LAUNCH(1);
+  uint32_t n = nch;
+  while (n > 1) {
+    uint32_t n_out = (n + 1) / 2;
+    k_b3_parents<<<(n_out + 127) / 128, 128, 0, st>>>(n, a, b, root); RP_COUNT_LAUNCH(1);
+    std::swap(a, b);
+    n = n_out;
+  }
+  uint32_t r[8];
+  RP_CUDA(cudaMemcpyAsync(r, root, 32, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < 8; ++i)
+    for (int k = 0; k < 4; ++k) out32[4 * i + k] = (uint8_t)(r[i] >> (8 * k));
+}
+
+// ------------------------------------------------------------------ allocation-free variant
+// step_hash_noalloc writes the same stream and runs the same kernels as step_hash, but every
+// scratch byte lives in g_noalloc_scratch, a fixed array in device memory reserved when the library
+// is loaded: no cudaMalloc / cudaFree and no allocating library routine on any call. Layout:
+//   [stream: NOALLOC_STREAM_MAX + 1088 B][chaining values: 16 * (NOALLOC_STREAM_MAX / 1024 + 1) + 16
+//   words][warm key starts: NOALLOC_WARM_MAX + 1 words][warm key ranks: same][scan temp: 64 KiB].
+// Only the stream must start at zero; each call clears the part it uses. The array is one per
+// device and shared by every world on it: two calls in flight at once would overwrite each other's
+// bytes, so calls are serialised by g_noalloc_mu and each returns after its work on the device ended.
+#define NOALLOC_STREAM_MAX (12u << 20)   // bytes of serialised state (about 150k bodies, few warm entries)
+#define NOALLOC_WARM_MAX (256u << 10)    // warm-start entries
+#define NOALLOC_CHUNKS (NOALLOC_STREAM_MAX / 1024u + 1u)
+#define NOALLOC_OFF_CV ((size_t)NOALLOC_STREAM_MAX + 1088u)
+#define NOALLOC_OFF_WOFF (NOALLOC_OFF_CV + 4u * (16u * (size_t)NOALLOC_CHUNKS + 16u))
+#define NOALLOC_OFF_WPOS (NOALLOC_OFF_WOFF + 4u * ((size_t)NOALLOC_WARM_MAX + 1u))
+#define NOALLOC_OFF_TEMP ((NOALLOC_OFF_WPOS + 4u * ((size_t)NOALLOC_WARM_MAX + 1u) + 255u) & ~(size_t)255u)
+#define NOALLOC_TEMP_BYTES (64u << 10)
+#define NOALLOC_BYTES (NOALLOC_OFF_TEMP + NOALLOC_TEMP_BYTES)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_ptr[64];  // per device ordinal, set by the first call on that device
+
+// The device address of g_noalloc_scratch on the current device, looked up on the first call there.
+static unsigned char* noalloc_scratch() {
+  int dev = 0;
+  RP_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw std::runtime_error("step_hash_noalloc: device ordinal above 63");
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    RP_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  unsigned char* base = noalloc_scratch();
+  cudaStream_t st = stream_;
+  const int T = 256;
+  uint32_t cap = cap_b_ > nb_ ? cap_b_ : nb_;
+  if (n_warm > NOALLOC_WARM_MAX)
+    throw std::length_error("step_hash_noalloc: " + std::to_string(n_warm) + " warm-start entries, at most " +
+                            std::to_string(NOALLOC_WARM_MAX));
+  uint32_t* woff = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WOFF);
+  uint32_t* wpos = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WPOS);
+  void* temp = base + NOALLOC_OFF_TEMP;
+  // the stream length bound holds with every warm entry under its own key (the most bytes)
+  uint64_t worst = 48 + 56ull * nb_ + 8 + 48ull * n_warm + 24 + 8 + 12ull * nb_ + 8 + cap + 8 + 2ull * cap;
+  if (worst > NOALLOC_STREAM_MAX)
+    throw std::length_error("step_hash_noalloc: state stream of up to " + std::to_string(worst) + " bytes (" +
+                            std::to_string(nb_) + " bodies, capacity " + std::to_string(cap) + ", " +
+                            std::to_string(n_warm) + " warm entries), at most " + std::to_string(NOALLOC_STREAM_MAX));
+  uint32_t nkeys = 0;
+  if (n_warm) {
+    size_t bytes = 0;
+    RP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, woff, wpos, (int)n_warm, st));
+    if (bytes > NOALLOC_TEMP_BYTES) throw std::length_error("step_hash_noalloc: scan needs more temporary bytes than reserved");
+    k_h_warm_flags<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, woff); RP_COUNT_LAUNCH(1);
+    RP_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, woff, wpos, (int)n_warm, st));
+    RP_COUNT_LAUNCH(2);
+    uint32_t a = 0, b = 0;
+    RP_CUDA(cudaMemcpyAsync(&a, wpos + n_warm - 1, 4, cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaMemcpyAsync(&b, woff + n_warm - 1, 4, cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaStreamSynchronize(st));
+    nkeys = a + b;
+  }
+  uint64_t off_bodies = 48;
+  uint64_t off_warm = off_bodies + 56ull * nb_;
+  uint64_t off_tail = off_warm + 8 + 20ull * nkeys + 28ull * n_warm + 24;
+  uint64_t len = off_tail + 8 + 12ull * nb_ + 8 + cap + 8 + 2ull * cap;
+  uint32_t nch = (uint32_t)((len + 1023) / 1024);
+  uint8_t* hbuf = base;
+  RP_CUDA(cudaMemsetAsync(hbuf, 0, (size_t)nch * 1024 + 64, st));
+  uint8_t head[48];
+  auto p64 = [&](uint8_t* p, uint64_t v) { for (int i = 0; i < 8; ++i) p[i] = (uint8_t)(v >> (8 * i)); };
+  p64(head, epoch_);
+  p64(head + 8, rng_);
+  static const uint8_t kEmpty[32] = {0xaf, 0x13, 0x49, 0xb9, 0xf5, 0xf9, 0xa1, 0xa6, 0xa0, 0x40, 0x4d,
+                                     0xea, 0x36, 0xdc, 0xc9, 0x49, 0x9b, 0xcb, 0x25, 0xc9, 0xad, 0xc1,
+                                     0x12, 0xb7, 0xcc, 0x9a, 0x93, 0xca, 0xe4, 0x1f, 0x32, 0x62};
+  std::memcpy(head + 16, kEmpty, 32);
+  uint8_t wcount[8];
+  p64(wcount, nkeys);
+  RP_CUDA(cudaMemcpyAsync(hbuf, head, 48, cudaMemcpyHostToDevice, st));
+  if (nb_) k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, hbuf + off_bodies); RP_COUNT_LAUNCH(1);
+  RP_CUDA(cudaMemcpyAsync(hbuf + off_warm, wcount, 8, cudaMemcpyHostToDevice, st));
+  if (n_warm)
+    k_h_warm<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, warm_a.p, warm_b.p, woff, wpos, hbuf + off_warm + 8);
+  if (n_warm) RP_COUNT_LAUNCH(1);
+  uint32_t nt = cap > nb_ ? cap : nb_;
+  k_h_tail<<<(nt + T) / T, T, 0, st>>>(nb_, cap, last_lin.p, awake.p, sleep_ticks.p, hbuf + off_tail); RP_COUNT_LAUNCH(1);
+  uint32_t* cv = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_CV);
+  uint32_t* root = cv;
+  uint32_t* a = cv + 8;
+  uint32_t* b = cv + 8 + 8 * (size_t)nch;
+  k_b3_chunks<<<(nch + 127) / 128, 128, 0, st>>>(hbuf, len, nch, a, root); RP_COUNT_LAUNCH(1);
   uint32_t n = nch;
   while (n > 1) {
     uint32_t n_out = (n + 1) / 2;

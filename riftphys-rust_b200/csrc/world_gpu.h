@@ -81,6 +81,9 @@ class WorldGpu {
   void step(float dt);      // World::step, asynchronous on the world's stream
   void synchronize();       // waits for the stream; raises on a device error
   void step_hash(uint8_t out[32]);
+  // The same digest with every scratch byte in one fixed device array (hash.cu); allocates
+  // nothing. Throws std::length_error when the world does not fit that array.
+  void step_hash_noalloc(uint8_t out[32]);
 
   // ---- inspection
   const StepStatsHost& stats();
