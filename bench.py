@@ -11,10 +11,11 @@ stream. ``--config box_drop`` is the 1,000-box drop (8 iterations).
 
 value   whole-job body-ticks/s (bodies x K summed over ranks / max over ranks of the timed span).
 e2e     the same metric through the C ABI's rphys_world_step_ex with the tick's state read back to
-        host memory (rphys_ext_get_body_states: pos, rot, lin, ang) every tick, timed on the host.
-roofline  the stage with the most device time in a separate profiled pass (CUDA events around each
-        stage on the world's stream): its algorithmic bytes per launch / its mean duration, against
-        the measured HBM copy bandwidth in MEASURED_PEAKS.json.
+        host memory (rphys_ext_get_body_states: pos, rot, lin, ang) every tick, timed on the host,
+        over the same K ticks (replayed from a snapshot taken before the timed region).
+roofline  the stage with the most device time in a profiled replay of the same K ticks (CUDA events
+        around each stage on the world's stream): its algorithmic bytes per launch / its mean
+        duration, against the measured HBM copy bandwidth in MEASURED_PEAKS.json.
 cpu_baseline  the CPU restatement of the reference step (C++, OpenMP) on a bounded sample of the
         same workload: a 50x50 m patch at the same body density and shape mix, settled, then timed.
 
@@ -61,9 +62,11 @@ BYTES = {
 
 def build_scene(lib, config, n_bodies=None, area=None, hf_n=None):
     if config == "box_drop":
-        w = lib.world(1024, 1024)
-        dt, n = scenes.box_drop(rp, w, n_side=10)
-        return w, dt, n, "box_drop: 1,000 boxes (he 0.5 m, 1 kg) on a static 50x0.5x50 ground box, dt 1/60, 8+8 iters"
+        side = max(1, round((n_bodies or 1000) ** (1.0 / 3.0)))
+        w = lib.world(side ** 3 + 24, side ** 3 + 24)
+        dt, n = scenes.box_drop(rp, w, n_side=side)
+        return w, dt, n, (f"box_drop: {side ** 3:,} boxes (he 0.5 m, 1 kg) on a static 50x0.5x50 ground box, dt 1/60, "
+                          "8+8 iters")
     n_bodies = n_bodies or 100_000
     w = lib.world(n_bodies + 16, n_bodies + 16)
     dt, n = scenes.terrain(rp, w, n_bodies=n_bodies, hf_n=hf_n or 512, area=area or 400.0)
@@ -175,7 +178,6 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--bodies", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-ticks", type=int, default=5)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -201,6 +203,9 @@ def main():
     for _ in range(args.warmup):
         w.step_n(dt, 1)
     stream = torch.cuda.ExternalStream(w.stream_handle())
+    # the e2e and profiled passes replay exactly the timed ticks from this snapshot (the restore is
+    # bit-exact, so all three passes see the same contacts, islands and sweeps)
+    snap = w.snapshot()
     launches0 = lib.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
@@ -227,7 +232,9 @@ def main():
     # e2e: the drop-in C-ABI call with the tick's state read back to host memory every tick
     import numpy as np
     host = np.empty((nb, 13), dtype=np.float32)
-    e2e_ticks = max(3, min(args.steps, 20))
+    e2e_ticks = args.steps
+    w.restore(snap)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_ticks):
         w.step(dt)
@@ -237,9 +244,10 @@ def main():
            "d2h_bytes_per_step": 64 * nb}
 
     # roofline: the stage with the most device time, in a separate profiled pass
+    w.restore(snap)
     w.profile(True)
     units = {"bodies": 0, "colliders": 0, "row_sweeps": 0, "pos_row_sweeps": 0, "pairs": 0}
-    for _ in range(args.profile_ticks):
+    for _ in range(args.steps):
         w.step_n(dt, 1)
         s = w.stats()
         units["bodies"] += nb
@@ -251,8 +259,9 @@ def main():
     w.profile(False)
     for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0]):
         print(f"[bench] stage {k:14s} {v[0] / max(1, v[1]):9.4f} ms/tick", file=sys.stderr)
-    total_ms = sum(v[0] for v in prof.values())
-    top = max(prof.items(), key=lambda kv: kv[1][0])
+    outer = {k: v for k, v in prof.items() if "." not in k}  # "a.b" phases are nested inside "a"
+    total_ms = sum(v[0] for v in outer.values())
+    top = max(outer.items(), key=lambda kv: kv[1][0])
     peak, peak_kind = peak_hbm()
     stage, (stage_ms, stage_calls) = top
     roof = {"kernel": stage, "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_source": peak_kind,
@@ -283,10 +292,17 @@ def main():
                            "parallelism": f"replicas{world_size}", "l2": "inputs larger than L2" if nb > 50000 else
                            "working set within L2", "sweeps_last_tick": st["sweeps"],
                            "residual_last_tick": st["residual"], "rows_last_tick": st["rows_scheduled"],
-                           "contacts_last_tick": st["contacts"], "islands_last_tick": st["islands"]},
+                           "contacts_last_tick": st["contacts"], "islands_last_tick": st["islands"],
+                           "levels_last_tick": st["levels"], "islands_capped_last_tick": st["islands_capped"],
+                           "row_sweeps_last_tick": st["row_sweeps"],
+                           "solve_groups_last_tick": {"shared_memory": st["groups_shared"],
+                                                      "global_memory": st["groups_global"],
+                                                      "max_rows": st["max_group_rows"],
+                                                      "max_bodies": st["max_group_bodies"]}},
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "stage_ms": stages}
         print(json.dumps(line), flush=True)
+    w.free_snapshot(snap)
     w.close()
     if world_size > 1:
         dist.destroy_process_group()

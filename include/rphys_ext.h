@@ -82,6 +82,11 @@ typedef struct RPhysStepStats {
     float residual;          /* residual of the last velocity sweep (m/s) */
     uint32_t row_sweeps;     /* velocity row updates run in the last tick (rows x sweeps) */
     uint32_t rows_scheduled; /* contact rows with a movable body in the last tick */
+    /* how the last tick's velocity solve was split (0 from the CPU restatement): solve groups whose
+     * rows and bodies fit in on-chip shared memory, groups solved over global memory, and the
+     * largest group */
+    uint32_t groups_shared, groups_global, max_group_rows, max_group_bodies;
+    uint32_t islands_capped; /* residual mode: solve islands still above the tolerance at the sweep cap */
 } RPhysStepStats;
 RPhysResult rphys_ext_get_stats(const RPhysWorld* world, RPhysStepStats* out);
 

@@ -480,6 +480,7 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
   o->max_batch = s.max_batch; o->warm_matched = s.warm_matched; o->sweeps = s.sweeps;
   o->bounce_skipped = s.bounce_skipped; o->residual = s.residual;
   o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
+  o->islands_capped = s.islands_capped;
   uint32_t we = 0;
   for (auto& kv : W->w.warm) we += (uint32_t)kv.second.size();
   o->warm_entries = we;

@@ -1064,6 +1064,38 @@ void World::step(float dt) {
       }
     }
     // iterations (:788-915)
+    // Residual stop (an extension; the reference always runs iters_v sweeps): each solve island --
+    // the rows joined through the bodies they move -- sweeps until the largest velocity change one
+    // of its rows made in a sweep is <= res_tol, or the cap. Islands share no body, so stopping one
+    // early leaves every other island's arithmetic unchanged.
+    std::vector<uint32_t> sroot(count);
+    std::iota(sroot.begin(), sroot.end(), 0u);
+    auto sfind = [&](uint32_t x) {
+      while (sroot[x] != x) { sroot[x] = sroot[sroot[x]]; x = sroot[x]; }
+      return x;
+    };
+    for (auto& b : batches)
+      for (uint32_t k : b) {
+        const CC& cs = cons[k];
+        if (cs.inv_a > 0.0f && !cs.terrain && cs.inv_b > 0.0f) {
+          uint32_t ra = sfind(cs.ai), rb = sfind(cs.bi);
+          if (ra != rb) sroot[ra < rb ? rb : ra] = ra < rb ? ra : rb;
+        }
+      }
+    std::vector<uint32_t> row_isl(nc, 0xFFFFFFFFu), isl_of_root(count, 0xFFFFFFFFu);
+    uint32_t n_sisl = 0;
+    for (auto& b : batches)
+      for (uint32_t k : b) {
+        const CC& cs = cons[k];
+        uint32_t r = sfind(cs.inv_a > 0.0f ? cs.ai : cs.bi);
+        if (isl_of_root[r] == 0xFFFFFFFFu) isl_of_root[r] = n_sisl++;
+        row_isl[k] = isl_of_root[r];
+      }
+    std::vector<float> row_res(nc, 0.0f), isl_res(n_sisl), isl_last(n_sisl, 0.0f);
+    std::vector<uint32_t> isl_sweeps(n_sisl, 0), isl_rows(n_sisl, 0);
+    std::vector<uint8_t> isl_done(n_sisl, 0);
+    for (auto& b : batches)
+      for (uint32_t k : b) isl_rows[row_isl[k]]++;
     auto row = [&](uint32_t k, float* resid) {
       const CC& cs = cons[k];
       float v_rel_n = dot(contact_rel_vel(*this, cs), cs.n);
@@ -1090,32 +1122,48 @@ void World::step(float dt) {
     };
     const bool residual_mode = res_tol > 0.0f;
     const uint32_t max_sweeps = residual_mode ? (res_max > 0 ? res_max : iters_v) : iters_v;
-    uint32_t sweeps = 0;
-    float resid = 0.0f;
-    for (uint32_t it = 0; it < max_sweeps; ++it) {
-      resid = 0.0f;
+    uint32_t active = n_sisl;
+    for (uint32_t it = 0; it < max_sweeps && active > 0; ++it) {
       for (auto& b : batches) {
 #ifdef _OPENMP
         if (threads > 1 && b.size() >= 64) {
-          float rr = 0.0f;
-#pragma omp parallel for reduction(max : rr) num_threads(threads)
-          for (long q = 0; q < (long)b.size(); ++q) row(b[q], &rr);
-          resid = rmax(resid, rr);
+#pragma omp parallel for num_threads(threads)
+          for (long q = 0; q < (long)b.size(); ++q) {
+            uint32_t k = b[q];
+            if (isl_done[row_isl[k]]) continue;
+            row_res[k] = 0.0f;
+            row(k, &row_res[k]);
+          }
         } else
 #endif
-          for (uint32_t k : b) row(k, &resid);
+          for (uint32_t k : b) {
+            if (isl_done[row_isl[k]]) continue;
+            row_res[k] = 0.0f;
+            row(k, &row_res[k]);
+          }
       }
-      sweeps++;
-      if (residual_mode && resid <= res_tol) break;
+      std::fill(isl_res.begin(), isl_res.end(), 0.0f);
+      for (auto& b : batches)
+        for (uint32_t k : b)
+          if (!isl_done[row_isl[k]]) isl_res[row_isl[k]] = rmax(isl_res[row_isl[k]], row_res[k]);
+      for (uint32_t i = 0; i < n_sisl; ++i) {
+        if (isl_done[i]) continue;
+        isl_sweeps[i] = it + 1;
+        isl_last[i] = isl_res[i];
+        if (residual_mode && isl_res[i] <= res_tol) { isl_done[i] = 1; active--; }
+      }
     }
-    stats.sweeps = sweeps;
-    {
-      uint32_t ns = 0;
-      for (auto& b : batches) ns += (uint32_t)b.size();
-      stats.rows_scheduled = ns;
-      stats.row_sweeps = ns * sweeps;
+    stats.sweeps = 0;
+    stats.residual = 0.0f;
+    stats.rows_scheduled = 0;
+    stats.row_sweeps = 0;
+    for (uint32_t i = 0; i < n_sisl; ++i) {
+      stats.sweeps = std::max(stats.sweeps, isl_sweeps[i]);
+      stats.residual = rmax(stats.residual, isl_last[i]);
+      stats.rows_scheduled += isl_rows[i];
+      stats.row_sweeps += isl_rows[i] * isl_sweeps[i];
+      if (residual_mode && !isl_done[i]) stats.islands_capped++;
     }
-    stats.residual = resid;
     // warm-start cache (:917-944)
     std::map<WarmKey, std::vector<WarmContact>> nw;
     for (uint32_t k = 0; k < nc; ++k) {

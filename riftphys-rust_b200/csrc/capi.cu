@@ -563,6 +563,9 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
     o->bounce_skipped = s.bounce_skipped; o->warm_entries = s.warm_entries; o->sleeping = s.sleeping;
     o->error_flags = s.error_flags; o->residual = s.residual;
     o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
+    o->groups_shared = s.groups_shared; o->groups_global = s.groups_global;
+    o->max_group_rows = s.max_group_rows; o->max_group_bodies = s.max_group_bodies;
+    o->islands_capped = s.islands_capped;
     return (RPhysResult)RPHYS_OK;
   });
 }

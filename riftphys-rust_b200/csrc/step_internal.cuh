@@ -43,6 +43,11 @@ enum : int {
   STAT_MAXBATCH = 7,
   STAT_NISL = 8,
   STAT_ROWSWEEPS = 9,    // velocity row updates this tick (rows x sweeps, summed over islands)
+  STAT_GROUPS_SHARED = 10,
+  STAT_GROUPS_GLOBAL = 11,
+  STAT_MAX_GROUP_ROWS = 12,
+  STAT_MAX_GROUP_BODIES = 13,
+  STAT_ISLANDS_CAPPED = 14,
   STAT_COUNT = 16
 };
 
@@ -52,11 +57,14 @@ enum : int {
 enum Phase : int {
   PH_FORCES = 0, PH_AABB, PH_BROAD, PH_NARROW, PH_TERRAIN, PH_CONTACTS, PH_ISLANDS, PH_ROWS, PH_SCHED,
   PH_WARM_MATCH, PH_VEL_SOLVE, PH_WARM_CACHE, PH_VEL_SHOCK, PH_BALLISTIC, PH_INTEGRATE, PH_POS_ITER,
-  PH_POS_SHOCK, PH_STAGE6, PH_COUNT
+  PH_POS_SHOCK, PH_STAGE6,
+  // parts of vel_solve (nested inside it; named "vel_solve.*")
+  PH_VEL_PACKED, PH_VEL_ISLAND, PH_VEL_ISLAND_L, PH_VEL_BIG, PH_COUNT
 };
 static const char* const kPhaseNames[PH_COUNT] = {
     "forces", "aabb_sweep", "broadphase", "narrow_pairs", "terrain", "contacts", "islands", "rows", "schedule",
-    "warm_match", "vel_solve", "warm_cache", "vel_shock", "ballistic", "integrate", "pos_iter", "pos_shock", "stage6"};
+    "warm_match", "vel_solve", "warm_cache", "vel_shock", "ballistic", "integrate", "pos_iter", "pos_shock", "stage6",
+    "vel_solve.packed", "vel_solve.island", "vel_solve.island_l", "vel_solve.big"};
 
 struct Profiler {
   bool on = false;
@@ -139,6 +147,7 @@ struct WorldGpu::Scratch {
   DBuf<unsigned long long> key64, key64b;
   DBuf<uint32_t> lvl_hist, row_level;
   DBuf<uint32_t> lv_key, lv_key2, lv_val, lv_val2, lv_pred, lv_level, lv_np1;  // parallel level schedule
+  DBuf<uint32_t> row_islid, row_lisl, li_flag, li_pre, g_nisl;                 // islands inside solve groups
   // solve groups (islands packed for one CTA each) and their shared-memory residents
   DBuf<uint32_t> g_small_rows, g_small_pre, g_big, g_big_pre, g_of_isl, g_key, g_key2, g_start, g_cnt, g_class,
       body_grp, gb_key, gb_key2, gb_list, gb_tmp, gb_start, gb_cnt, body_local;

@@ -9,6 +9,7 @@
 // (solver.rs:964-993, step.rs:450-456) sort rows by height first and get their own schedule.
 // Rows split into islands (connected through awake dynamic bodies); one warp owns an island and
 // walks its levels with __syncwarp between them, so no two warps ever touch the same body.
+#include <atomic>
 #include <cub/cub.cuh>
 
 #include "step_internal.cuh"
@@ -425,8 +426,8 @@ __device__ __forceinline__ float warp_max(float v) {
 // Warm start application, then the velocity sweeps (solver.rs:717-915).
 __global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* acc_jn, float2* acc_jt,
                             const int* __restrict__ wm_idx, const float4* __restrict__ wa, const float4* __restrict__ wb,
-                            int iters, float tol, uint32_t* stats, const uint32_t* __restrict__ g_class) {
-  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                            int iters, float tol, uint32_t* stats, const uint32_t* __restrict__ g_class, uint32_t g0) {
+  uint32_t warp = g0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   int lane = threadIdx.x & 31;
   if (warp >= nisl || g_class[warp] != 2u) return;
   uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
@@ -460,6 +461,7 @@ __global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* a
     atomicAdd(&stats[STAT_ROWSWEEPS], (S.lvl_start[off + nl] - S.lvl_start[off]) * (uint32_t)it);
     atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
     atomicMax(&stats[STAT_RESID], fbits(resid));
+    if (tol > 0.0f && !(resid <= tol)) atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
   }
 }
 // Shock propagation (solver.rs:964-993): rows in (1e-6 height key, index) order, the lower body
@@ -820,13 +822,22 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
 
 // ------------------------------------------------------------------ solve groups
 // Small islands (at most GROUP_ROWS rows) are packed, in island order, into groups of about
-// GROUP_ROWS rows (by the prefix sum of their row counts); bigger islands form a group alone.
+// GROUP_ROWS rows (by the prefix sum of their row counts, so a group holds at most
+// 2 * GROUP_ROWS - 1 rows and twice that many bodies); bigger islands form a group alone.
 // Islands are independent, so any interleaving of their rows is a valid serial order: a group
-// is scheduled and solved exactly like one island. One CTA solves one group with the bodies it
-// moves held in shared memory.
-#define GROUP_ROWS 256u
+// is scheduled and solved exactly like one island. Classes: 3, a packed group, and 4 / 5, an
+// island whose rows and bodies fit in one block's shared memory, are solved by one warp with all
+// of it on chip; 0 / 1, a bigger island, by one CTA with its bodies in shared memory (128 / 512
+// threads); 2 by one warp over global memory.
+#define GROUP_ROWS 32u
 #define SMALL_BODIES 640u   // shared-memory bodies of a 128-thread CTA (72 B each)
 #define BIG_BODIES 2800u    // shared-memory bodies of a 512-thread CTA
+#define WG_ROWS (2u * GROUP_ROWS)  // rows a packed group can hold
+#define WG_BODIES (2u * WG_ROWS)   // bodies those rows can move
+#define WG4_ROWS 256u              // single islands solved by one warp with everything on chip
+#define WG4_BODIES 512u
+#define WG5_ROWS 1152u
+#define WG5_BODIES 768u
 __global__ void k_group_flags(uint32_t nisl, const uint32_t* __restrict__ isl_cnt, uint32_t* small_rows, uint32_t* big) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nisl) return;
@@ -880,11 +891,43 @@ __global__ void k_body_local2(uint32_t n, const uint32_t* __restrict__ gkey, con
   uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p < n) body_local[blist[p]] = p - gb_start[gkey[p]];
 }
-__global__ void k_group_class(uint32_t ng, const uint32_t* __restrict__ gb_cnt, uint32_t* cls) {
+__global__ void k_group_class(uint32_t ng, uint32_t g_small, const uint32_t* __restrict__ gb_cnt,
+                              const uint32_t* __restrict__ g_cnt, uint32_t* cls, uint32_t* stats) {
   uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ng) return;
-  uint32_t nbg = gb_cnt[g];
-  cls[g] = nbg <= SMALL_BODIES ? 0u : (nbg <= BIG_BODIES ? 1u : 2u);
+  uint32_t nbg = gb_cnt[g], nr = g_cnt[g];
+  uint32_t c = g < g_small                              ? 3u
+               : (nr <= WG4_ROWS && nbg <= WG4_BODIES)  ? 4u
+               : (nr <= WG5_ROWS && nbg <= WG5_BODIES)  ? 5u
+               : (nbg <= SMALL_BODIES ? 0u : (nbg <= BIG_BODIES ? 1u : 2u));
+  cls[g] = c;
+  atomicAdd(&stats[c == 2u ? STAT_GROUPS_GLOBAL : STAT_GROUPS_SHARED], 1u);
+  atomicMax(&stats[STAT_MAX_GROUP_ROWS], nr);
+  atomicMax(&stats[STAT_MAX_GROUP_BODIES], nbg);
+}
+// Local island index of every scheduled row inside its solve group (islands of a group in island
+// order, numbered from 0), for the per-island residual stop; and each group's island count.
+__global__ void k_row_island(uint32_t n, const uint32_t* __restrict__ rows, const uint32_t* __restrict__ run_flag,
+                             const uint32_t* __restrict__ run_pre, uint32_t* row_isl) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) row_isl[rows[s]] = run_pre[s] + run_flag[s] - 1;
+}
+__global__ void k_local_isl_flags(uint32_t n, const uint32_t* __restrict__ ord, const uint32_t* __restrict__ gkey,
+                                  const uint32_t* __restrict__ row_isl, uint32_t* flag) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  flag[p] = (p == 0 || gkey[p - 1] != gkey[p] || row_isl[ord[p - 1]] != row_isl[ord[p]]) ? 1u : 0u;
+}
+__global__ void k_local_isl(uint32_t n, const uint32_t* __restrict__ ord, const uint32_t* __restrict__ gkey,
+                            const uint32_t* __restrict__ g_start, const uint32_t* __restrict__ g_cnt,
+                            const uint32_t* __restrict__ flag, const uint32_t* __restrict__ pre, uint32_t* row_lisl,
+                            uint32_t* g_nisl) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  uint32_t g = gkey[p], s0 = g_start[g];
+  uint32_t li = (pre[p] + flag[p]) - (pre[s0] + 1u);
+  row_lisl[ord[p]] = li;
+  if (p == s0 + g_cnt[g] - 1) g_nisl[g] = li + 1;
 }
 struct SRowsV {
   uint2* loc; uint32_t* flags; float2* inv; float4 *ra, *rb, *n, *t1, *t2, *mu, *va, *vb; float* jn; float2* jt; int* wm;
@@ -892,7 +935,8 @@ struct SRowsV {
 // Rows in schedule order, with local body indices and the constant velocity of a side that
 // cannot move (a static or sleeping body's velocity at the contact; zero for terrain).
 __global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, RowsV R, BodiesV B,
-                               const uint32_t* __restrict__ body_local, const int* __restrict__ wm_idx, SRowsV O) {
+                               const uint32_t* __restrict__ body_local, const int* __restrict__ wm_idx,
+                               const uint32_t* __restrict__ row_lisl, SRowsV O) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t r = ord[s];
@@ -900,7 +944,7 @@ __global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, Row
   uint32_t f = R.flags[r];
   float4 ra = R.ra[r], rb = R.rb[r];
   O.loc[s] = make_uint2((f & RF_WA) ? body_local[x.x] : 0xFFFFFFFFu, (f & RF_WB) ? body_local[x.y] : 0xFFFFFFFFu);
-  O.flags[s] = f;
+  O.flags[s] = (f & 0xFFFFu) | (row_lisl[r] << 16);  // bits 16..31: the row's island inside its group
   O.inv[s] = R.inv[r];
   O.ra[s] = ra; O.rb[s] = rb; O.n[s] = R.n[r]; O.t1[s] = R.t1[r]; O.t2[s] = R.t2[r]; O.mu[s] = R.mu[r];
   f3 va = mk3(0, 0, 0), vb = mk3(0, 0, 0);
@@ -915,10 +959,11 @@ __global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, Row
 
 // Shared-memory body state of one group
 struct SBodies { float4* lin; float4* ang; float* Iw; float* im; };
+// vfix: the velocity at the contact of the side that cannot move (a scheduled row has at most one)
 struct SRow {
   uint32_t la, lb, flags;
   float inv_a, inv_b;
-  f3 ra, rb, n, t1, t2, va, vb;
+  f3 ra, rb, n, t1, t2, vfix;
   float m_n, m_t1, m_t2, mu_s, mu_k, sv, bias;
 };
 __device__ __forceinline__ SRow ld_srow(const SRowsV& R, uint32_t s) {
@@ -929,12 +974,12 @@ __device__ __forceinline__ SRow ld_srow(const SRowsV& R, uint32_t s) {
   r.ra = xyz(a); r.m_n = a.w; r.rb = xyz(b); r.m_t1 = b.w; r.n = xyz(n); r.m_t2 = n.w;
   r.t1 = xyz(t1); r.bias = t1.w; r.t2 = xyz(t2);
   r.mu_s = mu.x; r.mu_k = mu.y; r.sv = mu.z;
-  r.va = xyz(R.va[s]); r.vb = xyz(R.vb[s]);
+  r.vfix = l.x == 0xFFFFFFFFu ? xyz(R.va[s]) : xyz(R.vb[s]);
   return r;
 }
 __device__ __forceinline__ f3 rel_vel_s(const SBodies& B, const SRow& r) {
-  f3 va = r.la != 0xFFFFFFFFu ? xyz(B.lin[r.la]) + cross(xyz(B.ang[r.la]), r.ra) : r.va;
-  f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : (r.lb != 0xFFFFFFFFu ? xyz(B.lin[r.lb]) + cross(xyz(B.ang[r.lb]), r.rb) : r.vb);
+  f3 va = r.la != 0xFFFFFFFFu ? xyz(B.lin[r.la]) + cross(xyz(B.ang[r.la]), r.ra) : r.vfix;
+  f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : (r.lb != 0xFFFFFFFFu ? xyz(B.lin[r.lb]) + cross(xyz(B.ang[r.lb]), r.rb) : r.vfix);
   return vb - va;
 }
 __device__ __forceinline__ void body_impulse_s(const SBodies& B, uint32_t l, f3 j, f3 tau) {
@@ -993,16 +1038,94 @@ __device__ __forceinline__ float pgs_row_s(const SBodies& B, const SRow& r, uint
   if (r.m_t2 > 0.0f) res = rmax(res, fabsf(d.y) / r.m_t2);
   return res;
 }
-// Warm start application and the velocity sweeps of one group (solver.rs:717-915), bodies in
-// shared memory, rows streamed from the schedule-ordered arrays; __syncthreads between levels.
+// pgs_row_s with the two bodies' velocities held in registers across the row (loaded once,
+// written back once) and the residual's divisions left to the caller: the same operations in
+// the same order, so the same bits, with a shorter dependent chain per level. dres receives
+// new_jn - old_jn and the two friction deltas; the row's residual is
+// max(|dres.x| / m_n, |dres.y| / m_t1, |dres.z| / m_t2) over the effective masses that are > 0.
+__device__ __forceinline__ void impulse_reg(f3& lin, f3& ang, float im, const float* q, f3 j, f3 tau) {
+  if (im > 0.0f && vfin(j)) lin = fin_v(lin + j * im);
+  if (im > 0.0f && vfin(tau)) {
+    m3 Iw = mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
+    ang = fin_v(ang + mvec(Iw, tau));
+  }
+}
+__device__ __forceinline__ void pgs_row_reg(const SBodies& B, const SRow& r, uint32_t s, float* jn_arr, float2* jt_arr,
+                                            float* dres) {
+  const bool ha = r.la != 0xFFFFFFFFu, hb = !(r.flags & RF_TERRAIN) && r.lb != 0xFFFFFFFFu;
+  const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
+  float4 LA = make_float4(0, 0, 0, 0), AA = LA, LB = LA, AB = LA;
+  if (ha || ia) { LA = B.lin[r.la]; AA = B.ang[r.la]; }
+  if (hb || ib) { LB = B.lin[r.lb]; AB = B.ang[r.lb]; }
+  f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
+  const float* qa = ia ? B.Iw + 9 * (size_t)r.la : B.Iw;
+  const float* qb = ib ? B.Iw + 9 * (size_t)r.lb : B.Iw;
+  float ima = ia ? B.im[r.la] : 0.0f, imb = ib ? B.im[r.lb] : 0.0f;
+  auto rel = [&]() {
+    f3 va = ha ? la + cross(aa, r.ra) : r.vfix;
+    f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : (hb ? lb + cross(ab, r.rb) : r.vfix);
+    return vb - va;
+  };
+  auto apply = [&](f3 j) {
+    if (ia) { f3 nj = -j; impulse_reg(la, aa, ima, qa, nj, cross(r.ra, nj)); }
+    if (ib) impulse_reg(lb, ab, imb, qb, j, cross(r.rb, j));
+  };
+  float v_rel_n = dot(rel(), r.n);
+  float jn_raw = (r.bias - v_rel_n) * r.m_n;
+  float old_jn = jn_arr[s];
+  float new_jn = rmax(old_jn + jn_raw, 0.0f);
+  jn_arr[s] = new_jn;
+  apply(r.n * (new_jn - old_jn));
+  f3 vf = rel();
+  float vt1 = dot(vf, r.t1), vt2 = dot(vf, r.t2);
+  float slip = sqrtf(vt1 * vt1 + vt2 * vt2);
+  float mu = mu_dynamic_s(r, slip);
+  float2 ot = jt_arr[s];
+  f3 old_t = mk3(ot.x, ot.y, 0.0f);
+  f3 new_t = clamp_length_max(old_t - mk3(vt1 * r.m_t1, vt2 * r.m_t2, 0.0f), mu * new_jn);
+  jt_arr[s] = make_float2(new_t.x, new_t.y);
+  f3 d = new_t - old_t;
+  apply((r.t1 * d.x) + (r.t2 * d.y));
+  if (ia) { B.lin[r.la] = f4(la, LA.w); B.ang[r.la] = f4(aa, AA.w); }
+  if (ib) { B.lin[r.lb] = f4(lb, LB.w); B.ang[r.lb] = f4(ab, AB.w); }
+  dres[3 * s] = new_jn - old_jn;
+  dres[3 * s + 1] = d.x;
+  dres[3 * s + 2] = d.y;
+}
+__device__ __forceinline__ float row_residual(const SRow& r, const float* dres, uint32_t s) {
+  float res = 0.0f;
+  if (r.m_n > 0.0f) res = rmax(res, fabsf(dres[3 * s]) / r.m_n);
+  if (r.m_t1 > 0.0f) res = rmax(res, fabsf(dres[3 * s + 1]) / r.m_t1);
+  if (r.m_t2 > 0.0f) res = rmax(res, fabsf(dres[3 * s + 2]) / r.m_t2);
+  return res;
+}
+
+// Per-island residual stop, shared by the group kernels below: after each sweep an island whose
+// rows changed no velocity by more than tol is done and its rows are skipped from then on
+// (islands share no body, so the other islands' arithmetic is unchanged). Fixed-iteration mode
+// (tol = 0) never marks an island done.
+
+// Warm start application and the velocity sweeps of one big island (solver.rs:717-915), bodies
+// in shared memory, rows streamed from the schedule-ordered arrays; __syncthreads between levels.
+#define GROUP_ISL_MAX 64u  // the CTA kernel solves single islands; the bound only has to cover that
 template <int NT>
-__global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t ng, uint32_t want_class, const uint32_t* __restrict__ g_class,
+__global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t g0, uint32_t ng, uint32_t want_class,
+                                                       const uint32_t* __restrict__ g_class,
                                                        const uint32_t* __restrict__ gb_start, const uint32_t* __restrict__ gb_cnt,
-                                                       const uint32_t* __restrict__ gb_list, Sched S, SRowsV R, BodiesV G,
+                                                       const uint32_t* __restrict__ gb_list, const uint32_t* __restrict__ g_nisl,
+                                                       Sched S, SRowsV R, BodiesV G,
                                                        const float4* __restrict__ wa, const float4* __restrict__ wb,
                                                        float* acc_jn, float2* acc_jt, int iters, float tol, uint32_t* stats) {
-  uint32_t g = blockIdx.x;
+  uint32_t g = g0 + blockIdx.x;
   if (g >= ng || g_class[g] != want_class) return;
+  const uint32_t nisl = g_nisl[g];
+  if (nisl > GROUP_ISL_MAX) {  // not reached: classes 0 and 1 are single islands
+    if (threadIdx.x == 0) atomicOr(&stats[STAT_ERR], 2u);
+    return;
+  }
+  __shared__ uint32_t isl_res[GROUP_ISL_MAX], isl_last[GROUP_ISL_MAX], isl_sw[GROUP_ISL_MAX];
+  __shared__ uint8_t isl_done[GROUP_ISL_MAX];
+  __shared__ uint32_t blk_rowsweeps, blk_capped;
   extern __shared__ float4 smem[];
   uint32_t nbg = gb_cnt[g], b0 = gb_start[g];
   SBodies B;
@@ -1017,6 +1140,8 @@ __global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t ng, uint32_t wan
     for (int k = 0; k < 9; ++k) B.Iw[9 * i + k] = G.Iw[9 * (size_t)b + k];
     B.im[i] = G.inv_mass[b];
   }
+  for (uint32_t i = threadIdx.x; i < nisl; i += NT) { isl_res[i] = 0u; isl_last[i] = 0u; isl_sw[i] = 0u; isl_done[i] = 0; }
+  if (threadIdx.x == 0) { blk_rowsweeps = 0u; blk_capped = 0u; }
   __syncthreads();
   uint32_t off = S.lvl_off[g], nl = S.nlev[g];
   for (uint32_t L = 0; L < nl; ++L) {
@@ -1027,27 +1152,31 @@ __global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t ng, uint32_t wan
     }
     __syncthreads();
   }
-  __shared__ float red[NT / 32];
   int it = 0;
-  float resid = 0.0f;
   while (it < iters) {
-    float rr = 0.0f;
     for (uint32_t L = 0; L < nl; ++L) {
       uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
       for (uint32_t s = s0 + threadIdx.x; s < s1; s += NT) {
+        uint32_t li = R.flags[s] >> 16;
+        if (isl_done[li]) continue;
         SRow r = ld_srow(R, s);
-        rr = rmax(rr, pgs_row_s(B, r, s, R.jn, R.jt));
+        float rr = pgs_row_s(B, r, s, R.jn, R.jt);
+        atomicMax(&isl_res[li], fbits(rr));  // non-negative floats: integer max, order-free
       }
       __syncthreads();
     }
     it++;
-    for (int o = 16; o > 0; o >>= 1) rr = fmaxf(rr, __shfl_xor_sync(0xffffffffu, rr, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = rr;
-    __syncthreads();
-    resid = 0.0f;
-    for (int w = 0; w < NT / 32; ++w) resid = fmaxf(resid, red[w]);
-    __syncthreads();
-    if (tol > 0.0f && resid <= tol) break;
+    bool active = false;
+    for (uint32_t i = threadIdx.x; i < nisl; i += NT) {
+      if (isl_done[i]) continue;
+      uint32_t rb = isl_res[i];
+      isl_res[i] = 0u;
+      isl_sw[i] = (uint32_t)it;
+      isl_last[i] = rb;
+      if (tol > 0.0f && __uint_as_float(rb) <= tol) isl_done[i] = 1;
+      else active = true;
+    }
+    if (!__syncthreads_or(active)) break;
   }
   for (uint32_t i = threadIdx.x; i < nbg; i += NT) {
     uint32_t b = gb_list[b0 + i];
@@ -1055,15 +1184,165 @@ __global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t ng, uint32_t wan
     G.ang[b] = B.ang[i];
   }
   uint32_t s_begin = S.lvl_start[off], s_end = nl ? S.lvl_start[off + nl] : s_begin;
+  uint32_t my_rs = 0;
   for (uint32_t s = s_begin + threadIdx.x; s < s_end; s += NT) {
     uint32_t r = S.ord[s];
     acc_jn[r] = R.jn[s];
     acc_jt[r] = R.jt[s];
+    my_rs += isl_sw[R.flags[s] >> 16];
   }
-  if (threadIdx.x == 0 && nl) {
-    atomicAdd(&stats[STAT_ROWSWEEPS], (s_end - s_begin) * (uint32_t)it);
-    atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
-    atomicMax(&stats[STAT_RESID], fbits(resid));
+  uint32_t my_sw = 0, my_res = 0, my_cap = 0;
+  for (uint32_t i = threadIdx.x; i < nisl; i += NT) {
+    my_sw = max(my_sw, isl_sw[i]);
+    my_res = max(my_res, isl_last[i]);
+    if (tol > 0.0f && !isl_done[i]) my_cap++;
+  }
+  atomicAdd(&blk_rowsweeps, my_rs);
+  atomicAdd(&blk_capped, my_cap);
+  if (my_sw) atomicMax(&stats[STAT_SWEEPS], my_sw);
+  if (my_res) atomicMax(&stats[STAT_RESID], my_res);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (blk_rowsweeps) atomicAdd(&stats[STAT_ROWSWEEPS], blk_rowsweeps);
+    if (blk_capped) atomicAdd(&stats[STAT_ISLANDS_CAPPED], blk_capped);
+  }
+}
+
+// A group solved by one warp with everything it touches in its block's shared memory: rows (in
+// schedule order), impulses, bodies, level starts and per-island residual state; __syncwarp
+// between levels. One warp per block, so the block scheduler hands an SM a new group as soon as
+// any of its groups finishes. Same arithmetic and order as k_vel_solve_smem. Capacities: RC rows,
+// BC bodies, IC islands -- class 3 (packed groups) 64 / 128 / 64 in about 19.5 KB, class 4
+// (islands up to 256 rows) 256 / 512 / 1 in about 75 KB, class 5 (up to 1152 rows)
+// 1152 / 768 / 1 in about 221 KB.
+template <uint32_t RC, uint32_t BC, uint32_t IC>
+struct WarpGroupSmem {
+  float4 lin[BC];
+  float4 ang[BC];
+  float2 jt[RC];
+  SRow rows[RC];
+  float jn[RC];
+  float dres[3 * RC];
+  float Iw[9 * BC];
+  float im[BC];
+  uint32_t lvl[RC + 1];
+  uint32_t isl_res[IC], isl_last[IC], isl_sw[IC];
+  uint8_t isl_done[IC];
+};
+typedef WarpGroupSmem<WG_ROWS, WG_BODIES, WG_ROWS> WarpSmem3;
+typedef WarpGroupSmem<WG4_ROWS, WG4_BODIES, 1> WarpSmem4;
+typedef WarpGroupSmem<WG5_ROWS, WG5_BODIES, 1> WarpSmem5;
+static_assert(sizeof(WarpSmem5) <= 232448, "class-5 warp group exceeds the per-block shared memory limit");
+template <uint32_t RC, uint32_t BC, uint32_t IC>
+__global__ void __launch_bounds__(32) k_vel_solve_warp(uint32_t g0, uint32_t ng, uint32_t want_class,
+                                                       const uint32_t* __restrict__ g_class,
+                                                       const uint32_t* __restrict__ gb_start,
+                                                       const uint32_t* __restrict__ gb_cnt,
+                                                       const uint32_t* __restrict__ gb_list,
+                                                       const uint32_t* __restrict__ g_nisl, Sched S, SRowsV R,
+                                                       BodiesV G, const float4* __restrict__ wa,
+                                                       const float4* __restrict__ wb, float* acc_jn, float2* acc_jt,
+                                                       int iters, float tol, uint32_t* stats) {
+  uint32_t g = g0 + blockIdx.x;
+  if (g >= ng || g_class[g] != want_class) return;
+  extern __shared__ float4 wsm_raw[];
+  WarpGroupSmem<RC, BC, IC>& W = *reinterpret_cast<WarpGroupSmem<RC, BC, IC>*>(wsm_raw);
+  const uint32_t lane = threadIdx.x;
+  const uint32_t nbg = gb_cnt[g], b0 = gb_start[g], nisl = g_nisl[g];
+  const uint32_t off = S.lvl_off[g], nl = S.nlev[g];
+  const uint32_t base = S.lvl_start[off], nr = S.lvl_start[off + nl] - base;
+  if (nbg > BC || nr > RC || nisl > IC) {  // not reached: the class was chosen by these sizes
+    if (lane == 0) atomicOr(&stats[STAT_ERR], 2u);
+    return;
+  }
+  for (uint32_t i = lane; i < nbg; i += 32) {
+    uint32_t b = gb_list[b0 + i];
+    W.lin[i] = G.lin[b];
+    W.ang[i] = G.ang[b];
+    for (int k = 0; k < 9; ++k) W.Iw[9 * i + k] = G.Iw[9 * (size_t)b + k];
+    W.im[i] = G.inv_mass[b];
+  }
+  for (uint32_t i = lane; i < nr; i += 32) {
+    W.rows[i] = ld_srow(R, base + i);
+    W.jn[i] = 0.0f;
+    W.jt[i] = make_float2(0.0f, 0.0f);
+  }
+  for (uint32_t L = lane; L <= nl; L += 32) W.lvl[L] = S.lvl_start[off + L] - base;
+  for (uint32_t i = lane; i < nisl; i += 32) { W.isl_res[i] = 0u; W.isl_last[i] = 0u; W.isl_sw[i] = 0u; W.isl_done[i] = 0; }
+  __syncwarp();
+  SBodies B{W.lin, W.ang, W.Iw, W.im};
+  for (uint32_t L = 0; L < nl; ++L) {
+    for (uint32_t i = W.lvl[L] + lane; i < W.lvl[L + 1]; i += 32) {
+      int e = R.wm[base + i];
+      if (e >= 0) warm_apply_s(B, W.rows[i], i, wa[e], wb[e], W.jn, W.jt);
+    }
+    __syncwarp();
+  }
+  int it = 0;
+  while (it < iters) {
+    for (uint32_t L = 0; L < nl; ++L) {
+      for (uint32_t i = W.lvl[L] + lane; i < W.lvl[L + 1]; i += 32) {
+        const SRow& r = W.rows[i];
+        if (IC > 1 && W.isl_done[r.flags >> 16]) continue;
+        pgs_row_reg(B, r, i, W.jn, W.jt, W.dres);
+      }
+      __syncwarp();
+    }
+    // the sweep's residual per island, off the level chain (non-negative floats: integer max)
+    if (IC == 1) {
+      uint32_t m = 0;
+      for (uint32_t i = lane; i < nr; i += 32) m = max(m, fbits(row_residual(W.rows[i], W.dres, i)));
+      m = __reduce_max_sync(0xffffffffu, m);
+      if (lane == 0) W.isl_res[0] = m;
+    } else {
+      for (uint32_t i = lane; i < nr; i += 32) {
+        uint32_t li = W.rows[i].flags >> 16;
+        if (!W.isl_done[li]) atomicMax(&W.isl_res[li], fbits(row_residual(W.rows[i], W.dres, i)));
+      }
+    }
+    __syncwarp();
+    it++;
+    bool active = false;
+    for (uint32_t i = lane; i < nisl; i += 32) {
+      if (W.isl_done[i]) continue;
+      uint32_t rb = W.isl_res[i];
+      W.isl_res[i] = 0u;
+      W.isl_sw[i] = (uint32_t)it;
+      W.isl_last[i] = rb;
+      if (tol > 0.0f && __uint_as_float(rb) <= tol) W.isl_done[i] = 1;
+      else active = true;
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    __syncwarp();
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < nbg; i += 32) {
+    uint32_t b = gb_list[b0 + i];
+    G.lin[b] = W.lin[i];
+    G.ang[b] = W.ang[i];
+  }
+  uint32_t my_rs = 0;
+  for (uint32_t i = lane; i < nr; i += 32) {
+    uint32_t r = S.ord[base + i];
+    acc_jn[r] = W.jn[i];
+    acc_jt[r] = W.jt[i];
+    my_rs += W.isl_sw[W.rows[i].flags >> 16];
+  }
+  uint32_t my_sw = 0, my_res = 0, my_cap = 0;
+  for (uint32_t i = lane; i < nisl; i += 32) {
+    my_sw = max(my_sw, W.isl_sw[i]);
+    my_res = max(my_res, W.isl_last[i]);
+    if (tol > 0.0f && !W.isl_done[i]) my_cap++;
+  }
+  my_rs = __reduce_add_sync(0xffffffffu, my_rs);
+  my_cap = __reduce_add_sync(0xffffffffu, my_cap);
+  my_sw = __reduce_max_sync(0xffffffffu, my_sw);
+  my_res = __reduce_max_sync(0xffffffffu, my_res);
+  if (lane == 0) {
+    if (my_rs) atomicAdd(&stats[STAT_ROWSWEEPS], my_rs);
+    if (my_cap) atomicAdd(&stats[STAT_ISLANDS_CAPPED], my_cap);
+    if (my_sw) atomicMax(&stats[STAT_SWEEPS], my_sw);
+    if (my_res) atomicMax(&stats[STAT_RESID], my_res);
   }
 }
 
@@ -1193,7 +1472,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cudaStreamSynchronize(st));
     }
     ctx.nsched = nsched;
-    uint32_t nisl = 0, ng = 0;
+    uint32_t nisl = 0, ng = 0, g_small = 0;
     S.isl_start.ensure(nsched + 1); S.isl_cnt.ensure(nsched + 1);
     S.ord_main.ensure(nsched + 1); S.ord_vs.ensure(nsched + 1); S.ord_ps.ensure(nsched + 1);
     if (nsched > 0) {
@@ -1211,7 +1490,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       k_group_flags<<<nblk(nisl), T, 0, st>>>(nisl, S.isl_cnt.p, S.g_small_rows.p, S.g_big.p); RP_COUNT_LAUNCH(1);
       uint32_t small_total = exclusive_scan_total(S, S.g_small_rows.p, S.g_small_pre.p, nisl, st);
       uint32_t nbig = exclusive_scan_total(S, S.g_big.p, S.g_big_pre.p, nisl, st);
-      uint32_t g_small = small_total ? (small_total - 1) / GROUP_ROWS + 1 : 0;
+      g_small = small_total ? (small_total - 1) / GROUP_ROWS + 1 : 0;
       ng = g_small + nbig;
       k_group_of_isl<<<nblk(nisl), T, 0, st>>>(nisl, S.isl_cnt.p, S.g_small_pre.p, S.g_big_pre.p, g_small, S.g_of_isl.p); RP_COUNT_LAUNCH(1);
       S.g_key.ensure(nsched + 1); S.g_key2.ensure(nsched + 1);
@@ -1225,6 +1504,14 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       k_group_ranges<<<nblk(nsched), T, 0, st>>>(nsched, S.g_key2.p, S.g_start.p, S.g_cnt.p); RP_COUNT_LAUNCH(1);
       S.row_isl2.ensure(nc + 1);
       k_scatter_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.row_isl2.p); RP_COUNT_LAUNCH(1);  // group of each row
+      // each row's island inside its group (the per-island residual stop)
+      S.row_islid.ensure(nc + 1); S.row_lisl.ensure(nc + 1); S.li_flag.ensure(nsched + 1); S.li_pre.ensure(nsched + 1);
+      S.g_nisl.ensure(ng + 1);
+      k_row_island<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched2.p, S.woff.p, S.wpos.p, S.row_islid.p); RP_COUNT_LAUNCH(1);
+      k_local_isl_flags<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.row_islid.p, S.li_flag.p); RP_COUNT_LAUNCH(1);
+      exclusive_scan(S, S.li_flag.p, S.li_pre.p, nsched, st);
+      k_local_isl<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.g_start.p, S.g_cnt.p, S.li_flag.p, S.li_pre.p,
+                                              S.row_lisl.p, S.g_nisl.p); RP_COUNT_LAUNCH(1);
       ctx.nisl = ng;
       // ---- main schedule (row order within each group)
       S.lvl_hist.ensure(nsched + 1);
@@ -1247,7 +1534,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cudaMemsetAsync(S.gb_cnt.p, 0, sizeof(uint32_t) * (ng + 1), st));
       k_body_local<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.gb_cnt.p, S.body_local.p); RP_COUNT_LAUNCH(1);
       k_body_local2<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.body_local.p); RP_COUNT_LAUNCH(1);
-      k_group_class<<<nblk(ng), T, 0, st>>>(ng, S.gb_cnt.p, S.g_class.p); RP_COUNT_LAUNCH(1);
+      k_group_class<<<nblk(ng), T, 0, st>>>(ng, g_small, S.gb_cnt.p, S.g_cnt.p, S.g_class.p, stats); RP_COUNT_LAUNCH(1);
       // levels / max batch (solver.rs:684-687)
       {
         size_t bytes = 0;
@@ -1283,21 +1570,65 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       S.s_jt.ensure(nsched + 1); S.s_wm.ensure(nsched + 1);
       SRowsV SR{S.s_loc.p, S.s_flags.p, S.s_inv.p, S.s_ra.p, S.s_rb.p, S.s_n.p, S.s_t1.p, S.s_t2.p, S.s_mu.p, S.s_va.p,
                 S.s_vb.p, S.s_jn.p, S.s_jt.p, S.s_wm.p};
-      k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, SR); RP_COUNT_LAUNCH(1);
+      k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, S.row_lisl.p, SR); RP_COUNT_LAUNCH(1);
       const float tol = resid_mode ? W.res_tol_ : 0.0f;
-      k_vel_solve_smem<128><<<ng, 128, SMALL_BODIES * 72, st>>>(ng, 0u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
-                                                                SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p,
-                                                                iters, tol, stats); RP_COUNT_LAUNCH(1);
-      static bool big_attr = false;
-      if (!big_attr) {
+      // dynamic shared memory above the 48 KB default, opted into once per device
+      static std::atomic<unsigned long long> smem_attr{0};
+      int dev = 0;
+      RP_CUDA(cudaGetDevice(&dev));
+      if (!((smem_attr.load() >> (dev & 63)) & 1ull)) {
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_smem<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMALL_BODIES * 72));
         RP_CUDA(cudaFuncSetAttribute(k_vel_solve_smem<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, BIG_BODIES * 72));
-        big_attr = true;
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_warp<WG4_ROWS, WG4_BODIES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(WarpSmem4)));
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_warp<WG5_ROWS, WG5_BODIES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(WarpSmem5)));
+        smem_attr.fetch_or(1ull << (dev & 63));
       }
-      k_vel_solve_smem<512><<<ng, 512, BIG_BODIES * 72, st>>>(ng, 1u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
-                                                              SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p,
-                                                              iters, tol, stats); RP_COUNT_LAUNCH(1);
-      k_vel_solve<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p, W.warm_a.p,
-                                                      W.warm_b.p, iters, tol, stats, S.g_class.p); RP_COUNT_LAUNCH(1);
+      // classes 4 and 5 (single islands, few blocks, long) run on two side streams while the
+      // packed groups and the big islands run here; their groups share no body
+      const bool big = ng > g_small;
+      if (big) {
+        RP_CUDA(cudaEventRecord(W.ev_fork_, st));
+        for (int k = 0; k < 2; ++k) RP_CUDA(cudaStreamWaitEvent(W.aux_[k], W.ev_fork_, 0));
+        P.begin(PH_VEL_ISLAND, W.aux_[0]);
+        k_vel_solve_warp<WG4_ROWS, WG4_BODIES, 1><<<ng - g_small, 32, sizeof(WarpSmem4), W.aux_[0]>>>(
+            g_small, ng, 4u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
+            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+        P.end(PH_VEL_ISLAND, W.aux_[0]);
+        P.begin(PH_VEL_ISLAND_L, W.aux_[1]);
+        k_vel_solve_warp<WG5_ROWS, WG5_BODIES, 1><<<ng - g_small, 32, sizeof(WarpSmem5), W.aux_[1]>>>(
+            g_small, ng, 5u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
+            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+        P.end(PH_VEL_ISLAND_L, W.aux_[1]);
+      }
+      P.begin(PH_VEL_PACKED, st);
+      if (g_small > 0)
+        k_vel_solve_warp<WG_ROWS, WG_BODIES, WG_ROWS><<<g_small, 32, sizeof(WarpSmem3), st>>>(
+            0u, g_small, 3u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
+            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+      P.end(PH_VEL_PACKED, st);
+      P.begin(PH_VEL_BIG, st);
+      if (big) {
+        k_vel_solve_smem<128><<<ng - g_small, 128, SMALL_BODIES * 72, st>>>(g_small, ng, 0u, S.g_class.p, S.gb_start.p, S.gb_cnt.p,
+                                                                            S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
+                                                                            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol,
+                                                                            stats); RP_COUNT_LAUNCH(1);
+        k_vel_solve_smem<512><<<ng - g_small, 512, BIG_BODIES * 72, st>>>(g_small, ng, 1u, S.g_class.p, S.gb_start.p, S.gb_cnt.p,
+                                                                          S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
+                                                                          W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol,
+                                                                          stats); RP_COUNT_LAUNCH(1);
+        k_vel_solve<<<nblk((ng - g_small) * 32, 128), 128, 0, st>>>(ng, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
+                                                                    W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
+                                                                    g_small); RP_COUNT_LAUNCH(1);
+      }
+      P.end(PH_VEL_BIG, st);
+      if (big) {
+        for (int k = 0; k < 2; ++k) {
+          RP_CUDA(cudaEventRecord(W.ev_join_[k], W.aux_[k]));
+          RP_CUDA(cudaStreamWaitEvent(st, W.ev_join_[k], 0));
+        }
+      }
     }
     P.end(PH_VEL_SOLVE, st);
     P.begin(PH_WARM_CACHE, st);

@@ -162,6 +162,11 @@ __global__ void k_restore_bodies(uint32_t n, const float4* __restrict__ sp, cons
 // ------------------------------------------------------------------ WorldGpu
 WorldGpu::WorldGpu(uint32_t max_bodies, uint32_t max_colliders) : cap_b_(max_bodies), cap_c_(max_colliders) {
   RP_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) {
+    RP_CUDA(cudaStreamCreateWithFlags(&aux_[k], cudaStreamNonBlocking));
+    RP_CUDA(cudaEventCreateWithFlags(&ev_join_[k], cudaEventDisableTiming));
+  }
+  RP_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
   s_ = new Scratch();
   size_t cb = cap_b_ > 0 ? cap_b_ : 1, cc = cap_c_ > 0 ? cap_c_ : 1;
   pos.ensure(cb); rot.ensure(cb); lin.ensure(cb); ang.ensure(cb); last_lin.ensure(cb);
@@ -181,7 +186,10 @@ WorldGpu::WorldGpu(uint32_t max_bodies, uint32_t max_colliders) : cap_b_(max_bod
 }
 WorldGpu::~WorldGpu() {
   cudaStreamSynchronize(stream_);
+  for (int k = 0; k < 2; ++k) cudaStreamSynchronize(aux_[k]);
   delete s_;
+  for (int k = 0; k < 2; ++k) { cudaEventDestroy(ev_join_[k]); cudaStreamDestroy(aux_[k]); }
+  cudaEventDestroy(ev_fork_);
   cudaStreamDestroy(stream_);
 }
 
@@ -449,6 +457,11 @@ const StepStatsHost& WorldGpu::stats() {
     st_.levels = h[STAT_LEVELS];
     st_.max_batch = h[STAT_MAXBATCH];
     st_.row_sweeps = h[STAT_ROWSWEEPS];
+    st_.groups_shared = h[STAT_GROUPS_SHARED];
+    st_.groups_global = h[STAT_GROUPS_GLOBAL];
+    st_.max_group_rows = h[STAT_MAX_GROUP_ROWS];
+    st_.max_group_bodies = h[STAT_MAX_GROUP_BODIES];
+    st_.islands_capped = h[STAT_ISLANDS_CAPPED];
     stats_dirty_ = false;
   }
   st_.warm_entries = n_warm;

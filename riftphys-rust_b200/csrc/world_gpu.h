@@ -26,6 +26,8 @@ struct StepStatsHost {
   uint32_t sweeps = 0, bounce_skipped = 0, warm_entries = 0, sleeping = 0, error_flags = 0;
   float residual = 0.0f;
   uint32_t row_sweeps = 0, rows_scheduled = 0;
+  uint32_t groups_shared = 0, groups_global = 0, max_group_rows = 0, max_group_bodies = 0;
+  uint32_t islands_capped = 0;
 };
 
 struct PairPropsHost { float mu_s, mu_k, restitution, stribeck_v, stiffness; };
@@ -98,6 +100,9 @@ class WorldGpu {
   static void snapshot_free(SnapshotGpu* s);
 
   cudaStream_t stream() const { return stream_; }
+  // two side streams the velocity solve forks onto (independent solve groups run concurrently)
+  cudaStream_t aux_[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork_ = nullptr, ev_join_[2] = {nullptr, nullptr};
   // per-stage CUDA-event timing (totals since the last reset)
   void profile_enable(bool on);
   int profile_read(double* ms, uint64_t* calls, int cap);

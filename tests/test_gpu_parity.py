@@ -42,7 +42,7 @@ def run_pair(oracle, gpu, build, ticks, check_every=1):
         assert wo.hash() == wg.hash(), f"tick {t}: tick hash differs"
         sto, stg = wo.stats(), wg.stats()
         for k in ("pairs", "contacts", "islands", "levels", "max_batch", "warm_matched", "warm_entries", "sleeping",
-                  "bounce_skipped", "sweeps"):
+                  "bounce_skipped", "sweeps", "row_sweeps", "rows_scheduled", "islands_capped", "residual"):
             assert sto[k] == stg[k], f"tick {t}: stat {k} {sto[k]} vs {stg[k]}"
     return wo, wg
 
@@ -60,3 +60,24 @@ def test_box_drop_1000(oracle, gpu):
 def test_terrain_small(oracle, gpu):
     build = {"cap": (2048, 2048), "fn": lambda rp_, w: scenes.terrain(rp_, w, n_bodies=1500, hf_n=96, area=80.0)}
     run_pair(oracle, gpu, build, 200, check_every=5)
+
+
+def _residual(fn, tol=1e-4, cap=80):
+    def build(rp_, w):
+        out = fn(rp_, w)
+        w.set_residual_mode(tol, cap)
+        return out
+    return build
+
+
+def test_box_drop_1000_residual_mode(oracle, gpu):
+    # each solve island sweeps until its largest velocity change is <= 1e-4 m/s (or 32 sweeps)
+    build = {"cap": (1024, 1024), "fn": _residual(lambda rp_, w: scenes.box_drop(rp_, w, n_side=10), cap=32)}
+    run_pair(oracle, gpu, build, 150, check_every=10)
+
+
+def test_terrain_small_residual_mode(oracle, gpu):
+    build = {"cap": (2048, 2048), "fn": _residual(lambda rp_, w: scenes.terrain(rp_, w, n_bodies=1500, hf_n=96, area=80.0))}
+    _, wg = run_pair(oracle, gpu, build, 160, check_every=8)
+    s = wg.stats()
+    assert s["rows_scheduled"] > 0 and s["row_sweeps"] < 80 * s["rows_scheduled"]  # islands stop on their own
