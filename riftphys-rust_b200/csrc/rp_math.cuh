@@ -10,6 +10,7 @@
 // CUDA's and libm's versions differ in the last ulp.
 #pragma once
 #include <cstdint>
+#include <cstring>
 #include <math.h>
 
 #ifdef __CUDACC__
@@ -195,7 +196,11 @@ RP_HD float exp_rp(float xf) {
   p = p * r + 0.5;
   p = p * r + 1.0;
   p = p * r + 1.0;
-  return (float)ldexp(p, (int)k);
+  // p * 2^k is exact (k in [-150, 128] keeps 2^k a normal double): the same value ldexp gives
+  long long eb = (long long)((int)k + 1023) << 52;
+  double two_k;
+  memcpy(&two_k, &eb, 8);
+  return (float)(p * two_k);
 }
 RP_HD q4 qfrom_axis_angle(f3 axis, float angle) {
   float s, c;

@@ -59,12 +59,12 @@ enum Phase : int {
   PH_WARM_MATCH, PH_VEL_SOLVE, PH_WARM_CACHE, PH_VEL_SHOCK, PH_BALLISTIC, PH_INTEGRATE, PH_POS_ITER,
   PH_POS_SHOCK, PH_STAGE6,
   // parts of vel_solve (nested inside it; named "vel_solve.*")
-  PH_VEL_PACKED, PH_VEL_ISLAND, PH_VEL_ISLAND_L, PH_VEL_BIG, PH_COUNT
+  PH_VEL_PACKED, PH_VEL_ISLAND, PH_VEL_BIG, PH_COUNT
 };
 static const char* const kPhaseNames[PH_COUNT] = {
     "forces", "aabb_sweep", "broadphase", "narrow_pairs", "terrain", "contacts", "islands", "rows", "schedule",
     "warm_match", "vel_solve", "warm_cache", "vel_shock", "ballistic", "integrate", "pos_iter", "pos_shock", "stage6",
-    "vel_solve.packed", "vel_solve.island", "vel_solve.island_l", "vel_solve.big"};
+    "vel_solve.packed", "vel_solve.island", "vel_solve.big"};
 
 struct Profiler {
   bool on = false;
@@ -95,14 +95,32 @@ struct Profiler {
   void reset() { for (int p = 0; p < PH_COUNT; ++p) { ms[p] = 0; calls[p] = 0; used[p] = false; } }
 };
 
+// Growth doubles (a buffer that tracks a rising contact count regrows rarely). Inside a tick the
+// world's stream is set in g_alloc_stream and growth goes through the stream-ordered allocator,
+// whose pool keeps freed memory (release threshold set at world creation): no device-wide
+// synchronisation in the middle of a tick. Contents are not kept across growth.
+extern thread_local cudaStream_t g_alloc_stream;
 template <class T>
 void DBuf<T>::ensure(size_t n) {
   if (n <= cap) return;
-  if (p) cudaFree(p);
-  size_t c = n < 16 ? 16 : n + n / 4;
-  RP_CUDA(cudaMalloc(&p, c * sizeof(T)));
+  size_t c = n < 16 ? 16 : 2 * n;
+  if (g_alloc_stream) {
+    if (p) RP_CUDA(cudaFreeAsync(p, g_alloc_stream));
+    p = nullptr;
+    RP_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), c * sizeof(T), g_alloc_stream));
+  } else {
+    if (p) cudaFree(p);
+    p = nullptr;
+    RP_CUDA(cudaMalloc(&p, c * sizeof(T)));
+  }
   cap = c;
 }
+// Sets g_alloc_stream for the scope of one tick.
+struct AllocStreamScope {
+  cudaStream_t prev;
+  explicit AllocStreamScope(cudaStream_t s) : prev(g_alloc_stream) { g_alloc_stream = s; }
+  ~AllocStreamScope() { g_alloc_stream = prev; }
+};
 template <class T>
 void DBuf<T>::release() {
   if (p) cudaFree(p);
@@ -148,6 +166,7 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> lvl_hist, row_level;
   DBuf<uint32_t> lv_key, lv_key2, lv_val, lv_val2, lv_pred, lv_level, lv_np1;  // parallel level schedule
   DBuf<uint32_t> row_islid, row_lisl, li_flag, li_pre, g_nisl;                 // islands inside solve groups
+  DBuf<uint32_t> cls_cnt, cls_list;                                            // solve groups by class
   // solve groups (islands packed for one CTA each) and their shared-memory residents
   DBuf<uint32_t> g_small_rows, g_small_pre, g_big, g_big_pre, g_of_isl, g_key, g_key2, g_start, g_cnt, g_class,
       body_grp, gb_key, gb_key2, gb_list, gb_tmp, gb_start, gb_cnt, body_local;

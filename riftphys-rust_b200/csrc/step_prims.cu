@@ -7,6 +7,7 @@
 namespace rp {
 
 unsigned long long g_launches = 0;
+thread_local cudaStream_t g_alloc_stream = nullptr;
 
 namespace {
 template <class F>

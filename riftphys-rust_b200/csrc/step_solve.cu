@@ -426,10 +426,13 @@ __device__ __forceinline__ float warp_max(float v) {
 // Warm start application, then the velocity sweeps (solver.rs:717-915).
 __global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* acc_jn, float2* acc_jt,
                             const int* __restrict__ wm_idx, const float4* __restrict__ wa, const float4* __restrict__ wb,
-                            int iters, float tol, uint32_t* stats, const uint32_t* __restrict__ g_class, uint32_t g0) {
-  uint32_t warp = g0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+                            int iters, float tol, uint32_t* stats, const uint32_t* __restrict__ g_class,
+                            const uint32_t* __restrict__ glist) {
+  uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (warp >= nisl || g_class[warp] != 2u) return;
+  if (wi >= nisl) return;
+  uint32_t warp = glist[wi];  // nisl: the number of listed groups
+  if (g_class[warp] != 2u) return;
   uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
   for (uint32_t L = 0; L < nl; ++L) {
     uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
@@ -834,10 +837,14 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
 #define BIG_BODIES 2800u    // shared-memory bodies of a 512-thread CTA
 #define WG_ROWS (2u * GROUP_ROWS)  // rows a packed group can hold
 #define WG_BODIES (2u * WG_ROWS)   // bodies those rows can move
-#define WG4_ROWS 256u              // single islands solved by one warp with everything on chip
-#define WG4_BODIES 512u
-#define WG5_ROWS 1152u
-#define WG5_BODIES 768u
+// single islands solved with everything on chip, by size bucket (class 10 + bucket): rows and
+// bodies held. An island moves at most rows + 1 bodies, so the smaller buckets hold that many;
+// the largest one (1152 rows, 768 bodies: 225.8 KB) is sized to the per-block limit.
+#define ISLAND_BUCKETS 6
+__constant__ uint32_t c_island_rows[ISLAND_BUCKETS] = {128u, 256u, 384u, 512u, 768u, 1152u};
+__constant__ uint32_t c_island_bodies[ISLAND_BUCKETS] = {129u, 257u, 385u, 513u, 769u, 768u};
+static const uint32_t kIslandRows[ISLAND_BUCKETS] = {128u, 256u, 384u, 512u, 768u, 1152u};
+static const uint32_t kIslandBodies[ISLAND_BUCKETS] = {129u, 257u, 385u, 513u, 769u, 768u};
 __global__ void k_group_flags(uint32_t nisl, const uint32_t* __restrict__ isl_cnt, uint32_t* small_rows, uint32_t* big) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nisl) return;
@@ -891,16 +898,20 @@ __global__ void k_body_local2(uint32_t n, const uint32_t* __restrict__ gkey, con
   uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p < n) body_local[blist[p]] = p - gb_start[gkey[p]];
 }
+// Class of every group, and the groups of each class other than 3 listed (in any order: groups
+// are independent, so the order they run in changes no result) for launches of exactly them.
 __global__ void k_group_class(uint32_t ng, uint32_t g_small, const uint32_t* __restrict__ gb_cnt,
-                              const uint32_t* __restrict__ g_cnt, uint32_t* cls, uint32_t* stats) {
+                              const uint32_t* __restrict__ g_cnt, uint32_t* cls, uint32_t* cls_cnt, uint32_t* cls_list,
+                              uint32_t* stats) {
   uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ng) return;
   uint32_t nbg = gb_cnt[g], nr = g_cnt[g];
-  uint32_t c = g < g_small                              ? 3u
-               : (nr <= WG4_ROWS && nbg <= WG4_BODIES)  ? 4u
-               : (nr <= WG5_ROWS && nbg <= WG5_BODIES)  ? 5u
-               : (nbg <= SMALL_BODIES ? 0u : (nbg <= BIG_BODIES ? 1u : 2u));
+  uint32_t c = g < g_small ? 3u : (nbg <= SMALL_BODIES ? 0u : (nbg <= BIG_BODIES ? 1u : 2u));
+  if (g >= g_small)
+    for (int b = ISLAND_BUCKETS - 1; b >= 0; --b)
+      if (nr <= c_island_rows[b] && nbg <= c_island_bodies[b]) c = 10u + (uint32_t)b;
   cls[g] = c;
+  if (c != 3u) cls_list[(size_t)c * ng + atomicAdd(&cls_cnt[c], 1u)] = g;  // classes 0..15
   atomicAdd(&stats[c == 2u ? STAT_GROUPS_GLOBAL : STAT_GROUPS_SHARED], 1u);
   atomicMax(&stats[STAT_MAX_GROUP_ROWS], nr);
   atomicMax(&stats[STAT_MAX_GROUP_BODIES], nbg);
@@ -1043,12 +1054,12 @@ __device__ __forceinline__ float pgs_row_s(const SBodies& B, const SRow& r, uint
 // the same order, so the same bits, with a shorter dependent chain per level. dres receives
 // new_jn - old_jn and the two friction deltas; the row's residual is
 // max(|dres.x| / m_n, |dres.y| / m_t1, |dres.z| / m_t2) over the effective masses that are > 0.
-__device__ __forceinline__ void impulse_reg(f3& lin, f3& ang, float im, const float* q, f3 j, f3 tau) {
+__device__ __forceinline__ void impulse_reg(f3& lin, f3& ang, float im, const m3& Iw, f3 j, f3 tau) {
   if (im > 0.0f && vfin(j)) lin = fin_v(lin + j * im);
-  if (im > 0.0f && vfin(tau)) {
-    m3 Iw = mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
-    ang = fin_v(ang + mvec(Iw, tau));
-  }
+  if (im > 0.0f && vfin(tau)) ang = fin_v(ang + mvec(Iw, tau));
+}
+__device__ __forceinline__ m3 load_iw(const float* q) {
+  return mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
 }
 __device__ __forceinline__ void pgs_row_reg(const SBodies& B, const SRow& r, uint32_t s, float* jn_arr, float2* jt_arr,
                                             float* dres) {
@@ -1058,8 +1069,8 @@ __device__ __forceinline__ void pgs_row_reg(const SBodies& B, const SRow& r, uin
   if (ha || ia) { LA = B.lin[r.la]; AA = B.ang[r.la]; }
   if (hb || ib) { LB = B.lin[r.lb]; AB = B.ang[r.lb]; }
   f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
-  const float* qa = ia ? B.Iw + 9 * (size_t)r.la : B.Iw;
-  const float* qb = ib ? B.Iw + 9 * (size_t)r.lb : B.Iw;
+  const m3 qa = load_iw(ia ? B.Iw + 9 * (size_t)r.la : B.Iw);  // loaded once for both impulses
+  const m3 qb = load_iw(ib ? B.Iw + 9 * (size_t)r.lb : B.Iw);
   float ima = ia ? B.im[r.la] : 0.0f, imb = ib ? B.im[r.lb] : 0.0f;
   auto rel = [&]() {
     f3 va = ha ? la + cross(aa, r.ra) : r.vfix;
@@ -1109,15 +1120,18 @@ __device__ __forceinline__ float row_residual(const SRow& r, const float* dres, 
 // in shared memory, rows streamed from the schedule-ordered arrays; __syncthreads between levels.
 #define GROUP_ISL_MAX 64u  // the CTA kernel solves single islands; the bound only has to cover that
 template <int NT>
-__global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t g0, uint32_t ng, uint32_t want_class,
+__global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t g0, uint32_t ng, const uint32_t* __restrict__ glist,
+                                                       uint32_t want_class,
                                                        const uint32_t* __restrict__ g_class,
                                                        const uint32_t* __restrict__ gb_start, const uint32_t* __restrict__ gb_cnt,
                                                        const uint32_t* __restrict__ gb_list, const uint32_t* __restrict__ g_nisl,
                                                        Sched S, SRowsV R, BodiesV G,
                                                        const float4* __restrict__ wa, const float4* __restrict__ wb,
                                                        float* acc_jn, float2* acc_jt, int iters, float tol, uint32_t* stats) {
-  uint32_t g = g0 + blockIdx.x;
-  if (g >= ng || g_class[g] != want_class) return;
+  if (glist && blockIdx.x >= ng) return;
+  uint32_t g = glist ? glist[blockIdx.x] : g0 + blockIdx.x;
+  if (!glist && g >= ng) return;
+  if (g_class[g] != want_class) return;
   const uint32_t nisl = g_nisl[g];
   if (nisl > GROUP_ISL_MAX) {  // not reached: classes 0 and 1 are single islands
     if (threadIdx.x == 0) atomicOr(&stats[STAT_ERR], 2u);
@@ -1208,102 +1222,134 @@ __global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t g0, uint32_t ng,
   }
 }
 
-// A group solved by one warp with everything it touches in its block's shared memory: rows (in
-// schedule order), impulses, bodies, level starts and per-island residual state; __syncwarp
-// between levels. One warp per block, so the block scheduler hands an SM a new group as soon as
-// any of its groups finishes. Same arithmetic and order as k_vel_solve_smem. Capacities: RC rows,
-// BC bodies, IC islands -- class 3 (packed groups) 64 / 128 / 64 in about 19.5 KB, class 4
-// (islands up to 256 rows) 256 / 512 / 1 in about 75 KB, class 5 (up to 1152 rows)
-// 1152 / 768 / 1 in about 221 KB.
-template <uint32_t RC, uint32_t BC, uint32_t IC>
-struct WarpGroupSmem {
-  float4 lin[BC];
-  float4 ang[BC];
-  float2 jt[RC];
-  SRow rows[RC];
-  float jn[RC];
-  float dres[3 * RC];
-  float Iw[9 * BC];
-  float im[BC];
-  uint32_t lvl[RC + 1];
-  uint32_t isl_res[IC], isl_last[IC], isl_sw[IC];
-  uint8_t isl_done[IC];
+// A group solved by one block with everything it touches in that block's shared memory: rows
+// (in schedule order), impulses, bodies, level starts and per-island residual state; a block
+// barrier between levels. Same arithmetic and order as k_vel_solve_smem. Capacities RC rows,
+// BC bodies, IC islands set the layout: packed groups (class 3) 64 / 128 / 64 in about 20 KB
+// with 64 threads; single islands (classes 10..15) R / R + 1 / 1 for R = 128 ... 1024 rows,
+// about 220 bytes per row (28 KB ... 225 KB), with 128 threads.
+struct OnchipLayout {
+  uint32_t RC, BC, IC;
+  uint32_t o_lin, o_ang, o_jt, o_rows, o_jn, o_dres, o_Iw, o_im, o_lvl, o_res, o_last, o_sw, o_done, bytes;
 };
-typedef WarpGroupSmem<WG_ROWS, WG_BODIES, WG_ROWS> WarpSmem3;
-typedef WarpGroupSmem<WG4_ROWS, WG4_BODIES, 1> WarpSmem4;
-typedef WarpGroupSmem<WG5_ROWS, WG5_BODIES, 1> WarpSmem5;
-static_assert(sizeof(WarpSmem5) <= 232448, "class-5 warp group exceeds the per-block shared memory limit");
-template <uint32_t RC, uint32_t BC, uint32_t IC>
-__global__ void __launch_bounds__(32) k_vel_solve_warp(uint32_t g0, uint32_t ng, uint32_t want_class,
-                                                       const uint32_t* __restrict__ g_class,
-                                                       const uint32_t* __restrict__ gb_start,
-                                                       const uint32_t* __restrict__ gb_cnt,
-                                                       const uint32_t* __restrict__ gb_list,
-                                                       const uint32_t* __restrict__ g_nisl, Sched S, SRowsV R,
-                                                       BodiesV G, const float4* __restrict__ wa,
-                                                       const float4* __restrict__ wb, float* acc_jn, float2* acc_jt,
-                                                       int iters, float tol, uint32_t* stats) {
-  uint32_t g = g0 + blockIdx.x;
-  if (g >= ng || g_class[g] != want_class) return;
+__host__ __device__ inline uint32_t onchip_take(uint32_t& o, uint32_t bytes) {
+  uint32_t a = o;
+  o = (o + bytes + 15u) & ~15u;
+  return a;
+}
+__host__ __device__ inline OnchipLayout onchip_layout(uint32_t RC, uint32_t BC, uint32_t IC) {
+  OnchipLayout L;
+  L.RC = RC; L.BC = BC; L.IC = IC;
+  uint32_t o = 0;
+  L.o_lin = onchip_take(o, 16u * BC);
+  L.o_ang = onchip_take(o, 16u * BC);
+  L.o_jt = onchip_take(o, 8u * RC);
+  L.o_rows = onchip_take(o, (uint32_t)sizeof(SRow) * RC);
+  L.o_jn = onchip_take(o, 4u * RC);
+  L.o_dres = onchip_take(o, 12u * RC);
+  L.o_Iw = onchip_take(o, 36u * BC);
+  L.o_im = onchip_take(o, 4u * BC);
+  L.o_lvl = onchip_take(o, 4u * (RC + 1u));
+  L.o_res = onchip_take(o, 4u * IC);
+  L.o_last = onchip_take(o, 4u * IC);
+  L.o_sw = onchip_take(o, 4u * IC);
+  L.o_done = onchip_take(o, IC);
+  L.bytes = o;
+  return L;
+}
+#define ONCHIP_T_PACKED 64   // threads of a packed-group block (levels of up to 63 rows in one pass)
+#define ONCHIP_T_ISLAND 128  // threads of a single-island block (wide first levels of terrain piles)
+template <bool MULTI, int NT>
+__global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32_t g0, uint32_t ng,
+                                                         const uint32_t* __restrict__ glist, uint32_t want_class,
+                                                         const uint32_t* __restrict__ g_class,
+                                                         const uint32_t* __restrict__ gb_start,
+                                                         const uint32_t* __restrict__ gb_cnt,
+                                                         const uint32_t* __restrict__ gb_list,
+                                                         const uint32_t* __restrict__ g_nisl, Sched S, SRowsV R,
+                                                         BodiesV G, const float4* __restrict__ wa,
+                                                         const float4* __restrict__ wb, float* acc_jn, float2* acc_jt,
+                                                         int iters, float tol, uint32_t* stats) {
+  if (glist && blockIdx.x >= ng) return;
+  uint32_t g = glist ? glist[blockIdx.x] : g0 + blockIdx.x;
+  if (!glist && g >= ng) return;
+  if (g_class[g] != want_class) return;
   extern __shared__ float4 wsm_raw[];
-  WarpGroupSmem<RC, BC, IC>& W = *reinterpret_cast<WarpGroupSmem<RC, BC, IC>*>(wsm_raw);
-  const uint32_t lane = threadIdx.x;
+  unsigned char* sb = reinterpret_cast<unsigned char*>(wsm_raw);
+  struct {
+    float4 *lin, *ang; float2* jt; SRow* rows; float *jn, *dres, *Iw, *im;
+    uint32_t *lvl, *isl_res, *isl_last, *isl_sw; uint8_t* isl_done;
+  } W{reinterpret_cast<float4*>(sb + Lo.o_lin), reinterpret_cast<float4*>(sb + Lo.o_ang),
+      reinterpret_cast<float2*>(sb + Lo.o_jt), reinterpret_cast<SRow*>(sb + Lo.o_rows),
+      reinterpret_cast<float*>(sb + Lo.o_jn), reinterpret_cast<float*>(sb + Lo.o_dres),
+      reinterpret_cast<float*>(sb + Lo.o_Iw), reinterpret_cast<float*>(sb + Lo.o_im),
+      reinterpret_cast<uint32_t*>(sb + Lo.o_lvl), reinterpret_cast<uint32_t*>(sb + Lo.o_res),
+      reinterpret_cast<uint32_t*>(sb + Lo.o_last), reinterpret_cast<uint32_t*>(sb + Lo.o_sw), sb + Lo.o_done};
+  const uint32_t RC = Lo.RC, BC = Lo.BC, IC = Lo.IC;
+  __shared__ uint32_t red[NT / 32][4];
+  const uint32_t tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const uint32_t nbg = gb_cnt[g], b0 = gb_start[g], nisl = g_nisl[g];
   const uint32_t off = S.lvl_off[g], nl = S.nlev[g];
   const uint32_t base = S.lvl_start[off], nr = S.lvl_start[off + nl] - base;
   if (nbg > BC || nr > RC || nisl > IC) {  // not reached: the class was chosen by these sizes
-    if (lane == 0) atomicOr(&stats[STAT_ERR], 2u);
+    if (tid == 0) atomicOr(&stats[STAT_ERR], 2u);
     return;
   }
-  for (uint32_t i = lane; i < nbg; i += 32) {
+  for (uint32_t i = tid; i < nbg; i += NT) {
     uint32_t b = gb_list[b0 + i];
     W.lin[i] = G.lin[b];
     W.ang[i] = G.ang[b];
     for (int k = 0; k < 9; ++k) W.Iw[9 * i + k] = G.Iw[9 * (size_t)b + k];
     W.im[i] = G.inv_mass[b];
   }
-  for (uint32_t i = lane; i < nr; i += 32) {
+  for (uint32_t i = tid; i < nr; i += NT) {
     W.rows[i] = ld_srow(R, base + i);
     W.jn[i] = 0.0f;
     W.jt[i] = make_float2(0.0f, 0.0f);
   }
-  for (uint32_t L = lane; L <= nl; L += 32) W.lvl[L] = S.lvl_start[off + L] - base;
-  for (uint32_t i = lane; i < nisl; i += 32) { W.isl_res[i] = 0u; W.isl_last[i] = 0u; W.isl_sw[i] = 0u; W.isl_done[i] = 0; }
-  __syncwarp();
+  for (uint32_t L = tid; L <= nl; L += NT) W.lvl[L] = S.lvl_start[off + L] - base;
+  for (uint32_t i = tid; i < nisl; i += NT) { W.isl_res[i] = 0u; W.isl_last[i] = 0u; W.isl_sw[i] = 0u; W.isl_done[i] = 0; }
+  __syncthreads();
   SBodies B{W.lin, W.ang, W.Iw, W.im};
   for (uint32_t L = 0; L < nl; ++L) {
-    for (uint32_t i = W.lvl[L] + lane; i < W.lvl[L + 1]; i += 32) {
+    for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1]; i += NT) {
       int e = R.wm[base + i];
       if (e >= 0) warm_apply_s(B, W.rows[i], i, wa[e], wb[e], W.jn, W.jt);
     }
-    __syncwarp();
+    __syncthreads();
   }
   int it = 0;
   while (it < iters) {
     for (uint32_t L = 0; L < nl; ++L) {
-      for (uint32_t i = W.lvl[L] + lane; i < W.lvl[L + 1]; i += 32) {
+      for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1]; i += NT) {
         const SRow& r = W.rows[i];
-        if (IC > 1 && W.isl_done[r.flags >> 16]) continue;
+        if (MULTI && W.isl_done[r.flags >> 16]) continue;
         pgs_row_reg(B, r, i, W.jn, W.jt, W.dres);
       }
-      __syncwarp();
+      __syncthreads();
     }
     // the sweep's residual per island, off the level chain (non-negative floats: integer max)
-    if (IC == 1) {
+    if (!MULTI) {
       uint32_t m = 0;
-      for (uint32_t i = lane; i < nr; i += 32) m = max(m, fbits(row_residual(W.rows[i], W.dres, i)));
+      for (uint32_t i = tid; i < nr; i += NT) m = max(m, fbits(row_residual(W.rows[i], W.dres, i)));
       m = __reduce_max_sync(0xffffffffu, m);
-      if (lane == 0) W.isl_res[0] = m;
+      if (lane == 0) red[wid][0] = m;
+      __syncthreads();
+      if (tid == 0) {
+        uint32_t x = 0;
+        for (int w = 0; w < NT / 32; ++w) x = max(x, red[w][0]);
+        W.isl_res[0] = x;
+      }
     } else {
-      for (uint32_t i = lane; i < nr; i += 32) {
+      for (uint32_t i = tid; i < nr; i += NT) {
         uint32_t li = W.rows[i].flags >> 16;
         if (!W.isl_done[li]) atomicMax(&W.isl_res[li], fbits(row_residual(W.rows[i], W.dres, i)));
       }
     }
-    __syncwarp();
+    __syncthreads();
     it++;
     bool active = false;
-    for (uint32_t i = lane; i < nisl; i += 32) {
+    for (uint32_t i = tid; i < nisl; i += NT) {
       if (W.isl_done[i]) continue;
       uint32_t rb = W.isl_res[i];
       W.isl_res[i] = 0u;
@@ -1312,24 +1358,22 @@ __global__ void __launch_bounds__(32) k_vel_solve_warp(uint32_t g0, uint32_t ng,
       if (tol > 0.0f && __uint_as_float(rb) <= tol) W.isl_done[i] = 1;
       else active = true;
     }
-    if (!__any_sync(0xffffffffu, active)) break;
-    __syncwarp();
+    if (!__syncthreads_or(active)) break;
   }
-  __syncwarp();
-  for (uint32_t i = lane; i < nbg; i += 32) {
+  for (uint32_t i = tid; i < nbg; i += NT) {
     uint32_t b = gb_list[b0 + i];
     G.lin[b] = W.lin[i];
     G.ang[b] = W.ang[i];
   }
   uint32_t my_rs = 0;
-  for (uint32_t i = lane; i < nr; i += 32) {
+  for (uint32_t i = tid; i < nr; i += NT) {
     uint32_t r = S.ord[base + i];
     acc_jn[r] = W.jn[i];
     acc_jt[r] = W.jt[i];
     my_rs += W.isl_sw[W.rows[i].flags >> 16];
   }
   uint32_t my_sw = 0, my_res = 0, my_cap = 0;
-  for (uint32_t i = lane; i < nisl; i += 32) {
+  for (uint32_t i = tid; i < nisl; i += NT) {
     my_sw = max(my_sw, W.isl_sw[i]);
     my_res = max(my_res, W.isl_last[i]);
     if (tol > 0.0f && !W.isl_done[i]) my_cap++;
@@ -1338,11 +1382,16 @@ __global__ void __launch_bounds__(32) k_vel_solve_warp(uint32_t g0, uint32_t ng,
   my_cap = __reduce_add_sync(0xffffffffu, my_cap);
   my_sw = __reduce_max_sync(0xffffffffu, my_sw);
   my_res = __reduce_max_sync(0xffffffffu, my_res);
-  if (lane == 0) {
-    if (my_rs) atomicAdd(&stats[STAT_ROWSWEEPS], my_rs);
-    if (my_cap) atomicAdd(&stats[STAT_ISLANDS_CAPPED], my_cap);
-    if (my_sw) atomicMax(&stats[STAT_SWEEPS], my_sw);
-    if (my_res) atomicMax(&stats[STAT_RESID], my_res);
+  __syncthreads();
+  if (lane == 0) { red[wid][0] = my_rs; red[wid][1] = my_cap; red[wid][2] = my_sw; red[wid][3] = my_res; }
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t a = 0, c = 0, w_ = 0, r_ = 0;
+    for (int w = 0; w < NT / 32; ++w) { a += red[w][0]; c += red[w][1]; w_ = max(w_, red[w][2]); r_ = max(r_, red[w][3]); }
+    if (a) atomicAdd(&stats[STAT_ROWSWEEPS], a);
+    if (c) atomicAdd(&stats[STAT_ISLANDS_CAPPED], c);
+    if (w_) atomicMax(&stats[STAT_SWEEPS], w_);
+    if (r_) atomicMax(&stats[STAT_RESID], r_);
   }
 }
 
@@ -1473,6 +1522,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     }
     ctx.nsched = nsched;
     uint32_t nisl = 0, ng = 0, g_small = 0;
+    uint32_t cls_n[16] = {};  // groups per class (class 3: g_small, not listed)
     S.isl_start.ensure(nsched + 1); S.isl_cnt.ensure(nsched + 1);
     S.ord_main.ensure(nsched + 1); S.ord_vs.ensure(nsched + 1); S.ord_ps.ensure(nsched + 1);
     if (nsched > 0) {
@@ -1534,7 +1584,12 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cudaMemsetAsync(S.gb_cnt.p, 0, sizeof(uint32_t) * (ng + 1), st));
       k_body_local<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.gb_cnt.p, S.body_local.p); RP_COUNT_LAUNCH(1);
       k_body_local2<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.body_local.p); RP_COUNT_LAUNCH(1);
-      k_group_class<<<nblk(ng), T, 0, st>>>(ng, g_small, S.gb_cnt.p, S.g_cnt.p, S.g_class.p, stats); RP_COUNT_LAUNCH(1);
+      S.cls_cnt.ensure(16); S.cls_list.ensure(16 * (size_t)ng + 16);
+      RP_CUDA(cudaMemsetAsync(S.cls_cnt.p, 0, 16 * 4, st));
+      k_group_class<<<nblk(ng), T, 0, st>>>(ng, g_small, S.gb_cnt.p, S.g_cnt.p, S.g_class.p, S.cls_cnt.p, S.cls_list.p,
+                                            stats); RP_COUNT_LAUNCH(1);
+      RP_CUDA(cudaMemcpyAsync(cls_n, S.cls_cnt.p, 16 * 4, cudaMemcpyDeviceToHost, st));
+      RP_CUDA(cudaStreamSynchronize(st));
       // levels / max batch (solver.rs:684-687)
       {
         size_t bytes = 0;
@@ -1573,58 +1628,65 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, S.row_lisl.p, SR); RP_COUNT_LAUNCH(1);
       const float tol = resid_mode ? W.res_tol_ : 0.0f;
       // dynamic shared memory above the 48 KB default, opted into once per device
+      const OnchipLayout lay_packed = onchip_layout(WG_ROWS, WG_BODIES, WG_ROWS);
+      const OnchipLayout lay_top = onchip_layout(kIslandRows[ISLAND_BUCKETS - 1], kIslandBodies[ISLAND_BUCKETS - 1], 1u);
       static std::atomic<unsigned long long> smem_attr{0};
       int dev = 0;
       RP_CUDA(cudaGetDevice(&dev));
       if (!((smem_attr.load() >> (dev & 63)) & 1ull)) {
         RP_CUDA(cudaFuncSetAttribute(k_vel_solve_smem<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMALL_BODIES * 72));
         RP_CUDA(cudaFuncSetAttribute(k_vel_solve_smem<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, BIG_BODIES * 72));
-        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_warp<WG4_ROWS, WG4_BODIES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(WarpSmem4)));
-        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_warp<WG5_ROWS, WG5_BODIES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(WarpSmem5)));
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_onchip<false, ONCHIP_T_ISLAND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)lay_top.bytes));
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_onchip<true, ONCHIP_T_PACKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)lay_packed.bytes));
         smem_attr.fetch_or(1ull << (dev & 63));
       }
-      // classes 4 and 5 (single islands, few blocks, long) run on two side streams while the
-      // packed groups and the big islands run here; their groups share no body
+      // single islands (classes 10..15, few blocks, long) run on the side streams, one bucket per
+      // stream, largest first, while the packed groups and the biggest islands run here; no two
+      // groups share a body
       const bool big = ng > g_small;
+      auto lst = [&](int c) { return S.cls_list.p + (size_t)c * ng; };
       if (big) {
         RP_CUDA(cudaEventRecord(W.ev_fork_, st));
-        for (int k = 0; k < 2; ++k) RP_CUDA(cudaStreamWaitEvent(W.aux_[k], W.ev_fork_, 0));
-        P.begin(PH_VEL_ISLAND, W.aux_[0]);
-        k_vel_solve_warp<WG4_ROWS, WG4_BODIES, 1><<<ng - g_small, 32, sizeof(WarpSmem4), W.aux_[0]>>>(
-            g_small, ng, 4u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
-            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
-        P.end(PH_VEL_ISLAND, W.aux_[0]);
-        P.begin(PH_VEL_ISLAND_L, W.aux_[1]);
-        k_vel_solve_warp<WG5_ROWS, WG5_BODIES, 1><<<ng - g_small, 32, sizeof(WarpSmem5), W.aux_[1]>>>(
-            g_small, ng, 5u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
-            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
-        P.end(PH_VEL_ISLAND_L, W.aux_[1]);
+        int top = -1;  // the largest non-empty bucket, timed as "vel_solve.island"
+        for (int b = ISLAND_BUCKETS - 1; b >= 0; --b) {
+          cudaStream_t sb = W.aux_[b];
+          RP_CUDA(cudaStreamWaitEvent(sb, W.ev_fork_, 0));
+          uint32_t n = cls_n[10 + b];
+          if (!n) continue;
+          if (top < 0) { top = b; P.begin(PH_VEL_ISLAND, sb); }
+          OnchipLayout lay = onchip_layout(kIslandRows[b], kIslandBodies[b], 1u);
+          k_vel_solve_onchip<false, ONCHIP_T_ISLAND><<<n, ONCHIP_T_ISLAND, lay.bytes, sb>>>(
+              lay, 0u, n, lst(10 + b), 10u + (uint32_t)b, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
+              S.g_nisl.p, SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+          if (b == top) P.end(PH_VEL_ISLAND, sb);
+        }
       }
       P.begin(PH_VEL_PACKED, st);
       if (g_small > 0)
-        k_vel_solve_warp<WG_ROWS, WG_BODIES, WG_ROWS><<<g_small, 32, sizeof(WarpSmem3), st>>>(
-            0u, g_small, 3u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
-            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+        k_vel_solve_onchip<true, ONCHIP_T_PACKED><<<g_small, ONCHIP_T_PACKED, lay_packed.bytes, st>>>(
+            lay_packed, 0u, g_small, nullptr, 3u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
+            W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
       P.end(PH_VEL_PACKED, st);
       P.begin(PH_VEL_BIG, st);
-      if (big) {
-        k_vel_solve_smem<128><<<ng - g_small, 128, SMALL_BODIES * 72, st>>>(g_small, ng, 0u, S.g_class.p, S.gb_start.p, S.gb_cnt.p,
-                                                                            S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
-                                                                            W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol,
-                                                                            stats); RP_COUNT_LAUNCH(1);
-        k_vel_solve_smem<512><<<ng - g_small, 512, BIG_BODIES * 72, st>>>(g_small, ng, 1u, S.g_class.p, S.gb_start.p, S.gb_cnt.p,
-                                                                          S.gb_list.p, S.g_nisl.p, SM, SR, B, W.warm_a.p,
-                                                                          W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol,
-                                                                          stats); RP_COUNT_LAUNCH(1);
-        k_vel_solve<<<nblk((ng - g_small) * 32, 128), 128, 0, st>>>(ng, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
-                                                                    W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
-                                                                    g_small); RP_COUNT_LAUNCH(1);
-      }
+      if (cls_n[0])
+        k_vel_solve_smem<128><<<cls_n[0], 128, SMALL_BODIES * 72, st>>>(0u, cls_n[0], lst(0), 0u, S.g_class.p, S.gb_start.p,
+                                                                        S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
+                                                                        W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters,
+                                                                        tol, stats); RP_COUNT_LAUNCH(1);
+      if (cls_n[1])
+        k_vel_solve_smem<512><<<cls_n[1], 512, BIG_BODIES * 72, st>>>(0u, cls_n[1], lst(1), 1u, S.g_class.p, S.gb_start.p,
+                                                                      S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
+                                                                      W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters,
+                                                                      tol, stats); RP_COUNT_LAUNCH(1);
+      if (cls_n[2])
+        k_vel_solve<<<nblk(cls_n[2] * 32, 128), 128, 0, st>>>(cls_n[2], SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
+                                                               W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
+                                                               lst(2)); RP_COUNT_LAUNCH(1);
       P.end(PH_VEL_BIG, st);
       if (big) {
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < ISLAND_BUCKETS; ++k) {
           RP_CUDA(cudaEventRecord(W.ev_join_[k], W.aux_[k]));
           RP_CUDA(cudaStreamWaitEvent(st, W.ev_join_[k], 0));
         }

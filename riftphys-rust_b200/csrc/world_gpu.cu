@@ -162,11 +162,25 @@ __global__ void k_restore_bodies(uint32_t n, const float4* __restrict__ sp, cons
 // ------------------------------------------------------------------ WorldGpu
 WorldGpu::WorldGpu(uint32_t max_bodies, uint32_t max_colliders) : cap_b_(max_bodies), cap_c_(max_colliders) {
   RP_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  for (int k = 0; k < 2; ++k) {
-    RP_CUDA(cudaStreamCreateWithFlags(&aux_[k], cudaStreamNonBlocking));
+  // the side streams carry the long single-island solves: highest priority, so the block
+  // scheduler places them before the many short packed groups queued on the main stream
+  int prio_least = 0, prio_greatest = 0;
+  RP_CUDA(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+  for (int k = 0; k < kAux; ++k) {
+    RP_CUDA(cudaStreamCreateWithPriority(&aux_[k], cudaStreamNonBlocking, prio_greatest));
     RP_CUDA(cudaEventCreateWithFlags(&ev_join_[k], cudaEventDisableTiming));
   }
   RP_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+  {
+    // the stream-ordered pool keeps what a tick frees, so regrowing scratch never returns memory
+    // to the driver mid-run (this process's default pool on this device only)
+    int dev = 0;
+    cudaMemPool_t pool;
+    RP_CUDA(cudaGetDevice(&dev));
+    RP_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thr = UINT64_MAX;
+    RP_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  }
   s_ = new Scratch();
   size_t cb = cap_b_ > 0 ? cap_b_ : 1, cc = cap_c_ > 0 ? cap_c_ : 1;
   pos.ensure(cb); rot.ensure(cb); lin.ensure(cb); ang.ensure(cb); last_lin.ensure(cb);
@@ -186,9 +200,9 @@ WorldGpu::WorldGpu(uint32_t max_bodies, uint32_t max_colliders) : cap_b_(max_bod
 }
 WorldGpu::~WorldGpu() {
   cudaStreamSynchronize(stream_);
-  for (int k = 0; k < 2; ++k) cudaStreamSynchronize(aux_[k]);
+  for (int k = 0; k < kAux; ++k) cudaStreamSynchronize(aux_[k]);
   delete s_;
-  for (int k = 0; k < 2; ++k) { cudaEventDestroy(ev_join_[k]); cudaStreamDestroy(aux_[k]); }
+  for (int k = 0; k < kAux; ++k) { cudaEventDestroy(ev_join_[k]); cudaStreamDestroy(aux_[k]); }
   cudaEventDestroy(ev_fork_);
   cudaStreamDestroy(stream_);
 }
@@ -408,6 +422,7 @@ void WorldGpu::clear_heightfield() { has_hf_ = false; }
 
 // ------------------------------------------------------------------ the tick
 void WorldGpu::step(float dt) {
+  AllocStreamScope alloc_scope(stream_);
   tick_ += 1;
   RP_CUDA(cudaMemsetAsync(d_stats.p, 0, STAT_COUNT * 4, stream_));
   StepCtx ctx;

@@ -100,9 +100,10 @@ class WorldGpu {
   static void snapshot_free(SnapshotGpu* s);
 
   cudaStream_t stream() const { return stream_; }
-  // two side streams the velocity solve forks onto (independent solve groups run concurrently)
-  cudaStream_t aux_[2] = {nullptr, nullptr};
-  cudaEvent_t ev_fork_ = nullptr, ev_join_[2] = {nullptr, nullptr};
+  // side streams the velocity solve forks onto (independent solve groups run concurrently)
+  static constexpr int kAux = 6;
+  cudaStream_t aux_[kAux] = {};
+  cudaEvent_t ev_fork_ = nullptr, ev_join_[kAux] = {};
   // per-stage CUDA-event timing (totals since the last reset)
   void profile_enable(bool on);
   int profile_read(double* ms, uint64_t* calls, int cap);
