@@ -60,7 +60,21 @@ BYTES = {
 }
 
 
-def build_scene(lib, config, n_bodies=None, area=None, hf_n=None):
+ITERS = {"terrain": 20, "box_drop": 8, "batch": 16}
+
+
+def build_scene(lib, config, n_bodies=None, area=None, hf_n=None, worlds=4096, rank=0):
+    if config == "batch":
+        # each rank steps its own set of worlds (the world table sharded across GPUs, no exchange)
+        descs = [scenes.batch_world_descs(rp, k, seed=3 + rank) for k in range(worlds)]
+        total = sum(len(d) for d in descs)
+        w = lib.world(total + 16, total + 16)
+        dt = scenes.batch_setup(w)
+        for d in descs:
+            w.add_world(d)
+        return w, dt, total, (f"batch: {worlds} independent worlds stepped together ({total:,} bodies), body counts "
+                              "log-uniform in [16, 4096], alternately square box pyramids and random box piles "
+                              "(half-extents U[0.25, 0.75] m, 1000 kg/m^3) on 50x0.5x50 ground boxes, dt 1/60, 16 iters")
     if config == "box_drop":
         side = max(1, round((n_bodies or 1000) ** (1.0 / 3.0)))
         w = lib.world(side ** 3 + 24, side ** 3 + 24)
@@ -173,7 +187,8 @@ def main():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--settle", type=int, default=240)
-    ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop"])
+    ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop", "batch"])
+    ap.add_argument("--worlds", type=int, default=4096, help="batch: number of worlds")
     ap.add_argument("--mode", default="residual", choices=["residual", "fixed"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--bodies", type=int, default=None)
@@ -192,9 +207,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
     lib = rp.load_product()
-    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies)
+    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, worlds=args.worlds, rank=rank)
     if args.mode == "residual":
-        w.set_residual_mode(TOL, 4 * (8 if args.config == "box_drop" else 20))
+        w.set_residual_mode(TOL, 4 * ITERS[args.config])
     # settle into the contact regime, then warm up
     t_settle = time.perf_counter()
     if args.settle:
@@ -255,7 +270,7 @@ def main():
         units["bodies"] += nb
         units["colliders"] += nb
         units["row_sweeps"] += s["row_sweeps"]
-        units["pos_row_sweeps"] += s["rows_scheduled"] * (8 if args.config == "box_drop" else 20)
+        units["pos_row_sweeps"] += s["rows_scheduled"] * ITERS[args.config]
         units["pairs"] += s["pairs"]
     prof = w.profile_read()
     w.profile(False)
@@ -286,6 +301,24 @@ def main():
         v, sample = cpu_sample_with(olib, 10, threads)
         cpu = {"value": v, "unit": "body-ticks/s", "cores": threads, "kind": "port", "sample": sample}
 
+    rollback = None
+    if args.config == "batch":
+        # the rollback workload: back to the snapshot, re-simulate 8 ticks twice from it (the first
+        # pass and the replay), the replay timed on the device; every world's hash must match
+        w.restore_exact(snap)
+        w.step_n(dt, 8)
+        h_first = w.world_hashes()
+        w.restore_exact(snap)
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        r0.record(stream)
+        w.step_n(dt, 8)
+        r1.record(stream)
+        torch.cuda.synchronize()
+        h_again = w.world_hashes()
+        rollback = {"ticks": 8, "ms": r0.elapsed_time(r1), "worlds": w.num_worlds(),
+                    "hashes_match": h_first == h_again}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "body-ticks/s", "n_gpus": world_size, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -303,6 +336,8 @@ def main():
                                                       "max_bodies": st["max_group_bodies"]}},
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "stage_ms": stages}
+        if rollback is not None:
+            line["rollback"] = rollback
         print(json.dumps(line), flush=True)
     w.free_snapshot(snap)
     w.close()

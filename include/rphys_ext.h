@@ -127,6 +127,32 @@ RPhysResult rphys_ext_stream_handle(const RPhysWorld* world, uint64_t* out_strea
  * counts its kernels, and each device-wide sort, scan or select counts the kernels it runs. */
 RPhysResult rphys_ext_launch_count(uint64_t* out_launches);
 
+/* ---- Batched worlds (no counterpart in the reference, which steps one World per call).
+ * Many independent worlds live in one RPhysWorld and are stepped together by rphys_world_step_ex
+ * / rphys_ext_step_n: every kernel of the tick covers all of them, bodies of different worlds never
+ * pair, and each world's results are bit-identical to stepping it alone. Worlds are appended in
+ * order, each with all its bodies in one call; the first call must be on an empty RPhysWorld.
+ * Ids stay global 1-based (a world's bodies are one contiguous run); gravity, pair properties,
+ * iterations, residual mode and a heightfield (if set) are shared. Snapshot and restore cover the
+ * whole batch (rollback of every world at once). */
+RPhysResult rphys_ext_batch_add_world(RPhysWorld* world, const RPhysBodyDescEx* descs, uint32_t count,
+                                      uint32_t* out_world, uint32_t* out_first_id);
+RPhysResult rphys_ext_batch_num_worlds(const RPhysWorld* world, uint32_t* out_count);
+RPhysResult rphys_ext_batch_world_range(const RPhysWorld* world, uint32_t world_index, uint32_t* out_first_id,
+                                        uint32_t* out_count);
+/* Restores every bit a snapshot holds (poses, velocities, carried state, warm-start cache) as a
+ * World clone would, where rphys_world_snapshot_restore follows the reference FFI
+ * (lib.rs:1754-1793) and re-injects poses through set_pose, which renormalises rotations, so a
+ * replay after it can differ in the last bits. For rollback windows whose re-simulation must
+ * reproduce the first pass's hashes (no counterpart in the reference FFI). The body set must be
+ * the snapshot's: RPHYS_ERR_BAD_ARG otherwise. */
+RPhysResult rphys_ext_snapshot_restore_exact(RPhysWorld* world, const RPhysWorldSnapshot* snapshot);
+
+/* Per-world tick hashes: world k's digest equals rphys_world_get_step_hash of a world created with
+ * capacity = its body count and holding only its bodies. */
+RPhysResult rphys_ext_batch_get_hashes(const RPhysWorld* world, uint32_t first_world, uint32_t count,
+                                       RPhysHash32* out_hashes);
+
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:
  * cudaMalloc and cudaFree can wait for all work on the device and their memory use varies with the

@@ -265,6 +265,32 @@ RPhysResult rphys_world_get_step_hash(const RPhysWorld* Wc, RPhysHash32* out) {
   W->w.step_hash(out->bytes);
   return RPHYS_OK;
 }
+// Batches are a property of the CUDA library; the restatement steps each world as its own World
+// (the tests build one oracle World per batch world), so these entry points only exist for the
+// shared bindings.
+RPhysResult rphys_ext_batch_add_world(RPhysWorld*, const RPhysBodyDescEx*, uint32_t, uint32_t* w, uint32_t* f) {
+  if (w) *w = 0;
+  if (f) *f = 0;
+  return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_batch_add_world: the CPU restatement steps one world per RPhysWorld");
+}
+RPhysResult rphys_ext_batch_num_worlds(const RPhysWorld* W, uint32_t* out) {
+  if (!W || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_batch_num_worlds: null arg");
+  *out = 1;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_batch_world_range(const RPhysWorld* W, uint32_t world, uint32_t* first, uint32_t* count) {
+  if (!W || !first || !count) return fail(RPHYS_ERR_NULL, "rphys_ext_batch_world_range: null arg");
+  if (world != 0) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_batch_world_range: no such world");
+  *first = 1;
+  *count = W->w.num_bodies();
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_batch_get_hashes(const RPhysWorld* W, uint32_t first, uint32_t count, RPhysHash32* out) {
+  if (!W || (!out && count)) return fail(RPHYS_ERR_NULL, "rphys_ext_batch_get_hashes: null arg");
+  if ((uint64_t)first + count > 1) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_batch_get_hashes: world range out of bounds");
+  for (uint32_t k = 0; k < count; ++k) rphys_world_get_step_hash(W, &out[k]);
+  return RPHYS_OK;
+}
 // The CPU restatement allocates as it likes; this entry point only mirrors the CUDA library's
 // symbol so both load through the same bindings, and returns the same digest.
 RPhysResult rphys_ext_world_step_hash_noalloc(const RPhysWorld* Wc, RPhysHash32* out) {
@@ -385,6 +411,24 @@ RPhysResult rphys_world_snapshot_restore(RPhysWorld* W, const RPhysWorldSnapshot
       w.set_body_pose(i, s->s.poses[i]);
       w.set_body_vel(i, s->s.lin[i], s->s.ang[i]);
     }
+  }
+  w.restore_carried_state(s->s.carried);
+  return RPHYS_OK;
+}
+// World-clone restore: the stored bits themselves, then the carried state.
+RPhysResult rphys_ext_snapshot_restore_exact(RPhysWorld* W, const RPhysWorldSnapshot* s) {
+  clear_err();
+  if (!W || !s) return fail(RPHYS_ERR_NULL, "rphys_ext_snapshot_restore_exact: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  World& w = W->w;
+  if (s->s.poses.size() != w.num_bodies())
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_snapshot_restore_exact: bodies were added since the snapshot");
+  w.tick = s->s.tick;
+  for (uint32_t i = 0; i < w.num_bodies(); ++i) {
+    w.pos[i] = s->s.poses[i].pos;
+    w.rot[i] = s->s.poses[i].rot;
+    w.lin[i] = s->s.lin[i];
+    w.ang[i] = s->s.ang[i];
   }
   w.restore_carried_state(s->s.carried);
   return RPHYS_OK;

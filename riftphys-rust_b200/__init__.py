@@ -91,6 +91,29 @@ class BodyDescEx(Structure):
                 ("sleep_allowed", c_uint32)]
 
 
+def desc_array(pos, rot, dims, shape, density, body_type, material=0, sleep_allowed=1, lin=None, ang=None):
+    """A numpy array laid out as RPhysBodyDescEx[n] (84 bytes each), built column-wise: for scenes
+    of millions of bodies, where one ctypes object per body is too slow."""
+    import numpy as np
+    n = len(pos)
+    a = np.zeros((n, 21), dtype=np.float32)
+    a[:, 0:3] = pos
+    a[:, 3:7] = rot
+    if lin is not None:
+        a[:, 7:10] = lin
+    if ang is not None:
+        a[:, 10:13] = ang
+    u = a.view(np.uint32)
+    u[:, 13] = shape
+    a[:, 14:17] = dims
+    a[:, 17] = density
+    u[:, 18] = body_type
+    u[:, 19] = material
+    u[:, 20] = sleep_allowed
+    assert a.strides[0] == ctypes.sizeof(BodyDescEx)
+    return a
+
+
 class PairProps(Structure):
     _fields_ = [("mu_s", c_float), ("mu_k", c_float), ("restitution", c_float), ("stribeck_v", c_float)]
 
@@ -142,6 +165,11 @@ ABI = [
     ("rphys_world_snapshot_restore", c_uint32, [c_void_p, c_void_p]),
     ("rphys_world_snapshot_free", None, [c_void_p]),
     ("rphys_ext_add_bodies", c_uint32, [c_void_p, POINTER(BodyDescEx), c_uint32, POINTER(c_uint32)]),
+    ("rphys_ext_snapshot_restore_exact", c_uint32, [c_void_p, c_void_p]),
+    ("rphys_ext_batch_add_world", c_uint32, [c_void_p, c_void_p, c_uint32, POINTER(c_uint32), POINTER(c_uint32)]),
+    ("rphys_ext_batch_num_worlds", c_uint32, [c_void_p, POINTER(c_uint32)]),
+    ("rphys_ext_batch_world_range", c_uint32, [c_void_p, c_uint32, POINTER(c_uint32), POINTER(c_uint32)]),
+    ("rphys_ext_batch_get_hashes", c_uint32, [c_void_p, c_uint32, c_uint32, c_void_p]),
     ("rphys_ext_set_pair_props", c_uint32, [c_void_p, c_uint32, c_uint32, POINTER(PairProps)]),
     ("rphys_ext_set_solver_iterations", c_uint32, [c_void_p, c_uint32, c_uint32]),
     ("rphys_ext_set_gravity", c_uint32, [c_void_p, Vec3]),
@@ -307,6 +335,9 @@ class World:
     def restore(self, snap):
         self.c("rphys_world_snapshot_restore", c_void_p(snap))
 
+    def restore_exact(self, snap):
+        self.c("rphys_ext_snapshot_restore_exact", c_void_p(snap))
+
     def free_snapshot(self, snap):
         self.lib.dll.rphys_world_snapshot_free(c_void_p(snap))
 
@@ -326,6 +357,40 @@ class World:
         out = c_uint32(0)
         self.c("rphys_ext_add_bodies", arr, len(descs), byref(out))
         return out.value
+
+    def add_bodies_array(self, desc):
+        """add_bodies from a desc_array; returns the first body id."""
+        out = c_uint32(0)
+        self.c("rphys_ext_add_bodies", ctypes.cast(c_void_p(desc.ctypes.data), POINTER(BodyDescEx)), len(desc), byref(out))
+        return out.value
+
+    def add_world(self, desc):
+        """Appends one world of a batch (desc: a desc_array or a list of BodyDescEx); returns
+        (world index, first body id)."""
+        if isinstance(desc, list):
+            desc = (BodyDescEx * len(desc))(*desc)
+            n, ptr = len(desc), ctypes.cast(desc, c_void_p)
+        else:
+            n, ptr = len(desc), c_void_p(desc.ctypes.data)
+        wi, first = c_uint32(0), c_uint32(0)
+        self.c("rphys_ext_batch_add_world", ptr, n, byref(wi), byref(first))
+        return wi.value, first.value
+
+    def num_worlds(self):
+        n = c_uint32(0)
+        self.c("rphys_ext_batch_num_worlds", byref(n))
+        return n.value
+
+    def world_range(self, k):
+        f, n = c_uint32(0), c_uint32(0)
+        self.c("rphys_ext_batch_world_range", k, byref(f), byref(n))
+        return f.value, n.value
+
+    def world_hashes(self, first=0, count=None):
+        count = self.num_worlds() - first if count is None else count
+        out = (Hash32 * count)()
+        self.c("rphys_ext_batch_get_hashes", first, count, ctypes.cast(out, c_void_p))
+        return [bytes(h.bytes) for h in out]
 
     def set_pair_props(self, a, b, mu_s, mu_k, restitution, stribeck_v):
         p = PairProps(mu_s, mu_k, restitution, stribeck_v)

@@ -443,6 +443,17 @@ RPhysResult rphys_world_snapshot_restore(RPhysWorld* W, const RPhysWorldSnapshot
     return (RPhysResult)RPHYS_OK;
   });
 }
+RPhysResult rphys_ext_snapshot_restore_exact(RPhysWorld* W, const RPhysWorldSnapshot* s) {
+  clear_err();
+  if (!W || !s) return fail(RPHYS_ERR_NULL, "rphys_ext_snapshot_restore_exact: null arg");
+  return guard("rphys_ext_snapshot_restore_exact", [&]() {
+    LOCK;
+    if (s->s->nb != W->w->num_bodies())
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_snapshot_restore_exact: bodies were added since the snapshot");
+    W->w->snapshot_restore_exact(s->s);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
 void rphys_world_snapshot_free(RPhysWorldSnapshot* s) {
   if (!s) return;
   try { WorldGpu::snapshot_free(s->s); } catch (...) {}
@@ -450,27 +461,35 @@ void rphys_world_snapshot_free(RPhysWorldSnapshot* s) {
 }
 
 // ---------------------------------------------------------------- extensions
-RPhysResult rphys_ext_add_bodies(RPhysWorld* W, const RPhysBodyDescEx* d, uint32_t n, uint32_t* out_first) {
-  clear_err();
-  if (out_first) *out_first = 0;
-  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_bodies: null arg");
+// Validates and adds n bodies (one collider each) in one upload; shared by rphys_ext_add_bodies
+// and rphys_ext_batch_add_world (which first opens a new world).
+static RPhysResult add_bodies_impl(RPhysWorld* W, const RPhysBodyDescEx* d, uint32_t n, uint32_t* out_first,
+                                   const char* ctx, bool new_world, uint32_t* out_world) {
+  const std::string c = ctx;
   for (uint32_t i = 0; i < n; ++i) {
     const RPhysBodyDescEx& e = d[i];
-    if (!fin_iso(e.pose) || !fin_vel(e.vel)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: pose/vel contains NaN/Inf");
+    if (!fin_iso(e.pose) || !fin_vel(e.vel)) return fail(RPHYS_ERR_BAD_ARG, c + ": pose/vel contains NaN/Inf");
     if (e.shape > 2 || e.body_type > 1 || !rp::material_known(e.material_id))
-      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: bad shape/body_type/material");
+      return fail(RPHYS_ERR_BAD_ARG, c + ": bad shape/body_type/material");
     int nd = e.shape == 0 ? 1 : (e.shape == 1 ? 3 : 1);
     for (int k = 0; k < nd; ++k)
-      if (!(std::isfinite(e.dims[k]) && e.dims[k] > 0)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: dims must be finite and > 0");
+      if (!(std::isfinite(e.dims[k]) && e.dims[k] > 0)) return fail(RPHYS_ERR_BAD_ARG, c + ": dims must be finite and > 0");
     if (e.shape == 2 && !(std::isfinite(e.dims[1]) && e.dims[1] >= 0))
-      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: half_height must be finite and >= 0");
+      return fail(RPHYS_ERR_BAD_ARG, c + ": half_height must be finite and >= 0");
     if (e.body_type == 1 && !(std::isfinite(e.density) && e.density > 0))
-      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_bodies: density must be finite and > 0");
+      return fail(RPHYS_ERR_BAD_ARG, c + ": density must be finite and > 0");
   }
-  return guard("rphys_ext_add_bodies", [&]() {
+  return guard(ctx, [&]() {
     LOCK;
-    if ((uint64_t)W->bodies_created + n > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_add_bodies: body capacity exceeded");
-    if ((uint64_t)W->colliders_created + n > W->max_colliders) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_add_bodies: collider capacity exceeded");
+    if ((uint64_t)W->bodies_created + n > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, c + ": body capacity exceeded");
+    if ((uint64_t)W->colliders_created + n > W->max_colliders) return fail(RPHYS_ERR_CAPACITY, c + ": collider capacity exceeded");
+    if (new_world) {
+      if (n == 0) return fail(RPHYS_ERR_BAD_ARG, c + ": a world needs at least one body");
+      if (!W->w->batched() && W->w->num_bodies() > 0)
+        return fail(RPHYS_ERR_BAD_ARG, c + ": a batch starts on an empty world");
+      W->w->begin_world();
+      if (out_world) *out_world = W->w->num_worlds() - 1;
+    }
     if (n == 0) return (RPhysResult)RPHYS_OK;
     std::vector<float> p7(7 * (size_t)n), v6(6 * (size_t)n), dims(3 * (size_t)n), im(n), in3(3 * (size_t)n);
     std::vector<uint32_t> sh(n), mat(n);
@@ -491,6 +510,57 @@ RPhysResult rphys_ext_add_bodies(RPhysWorld* W, const RPhysBodyDescEx* d, uint32
     W->bodies_created += n;
     W->colliders_created += n;
     *out_first = first + 1;
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_add_bodies(RPhysWorld* W, const RPhysBodyDescEx* d, uint32_t n, uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_bodies: null arg");
+  return add_bodies_impl(W, d, n, out_first, "rphys_ext_add_bodies", false, nullptr);
+}
+RPhysResult rphys_ext_batch_add_world(RPhysWorld* W, const RPhysBodyDescEx* d, uint32_t n, uint32_t* out_world,
+                                      uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (out_world) *out_world = 0;
+  if (!W || !d || !out_first || !out_world) return fail(RPHYS_ERR_NULL, "rphys_ext_batch_add_world: null arg");
+  return add_bodies_impl(W, d, n, out_first, "rphys_ext_batch_add_world", true, out_world);
+}
+RPhysResult rphys_ext_batch_num_worlds(const RPhysWorld* Wc, uint32_t* out) {
+  clear_err();
+  if (!Wc || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_batch_num_worlds: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  LOCK;
+  *out = W->w->batched() ? W->w->num_worlds() : 1u;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_batch_world_range(const RPhysWorld* Wc, uint32_t world, uint32_t* out_first, uint32_t* out_count) {
+  clear_err();
+  if (!Wc || !out_first || !out_count) return fail(RPHYS_ERR_NULL, "rphys_ext_batch_world_range: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  LOCK;
+  *out_first = 0; *out_count = 0;
+  uint32_t nw = W->w->batched() ? W->w->num_worlds() : 1u;
+  if (world >= nw) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_batch_world_range: no such world");
+  uint32_t b0 = W->w->batched() ? W->w->h_wb_start_[world] : 0u;
+  uint32_t b1 = (W->w->batched() && world + 1 < nw) ? W->w->h_wb_start_[world + 1] : W->w->num_bodies();
+  *out_first = b0 + 1;
+  *out_count = b1 - b0;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_batch_get_hashes(const RPhysWorld* Wc, uint32_t first, uint32_t count, RPhysHash32* out) {
+  clear_err();
+  if (!Wc || (!out && count)) return fail(RPHYS_ERR_NULL, "rphys_ext_batch_get_hashes: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_batch_get_hashes", [&]() {
+    LOCK;
+    uint32_t nw = W->w->batched() ? W->w->num_worlds() : 1u;
+    if ((uint64_t)first + count > nw) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_batch_get_hashes: world range out of bounds");
+    for (uint32_t k = 0; k < count; ++k) {
+      if (W->w->batched()) W->w->step_hash_world(first + k, out[k].bytes);
+      else W->w->step_hash(out[k].bytes);
+    }
     return (RPhysResult)RPHYS_OK;
   });
 }

@@ -136,7 +136,7 @@ __global__ void k_h_warm_flags(uint32_t n, const uint4* __restrict__ k, uint32_t
 // Entry e of group g sits after g+1 group headers (20 bytes) and e entries (28 bytes).
 __global__ void k_h_warm(uint32_t n, const uint4* __restrict__ k, const float4* __restrict__ wa,
                          const float4* __restrict__ wb, const uint32_t* __restrict__ flag, const uint32_t* __restrict__ gs,
-                         uint8_t* out) {
+                         uint8_t* out, uint32_t base = 0) {
   uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n) return;
   uint32_t g = gs[e] + flag[e] - 1;
@@ -145,7 +145,9 @@ __global__ void k_h_warm(uint32_t n, const uint4* __restrict__ k, const float4* 
     while (e + cnt < n && !flag[e + cnt]) cnt++;
     uint8_t* h = out + 20 * (size_t)g + 28 * (size_t)e;
     uint4 key = k[e];
-    put32(h, key.x); put32(h + 4, key.y); put32(h + 8, key.z); put32(h + 12, key.w); put32(h + 16, cnt);
+    // base: the first body of the hashed world (batched worlds hash with their own 0-based ids)
+    uint32_t kb = key.y == 0xFFFFFFFFu ? key.y : key.y - base;
+    put32(h, key.x - base); put32(h + 4, kb); put32(h + 8, key.z); put32(h + 12, key.w); put32(h + 16, cnt);
   }
   uint8_t* p = out + 20 * (size_t)(g + 1) + 28 * (size_t)e;
   float4 a = wa[e], b = wb[e];
@@ -209,6 +211,87 @@ void WorldGpu::step_hash(uint8_t out32[32]) {
   // the three zero-length maps are already zero bytes
   uint32_t nt = cap > nb_ ? cap : nb_;
   k_h_tail<<<(nt + T) / T, T, 0, st>>>(nb_, cap, last_lin.p, awake.p, sleep_ticks.p, S.hbuf.p + off_tail); RP_COUNT_LAUNCH(1);
+  S.hcv.ensure(16 * (size_t)nch + 16);
+  uint32_t* root = S.hcv.p;
+  uint32_t* a = S.hcv.p + 8;
+  uint32_t* b = S.hcv.p + 8 + 8 * (size_t)nch;
+  k_b3_chunks<<<(nch + 127) / 128, 128, 0, st>>>(S.hbuf.p, len, nch, a, root); RP_COUNT_LAUNCH(1);
+  uint32_t n = nch;
+  while (n > 1) {
+    uint32_t n_out = (n + 1) / 2;
+    k_b3_parents<<<(n_out + 127) / 128, 128, 0, st>>>(n, a, b, root); RP_COUNT_LAUNCH(1);
+    std::swap(a, b);
+    n = n_out;
+  }
+  uint32_t r[8];
+  RP_CUDA(cudaMemcpyAsync(r, root, 32, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < 8; ++i)
+    for (int k = 0; k < 4; ++k) out32[4 * i + k] = (uint8_t)(r[i] >> (8 * k));
+}
+
+// ------------------------------------------------------------------ one world of a batch
+// The digest a World holding exactly world w's bodies would compute (capacity = its body count):
+// bodies [b0, b1) with 0-based indices, the warm entries whose first body is in that range (one
+// contiguous run of the sorted cache) with body ids made 0-based, and that range's carried state.
+__global__ void k_warm_range(uint32_t n, const uint4* __restrict__ k, uint32_t b0, uint32_t b1, uint32_t* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (k[m].x < b0) lo = m + 1; else hi = m; }
+  uint32_t a = lo;
+  hi = n;
+  while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (k[m].x < b1) lo = m + 1; else hi = m; }
+  out[0] = a;
+  out[1] = lo;
+}
+void WorldGpu::step_hash_world(uint32_t w, uint8_t out32[32]) {
+  Scratch& S = *s_;
+  cudaStream_t st = stream_;
+  const int T = 256;
+  uint32_t b0 = h_wb_start_[w], b1 = w + 1 < h_wb_start_.size() ? h_wb_start_[w + 1] : nb_;
+  uint32_t nbw = b1 - b0, cap = nbw;
+  uint32_t lohi[2] = {0, 0};
+  S.counts.ensure(4);
+  if (n_warm) {
+    k_warm_range<<<1, 1, 0, st>>>(n_warm, warm_key.p, b0, b1, S.counts.p); RP_COUNT_LAUNCH(1);
+    RP_CUDA(cudaMemcpyAsync(lohi, S.counts.p, 8, cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaStreamSynchronize(st));
+  }
+  uint32_t wlo = lohi[0], nw = lohi[1] - lohi[0];
+  S.woff.ensure(nw + 1); S.wpos.ensure(nw + 1);
+  uint32_t nkeys = 0;
+  if (nw) {
+    k_h_warm_flags<<<(nw + T - 1) / T, T, 0, st>>>(nw, warm_key.p + wlo, S.woff.p); RP_COUNT_LAUNCH(1);
+    nkeys = exclusive_scan_total(S, S.woff.p, S.wpos.p, nw, st);
+  }
+  uint64_t off_bodies = 48;
+  uint64_t off_warm = off_bodies + 56ull * nbw;
+  uint64_t off_tail = off_warm + 8 + 20ull * nkeys + 28ull * nw + 24;
+  uint64_t len = off_tail + 8 + 12ull * nbw + 8 + cap + 8 + 2ull * cap;
+  uint32_t nch = (uint32_t)((len + 1023) / 1024);
+  S.hbuf.ensure((size_t)nch * 1024 + 64);
+  RP_CUDA(cudaMemsetAsync(S.hbuf.p, 0, (size_t)nch * 1024 + 64, st));
+  uint8_t head[48];
+  auto p64 = [&](uint8_t* p, uint64_t v) { for (int i = 0; i < 8; ++i) p[i] = (uint8_t)(v >> (8 * i)); };
+  p64(head, epoch_);
+  p64(head + 8, rng_);
+  static const uint8_t kEmpty[32] = {0xaf, 0x13, 0x49, 0xb9, 0xf5, 0xf9, 0xa1, 0xa6, 0xa0, 0x40, 0x4d,
+                                     0xea, 0x36, 0xdc, 0xc9, 0x49, 0x9b, 0xcb, 0x25, 0xc9, 0xad, 0xc1,
+                                     0x12, 0xb7, 0xcc, 0x9a, 0x93, 0xca, 0xe4, 0x1f, 0x32, 0x62};
+  std::memcpy(head + 16, kEmpty, 32);
+  uint8_t wcount[8];
+  p64(wcount, nkeys);
+  RP_CUDA(cudaMemcpyAsync(S.hbuf.p, head, 48, cudaMemcpyHostToDevice, st));
+  if (nbw)
+    k_h_bodies<<<(nbw + T - 1) / T, T, 0, st>>>(nbw, pos.p + b0, rot.p + b0, lin.p + b0, ang.p + b0, S.hbuf.p + off_bodies);
+  if (nbw) RP_COUNT_LAUNCH(1);
+  RP_CUDA(cudaMemcpyAsync(S.hbuf.p + off_warm, wcount, 8, cudaMemcpyHostToDevice, st));
+  if (nw)
+    k_h_warm<<<(nw + T - 1) / T, T, 0, st>>>(nw, warm_key.p + wlo, warm_a.p + wlo, warm_b.p + wlo, S.woff.p, S.wpos.p,
+                                              S.hbuf.p + off_warm + 8, b0);
+  if (nw) RP_COUNT_LAUNCH(1);
+  k_h_tail<<<(nbw + T) / T, T, 0, st>>>(nbw, cap, last_lin.p + b0, awake.p + b0, sleep_ticks.p + b0, S.hbuf.p + off_tail);
+  RP_COUNT_LAUNCH(1);
   S.hcv.ensure(16 * (size_t)nch + 16);
   uint32_t* root = S.hcv.p;
   uint32_t* a = S.hcv.p + 8;

@@ -96,19 +96,34 @@ __global__ void k_gather_minx(int n, const uint32_t* __restrict__ order, const f
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) minx[k] = smin[order[k]].x;
 }
+// Batched worlds: the sort key puts the world above min.x, so each world's colliders are one run
+// of the sorted order and the sweep stops at the end of its run.
+__global__ void k_sap_keys_world(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ smin,
+                                 const uint32_t* __restrict__ col_world, unsigned long long* keys) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) { uint32_t c = ids[k]; keys[k] = ((unsigned long long)col_world[c] << 32) | sortable(smin[c].x); }
+}
+__global__ void k_gather_world(int n, const uint32_t* __restrict__ order, const uint32_t* __restrict__ col_world,
+                               uint32_t* wsorted) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) wsorted[k] = col_world[order[k]];
+}
 // Sweep along x over the sorted in-grid colliders: every overlapping pair once, counted by the
 // earlier of the two in sort order. The set equals the grid's (broadphase.rs:49-81): two
 // finite AABBs that overlap share the cell of any point of their intersection.
 template <bool EMIT>
 __global__ void k_sap_sweep(int n, const uint32_t* __restrict__ order, const float* __restrict__ minx,
                             const float4* __restrict__ smin, const float4* __restrict__ smax,
-                            uint32_t* cnt, const uint32_t* __restrict__ off, unsigned long long* out) {
+                            uint32_t* cnt, const uint32_t* __restrict__ off, unsigned long long* out,
+                            const uint32_t* __restrict__ wsorted = nullptr) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   uint32_t i = order[p];
   float4 imn = smin[i], imx = smax[i];
   uint32_t c = 0, o = EMIT ? off[p] : 0;
+  const uint32_t wp = wsorted ? wsorted[p] : 0u;
   for (int q = p + 1; q < n; ++q) {
+    if (wsorted && wsorted[q] != wp) break;  // the next world's run
     if (minx[q] > imx.x) break;
     uint32_t j = order[q];
     if (overlaps4(imn, imx, smin[j], smax[j])) {
@@ -122,15 +137,29 @@ __global__ void k_sap_sweep(int n, const uint32_t* __restrict__ order, const flo
   if (!EMIT) cnt[p] = c;
 }
 // Oversized colliders against every collider (broadphase.rs:83-92), one thread per collider.
+// Batched worlds: only the oversized colliders of c's own world (a contiguous run of the
+// collider-ordered list, found by binary search on the world's collider range).
+__device__ __forceinline__ int lower_bound_u32(const uint32_t* a, int n, uint32_t v) {
+  int lo = 0, hi = n;
+  while (lo < hi) { int m = (lo + hi) >> 1; if (a[m] < v) lo = m + 1; else hi = m; }
+  return lo;
+}
 template <bool EMIT>
 __global__ void k_oversized(int ncol, int nover, const uint32_t* __restrict__ over, const float4* __restrict__ smin,
                             const float4* __restrict__ smax, uint32_t* cnt, const uint32_t* __restrict__ off,
-                            unsigned long long* out) {
+                            unsigned long long* out, const uint32_t* __restrict__ col_world = nullptr,
+                            const uint32_t* __restrict__ world_col_start = nullptr) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncol) return;
   float4 cmn = smin[c], cmx = smax[c];
   uint32_t k = 0, o = EMIT ? off[c] : 0;
-  for (int t = 0; t < nover; ++t) {
+  int t0 = 0, t1 = nover;
+  if (col_world) {
+    uint32_t w = col_world[c];
+    t0 = lower_bound_u32(over, nover, world_col_start[w]);
+    t1 = lower_bound_u32(over, nover, world_col_start[w + 1]);
+  }
+  for (int t = t0; t < t1; ++t) {
     uint32_t b = over[t];
     if (b == (uint32_t)c) continue;
     if (overlaps4(smin[b], smax[b], cmn, cmx)) {
@@ -429,27 +458,42 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   S.sap_cnt.ensure(n_sap + 1); S.sap_off.ensure(n_sap + 1);
   S.ov_cnt.ensure(ncol + 1); S.ov_off.ensure(ncol + 1);
   uint32_t n_sap_pairs = 0, n_ov_pairs = 0;
+  const bool batched = W.batched();
+  const uint32_t* wsorted = nullptr;
   if (n_sap > 0) {
-    k_sap_keys<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.sap_key.p); RP_COUNT_LAUNCH(1);
-    sort_pairs_u32(S, S.sap_key.p, S.sap_key2.p, S.sap_ids.p, S.sap_ord.p, n_sap, 0, 32, st);
+    if (batched) {
+      uint32_t nw = W.num_worlds();
+      int wbits = 1;
+      while ((1u << wbits) < nw && wbits < 31) wbits++;
+      S.sap_key64.ensure(n_sap + 1); S.sap_key64b.ensure(n_sap + 1); S.sap_w.ensure(n_sap + 1);
+      k_sap_keys_world<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, W.col_world.p, S.sap_key64.p); RP_COUNT_LAUNCH(1);
+      sort_pairs_u64(S, S.sap_key64.p, S.sap_key64b.p, S.sap_ids.p, S.sap_ord.p, n_sap, 0, 32 + wbits, st);
+      k_gather_world<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, W.col_world.p, S.sap_w.p); RP_COUNT_LAUNCH(1);
+      wsorted = S.sap_w.p;
+    } else {
+      k_sap_keys<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.sap_key.p); RP_COUNT_LAUNCH(1);
+      sort_pairs_u32(S, S.sap_key.p, S.sap_key2.p, S.sap_ids.p, S.sap_ord.p, n_sap, 0, 32, st);
+    }
     k_gather_minx<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.smin.p, S.minx.p); RP_COUNT_LAUNCH(1);
     k_sap_sweep<false><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, S.sap_cnt.p,
-                                                           nullptr, nullptr); RP_COUNT_LAUNCH(1);
+                                                           nullptr, nullptr, wsorted); RP_COUNT_LAUNCH(1);
     n_sap_pairs = exclusive_scan_total(S, S.sap_cnt.p, S.sap_off.p, n_sap, st);
   }
   if (n_over > 0 && ncol > 0) {
     k_oversized<false><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, S.ov_cnt.p,
-                                                          nullptr, nullptr); RP_COUNT_LAUNCH(1);
+                                                          nullptr, nullptr, batched ? W.col_world.p : nullptr,
+                                                          batched ? W.world_col_start.p : nullptr); RP_COUNT_LAUNCH(1);
     n_ov_pairs = exclusive_scan_total(S, S.ov_cnt.p, S.ov_off.p, ncol, st);
   }
   uint32_t n_raw = n_sap_pairs + n_ov_pairs;
   S.pairs.ensure(n_raw + 1); S.pairs2.ensure(n_raw + 1); S.flag8.ensure(n_raw + 1);
   if (n_sap_pairs > 0)
     k_sap_sweep<true><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, nullptr,
-                                                          S.sap_off.p, S.pairs2.p); RP_COUNT_LAUNCH(1);
+                                                          S.sap_off.p, S.pairs2.p, wsorted); RP_COUNT_LAUNCH(1);
   if (n_ov_pairs > 0)
     k_oversized<true><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, nullptr,
-                                                         S.ov_off.p, S.pairs2.p + n_sap_pairs); RP_COUNT_LAUNCH(1);
+                                                         S.ov_off.p, S.pairs2.p + n_sap_pairs, batched ? W.col_world.p : nullptr,
+                                                         batched ? W.world_col_start.p : nullptr); RP_COUNT_LAUNCH(1);
   uint32_t np = 0;
   if (n_raw > 0) {
     sort_keys_u64(S, S.pairs2.p, S.pairs.p, n_raw, st);  // -> S.pairs

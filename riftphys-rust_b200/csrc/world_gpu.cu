@@ -260,6 +260,7 @@ uint32_t WorldGpu::add_body(const float pose[7], const float vel[6], uint32_t sh
                                    inv_mass.p, inv_I.p, dyn.p, awake.p, sleep_allowed.p, sleep_ticks.p, alive_d.p, last); RP_COUNT_LAUNCH(1);
   h_alive_.push_back(1);
   uint32_t c = ncol_++;
+  if (batch_) worlds_dirty_ = true;
   h_col_body_.push_back(id); h_col_kind_.push_back(shape); h_col_mat_.push_back(mat);
   float dd[4] = {dims[0], shape == SH_SPHERE ? 0.0f : dims[1], shape == SH_BOX ? dims[2] : 0.0f, 0.0f};
   h_col_dims_.insert(h_col_dims_.end(), dd, dd + 4);
@@ -313,6 +314,31 @@ void WorldGpu::add_bodies_bulk(uint32_t n, const float* pose7, const float* vel6
   }
   nb_ += n;
   ncol_ += n;
+  if (batch_) worlds_dirty_ = true;
+}
+
+void WorldGpu::begin_world() {
+  batch_ = true;
+  h_wb_start_.push_back(nb_);
+  h_wc_start_.push_back(ncol_);
+  worlds_dirty_ = true;
+}
+void WorldGpu::upload_worlds() {
+  if (!batch_ || !worlds_dirty_) return;
+  uint32_t nw = num_worlds();
+  std::vector<uint32_t> cw(ncol_ ? ncol_ : 1, 0), ws(nw + 1);
+  for (uint32_t w = 0; w < nw; ++w) {
+    uint32_t c0 = h_wc_start_[w], c1 = w + 1 < nw ? h_wc_start_[w + 1] : ncol_;
+    for (uint32_t c = c0; c < c1; ++c) cw[c] = w;
+    ws[w] = c0;
+  }
+  ws[nw] = ncol_;
+  col_world.ensure(cw.size());
+  world_col_start.ensure(nw + 1);
+  RP_CUDA(cudaMemcpyAsync(col_world.p, cw.data(), 4 * cw.size(), cudaMemcpyHostToDevice, stream_));
+  RP_CUDA(cudaMemcpyAsync(world_col_start.p, ws.data(), 4 * ws.size(), cudaMemcpyHostToDevice, stream_));
+  RP_CUDA(cudaStreamSynchronize(stream_));
+  worlds_dirty_ = false;
 }
 
 void WorldGpu::filter_warm(int mode, uint32_t body) {
@@ -422,6 +448,7 @@ void WorldGpu::clear_heightfield() { has_hf_ = false; }
 
 // ------------------------------------------------------------------ the tick
 void WorldGpu::step(float dt) {
+  upload_worlds();
   AllocStreamScope alloc_scope(stream_);
   tick_ += 1;
   RP_CUDA(cudaMemsetAsync(d_stats.p, 0, STAT_COUNT * 4, stream_));
@@ -528,6 +555,26 @@ SnapshotGpu* WorldGpu::snapshot_create() {  // lib.rs:1707-1752 + carried_state 
   cp(s->wb.p, warm_b.p, 16 * (size_t)n_warm);
   RP_CUDA(cudaStreamSynchronize(stream_));
   return s;
+}
+// Every stored bit back (a World clone, not the FFI's pose injection): for rollback that must
+// replay bit for bit. The body set must be the one the snapshot saw.
+void WorldGpu::snapshot_restore_exact(const SnapshotGpu* s) {
+  if (s->nb != nb_) throw std::invalid_argument("exact restore needs the body set of the snapshot");
+  tick_ = s->tick;
+  auto cp = [&](void* d, const void* src, size_t bytes) {
+    if (bytes) RP_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, stream_));
+  };
+  cp(pos.p, s->pos.p, 16 * (size_t)nb_); cp(rot.p, s->rot.p, 16 * (size_t)nb_);
+  cp(lin.p, s->lin.p, 16 * (size_t)nb_); cp(ang.p, s->ang.p, 16 * (size_t)nb_);
+  cp(last_lin.p, s->last_lin.p, 16 * (size_t)nb_);
+  uint32_t cap = cap_b_ > nb_ ? cap_b_ : nb_;
+  uint32_t ncap = s->cap < cap ? s->cap : cap;
+  cp(awake.p, s->awake.p, ncap); cp(sleep_ticks.p, s->ticks.p, 2 * (size_t)ncap);
+  warm_key.ensure(s->n_warm + 1); warm_a.ensure(s->n_warm + 1); warm_b.ensure(s->n_warm + 1);
+  cp(warm_key.p, s->wk.p, 16 * (size_t)s->n_warm); cp(warm_a.p, s->wa.p, 16 * (size_t)s->n_warm);
+  cp(warm_b.p, s->wb.p, 16 * (size_t)s->n_warm);
+  n_warm = s->n_warm;
+  RP_CUDA(cudaStreamSynchronize(stream_));
 }
 void WorldGpu::snapshot_restore(const SnapshotGpu* s) {  // lib.rs:1754-1793 + restore_carried_state
   tick_ = s->tick;

@@ -87,6 +87,18 @@ class WorldGpu {
   // nothing. Throws std::length_error when the world does not fit that array.
   void step_hash_noalloc(uint8_t out[32]);
 
+  // ---- batched worlds: independent worlds in contiguous body / collider ranges of one device
+  // world. Bodies of different worlds never pair in the broadphase; every later stage works per
+  // island already, so nothing else couples them.
+  void begin_world();                                   // bodies added next form a new world
+  uint32_t num_worlds() const { return (uint32_t)h_wb_start_.size(); }
+  bool batched() const { return batch_; }
+  void step_hash_world(uint32_t w, uint8_t out[32]);    // that world's own digest
+  std::vector<uint32_t> h_wb_start_, h_wc_start_;       // first body / collider of each world
+  bool batch_ = false, worlds_dirty_ = false;
+  DBuf<uint32_t> col_world, world_col_start;           // per collider; per world (+ end)
+  void upload_worlds();
+
   // ---- inspection
   const StepStatsHost& stats();
   void get_pairs(std::vector<uint64_t>& out);
@@ -97,6 +109,7 @@ class WorldGpu {
   // ---- rollback
   SnapshotGpu* snapshot_create();
   void snapshot_restore(const SnapshotGpu* s);
+  void snapshot_restore_exact(const SnapshotGpu* s);  // every stored bit (rollback replay)
   static void snapshot_free(SnapshotGpu* s);
 
   cudaStream_t stream() const { return stream_; }

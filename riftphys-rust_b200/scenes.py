@@ -7,6 +7,10 @@ f32 inputs on every machine; the scenes are built through the C ABI of whichever
 box_drop      1,000 boxes (half-extent 0.5 m, 1 kg, mu 0.5, e 0) on a 10x10x10 grid at 1.1 m pitch,
               jitter U[-0.05, 0.05] m, yaw U[0, 2 pi), bottom layer 1 m above a static 50x0.5x50 ground
               box, dt 1/60, 8 velocity and 8 position iterations.
+batch         independent worlds for one batched launch: body counts log-uniform in [n_min, n_max],
+              alternately a square box pyramid (brick half-extent U[0.25, 0.75] m per world) and a
+              random pile (half-extents U[0.25, 0.75] m per box, random yaw, dropped from a grid), each
+              on its own static 50x0.5x50 ground box; density 1000, dt 1/60, 16 iterations.
 terrain       bodies (40% spheres r U[0.2,0.6], 30% capsules r U[0.15,0.4] hh U[0.3,0.8], 30% boxes
               he U[0.2,0.7], density 1000) at uniform positions in a square of side `area` x [0, 60] m,
               lifted above the terrain, velocities N(0,1) per axis, falling onto a heightfield
@@ -134,3 +138,47 @@ def terrain(rp, w, n_bodies=100_000, hf_n=512, area=400.0, seed=2, iterations=(2
         descs.append(rp.BodyDescEx(rp.iso(x, y, z, q=q), rp.vel(v), shape, dims, 1000.0, rp.RPHYS_BODY_DYNAMIC, 0, 1))
     w.add_bodies(descs)
     return 1.0 / 60.0, len(descs)
+
+
+def batch_world_descs(rp, k, seed=3, n_min=16, n_max=4096):
+    """World k of the batched-worlds scene as an RPhysBodyDescEx array (ground box first)."""
+    rng = np.random.Generator(np.random.PCG64([seed, k]))
+    n = int(math.floor(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+    n = max(n_min, min(n, n_max))
+    pos = np.zeros((n + 1, 3)); rot = np.zeros((n + 1, 4)); rot[:, 3] = 1.0
+    dims = np.zeros((n + 1, 3)); btype = np.ones(n + 1, dtype=np.uint32); dens = np.full(n + 1, 1000.0)
+    pos[0] = (0.0, -0.5, 0.0); dims[0] = (50.0, 0.5, 50.0); btype[0] = 0; dens[0] = 0.0
+    if k % 2 == 0:
+        # square pyramid, filled bottom-up, bricks of one size per world
+        he = rng.uniform(0.25, 0.75)
+        b = 1
+        while sum(j * j for j in range(1, b + 1)) < n:
+            b += 1
+        pts = []
+        for layer in range(b):
+            m = b - layer
+            for iz in range(m):
+                for ix in range(m):
+                    pts.append(((ix - (m - 1) * 0.5) * 2.02 * he, he + layer * (2.0 * he + 0.001),
+                                (iz - (m - 1) * 0.5) * 2.02 * he))
+        pos[1:] = np.array(pts[:n])
+        dims[1:] = he
+    else:
+        # random pile: a grid of falling boxes, random sizes and yaw
+        side = max(2, int(math.ceil(n ** (1.0 / 3.0))))
+        idx = np.arange(n)
+        ix, iz, iy = idx % side, (idx // side) % side, idx // (side * side)
+        pos[1:, 0] = (ix - (side - 1) * 0.5) * 1.6 + rng.uniform(-0.05, 0.05, n)
+        pos[1:, 1] = 1.0 + iy * 1.6 + rng.uniform(-0.05, 0.05, n)
+        pos[1:, 2] = (iz - (side - 1) * 0.5) * 1.6 + rng.uniform(-0.05, 0.05, n)
+        dims[1:] = rng.uniform(0.25, 0.75, (n, 3))
+        th = rng.uniform(0.0, 2.0 * math.pi, n)
+        rot[1:, 1] = np.sin(th * 0.5); rot[1:, 3] = np.cos(th * 0.5)
+    return rp.desc_array(pos, rot, dims, rp.SHAPE_BOX, dens, btype)
+
+
+def batch_setup(w, iterations=(16, 16)):
+    """Shared settings of the batched-worlds scene (also applied to each oracle world)."""
+    w.set_pair_props(0, 0, 0.5, 0.5, 0.0, 0.08)
+    w.set_iterations(*iterations)
+    return 1.0 / 60.0

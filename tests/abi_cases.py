@@ -8,7 +8,7 @@ from ctypes import byref, c_char_p, c_float, c_uint32, c_uint64
 
 import numpy as np
 
-from conftest import rp
+from conftest import rp, scenes
 
 DT = 1.0 / 60.0
 
@@ -246,6 +246,20 @@ def case_rollback_restores_exact_hash(lib):
     w.restore(snap)
     assert w.hash() == h0
     w.free_snapshot(snap)
+
+
+def case_exact_restore_replays_rotated_bodies(lib):
+    # rphys_ext_snapshot_restore_exact (a World clone): a yawed box pile replays bit for bit
+    w = lib.world(64, 64)
+    dt, _ = scenes.box_drop(rp, w, n_side=3)
+    for _ in range(45):
+        w.step(dt)
+    snap = w.snapshot()
+    first = [w.step_hash(dt) for _ in range(20)]
+    w.restore_exact(snap)
+    again = [w.step_hash(dt) for _ in range(20)]
+    w.free_snapshot(snap)
+    assert first == again
 
 
 def case_teleport_drops_only_its_warm_entries(lib):

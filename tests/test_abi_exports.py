@@ -30,3 +30,20 @@ def test_product_library_exports_every_declared_symbol():
     assert not missing, missing
     bound = {n for n, _, _ in rp.ABI}
     assert declared() <= bound, sorted(declared() - bound)
+
+
+def test_desc_array_matches_struct_layout():
+    import ctypes
+    import numpy as np
+    a = rp.desc_array(np.array([[1.0, 2.0, 3.0]]), np.array([[0.0, 0.0, 0.0, 1.0]]), np.array([[0.5, 0.25, 0.75]]),
+                      rp.SHAPE_BOX, np.array([1000.0]), np.array([rp.RPHYS_BODY_DYNAMIC]), 4, 1)
+    d = rp.BodyDescEx(rp.iso(1.0, 2.0, 3.0), rp.vel(), rp.SHAPE_BOX, (0.5, 0.25, 0.75), 1000.0, rp.RPHYS_BODY_DYNAMIC, 4, 1)
+    assert bytes(a.tobytes()) == ctypes.string_at(ctypes.addressof(d), ctypes.sizeof(d))
+
+
+def test_batch_scene_is_deterministic():
+    import numpy as np
+    from conftest import scenes
+    a = scenes.batch_world_descs(rp, 3, n_min=16, n_max=300)
+    b = scenes.batch_world_descs(rp, 3, n_min=16, n_max=300)
+    assert np.array_equal(a, b) and 17 <= len(a) <= 301
