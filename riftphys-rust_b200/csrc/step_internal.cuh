@@ -169,6 +169,7 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> cls_cnt, cls_list;                                            // solve groups by class
   DBuf<unsigned long long> sap_key64, sap_key64b;                              // batched worlds: (world, min x)
   DBuf<uint32_t> sap_w;
+  DBuf<float4> big_x, big_j;                                                   // big-island row stream
   // solve groups (islands packed for one CTA each) and their shared-memory residents
   DBuf<uint32_t> g_small_rows, g_small_pre, g_big, g_big_pre, g_of_isl, g_key, g_key2, g_start, g_cnt, g_class,
       body_grp, gb_key, gb_key2, gb_list, gb_tmp, gb_start, gb_cnt, body_local;

@@ -828,13 +828,19 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
 // GROUP_ROWS rows (by the prefix sum of their row counts, so a group holds at most
 // 2 * GROUP_ROWS - 1 rows and twice that many bodies); bigger islands form a group alone.
 // Islands are independent, so any interleaving of their rows is a valid serial order: a group
-// is scheduled and solved exactly like one island. Classes: 3, a packed group, and 4 / 5, an
-// island whose rows and bodies fit in one block's shared memory, are solved by one warp with all
-// of it on chip; 0 / 1, a bigger island, by one CTA with its bodies in shared memory (128 / 512
-// threads); 2 by one warp over global memory.
+// is scheduled and solved exactly like one island. Classes: 3, a packed group, and 10..15, an
+// island whose rows and bodies fit in one block's shared memory, are solved by one block with all
+// of it on chip; 0, a bigger island, by one CTA with its body velocities on chip and its rows
+// streamed through a cp.async double buffer; 2, an island beyond that, by one warp over global
+// memory.
 #define GROUP_ROWS 32u
-#define SMALL_BODIES 640u   // shared-memory bodies of a 128-thread CTA (72 B each)
-#define BIG_BODIES 2800u    // shared-memory bodies of a 512-thread CTA
+// big islands (classes 20..22): bodies and level starts held in shared memory, rows per staged
+// chunk (= threads per CTA) -- sized per bucket so that smaller ones share an SM
+#define BIG_BUCKETS 3
+__constant__ uint32_t c_big_bodies[BIG_BUCKETS] = {1024u, 2048u, 4500u};
+__constant__ uint32_t c_big_levels[BIG_BUCKETS] = {2048u, 4096u, 4096u};
+static const uint32_t kBigBodies[BIG_BUCKETS] = {1024u, 2048u, 4500u};
+static const uint32_t kBigLevels[BIG_BUCKETS] = {2048u, 4096u, 4096u};
 #define WG_ROWS (2u * GROUP_ROWS)  // rows a packed group can hold
 #define WG_BODIES (2u * WG_ROWS)   // bodies those rows can move
 // single islands solved with everything on chip, by size bucket (class 10 + bucket): rows and
@@ -901,17 +907,22 @@ __global__ void k_body_local2(uint32_t n, const uint32_t* __restrict__ gkey, con
 // Class of every group, and the groups of each class other than 3 listed (in any order: groups
 // are independent, so the order they run in changes no result) for launches of exactly them.
 __global__ void k_group_class(uint32_t ng, uint32_t g_small, const uint32_t* __restrict__ gb_cnt,
-                              const uint32_t* __restrict__ g_cnt, uint32_t* cls, uint32_t* cls_cnt, uint32_t* cls_list,
-                              uint32_t* stats) {
+                              const uint32_t* __restrict__ g_cnt, const uint32_t* __restrict__ nlev, uint32_t* cls,
+                              uint32_t* cls_cnt, uint32_t* cls_list, uint32_t* stats) {
   uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ng) return;
   uint32_t nbg = gb_cnt[g], nr = g_cnt[g];
-  uint32_t c = g < g_small ? 3u : (nbg <= SMALL_BODIES ? 0u : (nbg <= BIG_BODIES ? 1u : 2u));
+  uint32_t c = 3u;
+  if (g >= g_small) {
+    c = 2u;
+    for (int b = BIG_BUCKETS - 1; b >= 0; --b)
+      if (nbg <= c_big_bodies[b] && nlev[g] <= c_big_levels[b]) c = 20u + (uint32_t)b;
+  }
   if (g >= g_small)
     for (int b = ISLAND_BUCKETS - 1; b >= 0; --b)
       if (nr <= c_island_rows[b] && nbg <= c_island_bodies[b]) c = 10u + (uint32_t)b;
   cls[g] = c;
-  if (c != 3u) cls_list[(size_t)c * ng + atomicAdd(&cls_cnt[c], 1u)] = g;  // classes 0..15
+  if (c != 3u) cls_list[(size_t)c * ng + atomicAdd(&cls_cnt[c], 1u)] = g;  // classes 0..31
   atomicAdd(&stats[c == 2u ? STAT_GROUPS_GLOBAL : STAT_GROUPS_SHARED], 1u);
   atomicMax(&stats[STAT_MAX_GROUP_ROWS], nr);
   atomicMax(&stats[STAT_MAX_GROUP_BODIES], nbg);
@@ -1061,17 +1072,17 @@ __device__ __forceinline__ void impulse_reg(f3& lin, f3& ang, float im, const m3
 __device__ __forceinline__ m3 load_iw(const float* q) {
   return mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
 }
-__device__ __forceinline__ void pgs_row_reg(const SBodies& B, const SRow& r, uint32_t s, float* jn_arr, float2* jt_arr,
-                                            float* dres) {
+// The row update on bodies whose velocities live in lin / ang (shared memory), with both bodies'
+// world inverse inertia and inverse mass passed in; jn / jt are the row's accumulators, d3
+// receives (new_jn - old_jn, friction deltas) for the residual.
+__device__ __forceinline__ void pgs_row_core(float4* lin, float4* ang, const SRow& r, const m3& qa, const m3& qb,
+                                             float ima, float imb, float& jn_acc, float2& jt_acc, float* d3) {
   const bool ha = r.la != 0xFFFFFFFFu, hb = !(r.flags & RF_TERRAIN) && r.lb != 0xFFFFFFFFu;
   const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
   float4 LA = make_float4(0, 0, 0, 0), AA = LA, LB = LA, AB = LA;
-  if (ha || ia) { LA = B.lin[r.la]; AA = B.ang[r.la]; }
-  if (hb || ib) { LB = B.lin[r.lb]; AB = B.ang[r.lb]; }
+  if (ha || ia) { LA = lin[r.la]; AA = ang[r.la]; }
+  if (hb || ib) { LB = lin[r.lb]; AB = ang[r.lb]; }
   f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
-  const m3 qa = load_iw(ia ? B.Iw + 9 * (size_t)r.la : B.Iw);  // loaded once for both impulses
-  const m3 qb = load_iw(ib ? B.Iw + 9 * (size_t)r.lb : B.Iw);
-  float ima = ia ? B.im[r.la] : 0.0f, imb = ib ? B.im[r.lb] : 0.0f;
   auto rel = [&]() {
     f3 va = ha ? la + cross(aa, r.ra) : r.vfix;
     f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : (hb ? lb + cross(ab, r.rb) : r.vfix);
@@ -1083,25 +1094,59 @@ __device__ __forceinline__ void pgs_row_reg(const SBodies& B, const SRow& r, uin
   };
   float v_rel_n = dot(rel(), r.n);
   float jn_raw = (r.bias - v_rel_n) * r.m_n;
-  float old_jn = jn_arr[s];
+  float old_jn = jn_acc;
   float new_jn = rmax(old_jn + jn_raw, 0.0f);
-  jn_arr[s] = new_jn;
+  jn_acc = new_jn;
   apply(r.n * (new_jn - old_jn));
   f3 vf = rel();
   float vt1 = dot(vf, r.t1), vt2 = dot(vf, r.t2);
   float slip = sqrtf(vt1 * vt1 + vt2 * vt2);
   float mu = mu_dynamic_s(r, slip);
-  float2 ot = jt_arr[s];
+  float2 ot = jt_acc;
   f3 old_t = mk3(ot.x, ot.y, 0.0f);
   f3 new_t = clamp_length_max(old_t - mk3(vt1 * r.m_t1, vt2 * r.m_t2, 0.0f), mu * new_jn);
-  jt_arr[s] = make_float2(new_t.x, new_t.y);
+  jt_acc = make_float2(new_t.x, new_t.y);
   f3 d = new_t - old_t;
   apply((r.t1 * d.x) + (r.t2 * d.y));
-  if (ia) { B.lin[r.la] = f4(la, LA.w); B.ang[r.la] = f4(aa, AA.w); }
-  if (ib) { B.lin[r.lb] = f4(lb, LB.w); B.ang[r.lb] = f4(ab, AB.w); }
-  dres[3 * s] = new_jn - old_jn;
-  dres[3 * s + 1] = d.x;
-  dres[3 * s + 2] = d.y;
+  if (ia) { lin[r.la] = f4(la, LA.w); ang[r.la] = f4(aa, AA.w); }
+  if (ib) { lin[r.lb] = f4(lb, LB.w); ang[r.lb] = f4(ab, AB.w); }
+  d3[0] = new_jn - old_jn;
+  d3[1] = d.x;
+  d3[2] = d.y;
+}
+// warm_apply_s on register copies (same operations, same order)
+__device__ __forceinline__ void warm_core(float4* lin, float4* ang, const SRow& r, const m3& qa, const m3& qb,
+                                          float ima, float imb, float4 ea, float4 eb, float& jn_acc, float2& jt_acc) {
+  const bool ha = r.la != 0xFFFFFFFFu, hb = !(r.flags & RF_TERRAIN) && r.lb != 0xFFFFFFFFu;
+  const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
+  float4 LA = make_float4(0, 0, 0, 0), AA = LA, LB = LA, AB = LA;
+  if (ha || ia) { LA = lin[r.la]; AA = ang[r.la]; }
+  if (hb || ib) { LB = lin[r.lb]; AB = ang[r.lb]; }
+  f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
+  float jn = ea.w;
+  f3 jt = xyz(eb);
+  jn_acc = jn;
+  f3 imp = r.n * jn;
+  f3 va = ha ? la + cross(aa, r.ra) : r.vfix;
+  f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : (hb ? lb + cross(ab, r.rb) : r.vfix);
+  f3 v = vb - va;
+  float a = dot(v, r.t1), b = dot(v, r.t2);
+  float mu = mu_dynamic_s(r, sqrtf(a * a + b * b));
+  f3 t = clamp_length_max(mk3(dot(jt, r.t1), dot(jt, r.t2), 0.0f), mu * jn);
+  jt_acc = make_float2(t.x, t.y);
+  imp = imp + ((r.t1 * t.x) + (r.t2 * t.y));
+  if (ia) { f3 nj = -imp; impulse_reg(la, aa, ima, qa, nj, cross(r.ra, nj)); }
+  if (ib) impulse_reg(lb, ab, imb, qb, imp, cross(r.rb, imp));
+  if (ia) { lin[r.la] = f4(la, LA.w); ang[r.la] = f4(aa, AA.w); }
+  if (ib) { lin[r.lb] = f4(lb, LB.w); ang[r.lb] = f4(ab, AB.w); }
+}
+__device__ __forceinline__ void pgs_row_reg(const SBodies& B, const SRow& r, uint32_t s, float* jn_arr, float2* jt_arr,
+                                            float* dres) {
+  const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
+  const m3 qa = load_iw(ia ? B.Iw + 9 * (size_t)r.la : B.Iw);  // loaded once for both impulses
+  const m3 qb = load_iw(ib ? B.Iw + 9 * (size_t)r.lb : B.Iw);
+  float ima = ia ? B.im[r.la] : 0.0f, imb = ib ? B.im[r.lb] : 0.0f;
+  pgs_row_core(B.lin, B.ang, r, qa, qb, ima, imb, jn_arr[s], jt_arr[s], dres + 3 * (size_t)s);
 }
 __device__ __forceinline__ float row_residual(const SRow& r, const float* dres, uint32_t s) {
   float res = 0.0f;
@@ -1116,115 +1161,9 @@ __device__ __forceinline__ float row_residual(const SRow& r, const float* dres, 
 // (islands share no body, so the other islands' arithmetic is unchanged). Fixed-iteration mode
 // (tol = 0) never marks an island done.
 
-// Warm start application and the velocity sweeps of one big island (solver.rs:717-915), bodies
-// in shared memory, rows streamed from the schedule-ordered arrays; __syncthreads between levels.
-#define GROUP_ISL_MAX 64u  // the CTA kernel solves single islands; the bound only has to cover that
-template <int NT>
-__global__ void __launch_bounds__(NT) k_vel_solve_smem(uint32_t g0, uint32_t ng, const uint32_t* __restrict__ glist,
-                                                       uint32_t want_class,
-                                                       const uint32_t* __restrict__ g_class,
-                                                       const uint32_t* __restrict__ gb_start, const uint32_t* __restrict__ gb_cnt,
-                                                       const uint32_t* __restrict__ gb_list, const uint32_t* __restrict__ g_nisl,
-                                                       Sched S, SRowsV R, BodiesV G,
-                                                       const float4* __restrict__ wa, const float4* __restrict__ wb,
-                                                       float* acc_jn, float2* acc_jt, int iters, float tol, uint32_t* stats) {
-  if (glist && blockIdx.x >= ng) return;
-  uint32_t g = glist ? glist[blockIdx.x] : g0 + blockIdx.x;
-  if (!glist && g >= ng) return;
-  if (g_class[g] != want_class) return;
-  const uint32_t nisl = g_nisl[g];
-  if (nisl > GROUP_ISL_MAX) {  // not reached: classes 0 and 1 are single islands
-    if (threadIdx.x == 0) atomicOr(&stats[STAT_ERR], 2u);
-    return;
-  }
-  __shared__ uint32_t isl_res[GROUP_ISL_MAX], isl_last[GROUP_ISL_MAX], isl_sw[GROUP_ISL_MAX];
-  __shared__ uint8_t isl_done[GROUP_ISL_MAX];
-  __shared__ uint32_t blk_rowsweeps, blk_capped;
-  extern __shared__ float4 smem[];
-  uint32_t nbg = gb_cnt[g], b0 = gb_start[g];
-  SBodies B;
-  B.lin = smem;
-  B.ang = smem + nbg;
-  B.Iw = reinterpret_cast<float*>(smem + 2 * nbg);
-  B.im = B.Iw + 9 * nbg;
-  for (uint32_t i = threadIdx.x; i < nbg; i += NT) {
-    uint32_t b = gb_list[b0 + i];
-    B.lin[i] = G.lin[b];
-    B.ang[i] = G.ang[b];
-    for (int k = 0; k < 9; ++k) B.Iw[9 * i + k] = G.Iw[9 * (size_t)b + k];
-    B.im[i] = G.inv_mass[b];
-  }
-  for (uint32_t i = threadIdx.x; i < nisl; i += NT) { isl_res[i] = 0u; isl_last[i] = 0u; isl_sw[i] = 0u; isl_done[i] = 0; }
-  if (threadIdx.x == 0) { blk_rowsweeps = 0u; blk_capped = 0u; }
-  __syncthreads();
-  uint32_t off = S.lvl_off[g], nl = S.nlev[g];
-  for (uint32_t L = 0; L < nl; ++L) {
-    uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
-    for (uint32_t s = s0 + threadIdx.x; s < s1; s += NT) {
-      int e = R.wm[s];
-      if (e >= 0) { SRow r = ld_srow(R, s); warm_apply_s(B, r, s, wa[e], wb[e], R.jn, R.jt); }
-    }
-    __syncthreads();
-  }
-  int it = 0;
-  while (it < iters) {
-    for (uint32_t L = 0; L < nl; ++L) {
-      uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
-      for (uint32_t s = s0 + threadIdx.x; s < s1; s += NT) {
-        uint32_t li = R.flags[s] >> 16;
-        if (isl_done[li]) continue;
-        SRow r = ld_srow(R, s);
-        float rr = pgs_row_s(B, r, s, R.jn, R.jt);
-        atomicMax(&isl_res[li], fbits(rr));  // non-negative floats: integer max, order-free
-      }
-      __syncthreads();
-    }
-    it++;
-    bool active = false;
-    for (uint32_t i = threadIdx.x; i < nisl; i += NT) {
-      if (isl_done[i]) continue;
-      uint32_t rb = isl_res[i];
-      isl_res[i] = 0u;
-      isl_sw[i] = (uint32_t)it;
-      isl_last[i] = rb;
-      if (tol > 0.0f && __uint_as_float(rb) <= tol) isl_done[i] = 1;
-      else active = true;
-    }
-    if (!__syncthreads_or(active)) break;
-  }
-  for (uint32_t i = threadIdx.x; i < nbg; i += NT) {
-    uint32_t b = gb_list[b0 + i];
-    G.lin[b] = B.lin[i];
-    G.ang[b] = B.ang[i];
-  }
-  uint32_t s_begin = S.lvl_start[off], s_end = nl ? S.lvl_start[off + nl] : s_begin;
-  uint32_t my_rs = 0;
-  for (uint32_t s = s_begin + threadIdx.x; s < s_end; s += NT) {
-    uint32_t r = S.ord[s];
-    acc_jn[r] = R.jn[s];
-    acc_jt[r] = R.jt[s];
-    my_rs += isl_sw[R.flags[s] >> 16];
-  }
-  uint32_t my_sw = 0, my_res = 0, my_cap = 0;
-  for (uint32_t i = threadIdx.x; i < nisl; i += NT) {
-    my_sw = max(my_sw, isl_sw[i]);
-    my_res = max(my_res, isl_last[i]);
-    if (tol > 0.0f && !isl_done[i]) my_cap++;
-  }
-  atomicAdd(&blk_rowsweeps, my_rs);
-  atomicAdd(&blk_capped, my_cap);
-  if (my_sw) atomicMax(&stats[STAT_SWEEPS], my_sw);
-  if (my_res) atomicMax(&stats[STAT_RESID], my_res);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (blk_rowsweeps) atomicAdd(&stats[STAT_ROWSWEEPS], blk_rowsweeps);
-    if (blk_capped) atomicAdd(&stats[STAT_ISLANDS_CAPPED], blk_capped);
-  }
-}
-
 // A group solved by one block with everything it touches in that block's shared memory: rows
 // (in schedule order), impulses, bodies, level starts and per-island residual state; a block
-// barrier between levels. Same arithmetic and order as k_vel_solve_smem. Capacities RC rows,
+// barrier between levels. Same arithmetic and order as the serial sweep. Capacities RC rows,
 // BC bodies, IC islands set the layout: packed groups (class 3) 64 / 128 / 64 in about 20 KB
 // with 64 threads; single islands (classes 10..15) R / R + 1 / 1 for R = 128 ... 1024 rows,
 // about 220 bytes per row (28 KB ... 225 KB), with 128 threads.
@@ -1395,6 +1334,218 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
   }
 }
 
+// ------------------------------------------------------------------ big islands
+// An island beyond the on-chip buckets (bodies and levels within its bucket's caps) solved by one
+// CTA: body velocities in shared memory, rows streamed through a double-buffered stage. Each level
+// is cut into chunks of at most CH rows (one per thread); while a chunk is solved, cp.async
+// copies the next chunk -- its row data, both bodies' world inverse inertia and inverse mass
+// (BigRowX, built per tick) and its accumulators -- into the other buffer, so the level chain
+// never waits on L2. Accumulators (jn, jt) live in global memory between sweeps (BigJ).
+template <int CH>
+struct BigStage {
+  float4 ra[CH], rb[CH], n[CH], t1[CH], t2[CH], mu[CH];
+  float4 x[CH][7];  // Iw a (9) im a | Iw b (9) im b (3 float4 each: 12 floats), vfix
+  float4 j[CH];     // jn, jt.x, jt.y
+  uint2 loc[CH];
+  float2 inv[CH];
+  uint32_t flags[CH];
+};
+static_assert(sizeof(BigStage<64>) % 16 == 0 && sizeof(BigStage<128>) % 16 == 0, "stage buffers stay 16-byte aligned");
+template <int CH>
+constexpr size_t big_smem(uint32_t bodies, uint32_t levels) {
+  return 2 * sizeof(BigStage<CH>) + 32u * (size_t)bodies + ((4u * (levels + 1u) + 15u) & ~15u);
+}
+static_assert(big_smem<128>(4500u, 4096u) + 16 <= 232448, "largest big-island block exceeds the shared memory limit");
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// Per row (schedule position) of a big island: Iw and inverse mass of both bodies, vfix.
+__global__ void k_big_rows_x(uint32_t n, const uint32_t* __restrict__ ord, const uint32_t* __restrict__ row_group,
+                             const uint32_t* __restrict__ g_class, RowsV R, BodiesV B, SRowsV SR, float4* X, float4* J) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  uint32_t r = ord[s];
+  uint32_t c = g_class[row_group[r]];
+  if (c < 20u || c >= 20u + BIG_BUCKETS) return;
+  uint2 ab = R.ab[r];
+  uint32_t f = R.flags[r];
+  float q[24];
+  for (int k = 0; k < 24; ++k) q[k] = 0.0f;
+  if (f & RF_WA) { for (int k = 0; k < 9; ++k) q[k] = B.Iw[9 * (size_t)ab.x + k]; q[9] = B.inv_mass[ab.x]; }
+  if (f & RF_WB) { for (int k = 0; k < 9; ++k) q[12 + k] = B.Iw[9 * (size_t)ab.y + k]; q[21] = B.inv_mass[ab.y]; }
+  float4* o = X + 7 * (size_t)s;
+  for (int k = 0; k < 6; ++k) o[k] = make_float4(q[4 * k], q[4 * k + 1], q[4 * k + 2], q[4 * k + 3]);
+  uint2 l = SR.loc[s];
+  o[6] = l.x == 0xFFFFFFFFu ? SR.va[s] : SR.vb[s];
+  J[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+template <int CH>
+__device__ __forceinline__ void big_stage_issue(BigStage<CH>& st, uint32_t s0, uint32_t n, const SRowsV& R,
+                                                const float4* __restrict__ X, const float4* J) {
+  for (uint32_t i = threadIdx.x; i < n; i += CH) {
+    uint32_t s = s0 + i;
+    cp_async16(&st.ra[i], &R.ra[s]); cp_async16(&st.rb[i], &R.rb[s]); cp_async16(&st.n[i], &R.n[s]);
+    cp_async16(&st.t1[i], &R.t1[s]); cp_async16(&st.t2[i], &R.t2[s]); cp_async16(&st.mu[i], &R.mu[s]);
+    for (int k = 0; k < 7; ++k) cp_async16(&st.x[i][k], &X[7 * (size_t)s + k]);
+    cp_async16(&st.j[i], &J[s]);
+    cp_async8(&st.loc[i], &R.loc[s]); cp_async8(&st.inv[i], &R.inv[s]); cp_async4(&st.flags[i], &R.flags[s]);
+  }
+}
+template <int CH>
+__device__ __forceinline__ SRow big_row(const BigStage<CH>& st, uint32_t i, m3* qa, m3* qb, float* ima, float* imb) {
+  SRow r;
+  uint2 l = st.loc[i]; r.la = l.x; r.lb = l.y; r.flags = st.flags[i];
+  float2 iv = st.inv[i]; r.inv_a = iv.x; r.inv_b = iv.y;
+  float4 a = st.ra[i], b = st.rb[i], n = st.n[i], t1 = st.t1[i], t2 = st.t2[i], mu = st.mu[i];
+  r.ra = xyz(a); r.m_n = a.w; r.rb = xyz(b); r.m_t1 = b.w; r.n = xyz(n); r.m_t2 = n.w;
+  r.t1 = xyz(t1); r.bias = t1.w; r.t2 = xyz(t2);
+  r.mu_s = mu.x; r.mu_k = mu.y; r.sv = mu.z;
+  r.vfix = xyz(st.x[i][6]);
+  float q[24];
+  for (int k = 0; k < 6; ++k) { float4 v = st.x[i][k]; q[4 * k] = v.x; q[4 * k + 1] = v.y; q[4 * k + 2] = v.z; q[4 * k + 3] = v.w; }
+  *qa = mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
+  *ima = q[9];
+  *qb = mcols(mk3(q[12], q[13], q[14]), mk3(q[15], q[16], q[17]), mk3(q[18], q[19], q[20]));
+  *imb = q[21];
+  return r;
+}
+template <int CH>
+__global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, uint32_t want_class,
+                                                      uint32_t n_listed, const uint32_t* __restrict__ glist,
+                                                           const uint32_t* __restrict__ g_class,
+                                                           const uint32_t* __restrict__ gb_start,
+                                                           const uint32_t* __restrict__ gb_cnt,
+                                                           const uint32_t* __restrict__ gb_list, Sched S, SRowsV R,
+                                                           const float4* __restrict__ X, float4* J, BodiesV G,
+                                                           const float4* __restrict__ wa, const float4* __restrict__ wb,
+                                                           float* acc_jn, float2* acc_jt, int iters, float tol,
+                                                           uint32_t* stats) {
+  if (blockIdx.x >= n_listed) return;
+  const uint32_t g = glist[blockIdx.x];
+  if (g_class[g] != want_class) return;
+  extern __shared__ float4 big_raw[];
+  BigStage<CH>* stg = reinterpret_cast<BigStage<CH>*>(big_raw);
+  float4* lin = reinterpret_cast<float4*>(stg + 2);
+  float4* ang = lin + BC;
+  uint32_t* lvl = reinterpret_cast<uint32_t*>(ang + BC);
+  __shared__ uint32_t res_bits;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t nbg = gb_cnt[g], b0 = gb_start[g];
+  const uint32_t off = S.lvl_off[g], nl = S.nlev[g];
+  if (nbg > BC || nl > LC) {  // not reached: the class was chosen by these sizes
+    if (tid == 0) atomicOr(&stats[STAT_ERR], 2u);
+    return;
+  }
+  for (uint32_t i = tid; i < nbg; i += CH) {
+    uint32_t b = gb_list[b0 + i];
+    lin[i] = G.lin[b];
+    ang[i] = G.ang[b];
+  }
+  for (uint32_t L = tid; L <= nl; L += CH) lvl[L] = S.lvl_start[off + L];
+  if (tid == 0) res_bits = 0u;
+  __syncthreads();
+  // warm start application, level by level, rows read directly (one pass)
+  for (uint32_t L = 0; L < nl; ++L) {
+    for (uint32_t s = lvl[L] + tid; s < lvl[L + 1]; s += CH) {
+      int e = R.wm[s];
+      if (e < 0) continue;
+      SRow r = ld_srow(R, s);
+      const float4* x = X + 7 * (size_t)s;
+      float q[24];
+      for (int k = 0; k < 6; ++k) { float4 v = x[k]; q[4 * k] = v.x; q[4 * k + 1] = v.y; q[4 * k + 2] = v.z; q[4 * k + 3] = v.w; }
+      m3 qa = mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
+      m3 qb = mcols(mk3(q[12], q[13], q[14]), mk3(q[15], q[16], q[17]), mk3(q[18], q[19], q[20]));
+      float jn = 0.0f; float2 jt = make_float2(0.0f, 0.0f);
+      warm_core(lin, ang, r, qa, qb, q[9], q[21], wa[e], wb[e], jn, jt);
+      J[s] = make_float4(jn, jt.x, jt.y, 0.0f);
+    }
+    __threadfence_block();
+    __syncthreads();
+  }
+  // sweeps: chunk (L, c0, c1) -> the next chunk of this sweep, or the first one of the next
+  uint32_t cL = 0, c0 = lvl[0], c1 = min(lvl[0] + (uint32_t)CH, lvl[1]);
+  int it = 0, buf = 0;
+  big_stage_issue(stg[0], c0, c1 - c0, R, X, J);
+  cp_async_commit();
+  bool done = nl == 0;
+  while (!done) {
+    uint32_t nL = cL, n0, n1;
+    bool last_of_sweep = false;
+    if (c1 < lvl[cL + 1]) { n0 = c1; n1 = min(c1 + (uint32_t)CH, lvl[cL + 1]); }
+    else if (cL + 1 < nl) { nL = cL + 1; n0 = lvl[nL]; n1 = min(n0 + (uint32_t)CH, lvl[nL + 1]); }
+    else { last_of_sweep = true; nL = 0; n0 = lvl[0]; n1 = min(n0 + (uint32_t)CH, lvl[1]); }
+    // a sweep of one chunk would prefetch the rows it is about to write: stage those after it
+    const bool self_next = n0 == c0;
+    if (!self_next) big_stage_issue(stg[buf ^ 1], n0, n1 - n0, R, X, J);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    if (tid < c1 - c0) {
+      BigStage<CH>& st = stg[buf];
+      m3 qa, qb; float ima, imb;
+      SRow r = big_row(st, tid, &qa, &qb, &ima, &imb);
+      float4 jj = st.j[tid];
+      float jn = jj.x; float2 jt = make_float2(jj.y, jj.z);
+      float d3[3];
+      pgs_row_core(lin, ang, r, qa, qb, ima, imb, jn, jt, d3);
+      J[c0 + tid] = make_float4(jn, jt.x, jt.y, 0.0f);
+      float rr = 0.0f;
+      if (r.m_n > 0.0f) rr = rmax(rr, fabsf(d3[0]) / r.m_n);
+      if (r.m_t1 > 0.0f) rr = rmax(rr, fabsf(d3[1]) / r.m_t1);
+      if (r.m_t2 > 0.0f) rr = rmax(rr, fabsf(d3[2]) / r.m_t2);
+      atomicMax(&res_bits, fbits(rr));  // non-negative floats: integer max, order-free
+    }
+    __threadfence_block();
+    __syncthreads();
+    if (self_next) {
+      big_stage_issue(stg[buf ^ 1], n0, n1 - n0, R, X, J);
+      cp_async_commit();
+    }
+    if (last_of_sweep) {
+      it++;
+      uint32_t rb = res_bits;
+      __syncthreads();
+      if (tid == 0) res_bits = 0u;
+      if ((tol > 0.0f && __uint_as_float(rb) <= tol) || it >= iters) {
+        done = true;
+        if (tid == 0) {
+          atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
+          atomicMax(&stats[STAT_RESID], rb);
+          atomicAdd(&stats[STAT_ROWSWEEPS], (lvl[nl] - lvl[0]) * (uint32_t)it);
+          if (tol > 0.0f && !(__uint_as_float(rb) <= tol)) atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
+        }
+      }
+      __syncthreads();
+    }
+    cL = nL; c0 = n0; c1 = n1; buf ^= 1;
+  }
+  cp_async_wait0();
+  __syncthreads();
+  for (uint32_t i = tid; i < nbg; i += CH) {
+    uint32_t b = gb_list[b0 + i];
+    G.lin[b] = lin[i];
+    G.ang[b] = ang[i];
+  }
+  for (uint32_t s = lvl[0] + tid; s < lvl[nl]; s += CH) {
+    uint32_t r = S.ord[s];
+    float4 jj = J[s];
+    acc_jn[r] = jj.x;
+    acc_jt[r] = make_float2(jj.y, jj.z);
+  }
+}
+
 // ------------------------------------------------------------------ small helpers
 __global__ void k_scatter_u32(uint32_t n, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ src, uint32_t* dst) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1522,7 +1673,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     }
     ctx.nsched = nsched;
     uint32_t nisl = 0, ng = 0, g_small = 0;
-    uint32_t cls_n[16] = {};  // groups per class (class 3: g_small, not listed)
+    uint32_t cls_n[32] = {};  // groups per class (class 3: g_small, not listed)
     S.isl_start.ensure(nsched + 1); S.isl_cnt.ensure(nsched + 1);
     S.ord_main.ensure(nsched + 1); S.ord_vs.ensure(nsched + 1); S.ord_ps.ensure(nsched + 1);
     if (nsched > 0) {
@@ -1584,11 +1735,11 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cudaMemsetAsync(S.gb_cnt.p, 0, sizeof(uint32_t) * (ng + 1), st));
       k_body_local<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.gb_cnt.p, S.body_local.p); RP_COUNT_LAUNCH(1);
       k_body_local2<<<nblk(ngb), T, 0, st>>>(ngb, S.gb_key2.p, S.gb_list.p, S.gb_start.p, S.body_local.p); RP_COUNT_LAUNCH(1);
-      S.cls_cnt.ensure(16); S.cls_list.ensure(16 * (size_t)ng + 16);
-      RP_CUDA(cudaMemsetAsync(S.cls_cnt.p, 0, 16 * 4, st));
-      k_group_class<<<nblk(ng), T, 0, st>>>(ng, g_small, S.gb_cnt.p, S.g_cnt.p, S.g_class.p, S.cls_cnt.p, S.cls_list.p,
-                                            stats); RP_COUNT_LAUNCH(1);
-      RP_CUDA(cudaMemcpyAsync(cls_n, S.cls_cnt.p, 16 * 4, cudaMemcpyDeviceToHost, st));
+      S.cls_cnt.ensure(32); S.cls_list.ensure(32 * (size_t)ng + 32);
+      RP_CUDA(cudaMemsetAsync(S.cls_cnt.p, 0, 32 * 4, st));
+      k_group_class<<<nblk(ng), T, 0, st>>>(ng, g_small, S.gb_cnt.p, S.g_cnt.p, S.nlev.p, S.g_class.p, S.cls_cnt.p,
+                                            S.cls_list.p, stats); RP_COUNT_LAUNCH(1);
+      RP_CUDA(cudaMemcpyAsync(cls_n, S.cls_cnt.p, 32 * 4, cudaMemcpyDeviceToHost, st));
       RP_CUDA(cudaStreamSynchronize(st));
       // levels / max batch (solver.rs:684-687)
       {
@@ -1634,8 +1785,10 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       int dev = 0;
       RP_CUDA(cudaGetDevice(&dev));
       if (!((smem_attr.load() >> (dev & 63)) & 1ull)) {
-        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_smem<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMALL_BODIES * 72));
-        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_smem<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, BIG_BODIES * 72));
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_big<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)big_smem<128>(kBigBodies[2], kBigLevels[2])));
+        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_big<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)big_smem<64>(kBigBodies[1], kBigLevels[1])));
         RP_CUDA(cudaFuncSetAttribute(k_vel_solve_onchip<false, ONCHIP_T_ISLAND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)lay_top.bytes));
         RP_CUDA(cudaFuncSetAttribute(k_vel_solve_onchip<true, ONCHIP_T_PACKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1670,16 +1823,28 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
             W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
       P.end(PH_VEL_PACKED, st);
       P.begin(PH_VEL_BIG, st);
-      if (cls_n[0])
-        k_vel_solve_smem<128><<<cls_n[0], 128, SMALL_BODIES * 72, st>>>(0u, cls_n[0], lst(0), 0u, S.g_class.p, S.gb_start.p,
-                                                                        S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
-                                                                        W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters,
-                                                                        tol, stats); RP_COUNT_LAUNCH(1);
-      if (cls_n[1])
-        k_vel_solve_smem<512><<<cls_n[1], 512, BIG_BODIES * 72, st>>>(0u, cls_n[1], lst(1), 1u, S.g_class.p, S.gb_start.p,
-                                                                      S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
-                                                                      W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters,
-                                                                      tol, stats); RP_COUNT_LAUNCH(1);
+      {
+        // big islands: per-row inverse inertias for the staged stream, then one CTA each, per bucket
+        uint32_t nbig = cls_n[20] + cls_n[21] + cls_n[22];
+        if (nbig) {
+          S.big_x.ensure(7 * (size_t)nsched + 7); S.big_j.ensure(nsched + 1);
+          k_big_rows_x<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, S.row_isl2.p, S.g_class.p, R, B, SR, S.big_x.p,
+                                                   S.big_j.p); RP_COUNT_LAUNCH(1);
+        }
+        for (int b = BIG_BUCKETS - 1; b >= 0; --b) {
+          uint32_t n = cls_n[20 + b];
+          if (!n) continue;
+          if (b == BIG_BUCKETS - 1)
+            k_vel_solve_big<128><<<n, 128, big_smem<128>(kBigBodies[b], kBigLevels[b]), st>>>(
+                kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
+                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats);
+          else
+            k_vel_solve_big<64><<<n, 64, big_smem<64>(kBigBodies[b], kBigLevels[b]), st>>>(
+                kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
+                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats);
+          RP_COUNT_LAUNCH(1);
+        }
+      }
       if (cls_n[2])
         k_vel_solve<<<nblk(cls_n[2] * 32, 128), 128, 0, st>>>(cls_n[2], SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
                                                                W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
