@@ -153,6 +153,27 @@ RPhysResult rphys_ext_snapshot_restore_exact(RPhysWorld* world, const RPhysWorld
 RPhysResult rphys_ext_batch_get_hashes(const RPhysWorld* world, uint32_t first_world, uint32_t count,
                                        RPhysHash32* out_hashes);
 
+/* ---- The learned warm start's model (no counterpart in the reference). An MLP 24 -> 128 -> 128 ->
+ * 128 -> 3 with SiLU, bf16 weights and activations with f32 accumulation on the tensor cores,
+ * trained on the GPU with Adam on f32 master weights. Inputs: 24 f32 features per contact row (the
+ * layout rphys_ext_get_row_features writes); outputs: the row's impulse (normal, two friction
+ * components) in units of the row's effective mass x 9.81 / 60. Weights are one f32 array of
+ * rphys_ext_model_num_params() values (W1 [128 x 32], b1, W2 [128 x 128], b2, W3, b3, W4 [16 x 128],
+ * b4 [16]; the padding columns of W1 and rows of W4 stay 0). */
+typedef struct RPhysWarmModel RPhysWarmModel;
+RPhysWarmModel* rphys_ext_model_create(uint64_t seed);
+void rphys_ext_model_destroy(RPhysWarmModel* model);
+uint32_t rphys_ext_model_num_params(void);
+RPhysResult rphys_ext_model_get_weights(const RPhysWarmModel* model, float* out, uint32_t count);
+RPhysResult rphys_ext_model_set_weights(RPhysWarmModel* model, const float* in, uint32_t count);
+RPhysResult rphys_ext_model_predict(RPhysWarmModel* model, const float* feats24, uint32_t rows, float* out3);
+/* One forward/backward pass (mean squared error over the 3 outputs): gradients of every weight. */
+RPhysResult rphys_ext_model_gradients(RPhysWarmModel* model, const float* feats24, const float* targets3, uint32_t rows,
+                                      float* out_grads, float* out_loss);
+/* `epochs` passes of mini-batch Adam over the rows in order; returns the last epoch's mean loss. */
+RPhysResult rphys_ext_model_train(RPhysWarmModel* model, const float* feats24, const float* targets3, uint32_t rows,
+                                  uint32_t epochs, uint32_t batch, float learning_rate, float* out_loss);
+
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:
  * cudaMalloc and cudaFree can wait for all work on the device and their memory use varies with the

@@ -638,3 +638,21 @@ extern "C" int rphys_oracle_collide(uint32_t sa, const float* da, const float* p
   }
   return m.len;
 }
+
+// The learned warm start's model runs on the tensor cores only; the CPU restatement exports the
+// symbols for the shared bindings and refuses (the tests check the model against numpy).
+struct RPhysWarmModel { int unused; };
+extern "C" {
+RPhysWarmModel* rphys_ext_model_create(uint64_t) { fail(RPHYS_ERR_BAD_ARG, "model: GPU only"); return nullptr; }
+void rphys_ext_model_destroy(RPhysWarmModel*) {}
+uint32_t rphys_ext_model_num_params(void) { return 39312u; }
+RPhysResult rphys_ext_model_get_weights(const RPhysWarmModel*, float*, uint32_t) { return fail(RPHYS_ERR_BAD_ARG, "model: GPU only"); }
+RPhysResult rphys_ext_model_set_weights(RPhysWarmModel*, const float*, uint32_t) { return fail(RPHYS_ERR_BAD_ARG, "model: GPU only"); }
+RPhysResult rphys_ext_model_predict(RPhysWarmModel*, const float*, uint32_t, float*) { return fail(RPHYS_ERR_BAD_ARG, "model: GPU only"); }
+RPhysResult rphys_ext_model_gradients(RPhysWarmModel*, const float*, const float*, uint32_t, float*, float*) {
+  return fail(RPHYS_ERR_BAD_ARG, "model: GPU only");
+}
+RPhysResult rphys_ext_model_train(RPhysWarmModel*, const float*, const float*, uint32_t, uint32_t, uint32_t, float, float*) {
+  return fail(RPHYS_ERR_BAD_ARG, "model: GPU only");
+}
+}

@@ -166,6 +166,15 @@ ABI = [
     ("rphys_world_snapshot_free", None, [c_void_p]),
     ("rphys_ext_add_bodies", c_uint32, [c_void_p, POINTER(BodyDescEx), c_uint32, POINTER(c_uint32)]),
     ("rphys_ext_snapshot_restore_exact", c_uint32, [c_void_p, c_void_p]),
+    ("rphys_ext_model_create", c_void_p, [c_uint64]),
+    ("rphys_ext_model_destroy", None, [c_void_p]),
+    ("rphys_ext_model_num_params", c_uint32, []),
+    ("rphys_ext_model_get_weights", c_uint32, [c_void_p, c_void_p, c_uint32]),
+    ("rphys_ext_model_set_weights", c_uint32, [c_void_p, c_void_p, c_uint32]),
+    ("rphys_ext_model_predict", c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p]),
+    ("rphys_ext_model_gradients", c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, POINTER(c_float)]),
+    ("rphys_ext_model_train", c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_float,
+                                         POINTER(c_float)]),
     ("rphys_ext_batch_add_world", c_uint32, [c_void_p, c_void_p, c_uint32, POINTER(c_uint32), POINTER(c_uint32)]),
     ("rphys_ext_batch_num_worlds", c_uint32, [c_void_p, POINTER(c_uint32)]),
     ("rphys_ext_batch_world_range", c_uint32, [c_void_p, c_uint32, POINTER(c_uint32), POINTER(c_uint32)]),
@@ -225,6 +234,9 @@ class Lib:
 
     def world(self, max_bodies=1024, max_colliders=2048):
         return World(self, max_bodies, max_colliders)
+
+    def model(self, seed=1):
+        return WarmModel(self, seed)
 
 
 def load_product():
@@ -461,3 +473,63 @@ class World:
         if count:
             self.c("rphys_ext_get_body_states", first, count, out.ctypes.data_as(c_void_p))
         return out
+
+
+class WarmModel:
+    """The learned warm start's MLP (24 -> 128 -> 128 -> 128 -> 3) on the tensor cores."""
+
+    def __init__(self, lib, seed=1):
+        self.lib = lib
+        self.h = lib.dll.rphys_ext_model_create(seed)
+        if not self.h:
+            msg = lib.dll.rphys_last_error_message()
+            raise RPhysError(RPHYS_ERR_INTERNAL, msg.decode() if msg else "model create failed")
+        self.n_params = lib.dll.rphys_ext_model_num_params()
+
+    def close(self):
+        if self.h:
+            self.lib.dll.rphys_ext_model_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def weights(self):
+        import numpy as np
+        w = np.zeros(self.n_params, dtype=np.float32)
+        self.lib.call("rphys_ext_model_get_weights", self.h, w.ctypes.data_as(c_void_p), self.n_params)
+        return w
+
+    def set_weights(self, w):
+        import numpy as np
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self.lib.call("rphys_ext_model_set_weights", self.h, w.ctypes.data_as(c_void_p), self.n_params)
+
+    def predict(self, feats):
+        import numpy as np
+        f = np.ascontiguousarray(feats, dtype=np.float32)
+        out = np.zeros((len(f), 3), dtype=np.float32)
+        self.lib.call("rphys_ext_model_predict", self.h, f.ctypes.data_as(c_void_p), len(f), out.ctypes.data_as(c_void_p))
+        return out
+
+    def gradients(self, feats, targets):
+        import numpy as np
+        f = np.ascontiguousarray(feats, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = c_float(0)
+        self.lib.call("rphys_ext_model_gradients", self.h, f.ctypes.data_as(c_void_p), t.ctypes.data_as(c_void_p), len(f),
+                      g.ctypes.data_as(c_void_p), byref(loss))
+        return g, loss.value
+
+    def train(self, feats, targets, epochs=1, batch=4096, lr=1e-3):
+        import numpy as np
+        f = np.ascontiguousarray(feats, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        loss = c_float(0)
+        self.lib.call("rphys_ext_model_train", self.h, f.ctypes.data_as(c_void_p), t.ctypes.data_as(c_void_p), len(f),
+                      epochs, batch, c_float(lr), byref(loss))
+        return loss.value

@@ -12,6 +12,7 @@
 #include <string>
 
 #include "../../include/rphys_ext.h"
+#include "warm_model.h"
 #include "world_gpu.h"
 
 using rp::WorldGpu;
@@ -725,4 +726,68 @@ RPhysResult rphys_ext_launch_count(uint64_t* out) {
   return RPHYS_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------- learned warm-start model
+struct RPhysWarmModel {
+  std::mutex mu;
+  std::unique_ptr<rp::WarmModel> m;
+};
+extern "C" {
+RPhysWarmModel* rphys_ext_model_create(uint64_t seed) {
+  clear_err();
+  try {
+    auto* M = new RPhysWarmModel();
+    M->m.reset(new rp::WarmModel(seed));
+    return M;
+  } catch (const std::exception& e) {
+    fail(RPHYS_ERR_INTERNAL, std::string("rphys_ext_model_create: ") + e.what());
+    return nullptr;
+  }
+}
+void rphys_ext_model_destroy(RPhysWarmModel* M) {
+  try { delete M; } catch (...) {}
+}
+uint32_t rphys_ext_model_num_params(void) { return rp::WarmModel::kParams; }
+RPhysResult rphys_ext_model_get_weights(const RPhysWarmModel* Mc, float* out, uint32_t n) {
+  clear_err();
+  if (!Mc || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_model_get_weights: null arg");
+  if (n != rp::WarmModel::kParams) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_model_get_weights: count != num_params");
+  auto* M = const_cast<RPhysWarmModel*>(Mc);
+  return guard("rphys_ext_model_get_weights", [&]() { std::lock_guard<std::mutex> g(M->mu); M->m->get_weights(out); return (RPhysResult)RPHYS_OK; });
+}
+RPhysResult rphys_ext_model_set_weights(RPhysWarmModel* M, const float* in, uint32_t n) {
+  clear_err();
+  if (!M || !in) return fail(RPHYS_ERR_NULL, "rphys_ext_model_set_weights: null arg");
+  if (n != rp::WarmModel::kParams) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_model_set_weights: count != num_params");
+  for (uint32_t i = 0; i < n; ++i)
+    if (!std::isfinite(in[i])) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_model_set_weights: non-finite weight");
+  return guard("rphys_ext_model_set_weights", [&]() { std::lock_guard<std::mutex> g(M->mu); M->m->set_weights(in); return (RPhysResult)RPHYS_OK; });
+}
+RPhysResult rphys_ext_model_predict(RPhysWarmModel* M, const float* f, uint32_t n, float* out) {
+  clear_err();
+  if (!M || (n && (!f || !out))) return fail(RPHYS_ERR_NULL, "rphys_ext_model_predict: null arg");
+  return guard("rphys_ext_model_predict", [&]() { std::lock_guard<std::mutex> g(M->mu); M->m->predict(n, f, out, false); return (RPhysResult)RPHYS_OK; });
+}
+RPhysResult rphys_ext_model_gradients(RPhysWarmModel* M, const float* f, const float* t, uint32_t n, float* grads, float* loss) {
+  clear_err();
+  if (!M || !f || !t || !grads || !loss || !n) return fail(RPHYS_ERR_NULL, "rphys_ext_model_gradients: null arg or no rows");
+  return guard("rphys_ext_model_gradients", [&]() {
+    std::lock_guard<std::mutex> g(M->mu);
+    *loss = M->m->gradients(n, f, t, false);
+    M->m->get_grads(grads);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_model_train(RPhysWarmModel* M, const float* f, const float* t, uint32_t n, uint32_t epochs, uint32_t batch,
+                                  float lr, float* loss) {
+  clear_err();
+  if (!M || !f || !t || !loss || !n) return fail(RPHYS_ERR_NULL, "rphys_ext_model_train: null arg or no rows");
+  if (batch == 0 || !(std::isfinite(lr) && lr > 0)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_model_train: batch > 0 and lr > 0");
+  return guard("rphys_ext_model_train", [&]() {
+    std::lock_guard<std::mutex> g(M->mu);
+    *loss = M->m->train(n, f, t, epochs, batch, lr);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
 }  // extern "C"
