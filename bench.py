@@ -189,6 +189,7 @@ def main():
     ap.add_argument("--settle", type=int, default=240)
     ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop", "batch"])
     ap.add_argument("--worlds", type=int, default=4096, help="batch: number of worlds")
+    ap.add_argument("--learned", type=int, default=1, help="terrain: also time the learned warm start (1/0)")
     ap.add_argument("--mode", default="residual", choices=["residual", "fixed"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--bodies", type=int, default=None)
@@ -212,8 +213,21 @@ def main():
         w.set_residual_mode(TOL, 4 * ITERS[args.config])
     # settle into the contact regime, then warm up
     t_settle = time.perf_counter()
+    learn_f, learn_t = [], []
+    learned_on = args.learned and args.config == "terrain"
     if args.settle:
-        w.step_n(dt, args.settle)
+        if learned_on and args.settle > 60:
+            # the learned warm start's training rows: every 10th of the last 60 settle ticks
+            w.step_n(dt, args.settle - 60)
+            w.set_feature_logging(True)
+            for k in range(60):
+                w.step_n(dt, 1)
+                if k % 10 == 9:
+                    f, t = w.row_features()
+                    learn_f.append(f); learn_t.append(t)
+            w.set_feature_logging(False)
+        else:
+            w.step_n(dt, args.settle)
     print(f"[bench] {nb} bodies, settle {args.settle} ticks in {time.perf_counter() - t_settle:.2f}s", file=sys.stderr)
     for _ in range(args.warmup):
         w.step_n(dt, 1)
@@ -301,6 +315,41 @@ def main():
         v, sample = cpu_sample_with(olib, 10, threads)
         cpu = {"value": v, "unit": "body-ticks/s", "cores": threads, "kind": "port", "sample": sample}
 
+    learned = None
+    if learned_on and learn_f:
+        # train on the settle rows (new contacts, targets clipped to +-20 units), then replay the
+        # timed ticks with the model offering starts to the rows the previous tick has nothing for
+        import numpy as np
+        F, T = np.concatenate(learn_f), np.concatenate(learn_t)
+        cold = F[:, 22] == 0
+        F, T = F[cold], np.clip(T[cold], -20.0, 20.0)
+        model = lib.model(seed=2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = model.train(F, T, epochs=3, batch=2048, lr=1e-3)
+        t_train = time.perf_counter() - t0
+        w.restore_exact(snap)
+        w.set_warm_model(model)
+        w.set_warm_policy(True)
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        l0.record(stream)
+        rs = pu = 0
+        for _ in range(args.steps):
+            w.step_n(dt, 1)
+            s_ = w.stats()
+            rs += s_["row_sweeps"]
+            pu += s_["pred_used"]
+        l1.record(stream)
+        torch.cuda.synchronize()
+        lms = l0.elapsed_time(l1)
+        w.set_warm_model(None)
+        learned = {"value": nb * args.steps / (lms / 1000.0), "unit": "body-ticks/s", "ms_per_step": lms / args.steps,
+                   "row_updates": rs, "row_updates_previous_tick_start": units["row_sweeps"],
+                   "rows_started_from_prediction": pu, "train_rows": int(len(F)), "train_epochs": 3,
+                   "train_seconds": t_train, "train_loss": loss,
+                   "note": "same timed ticks replayed from the snapshot; per-tick stats read between ticks"}
+
     rollback = None
     if args.config == "batch":
         # the rollback workload: back to the snapshot, re-simulate 8 ticks twice from it (the first
@@ -338,6 +387,8 @@ def main():
                 "gpu_launches": launches, "stage_ms": stages}
         if rollback is not None:
             line["rollback"] = rollback
+        if learned is not None:
+            line["learned_warm_start"] = learned
         print(json.dumps(line), flush=True)
     w.free_snapshot(snap)
     w.close()

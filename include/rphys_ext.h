@@ -87,6 +87,7 @@ typedef struct RPhysStepStats {
      * largest group */
     uint32_t groups_shared, groups_global, max_group_rows, max_group_bodies;
     uint32_t islands_capped; /* residual mode: solve islands still above the tolerance at the sweep cap */
+    uint32_t pred_used;      /* rows whose warm start came from the learned prediction */
 } RPhysStepStats;
 RPhysResult rphys_ext_get_stats(const RPhysWorld* world, RPhysStepStats* out);
 
@@ -173,6 +174,26 @@ RPhysResult rphys_ext_model_gradients(RPhysWarmModel* model, const float* feats2
 /* `epochs` passes of mini-batch Adam over the rows in order; returns the last epoch's mean loss. */
 RPhysResult rphys_ext_model_train(RPhysWarmModel* model, const float* feats24, const float* targets3, uint32_t rows,
                                   uint32_t epochs, uint32_t batch, float learning_rate, float* out_loss);
+
+/* The learned warm start in a world (no counterpart in the reference). With a model set (it must
+ * outlive its use; NULL switches it off), every tick computes each contact row's features and the
+ * model's predicted impulse; at the row's place in the warm-start order the solver tries both the
+ * previous tick's impulse (or none) and the prediction on copies of the two bodies and keeps the
+ * one that leaves the smaller normal velocity error, so a prediction that would start the row
+ * worse falls back to the reference warm start. Counted in RPhysStepStats.pred_used. The
+ * predictions are computed on the tensor cores and are deterministic, so replays and hashes are. */
+RPhysResult rphys_ext_set_warm_model(RPhysWorld* world, RPhysWarmModel* model);
+/* cold_only = 1: offer predictions only to rows the previous tick's cache has no impulse for (new
+ * contacts); 0 (the default): to every row. */
+RPhysResult rphys_ext_set_warm_policy(RPhysWorld* world, uint32_t cold_only);
+/* Training data: with logging on, the last tick's feature rows (24 floats) and converged impulses
+ * (3 floats, the model's output unit) of the contacts with a movable body, in contact order. */
+RPhysResult rphys_ext_set_feature_logging(RPhysWorld* world, uint32_t on);
+RPhysResult rphys_ext_get_row_features(const RPhysWorld* world, float* out_feats24, float* out_targets3, uint32_t cap_rows,
+                                       uint32_t* out_rows);
+/* The predictions the last tick offered, per contact in contact order: 4 floats (normal, friction 1,
+ * friction 2, 1) or zeros where none was offered. */
+RPhysResult rphys_ext_get_row_predictions(const RPhysWorld* world, float* out4, uint32_t cap_contacts, uint32_t* out_count);
 
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:

@@ -525,6 +525,7 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
   o->bounce_skipped = s.bounce_skipped; o->residual = s.residual;
   o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
   o->islands_capped = s.islands_capped;
+  o->pred_used = s.pred_used;
   uint32_t we = 0;
   for (auto& kv : W->w.warm) we += (uint32_t)kv.second.size();
   o->warm_entries = we;
@@ -654,5 +655,38 @@ RPhysResult rphys_ext_model_gradients(RPhysWarmModel*, const float*, const float
 }
 RPhysResult rphys_ext_model_train(RPhysWarmModel*, const float*, const float*, uint32_t, uint32_t, uint32_t, float, float*) {
   return fail(RPHYS_ERR_BAD_ARG, "model: GPU only");
+}
+}
+
+// The learned warm start's model runs on the GPU; the restatement takes the predictions the GPU
+// offered (rphys_ext_get_row_predictions) through rphys_oracle_set_predictions and makes the same
+// per-row choice, so a learned-mode tick is checked bit for bit.
+extern "C" {
+RPhysResult rphys_ext_set_warm_model(RPhysWorld* W, RPhysWarmModel* M) {
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_warm_model: world is null");
+  return M ? fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_warm_model: the restatement takes predictions, not a model") : RPHYS_OK;
+}
+RPhysResult rphys_ext_set_warm_policy(RPhysWorld* W, uint32_t) {
+  return W ? RPHYS_OK : fail(RPHYS_ERR_NULL, "rphys_ext_set_warm_policy: world is null");
+}
+RPhysResult rphys_ext_set_feature_logging(RPhysWorld* W, uint32_t on) {
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_feature_logging: world is null");
+  return on ? fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_feature_logging: GPU only") : RPHYS_OK;
+}
+RPhysResult rphys_ext_get_row_features(const RPhysWorld* W, float*, float*, uint32_t, uint32_t* n) {
+  if (!W || !n) return fail(RPHYS_ERR_NULL, "rphys_ext_get_row_features: null arg");
+  *n = 0;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_row_predictions(const RPhysWorld* W, float*, uint32_t, uint32_t* n) {
+  if (!W || !n) return fail(RPHYS_ERR_NULL, "rphys_ext_get_row_predictions: null arg");
+  *n = 0;
+  return RPHYS_OK;
+}
+RPhysResult rphys_oracle_set_predictions(RPhysWorld* W, const float* pred4, uint32_t n_contacts) {
+  if (!W || (!pred4 && n_contacts)) return fail(RPHYS_ERR_NULL, "rphys_oracle_set_predictions: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.next_pred.assign(pred4, pred4 + 4 * (size_t)n_contacts);
+  return RPHYS_OK;
 }
 }

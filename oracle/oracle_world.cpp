@@ -1037,6 +1037,9 @@ void World::step(float dt) {
     {
       std::map<WarmKey, std::vector<bool>> used;
       const float tol2 = kWarmTol * kWarmTol;
+      std::vector<float> ref_jn(nc, 0.0f);
+      std::vector<V3> ref_jt(nc, V3{0, 0, 0});
+      std::vector<uint8_t> ref_have(nc, 0);
       for (uint32_t k = 0; k < nc; ++k) {
         const CC& cs = cons[k];
         if (cs.soft) continue;
@@ -1053,15 +1056,51 @@ void World::step(float dt) {
         if (!have) continue;
         taken[bk] = true;
         stats.warm_matched++;
-        const WarmContact& e = entries[bk];
-        acc_jn[k] = e.jn;
-        V3 imp = mul(cs.n, e.jn);
+        ref_jn[k] = entries[bk].jn;
+        ref_jt[k] = entries[bk].jt;
+        ref_have[k] = 1;
+      }
+      // application in contact order (solver.rs:749-760); with predictions offered (the learned
+      // warm start), each row keeps the start -- the previous tick's impulse or none, against the
+      // prediction -- that leaves the smaller normal velocity error |bias - v_rel . n|
+      const bool preds = next_pred.size() >= 4 * (size_t)nc;
+      auto apply_start = [&](const CC& cs, float jn, V3 jt, float* out_jn, float* out_t) {
+        V3 imp = mul(cs.n, jn);
         float mu = mu_dynamic(cs, slip_speed(*this, cs));
-        V3 t = clamp_length_max(V3{dot(e.jt, cs.t1), dot(e.jt, cs.t2), 0.0f}, mu * e.jn);
-        acc_jt[2 * k] = t.x; acc_jt[2 * k + 1] = t.y;
+        V3 t = clamp_length_max(V3{dot(jt, cs.t1), dot(jt, cs.t2), 0.0f}, mu * jn);
+        if (out_jn) { *out_jn = jn; out_t[0] = t.x; out_t[1] = t.y; }
         imp = add(imp, add(mul(cs.t1, t.x), mul(cs.t2, t.y)));
         apply_contact_impulse(*this, cs, imp);
+      };
+      auto trial_err = [&](const CC& cs, bool apply, float jn, V3 jt) {
+        V3 la = lin[cs.ai], aa = ang[cs.ai], lb{}, ab{};
+        if (!cs.terrain) { lb = lin[cs.bi]; ab = ang[cs.bi]; }
+        if (apply) apply_start(cs, jn, jt, nullptr, nullptr);
+        float e = std::fabs(cs.depth_bias - dot(contact_rel_vel(*this, cs), cs.n));
+        lin[cs.ai] = la; ang[cs.ai] = aa;
+        if (!cs.terrain) { lin[cs.bi] = lb; ang[cs.bi] = ab; }
+        return e;
+      };
+      for (uint32_t k = 0; k < nc; ++k) {
+        const CC& cs = cons[k];
+        if (cs.soft) continue;
+        const bool hp = preds && next_pred[4 * (size_t)k + 3] != 0.0f;
+        if (!ref_have[k] && !hp) continue;
+        if (hp) {
+          const float su = cs.m_n * kImpulseUnit;
+          float pjn = rmax(next_pred[4 * (size_t)k] * su, 0.0f);
+          V3 pjt = add(mul(cs.t1, next_pred[4 * (size_t)k + 1] * su), mul(cs.t2, next_pred[4 * (size_t)k + 2] * su));
+          float e_ref = trial_err(cs, ref_have[k] != 0, ref_jn[k], ref_jt[k]);
+          float e_pred = trial_err(cs, true, pjn, pjt);
+          if (e_pred < e_ref) {
+            apply_start(cs, pjn, pjt, &acc_jn[k], &acc_jt[2 * k]);
+            stats.pred_used++;
+            continue;
+          }
+        }
+        if (ref_have[k]) apply_start(cs, ref_jn[k], ref_jt[k], &acc_jn[k], &acc_jt[2 * k]);
       }
+      next_pred.clear();
     }
     // iterations (:788-915)
     // Residual stop (an extension; the reference always runs iters_v sweeps): each solve island --

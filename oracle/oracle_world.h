@@ -67,8 +67,12 @@ struct Stats {
   uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
   uint32_t sweeps = 0, bounce_skipped = 0, row_sweeps = 0, rows_scheduled = 0;
   uint32_t islands_capped = 0;  // residual mode: solve islands still above the tolerance at the cap
+  uint32_t pred_used = 0;       // rows started from an offered prediction
   float residual = 0;
 };
+
+// Unit of the learned warm start's impulses (a row's effective mass x 9.81 / 60), one f32 constant.
+constexpr float kImpulseUnit = 0.1635f;
 
 struct World {
   V3 gravity{0.0f, -9.81f, 0.0f};
@@ -98,6 +102,9 @@ struct World {
   std::vector<uint32_t> last_levels;  // per last_frame_contacts entry
   Stats stats;
   float res_tol = 0.0f;
+  // predictions offered to the next tick's warm start, 4 floats per contact in contact order
+  // (normal, friction 1, friction 2 in kImpulseUnit x m_n; 1 when offered), consumed by step()
+  std::vector<float> next_pred;
   uint32_t res_max = 0;
   int threads = 1;  // >1: narrowphase and level batches on OpenMP (order-preserving)
 

@@ -123,7 +123,7 @@ class StepStats(Structure):
                                         "sweeps", "bounce_skipped", "warm_entries", "sleeping", "error_flags")] + \
                [("residual", c_float), ("row_sweeps", c_uint32), ("rows_scheduled", c_uint32)] + \
                [(n, c_uint32) for n in ("groups_shared", "groups_global", "max_group_rows", "max_group_bodies",
-                                        "islands_capped")]
+                                        "islands_capped", "pred_used")]
 
 
 class ContactRecord(Structure):
@@ -166,6 +166,11 @@ ABI = [
     ("rphys_world_snapshot_free", None, [c_void_p]),
     ("rphys_ext_add_bodies", c_uint32, [c_void_p, POINTER(BodyDescEx), c_uint32, POINTER(c_uint32)]),
     ("rphys_ext_snapshot_restore_exact", c_uint32, [c_void_p, c_void_p]),
+    ("rphys_ext_set_warm_model", c_uint32, [c_void_p, c_void_p]),
+    ("rphys_ext_set_warm_policy", c_uint32, [c_void_p, c_uint32]),
+    ("rphys_ext_set_feature_logging", c_uint32, [c_void_p, c_uint32]),
+    ("rphys_ext_get_row_features", c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, POINTER(c_uint32)]),
+    ("rphys_ext_get_row_predictions", c_uint32, [c_void_p, c_void_p, c_uint32, POINTER(c_uint32)]),
     ("rphys_ext_model_create", c_void_p, [c_uint64]),
     ("rphys_ext_model_destroy", None, [c_void_p]),
     ("rphys_ext_model_num_params", c_uint32, []),
@@ -375,6 +380,47 @@ class World:
         out = c_uint32(0)
         self.c("rphys_ext_add_bodies", ctypes.cast(c_void_p(desc.ctypes.data), POINTER(BodyDescEx)), len(desc), byref(out))
         return out.value
+
+    def set_warm_model(self, model):
+        """Learned warm start on (a WarmModel) or off (None); the model must outlive its use."""
+        self.c("rphys_ext_set_warm_model", c_void_p(model.h) if model is not None else None)
+        self._model = model
+
+    def set_warm_policy(self, cold_only):
+        self.c("rphys_ext_set_warm_policy", 1 if cold_only else 0)
+
+    def set_feature_logging(self, on):
+        self.c("rphys_ext_set_feature_logging", 1 if on else 0)
+
+    def row_features(self):
+        import numpy as np
+        n = c_uint32(0)
+        self.c("rphys_ext_get_row_features", None, None, 0, byref(n))
+        f = np.zeros((n.value, 24), np.float32)
+        t = np.zeros((n.value, 3), np.float32)
+        if n.value:
+            self.c("rphys_ext_get_row_features", f.ctypes.data_as(c_void_p), t.ctypes.data_as(c_void_p), n.value, byref(n))
+        return f, t
+
+    def row_predictions(self):
+        import numpy as np
+        n = c_uint32(0)
+        self.c("rphys_ext_get_row_predictions", None, 0, byref(n))
+        p = np.zeros((n.value, 4), np.float32)
+        if n.value:
+            self.c("rphys_ext_get_row_predictions", p.ctypes.data_as(c_void_p), n.value, byref(n))
+        return p
+
+    def oracle_set_predictions(self, pred4):
+        """CPU restatement only: offer these per-contact predictions to the next tick's warm start."""
+        import numpy as np
+        p = np.ascontiguousarray(pred4, dtype=np.float32)
+        f = self.lib.dll.rphys_oracle_set_predictions
+        f.argtypes = [c_void_p, c_void_p, c_uint32]
+        f.restype = c_uint32
+        r = f(self.h, p.ctypes.data_as(c_void_p), len(p))
+        if r:
+            raise RPhysError(r, "rphys_oracle_set_predictions failed")
 
     def add_world(self, desc):
         """Appends one world of a batch (desc: a desc_array or a list of BodyDescEx); returns

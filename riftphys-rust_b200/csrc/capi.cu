@@ -637,6 +637,7 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
     o->groups_shared = s.groups_shared; o->groups_global = s.groups_global;
     o->max_group_rows = s.max_group_rows; o->max_group_bodies = s.max_group_bodies;
     o->islands_capped = s.islands_capped;
+    o->pred_used = s.pred_used;
     return (RPhysResult)RPHYS_OK;
   });
 }
@@ -787,6 +788,63 @@ RPhysResult rphys_ext_model_train(RPhysWarmModel* M, const float* f, const float
   return guard("rphys_ext_model_train", [&]() {
     std::lock_guard<std::mutex> g(M->mu);
     *loss = M->m->train(n, f, t, epochs, batch, lr);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+}  // extern "C"
+
+// ---------------------------------------------------------------- learned warm start in a world
+extern "C" {
+RPhysResult rphys_ext_set_warm_model(RPhysWorld* W, RPhysWarmModel* M) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_warm_model: world is null");
+  LOCK;
+  W->w->model_ = M ? M->m.get() : nullptr;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_warm_policy(RPhysWorld* W, uint32_t cold_only) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_warm_policy: world is null");
+  LOCK;
+  W->w->pred_cold_only_ = cold_only != 0;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_feature_logging(RPhysWorld* W, uint32_t on) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_feature_logging: world is null");
+  LOCK;
+  W->w->feat_log_ = on != 0;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_row_features(const RPhysWorld* Wc, float* feats, float* targets, uint32_t cap, uint32_t* out_n) {
+  clear_err();
+  if (!Wc || !out_n) return fail(RPHYS_ERR_NULL, "rphys_ext_get_row_features: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_get_row_features", [&]() {
+    LOCK;
+    std::vector<float> f, t;
+    W->w->get_row_features(f, t);
+    uint32_t n = (uint32_t)(t.size() / 3);
+    *out_n = n;
+    if (feats && targets)
+      for (uint32_t i = 0; i < n && i < cap; ++i) {
+        std::memcpy(feats + 24 * (size_t)i, f.data() + 24 * (size_t)i, 96);
+        std::memcpy(targets + 3 * (size_t)i, t.data() + 3 * (size_t)i, 12);
+      }
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_get_row_predictions(const RPhysWorld* Wc, float* out4, uint32_t cap, uint32_t* out_n) {
+  clear_err();
+  if (!Wc || !out_n) return fail(RPHYS_ERR_NULL, "rphys_ext_get_row_predictions: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_get_row_predictions", [&]() {
+    LOCK;
+    std::vector<float> p;
+    W->w->get_row_predictions(p);
+    uint32_t n = (uint32_t)(p.size() / 4);
+    *out_n = n;
+    if (out4) std::memcpy(out4, p.data(), 16 * (size_t)(n < cap ? n : cap));
     return (RPhysResult)RPHYS_OK;
   });
 }

@@ -174,6 +174,9 @@ RP_HD void sincos_rp(float xf, float* s, float* c) {
   else { sv = -cr; cv = sr; }
   *s = (float)sv; *c = (float)cv;
 }
+// Unit of the learned warm start's impulses: a row's effective mass times 9.81 m/s^2 / 60 Hz (the
+// impulse that holds the row's mass against gravity for one tick), written as one f32 constant.
+constexpr float kImpulseUnit = 0.1635f;
 RP_HD float exp_rp(float xf) {
   double x = (double)xf;
   if (isnan(x)) return NAN;

@@ -48,6 +48,7 @@ enum : int {
   STAT_MAX_GROUP_ROWS = 12,
   STAT_MAX_GROUP_BODIES = 13,
   STAT_ISLANDS_CAPPED = 14,
+  STAT_PRED_USED = 15,   // rows that started from the learned prediction
   STAT_COUNT = 16
 };
 
@@ -170,6 +171,9 @@ struct WorldGpu::Scratch {
   DBuf<unsigned long long> sap_key64, sap_key64b;                              // batched worlds: (world, min x)
   DBuf<uint32_t> sap_w;
   DBuf<float4> big_x, big_j;                                                   // big-island row stream
+  DBuf<float> feat, pred3, targets;                                            // learned warm start
+  DBuf<uint8_t> feat_valid;
+  DBuf<float4> pred_used, s_pred;
   // solve groups (islands packed for one CTA each) and their shared-memory residents
   DBuf<uint32_t> g_small_rows, g_small_pre, g_big, g_big_pre, g_of_isl, g_key, g_key2, g_start, g_cnt, g_class,
       body_grp, gb_key, gb_key2, gb_list, gb_tmp, gb_start, gb_cnt, body_local;

@@ -13,6 +13,7 @@
 #include <cub/cub.cuh>
 
 #include "step_internal.cuh"
+#include "warm_model.h"
 
 namespace rp {
 
@@ -953,12 +954,15 @@ __global__ void k_local_isl(uint32_t n, const uint32_t* __restrict__ ord, const 
 }
 struct SRowsV {
   uint2* loc; uint32_t* flags; float2* inv; float4 *ra, *rb, *n, *t1, *t2, *mu, *va, *vb; float* jn; float2* jt; int* wm;
+  float4* pred;  // learned warm start: (normal, friction 1, friction 2) in impulse units, w = 1 when valid
 };
 // Rows in schedule order, with local body indices and the constant velocity of a side that
 // cannot move (a static or sleeping body's velocity at the contact; zero for terrain).
 __global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, RowsV R, BodiesV B,
                                const uint32_t* __restrict__ body_local, const int* __restrict__ wm_idx,
-                               const uint32_t* __restrict__ row_lisl, SRowsV O) {
+                               const uint32_t* __restrict__ row_lisl, const float* __restrict__ pred3,
+                               const uint32_t* __restrict__ row_group, const uint32_t* __restrict__ g_class,
+                               float4* pred_used, uint32_t cold_only, SRowsV O) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t r = ord[s];
@@ -977,6 +981,13 @@ __global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, Row
   O.jn[s] = 0.0f;
   O.jt[s] = make_float2(0.0f, 0.0f);
   O.wm[s] = wm_idx[r];
+  // predictions reach every solver class except the global-memory one (islands beyond 4500 bodies)
+  float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // (cold_only: only rows the previous tick's cache has nothing for)
+  if (pred3 && g_class[row_group[r]] != 2u && (!cold_only || wm_idx[r] < 0))
+    p = make_float4(pred3[3 * r], pred3[3 * r + 1], pred3[3 * r + 2], 1.0f);
+  O.pred[s] = p;
+  if (pred_used) pred_used[r] = p;
 }
 
 // Shared-memory body state of one group
@@ -1140,6 +1151,55 @@ __device__ __forceinline__ void warm_core(float4* lin, float4* ang, const SRow& 
   if (ia) { lin[r.la] = f4(la, LA.w); ang[r.la] = f4(aa, AA.w); }
   if (ib) { lin[r.lb] = f4(lb, LB.w); ang[r.lb] = f4(ab, AB.w); }
 }
+// Learned warm start: the row's normal velocity error |bias - v_rel . n| after a candidate start
+// (applied to register copies, nothing written), and the choice between the previous tick's
+// impulse (or none) and the predicted one: the prediction is kept only when it leaves the smaller
+// error. Returns 1 when the prediction was applied.
+__device__ __forceinline__ float warm_trial_err(const float4* lin, const float4* ang, const SRow& r, const m3& qa,
+                                                const m3& qb, float ima, float imb, bool apply_start, float4 ea, float4 eb) {
+  const bool ha = r.la != 0xFFFFFFFFu, hb = !(r.flags & RF_TERRAIN) && r.lb != 0xFFFFFFFFu;
+  const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
+  f3 la = mk3(0, 0, 0), aa = la, lb = la, ab = la;
+  if (ha || ia) { la = xyz(lin[r.la]); aa = xyz(ang[r.la]); }
+  if (hb || ib) { lb = xyz(lin[r.lb]); ab = xyz(ang[r.lb]); }
+  auto rel = [&]() {
+    f3 va = ha ? la + cross(aa, r.ra) : r.vfix;
+    f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : (hb ? lb + cross(ab, r.rb) : r.vfix);
+    return vb - va;
+  };
+  if (apply_start) {
+    float jn = ea.w;
+    f3 jt = xyz(eb);
+    f3 imp = r.n * jn;
+    f3 v = rel();
+    float a = dot(v, r.t1), b = dot(v, r.t2);
+    float mu = mu_dynamic_s(r, sqrtf(a * a + b * b));
+    f3 t = clamp_length_max(mk3(dot(jt, r.t1), dot(jt, r.t2), 0.0f), mu * jn);
+    imp = imp + ((r.t1 * t.x) + (r.t2 * t.y));
+    if (ia) { f3 nj = -imp; impulse_reg(la, aa, ima, qa, nj, cross(r.ra, nj)); }
+    if (ib) impulse_reg(lb, ab, imb, qb, imp, cross(r.rb, imp));
+  }
+  return fabsf(r.bias - dot(rel(), r.n));
+}
+__device__ __forceinline__ int warm_select(float4* lin, float4* ang, const SRow& r, const m3& qa, const m3& qb, float ima,
+                                           float imb, bool has_ref, float4 ea, float4 eb, float4 pred, float& jn_acc,
+                                           float2& jt_acc) {
+  if (pred.w == 0.0f) {
+    if (has_ref) warm_core(lin, ang, r, qa, qb, ima, imb, ea, eb, jn_acc, jt_acc);
+    return 0;
+  }
+  const float su = r.m_n * kImpulseUnit;
+  float4 pa = make_float4(0.0f, 0.0f, 0.0f, rmax(pred.x * su, 0.0f));
+  float4 pb = f4((r.t1 * (pred.y * su)) + (r.t2 * (pred.z * su)));
+  float e_ref = warm_trial_err(lin, ang, r, qa, qb, ima, imb, has_ref, ea, eb);
+  float e_pred = warm_trial_err(lin, ang, r, qa, qb, ima, imb, true, pa, pb);
+  if (e_pred < e_ref) {
+    warm_core(lin, ang, r, qa, qb, ima, imb, pa, pb, jn_acc, jt_acc);
+    return 1;
+  }
+  if (has_ref) warm_core(lin, ang, r, qa, qb, ima, imb, ea, eb, jn_acc, jt_acc);
+  return 0;
+}
 __device__ __forceinline__ void pgs_row_reg(const SBodies& B, const SRow& r, uint32_t s, float* jn_arr, float2* jt_arr,
                                             float* dres) {
   const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
@@ -1250,13 +1310,22 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
   for (uint32_t i = tid; i < nisl; i += NT) { W.isl_res[i] = 0u; W.isl_last[i] = 0u; W.isl_sw[i] = 0u; W.isl_done[i] = 0; }
   __syncthreads();
   SBodies B{W.lin, W.ang, W.Iw, W.im};
+  uint32_t n_pred = 0;
   for (uint32_t L = 0; L < nl; ++L) {
     for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1]; i += NT) {
       int e = R.wm[base + i];
-      if (e >= 0) warm_apply_s(B, W.rows[i], i, wa[e], wb[e], W.jn, W.jt);
+      float4 p = R.pred[base + i];
+      if (e < 0 && p.w == 0.0f) continue;
+      const SRow& r = W.rows[i];
+      const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
+      const m3 qa = load_iw(ia ? B.Iw + 9 * (size_t)r.la : B.Iw), qb = load_iw(ib ? B.Iw + 9 * (size_t)r.lb : B.Iw);
+      n_pred += warm_select(B.lin, B.ang, r, qa, qb, ia ? B.im[r.la] : 0.0f, ib ? B.im[r.lb] : 0.0f, e >= 0,
+                            e >= 0 ? wa[e] : make_float4(0, 0, 0, 0), e >= 0 ? wb[e] : make_float4(0, 0, 0, 0), p,
+                            W.jn[i], W.jt[i]);
     }
     __syncthreads();
   }
+  if (n_pred) atomicAdd(&stats[STAT_PRED_USED], n_pred);
   int it = 0;
   while (it < iters) {
     for (uint32_t L = 0; L < nl; ++L) {
@@ -1460,7 +1529,8 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
   for (uint32_t L = 0; L < nl; ++L) {
     for (uint32_t s = lvl[L] + tid; s < lvl[L + 1]; s += CH) {
       int e = R.wm[s];
-      if (e < 0) continue;
+      float4 pr = R.pred[s];
+      if (e < 0 && pr.w == 0.0f) continue;
       SRow r = ld_srow(R, s);
       const float4* x = X + 7 * (size_t)s;
       float q[24];
@@ -1468,7 +1538,9 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
       m3 qa = mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
       m3 qb = mcols(mk3(q[12], q[13], q[14]), mk3(q[15], q[16], q[17]), mk3(q[18], q[19], q[20]));
       float jn = 0.0f; float2 jt = make_float2(0.0f, 0.0f);
-      warm_core(lin, ang, r, qa, qb, q[9], q[21], wa[e], wb[e], jn, jt);
+      if (warm_select(lin, ang, r, qa, qb, q[9], q[21], e >= 0, e >= 0 ? wa[e] : make_float4(0, 0, 0, 0),
+                      e >= 0 ? wb[e] : make_float4(0, 0, 0, 0), pr, jn, jt))
+        atomicAdd(&stats[STAT_PRED_USED], 1u);
       J[s] = make_float4(jn, jt.x, jt.y, 0.0f);
     }
     __threadfence_block();
@@ -1546,6 +1618,71 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
   }
 }
 
+// ------------------------------------------------------------------ learned warm start: features
+// 24 features per scheduled contact row (rows with no movable body stay invalid), in the
+// impulse unit u = m_n * kImpulseUnit where impulses appear:
+//   0-2 normal; 3-5 relative linear velocity (B - A); 6-8 relative angular velocity (B - A);
+//   9 depth x 10; 10-11 inverse masses x m_n; 12-14 A's angular response along n, t1, t2
+//   ((r x d) . Iw (r x d)) x m_n; 15-17 the same for B; 18 static friction; 19-21 the previous
+//   tick's impulse (normal, t1, t2) / u, 0 when cold; 22 1 when a previous impulse matched;
+//   23 depth bias x 0.1.
+__device__ __forceinline__ float ang_resp(const float* Iw, f3 r, f3 d) {
+  m3 M = mcols(mk3(Iw[0], Iw[1], Iw[2]), mk3(Iw[3], Iw[4], Iw[5]), mk3(Iw[6], Iw[7], Iw[8]));
+  f3 c = cross(r, d);
+  return dot(c, mvec(M, c));
+}
+__global__ void k_row_features(uint32_t nc, RowsV R, BodiesV B, const float4* __restrict__ c_pt,
+                               const int* __restrict__ wm_idx, const float4* __restrict__ wa, const float4* __restrict__ wb,
+                               float* feat, uint8_t* valid) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  float* f = feat + 24 * (size_t)k;
+  uint32_t fl = R.flags[k];
+  if (!(fl & (RF_WA | RF_WB))) { valid[k] = 0; for (int q = 0; q < 24; ++q) f[q] = 0.0f; return; }
+  valid[k] = 1;
+  uint2 ab = R.ab[k];
+  const bool terr = fl & RF_TERRAIN;
+  float4 ra = R.ra[k], rb = R.rb[k], n4 = R.n[k], t14 = R.t1[k], t24 = R.t2[k];
+  f3 n = xyz(n4), t1 = xyz(t14), t2 = xyz(t24);
+  float mn = ra.w, u = mn > 0.0f ? mn * kImpulseUnit : 1.0f;
+  float2 iv = R.inv[k];
+  f3 la = xyz(B.lin[ab.x]), aa = xyz(B.ang[ab.x]);
+  f3 lb = terr ? mk3(0, 0, 0) : xyz(B.lin[ab.y]), abv = terr ? mk3(0, 0, 0) : xyz(B.ang[ab.y]);
+  f3 dl = lb - la, da = abv - aa;
+  f[0] = n.x; f[1] = n.y; f[2] = n.z;
+  f[3] = dl.x; f[4] = dl.y; f[5] = dl.z;
+  f[6] = da.x; f[7] = da.y; f[8] = da.z;
+  f[9] = c_pt[k].w * 10.0f;
+  f[10] = iv.x * mn; f[11] = iv.y * mn;
+  for (int q = 12; q < 18; ++q) f[q] = 0.0f;
+  if (iv.x > 0.0f) {
+    const float* I = B.Iw + 9 * (size_t)ab.x;
+    f[12] = ang_resp(I, xyz(ra), n) * mn; f[13] = ang_resp(I, xyz(ra), t1) * mn; f[14] = ang_resp(I, xyz(ra), t2) * mn;
+  }
+  if (iv.y > 0.0f) {
+    const float* I = B.Iw + 9 * (size_t)ab.y;
+    f[15] = ang_resp(I, xyz(rb), n) * mn; f[16] = ang_resp(I, xyz(rb), t1) * mn; f[17] = ang_resp(I, xyz(rb), t2) * mn;
+  }
+  f[18] = R.mu[k].x;
+  int e = wm_idx[k];
+  if (e >= 0) {
+    f3 jt = xyz(wb[e]);
+    f[19] = wa[e].w / u; f[20] = dot(jt, t1) / u; f[21] = dot(jt, t2) / u; f[22] = 1.0f;
+  } else {
+    f[19] = f[20] = f[21] = 0.0f; f[22] = 0.0f;
+  }
+  f[23] = t14.w * 0.1f;
+}
+// The rows' converged impulses after the velocity sweeps, in the same unit (training targets).
+__global__ void k_row_targets(uint32_t nc, RowsV R, const float* __restrict__ acc_jn, const float2* __restrict__ acc_jt,
+                              float* t) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nc) return;
+  float mn = R.ra[k].w, u = mn > 0.0f ? mn * kImpulseUnit : 1.0f;
+  float2 jt = acc_jt[k];
+  t[3 * k] = acc_jn[k] / u; t[3 * k + 1] = jt.x / u; t[3 * k + 2] = jt.y / u;
+}
+
 // ------------------------------------------------------------------ small helpers
 __global__ void k_scatter_u32(uint32_t n, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ src, uint32_t* dst) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1609,6 +1746,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   cudaStream_t st = W.stream();
   const uint32_t nb = W.num_bodies(), nc = ctx.nc;
   uint32_t* stats = W.d_stats.p;
+  W.pred_valid_ = false;
   S.constrained.ensure(nb + 1); S.loaded.ensure(nb + 1); S.ballistic.ensure(nb + 1); S.touching.ensure(nb + 1);
   S.uf.ensure(nb + 1); S.uf2.ensure(nb + 1); S.body_level.ensure(nb + 1); S.root_mark.ensure(nb + 1);
   S.Iw.ensure(9 * (size_t)nb + 9);
@@ -1762,6 +1900,18 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     k_warm_match<<<nblk(nc), T, 0, st>>>(nc, S.r_ab.p, S.r_flags.p, S.r_la.p, W.warm_key.p, W.warm_a.p, W.n_warm,
                                          S.wm_idx.p, stats + STAT_WARM_MATCHED, stats + STAT_ERR); RP_COUNT_LAUNCH(1);
     k_warm_unscheduled<<<nblk(nc), T, 0, st>>>(nc, R, B, S.wm_idx.p, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p); RP_COUNT_LAUNCH(1);
+    // learned warm start: row features, and the model's prediction of every row's impulse
+    const bool learned = W.model_ != nullptr;
+    if (learned || W.feat_log_) {
+      S.feat.ensure(24 * (size_t)nc + 24); S.feat_valid.ensure(nc + 1);
+      k_row_features<<<nblk(nc), T, 0, st>>>(nc, R, B, S.c_pt.p, S.wm_idx.p, W.warm_a.p, W.warm_b.p, S.feat.p,
+                                             S.feat_valid.p); RP_COUNT_LAUNCH(1);
+    }
+    if (learned) {
+      S.pred3.ensure(3 * (size_t)nc + 3); S.pred_used.ensure(nc + 1);
+      W.model_->predict(nc, S.feat.p, S.pred3.p, true, st);
+    }
+    W.pred_valid_ = learned;
     P.end(PH_WARM_MATCH, st);
     P.begin(PH_VEL_SOLVE, st);
     // ---- warm application + velocity sweeps
@@ -1773,10 +1923,13 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       S.s_loc.ensure(nsched + 1); S.s_flags.ensure(nsched + 1); S.s_inv.ensure(nsched + 1); S.s_ra.ensure(nsched + 1);
       S.s_rb.ensure(nsched + 1); S.s_n.ensure(nsched + 1); S.s_t1.ensure(nsched + 1); S.s_t2.ensure(nsched + 1);
       S.s_mu.ensure(nsched + 1); S.s_va.ensure(nsched + 1); S.s_vb.ensure(nsched + 1); S.s_jn.ensure(nsched + 1);
-      S.s_jt.ensure(nsched + 1); S.s_wm.ensure(nsched + 1);
+      S.s_jt.ensure(nsched + 1); S.s_wm.ensure(nsched + 1); S.s_pred.ensure(nsched + 1);
+      if (learned) RP_CUDA(cudaMemsetAsync(S.pred_used.p, 0, 16 * (size_t)nc, st));  // unscheduled rows: none
       SRowsV SR{S.s_loc.p, S.s_flags.p, S.s_inv.p, S.s_ra.p, S.s_rb.p, S.s_n.p, S.s_t1.p, S.s_t2.p, S.s_mu.p, S.s_va.p,
-                S.s_vb.p, S.s_jn.p, S.s_jt.p, S.s_wm.p};
-      k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, S.row_lisl.p, SR); RP_COUNT_LAUNCH(1);
+                S.s_vb.p, S.s_jn.p, S.s_jt.p, S.s_wm.p, S.s_pred.p};
+      k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, S.row_lisl.p,
+                                                 learned ? S.pred3.p : nullptr, S.row_isl2.p, S.g_class.p,
+                                                 learned ? S.pred_used.p : nullptr, W.pred_cold_only_ ? 1u : 0u, SR); RP_COUNT_LAUNCH(1);
       const float tol = resid_mode ? W.res_tol_ : 0.0f;
       // dynamic shared memory above the 48 KB default, opted into once per device
       const OnchipLayout lay_packed = onchip_layout(WG_ROWS, WG_BODIES, WG_ROWS);
@@ -1858,6 +2011,10 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       }
     }
     P.end(PH_VEL_SOLVE, st);
+    if (W.feat_log_) {
+      S.targets.ensure(3 * (size_t)nc + 3);
+      k_row_targets<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.targets.p); RP_COUNT_LAUNCH(1);
+    }
     P.begin(PH_WARM_CACHE, st);
     // ---- warm-start cache for the next tick (solver.rs:917-944)
     {

@@ -317,6 +317,35 @@ void WorldGpu::add_bodies_bulk(uint32_t n, const float* pose7, const float* vel6
   if (batch_) worlds_dirty_ = true;
 }
 
+// The last tick's feature rows (24 floats) and converged impulses (3 floats) of the contacts that
+// had a movable body, in contact order (the learned warm start's training data).
+void WorldGpu::get_row_features(std::vector<float>& feats, std::vector<float>& targets) {
+  feats.clear(); targets.clear();
+  uint32_t n = n_contacts;
+  if (!feat_log_ || !n || s_->feat.cap < 24 * (size_t)n || s_->targets.cap < 3 * (size_t)n) return;
+  std::vector<float> f(24 * (size_t)n), t(3 * (size_t)n);
+  std::vector<uint8_t> v(n);
+  RP_CUDA(cudaMemcpyAsync(f.data(), s_->feat.p, 4 * f.size(), cudaMemcpyDeviceToHost, stream_));
+  RP_CUDA(cudaMemcpyAsync(t.data(), s_->targets.p, 4 * t.size(), cudaMemcpyDeviceToHost, stream_));
+  RP_CUDA(cudaMemcpyAsync(v.data(), s_->feat_valid.p, n, cudaMemcpyDeviceToHost, stream_));
+  RP_CUDA(cudaStreamSynchronize(stream_));
+  for (uint32_t k = 0; k < n; ++k) {
+    if (!v[k]) continue;
+    feats.insert(feats.end(), f.begin() + 24 * (size_t)k, f.begin() + 24 * (size_t)(k + 1));
+    targets.insert(targets.end(), t.begin() + 3 * (size_t)k, t.begin() + 3 * (size_t)(k + 1));
+  }
+}
+// The predictions the last tick's warm start was offered, per contact in contact order:
+// (normal, friction 1, friction 2, 1) or zeros where none was (no model, no movable body, or an
+// island solved over global memory).
+void WorldGpu::get_row_predictions(std::vector<float>& pred4) {
+  uint32_t n = n_contacts;
+  pred4.assign(4 * (size_t)n, 0.0f);
+  if (!pred_valid_ || !n) return;
+  RP_CUDA(cudaMemcpyAsync(pred4.data(), s_->pred_used.p, 16 * (size_t)n, cudaMemcpyDeviceToHost, stream_));
+  RP_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void WorldGpu::begin_world() {
   batch_ = true;
   h_wb_start_.push_back(nb_);
@@ -504,6 +533,7 @@ const StepStatsHost& WorldGpu::stats() {
     st_.max_group_rows = h[STAT_MAX_GROUP_ROWS];
     st_.max_group_bodies = h[STAT_MAX_GROUP_BODIES];
     st_.islands_capped = h[STAT_ISLANDS_CAPPED];
+    st_.pred_used = h[STAT_PRED_USED];
     stats_dirty_ = false;
   }
   st_.warm_entries = n_warm;

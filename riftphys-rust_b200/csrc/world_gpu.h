@@ -21,13 +21,15 @@
 
 namespace rp {
 
+class WarmModel;
+
 struct StepStatsHost {
   uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
   uint32_t sweeps = 0, bounce_skipped = 0, warm_entries = 0, sleeping = 0, error_flags = 0;
   float residual = 0.0f;
   uint32_t row_sweeps = 0, rows_scheduled = 0;
   uint32_t groups_shared = 0, groups_global = 0, max_group_rows = 0, max_group_bodies = 0;
-  uint32_t islands_capped = 0;
+  uint32_t islands_capped = 0, pred_used = 0;
 };
 
 struct PairPropsHost { float mu_s, mu_k, restitution, stribeck_v, stiffness; };
@@ -113,6 +115,12 @@ class WorldGpu {
   static void snapshot_free(SnapshotGpu* s);
 
   cudaStream_t stream() const { return stream_; }
+  // learned warm start: a model (owned by the caller) predicting each row's start, and logging of
+  // the rows' features and converged impulses (its training data)
+  WarmModel* model_ = nullptr;
+  bool feat_log_ = false, pred_valid_ = false, pred_cold_only_ = false;
+  void get_row_features(std::vector<float>& feats, std::vector<float>& targets);
+  void get_row_predictions(std::vector<float>& pred4);
   // side streams the velocity solve forks onto (independent solve groups run concurrently)
   static constexpr int kAux = 6;
   cudaStream_t aux_[kAux] = {};
