@@ -136,6 +136,63 @@ def peak_hbm():
         return 6650.0, "fallback"
 
 
+def job_throughput(local_units, local_ms, dist=None, device="cpu"):
+    """Whole-job throughput over the ranks: units summed over ranks (each rank steps its own worlds
+    or replica) over the slowest rank's device time. Returns (units per second, max ms, total units).
+    Every rank makes the same two collective calls."""
+    import torch
+    units = torch.tensor([float(local_units)], dtype=torch.float64, device=device)
+    ms = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    if dist is not None and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(units, op=dist.ReduceOp.SUM)
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    total, ms_max = float(units.item()), float(ms.item())
+    return total / (ms_max / 1000.0), ms_max, total
+
+
+def peak_bf16():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def run_model(args, lib, torch):
+    """The learned warm start's MLP alone: predictions for --rows device-resident rows per step
+    (the inference a tick runs for its contact rows), timed on the device; tensor roofline."""
+    rows = args.rows
+    m = lib.model(seed=2)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    feats = torch.randn(rows, 24, device="cuda", generator=g, dtype=torch.float32)
+    out = torch.empty(rows, 3, device="cuda", dtype=torch.float32)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        m.predict_device(feats.data_ptr(), rows, out.data_ptr(), stream.cuda_stream)
+    launches0 = lib.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        m.predict_device(feats.data_ptr(), rows, out.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    padded = (rows + 127) // 128 * 128
+    flops = 2.0 * padded * (32 * 128 + 2 * 128 * 128 + 128 * 16)  # the padded products the GEMMs run
+    peak, kind = peak_bf16()
+    achieved = flops / (ms / 1000.0) / 1e12
+    line = {"metric": "warm-start model rows/s", "value": rows / (ms / 1000.0), "unit": "rows/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": f"MLP 24-128-128-128-3 (SiLU) forward on {rows:,} rows, bf16 x bf16 -> f32 on tcgen05"},
+            "roofline": {"kernel": "k_tc_gemm (4 products + activations)", "bound": "tensor", "unit": "TFLOP/s",
+                         "achieved": achieved, "peak": peak, "peak_source": kind, "frac": achieved / peak,
+                         "traffic": None, "flops_per_step": flops},
+            "gpu_launches": lib.launch_count() - launches0}
+    print(json.dumps(line), flush=True)
+
+
 def oracle_path():
     p = os.path.join(ROOT, "oracle", "build", "liboracle_rphys.so")
     if not os.path.exists(p):
@@ -187,7 +244,8 @@ def main():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--settle", type=int, default=240)
-    ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop", "batch"])
+    ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop", "batch", "model"])
+    ap.add_argument("--rows", type=int, default=1 << 20, help="model: rows per step")
     ap.add_argument("--worlds", type=int, default=4096, help="batch: number of worlds")
     ap.add_argument("--learned", type=int, default=1, help="terrain: also time the learned warm start (1/0)")
     ap.add_argument("--mode", default="residual", choices=["residual", "fixed"])
@@ -208,6 +266,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
     lib = rp.load_product()
+    if args.config == "model":
+        return run_model(args, lib, torch)
     w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, worlds=args.worlds, rank=rank)
     if args.mode == "residual":
         w.set_residual_mode(TOL, 4 * ITERS[args.config])
@@ -254,11 +314,7 @@ def main():
         dist.barrier()
     ms = e0.elapsed_time(e1)
     st = w.stats()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world_size > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = nb * args.steps * world_size / (ms_max / 1000.0)
+    value, ms_max, _ = job_throughput(nb * args.steps, ms, dist, "cuda")
 
     # e2e: the drop-in C-ABI call with the tick's state read back to host memory every tick
     import numpy as np

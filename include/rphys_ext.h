@@ -168,6 +168,10 @@ uint32_t rphys_ext_model_num_params(void);
 RPhysResult rphys_ext_model_get_weights(const RPhysWarmModel* model, float* out, uint32_t count);
 RPhysResult rphys_ext_model_set_weights(RPhysWarmModel* model, const float* in, uint32_t count);
 RPhysResult rphys_ext_model_predict(RPhysWarmModel* model, const float* feats24, uint32_t rows, float* out3);
+/* The same with device pointers (24 floats in, 3 out per row) on the given CUDA stream (0: the
+ * model's own); returns after the predictions are written. */
+RPhysResult rphys_ext_model_predict_device(RPhysWarmModel* model, const float* dev_feats24, uint32_t rows, float* dev_out3,
+                                           uint64_t cuda_stream);
 /* One forward/backward pass (mean squared error over the 3 outputs): gradients of every weight. */
 RPhysResult rphys_ext_model_gradients(RPhysWarmModel* model, const float* feats24, const float* targets3, uint32_t rows,
                                       float* out_grads, float* out_loss);

@@ -650,6 +650,9 @@ uint32_t rphys_ext_model_num_params(void) { return 39312u; }
 RPhysResult rphys_ext_model_get_weights(const RPhysWarmModel*, float*, uint32_t) { return fail(RPHYS_ERR_BAD_ARG, "model: GPU only"); }
 RPhysResult rphys_ext_model_set_weights(RPhysWarmModel*, const float*, uint32_t) { return fail(RPHYS_ERR_BAD_ARG, "model: GPU only"); }
 RPhysResult rphys_ext_model_predict(RPhysWarmModel*, const float*, uint32_t, float*) { return fail(RPHYS_ERR_BAD_ARG, "model: GPU only"); }
+RPhysResult rphys_ext_model_predict_device(RPhysWarmModel*, const float*, uint32_t, float*, uint64_t) {
+  return fail(RPHYS_ERR_BAD_ARG, "model: GPU only");
+}
 RPhysResult rphys_ext_model_gradients(RPhysWarmModel*, const float*, const float*, uint32_t, float*, float*) {
   return fail(RPHYS_ERR_BAD_ARG, "model: GPU only");
 }

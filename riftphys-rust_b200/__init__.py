@@ -177,6 +177,7 @@ ABI = [
     ("rphys_ext_model_get_weights", c_uint32, [c_void_p, c_void_p, c_uint32]),
     ("rphys_ext_model_set_weights", c_uint32, [c_void_p, c_void_p, c_uint32]),
     ("rphys_ext_model_predict", c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p]),
+    ("rphys_ext_model_predict_device", c_uint32, [c_void_p, c_void_p, c_uint32, c_void_p, c_uint64]),
     ("rphys_ext_model_gradients", c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, POINTER(c_float)]),
     ("rphys_ext_model_train", c_uint32, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_float,
                                          POINTER(c_float)]),
@@ -560,6 +561,10 @@ class WarmModel:
         out = np.zeros((len(f), 3), dtype=np.float32)
         self.lib.call("rphys_ext_model_predict", self.h, f.ctypes.data_as(c_void_p), len(f), out.ctypes.data_as(c_void_p))
         return out
+
+    def predict_device(self, feats_ptr, rows, out_ptr, stream=0):
+        """Device pointers (e.g. torch tensors' data_ptr()); runs on `stream` (a cudaStream_t)."""
+        self.lib.call("rphys_ext_model_predict_device", self.h, c_void_p(feats_ptr), rows, c_void_p(out_ptr), stream)
 
     def gradients(self, feats, targets):
         import numpy as np

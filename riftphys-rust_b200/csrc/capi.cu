@@ -733,6 +733,7 @@ RPhysResult rphys_ext_launch_count(uint64_t* out) {
 struct RPhysWarmModel {
   std::mutex mu;
   std::unique_ptr<rp::WarmModel> m;
+  std::mutex& m_mu() { return mu; }
 };
 extern "C" {
 RPhysWarmModel* rphys_ext_model_create(uint64_t seed) {
@@ -769,6 +770,15 @@ RPhysResult rphys_ext_model_predict(RPhysWarmModel* M, const float* f, uint32_t 
   clear_err();
   if (!M || (n && (!f || !out))) return fail(RPHYS_ERR_NULL, "rphys_ext_model_predict: null arg");
   return guard("rphys_ext_model_predict", [&]() { std::lock_guard<std::mutex> g(M->mu); M->m->predict(n, f, out, false); return (RPhysResult)RPHYS_OK; });
+}
+RPhysResult rphys_ext_model_predict_device(RPhysWarmModel* M, const float* d_f, uint32_t n, float* d_out, uint64_t stream) {
+  clear_err();
+  if (!M || (n && (!d_f || !d_out))) return fail(RPHYS_ERR_NULL, "rphys_ext_model_predict_device: null arg");
+  return guard("rphys_ext_model_predict_device", [&]() {
+    std::lock_guard<std::mutex> g(M->m_mu());
+    M->m->predict(n, d_f, d_out, true, reinterpret_cast<cudaStream_t>(stream));
+    return (RPhysResult)RPHYS_OK;
+  });
 }
 RPhysResult rphys_ext_model_gradients(RPhysWarmModel* M, const float* f, const float* t, uint32_t n, float* grads, float* loss) {
   clear_err();
