@@ -1,5 +1,5 @@
 // step_front.cu -- stages 1 and 2 of the tick on the GPU: forces, AABBs and swept AABBs,
-// the sweep-and-prune broadphase, pair and terrain narrowphase, contact culling and orientation.
+// the uniform-grid broadphase, pair and terrain narrowphase, contact culling and orientation.
 // Reference: riftphys-world/src/world/step.rs:53-150, 499-542; broadphase.rs:29-99;
 // narrowphase.rs; terrain.rs:300-358.
 #include <cub/cub.cuh>
@@ -84,58 +84,91 @@ __global__ void k_aabbs(int ncol, const uint32_t* __restrict__ cbody, const uint
 __device__ __forceinline__ bool overlaps4(float4 amn, float4 amx, float4 bmn, float4 bmx) {
   return !(amx.x < bmn.x || amn.x > bmx.x || amx.y < bmn.y || amn.y > bmx.y || amx.z < bmn.z || amn.z > bmx.z);
 }
-__device__ __forceinline__ uint32_t sortable(float f) {
-  uint32_t u = fbits(f);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+// ------------------------------------------------------------------ uniform grid (2.5 m cells)
+// The reference's own grid (broadphase.rs:29-81): each in-grid collider goes into every cell its
+// swept AABB spans (cell = floor(v / 2.5) as i32, saturating, NaN -> 0); colliders sharing a cell
+// are tested with the inclusive overlap. On the GPU the (world, cell) keys are sorted, and a
+// pair is emitted only from its home cell -- the cell of the min corner of the two AABBs'
+// intersection, which both span -- so each overlapping pair comes out once per home-cell key
+// (a later sort + unique removes any repeats). Cell coordinates are packed 14 bits each
+// (wrapping beyond +-8192 cells only merges distant cells into one key: more tests, same set).
+#define GRID_CELL 2.5f
+__device__ __forceinline__ int grid_cell(float v) {
+  float f = floorf(v / GRID_CELL);
+  if (isnan(f)) return 0;
+  if (f >= 2147483647.0f) return 2147483647;
+  if (f <= -2147483648.0f) return (int)0x80000000;
+  return (int)f;
 }
-__global__ void k_sap_keys(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ smin, uint32_t* keys) {
+__device__ __forceinline__ unsigned long long grid_key(uint32_t world, int x, int y, int z) {
+  return ((unsigned long long)world << 42) | ((unsigned long long)((uint32_t)(x + 8192) & 0x3FFFu) << 28) |
+         ((unsigned long long)((uint32_t)(y + 8192) & 0x3FFFu) << 14) | (unsigned long long)((uint32_t)(z + 8192) & 0x3FFFu);
+}
+// cell range of one dimension, at most 6 cells (an in-grid AABB spans <= 12.5 m; more means a
+// non-finite extent, already flagged by k_aabbs)
+__device__ __forceinline__ void grid_span(float lo, float hi, int* c0, int* n) {
+  int a = grid_cell(lo), b = grid_cell(hi);
+  long long w = (long long)b - (long long)a + 1;
+  *c0 = a;
+  *n = w < 0 ? 0 : (w > 6 ? 6 : (int)w);
+}
+__global__ void k_grid_count(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ smin,
+                             const float4* __restrict__ smax, uint32_t* cnt) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) keys[k] = sortable(smin[ids[k]].x);
+  if (k >= n) return;
+  uint32_t c = ids[k];
+  float4 mn = smin[c], mx = smax[c];
+  int x0, nx, y0, ny, z0, nz;
+  grid_span(mn.x, mx.x, &x0, &nx); grid_span(mn.y, mx.y, &y0, &ny); grid_span(mn.z, mx.z, &z0, &nz);
+  cnt[k] = (uint32_t)(nx * ny * nz);
 }
-__global__ void k_gather_minx(int n, const uint32_t* __restrict__ order, const float4* __restrict__ smin, float* minx) {
+__global__ void k_grid_emit(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ smin,
+                            const float4* __restrict__ smax, const uint32_t* __restrict__ col_world,
+                            const uint32_t* __restrict__ off, unsigned long long* keys, uint32_t* vals) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) minx[k] = smin[order[k]].x;
-}
-// Batched worlds: the sort key puts the world above min.x, so each world's colliders are one run
-// of the sorted order and the sweep stops at the end of its run.
-__global__ void k_sap_keys_world(int n, const uint32_t* __restrict__ ids, const float4* __restrict__ smin,
-                                 const uint32_t* __restrict__ col_world, unsigned long long* keys) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) { uint32_t c = ids[k]; keys[k] = ((unsigned long long)col_world[c] << 32) | sortable(smin[c].x); }
-}
-__global__ void k_gather_world(int n, const uint32_t* __restrict__ order, const uint32_t* __restrict__ col_world,
-                               uint32_t* wsorted) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) wsorted[k] = col_world[order[k]];
-}
-// Sweep along x over the sorted in-grid colliders: every overlapping pair once, counted by the
-// earlier of the two in sort order. The set equals the grid's (broadphase.rs:49-81): two
-// finite AABBs that overlap share the cell of any point of their intersection.
-template <bool EMIT>
-__global__ void k_sap_sweep(int n, const uint32_t* __restrict__ order, const float* __restrict__ minx,
-                            const float4* __restrict__ smin, const float4* __restrict__ smax,
-                            uint32_t* cnt, const uint32_t* __restrict__ off, unsigned long long* out,
-                            const uint32_t* __restrict__ wsorted = nullptr) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  uint32_t i = order[p];
-  float4 imn = smin[i], imx = smax[i];
-  uint32_t c = 0, o = EMIT ? off[p] : 0;
-  const uint32_t wp = wsorted ? wsorted[p] : 0u;
-  for (int q = p + 1; q < n; ++q) {
-    if (wsorted && wsorted[q] != wp) break;  // the next world's run
-    if (minx[q] > imx.x) break;
-    uint32_t j = order[q];
-    if (overlaps4(imn, imx, smin[j], smax[j])) {
-      if (EMIT) {
-        uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
-        out[o + c] = ((unsigned long long)lo << 32) | hi;
+  if (k >= n) return;
+  uint32_t c = ids[k], w = col_world ? col_world[c] : 0u;
+  float4 mn = smin[c], mx = smax[c];
+  int x0, nx, y0, ny, z0, nz;
+  grid_span(mn.x, mx.x, &x0, &nx); grid_span(mn.y, mx.y, &y0, &ny); grid_span(mn.z, mx.z, &z0, &nz);
+  uint32_t o = off[k];
+  for (int x = 0; x < nx; ++x)
+    for (int y = 0; y < ny; ++y)
+      for (int z = 0; z < nz; ++z) {
+        keys[o] = grid_key(w, x0 + x, y0 + y, z0 + z);
+        vals[o] = c;
+        o++;
       }
-      c++;
-    }
-  }
-  if (!EMIT) cnt[p] = c;
 }
+template <bool EMIT>
+__global__ void k_grid_pairs(uint32_t n, const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ vals,
+                             const float4* __restrict__ smin, const float4* __restrict__ smax,
+                             const uint32_t* __restrict__ col_world, uint32_t* cnt, const uint32_t* __restrict__ off,
+                             unsigned long long* out) {
+  uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const unsigned long long key = keys[e];
+  const uint32_t i = vals[e];
+  const float4 imn = smin[i], imx = smax[i];
+  const uint32_t w = col_world ? col_world[i] : 0u;
+  uint32_t c = 0, o = EMIT ? off[e] : 0;
+  for (uint32_t f = e + 1; f < n && keys[f] == key; ++f) {
+    uint32_t j = vals[f];
+    if (j == i) continue;
+    float4 jmn = smin[j], jmx = smax[j];
+    if (!overlaps4(imn, imx, jmn, jmx)) continue;
+    unsigned long long home = grid_key(w, grid_cell(fmaxf(imn.x, jmn.x)), grid_cell(fmaxf(imn.y, jmn.y)),
+                                       grid_cell(fmaxf(imn.z, jmn.z)));
+    if (home != key) continue;
+    if (EMIT) {
+      uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
+      out[o + c] = ((unsigned long long)lo << 32) | hi;
+    }
+    c++;
+  }
+  if (!EMIT) cnt[e] = c;
+}
+
 // Oversized colliders against every collider (broadphase.rs:83-92), one thread per collider.
 // Batched worlds: only the oversized colliders of c's own world (a contiguous run of the
 // collider-ordered list, found by binary search on the world's collider range).
@@ -454,30 +487,25 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
     cudaStreamSynchronize(st);
     n_sap = hc[0]; n_over = hc[1];
   }
-  S.sap_key.ensure(n_sap + 1); S.sap_key2.ensure(n_sap + 1); S.sap_ord.ensure(n_sap + 1); S.minx.ensure(n_sap + 1);
   S.sap_cnt.ensure(n_sap + 1); S.sap_off.ensure(n_sap + 1);
   S.ov_cnt.ensure(ncol + 1); S.ov_off.ensure(ncol + 1);
-  uint32_t n_sap_pairs = 0, n_ov_pairs = 0;
+  uint32_t n_sap_pairs = 0, n_ov_pairs = 0, n_ent = 0;
   const bool batched = W.batched();
-  const uint32_t* wsorted = nullptr;
+  const uint32_t* cw = batched ? W.col_world.p : nullptr;
   if (n_sap > 0) {
-    if (batched) {
-      uint32_t nw = W.num_worlds();
-      int wbits = 1;
-      while ((1u << wbits) < nw && wbits < 31) wbits++;
-      S.sap_key64.ensure(n_sap + 1); S.sap_key64b.ensure(n_sap + 1); S.sap_w.ensure(n_sap + 1);
-      k_sap_keys_world<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, W.col_world.p, S.sap_key64.p); RP_COUNT_LAUNCH(1);
-      sort_pairs_u64(S, S.sap_key64.p, S.sap_key64b.p, S.sap_ids.p, S.sap_ord.p, n_sap, 0, 32 + wbits, st);
-      k_gather_world<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, W.col_world.p, S.sap_w.p); RP_COUNT_LAUNCH(1);
-      wsorted = S.sap_w.p;
-    } else {
-      k_sap_keys<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.sap_key.p); RP_COUNT_LAUNCH(1);
-      sort_pairs_u32(S, S.sap_key.p, S.sap_key2.p, S.sap_ids.p, S.sap_ord.p, n_sap, 0, 32, st);
-    }
-    k_gather_minx<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.smin.p, S.minx.p); RP_COUNT_LAUNCH(1);
-    k_sap_sweep<false><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, S.sap_cnt.p,
-                                                           nullptr, nullptr, wsorted); RP_COUNT_LAUNCH(1);
-    n_sap_pairs = exclusive_scan_total(S, S.sap_cnt.p, S.sap_off.p, n_sap, st);
+    // grid entries: one per (collider, spanned cell), sorted by (world, cell) key
+    k_grid_count<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.smax.p, S.sap_cnt.p); RP_COUNT_LAUNCH(1);
+    n_ent = exclusive_scan_total(S, S.sap_cnt.p, S.sap_off.p, n_sap, st);
+    S.sap_key64.ensure(n_ent + 1); S.sap_key64b.ensure(n_ent + 1); S.sap_ord.ensure(n_ent + 1); S.sap_w.ensure(n_ent + 1);
+    k_grid_emit<<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ids.p, S.smin.p, S.smax.p, cw, S.sap_off.p, S.sap_key64.p,
+                                                    S.sap_ord.p); RP_COUNT_LAUNCH(1);
+    int wbits = 0;
+    if (batched) while ((1u << wbits) < W.num_worlds() && wbits < 22) wbits++;
+    sort_pairs_u64(S, S.sap_key64.p, S.sap_key64b.p, S.sap_ord.p, S.sap_w.p, n_ent, 0, 42 + wbits, st);
+    S.gp_cnt.ensure(n_ent + 1); S.gp_off.ensure(n_ent + 1);
+    k_grid_pairs<false><<<(n_ent + T - 1) / T, T, 0, st>>>(n_ent, S.sap_key64b.p, S.sap_w.p, S.smin.p, S.smax.p, cw,
+                                                           S.gp_cnt.p, nullptr, nullptr); RP_COUNT_LAUNCH(1);
+    n_sap_pairs = exclusive_scan_total(S, S.gp_cnt.p, S.gp_off.p, n_ent, st);
   }
   if (n_over > 0 && ncol > 0) {
     k_oversized<false><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, S.ov_cnt.p,
@@ -488,8 +516,8 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   uint32_t n_raw = n_sap_pairs + n_ov_pairs;
   S.pairs.ensure(n_raw + 1); S.pairs2.ensure(n_raw + 1); S.flag8.ensure(n_raw + 1);
   if (n_sap_pairs > 0)
-    k_sap_sweep<true><<<(n_sap + T - 1) / T, T, 0, st>>>(n_sap, S.sap_ord.p, S.minx.p, S.smin.p, S.smax.p, nullptr,
-                                                          S.sap_off.p, S.pairs2.p, wsorted); RP_COUNT_LAUNCH(1);
+    k_grid_pairs<true><<<(n_ent + T - 1) / T, T, 0, st>>>(n_ent, S.sap_key64b.p, S.sap_w.p, S.smin.p, S.smax.p, cw, nullptr,
+                                                          S.gp_off.p, S.pairs2.p); RP_COUNT_LAUNCH(1);
   if (n_ov_pairs > 0)
     k_oversized<true><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, nullptr,
                                                          S.ov_off.p, S.pairs2.p + n_sap_pairs, batched ? W.col_world.p : nullptr,

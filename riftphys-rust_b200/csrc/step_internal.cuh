@@ -169,7 +169,7 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> row_islid, row_lisl, li_flag, li_pre, g_nisl;                 // islands inside solve groups
   DBuf<uint32_t> cls_cnt, cls_list;                                            // solve groups by class
   DBuf<unsigned long long> sap_key64, sap_key64b;                              // batched worlds: (world, min x)
-  DBuf<uint32_t> sap_w;
+  DBuf<uint32_t> sap_w, gp_cnt, gp_off;
   DBuf<float4> big_x, big_j;                                                   // big-island row stream
   DBuf<float> feat, pred3, targets;                                            // learned warm start
   DBuf<uint8_t> feat_valid;

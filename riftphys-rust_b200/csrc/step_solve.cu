@@ -834,7 +834,9 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
 // of it on chip; 0, a bigger island, by one CTA with its body velocities on chip and its rows
 // streamed through a cp.async double buffer; 2, an island beyond that, by one warp over global
 // memory.
+#ifndef GROUP_ROWS
 #define GROUP_ROWS 32u
+#endif
 // big islands (classes 20..22): bodies and level starts held in shared memory, rows per staged
 // chunk (= threads per CTA) -- sized per bucket so that smaller ones share an SM
 #define BIG_BUCKETS 3
@@ -1256,7 +1258,9 @@ __host__ __device__ inline OnchipLayout onchip_layout(uint32_t RC, uint32_t BC, 
   L.bytes = o;
   return L;
 }
+#ifndef ONCHIP_T_PACKED
 #define ONCHIP_T_PACKED 64   // threads of a packed-group block (levels of up to 63 rows in one pass)
+#endif
 #define ONCHIP_T_ISLAND 128  // threads of a single-island block (wide first levels of terrain piles)
 template <bool MULTI, int NT>
 __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32_t g0, uint32_t ng,
