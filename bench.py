@@ -60,7 +60,7 @@ BYTES = {
 }
 
 
-ITERS = {"terrain": 20, "box_drop": 8, "batch": 16}
+ITERS = {"terrain": 20, "box_drop": 8, "batch": 16, "ragdolls": 24}
 
 
 def build_scene(lib, config, n_bodies=None, area=None, hf_n=None, worlds=4096, rank=0):
@@ -75,6 +75,33 @@ def build_scene(lib, config, n_bodies=None, area=None, hf_n=None, worlds=4096, r
         return w, dt, total, (f"batch: {worlds} independent worlds stepped together ({total:,} bodies), body counts "
                               "log-uniform in [16, 4096], alternately square box pyramids and random box piles "
                               "(half-extents U[0.25, 0.75] m, 1000 kg/m^3) on 50x0.5x50 ground boxes, dt 1/60, 16 iters")
+    if config == "ragdolls":
+        # worlds of 5 ragdolls each (15 capsules, 14 ball / hinge joints with limits), all on the same
+        # 128^2 heightfield; the worlds' joints added in world order in one call
+        import numpy as np
+        per = 5
+        h, origin = scenes.heightfield(128, 1.0, 5)
+        parts = [scenes.ragdoll_arrays(rp, per, 1000 * (rank + 1) + k, 0.8 * 127, base_id=1,
+                                       y0=float(h.max()) + 1.0) for k in range(worlds)]
+        total = sum(len(b) for b, _, _ in parts)
+        w = lib.world(total + 16, total + 16)
+        w.set_heightfield(h, 128, 128, 1.0, 1.0, origin, origin, material=4)
+        w.set_pair_props(0, 0, 0.6, 0.5, 0.0, 0.08)
+        w.set_pair_props(0, 4, 0.883176, 0.724569, 0.0, 0.1)
+        w.set_iterations(24, 24)
+        jds, lds, nj = [], [], 0
+        for bd, jd, ld in parts:
+            _, first = w.add_world(bd)
+            jd[:, 2:4].view(np.uint32)[:] += first - 1
+            ld[:, 0].view(np.uint32)[:] += nj
+            nj += len(jd)
+            jds.append(jd); lds.append(ld)
+        w.add_joint_array(np.concatenate(jds))
+        w.set_joint_limit_array(np.concatenate(lds))
+        return w, 1.0 / 120.0, total, (f"ragdolls: {worlds} independent worlds of {per} ragdolls ({total:,} capsule "
+                                       f"bodies, {nj:,} joints: balls with +-45 deg swing limits, hinges limited to "
+                                       "[-120, 0] deg; capsule r U[0.05, 0.12] m, segment U[0.2, 0.5] m, 1-8 kg) on one "
+                                       "128^2 heightfield, dt 1/120, 24 iters")
     if config == "box_drop":
         side = max(1, round((n_bodies or 1000) ** (1.0 / 3.0)))
         w = lib.world(side ** 3 + 24, side ** 3 + 24)
@@ -244,9 +271,9 @@ def main():
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--settle", type=int, default=240)
-    ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop", "batch", "model"])
+    ap.add_argument("--config", default="terrain", choices=["terrain", "box_drop", "batch", "ragdolls", "model"])
     ap.add_argument("--rows", type=int, default=1 << 20, help="model: rows per step")
-    ap.add_argument("--worlds", type=int, default=4096, help="batch: number of worlds")
+    ap.add_argument("--worlds", type=int, default=None, help="batch / ragdolls: number of worlds (4096 / 2000)")
     ap.add_argument("--learned", type=int, default=1, help="terrain: also time the learned warm start (1/0)")
     ap.add_argument("--mode", default="residual", choices=["residual", "fixed"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -268,7 +295,8 @@ def main():
     lib = rp.load_product()
     if args.config == "model":
         return run_model(args, lib, torch)
-    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, worlds=args.worlds, rank=rank)
+    worlds = args.worlds or (2000 if args.config == "ragdolls" else 4096)
+    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, worlds=worlds, rank=rank)
     if args.mode == "residual":
         w.set_residual_mode(TOL, 4 * ITERS[args.config])
     # settle into the contact regime, then warm up
@@ -407,7 +435,7 @@ def main():
                    "note": "same timed ticks replayed from the snapshot; per-tick stats read between ticks"}
 
     rollback = None
-    if args.config == "batch":
+    if args.config in ("batch", "ragdolls"):
         # the rollback workload: back to the snapshot, re-simulate 8 ticks twice from it (the first
         # pass and the replay), the replay timed on the device; every world's hash must match
         w.restore_exact(snap)

@@ -71,8 +71,8 @@ typedef struct RPhysStepStats {
     uint32_t pairs;          /* broadphase pairs (StepStats::pairs_tested) */
     uint32_t contacts;       /* culled contact points (StepStats::contacts) */
     uint32_t islands;        /* StepStats::islands */
-    uint32_t levels;         /* contact levels of the solve schedule */
-    uint32_t max_batch;      /* largest level (World::last_max_batch().0) */
+    uint32_t levels;         /* levels of the solve schedule (joint rows, then contact rows) */
+    uint32_t max_batch;      /* largest level (World::last_max_batch().0 without joints) */
     uint32_t warm_matched;   /* contacts started warm (World::warm_matched) */
     uint32_t sweeps;         /* velocity sweeps run in the last tick */
     uint32_t bounce_skipped; /* rows that would take the W6 bounce passes (solved inelastic here) */
@@ -81,7 +81,7 @@ typedef struct RPhysStepStats {
     uint32_t error_flags;    /* RPHYS_STATERR_* */
     float residual;          /* residual of the last velocity sweep (m/s) */
     uint32_t row_sweeps;     /* velocity row updates run in the last tick (rows x sweeps) */
-    uint32_t rows_scheduled; /* contact rows with a movable body in the last tick */
+    uint32_t rows_scheduled; /* contact rows with a movable body, and joint rows, in the last tick */
     /* how the last tick's velocity solve was split (0 from the CPU restatement): solve groups whose
      * rows and bodies fit in on-chip shared memory, groups solved over global memory, and the
      * largest group */
@@ -198,6 +198,40 @@ RPhysResult rphys_ext_get_row_features(const RPhysWorld* world, float* out_feats
 /* The predictions the last tick offered, per contact in contact order: 4 floats (normal, friction 1,
  * friction 2, 1) or zeros where none was offered. */
 RPhysResult rphys_ext_get_row_predictions(const RPhysWorld* world, float* out4, uint32_t cap_contacts, uint32_t* out_count);
+
+/* D6 joints: World::add_ball_joint / add_hinge_joint (riftphys-world/src/world/world.rs:718-719;
+ * Joints::add_ball / add_hinge, riftphys-articulation/src/bodies.rs:326-338). frame_a / frame_b
+ * place the joint frame in body A's / body B's frame. A ball locks the three translations and
+ * leaves rotation free; a hinge also locks the two rotations other than hinge_axis (0, 1, 2 = x,
+ * y, z of frame A). Bodies joined by a joint never collide with each other (step.rs:85-102).
+ * Joint ids are 0-based, in creation order; *out_first_id receives the first. Body ids as
+ * everywhere (1-based, live); body_a != body_b; frames finite. In a batch (rphys_ext_batch_*), a
+ * joint joins two bodies of one world and joints come in world order (each world's joints one
+ * id range, hashed by rphys_ext_batch_get_hashes with ids from 0). All-or-nothing: a bad
+ * descriptor adds none. */
+#define RPHYS_JOINT_BALL  0u
+#define RPHYS_JOINT_HINGE 1u
+typedef struct RPhysJointDesc {
+    uint32_t kind;         /* RPHYS_JOINT_* */
+    uint32_t hinge_axis;   /* RPHYS_JOINT_HINGE only */
+    uint32_t body_a, body_b;
+    RPhysIsometry frame_a, frame_b;
+} RPhysJointDesc;
+RPhysResult rphys_ext_add_joints(RPhysWorld* world, const RPhysJointDesc* descs, uint32_t n, uint32_t* out_first_id);
+/* Joints::set_d6_limit_t (angular = 0) / set_d6_limit_r (angular = 1) (bodies.rs:367-391): with
+ * enabled, the axis becomes a limited row on [lo, hi] (metres along frame A's axis, or radians:
+ * the twist angle on a hinge's own axis, 2 sin(angle / 2) about the other axes); a limit on a
+ * rotational axis other than a hinge's own makes the joint no longer a hinge. enabled = 0 clears
+ * the limit and leaves the axis as it was. lo <= hi, both finite. */
+RPhysResult rphys_ext_set_joint_limit(RPhysWorld* world, uint32_t joint, uint32_t angular, uint32_t axis,
+                                      uint32_t enabled, float lo, float hi);
+/* The same for many limits at once, applied in array order; all-or-nothing. */
+typedef struct RPhysJointLimit {
+    uint32_t joint, angular, axis, enabled;
+    float lo, hi;
+} RPhysJointLimit;
+RPhysResult rphys_ext_set_joint_limits(RPhysWorld* world, const RPhysJointLimit* limits, uint32_t n);
+RPhysResult rphys_ext_num_joints(const RPhysWorld* world, uint32_t* out_count);
 
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:

@@ -213,6 +213,55 @@ static inline Q4 qfrom_axis_angle(V3 axis, float angle) {
   return Q4{v.x, v.y, v.z, c};
 }
 
+// atan of a non-negative double: 1/x for x > 1, then two half-angle reductions
+// t -> t / (1 + sqrt(1 + t^2)) (atan t = 2 atan of the result) leave |t| <= tan(pi/16) ~ 0.199,
+// then the Taylor series t - t^3/3 + ... through t^27 and the sum times 4.
+static const double kPio2Hi = 0x1.921fb54442d18p+0;
+static const double kPio2Lo = 0x1.1a62633145c07p-54;
+static inline double atan_d(double x) {
+  bool inv = x > 1.0;
+  if (inv) x = 1.0 / x;
+  double t = x / (1.0 + std::sqrt(1.0 + x * x));
+  t = t / (1.0 + std::sqrt(1.0 + t * t));
+  double z = t * t;
+  double p = -1.0 / 27.0;
+  p = p * z + 1.0 / 25.0;
+  p = p * z - 1.0 / 23.0;
+  p = p * z + 1.0 / 21.0;
+  p = p * z - 1.0 / 19.0;
+  p = p * z + 1.0 / 17.0;
+  p = p * z - 1.0 / 15.0;
+  p = p * z + 1.0 / 13.0;
+  p = p * z - 1.0 / 11.0;
+  p = p * z + 1.0 / 9.0;
+  p = p * z - 1.0 / 7.0;
+  p = p * z + 1.0 / 5.0;
+  p = p * z - 1.0 / 3.0;
+  double a = 4.0 * (t + (t * z) * p);
+  if (inv) a = (kPio2Hi - a) + kPio2Lo;
+  return a;
+}
+// f32 atan2 with IEEE's special cases, evaluated in double and rounded once.
+static inline float atan2f_rp(float yf, float xf) {
+  if (std::isnan(yf) || std::isnan(xf)) return NAN;
+  const double pi = 2.0 * kPio2Hi;
+  double y = (double)yf, x = (double)xf, a;
+  if (yf == 0.0f) a = std::signbit(xf) ? pi : 0.0;
+  else if (std::isinf(xf) && std::isinf(yf)) a = xf > 0.0f ? 0.5 * kPio2Hi : 1.5 * kPio2Hi;
+  else if (std::isinf(xf)) a = xf > 0.0f ? 0.0 : pi;
+  else if (xf == 0.0f || std::isinf(yf)) a = kPio2Hi;
+  else {
+    a = atan_d(std::fabs(y) / std::fabs(x));
+    if (xf < 0.0f) a = pi - a;
+  }
+  return (float)(std::signbit(yf) ? -a : a);
+}
+// f32 acos of d in [0, 1]: 2 atan(sqrt((1 - d) / (1 + d))), rounded once.
+static inline float acosf_unit_rp(float df) {
+  double d = (double)df;
+  return (float)(2.0 * atan_d(std::sqrt((1.0 - d) / (1.0 + d))));
+}
+
 // ---- determinism helpers (riftphys-core/src/det.rs, determinism.rs) ----
 // q6 (det.rs:11-17): non-finite -> 0; round(x / 1e-6) * 1e-6
 static inline float q6(float x) {

@@ -505,6 +505,61 @@ RPhysResult rphys_ext_set_residual_mode(RPhysWorld* W, float tol, uint32_t max_s
   W->w.res_tol = tol; W->w.res_max = max_sweeps;
   return RPHYS_OK;
 }
+RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_t n, uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_joints: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  std::vector<std::pair<uint32_t, uint32_t>> ab(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (d[i].kind > RPHYS_JOINT_HINGE || (d[i].kind == RPHYS_JOINT_HINGE && d[i].hinge_axis > 2))
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: bad kind or hinge axis");
+    if (!fin_iso(d[i].frame_a) || !fin_iso(d[i].frame_b)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: frame contains NaN/Inf");
+    RPhysResult r = live_id(W, d[i].body_a, "rphys_ext_add_joints", &ab[i].first);
+    if (r) return r;
+    r = live_id(W, d[i].body_b, "rphys_ext_add_joints", &ab[i].second);
+    if (r) return r;
+    if (ab[i].first == ab[i].second) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: body_a == body_b");
+  }
+  *out_first = (uint32_t)W->w.joints.size();
+  for (uint32_t i = 0; i < n; ++i) {
+    Iso fa{v(d[i].frame_a.pos), q(d[i].frame_a.rot)}, fb{v(d[i].frame_b.pos), q(d[i].frame_b.rot)};
+    if (d[i].kind == RPHYS_JOINT_BALL) W->w.add_ball_joint(ab[i].first, ab[i].second, fa, fb);
+    else W->w.add_hinge_joint(ab[i].first, ab[i].second, fa, fb, d[i].hinge_axis);
+  }
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_joint_limit(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, uint32_t enabled,
+                                      float lo, float hi) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_limit: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  if (joint >= W->w.joints.size()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_limit: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limit: axis > 2");
+  if (enabled && !(std::isfinite(lo) && std::isfinite(hi) && lo <= hi))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limit: limit must be finite with lo <= hi");
+  W->w.set_d6_limit(joint, angular != 0, axis, enabled != 0, lo, hi);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_joint_limits(RPhysWorld* W, const RPhysJointLimit* l, uint32_t n) {
+  clear_err();
+  if (!W || (!l && n)) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_limits: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (l[i].joint >= W->w.joints.size()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_limits: joint out of range");
+    if (l[i].axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limits: axis > 2");
+    if (l[i].enabled && !(std::isfinite(l[i].lo) && std::isfinite(l[i].hi) && l[i].lo <= l[i].hi))
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limits: limit must be finite with lo <= hi");
+  }
+  for (uint32_t i = 0; i < n; ++i) W->w.set_d6_limit(l[i].joint, l[i].angular != 0, l[i].axis, l[i].enabled != 0, l[i].lo, l[i].hi);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_num_joints(const RPhysWorld* W, uint32_t* out) {
+  clear_err();
+  if (!W || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_num_joints: null arg");
+  *out = (uint32_t)W->w.joints.size();
+  return RPHYS_OK;
+}
 RPhysResult rphys_ext_step_n(RPhysWorld* W, float dt, uint32_t n) {
   clear_err();
   if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_step_n: world is null");

@@ -1,0 +1,36 @@
+// oracle/oracle_joints.h -- TEST INFRASTRUCTURE (the oracle): D6 joint rows and the joint
+// position solve, restated from riftphys-world/src/world/solver.rs:264-424 and
+// riftphys-articulation/src/bodies.rs:422-922. Only the oracle's World::step uses it.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "oracle_world.h"
+
+namespace orc {
+
+// JointRow (solver.rs:264-288) with gamma = 0 (no damper rows are restated).
+struct JRow {
+  uint32_t a, b, joint;
+  bool angular;
+  V3 u, ra, rb;
+  float wa, wb, m_eff, target, lam_min, lam_max;
+  uint8_t tag;
+};
+
+// d6_hinge_axis (bodies.rs:891-901) at the restated feature set: -1 for none.
+int d6_hinge_axis(const Joint& j);
+// d6_row_angle (bodies.rs:908-918)
+float d6_row_angle(const Joint& j, Q4 rot_a, Q4 rot_b, int i);
+// d6_rows (solver.rs:336-424): the joint's velocity rows, appended to out.
+void d6_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vector<JRow>& out);
+// joint_row_vel / joint_row_apply (solver.rs:291-307)
+float joint_row_vel(const World& w, const JRow& r);
+void joint_row_apply(World& w, const JRow& r, float lam);
+// One Gauss-Seidel update of a joint row (solver.rs:821-830); returns new - old.
+float joint_row_update(World& w, const JRow& r, float& acc);
+// Joints::solve_step_with for one sweep (bodies.rs:422-471) with SHAKE directions from start
+// (indexed by body) and joints between two frozen bodies skipped.
+void solve_joints_pass(World& w, float dt, const std::vector<Iso>& start, const std::vector<uint8_t>& frozen);
+
+}  // namespace orc

@@ -2,6 +2,7 @@
 // reference's World::step; see oracle_world.h for scope. Every function cites the reference
 // lines it follows (paths relative to the reference's crates/ directory).
 #include "oracle_world.h"
+#include "oracle_joints.h"
 
 #include <algorithm>
 #include <climits>
@@ -625,6 +626,10 @@ void World::drop_warm_of(uint32_t b) {
   for (auto it = warm.begin(); it != warm.end();) {
     if (std::get<0>(it->first) == b || std::get<1>(it->first) == b) it = warm.erase(it); else ++it;
   }
+  for (auto it = warm_joints.begin(); it != warm_joints.end();) {
+    const Joint& j = joints[it->first];
+    if (j.a == b || j.b == b) it = warm_joints.erase(it); else ++it;
+  }
 }
 // World::set_body_pose (world.rs:501-513)
 void World::set_body_pose(uint32_t id, const Iso& p) {
@@ -670,7 +675,7 @@ uint32_t World::num_sleeping() const {
 }
 CarriedState World::carried_state() const {  // world.rs:912-923
   CarriedState s;
-  s.warm = warm; s.last_lin_vel = last_lin_vel; s.awake = awake; s.sleep_ticks = sleep_ticks;
+  s.warm = warm; s.warm_joints = warm_joints; s.last_lin_vel = last_lin_vel; s.awake = awake; s.sleep_ticks = sleep_ticks;
   return s;
 }
 void World::restore_carried_state(const CarriedState& s) {  // world.rs:927-961
@@ -682,6 +687,11 @@ void World::restore_carried_state(const CarriedState& s) {  // world.rs:927-961
   auto al = [&](uint32_t b) { return b == 0xFFFFFFFFu || (b < alive.size() && alive[b] != 0); };
   for (auto it = warm.begin(); it != warm.end();) {
     if (!(al(std::get<0>(it->first)) && al(std::get<1>(it->first)))) it = warm.erase(it); else ++it;
+  }
+  warm_joints = s.warm_joints;
+  for (auto it = warm_joints.begin(); it != warm_joints.end();) {
+    bool keep = it->first < joints.size() && al(joints[it->first].a) && al(joints[it->first].b);
+    if (!keep) it = warm_joints.erase(it); else ++it;
   }
 }
 
@@ -852,13 +862,23 @@ void World::step(float dt) {
   broadphase(swept, pairs);
   stats.pairs = (uint32_t)pairs.size();
   last_pairs = pairs;
-  // --- Stage 2: narrowphase (step.rs:85-142); no joints, so no jointed pairs
+  // --- Stage 2: narrowphase (step.rs:85-142); bodies joined by a joint do not collide
+  std::vector<uint64_t> jointed_pairs;
+  for (auto& jt : joints) {
+    uint32_t lo = std::min(jt.a, jt.b), hi = std::max(jt.a, jt.b);
+    jointed_pairs.push_back(((uint64_t)lo << 32) | hi);
+  }
+  std::sort(jointed_pairs.begin(), jointed_pairs.end());
   std::vector<std::vector<Contact>> per_pair(pairs.size());
   auto narrow = [&](size_t p) {
     uint32_t i = pairs[p].first, j = pairs[p].second;
     const Collider& ca = colliders[i];
     const Collider& cb = colliders[j];
     if (ca.body == cb.body) return;
+    {
+      uint32_t lo = std::min(ca.body, cb.body), hi = std::max(ca.body, cb.body);
+      if (std::binary_search(jointed_pairs.begin(), jointed_pairs.end(), ((uint64_t)lo << 32) | hi)) return;
+    }
     float reach = sweep[i] + sweep[j] - kMargin;
     Manifold m;
     if (collide_shapes(ca.shape, Iso{pos[ca.body], rot[ca.body]}, cb.shape, Iso{pos[cb.body], rot[cb.body]}, reach, &m)) {
@@ -938,8 +958,12 @@ void World::step(float dt) {
   }
   const uint32_t nc = (uint32_t)contacts.size();
   stats.contacts = nc;
-  // --- islands (islands.rs:27-93): the count, and whether the solve runs
+  // bodies in any joint (solver.rs:483-491, step.rs:160-170)
+  std::vector<uint8_t> jointed(count, 0);
+  for (auto& jt : joints) { jointed[jt.a] = 1; jointed[jt.b] = 1; }
+  // --- islands (islands.rs:27-93): the count, whether the solve runs, the joints' order
   uint32_t n_islands = 0;
+  std::vector<uint32_t> active_joints;
   {
     std::vector<uint32_t> parent(count), rank(count, 0), lookup(count, 0xFFFFFFFFu);
     std::iota(parent.begin(), parent.end(), 0u);
@@ -949,18 +973,33 @@ void World::step(float dt) {
       return r;
     };
     auto isdyn = [&](uint32_t id) { return inv_mass[id] > 0.0f; };
+    auto unite = [&](uint32_t a, uint32_t b) {
+      uint32_t ri = find(a), rj = find(b);
+      if (ri != rj) {
+        if (rank[ri] < rank[rj]) parent[ri] = rj;
+        else if (rank[ri] > rank[rj]) parent[rj] = ri;
+        else { parent[ri] = rj; rank[rj] += 1; }
+      }
+    };
+    for (auto& jt : joints)
+      if (isdyn(jt.a) && isdyn(jt.b)) unite(jt.a, jt.b);
     for (auto& c : contacts) {
       if (c.b_collider == kTerrain) continue;
       uint32_t a = colliders[c.a_collider].body, b = colliders[c.b_collider].body;
-      if (isdyn(a) && isdyn(b)) {
-        uint32_t ri = find(a), rj = find(b);
-        if (ri != rj) {
-          if (rank[ri] < rank[rj]) parent[ri] = rj;
-          else if (rank[ri] > rank[rj]) parent[rj] = ri;
-          else { parent[ri] = rj; rank[rj] += 1; }
-        }
-      }
+      if (isdyn(a) && isdyn(b)) unite(a, b);
     }
+    // active joints (solver.rs:646-648): islands in root order, each island's joints in index order
+    std::vector<std::pair<uint32_t, uint32_t>> jorder;
+    for (uint32_t k = 0; k < (uint32_t)joints.size(); ++k) {
+      const Joint& jt = joints[k];
+      bool da = isdyn(jt.a), db = isdyn(jt.b);
+      if (!da && !db) continue;
+      uint32_t root = da ? find(jt.a) : find(jt.b);
+      if (lookup[root] == 0xFFFFFFFFu) lookup[root] = n_islands++;
+      jorder.push_back({root, k});
+    }
+    std::stable_sort(jorder.begin(), jorder.end(), [](auto& x, auto& y) { return x.first < y.first; });
+    for (auto& x : jorder) active_joints.push_back(x.second);
     for (auto& c : contacts) {
       uint32_t a = colliders[c.a_collider].body;
       uint32_t b = 0; bool db = false;
@@ -1014,16 +1053,74 @@ void World::step(float dt) {
       float v_rel_n = 0.5f * (v_pre + dot(contact_rel_vel(*this, cs), cs.n));
       if (v_rel_n < -1.0f) {
         cs.restitution_bias = (-pp.restitution) * v_rel_n;
-        cs.toi = true;  // no body is jointed in the configured path
+        cs.toi = !jointed[cs.ai] && (cs.terrain || !jointed[cs.bi]);  // W6: free bodies only
       }
     }
     // 2a. level schedule (:621-642)
-    std::vector<uint32_t> order(nc);
-    std::iota(order.begin(), order.end(), 0u);
-    uint32_t nlev = level_schedule(cons, order, count, level, batches);
-    stats.levels = nlev;
+    // 2b. joint rows (:644-664), in active order, one contiguous range per joint
+    std::vector<JRow> jrows;
+    std::vector<std::pair<uint32_t, uint32_t>> jrange(joints.size(), {0u, 0u});
+    for (uint32_t jk : active_joints) {
+      uint32_t s = (uint32_t)jrows.size();
+      d6_rows(*this, joints[jk], jk, dt, jrows);
+      jrange[jk] = {s, (uint32_t)jrows.size()};
+    }
+    const uint32_t njr = (uint32_t)jrows.size();
+    std::vector<float> jacc(njr, 0.0f);
+    // 2a. one level schedule (:621-642, 666-683) over the joint rows, then the contact rows: entry
+    // e < njr is joint row e, entry njr + k contact k. Every sweep then runs an island's joint rows
+    // before its contacts, as the reference's joint batches run before its contact batches. A
+    // contact's side on a sleeping jointed body is read-only for the contact but moved by that
+    // body's joint rows, so the schedule and the solve islands count it as touched.
+    auto ent = [&](uint32_t e, uint32_t* a, uint32_t* b, bool* ta, bool* tb) {
+      if (e < njr) {
+        const JRow& r = jrows[e];
+        *a = r.a; *b = r.b; *ta = r.wa > 0.0f; *tb = r.wb > 0.0f;
+        return true;
+      }
+      const CC& c = cons[e - njr];
+      *a = c.ai; *b = c.bi;
+      *ta = c.inv_a > 0.0f || (jointed[c.ai] && inv_mass[c.ai] > 0.0f);
+      *tb = !c.terrain && (c.inv_b > 0.0f || (jointed[c.bi] && inv_mass[c.bi] > 0.0f));
+      return c.inv_a > 0.0f || (!c.terrain && c.inv_b > 0.0f);
+    };
+    const uint32_t nent = njr + nc;
+    std::vector<uint32_t> ent_level(nent, 0xFFFFFFFFu);
+    {
+      std::vector<uint32_t> bl(count, 0);
+      batches.clear();
+      for (uint32_t e = 0; e < nent; ++e) {
+        uint32_t a, b; bool ta, tb;
+        if (!ent(e, &a, &b, &ta, &tb)) continue;
+        uint32_t la = ta ? bl[a] : 0, lb = tb ? bl[b] : 0;
+        uint32_t t = la > lb ? la : lb;
+        if (t >= batches.size()) batches.emplace_back();
+        batches[t].push_back(e);
+        ent_level[e] = t;
+        if (ta) bl[a] = t + 1;
+        if (tb) bl[b] = t + 1;
+      }
+    }
+    stats.levels = (uint32_t)batches.size();
     for (auto& b : batches) stats.max_batch = std::max<uint32_t>(stats.max_batch, (uint32_t)b.size());
-    for (uint32_t k = 0; k < nc; ++k) levels_out[k] = level[k];
+    for (uint32_t k = 0; k < nc; ++k) levels_out[k] = ent_level[njr + k];
+    // warm start, joints (:699-712): serial in joint order, clamped to each row's bounds
+    for (uint32_t jk = 0; jk < (uint32_t)joints.size(); ++jk) {
+      uint32_t s = jrange[jk].first, e = jrange[jk].second;
+      if (e == s) continue;
+      auto it = warm_joints.find(jk);
+      if (it == warm_joints.end()) continue;
+      const WarmJointRows& prev = it->second;
+      if (prev.size() != e - s) continue;
+      bool same = true;
+      for (uint32_t k = s; k < e; ++k) same = same && prev[k - s].first == jrows[k].tag;
+      if (!same) continue;
+      for (uint32_t k = s; k < e; ++k) {
+        float lam = clampf(prev[k - s].second, jrows[k].lam_min, jrows[k].lam_max);
+        jacc[k] = lam;
+        if (lam != 0.0f) joint_row_apply(*this, jrows[k], lam);
+      }
+    }
     std::vector<float> acc_jn(nc, 0.0f), acc_jt(2 * (size_t)nc, 0.0f);
     // 3. warm start (:717-762)
     std::vector<WarmKey> keys(nc);
@@ -1114,27 +1211,29 @@ void World::step(float dt) {
       return x;
     };
     for (auto& b : batches)
-      for (uint32_t k : b) {
-        const CC& cs = cons[k];
-        if (cs.inv_a > 0.0f && !cs.terrain && cs.inv_b > 0.0f) {
-          uint32_t ra = sfind(cs.ai), rb = sfind(cs.bi);
+      for (uint32_t e : b) {
+        uint32_t a, bb; bool ta, tb;
+        ent(e, &a, &bb, &ta, &tb);
+        if (ta && tb) {
+          uint32_t ra = sfind(a), rb = sfind(bb);
           if (ra != rb) sroot[ra < rb ? rb : ra] = ra < rb ? ra : rb;
         }
       }
-    std::vector<uint32_t> row_isl(nc, 0xFFFFFFFFu), isl_of_root(count, 0xFFFFFFFFu);
+    std::vector<uint32_t> row_isl(nent, 0xFFFFFFFFu), isl_of_root(count, 0xFFFFFFFFu);
     uint32_t n_sisl = 0;
     for (auto& b : batches)
-      for (uint32_t k : b) {
-        const CC& cs = cons[k];
-        uint32_t r = sfind(cs.inv_a > 0.0f ? cs.ai : cs.bi);
+      for (uint32_t e : b) {
+        uint32_t a, bb; bool ta, tb;
+        ent(e, &a, &bb, &ta, &tb);
+        uint32_t r = sfind(ta ? a : bb);
         if (isl_of_root[r] == 0xFFFFFFFFu) isl_of_root[r] = n_sisl++;
-        row_isl[k] = isl_of_root[r];
+        row_isl[e] = isl_of_root[r];
       }
-    std::vector<float> row_res(nc, 0.0f), isl_res(n_sisl), isl_last(n_sisl, 0.0f);
+    std::vector<float> row_res(nent, 0.0f), isl_res(n_sisl), isl_last(n_sisl, 0.0f);
     std::vector<uint32_t> isl_sweeps(n_sisl, 0), isl_rows(n_sisl, 0);
     std::vector<uint8_t> isl_done(n_sisl, 0);
     for (auto& b : batches)
-      for (uint32_t k : b) isl_rows[row_isl[k]]++;
+      for (uint32_t e : b) isl_rows[row_isl[e]]++;
     auto row = [&](uint32_t k, float* resid) {
       const CC& cs = cons[k];
       float v_rel_n = dot(contact_rel_vel(*this, cs), cs.n);
@@ -1159,6 +1258,15 @@ void World::step(float dt) {
       if (cs.m_t2 > 0.0f) r = rmax(r, std::fabs(d.y) / cs.m_t2);
       *resid = rmax(*resid, r);
     };
+    // one entry: a joint row (solver.rs:821-830; residual |delta lambda| / m_eff) or a contact
+    auto solve_ent = [&](uint32_t e, float* resid) {
+      if (e < njr) {
+        float d = joint_row_update(*this, jrows[e], jacc[e]);
+        *resid = rmax(*resid, std::fabs(d) / jrows[e].m_eff);
+      } else {
+        row(e - njr, resid);
+      }
+    };
     const bool residual_mode = res_tol > 0.0f;
     const uint32_t max_sweeps = residual_mode ? (res_max > 0 ? res_max : iters_v) : iters_v;
     uint32_t active = n_sisl;
@@ -1168,23 +1276,23 @@ void World::step(float dt) {
         if (threads > 1 && b.size() >= 64) {
 #pragma omp parallel for num_threads(threads)
           for (long q = 0; q < (long)b.size(); ++q) {
-            uint32_t k = b[q];
-            if (isl_done[row_isl[k]]) continue;
-            row_res[k] = 0.0f;
-            row(k, &row_res[k]);
+            uint32_t e = b[q];
+            if (isl_done[row_isl[e]]) continue;
+            row_res[e] = 0.0f;
+            solve_ent(e, &row_res[e]);
           }
         } else
 #endif
-          for (uint32_t k : b) {
-            if (isl_done[row_isl[k]]) continue;
-            row_res[k] = 0.0f;
-            row(k, &row_res[k]);
+          for (uint32_t e : b) {
+            if (isl_done[row_isl[e]]) continue;
+            row_res[e] = 0.0f;
+            solve_ent(e, &row_res[e]);
           }
       }
       std::fill(isl_res.begin(), isl_res.end(), 0.0f);
       for (auto& b : batches)
-        for (uint32_t k : b)
-          if (!isl_done[row_isl[k]]) isl_res[row_isl[k]] = rmax(isl_res[row_isl[k]], row_res[k]);
+        for (uint32_t e : b)
+          if (!isl_done[row_isl[e]]) isl_res[row_isl[e]] = rmax(isl_res[row_isl[e]], row_res[e]);
       for (uint32_t i = 0; i < n_sisl; ++i) {
         if (isl_done[i]) continue;
         isl_sweeps[i] = it + 1;
@@ -1202,6 +1310,14 @@ void World::step(float dt) {
       stats.rows_scheduled += isl_rows[i];
       stats.row_sweeps += isl_rows[i] * isl_sweeps[i];
       if (residual_mode && !isl_done[i]) stats.islands_capped++;
+    }
+    // joints solved this tick replace their rows; the rest keep theirs (:946-952)
+    for (uint32_t jk = 0; jk < (uint32_t)joints.size(); ++jk) {
+      uint32_t s = jrange[jk].first, e = jrange[jk].second;
+      if (e == s) continue;
+      WarmJointRows rows;
+      for (uint32_t k = s; k < e; ++k) rows.push_back({jrows[k].tag, jacc[k]});
+      warm_joints[jk] = rows;
     }
     // warm-start cache (:917-944)
     std::map<WarmKey, std::vector<WarmContact>> nw;
@@ -1272,8 +1388,9 @@ void World::step(float dt) {
     constrained[colliders[c.a_collider].body] = 1;
     if (c.b_collider != kTerrain) constrained[colliders[c.b_collider].body] = 1;
   }
+  for (auto& jt : joints) { constrained[jt.a] = 1; constrained[jt.b] = 1; }
   std::vector<uint8_t> ballistic(count);
-  for (uint32_t i = 0; i < count; ++i) ballistic[i] = !constrained[i] || !contact_loaded[i];
+  for (uint32_t i = 0; i < count; ++i) ballistic[i] = !constrained[i] || (!jointed[i] && !contact_loaded[i]);
   for (auto& c : contacts) {
     uint32_t a = colliders[c.a_collider].body;
     bool hb = c.b_collider != kTerrain;
@@ -1412,8 +1529,26 @@ void World::step(float dt) {
       if (pc.hb && bm) move_body(pc.b, pb, imb, iib, rb, mul(pc.n, lambda));
     }
   };
-  if (!pcs.empty()) {
-    for (uint32_t it = 0; it < iters_p; ++it) project(false);
+  // joints and contacts interleaved (step.rs:287-308): each sweep the joint pass (SHAKE
+  // directions from the step's start poses) then one contact projection
+  const bool has_joints = !joints.empty();
+  std::vector<Iso> start_poses;
+  std::vector<uint8_t> frozen;
+  if (has_joints) {
+    start_poses.resize(count);
+    frozen.resize(count);
+    for (uint32_t i = 0; i < count; ++i) {
+      start_poses[i] = (dyn[i] && awake[i]) ? original[i] : Iso{pos[i], rot[i]};
+      frozen[i] = (!dyn[i] || !awake[i]) ? 1 : 0;
+    }
+    for (auto& jt : joints)  // Joints::begin_step (bodies.rs:290-300)
+      for (int k = 0; k < 3; ++k) { jt.lam_t[k] = 0.0f; jt.lam_r[k] = 0.0f; }
+  }
+  if (has_joints || !pcs.empty()) {
+    for (uint32_t it = 0; it < iters_p; ++it) {
+      if (has_joints) solve_joints_pass(*this, dt, start_poses, frozen);
+      project(false);
+    }
     project(true);
   }
   // --- Stage 6: velocity from corrections (step.rs:316-379)
@@ -1429,7 +1564,9 @@ void World::step(float dt) {
     V3 vl = lin[i], va = ang[i];
     Iso old = original[i], pred = predicted[i];
     Iso np{pos[i], rot[i]};
-    V3 d_lin = sub(sub(np.pos, pred.pos), split_l[i]);
+    // split impulse only outside articulations (step.rs:324-329)
+    V3 sl = jointed[i] ? V3{0, 0, 0} : split_l[i], sa = jointed[i] ? V3{0, 0, 0} : split_a[i];
+    V3 d_lin = sub(sub(np.pos, pred.pos), sl);
     if (!vzero(d_lin)) vl = add(vl, divs(d_lin, dt));
     if (touching[i] && vl.y < 0.0f) {
       vl.y = 0.0f;
@@ -1440,7 +1577,7 @@ void World::step(float dt) {
       Q4 dq = qmul(np.rot, qconj(pred.rot));
       V3 d_ang = mul(V3{dq.x, dq.y, dq.z}, 2.0f);
       if (dq.w < 0.0f) d_ang = neg(d_ang);
-      va = add(va, divs(sub(d_ang, split_a[i]), dt));
+      va = add(va, divs(sub(d_ang, sa), dt));  // no velocity drives: never motor-driven
     }
     set_vel(i, vl, va);
   }
@@ -1487,7 +1624,12 @@ void World::step_hash(uint8_t out[32]) const {
     for (auto& c : kv.second) { v3h(c.la); h.update_u32(canon_bits(c.jn)); v3h(c.jt); }
   }
   h.update_u64(0);  // warm_patches
-  h.update_u64(0);  // warm_joints
+  h.update_u64(warm_joints.size());
+  for (auto& kv : warm_joints) {
+    h.update_u32(kv.first);
+    h.update_u32((uint32_t)kv.second.size());
+    for (auto& r : kv.second) { h.update_u8(r.first); h.update_u32(canon_bits(r.second)); }
+  }
   h.update_u64(0);  // rotor
   h.update_u64(last_lin_vel.size());
   for (auto& v : last_lin_vel) v3h(v);

@@ -5,7 +5,11 @@
 // sleeping, the BLAKE3 tick hash. Only tests/, __graft_entry__.smoke() and bench.py's
 // cpu_baseline leg use it; the product (riftphys-rust_b200/) never links it.
 //
-// Not restated (no configuration reaches them, or the C ABI cannot): joints, compliant and
+// Joints: D6 joints (ball, hinge, per-axis limits; riftphys-articulation/src/bodies.rs:326-391)
+// with their velocity rows (solver.rs:291-424, 644-687, 699-712, 788-834, 946-952) and the XPBD
+// position pass with SHAKE directions (bodies.rs:422-471, 616-873). Drives, compliance, joint
+// damping / friction, armature and distance joints are not restated.
+// Not restated (no configuration reaches them, or the C ABI cannot): compliant and
 // patch-friction pairs, collider offsets, players, accel components, pending epoch swaps. The
 // W6 bounce passes (solver.rs:1047-1241) are detected and counted, and the rows that would take
 // them are left as the inelastic solve produced them (the same rule the GPU path follows).
@@ -49,8 +53,22 @@ struct HeightField {
   uint32_t mat = 4;
 };
 
+// D6 joint (bodies.rs:55-137) at the restated feature set: an axis is enabled (locked) or free,
+// with an optional limit [lo, hi]; hinge is the stored hinge axis (add_hinge) or -1.
+struct D6Axis { bool enabled = false, has_limit = false; float lo = 0.0f, hi = 0.0f; };
+struct Joint {
+  uint32_t a, b;
+  Iso fa, fb;
+  D6Axis t[3], r[3];
+  int hinge = -1;
+  float lam_t[3] = {0, 0, 0}, lam_r[3] = {0, 0, 0};  // XPBD multipliers of the current step
+};
+// warm_joints entry (solver.rs:946-952): per row, its tag and accumulated impulse
+using WarmJointRows = std::vector<std::pair<uint8_t, float>>;
+
 struct CarriedState {
   std::map<WarmKey, std::vector<WarmContact>> warm;
+  std::map<uint32_t, WarmJointRows> warm_joints;
   std::vector<V3> last_lin_vel;
   std::vector<uint8_t> awake;
   std::vector<uint16_t> sleep_ticks;
@@ -92,6 +110,8 @@ struct World {
   std::vector<uint8_t> alive;
   std::vector<V3> last_lin_vel;
   std::map<WarmKey, std::vector<WarmContact>> warm;
+  std::vector<Joint> joints;
+  std::map<uint32_t, WarmJointRows> warm_joints;
   uint32_t iters_v = 20, iters_p = 20;
   std::vector<std::pair<std::pair<uint32_t, uint32_t>, PairProps>> overrides;
   bool has_hf = false;
@@ -127,6 +147,10 @@ struct World {
   void apply_impulse_world(uint32_t id, V3 j);
   bool remove_body(uint32_t id);
   void drop_warm_of(uint32_t b);
+  // joints (world.rs:718-720, 966-968; bodies.rs:326-391)
+  uint32_t add_ball_joint(uint32_t a, uint32_t b, const Iso& fa, const Iso& fb);
+  uint32_t add_hinge_joint(uint32_t a, uint32_t b, const Iso& fa, const Iso& fb, uint32_t axis);
+  void set_d6_limit(uint32_t id, bool angular, uint32_t axis, bool has, float lo, float hi);
   PairProps pair_props(uint32_t a, uint32_t b) const;
   void set_pair_props(uint32_t a, uint32_t b, const PairProps& p);
   void update_colliders_aabb();

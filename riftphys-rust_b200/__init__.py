@@ -118,6 +118,54 @@ class PairProps(Structure):
     _fields_ = [("mu_s", c_float), ("mu_k", c_float), ("restitution", c_float), ("stribeck_v", c_float)]
 
 
+class JointDesc(Structure):
+    _fields_ = [("kind", c_uint32), ("hinge_axis", c_uint32), ("body_a", c_uint32), ("body_b", c_uint32),
+                ("frame_a", Isometry), ("frame_b", Isometry)]
+
+
+JOINT_BALL = 0
+JOINT_HINGE = 1
+
+
+class JointLimit(Structure):
+    _fields_ = [("joint", c_uint32), ("angular", c_uint32), ("axis", c_uint32), ("enabled", c_uint32),
+                ("lo", c_float), ("hi", c_float)]
+
+
+def joint_array(kind, axis, a, b, fa_pos, fa_rot, fb_pos, fb_rot):
+    """A numpy array laid out as RPhysJointDesc[n] (72 bytes each), built column-wise."""
+    import numpy as np
+    n = len(kind)
+    x = np.zeros((n, 18), dtype=np.float32)
+    u = x.view(np.uint32)
+    u[:, 0] = kind
+    u[:, 1] = axis
+    u[:, 2] = a
+    u[:, 3] = b
+    x[:, 4:7] = fa_pos
+    x[:, 7:11] = fa_rot
+    x[:, 11:14] = fb_pos
+    x[:, 14:18] = fb_rot
+    assert x.strides[0] == ctypes.sizeof(JointDesc)
+    return x
+
+
+def limit_array(joint, angular, axis, lo, hi):
+    """A numpy array laid out as RPhysJointLimit[n] (24 bytes each), every limit enabled."""
+    import numpy as np
+    n = len(joint)
+    x = np.zeros((n, 6), dtype=np.float32)
+    u = x.view(np.uint32)
+    u[:, 0] = joint
+    u[:, 1] = angular
+    u[:, 2] = axis
+    u[:, 3] = 1
+    x[:, 4] = lo
+    x[:, 5] = hi
+    assert x.strides[0] == ctypes.sizeof(JointLimit)
+    return x
+
+
 class StepStats(Structure):
     _fields_ = [(n, c_uint32) for n in ("pairs", "contacts", "islands", "levels", "max_batch", "warm_matched",
                                         "sweeps", "bounce_skipped", "warm_entries", "sleeping", "error_flags")] + \
@@ -202,6 +250,10 @@ ABI = [
     ("rphys_ext_stream_handle", c_uint32, [c_void_p, POINTER(c_uint64)]),
     ("rphys_ext_launch_count", c_uint32, [POINTER(c_uint64)]),
     ("rphys_ext_world_step_hash_noalloc", c_uint32, [c_void_p, POINTER(Hash32)]),
+    ("rphys_ext_add_joints", c_uint32, [c_void_p, POINTER(JointDesc), c_uint32, POINTER(c_uint32)]),
+    ("rphys_ext_set_joint_limit", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float, c_float]),
+    ("rphys_ext_num_joints", c_uint32, [c_void_p, POINTER(c_uint32)]),
+    ("rphys_ext_set_joint_limits", c_uint32, [c_void_p, c_void_p, c_uint32]),
 ]
 
 
@@ -450,6 +502,41 @@ class World:
         out = (Hash32 * count)()
         self.c("rphys_ext_batch_get_hashes", first, count, ctypes.cast(out, c_void_p))
         return [bytes(h.bytes) for h in out]
+
+    def add_joints(self, joints):
+        """joints: iterable of (kind, body_a, body_b, frame_a, frame_b, hinge_axis) with frames as
+        ((x, y, z), (qx, qy, qz, qw)). Returns the first joint id."""
+        joints = list(joints)
+        arr = (JointDesc * max(1, len(joints)))()
+        for i, (kind, a, b, fa, fb, axis) in enumerate(joints):
+            arr[i].kind = kind
+            arr[i].hinge_axis = axis
+            arr[i].body_a = a
+            arr[i].body_b = b
+            arr[i].frame_a = iso(*fa[0], q=tuple(fa[1]))
+            arr[i].frame_b = iso(*fb[0], q=tuple(fb[1]))
+        first = c_uint32(0)
+        self.c("rphys_ext_add_joints", arr, len(joints), byref(first))
+        return first.value
+
+    def add_joint_array(self, arr):
+        """Adds the joints of a joint_array(). Returns the first joint id."""
+        first = c_uint32(0)
+        self.c("rphys_ext_add_joints", ctypes.cast(arr.ctypes.data, POINTER(JointDesc)), len(arr), byref(first))
+        return first.value
+
+    def set_joint_limit_array(self, arr):
+        self.c("rphys_ext_set_joint_limits", arr.ctypes.data_as(c_void_p), len(arr))
+
+    def set_joint_limit(self, joint, angular, axis, lo=None, hi=None):
+        on = lo is not None
+        self.c("rphys_ext_set_joint_limit", joint, 1 if angular else 0, axis, 1 if on else 0,
+               float(lo if on else 0.0), float(hi if on else 0.0))
+
+    def num_joints(self):
+        n = c_uint32(0)
+        self.c("rphys_ext_num_joints", byref(n))
+        return n.value
 
     def set_pair_props(self, a, b, mu_s, mu_k, restitution, stribeck_v):
         p = PairProps(mu_s, mu_k, restitution, stribeck_v)

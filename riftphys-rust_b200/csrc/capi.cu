@@ -603,6 +603,81 @@ RPhysResult rphys_ext_set_heightfield_f32(RPhysWorld* W, uint32_t nx, uint32_t n
     return set_hf(W, nx, nz, cx, cz, ox, oz, std::move(hh), mat);
   });
 }
+// World::add_ball_joint / add_hinge_joint (world.rs:718-719), all-or-nothing over the array.
+RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_t n, uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_joints: null arg");
+  LOCK;
+  return guard("rphys_ext_add_joints", [&]() {
+    std::vector<uint32_t> ab(2 * (size_t)n);
+    for (uint32_t i = 0; i < n; ++i) {
+      if (d[i].kind > RPHYS_JOINT_HINGE || (d[i].kind == RPHYS_JOINT_HINGE && d[i].hinge_axis > 2))
+        return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: bad kind or hinge axis");
+      if (!fin_iso(d[i].frame_a) || !fin_iso(d[i].frame_b))
+        return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: frame contains NaN/Inf");
+      RPhysResult r = live_id(W, d[i].body_a, "rphys_ext_add_joints", &ab[2 * i]);
+      if (r) return r;
+      r = live_id(W, d[i].body_b, "rphys_ext_add_joints", &ab[2 * i + 1]);
+      if (r) return r;
+      if (ab[2 * i] == ab[2 * i + 1]) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: body_a == body_b");
+      if (W->w->batched() && W->w->num_worlds() > 0) {
+        uint32_t wa = W->w->world_of(ab[2 * i]), wb = W->w->world_of(ab[2 * i + 1]);
+        if (wa != wb) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: in a batch, a joint joins two bodies of one world");
+        uint32_t prev = i ? W->w->world_of(ab[2 * i - 2])
+                          : (W->w->num_joints() ? W->w->world_of(W->w->h_joints_.back().a) : 0u);
+        if (wa < prev) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: in a batch, joints come in world order");
+      }
+    }
+    *out_first = W->w->num_joints();
+    for (uint32_t i = 0; i < n; ++i) {
+      float fa[7], fb[7];
+      pose7(d[i].frame_a, fa);
+      pose7(d[i].frame_b, fb);
+      W->w->add_joint(d[i].kind, ab[2 * i], ab[2 * i + 1], fa, fb, d[i].hinge_axis);
+    }
+    W->w->upload_joints();
+    return RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_set_joint_limit(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, uint32_t enabled,
+                                      float lo, float hi) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_limit: world is null");
+  LOCK;
+  if (joint >= W->w->num_joints()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_limit: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limit: axis > 2");
+  if (enabled && !(std::isfinite(lo) && std::isfinite(hi) && lo <= hi))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limit: limit must be finite with lo <= hi");
+  return guard("rphys_ext_set_joint_limit", [&]() {
+    W->w->set_joint_limit(joint, angular != 0, axis, enabled != 0, lo, hi);
+    W->w->upload_joints();
+    return RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_set_joint_limits(RPhysWorld* W, const RPhysJointLimit* l, uint32_t n) {
+  clear_err();
+  if (!W || (!l && n)) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_limits: null arg");
+  LOCK;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (l[i].joint >= W->w->num_joints()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_limits: joint out of range");
+    if (l[i].axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limits: axis > 2");
+    if (l[i].enabled && !(std::isfinite(l[i].lo) && std::isfinite(l[i].hi) && l[i].lo <= l[i].hi))
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_limits: limit must be finite with lo <= hi");
+  }
+  return guard("rphys_ext_set_joint_limits", [&]() {
+    for (uint32_t i = 0; i < n; ++i)
+      W->w->set_joint_limit(l[i].joint, l[i].angular != 0, l[i].axis, l[i].enabled != 0, l[i].lo, l[i].hi);
+    W->w->upload_joints();
+    return RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_num_joints(const RPhysWorld* W, uint32_t* out) {
+  clear_err();
+  if (!W || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_num_joints: null arg");
+  *out = W->w->num_joints();
+  return RPHYS_OK;
+}
 RPhysResult rphys_ext_set_residual_mode(RPhysWorld* W, float tol, uint32_t max_sweeps) {
   clear_err();
   if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_residual_mode: world is null");

@@ -8,7 +8,8 @@
 // Stream layout: epoch u64 | rng state u64 | BLAKE3("") (the empty schedule digest) |
 //   per body: index u32, pos xyz, rot xyzw, lin xyz, ang xyz (canonical f32 bits) |
 //   warm keys u64 | per key: 4 x u32, count u32, per entry la xyz, jn, jt xyz |
-//   warm patches u64 0 | warm joints u64 0 | rotors u64 0 |
+//   warm patches u64 0 | warm joints u64 | per entry: joint u32, rows u32, per row tag u8 +
+//   impulse | rotors u64 0 |
 //   last_lin_vel count u64 + xyz each | awake count u64 + u8 each | sleep ticks count u64 + u16 each.
 #include <cstring>
 #include <mutex>
@@ -173,7 +174,49 @@ __global__ void k_h_tail(uint32_t nb, uint32_t cap, const float4* __restrict__ l
   if (i < cap) { uint16_t v = ticks[i]; t[8 + 2 * i] = (uint8_t)v; t[9 + 2 * i] = (uint8_t)(v >> 8); }
 }
 
+// warm_joints (hash_carried, world.rs:895-900), entries in joint order. Joints [j0, j0 + n) of a
+// batch's world hash with ids j - j0 (the arrays passed start at j0).
+__global__ void k_hj_sizes(uint32_t n, const uint32_t* __restrict__ jw_n, uint32_t* sz, uint32_t* has) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint32_t c = jw_n[j];
+  bool h = c != 0xFFFFFFFFu;
+  has[j] = h ? 1u : 0u;
+  sz[j] = h ? 8u + 5u * c : 0u;
+}
+__global__ void k_hj_write(uint32_t n, const uint32_t* __restrict__ jw_n, const uint8_t* __restrict__ tag,
+                           const float* __restrict__ lam, const uint32_t* __restrict__ off, uint8_t* out) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint32_t c = jw_n[j];
+  if (c == 0xFFFFFFFFu) return;
+  uint8_t* p = out + off[j];
+  put32(p, j);
+  put32(p + 4, c);
+  for (uint32_t k = 0; k < c; ++k) {
+    p[8 + 5 * k] = tag[12 * (size_t)j + k];
+    put32(p + 9 + 5 * k, canon_bits(lam[12 * (size_t)j + k]));
+  }
+}
+// Sizes the joint section of joints [j0, j0 + n): bytes of its entries and their count.
+static void joint_section(WorldGpu& W, uint32_t j0, uint32_t n, uint32_t* sz, uint32_t* off, uint32_t* has,
+                          uint32_t* pos, uint64_t* bytes, uint64_t* count, cudaStream_t st) {
+  *bytes = 0; *count = 0;
+  if (!n) return;
+  const int T = 256;
+  k_hj_sizes<<<(n + T - 1) / T, T, 0, st>>>(n, W.jw_n.p + j0, sz, has); RP_COUNT_LAUNCH(1);
+  *bytes = exclusive_scan_total(*W.s_, sz, off, n, st);
+  *count = exclusive_scan_total(*W.s_, has, pos, n, st);
+}
+static void joint_write(WorldGpu& W, uint32_t j0, uint32_t n, const uint32_t* off, uint8_t* out, cudaStream_t st) {
+  if (!n) return;
+  const int T = 256;
+  k_hj_write<<<(n + T - 1) / T, T, 0, st>>>(n, W.jw_n.p + j0, W.jw_tag.p + 12 * (size_t)j0, W.jw_lam.p + 12 * (size_t)j0,
+                                             off, out); RP_COUNT_LAUNCH(1);
+}
+
 void WorldGpu::step_hash(uint8_t out32[32]) {
+  upload_joints();
   Scratch& S = *s_;
   cudaStream_t st = stream_;
   const int T = 256;
@@ -185,9 +228,14 @@ void WorldGpu::step_hash(uint8_t out32[32]) {
     k_h_warm_flags<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, S.woff.p); RP_COUNT_LAUNCH(1);
     nkeys = exclusive_scan_total(S, S.woff.p, S.wpos.p, n_warm, st);
   }
+  const uint32_t nj = num_joints();
+  uint64_t jbytes = 0, jcount = 0;
+  S.jh_sz.ensure(nj + 1); S.jh_off.ensure(nj + 1); S.jh_has.ensure(nj + 1); S.jh_pos.ensure(nj + 1);
+  joint_section(*this, 0, nj, S.jh_sz.p, S.jh_off.p, S.jh_has.p, S.jh_pos.p, &jbytes, &jcount, st);
   uint64_t off_bodies = 48;
   uint64_t off_warm = off_bodies + 56ull * nb_;
-  uint64_t off_tail = off_warm + 8 + 20ull * nkeys + 28ull * n_warm + 24;
+  uint64_t off_joints = off_warm + 8 + 20ull * nkeys + 28ull * n_warm + 8;
+  uint64_t off_tail = off_joints + 8 + jbytes + 8;
   uint64_t len = off_tail + 8 + 12ull * nb_ + 8 + cap + 8 + 2ull * cap;
   uint32_t nch = (uint32_t)((len + 1023) / 1024);
   S.hbuf.ensure((size_t)nch * 1024 + 64);
@@ -201,14 +249,19 @@ void WorldGpu::step_hash(uint8_t out32[32]) {
                                      0x12, 0xb7, 0xcc, 0x9a, 0x93, 0xca, 0xe4, 0x1f, 0x32, 0x62};
   std::memcpy(head + 16, kEmpty, 32);
   RP_CUDA(cudaMemcpyAsync(S.hbuf.p, head, 48, cudaMemcpyHostToDevice, st));
-  if (nb_) k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, S.hbuf.p + off_bodies); RP_COUNT_LAUNCH(1);
+  if (nb_) { k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, S.hbuf.p + off_bodies); RP_COUNT_LAUNCH(1); }
   uint8_t wcount[8];
   p64(wcount, nkeys);
   RP_CUDA(cudaMemcpyAsync(S.hbuf.p + off_warm, wcount, 8, cudaMemcpyHostToDevice, st));
-  if (n_warm)
+  if (n_warm) {
     k_h_warm<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, warm_a.p, warm_b.p, S.woff.p, S.wpos.p,
                                                   S.hbuf.p + off_warm + 8); RP_COUNT_LAUNCH(1);
-  // the three zero-length maps are already zero bytes
+  }
+  // the empty patch and rotor maps are zero bytes already; the joint section between them
+  uint8_t jc[8];
+  p64(jc, jcount);
+  RP_CUDA(cudaMemcpyAsync(S.hbuf.p + off_joints, jc, 8, cudaMemcpyHostToDevice, st));
+  joint_write(*this, 0, nj, S.jh_off.p, S.hbuf.p + off_joints + 8, st);
   uint32_t nt = cap > nb_ ? cap : nb_;
   k_h_tail<<<(nt + T) / T, T, 0, st>>>(nb_, cap, last_lin.p, awake.p, sleep_ticks.p, S.hbuf.p + off_tail); RP_COUNT_LAUNCH(1);
   S.hcv.ensure(16 * (size_t)nch + 16);
@@ -245,6 +298,7 @@ __global__ void k_warm_range(uint32_t n, const uint4* __restrict__ k, uint32_t b
   out[1] = lo;
 }
 void WorldGpu::step_hash_world(uint32_t w, uint8_t out32[32]) {
+  upload_joints();
   Scratch& S = *s_;
   cudaStream_t st = stream_;
   const int T = 256;
@@ -264,9 +318,24 @@ void WorldGpu::step_hash_world(uint32_t w, uint8_t out32[32]) {
     k_h_warm_flags<<<(nw + T - 1) / T, T, 0, st>>>(nw, warm_key.p + wlo, S.woff.p); RP_COUNT_LAUNCH(1);
     nkeys = exclusive_scan_total(S, S.woff.p, S.wpos.p, nw, st);
   }
+  // the world's joints: one contiguous id range (a batch's joints join bodies of the world added last)
+  uint32_t j0 = 0, j1 = 0;
+  {
+    auto first_at = [&](uint32_t b) {
+      uint32_t lo = 0, hi = num_joints();
+      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (h_joints_[m].a < b) lo = m + 1; else hi = m; }
+      return lo;
+    };
+    j0 = first_at(b0); j1 = first_at(b1);
+  }
+  const uint32_t njw = j1 - j0;
+  uint64_t jbytes = 0, jcount = 0;
+  S.jh_sz.ensure(njw + 1); S.jh_off.ensure(njw + 1); S.jh_has.ensure(njw + 1); S.jh_pos.ensure(njw + 1);
+  joint_section(*this, j0, njw, S.jh_sz.p, S.jh_off.p, S.jh_has.p, S.jh_pos.p, &jbytes, &jcount, st);
   uint64_t off_bodies = 48;
   uint64_t off_warm = off_bodies + 56ull * nbw;
-  uint64_t off_tail = off_warm + 8 + 20ull * nkeys + 28ull * nw + 24;
+  uint64_t off_joints = off_warm + 8 + 20ull * nkeys + 28ull * nw + 8;
+  uint64_t off_tail = off_joints + 8 + jbytes + 8;
   uint64_t len = off_tail + 8 + 12ull * nbw + 8 + cap + 8 + 2ull * cap;
   uint32_t nch = (uint32_t)((len + 1023) / 1024);
   S.hbuf.ensure((size_t)nch * 1024 + 64);
@@ -290,6 +359,10 @@ void WorldGpu::step_hash_world(uint32_t w, uint8_t out32[32]) {
     k_h_warm<<<(nw + T - 1) / T, T, 0, st>>>(nw, warm_key.p + wlo, warm_a.p + wlo, warm_b.p + wlo, S.woff.p, S.wpos.p,
                                               S.hbuf.p + off_warm + 8, b0);
   if (nw) RP_COUNT_LAUNCH(1);
+  uint8_t jc[8];
+  p64(jc, jcount);
+  RP_CUDA(cudaMemcpyAsync(S.hbuf.p + off_joints, jc, 8, cudaMemcpyHostToDevice, st));
+  joint_write(*this, j0, njw, S.jh_off.p, S.hbuf.p + off_joints + 8, st);
   k_h_tail<<<(nbw + T) / T, T, 0, st>>>(nbw, cap, last_lin.p + b0, awake.p + b0, sleep_ticks.p + b0, S.hbuf.p + off_tail);
   RP_COUNT_LAUNCH(1);
   S.hcv.ensure(16 * (size_t)nch + 16);
@@ -316,7 +389,8 @@ void WorldGpu::step_hash_world(uint32_t w, uint8_t out32[32]) {
 // scratch byte lives in g_noalloc_scratch, a fixed array in device memory reserved when the library
 // is loaded: no cudaMalloc / cudaFree and no allocating library routine on any call. Layout:
 //   [stream: NOALLOC_STREAM_MAX + 1088 B][chaining values: 16 * (NOALLOC_STREAM_MAX / 1024 + 1) + 16
-//   words][warm key starts: NOALLOC_WARM_MAX + 1 words][warm key ranks: same][scan temp: 64 KiB].
+//   words][warm key starts: NOALLOC_WARM_MAX + 1 words][warm key ranks: same][joint entry sizes,
+//   offsets, flags, ranks: NOALLOC_JOINT_MAX + 1 words each][scan temp: 64 KiB].
 // Only the stream must start at zero; each call clears the part it uses. The array is one per
 // device and shared by every world on it: two calls in flight at once would overwrite each other's
 // bytes, so calls are serialised by g_noalloc_mu and each returns after its work on the device ended.
@@ -326,7 +400,12 @@ void WorldGpu::step_hash_world(uint32_t w, uint8_t out32[32]) {
 #define NOALLOC_OFF_CV ((size_t)NOALLOC_STREAM_MAX + 1088u)
 #define NOALLOC_OFF_WOFF (NOALLOC_OFF_CV + 4u * (16u * (size_t)NOALLOC_CHUNKS + 16u))
 #define NOALLOC_OFF_WPOS (NOALLOC_OFF_WOFF + 4u * ((size_t)NOALLOC_WARM_MAX + 1u))
-#define NOALLOC_OFF_TEMP ((NOALLOC_OFF_WPOS + 4u * ((size_t)NOALLOC_WARM_MAX + 1u) + 255u) & ~(size_t)255u)
+#define NOALLOC_JOINT_MAX (64u << 10)    // joints
+#define NOALLOC_OFF_JSZ (NOALLOC_OFF_WPOS + 4u * ((size_t)NOALLOC_WARM_MAX + 1u))
+#define NOALLOC_OFF_JOFF (NOALLOC_OFF_JSZ + 4u * ((size_t)NOALLOC_JOINT_MAX + 1u))
+#define NOALLOC_OFF_JHAS (NOALLOC_OFF_JOFF + 4u * ((size_t)NOALLOC_JOINT_MAX + 1u))
+#define NOALLOC_OFF_JPOS (NOALLOC_OFF_JHAS + 4u * ((size_t)NOALLOC_JOINT_MAX + 1u))
+#define NOALLOC_OFF_TEMP ((NOALLOC_OFF_JPOS + 4u * ((size_t)NOALLOC_JOINT_MAX + 1u) + 255u) & ~(size_t)255u)
 #define NOALLOC_TEMP_BYTES (64u << 10)
 #define NOALLOC_BYTES (NOALLOC_OFF_TEMP + NOALLOC_TEMP_BYTES)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
@@ -356,11 +435,22 @@ void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
   if (n_warm > NOALLOC_WARM_MAX)
     throw std::length_error("step_hash_noalloc: " + std::to_string(n_warm) + " warm-start entries, at most " +
                             std::to_string(NOALLOC_WARM_MAX));
+  upload_joints();
+  const uint32_t nj = num_joints();
+  if (nj > NOALLOC_JOINT_MAX)
+    throw std::length_error("step_hash_noalloc: " + std::to_string(nj) + " joints, at most " +
+                            std::to_string(NOALLOC_JOINT_MAX));
   uint32_t* woff = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WOFF);
   uint32_t* wpos = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WPOS);
+  uint32_t* jsz = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JSZ);
+  uint32_t* joff = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JOFF);
+  uint32_t* jhas = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JHAS);
+  uint32_t* jpos = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JPOS);
   void* temp = base + NOALLOC_OFF_TEMP;
-  // the stream length bound holds with every warm entry under its own key (the most bytes)
-  uint64_t worst = 48 + 56ull * nb_ + 8 + 48ull * n_warm + 24 + 8 + 12ull * nb_ + 8 + cap + 8 + 2ull * cap;
+  // the stream length bound holds with every warm entry under its own key (the most bytes) and
+  // every joint holding the most rows
+  uint64_t worst = 48 + 56ull * nb_ + 8 + 48ull * n_warm + 24 + (8 + 5ull * 12) * nj + 8 + 12ull * nb_ + 8 + cap + 8 +
+                   2ull * cap;
   if (worst > NOALLOC_STREAM_MAX)
     throw std::length_error("step_hash_noalloc: state stream of up to " + std::to_string(worst) + " bytes (" +
                             std::to_string(nb_) + " bodies, capacity " + std::to_string(cap) + ", " +
@@ -379,9 +469,29 @@ void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
     RP_CUDA(cudaStreamSynchronize(st));
     nkeys = a + b;
   }
+  uint64_t jbytes = 0, jcount = 0;
+  if (nj) {
+    size_t bytes = 0;
+    RP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, jsz, joff, (int)nj, st));
+    if (bytes > NOALLOC_TEMP_BYTES) throw std::length_error("step_hash_noalloc: scan needs more temporary bytes than reserved");
+    k_hj_sizes<<<(nj + T - 1) / T, T, 0, st>>>(nj, jw_n.p, jsz, jhas); RP_COUNT_LAUNCH(1);
+    RP_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, jsz, joff, (int)nj, st));
+    RP_COUNT_LAUNCH(2);
+    RP_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, jhas, jpos, (int)nj, st));
+    RP_COUNT_LAUNCH(2);
+    uint32_t v[4] = {0, 0, 0, 0};
+    RP_CUDA(cudaMemcpyAsync(&v[0], joff + nj - 1, 4, cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaMemcpyAsync(&v[1], jsz + nj - 1, 4, cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaMemcpyAsync(&v[2], jpos + nj - 1, 4, cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaMemcpyAsync(&v[3], jhas + nj - 1, 4, cudaMemcpyDeviceToHost, st));
+    RP_CUDA(cudaStreamSynchronize(st));
+    jbytes = (uint64_t)v[0] + v[1];
+    jcount = (uint64_t)v[2] + v[3];
+  }
   uint64_t off_bodies = 48;
   uint64_t off_warm = off_bodies + 56ull * nb_;
-  uint64_t off_tail = off_warm + 8 + 20ull * nkeys + 28ull * n_warm + 24;
+  uint64_t off_joints = off_warm + 8 + 20ull * nkeys + 28ull * n_warm + 8;
+  uint64_t off_tail = off_joints + 8 + jbytes + 8;
   uint64_t len = off_tail + 8 + 12ull * nb_ + 8 + cap + 8 + 2ull * cap;
   uint32_t nch = (uint32_t)((len + 1023) / 1024);
   uint8_t* hbuf = base;
@@ -397,11 +507,15 @@ void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
   uint8_t wcount[8];
   p64(wcount, nkeys);
   RP_CUDA(cudaMemcpyAsync(hbuf, head, 48, cudaMemcpyHostToDevice, st));
-  if (nb_) k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, hbuf + off_bodies); RP_COUNT_LAUNCH(1);
+  if (nb_) { k_h_bodies<<<(nb_ + T - 1) / T, T, 0, st>>>(nb_, pos.p, rot.p, lin.p, ang.p, hbuf + off_bodies); RP_COUNT_LAUNCH(1); }
   RP_CUDA(cudaMemcpyAsync(hbuf + off_warm, wcount, 8, cudaMemcpyHostToDevice, st));
   if (n_warm)
     k_h_warm<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, warm_a.p, warm_b.p, woff, wpos, hbuf + off_warm + 8);
   if (n_warm) RP_COUNT_LAUNCH(1);
+  uint8_t jc[8];
+  p64(jc, jcount);
+  RP_CUDA(cudaMemcpyAsync(hbuf + off_joints, jc, 8, cudaMemcpyHostToDevice, st));
+  joint_write(*this, 0, nj, joff, hbuf + off_joints + 8, st);
   uint32_t nt = cap > nb_ ? cap : nb_;
   k_h_tail<<<(nt + T) / T, T, 0, st>>>(nb_, cap, last_lin.p, awake.p, sleep_ticks.p, hbuf + off_tail); RP_COUNT_LAUNCH(1);
   uint32_t* cv = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_CV);

@@ -1,0 +1,230 @@
+// joints.cuh -- D6 joints on the GPU: the joint record the kernels read, its velocity rows
+// (d6_rows, riftphys-world/src/world/solver.rs:336-424) and its XPBD position solve with SHAKE
+// directions (solve_d6, riftphys-articulation/src/bodies.rs:616-873) for locked and limited axes.
+// Every fin / normalize of the reference is kept where it stands: those sanitations change bits.
+#pragma once
+#include "step_rows.cuh"
+
+namespace rp {
+
+// One joint, 128 bytes. flags: bit i (i < 6) axis i enabled (t0 t1 t2 r0 r1 r2), bit 6 + i axis i
+// limited to [lo[i], hi[i]], bits 12..14 the hinge axis + 1 (0: none; d6_hinge_axis, resolved on
+// the host whenever the joint changes).
+struct JointGpu {
+  uint32_t a, b, flags, pad;
+  float4 fa_p, fa_q, fb_p, fb_q;
+  float lo[6], hi[6];
+};
+static_assert(sizeof(JointGpu) == 128, "JointGpu layout");
+#define JF_LIMIT_SHIFT 6u
+#define JF_HINGE_SHIFT 12u
+#define JMAX_ROWS 12u  // 6 axes, 2 rows each when limited
+
+__host__ __device__ inline int joint_hinge(uint32_t flags) { return (int)((flags >> JF_HINGE_SHIFT) & 7u) - 1; }
+
+// A joint velocity row (JointRow, solver.rs:264-288; no damper rows, so gamma = 0).
+struct JRowD {
+  f3 u, ra, rb;
+  float wa, wb, m_eff, target, lo, hi;
+  uint32_t tag;
+  bool angular;
+};
+
+__device__ __forceinline__ f3 unit_axis(int i) { return i == 0 ? mk3(1, 0, 0) : (i == 1 ? mk3(0, 1, 0) : mk3(0, 0, 1)); }
+__device__ __forceinline__ float comp3(f3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+// normalize_fin (bodies.rs:19-27)
+__device__ __forceinline__ f3 normalize_fin(f3 v) {
+  v = fin_v(v);
+  float l2 = len2(v);
+  if (l2 > 1.0e-12f) return v * (1.0f / sqrtf(l2));
+  return mk3(0, 0, 0);
+}
+// d6_row_angle (bodies.rs:908-918)
+__device__ __forceinline__ float d6_row_angle_dev(int hinge, q4 rot_a, q4 rot_b, int i) {
+  q4 q = qmul(qconj(rot_a), rot_b);
+  if (q.w < 0.0f) q = qneg(q);
+  f3 v = mk3(q.x, q.y, q.z);
+  if (hinge == i) return 2.0f * atan2_rp(comp3(v, i), q.w);
+  return dot(qrot(rot_a, v * 2.0f), qrot(rot_a, unit_axis(i)));
+}
+// World inverse inertia the way Bodies::inv_inertia_world gives it (zero for inv_mass 0).
+__device__ __forceinline__ m3 inv_inertia_world_dev(const BodiesV& B, uint32_t id, q4 rot) {
+  if (B.inv_mass[id] == 0.0f) return mzero();
+  return world_inertia(rot, ld_m3(B.inv_I, id));
+}
+
+// d6_rows (solver.rs:336-424): the joint's rows in (linear x y z, angular x y z) order, limited
+// axes as a lower and an upper row. Returns the row count (0 when neither body is dynamic).
+__device__ __forceinline__ uint32_t d6_rows_dev(const JointGpu& j, const BodiesV& B, float dt, JRowD* out) {
+  const uint32_t a = j.a, b = j.b;
+  f3 pa = xyz(B.pos[a]), pb = xyz(B.pos[b]);
+  q4 qa = asq(B.rot[a]), qb = asq(B.rot[b]);
+  q4 rot_a = qmul(qa, asq(j.fa_q)), rot_b = qmul(qb, asq(j.fb_q));
+  f3 xa = pa + qrot(qa, xyz(j.fa_p)), xb = pb + qrot(qb, xyz(j.fb_p));
+  float wa = B.inv_mass[a], wb = B.inv_mass[b];
+  if (wa == 0.0f && wb == 0.0f) return 0;
+  m3 ia = wa == 0.0f ? mzero() : ld_m3(B.Iw, a), ib = wb == 0.0f ? mzero() : ld_m3(B.Iw, b);
+  f3 ra = xa - pa, rb = xb - pb, d = xb - xa;
+  const int hinge = joint_hinge(j.flags);
+  uint32_t n = 0;
+  for (int ang = 0; ang < 2; ++ang) {
+    for (int i = 0; i < 3; ++i) {
+      const int ax = 3 * ang + i;
+      if (!((j.flags >> ax) & 1u)) continue;
+      f3 u = qrot(rot_a, unit_axis(i));
+      float k;
+      if (ang) k = dot(u, mvec(ia, u)) + dot(u, mvec(ib, u));
+      else {
+        f3 ca = cross(ra, u), cb = cross(rb, u);
+        k = ((wa + wb) + dot(ca, mvec(ia, ca))) + dot(cb, mvec(ib, cb));
+      }
+      if (k <= 1.0e-9f) continue;
+      JRowD r;
+      r.u = u; r.ra = ra; r.rb = rb; r.wa = wa; r.wb = wb; r.m_eff = 1.0f / k;
+      r.target = 0.0f; r.lo = -INFINITY; r.hi = INFINITY;
+      r.tag = (uint32_t)((ang << 5) | (i << 3));
+      r.angular = ang != 0;
+      if (!((j.flags >> (JF_LIMIT_SHIFT + ax)) & 1u)) { out[n++] = r; continue; }
+      float x = ang ? d6_row_angle_dev(hinge, rot_a, rot_b, i) : dot(d, u);
+      JRowD lo = r, hi = r;
+      lo.target = rmin((j.lo[ax] - x) / dt, 0.0f); lo.lo = 0.0f; lo.tag = r.tag | 2u;
+      hi.target = rmax((j.hi[ax] - x) / dt, 0.0f); hi.hi = 0.0f; hi.lo = -INFINITY; hi.tag = r.tag | 3u;
+      out[n++] = lo;
+      out[n++] = hi;
+    }
+  }
+  return n;
+}
+
+// ---- the position solve (bodies.rs:616-873) on the bodies' global pose arrays
+// Bodies::apply_position_delta / apply_orientation_delta (dynamics.rs:71-88, 207-210)
+__device__ __forceinline__ void apply_position_delta_dev(const BodiesV& B, uint32_t id, f3 dp) {
+  if (B.inv_mass[id] > 0.0f && vfin(dp)) { float4 P = B.pos[id]; B.pos[id] = f4(fin_v(xyz(P) + dp), P.w); }
+}
+__device__ __forceinline__ void apply_orientation_delta_dev(const BodiesV& B, uint32_t id, f3 dth) {
+  if (B.inv_mass[id] <= 0.0f || !vfin(dth)) return;
+  f3 d = fin_v(dth);
+  if (len2(d) <= 1.0e-24f) return;
+  q4 dq = qnormalize(mkq(d.x * 0.5f, d.y * 0.5f, d.z * 0.5f, 1.0f));
+  B.rot[id] = f4q(fin_q(qnormalize(qmul(dq, asq(B.rot[id])))));
+}
+// turned (bodies.rs:486-490)
+__device__ __forceinline__ float turned_dev(q4 a, q4 b) {
+  float d = rmin(fabsf(qmul(a, qconj(b)).w), 1.0f);
+  return 2.0f * acos_unit_rp(d);
+}
+// solve_d6 for locked and limited axes (compliance 0: alpha = 0; no drives, no rotors). lam: the
+// joint's six XPBD multipliers of this step (t0 t1 t2 r0 r1 r2). sa / sb: the step's start poses.
+__device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, const BodiesV& B, f3 sa_p, q4 sa_q,
+                                             f3 sb_p, q4 sb_q) {
+  const uint32_t A = j.a, Bb = j.b;
+  const float wa = fin0(B.inv_mass[A]), wb = fin0(B.inv_mass[Bb]);
+  const bool shake = turned_dev(sa_q, asq(B.rot[A])) < 0.5f && turned_dev(sb_q, asq(B.rot[Bb])) < 0.5f;
+  f3 ax0[3] = {mk3(0, 0, 0), mk3(0, 0, 0), mk3(0, 0, 0)}, la0 = mk3(0, 0, 0), lb0 = mk3(0, 0, 0);
+  m3 ia0 = mzero(), ib0 = mzero();
+  q4 fa_q = asq(j.fa_q), fb_q = asq(j.fb_q);
+  f3 fa_p = xyz(j.fa_p), fb_p = xyz(j.fb_p);
+  if (shake) {
+    q4 r0 = qmul(sa_q, fa_q);
+    for (int i = 0; i < 3; ++i) ax0[i] = normalize_fin(qrot(r0, unit_axis(i)));
+    la0 = fin_v(qrot(sa_q, fa_p));
+    lb0 = fin_v(qrot(sb_q, fb_p));
+    ia0 = world_inertia(sa_q, ld_m3(B.inv_I, A));
+    ib0 = world_inertia(sb_q, ld_m3(B.inv_I, Bb));
+  }
+  const float alpha = 0.0f, bias_vel = 0.0f, dt_unused = 0.0f;
+  for (int i = 0; i < 3; ++i) {
+    if (!((j.flags >> i) & 1u)) continue;
+    f3 pap = xyz(B.pos[A]), pbp = xyz(B.pos[Bb]);
+    q4 paq = asq(B.rot[A]), pbq = asq(B.rot[Bb]);
+    f3 u = normalize_fin(qrot(qmul(paq, fa_q), unit_axis(i)));
+    if (vzero(u)) continue;
+    f3 xa = fin_v(pap + qrot(paq, fa_p)), xb = fin_v(pbp + qrot(pbq, fb_p));
+    f3 d = fin_v(xb - xa);
+    f3 un, lever_a, lever_b;
+    m3 iaw, ibw;
+    if (shake) { un = ax0[i]; lever_a = la0; lever_b = lb0; iaw = ia0; ibw = ib0; }
+    else {
+      un = u; lever_a = xa - pap; lever_b = xb - pbp;
+      iaw = inv_inertia_world_dev(B, A, paq); ibw = inv_inertia_world_dev(B, Bb, pbq);
+    }
+    float coord = fin0(dot(d, u));
+    float c = fin0(coord - 0.0f);
+    if ((j.flags >> (JF_LIMIT_SHIFT + i)) & 1u) {
+      float lo = fin0(j.lo[i]), hi = fin0(j.hi[i]);
+      if (coord < lo) c = fin0(coord - lo);
+      else if (coord > hi) c = fin0(coord - hi);
+      else continue;
+    }
+    f3 ra_u = fin_v(cross(lever_a, un)), rb_u = fin_v(cross(lever_b, un));
+    float w_rot_a = fin0(dot(ra_u, mvec(iaw, ra_u)));
+    float w_rot_b = fin0(dot(rb_u, mvec(ibw, rb_u)));
+    float ws = fin0(((wa + wb) + w_rot_a) + w_rot_b);
+    float denom = fin0(ws + alpha);
+    if (denom <= 0.0f) continue;
+    c = fin0(c + fin0(bias_vel * dt_unused));
+    float lambda_old = fin0(lam[i]);
+    float dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    lam[i] = fin0(lambda_old + dl);
+    apply_position_delta_dev(B, A, fin_v((-un) * fin0(dl * wa)));
+    apply_position_delta_dev(B, Bb, fin_v(un * fin0(dl * wb)));
+    apply_orientation_delta_dev(B, A, fin_v((-mvec(iaw, ra_u)) * dl));
+    apply_orientation_delta_dev(B, Bb, fin_v(mvec(ibw, rb_u) * dl));
+  }
+  const int hinge = joint_hinge(j.flags);
+  for (int i = 0; i < 3; ++i) {
+    if (!((j.flags >> (3 + i)) & 1u)) continue;
+    q4 paq = asq(B.rot[A]), pbq = asq(B.rot[Bb]);
+    q4 ra = qmul(paq, fa_q), rb = qmul(pbq, fb_q);
+    f3 u = normalize_fin(qrot(ra, unit_axis(i)));
+    if (vzero(u)) continue;
+    q4 q = qmul(qconj(ra), rb);
+    if (q.w < 0.0f) q = qneg(q);
+    f3 v = mk3(q.x, q.y, q.z);
+    float angle;
+    if (hinge == i) angle = fin0(2.0f * atan2_rp(comp3(v, i), q.w));
+    else if (hinge >= 0)
+      angle = fin0(dot(fin_v(cross(normalize_fin(qrot(ra, unit_axis(hinge))), normalize_fin(qrot(rb, unit_axis(hinge))))), u));
+    else angle = fin0(dot(fin_v(qrot(ra, fin_v(v * 2.0f))), u));
+    f3 un;
+    m3 iaw, ibw;
+    if (shake) { un = ax0[i]; iaw = ia0; ibw = ib0; }
+    else { un = u; iaw = inv_inertia_world_dev(B, A, paq); ibw = inv_inertia_world_dev(B, Bb, pbq); }
+    float c = fin0(angle - 0.0f);
+    if ((j.flags >> (JF_LIMIT_SHIFT + 3 + i)) & 1u) {
+      float lo = fin0(j.lo[3 + i]), hi = fin0(j.hi[3 + i]);
+      if (angle < lo) c = fin0(angle - lo);
+      else if (angle > hi) c = fin0(angle - hi);
+      else continue;
+    }
+    float ws = fin0(dot(un, mvec(iaw, un)) + dot(un, mvec(ibw, un)));
+    float denom = fin0(ws + alpha);
+    if (denom <= 0.0f) continue;
+    c = fin0(c + fin0(bias_vel * dt_unused));
+    float lambda_old = fin0(lam[3 + i]);
+    float dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    lam[3 + i] = fin0(lambda_old + dl);
+    apply_orientation_delta_dev(B, A, fin_v((-mvec(iaw, un)) * dl));
+    apply_orientation_delta_dev(B, Bb, fin_v(mvec(ibw, un) * dl));
+  }
+}
+
+// ---- host side (joints.cu)
+struct StepCtx;
+// Reference islands: joint unions (both bodies dynamic) into uf and the island marks.
+void joints_ref_islands(WorldGpu& W, uint32_t* uf, uint32_t* root_mark, bool unions, cudaStream_t st);
+// Row counts and offsets per joint; returns the total number of joint velocity rows.
+uint32_t joints_count_rows(WorldGpu& W, float dt, const BodiesV& B, cudaStream_t st);
+// Joint rows at R[base .. base + njr): geometry, bounds, warm start from the joint cache, flags;
+// then the joint-row unions into the solve union-find uf.
+void joints_build_rows(WorldGpu& W, float dt, const BodiesV& B, const RowsV& R, uint32_t base, float* acc_jn,
+                       float2* acc_jt, uint32_t* uf, cudaStream_t st);
+// The solve-island root of every joint row (after every union is in).
+void joints_row_roots(WorldGpu& W, const RowsV& R, uint32_t base, uint32_t njr, uint32_t* uf, uint32_t* row_root,
+                      cudaStream_t st);
+// The joint warm cache (solver.rs:946-952) from the accumulated impulses.
+void joints_store_warm(WorldGpu& W, const RowsV& R, uint32_t base, const float* acc_jn, cudaStream_t st);
+// Bodies in joints count as constrained (step.rs:160-170).
+void joints_mark_constrained(WorldGpu& W, uint8_t* constrained, cudaStream_t st);
+
+}  // namespace rp

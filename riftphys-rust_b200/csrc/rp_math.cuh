@@ -205,6 +205,53 @@ RP_HD float exp_rp(float xf) {
   memcpy(&two_k, &eb, 8);
   return (float)(p * two_k);
 }
+// atan of a non-negative double: 1/x for x > 1, two half-angle reductions
+// t -> t / (1 + sqrt(1 + t^2)) to |t| <= tan(pi/16), the Taylor series through t^27, times 4.
+#define RP_PIO2_HI 0x1.921fb54442d18p+0
+#define RP_PIO2_LO 0x1.1a62633145c07p-54
+RP_HD double atan_d(double x) {
+  bool inv = x > 1.0;
+  if (inv) x = 1.0 / x;
+  double t = x / (1.0 + sqrt(1.0 + x * x));
+  t = t / (1.0 + sqrt(1.0 + t * t));
+  double z = t * t;
+  double p = -1.0 / 27.0;
+  p = p * z + 1.0 / 25.0;
+  p = p * z - 1.0 / 23.0;
+  p = p * z + 1.0 / 21.0;
+  p = p * z - 1.0 / 19.0;
+  p = p * z + 1.0 / 17.0;
+  p = p * z - 1.0 / 15.0;
+  p = p * z + 1.0 / 13.0;
+  p = p * z - 1.0 / 11.0;
+  p = p * z + 1.0 / 9.0;
+  p = p * z - 1.0 / 7.0;
+  p = p * z + 1.0 / 5.0;
+  p = p * z - 1.0 / 3.0;
+  double a = 4.0 * (t + (t * z) * p);
+  if (inv) a = (RP_PIO2_HI - a) + RP_PIO2_LO;
+  return a;
+}
+// f32 atan2 with IEEE's special cases, evaluated in double and rounded once.
+RP_HD float atan2_rp(float yf, float xf) {
+  if (isnan(yf) || isnan(xf)) return NAN;
+  const double pi = 2.0 * RP_PIO2_HI;
+  double y = (double)yf, x = (double)xf, a;
+  if (yf == 0.0f) a = signbit(xf) ? pi : 0.0;
+  else if (isinf(xf) && isinf(yf)) a = xf > 0.0f ? 0.5 * RP_PIO2_HI : 1.5 * RP_PIO2_HI;
+  else if (isinf(xf)) a = xf > 0.0f ? 0.0 : pi;
+  else if (xf == 0.0f || isinf(yf)) a = RP_PIO2_HI;
+  else {
+    a = atan_d(fabs(y) / fabs(x));
+    if (xf < 0.0f) a = pi - a;
+  }
+  return (float)(signbit(yf) ? -a : a);
+}
+// f32 acos of d in [0, 1]: 2 atan(sqrt((1 - d) / (1 + d))), rounded once.
+RP_HD float acos_unit_rp(float df) {
+  double d = (double)df;
+  return (float)(2.0 * atan_d(sqrt((1.0 - d) / (1.0 + d))));
+}
 RP_HD q4 qfrom_axis_angle(f3 axis, float angle) {
   float s, c;
   sincos_rp(angle * 0.5f, &s, &c);

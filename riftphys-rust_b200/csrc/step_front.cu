@@ -211,19 +211,29 @@ __global__ void k_unique_flags(int n, const unsigned long long* __restrict__ a, 
 }
 
 // ------------------------------------------------------------------ narrowphase
+// Bodies joined by a joint (step.rs:85-102): binary search of (min << 32 | max) in the sorted keys.
+__device__ __forceinline__ bool jointed_pair(uint32_t a, uint32_t b, const unsigned long long* __restrict__ keys,
+                                             uint32_t n) {
+  unsigned long long k = a < b ? (((unsigned long long)a << 32) | b) : (((unsigned long long)b << 32) | a);
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (keys[m] < k) lo = m + 1; else hi = m; }
+  return lo < n && keys[lo] == k;
+}
 // One thread per broadphase pair (step.rs:97-113): contact distance reach = s_i + s_j - 0.05;
-// depth = penetration - reach + 0.05. Up to 4 points in fixed slots.
+// depth = penetration - reach + 0.05. Up to 4 points in fixed slots. Same-body and jointed pairs
+// make no contact.
 __global__ void k_narrow_pairs(int np, const unsigned long long* __restrict__ pairs, const uint32_t* __restrict__ cbody,
                                const uint32_t* __restrict__ ckind, const float4* __restrict__ cdims,
                                const float4* __restrict__ pos, const float4* __restrict__ rot,
-                               const float* __restrict__ sweep, float4* out_pt, float4* out_n, uint32_t* out_cnt) {
+                               const float* __restrict__ sweep, const unsigned long long* __restrict__ jkeys,
+                               uint32_t njk, float4* out_pt, float4* out_n, uint32_t* out_cnt) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
   unsigned long long key = pairs[p];
   uint32_t i = (uint32_t)(key >> 32), j = (uint32_t)key;
   uint32_t ba = cbody[i], bb = cbody[j];
   uint32_t cnt = 0;
-  if (ba != bb) {
+  if (ba != bb && !(njk && jointed_pair(ba, bb, jkeys, njk))) {
     float reach = sweep[i] + sweep[j] - 0.05f;
     float4 da = cdims[i], db = cdims[j];
     Shape sa; sa.kind = ckind[i]; sa.a = da.x; sa.b = da.y; sa.c = da.z;
@@ -462,18 +472,20 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   auto& P = S.prof;
   // stage 1
   P.begin(PH_FORCES, st);
-  if (nb > 0)
+  if (nb > 0) {
     k_forces<<<(nb + T - 1) / T, T, 0, st>>>(nb, W.lin.p, W.ang.p, W.lin.p, S.pre_lin.p, S.pre_ang.p, W.dyn.p,
                                               W.awake.p, ctx.g, ctx.dt); RP_COUNT_LAUNCH(1);
+  }
   P.end(PH_FORCES, st);
   P.begin(PH_AABB, st);
   // stage 2: AABBs, sweep, classification
   S.amin.ensure(ncol); S.amax.ensure(ncol); S.smin.ensure(ncol); S.smax.ensure(ncol); S.sweep.ensure(ncol);
   S.u32a.ensure(ncol + 1); S.u32b.ensure(ncol + 1);
-  if (ncol > 0)
+  if (ncol > 0) {
     k_aabbs<<<(ncol + T - 1) / T, T, 0, st>>>(ncol, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, W.lin.p,
                                                W.ang.p, ctx.dt, S.amin.p, S.amax.p, S.smin.p, S.smax.p, S.sweep.p,
                                                S.u32a.p, S.u32b.p, W.d_stats.p + STAT_ERR); RP_COUNT_LAUNCH(1);
+  }
   P.end(PH_AABB, st);
   P.begin(PH_BROAD, st);
   // broadphase: in-grid colliders sorted along x, oversized list
@@ -515,13 +527,15 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   }
   uint32_t n_raw = n_sap_pairs + n_ov_pairs;
   S.pairs.ensure(n_raw + 1); S.pairs2.ensure(n_raw + 1); S.flag8.ensure(n_raw + 1);
-  if (n_sap_pairs > 0)
+  if (n_sap_pairs > 0) {
     k_grid_pairs<true><<<(n_ent + T - 1) / T, T, 0, st>>>(n_ent, S.sap_key64b.p, S.sap_w.p, S.smin.p, S.smax.p, cw, nullptr,
                                                           S.gp_off.p, S.pairs2.p); RP_COUNT_LAUNCH(1);
-  if (n_ov_pairs > 0)
+  }
+  if (n_ov_pairs > 0) {
     k_oversized<true><<<(ncol + T - 1) / T, T, 0, st>>>(ncol, n_over, S.over_ids.p, S.smin.p, S.smax.p, nullptr,
                                                          S.ov_off.p, S.pairs2.p + n_sap_pairs, batched ? W.col_world.p : nullptr,
                                                          batched ? W.world_col_start.p : nullptr); RP_COUNT_LAUNCH(1);
+  }
   uint32_t np = 0;
   if (n_raw > 0) {
     sort_keys_u64(S, S.pairs2.p, S.pairs.p, n_raw, st);  // -> S.pairs
@@ -535,9 +549,11 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   P.begin(PH_NARROW, st);
   // narrowphase over pairs
   S.p_pt.ensure(4 * (size_t)np + 4); S.p_n.ensure(4 * (size_t)np + 4); S.p_cnt.ensure(np + 1);
-  if (np > 0)
+  if (np > 0) {
     k_narrow_pairs<<<(np + 127) / 128, 128, 0, st>>>(np, S.pairs.p, W.col_body.p, W.col_kind.p, W.col_dims.p, W.pos.p,
-                                                    W.rot.p, S.sweep.p, S.p_pt.p, S.p_n.p, S.p_cnt.p); RP_COUNT_LAUNCH(1);
+                                                    W.rot.p, S.sweep.p, W.jpair_keys.p, W.n_jpairs, S.p_pt.p, S.p_n.p,
+                                                    S.p_cnt.p); RP_COUNT_LAUNCH(1);
+  }
   P.end(PH_NARROW, st);
   P.begin(PH_TERRAIN, st);
   // terrain
@@ -556,10 +572,11 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
       ncand = exclusive_scan_total(S, S.t_icnt.p, S.t_ioff.p, nitems, st);
     }
     S.t_cp.ensure(ncand + 1); S.t_cn.ensure(ncand + 1);
-    if (ncand > 0)
+    if (ncand > 0) {
       k_terrain_items<true><<<(nitems + 127) / 128, 128, 0, st>>>(nitems, ncol, ctx.hf, S.t_celloff.p, S.t_win.p, W.col_body.p,
                                                                  W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, S.sweep.p,
                                                                  nullptr, S.t_ioff.p, S.t_cp.p, S.t_cn.p); RP_COUNT_LAUNCH(1);
+    }
     k_terrain_cull<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, W.col_kind.p, S.t_celloff.p, S.t_ncell.p, S.t_ioff.p, nitems,
                                                       ncand, S.t_cp.p, S.t_cn.p, S.t_pt.p, S.t_n.p, S.t_cnt.p); RP_COUNT_LAUNCH(1);
   }
@@ -579,11 +596,12 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
   ctx.nc = nc;
   W.n_contacts = nc;
   S.c_a.ensure(nc + 1); S.c_b.ensure(nc + 1); S.c_pt.ensure(nc + 1); S.c_n.ensure(nc + 1);
-  if (nc > 0)
+  if (nc > 0) {
     k_scatter_contacts<<<(nbk + T - 1) / T, T, 0, st>>>(np, ncol, S.pairs.p, S.p_cnt.p, S.p_pt.p, S.p_n.p,
                                                        terrain ? S.t_cnt.p : nullptr, S.t_pt.p, S.t_n.p, S.pstart.p,
                                                        S.boff.p, W.col_body.p, W.pos.p, S.c_a.p, S.c_b.p, S.c_pt.p,
                                                        S.c_n.p); RP_COUNT_LAUNCH(1);
+  }
   P.end(PH_CONTACTS, st);
 }
 

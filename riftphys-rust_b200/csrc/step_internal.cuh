@@ -192,7 +192,7 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> woff, wpos;
   // hash
   DBuf<uint8_t> hbuf;
-  DBuf<uint32_t> hcv;
+  DBuf<uint32_t> hcv, jh_sz, jh_off, jh_has, jh_pos;
   // primitives' temporary storage
   DBuf<uint8_t> cub_tmp;
   DBuf<uint4> kept_k;

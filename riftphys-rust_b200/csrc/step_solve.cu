@@ -13,6 +13,8 @@
 #include <cub/cub.cuh>
 
 #include "step_internal.cuh"
+#include "step_rows.cuh"
+#include "joints.cuh"
 #include "warm_model.h"
 
 namespace rp {
@@ -23,53 +25,27 @@ const int T = 256;
 inline int nblk(uint32_t n, int t = T) { return n ? (int)((n + t - 1) / t) : 1; }
 }  // namespace
 
-// row flag bits
-enum : uint32_t { RF_TERRAIN = 1, RF_TOI = 4, RF_WA = 8, RF_WB = 16 };
-
-__device__ __forceinline__ m3 ld_m3(const float* p, uint32_t i) {
-  const float* q = p + 9 * (size_t)i;
-  return mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
-}
-__device__ __forceinline__ void st_m3(float* p, uint32_t i, const m3& m) {
-  float* q = p + 9 * (size_t)i;
-  q[0] = m.c0.x; q[1] = m.c0.y; q[2] = m.c0.z; q[3] = m.c1.x; q[4] = m.c1.y; q[5] = m.c1.z;
-  q[6] = m.c2.x; q[7] = m.c2.y; q[8] = m.c2.z;
-}
-
 // ------------------------------------------------------------------ islands (islands.rs:27-93)
-__device__ __forceinline__ uint32_t uf_find(uint32_t* p, uint32_t x) {
-  volatile uint32_t* vp = p;
-  while (true) {
-    uint32_t px = vp[x];
-    if (px == x) return x;
-    uint32_t ppx = vp[px];
-    if (ppx != px) atomicCAS(&p[x], px, ppx);  // path halving
-    x = px;
-  }
-}
-// Union by hooking the larger root under the smaller: each component's root is its least body.
-__device__ __forceinline__ void uf_union(uint32_t* p, uint32_t a, uint32_t b) {
-  while (true) {
-    uint32_t ra = uf_find(p, a), rb = uf_find(p, b);
-    if (ra == rb) return;
-    if (ra > rb) { uint32_t t = ra; ra = rb; rb = t; }
-    if (atomicCAS(&p[rb], rb, ra) == rb) return;
-  }
-}
 __global__ void k_iota(uint32_t n, uint32_t* p) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = i;
 }
 // mode 0: the reference's islands (bodies with inv_mass > 0, asleep or not, islands.rs:266-287);
-// mode 1: solve islands (bodies an impulse can move: awake and dynamic).
+// mode 1: solve islands (bodies an impulse can move: awake and dynamic; and a sleeping body in a
+// joint, which the joint's rows move while the contact reads it).
 __global__ void k_union_contacts(uint32_t nc, int mode, const uint32_t* __restrict__ c_a, const uint32_t* __restrict__ c_b,
                                  const uint32_t* __restrict__ cbody, const float* __restrict__ inv_mass,
-                                 const uint8_t* __restrict__ awake, uint32_t* parent) {
+                                 const uint8_t* __restrict__ awake, const uint8_t* __restrict__ jointed, uint32_t* parent) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nc || c_b[k] == 0xFFFFFFFFu) return;
   uint32_t a = cbody[c_a[k]], b = cbody[c_b[k]];
   bool da = inv_mass[a] > 0.0f, db = inv_mass[b] > 0.0f;
-  if (mode == 1) { da = da && awake[a]; db = db && awake[b]; }
+  if (mode == 1) {
+    // a row with no awake body is not solved: it joins nothing
+    if (!((da && awake[a]) || (db && awake[b]))) return;
+    da = da && (awake[a] || (jointed && jointed[a]));
+    db = db && (awake[b] || (jointed && jointed[b]));
+  }
   if (da && db) uf_union(parent, a, b);
 }
 // route_to_island (islands.rs:316-345): the root each contact lands in, marked.
@@ -110,14 +86,6 @@ __device__ __forceinline__ void orthonormal_basis(f3 n, f3* t1, f3* t2) {
   *t2 = cross(n, *t1);
 }
 
-struct RowsV {
-  uint2* ab; uint32_t* flags; float2* inv; float4 *ra, *rb, *n, *t1, *t2, *mu, *la;
-};
-struct BodiesV {
-  float4 *pos, *rot, *lin, *ang;
-  const float* inv_mass; const float* Iw; const float* inv_I; const uint8_t* awake; const uint8_t* dyn;
-};
-
 // Constraint pre-processing (solver.rs:494-590), one thread per contact. Also the anchors in
 // body A's frame (solver.rs:728-731) and the island of each row that has a movable body.
 __global__ void k_build_rows(uint32_t nc, float dt, const uint32_t* __restrict__ c_a, const uint32_t* __restrict__ c_b,
@@ -125,7 +93,7 @@ __global__ void k_build_rows(uint32_t nc, float dt, const uint32_t* __restrict__
                              const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ cmat, uint32_t hf_mat,
                              const float* __restrict__ ptab, BodiesV B, const float4* __restrict__ pre_lin,
                              const float4* __restrict__ pre_ang, RowsV R, float* acc_jn, float2* acc_jt,
-                             const uint32_t* __restrict__ uf, uint32_t* row_root) {
+                             const uint32_t* __restrict__ uf, uint32_t* row_root, const uint8_t* __restrict__ jointed) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nc) return;
   bool terrain = c_b[k] == 0xFFFFFFFFu;
@@ -158,10 +126,17 @@ __global__ void k_build_rows(uint32_t nc, float dt, const uint32_t* __restrict__
   float v_rel_n = 0.5f * (v_pre + dot(vb - va, n));
   float rbias = 0.0f;
   uint32_t flags = terrain ? RF_TERRAIN : 0u;
-  if (v_rel_n < -1.0f) { rbias = (-rest) * v_rel_n; flags |= RF_TOI; }  // no body is jointed
+  const bool ja = jointed && jointed[ai], jb = jointed && !terrain && jointed[bi];
+  if (v_rel_n < -1.0f) {
+    rbias = (-rest) * v_rel_n;
+    if (!ja && !jb) flags |= RF_TOI;  // W6: free bodies only (solver.rs:571-573)
+  }
   bool wa = inv_a > 0.0f, wb = !terrain && inv_b > 0.0f;
   if (wa) flags |= RF_WA;
   if (wb) flags |= RF_WB;
+  // a sleeping side in a joint: read while its joint rows move it, so ordered like a write
+  if ((wa || wb) && !wa && ja && B.inv_mass[ai] > 0.0f) flags |= RF_RA;
+  if ((wa || wb) && !wb && jb && B.inv_mass[bi] > 0.0f) flags |= RF_RB;
   R.ab[k] = make_uint2(ai, bi);
   R.flags[k] = flags;
   R.inv[k] = make_float2(inv_a, inv_b);
@@ -174,7 +149,7 @@ __global__ void k_build_rows(uint32_t nc, float dt, const uint32_t* __restrict__
   R.la[k] = f4(qrot(qconj(asq(B.rot[ai])), point - pa));
   acc_jn[k] = 0.0f;
   acc_jt[k] = make_float2(0.0f, 0.0f);
-  row_root[k] = (wa || wb) ? uf_find(const_cast<uint32_t*>(uf), wa ? ai : bi) : 0xFFFFFFFFu;
+  row_root[k] = (wa || wb) ? uf_find(const_cast<uint32_t*>(uf), (flags & RF_TA) ? ai : bi) : 0xFFFFFFFFu;
 }
 
 // ------------------------------------------------------------------ row math shared by passes
@@ -257,6 +232,39 @@ __device__ __forceinline__ float pgs_row(const BodiesV& B, const Row& r, uint32_
   if (r.m_t1 > 0.0f) res = rmax(res, fabsf(d.x) / r.m_t1);
   if (r.m_t2 > 0.0f) res = rmax(res, fabsf(d.y) / r.m_t2);
   return res;
+}
+
+// A joint velocity row on the global body arrays (the warp kernel of the largest islands).
+__device__ __forceinline__ void joint_apply_glob(const BodiesV& B, const Row& r, float lam) {
+  f3 p = r.n * lam;
+  if (r.flags & RF_JANG) {
+    f3 t = -p;
+    if (r.inv_a > 0.0f && B.inv_mass[r.ai] > 0.0f && vfin(t)) {
+      float4 a = B.ang[r.ai];
+      B.ang[r.ai] = f4(fin_v(xyz(a) + mvec(ld_m3(B.Iw, r.ai), t)), a.w);
+    }
+    if (r.inv_b > 0.0f && B.inv_mass[r.bi] > 0.0f && vfin(p)) {
+      float4 a = B.ang[r.bi];
+      B.ang[r.bi] = f4(fin_v(xyz(a) + mvec(ld_m3(B.Iw, r.bi), p)), a.w);
+    }
+  } else {
+    if (r.inv_a > 0.0f) { f3 nj = -p; body_impulse(B, r.ai, nj, cross(r.ra, nj)); }
+    if (r.inv_b > 0.0f) body_impulse(B, r.bi, p, cross(r.rb, p));
+  }
+}
+__device__ __forceinline__ float joint_row_glob(const BodiesV& B, const Row& r, uint32_t k, float* acc_jn) {
+  f3 va, vb;
+  if (r.flags & RF_JANG) { va = xyz(B.ang[r.ai]); vb = xyz(B.ang[r.bi]); }
+  else {
+    va = xyz(B.lin[r.ai]) + cross(xyz(B.ang[r.ai]), r.ra);
+    vb = xyz(B.lin[r.bi]) + cross(xyz(B.ang[r.bi]), r.rb);
+  }
+  float v = dot(vb - va, r.n);
+  float old = acc_jn[k];
+  float nw = clampf(old + (r.bias - v) * r.m_n, r.mu_s, r.mu_k);
+  acc_jn[k] = nw;
+  if (nw != old) joint_apply_glob(B, r, nw - old);
+  return fabsf(nw - old) / r.m_n;
 }
 
 // ------------------------------------------------------------------ warm matching
@@ -342,8 +350,8 @@ __global__ void k_level_entries(uint32_t n, const uint32_t* __restrict__ ord_in,
   uint32_t r = ord_in[s];
   uint2 x = ab[r];
   uint32_t f = flags[r];
-  key[2 * s] = (f & RF_WA) ? x.x : 0xFFFFFFFFu;
-  key[2 * s + 1] = (f & RF_WB) ? x.y : 0xFFFFFFFFu;
+  key[2 * s] = (f & RF_TA) ? x.x : 0xFFFFFFFFu;
+  key[2 * s + 1] = (f & RF_TB) ? x.y : 0xFFFFFFFFu;
   val[2 * s] = 2 * s;
   val[2 * s + 1] = 2 * s + 1;
 }
@@ -419,13 +427,36 @@ __global__ void k_gather_u32(uint32_t n, const uint32_t* __restrict__ idx, const
 
 struct Sched { uint32_t* ord; uint32_t* lvl_off; uint32_t* lvl_start; uint32_t* nlev; };
 
+// Warm start, joints (solver.rs:699-712): every joint row's clamped previous impulse, applied when
+// not 0, before any contact's warm start -- the reference's order (all joints, then the contacts,
+// whose friction clamp reads the bodies' velocities after the joints' impulses). One warp per solve
+// group walks its levels: the joint rows of a body come in joint order.
+__global__ void k_joint_warm(uint32_t ng, uint32_t nc, Sched S, RowsV R, BodiesV B, float* acc_jn) {
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= ng) return;
+  uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+  for (uint32_t L = 0; L < nl; ++L) {
+    uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+    for (uint32_t s = s0 + lane; s < s1; s += 32) {
+      uint32_t k = S.ord[s];
+      if (k < nc || !(R.flags[k] & RF_JWARM)) continue;
+      Row r = ld_row(R, k);
+      acc_jn[k] = r.t2.x;
+      if (r.t2.x != 0.0f) joint_apply_glob(B, r, r.t2.x);
+    }
+    __syncwarp();
+  }
+}
+
+
 // ------------------------------------------------------------------ island passes (warp per island)
 __device__ __forceinline__ float warp_max(float v) {
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 // Warm start application, then the velocity sweeps (solver.rs:717-915).
-__global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* acc_jn, float2* acc_jt,
+__global__ void k_vel_solve(uint32_t nisl, uint32_t nc, Sched S, RowsV R, BodiesV B, float* acc_jn, float2* acc_jt,
                             const int* __restrict__ wm_idx, const float4* __restrict__ wa, const float4* __restrict__ wb,
                             int iters, float tol, uint32_t* stats, const uint32_t* __restrict__ g_class,
                             const uint32_t* __restrict__ glist) {
@@ -439,6 +470,7 @@ __global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* a
     uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
     for (uint32_t s = s0 + lane; s < s1; s += 32) {
       uint32_t k = S.ord[s];
+      if (k >= nc) continue;  // joint rows: started by k_joint_warm
       int e = wm_idx[k];
       if (e >= 0) { Row r = ld_row(R, k); warm_apply(B, r, k, wa[e], wb[e], acc_jn, acc_jt); }
     }
@@ -453,7 +485,7 @@ __global__ void k_vel_solve(uint32_t nisl, Sched S, RowsV R, BodiesV B, float* a
       for (uint32_t s = s0 + lane; s < s1; s += 32) {
         uint32_t k = S.ord[s];
         Row r = ld_row(R, k);
-        resid = rmax(resid, pgs_row(B, r, k, acc_jn, acc_jt));
+        resid = rmax(resid, k >= nc ? joint_row_glob(B, r, k, acc_jn) : pgs_row(B, r, k, acc_jn, acc_jt));
       }
       __syncwarp();
     }
@@ -480,6 +512,7 @@ __global__ void k_vel_shock(uint32_t nisl, Sched S, RowsV R, BodiesV B, f3 up, f
     for (uint32_t s = s0 + lane; s < s1; s += 32) {
       uint32_t k = S.ord[s];
       Row r = ld_row(R, k);
+      if (r.flags & RF_JOINT) continue;
       m3 IA = r.inv_a > 0.0f ? ld_m3(B.Iw, r.ai) : mzero();
       m3 IB = r.inv_b > 0.0f ? ld_m3(B.Iw, r.bi) : mzero();
       if (r.inv_a > 0.0f && r.inv_b > 0.0f) {
@@ -581,9 +614,9 @@ __global__ void k_constrained(uint32_t nc, const uint32_t* __restrict__ c_a, con
   if (c_b[k] != 0xFFFFFFFFu) constrained[cbody[c_b[k]]] = 1;
 }
 __global__ void k_ballistic_init(uint32_t nb, const uint8_t* __restrict__ constrained, const uint8_t* __restrict__ loaded,
-                                 uint8_t* ballistic) {
+                                 const uint8_t* __restrict__ jointed, uint8_t* ballistic) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < nb) ballistic[i] = (!constrained[i] || !loaded[i]) ? 1 : 0;
+  if (i < nb) ballistic[i] = (!constrained[i] || (!(jointed && jointed[i]) && !loaded[i])) ? 1 : 0;
 }
 // step.rs:180-206 per contact, on the solve schedule. Flags of bodies that can't move are read
 // at their initial value and never written: for those last_lin_vel equals the velocity, so
@@ -601,6 +634,7 @@ __global__ void k_ballistic(uint32_t nisl, Sched S, RowsV R, BodiesV B, const fl
       uint32_t k = S.ord[s];
       uint2 x = R.ab[k];
       uint32_t f = R.flags[k];
+      if (f & RF_JOINT) continue;
       bool hb = !(f & RF_TERRAIN);
       uint32_t a = x.x, b = x.y;
       bool ba = ballistic[a] != 0, bb = hb ? ballistic[b] != 0 : false;
@@ -616,8 +650,8 @@ __global__ void k_ballistic(uint32_t nisl, Sched S, RowsV R, BodiesV B, const fl
       float v_end = dot((vbl + cross(vba, rb)) - (xyz(B.lin[a]) + cross(xyz(B.ang[a]), ra)), n);
       float s0v = -(c_pt[k].w - 0.05f);
       if (s0v + (2.0f * v_end) * dt < 0.0f || s0v + approach * dt < 0.0f) {
-        if (f & RF_WA) ballistic[a] = 0;
-        if (f & RF_WB) ballistic[b] = 0;
+        if (f & RF_TA) ballistic[a] = 0;
+        if (f & RF_TB) ballistic[b] = 0;
       }
     }
     __syncwarp();
@@ -749,20 +783,62 @@ __device__ __forceinline__ void project_one(const BodiesV& B, const RowsV& R, ui
   if (am) move_body(a, pa_pos, pa_rot, ima, iia, ra, (-n) * lambda);
   if (hb && bm) move_body(b, pb_pos, pb_rot, imb, iib, rb, n * lambda);
 }
-__global__ void k_pos_iterations(uint32_t nisl, Sched S, RowsV R, BodiesV B, int iters, int shock, f3 up,
+// Position sweeps (step.rs:301-308): each joint's solve (bodies.rs:422-471, SHAKE directions from the
+// step's start poses spos / srot) rides on its first velocity row, which the schedule places before
+// every later row touching its bodies -- the reference's joints-then-contacts order; joints between
+// two frozen (static or sleeping) bodies are skipped. The shock projection has no joints.
+__global__ void k_pos_iterations(uint32_t nisl, uint32_t nc, Sched S, RowsV R, BodiesV B, int iters, int shock, f3 up,
                                  const float4* __restrict__ c_pt, const float4* __restrict__ c_n,
-                                 const float4* __restrict__ lbv, float4* split_l, float4* split_a) {
+                                 const float4* __restrict__ lbv, float4* split_l, float4* split_a,
+                                 const JointGpu* __restrict__ J, float* jlam, const float4* __restrict__ spos,
+                                 const float4* __restrict__ srot, float dt) {
   uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= nisl) return;
   uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+  const bool joints_on = !shock && fin(dt) && dt > 0.0f;
   for (int it = 0; it < iters; ++it) {
     for (uint32_t L = 0; L < nl; ++L) {
       uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
-      for (uint32_t s = s0 + lane; s < s1; s += 32)
-        project_one(B, R, S.ord[s], shock != 0, up, c_pt, c_n, lbv, split_l, split_a);
+      for (uint32_t s = s0 + lane; s < s1; s += 32) {
+        uint32_t k = S.ord[s];
+        if (k >= nc) {
+          if (joints_on && (R.flags[k] & RF_JFIRST)) {
+            uint32_t j = __float_as_uint(R.la[k].x);
+            const JointGpu jt = J[j];
+            bool fa = !B.dyn[jt.a] || !B.awake[jt.a], fb = !B.dyn[jt.b] || !B.awake[jt.b];
+            if (!(fa && fb))
+              solve_d6_dev(jt, jlam + 6 * (size_t)j, B, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]), asq(srot[jt.b]));
+          }
+          continue;
+        }
+        project_one(B, R, k, shock != 0, up, c_pt, c_n, lbv, split_l, split_a);
+      }
       __syncwarp();
     }
+  }
+}
+// Restitution (solver.rs:1001-1008) for the rows the W6 passes leave to it -- contacts on jointed
+// bodies: one normal update each, in contact order, after the shock pass.
+__global__ void k_restitution(uint32_t nisl, uint32_t nc, Sched S, RowsV R, BodiesV B, float* acc_jn) {
+  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= nisl) return;
+  uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+  for (uint32_t L = 0; L < nl; ++L) {
+    uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+    for (uint32_t s = s0 + lane; s < s1; s += 32) {
+      uint32_t k = S.ord[s];
+      if (k >= nc) continue;
+      Row r = ld_row(R, k);
+      if ((r.flags & RF_TOI) || r.rbias <= 0.0f || acc_jn[k] <= 0.0f) continue;
+      float v = dot(rel_vel(B, r), r.n);
+      float old = acc_jn[k];
+      float nw = rmax(old + (r.rbias - v) * r.m_n, 0.0f);
+      acc_jn[k] = nw;
+      contact_impulse(B, r, r.n * (nw - old));
+    }
+    __syncwarp();
   }
 }
 
@@ -776,9 +852,9 @@ __global__ void k_touching(uint32_t nc, const uint32_t* __restrict__ c_a, const 
 // Velocity from corrections (step.rs:316-376), last velocities (:378-379), sleep (sleep.rs:59-80).
 __global__ void k_stage6(uint32_t nb, BodiesV B, const float4* __restrict__ orig_pos, const float4* __restrict__ pred_pos,
                          const float4* __restrict__ pred_rot, const float4* __restrict__ split_l,
-                         const float4* __restrict__ split_a, const uint8_t* __restrict__ touching, float dt,
-                         float4* last_lin, uint8_t* awake, uint16_t* sleep_ticks, const uint8_t* __restrict__ sleep_allowed,
-                         uint32_t* stats) {
+                         const float4* __restrict__ split_a, const uint8_t* __restrict__ touching,
+                         const uint8_t* __restrict__ jointed, float dt, float4* last_lin, uint8_t* awake,
+                         uint16_t* sleep_ticks, const uint8_t* __restrict__ sleep_allowed, uint32_t* stats) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nb) return;
   float4 L = B.lin[i], A = B.ang[i];
@@ -787,7 +863,10 @@ __global__ void k_stage6(uint32_t nb, BodiesV B, const float4* __restrict__ orig
     float4 P = B.pos[i];
     f3 np = xyz(P);
     q4 nr = asq(B.rot[i]);
-    f3 d_lin = (np - xyz(pred_pos[i])) - xyz(split_l[i]);
+    // split impulse only outside articulations (step.rs:324-329)
+    const bool jb = jointed && jointed[i];
+    const f3 sl = jb ? mk3(0, 0, 0) : xyz(split_l[i]), sa = jb ? mk3(0, 0, 0) : xyz(split_a[i]);
+    f3 d_lin = (np - xyz(pred_pos[i])) - sl;
     if (!vzero(d_lin)) vl = vl + d_lin / dt;
     if (touching[i] && vl.y < 0.0f) {
       vl.y = 0.0f;
@@ -800,7 +879,7 @@ __global__ void k_stage6(uint32_t nb, BodiesV B, const float4* __restrict__ orig
       q4 dq = qmul(nr, qconj(pr));
       f3 d_ang = mk3(dq.x, dq.y, dq.z) * 2.0f;
       if (dq.w < 0.0f) d_ang = -d_ang;
-      va = va + (d_ang - xyz(split_a[i])) / dt;
+      va = va + (d_ang - sa) / dt;  // no velocity drives: no body is motor-driven
     }
     if (vfin(vl)) L = f4(fin_v(vl), L.w);
     if (vfin(va)) A = f4(fin_v(va), A.w);
@@ -887,8 +966,8 @@ __global__ void k_body_groups(uint32_t n, const uint32_t* __restrict__ ord, cons
   if (s >= n) return;
   uint32_t r = ord[s], g = key[s], f = flags[r];
   uint2 x = ab[r];
-  if (f & RF_WA) body_grp[x.x] = g;
-  if (f & RF_WB) body_grp[x.y] = g;
+  if (f & RF_TA) body_grp[x.x] = g;
+  if (f & RF_TB) body_grp[x.y] = g;
 }
 __global__ void k_flag_grouped(uint32_t nb, const uint32_t* __restrict__ body_grp, uint32_t* flag) {
   uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -960,7 +1039,9 @@ struct SRowsV {
 };
 // Rows in schedule order, with local body indices and the constant velocity of a side that
 // cannot move (a static or sleeping body's velocity at the contact; zero for terrain).
-__global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, RowsV R, BodiesV B,
+// Joint rows (index >= nc) carry no warm-cache index and no prediction; the fixed side of an angular
+// joint row is that body's angular velocity.
+__global__ void k_permute_rows(uint32_t n, uint32_t nc, const uint32_t* __restrict__ ord, RowsV R, BodiesV B,
                                const uint32_t* __restrict__ body_local, const int* __restrict__ wm_idx,
                                const uint32_t* __restrict__ row_lisl, const float* __restrict__ pred3,
                                const uint32_t* __restrict__ row_group, const uint32_t* __restrict__ g_class,
@@ -971,25 +1052,27 @@ __global__ void k_permute_rows(uint32_t n, const uint32_t* __restrict__ ord, Row
   uint2 x = R.ab[r];
   uint32_t f = R.flags[r];
   float4 ra = R.ra[r], rb = R.rb[r];
-  O.loc[s] = make_uint2((f & RF_WA) ? body_local[x.x] : 0xFFFFFFFFu, (f & RF_WB) ? body_local[x.y] : 0xFFFFFFFFu);
+  O.loc[s] = make_uint2((f & RF_TA) ? body_local[x.x] : 0xFFFFFFFFu, (f & RF_TB) ? body_local[x.y] : 0xFFFFFFFFu);
   O.flags[s] = (f & 0xFFFFu) | (row_lisl[r] << 16);  // bits 16..31: the row's island inside its group
   O.inv[s] = R.inv[r];
   O.ra[s] = ra; O.rb[s] = rb; O.n[s] = R.n[r]; O.t1[s] = R.t1[r]; O.t2[s] = R.t2[r]; O.mu[s] = R.mu[r];
   f3 va = mk3(0, 0, 0), vb = mk3(0, 0, 0);
-  if (!(f & RF_WA)) va = xyz(B.lin[x.x]) + cross(xyz(B.ang[x.x]), xyz(ra));
-  if (!(f & RF_TERRAIN) && !(f & RF_WB)) vb = xyz(B.lin[x.y]) + cross(xyz(B.ang[x.y]), xyz(rb));
+  const bool jang = (f & RF_JANG) != 0;
+  if (!(f & RF_TA)) va = jang ? xyz(B.ang[x.x]) : xyz(B.lin[x.x]) + cross(xyz(B.ang[x.x]), xyz(ra));
+  if (!(f & RF_TERRAIN) && !(f & RF_TB)) vb = jang ? xyz(B.ang[x.y]) : xyz(B.lin[x.y]) + cross(xyz(B.ang[x.y]), xyz(rb));
   O.va[s] = f4(va);
   O.vb[s] = f4(vb);
   O.jn[s] = 0.0f;
   O.jt[s] = make_float2(0.0f, 0.0f);
-  O.wm[s] = wm_idx[r];
+  const bool contact = r < nc;
+  O.wm[s] = contact ? wm_idx[r] : -1;
   // predictions reach every solver class except the global-memory one (islands beyond 4500 bodies)
   float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   // (cold_only: only rows the previous tick's cache has nothing for)
-  if (pred3 && g_class[row_group[r]] != 2u && (!cold_only || wm_idx[r] < 0))
+  if (contact && pred3 && g_class[row_group[r]] != 2u && (!cold_only || wm_idx[r] < 0))
     p = make_float4(pred3[3 * r], pred3[3 * r + 1], pred3[3 * r + 2], 1.0f);
   O.pred[s] = p;
-  if (pred_used) pred_used[r] = p;
+  if (pred_used && contact) pred_used[r] = p;
 }
 
 // Shared-memory body state of one group
@@ -1085,11 +1168,51 @@ __device__ __forceinline__ void impulse_reg(f3& lin, f3& ang, float im, const m3
 __device__ __forceinline__ m3 load_iw(const float* q) {
   return mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
 }
+// ---- joint velocity rows (solver.rs:291-307 joint_row_vel / joint_row_apply, :821-830 the update):
+// v = (v_b - v_a) . u over the anchors (linear) or the angular velocities (angular); the impulse
+// stays in [lam_min, lam_max] = (mu_s, mu_k) of the row; bias is the target, m_n = 1 / k.
+__device__ __forceinline__ void joint_apply_reg(f3& la, f3& aa, f3& lb, f3& ab, const SRow& r, const m3& qa, const m3& qb,
+                                                float ima, float imb, float lam) {
+  f3 p = r.n * lam;
+  const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
+  if (r.flags & RF_JANG) {
+    if (ia) { f3 t = -p; if (ima > 0.0f && vfin(t)) aa = fin_v(aa + mvec(qa, t)); }
+    if (ib && imb > 0.0f && vfin(p)) ab = fin_v(ab + mvec(qb, p));
+  } else {
+    if (ia) { f3 nj = -p; impulse_reg(la, aa, ima, qa, nj, cross(r.ra, nj)); }
+    if (ib) impulse_reg(lb, ab, imb, qb, p, cross(r.rb, p));
+  }
+}
+__device__ __noinline__ void joint_row_core(float4* lin, float4* ang, const SRow& r, const m3& qa, const m3& qb,
+                                               float ima, float imb, float& acc, float* d3) {
+  const bool ha = r.la != 0xFFFFFFFFu, hb = r.lb != 0xFFFFFFFFu;
+  const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
+  float4 LA = make_float4(0, 0, 0, 0), AA = LA, LB = LA, AB = LA;
+  if (ha) { LA = lin[r.la]; AA = ang[r.la]; }
+  if (hb) { LB = lin[r.lb]; AB = ang[r.lb]; }
+  f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
+  f3 va, vb;
+  if (r.flags & RF_JANG) { va = ha ? aa : r.vfix; vb = hb ? ab : r.vfix; }
+  else { va = ha ? la + cross(aa, r.ra) : r.vfix; vb = hb ? lb + cross(ab, r.rb) : r.vfix; }
+  float v = dot(vb - va, r.n);
+  float old = acc;
+  float nw = clampf(old + (r.bias - v) * r.m_n, r.mu_s, r.mu_k);
+  acc = nw;
+  if (nw != old) {
+    joint_apply_reg(la, aa, lb, ab, r, qa, qb, ima, imb, nw - old);
+    if (ia) { lin[r.la] = f4(la, LA.w); ang[r.la] = f4(aa, AA.w); }
+    if (ib) { lin[r.lb] = f4(lb, LB.w); ang[r.lb] = f4(ab, AB.w); }
+  }
+  d3[0] = nw - old;
+  d3[1] = 0.0f;
+  d3[2] = 0.0f;
+}
 // The row update on bodies whose velocities live in lin / ang (shared memory), with both bodies'
 // world inverse inertia and inverse mass passed in; jn / jt are the row's accumulators, d3
 // receives (new_jn - old_jn, friction deltas) for the residual.
 __device__ __forceinline__ void pgs_row_core(float4* lin, float4* ang, const SRow& r, const m3& qa, const m3& qb,
                                              float ima, float imb, float& jn_acc, float2& jt_acc, float* d3) {
+  if (r.flags & RF_JOINT) { joint_row_core(lin, ang, r, qa, qb, ima, imb, jn_acc, d3); return; }
   const bool ha = r.la != 0xFFFFFFFFu, hb = !(r.flags & RF_TERRAIN) && r.lb != 0xFFFFFFFFu;
   const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
   float4 LA = make_float4(0, 0, 0, 0), AA = LA, LB = LA, AB = LA;
@@ -1186,6 +1309,10 @@ __device__ __forceinline__ float warm_trial_err(const float4* lin, const float4*
 __device__ __forceinline__ int warm_select(float4* lin, float4* ang, const SRow& r, const m3& qa, const m3& qb, float ima,
                                            float imb, bool has_ref, float4 ea, float4 eb, float4 pred, float& jn_acc,
                                            float2& jt_acc) {
+  if (r.flags & RF_JOINT) {  // impulse applied by k_joint_warm before every contact's warm start
+    jn_acc = (r.flags & RF_JWARM) ? r.t2.x : 0.0f;
+    return 0;
+  }
   if (pred.w == 0.0f) {
     if (has_ref) warm_core(lin, ang, r, qa, qb, ima, imb, ea, eb, jn_acc, jt_acc);
     return 0;
@@ -1319,8 +1446,8 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
     for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1]; i += NT) {
       int e = R.wm[base + i];
       float4 p = R.pred[base + i];
-      if (e < 0 && p.w == 0.0f) continue;
       const SRow& r = W.rows[i];
+      if (e < 0 && p.w == 0.0f && !(r.flags & RF_JWARM)) continue;
       const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
       const m3 qa = load_iw(ia ? B.Iw + 9 * (size_t)r.la : B.Iw), qb = load_iw(ib ? B.Iw + 9 * (size_t)r.lb : B.Iw);
       n_pred += warm_select(B.lin, B.ang, r, qa, qb, ia ? B.im[r.la] : 0.0f, ib ? B.im[r.lb] : 0.0f, e >= 0,
@@ -1534,7 +1661,7 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
     for (uint32_t s = lvl[L] + tid; s < lvl[L + 1]; s += CH) {
       int e = R.wm[s];
       float4 pr = R.pred[s];
-      if (e < 0 && pr.w == 0.0f) continue;
+      if (e < 0 && pr.w == 0.0f && !(R.flags[s] & RF_JWARM)) continue;
       SRow r = ld_srow(R, s);
       const float4* x = X + 7 * (size_t)s;
       float q[24];
@@ -1718,6 +1845,16 @@ __global__ void k_warm_merge_kept(uint32_t n, const uint4* __restrict__ kk, cons
   ok[p] = kk[j]; oa[p] = ka[j]; ob[p] = kb[j];
 }
 
+// Position i of the scheduled-row scan: joint rows (index nc .. nc + njr) first, then the contacts;
+// the row there and whether it is scheduled (a root was found for it).
+__global__ void k_joint_first_order(uint32_t n, uint32_t nc, uint32_t njr, const uint32_t* __restrict__ root,
+                                    uint32_t* idx, uint8_t* fl) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t r = i < njr ? nc + i : i - njr;
+  idx[i] = r;
+  fl[i] = root[r] != 0xFFFFFFFFu ? 1 : 0;
+}
 // ------------------------------------------------------------------ host driver
 static void build_schedule(WorldGpu::Scratch& S, uint32_t* W_err, uint32_t nsched, uint32_t nisl, const uint32_t* ord_in,
                            const uint32_t* isl_start, const uint32_t* isl_cnt, uint32_t* ord_out, DBuf<uint32_t>& lvl_off,
@@ -1751,6 +1888,10 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   const uint32_t nb = W.num_bodies(), nc = ctx.nc;
   uint32_t* stats = W.d_stats.p;
   W.pred_valid_ = false;
+  // joints: their rows follow the contact rows in the row arrays (index nc + r)
+  const uint32_t nj = W.num_joints();
+  const uint8_t* jointed = nj ? W.jointed_d.p : nullptr;
+  uint32_t njr = 0;
   S.constrained.ensure(nb + 1); S.loaded.ensure(nb + 1); S.ballistic.ensure(nb + 1); S.touching.ensure(nb + 1);
   S.uf.ensure(nb + 1); S.uf2.ensure(nb + 1); S.body_level.ensure(nb + 1); S.root_mark.ensure(nb + 1);
   S.Iw.ensure(9 * (size_t)nb + 9);
@@ -1768,11 +1909,16 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   P.begin(PH_ISLANDS, st);
   // ---- the reference's islands: their count, and whether the solve runs (step.rs:146-150)
   uint32_t nref = 0;
-  if (nc > 0 && nb > 0) {
+  if ((nc > 0 || nj > 0) && nb > 0) {
     k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf2.p); RP_COUNT_LAUNCH(1);
     RP_CUDA(cudaMemsetAsync(S.root_mark.p, 0, sizeof(uint32_t) * nb, st));
-    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 0, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf2.p); RP_COUNT_LAUNCH(1);
-    k_ref_island_marks<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, S.uf2.p, S.root_mark.p); RP_COUNT_LAUNCH(1);
+    joints_ref_islands(W, S.uf2.p, nullptr, true, st);
+    if (nc) {
+      k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 0, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, nullptr,
+                                               S.uf2.p); RP_COUNT_LAUNCH(1);
+      k_ref_island_marks<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, S.uf2.p, S.root_mark.p); RP_COUNT_LAUNCH(1);
+    }
+    joints_ref_islands(W, S.uf2.p, S.root_mark.p, false, st);
     S.tmp32.ensure(nb + 1);
     nref = exclusive_scan_total(S, S.root_mark.p, S.tmp32.p, nb, st);
   }
@@ -1786,29 +1932,43 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     // ---- rows
     P.begin(PH_ROWS, st);
     k_world_inertia<<<nblk(nb), T, 0, st>>>(nb, W.rot.p, W.inv_mass.p, W.inv_I.p, S.Iw.p); RP_COUNT_LAUNCH(1);
-    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf.p); RP_COUNT_LAUNCH(1);
-    k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 1, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, S.uf.p); RP_COUNT_LAUNCH(1);
-    S.r_ab.ensure(nc); S.r_flags.ensure(nc); S.r_inv.ensure(nc); S.r_ra.ensure(nc); S.r_rb.ensure(nc); S.r_n.ensure(nc);
-    S.r_t1.ensure(nc); S.r_t2.ensure(nc); S.r_mu.ensure(nc); S.r_la.ensure(nc); S.acc_jn.ensure(nc); S.acc_jt.ensure(nc);
-    S.wm_idx.ensure(nc); S.row_isl.ensure(nc + 1); S.row_isl2.ensure(nc + 1);
+    njr = joints_count_rows(W, ctx.dt, B, st);
+    const uint32_t nall = nc + njr;
+    if (njr) {  // the level of every scheduled row is written, joint rows included
+      S.row_level.ensure(nall + 1);
+      RP_CUDA(cudaMemsetAsync(S.row_level.p, 0xFF, sizeof(uint32_t) * (nall + 1), st));
+    }
+    S.r_ab.ensure(nall + 1); S.r_flags.ensure(nall + 1); S.r_inv.ensure(nall + 1); S.r_ra.ensure(nall + 1);
+    S.r_rb.ensure(nall + 1); S.r_n.ensure(nall + 1); S.r_t1.ensure(nall + 1); S.r_t2.ensure(nall + 1);
+    S.r_mu.ensure(nall + 1); S.r_la.ensure(nall + 1); S.acc_jn.ensure(nall + 1); S.acc_jt.ensure(nall + 1);
+    S.wm_idx.ensure(nc + 1); S.row_isl.ensure(nall + 1); S.row_isl2.ensure(nall + 1);
     R = RowsV{S.r_ab.p, S.r_flags.p, S.r_inv.p, S.r_ra.p, S.r_rb.p, S.r_n.p, S.r_t1.p, S.r_t2.p, S.r_mu.p, S.r_la.p};
-    k_build_rows<<<nblk(nc), T, 0, st>>>(nc, ctx.dt, S.c_a.p, S.c_b.p, S.c_pt.p, S.c_n.p, W.col_body.p, W.col_mat.p,
-                                         ctx.hf_mat, W.pair_table.p, B, S.pre_lin.p, S.pre_ang.p, R, S.acc_jn.p,
-                                         S.acc_jt.p, S.uf.p, S.row_isl.p); RP_COUNT_LAUNCH(1);
+    // solve islands: joint rows, then contacts (a sleeping jointed side counts), then every row's root
+    k_iota<<<nblk(nb), T, 0, st>>>(nb, S.uf.p); RP_COUNT_LAUNCH(1);
+    joints_build_rows(W, ctx.dt, B, R, nc, S.acc_jn.p, S.acc_jt.p, S.uf.p, st);
+    if (nc) {
+      k_union_contacts<<<nblk(nc), T, 0, st>>>(nc, 1, S.c_a.p, S.c_b.p, W.col_body.p, W.inv_mass.p, W.awake.p, jointed,
+                                               S.uf.p); RP_COUNT_LAUNCH(1);
+      k_build_rows<<<nblk(nc), T, 0, st>>>(nc, ctx.dt, S.c_a.p, S.c_b.p, S.c_pt.p, S.c_n.p, W.col_body.p, W.col_mat.p,
+                                           ctx.hf_mat, W.pair_table.p, B, S.pre_lin.p, S.pre_ang.p, R, S.acc_jn.p,
+                                           S.acc_jt.p, S.uf.p, S.row_isl.p, jointed); RP_COUNT_LAUNCH(1);
+    }
+    joints_row_roots(W, R, nc, njr, S.uf.p, S.row_isl.p, st);
     P.end(PH_ROWS, st);
     P.begin(PH_SCHED, st);
     // ---- solve islands: roots of scheduled rows -> dense island ids, rows grouped by island
-    S.flag8.ensure(nc + 1); S.rows_sched.ensure(nc + 1); S.rows_sched2.ensure(nc + 1);
-    S.tmp32.ensure(nc + 1); S.tmp32b.ensure(nc + 1);
+    S.flag8.ensure(nall + 1); S.rows_sched.ensure(nall + 1); S.rows_sched2.ensure(nall + 1);
+    S.tmp32.ensure(nall + 1); S.tmp32b.ensure(nall + 1);
     uint32_t nsched = 0;
-    k_flag_sched<<<nblk(nc), T, 0, st>>>(nc, S.row_isl.p, S.flag8.p); RP_COUNT_LAUNCH(1);
+    // scheduled rows in the order joint rows, then contacts: the stable sort by island below keeps
+    // every island's joint rows ahead of its contacts
+    k_joint_first_order<<<nblk(nall), T, 0, st>>>(nall, nc, njr, S.row_isl.p, S.tmp32b.p, S.flag8.p); RP_COUNT_LAUNCH(1);
     {
-      cub::CountingInputIterator<uint32_t> it0(0);
       size_t bytes = 0;
       S.counts.ensure(4);
-      RP_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, it0, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nc, st));
+      RP_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, S.tmp32b.p, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nall, st));
       S.cub_tmp.ensure(bytes + 16);
-      RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, it0, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nc, st));
+      RP_CUDA(cub::DeviceSelect::Flagged(S.cub_tmp.p, bytes, S.tmp32b.p, S.flag8.p, S.rows_sched.p, S.counts.p + 3, nall, st));
       RP_COUNT_LAUNCH(2);
       RP_CUDA(cudaMemcpyAsync(&nsched, S.counts.p + 3, 4, cudaMemcpyDeviceToHost, st));
       RP_CUDA(cudaStreamSynchronize(st));
@@ -1845,10 +2005,10 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cudaMemsetAsync(S.g_start.p, 0, sizeof(uint32_t) * (ng + 1), st));
       RP_CUDA(cudaMemsetAsync(S.g_cnt.p, 0, sizeof(uint32_t) * (ng + 1), st));
       k_group_ranges<<<nblk(nsched), T, 0, st>>>(nsched, S.g_key2.p, S.g_start.p, S.g_cnt.p); RP_COUNT_LAUNCH(1);
-      S.row_isl2.ensure(nc + 1);
+      S.row_isl2.ensure(nall + 1);
       k_scatter_u32<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.row_isl2.p); RP_COUNT_LAUNCH(1);  // group of each row
       // each row's island inside its group (the per-island residual stop)
-      S.row_islid.ensure(nc + 1); S.row_lisl.ensure(nc + 1); S.li_flag.ensure(nsched + 1); S.li_pre.ensure(nsched + 1);
+      S.row_islid.ensure(nall + 1); S.row_lisl.ensure(nall + 1); S.li_flag.ensure(nsched + 1); S.li_pre.ensure(nsched + 1);
       S.g_nisl.ensure(ng + 1);
       k_row_island<<<nblk(nsched), T, 0, st>>>(nsched, S.rows_sched2.p, S.woff.p, S.wpos.p, S.row_islid.p); RP_COUNT_LAUNCH(1);
       k_local_isl_flags<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.row_islid.p, S.li_flag.p); RP_COUNT_LAUNCH(1);
@@ -1903,6 +2063,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     // ---- warm start matching (solver.rs:717-762)
     k_warm_match<<<nblk(nc), T, 0, st>>>(nc, S.r_ab.p, S.r_flags.p, S.r_la.p, W.warm_key.p, W.warm_a.p, W.n_warm,
                                          S.wm_idx.p, stats + STAT_WARM_MATCHED, stats + STAT_ERR); RP_COUNT_LAUNCH(1);
+    if (njr && ng) { k_joint_warm<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, nc, SM, R, B, S.acc_jn.p); RP_COUNT_LAUNCH(1); }
     k_warm_unscheduled<<<nblk(nc), T, 0, st>>>(nc, R, B, S.wm_idx.p, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p); RP_COUNT_LAUNCH(1);
     // learned warm start: row features, and the model's prediction of every row's impulse
     const bool learned = W.model_ != nullptr;
@@ -1931,7 +2092,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       if (learned) RP_CUDA(cudaMemsetAsync(S.pred_used.p, 0, 16 * (size_t)nc, st));  // unscheduled rows: none
       SRowsV SR{S.s_loc.p, S.s_flags.p, S.s_inv.p, S.s_ra.p, S.s_rb.p, S.s_n.p, S.s_t1.p, S.s_t2.p, S.s_mu.p, S.s_va.p,
                 S.s_vb.p, S.s_jn.p, S.s_jt.p, S.s_wm.p, S.s_pred.p};
-      k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, S.row_lisl.p,
+      k_permute_rows<<<nblk(nsched), T, 0, st>>>(nsched, nc, S.ord_main.p, R, B, S.body_local.p, S.wm_idx.p, S.row_lisl.p,
                                                  learned ? S.pred3.p : nullptr, S.row_isl2.p, S.g_class.p,
                                                  learned ? S.pred_used.p : nullptr, W.pred_cold_only_ ? 1u : 0u, SR); RP_COUNT_LAUNCH(1);
       const float tol = resid_mode ? W.res_tol_ : 0.0f;
@@ -1974,10 +2135,11 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
         }
       }
       P.begin(PH_VEL_PACKED, st);
-      if (g_small > 0)
+      if (g_small > 0) {
         k_vel_solve_onchip<true, ONCHIP_T_PACKED><<<g_small, ONCHIP_T_PACKED, lay_packed.bytes, st>>>(
             lay_packed, 0u, g_small, nullptr, 3u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
             W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+      }
       P.end(PH_VEL_PACKED, st);
       P.begin(PH_VEL_BIG, st);
       {
@@ -2002,10 +2164,11 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           RP_COUNT_LAUNCH(1);
         }
       }
-      if (cls_n[2])
-        k_vel_solve<<<nblk(cls_n[2] * 32, 128), 128, 0, st>>>(cls_n[2], SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
+      if (cls_n[2]) {
+        k_vel_solve<<<nblk(cls_n[2] * 32, 128), 128, 0, st>>>(cls_n[2], nc, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
                                                                W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
                                                                lst(2)); RP_COUNT_LAUNCH(1);
+      }
       P.end(PH_VEL_BIG, st);
       if (big) {
         for (int k = 0; k < ISLAND_BUCKETS; ++k) {
@@ -2015,6 +2178,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       }
     }
     P.end(PH_VEL_SOLVE, st);
+    joints_store_warm(W, R, nc, S.acc_jn.p, st);
     if (W.feat_log_) {
       S.targets.ensure(3 * (size_t)nc + 3);
       k_row_targets<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.targets.p); RP_COUNT_LAUNCH(1);
@@ -2079,31 +2243,38 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                      S.lvl_start_vs, S.nlev_vs, nullptr, nullptr, st);
       Sched SV{S.ord_vs.p, S.lvl_off_vs.p, S.lvl_start_vs.p, S.nlev_vs.p};
       k_vel_shock<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, SV, R, B, ctx.up, S.acc_jn.p); RP_COUNT_LAUNCH(1);
+      // restitution for the contacts W6 leaves alone (jointed bodies); without joints there are none
+      if (nj) { k_restitution<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, nc, SM, R, B, S.acc_jn.p); RP_COUNT_LAUNCH(1); }
     }
     P.end(PH_VEL_SHOCK, st);
     k_after_solve<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.loaded.p, S.c_n.p, stats); RP_COUNT_LAUNCH(1);
   }
   // ---- stage 4
   P.begin(PH_BALLISTIC, st);
-  if (nc > 0) k_constrained<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, S.constrained.p); RP_COUNT_LAUNCH(1);
-  if (nb > 0) k_ballistic_init<<<nblk(nb), T, 0, st>>>(nb, S.constrained.p, S.loaded.p, S.ballistic.p); RP_COUNT_LAUNCH(1);
+  if (nc > 0) { k_constrained<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, W.col_body.p, S.constrained.p); RP_COUNT_LAUNCH(1); }
+  joints_mark_constrained(W, S.constrained.p, st);
+  if (nb > 0) { k_ballistic_init<<<nblk(nb), T, 0, st>>>(nb, S.constrained.p, S.loaded.p, jointed, S.ballistic.p); RP_COUNT_LAUNCH(1); }
   Sched SM{S.ord_main.p, S.lvl_off.p, S.lvl_start.p, S.nlev.p};
-  if (ctx.nisl > 0)
+  if (ctx.nisl > 0) {
     k_ballistic<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SM, R, B, S.c_pt.p, S.c_n.p, W.last_lin.p, ctx.dt,
                                                           S.ballistic.p); RP_COUNT_LAUNCH(1);
+  }
   P.end(PH_BALLISTIC, st);
   P.begin(PH_INTEGRATE, st);
-  if (nb > 0)
+  if (nb > 0) {
     k_integrate<<<nblk(nb, 128), 128, 0, st>>>(nb, B, S.ballistic.p, W.last_lin.p, ctx.dt, S.orig_pos.p, S.orig_rot.p,
                                                S.pred_pos.p, S.pred_rot.p); RP_COUNT_LAUNCH(1);
+  }
   P.end(PH_INTEGRATE, st);
   // ---- stage 5: position pass (step.rs:284-309); its contacts are the scheduled rows
   if (ctx.nisl > 0) {
     P.begin(PH_POS_ITER, st);
     S.pc_lb.ensure(nc + 1);
     k_pos_anchors<<<nblk(nc), T, 0, st>>>(nc, R, S.c_pt.p, S.orig_pos.p, S.orig_rot.p, S.pc_lb.p); RP_COUNT_LAUNCH(1);
-    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SM, R, B, (int)W.iters_p_, 0, ctx.up, S.c_pt.p,
-                                                               S.c_n.p, S.pc_lb.p, S.split_l.p, S.split_a.p); RP_COUNT_LAUNCH(1);
+    if (nj) RP_CUDA(cudaMemsetAsync(W.jlam.p, 0, sizeof(float) * 6 * (size_t)nj, st));  // Joints::begin_step
+    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, nc, SM, R, B, (int)W.iters_p_, 0, ctx.up, S.c_pt.p,
+                                                               S.c_n.p, S.pc_lb.p, S.split_l.p, S.split_a.p, W.joints_d.p,
+                                                               W.jlam.p, S.orig_pos.p, S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
     P.end(PH_POS_ITER, st);
     P.begin(PH_POS_SHOCK, st);
     // shock projection in (height key, index) order at the poses the iterations left
@@ -2115,17 +2286,19 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     build_schedule(S, stats + STAT_ERR, nsched, ctx.nisl, S.rows_sched2.p, S.g_start.p, S.g_cnt.p, S.ord_ps.p, S.lvl_off_ps,
                    S.lvl_start_ps, S.nlev_ps, nullptr, nullptr, st);
     Sched SP{S.ord_ps.p, S.lvl_off_ps.p, S.lvl_start_ps.p, S.nlev_ps.p};
-    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, SP, R, B, 1, 1, ctx.up, S.c_pt.p, S.c_n.p,
-                                                               S.pc_lb.p, S.split_l.p, S.split_a.p); RP_COUNT_LAUNCH(1);
+    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, nc, SP, R, B, 1, 1, ctx.up, S.c_pt.p, S.c_n.p,
+                                                               S.pc_lb.p, S.split_l.p, S.split_a.p, W.joints_d.p,
+                                                               W.jlam.p, S.orig_pos.p, S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
     P.end(PH_POS_SHOCK, st);
   }
   // ---- stages 6 and 7
   P.begin(PH_STAGE6, st);
-  if (nc > 0) k_touching<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, S.c_pt.p, W.col_body.p, S.touching.p); RP_COUNT_LAUNCH(1);
-  if (nb > 0)
+  if (nc > 0) { k_touching<<<nblk(nc), T, 0, st>>>(nc, S.c_a.p, S.c_b.p, S.c_pt.p, W.col_body.p, S.touching.p); RP_COUNT_LAUNCH(1); }
+  if (nb > 0) {
     k_stage6<<<nblk(nb), T, 0, st>>>(nb, B, S.orig_pos.p, S.pred_pos.p, S.pred_rot.p, S.split_l.p, S.split_a.p,
-                                     S.touching.p, ctx.dt, W.last_lin.p, W.awake.p, W.sleep_ticks.p, W.sleep_allowed.p,
+                                     S.touching.p, jointed, ctx.dt, W.last_lin.p, W.awake.p, W.sleep_ticks.p, W.sleep_allowed.p,
                                      stats); RP_COUNT_LAUNCH(1);
+  }
   uint32_t ncap = W.capacity() > nb ? W.capacity() : nb;
   k_count_sleeping<<<nblk(ncap), T, 0, st>>>(ncap, W.awake.p, stats); RP_COUNT_LAUNCH(1);
   P.end(PH_STAGE6, st);

@@ -420,11 +420,13 @@ bool WorldGpu::remove_body(uint32_t id) {  // World::remove_body (world.rs:696-7
     }
   }
   drop_warm_of(id);
+  drop_joint_warm_of(id);
   RP_CUDA(cudaStreamSynchronize(stream_));
   return true;
 }
 void WorldGpu::set_body_pose(uint32_t id, const float p[7]) {  // world.rs:501-513
   drop_warm_of(id);
+  drop_joint_warm_of(id);
   k_set_pose<<<1, 1, 0, stream_>>>(id, make_float4(p[0], p[1], p[2], 0), make_float4(p[3], p[4], p[5], p[6]), pos.p, rot.p); RP_COUNT_LAUNCH(1);
   RP_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -478,6 +480,7 @@ void WorldGpu::clear_heightfield() { has_hf_ = false; }
 // ------------------------------------------------------------------ the tick
 void WorldGpu::step(float dt) {
   upload_worlds();
+  upload_joints();
   AllocStreamScope alloc_scope(stream_);
   tick_ += 1;
   RP_CUDA(cudaMemsetAsync(d_stats.p, 0, STAT_COUNT * 4, stream_));
@@ -583,6 +586,12 @@ SnapshotGpu* WorldGpu::snapshot_create() {  // lib.rs:1707-1752 + carried_state 
   cp(s->awake.p, awake.p, s->cap); cp(s->ticks.p, sleep_ticks.p, 2 * (size_t)s->cap);
   cp(s->wk.p, warm_key.p, 16 * (size_t)n_warm); cp(s->wa.p, warm_a.p, 16 * (size_t)n_warm);
   cp(s->wb.p, warm_b.p, 16 * (size_t)n_warm);
+  upload_joints();
+  s->nj = num_joints();
+  s->jw_n.ensure(s->nj + 1); s->jw_tag.ensure(12 * (size_t)s->nj + 12); s->jw_lam.ensure(12 * (size_t)s->nj + 12);
+  cp(s->jw_n.p, jw_n.p, 4 * (size_t)s->nj);
+  cp(s->jw_tag.p, jw_tag.p, 12 * (size_t)s->nj);
+  cp(s->jw_lam.p, jw_lam.p, 48 * (size_t)s->nj);
   RP_CUDA(cudaStreamSynchronize(stream_));
   return s;
 }
@@ -604,15 +613,28 @@ void WorldGpu::snapshot_restore_exact(const SnapshotGpu* s) {
   cp(warm_key.p, s->wk.p, 16 * (size_t)s->n_warm); cp(warm_a.p, s->wa.p, 16 * (size_t)s->n_warm);
   cp(warm_b.p, s->wb.p, 16 * (size_t)s->n_warm);
   n_warm = s->n_warm;
+  restore_joint_warm(s);
   RP_CUDA(cudaStreamSynchronize(stream_));
+}
+// The joint cache as the snapshot held it; joints added since have no entry.
+void WorldGpu::restore_joint_warm(const SnapshotGpu* s) {
+  upload_joints();
+  uint32_t nj = num_joints(), n = s->nj < nj ? s->nj : nj;
+  if (n) {
+    RP_CUDA(cudaMemcpyAsync(jw_n.p, s->jw_n.p, 4 * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
+    RP_CUDA(cudaMemcpyAsync(jw_tag.p, s->jw_tag.p, 12 * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
+    RP_CUDA(cudaMemcpyAsync(jw_lam.p, s->jw_lam.p, 48 * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
+  }
+  if (nj > n) RP_CUDA(cudaMemsetAsync(jw_n.p + n, 0xFF, 4 * (size_t)(nj - n), stream_));
 }
 void WorldGpu::snapshot_restore(const SnapshotGpu* s) {  // lib.rs:1754-1793 + restore_carried_state
   tick_ = s->tick;
   uint32_t n = s->nb < nb_ ? s->nb : nb_;
   const int T = 256;
-  if (n)
+  if (n) {
     k_restore_bodies<<<(n + T - 1) / T, T, 0, stream_>>>(n, s->pos.p, s->rot.p, s->lin.p, s->ang.p, s->last_lin.p,
                                                           alive_d.p, pos.p, rot.p, lin.p, ang.p, last_lin.p); RP_COUNT_LAUNCH(1);
+  }
   uint32_t ncap = s->cap < (cap_b_ > nb_ ? cap_b_ : nb_) ? s->cap : (cap_b_ > nb_ ? cap_b_ : nb_);
   if (ncap) {
     RP_CUDA(cudaMemcpyAsync(awake.p, s->awake.p, ncap, cudaMemcpyDeviceToDevice, stream_));
@@ -626,6 +648,8 @@ void WorldGpu::snapshot_restore(const SnapshotGpu* s) {  // lib.rs:1754-1793 + r
   }
   n_warm = s->n_warm;
   filter_warm(1, 0);
+  restore_joint_warm(s);
+  filter_joint_warm_alive();
   RP_CUDA(cudaStreamSynchronize(stream_));
 }
 void WorldGpu::snapshot_free(SnapshotGpu* s) { delete s; }

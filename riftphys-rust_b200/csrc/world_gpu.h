@@ -22,6 +22,7 @@
 namespace rp {
 
 class WarmModel;
+struct JointGpu;
 
 struct StepStatsHost {
   uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
@@ -100,6 +101,42 @@ class WorldGpu {
   bool batch_ = false, worlds_dirty_ = false;
   DBuf<uint32_t> col_world, world_col_start;           // per collider; per world (+ end)
   void upload_worlds();
+
+  // ---- D6 joints (world.rs:718-720, 966-968; bodies.rs:326-391): ball and hinge joints with
+  // per-axis limits. Joint ids are 0-based in creation order. In a batch, a joint joins two
+  // bodies of one world and joints come in world order, so each world's joints form one
+  // contiguous id range.
+  struct JointHost {
+    uint32_t a, b;
+    float fa[7], fb[7];            // frame in body A / B: pos xyz, quat xyzw
+    bool en[6], lim[6];            // t0 t1 t2 r0 r1 r2
+    float lo[6], hi[6];
+    int hinge;                     // stored hinge axis (add_hinge), -1 none
+  };
+  uint32_t num_joints() const { return (uint32_t)h_joints_.size(); }
+  uint32_t world_of(uint32_t body) const;
+  uint32_t add_joint(uint32_t kind, uint32_t a, uint32_t b, const float fa[7], const float fb[7], uint32_t axis);
+  void set_joint_limit(uint32_t j, bool angular, uint32_t axis, bool on, float lo, float hi);
+  void upload_joints();            // the joint records, jointed bodies and jointed pairs, on change
+  std::vector<JointHost> h_joints_;
+  bool joints_dirty_ = false;
+  uint32_t jw_init_ = 0;                       // joints whose cache entry is initialised
+  DBuf<JointGpu> joints_d;
+  DBuf<uint8_t> jointed_d;                     // per body: in some joint
+  DBuf<unsigned long long> jpair_keys;         // (min body << 32 | max body), sorted, unique
+  uint32_t n_jpairs = 0;
+  // the joint warm cache (warm_joints, solver.rs:946-952): per joint the row count (0xFFFFFFFF:
+  // no entry), tags and impulses of its last solved rows
+  DBuf<uint32_t> jw_n;
+  DBuf<uint8_t> jw_tag;
+  DBuf<float> jw_lam;
+  // per tick: each joint's first row and row count, and its six XPBD multipliers
+  DBuf<uint32_t> jr_cnt, jr_off;
+  DBuf<float> jlam;
+  uint32_t njr_ = 0;
+  void drop_joint_warm_of(uint32_t body);      // drop_warm_of's joint part (world.rs:821-825)
+  void restore_joint_warm(const SnapshotGpu* s);
+  void filter_joint_warm_alive();              // restore_carried_state's joint part (world.rs:951-955)
 
   // ---- inspection
   const StepStatsHost& stats();
@@ -186,6 +223,10 @@ struct SnapshotGpu {
   DBuf<uint16_t> ticks;
   DBuf<uint4> wk;
   DBuf<float4> wa, wb;
+  uint32_t nj;
+  DBuf<uint32_t> jw_n;
+  DBuf<uint8_t> jw_tag;
+  DBuf<float> jw_lam;
 };
 
 // MassProps::from_*_density (riftphys-geom/src/mass.rs:75-145); host side.

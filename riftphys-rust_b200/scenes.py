@@ -11,6 +11,12 @@ batch         independent worlds for one batched launch: body counts log-uniform
               alternately a square box pyramid (brick half-extent U[0.25, 0.75] m per world) and a
               random pile (half-extents U[0.25, 0.75] m per box, random yaw, dropped from a grid), each
               on its own static 50x0.5x50 ground box; density 1000, dt 1/60, 16 iterations.
+ragdolls      humanoids of 15 capsules (radius U[0.05, 0.12] m, segment U[0.2, 0.5] m, mass U[1, 8] kg
+              through the density) and 14 joints each: ball joints with swing limits of +-45 degrees
+              about joint-frame y and z (two per-axis limits: the reference has no cone limit) and
+              hinges about joint-frame z limited to [-120, 0] degrees; dropped with random yaw and a
+              random initial velocity onto a 128 x 128 heightfield of the terrain scene's form;
+              dt 1/120, 24 velocity and 24 position iterations.
 terrain       bodies (40% spheres r U[0.2,0.6], 30% capsules r U[0.15,0.4] hh U[0.3,0.8], 30% boxes
               he U[0.2,0.7], density 1000) at uniform positions in a square of side `area` x [0, 60] m,
               lifted above the terrain, velocities N(0,1) per axis, falling onto a heightfield
@@ -182,3 +188,144 @@ def batch_setup(w, iterations=(16, 16)):
     w.set_pair_props(0, 0, 0.5, 0.5, 0.0, 0.08)
     w.set_iterations(*iterations)
     return 1.0 / 60.0
+
+
+# ---- ragdolls
+# bone: (parent, direction the capsule's local y takes, attach: the parent's end (+1 / -1 along its
+# local y), its centre (0), or a shoulder (+2 / -2: beside its top end, clear of the head), joint
+# kind (0 ball, 1 hinge) to the parent, hinge axis of the joint frame)
+_BONES = [
+    (-1, (1, 0, 0), 0, 0, 2),    # 0 pelvis (horizontal)
+    (0, (0, 1, 0), 0, 0, 2),     # 1 chest
+    (1, (0, 1, 0), 1, 0, 2),     # 2 head
+    (1, (-1, 0, 0), 2, 0, 2),    # 3 left upper arm (shoulder beside the top of the chest)
+    (3, (-1, 0, 0), 1, 1, 2),    # 4 left forearm (elbow hinge about z)
+    (4, (-1, 0, 0), 1, 0, 2),    # 5 left hand
+    (1, (1, 0, 0), -2, 0, 2),    # 6 right upper arm
+    (6, (1, 0, 0), 1, 1, 2),     # 7 right forearm
+    (7, (1, 0, 0), 1, 0, 2),     # 8 right hand
+    (0, (0, -1, 0), -1, 0, 2),   # 9 left thigh (hip at the pelvis' -x end)
+    (9, (0, -1, 0), 1, 1, 0),    # 10 left shin (knee hinge about x)
+    (10, (0, 0, 1), 1, 1, 0),    # 11 left foot (ankle hinge about x)
+    (0, (0, -1, 0), 1, 0, 2),    # 12 right thigh (hip at the pelvis' +x end)
+    (12, (0, -1, 0), 1, 1, 0),   # 13 right shin
+    (13, (0, 0, 1), 1, 1, 0),    # 14 right foot
+]
+_S45 = math.sqrt(0.5)
+_DIR_Q = {(0, 1, 0): (0.0, 0.0, 0.0, 1.0), (0, -1, 0): (0.0, 0.0, 1.0, 0.0),
+          (1, 0, 0): (0.0, 0.0, -_S45, _S45), (-1, 0, 0): (0.0, 0.0, _S45, _S45),
+          (0, 0, 1): (_S45, 0.0, 0.0, _S45)}
+
+
+def _qmul(a, b):
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    return (aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+            aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz)
+
+
+def _qrot(q, v):
+    x, y, z, w = q
+    u = (x, y, z)
+    uv = (u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0])
+    uuv = (u[1] * uv[2] - u[2] * uv[1], u[2] * uv[0] - u[0] * uv[2], u[0] * uv[1] - u[1] * uv[0])
+    return tuple(v[i] + 2.0 * (w * uv[i] + uuv[i]) for i in range(3))
+
+
+def _conj(q):
+    return (-q[0], -q[1], -q[2], q[3])
+
+
+def ragdoll_parts(rng, origin, yaw, v0):
+    """One humanoid: body rows (pos, rot, (r, hh), density, lin) and joints (kind, axis, parent,
+    child, frame a, frame b, limits [(angular, axis, lo, hi)]), indices local to the ragdoll."""
+    bodies, joints = [], []
+    qy = (0.0, math.sin(0.5 * yaw), 0.0, math.cos(0.5 * yaw))
+    ends = []  # per bone: (centre, local rot, half length to the end = hh + r)
+    for k, (par, d, attach, kind, hax) in enumerate(_BONES):
+        r = rng.uniform(0.05, 0.12)
+        hh = 0.5 * rng.uniform(0.2, 0.5)
+        m = rng.uniform(1.0, 8.0)
+        vol = math.pi * r * r * 2.0 * hh + 4.0 / 3.0 * math.pi * r ** 3
+        q = _DIR_Q[d]
+        if par < 0:
+            c = (0.0, 0.0, 0.0)
+        else:
+            pc, pq, pe, pr = ends[par]
+            if abs(attach) == 2:  # shoulder: below the top end, out to the side by the chest's radius
+                la = (-math.copysign(1.0, attach) * (pr + 0.1), pe - pr, 0.0)
+            else:
+                la = (0.0, attach * pe, 0.0)
+            a = tuple(pc[i] + _qrot(pq, la)[i] for i in range(3))
+            c = tuple(a[i] + d[i] * (hh + r) for i in range(3))
+            fa = (la, _conj(pq))
+            fb = ((0.0, -(hh + r), 0.0), _conj(q))
+            if kind == 0:
+                lim = [(1, 1, -math.pi / 4, math.pi / 4), (1, 2, -math.pi / 4, math.pi / 4)]
+            else:
+                lim = [(1, hax, -2.0 * math.pi / 3.0, 0.0)]
+            joints.append((kind, hax, par, k, fa, fb, lim))
+        ends.append((c, q, hh + r, r))
+        wc = _qrot(qy, c)
+        bodies.append(((origin[0] + wc[0], origin[1] + wc[1], origin[2] + wc[2]), _qmul(qy, q), (r, hh), m / vol, v0))
+    return bodies, joints
+
+
+def ragdoll_arrays(rp, n, seed, area, base_id=1, y0=None, hf=None):
+    """n ragdolls as (body desc array, joint desc array, limit array); joint and body ids assume
+    the bodies get consecutive ids from base_id and the joints from 0."""
+    rng = SplitMix64(seed)
+    pos, rot, dims, dens, lin = [], [], [], [], []
+    kinds, axes, ja, jb, fap, faq, fbp, fbq = [], [], [], [], [], [], [], []
+    lj, la, lx, llo, lhi = [], [], [], [], []
+    half = 0.5 * area
+    for i in range(n):
+        x, z = rng.uniform(-half, half), rng.uniform(-half, half)
+        y = (y0 if y0 is not None else 0.0) + rng.uniform(0.5, 3.0)
+        if hf is not None:
+            y += hf(x, z)
+        yaw = rng.uniform(0.0, 2.0 * math.pi)
+        v0 = (rng.normal(), rng.normal() - 1.0, rng.normal())
+        bodies, joints = ragdoll_parts(rng, (x, y, z), yaw, v0)
+        b0 = len(pos)
+        for (p, q, (r, hh), de, v) in bodies:
+            pos.append(p); rot.append(q); dims.append((r, hh, 0.0)); dens.append(de); lin.append(v)
+        for (kind, axis, par, ch, fa, fb, lim) in joints:
+            j = len(kinds)
+            kinds.append(kind); axes.append(axis)
+            ja.append(base_id + b0 + par); jb.append(base_id + b0 + ch)
+            fap.append(fa[0]); faq.append(fa[1]); fbp.append(fb[0]); fbq.append(fb[1])
+            for (ang, ax, lo, hi) in lim:
+                lj.append(j); la.append(ang); lx.append(ax); llo.append(lo); lhi.append(hi)
+    nb = len(pos)
+    bd = rp.desc_array(np.array(pos), np.array(rot), np.array(dims), rp.SHAPE_CAPSULE, np.array(dens),
+                       np.ones(nb, dtype=np.uint32), lin=np.array(lin))
+    jd = rp.joint_array(np.array(kinds), np.array(axes), np.array(ja), np.array(jb), np.array(fap), np.array(faq),
+                        np.array(fbp), np.array(fbq))
+    ld = rp.limit_array(np.array(lj), np.array(la), np.array(lx), np.array(llo), np.array(lhi))
+    return bd, jd, ld
+
+
+def ragdolls(rp, w, n_ragdolls=100, hf_n=128, seed=5, iterations=(24, 24), flat_area=None):
+    """Builds the ragdoll scene into World ``w``; returns (dt, body count, joint count). With
+    flat_area, the ragdolls fall in a square of that side onto a static ground box instead."""
+    w.set_pair_props(0, 0, 0.6, 0.5, 0.0, 0.08)
+    w.set_pair_props(0, 4, 0.883176, 0.724569, 0.0, 0.1)
+    w.set_iterations(*iterations)
+    if flat_area is None:
+        h, origin = heightfield(hf_n, 1.0, seed)
+        w.set_heightfield(h, hf_n, hf_n, 1.0, 1.0, origin, origin, material=4)
+        y0, area = float(h.max()) + 1.0, 0.8 * (hf_n - 1)
+    else:
+        g = rp.desc_array(np.array([[0.0, -0.5, 0.0]]), np.array([[0.0, 0.0, 0.0, 1.0]]), np.array([[50.0, 0.5, 50.0]]),
+                          rp.SHAPE_BOX, np.array([0.0]), np.array([0], dtype=np.uint32))
+        w.add_bodies_array(g)
+        y0, area = 0.5, flat_area
+    first = w.num_bodies() + 1
+    bd, jd, ld = ragdoll_arrays(rp, n_ragdolls, seed, area, base_id=first, y0=y0)
+    w.add_bodies_array(bd)
+    j0 = w.add_joint_array(jd)
+    if j0:
+        ld[:, 0].view(np.uint32)[:] += j0
+    w.set_joint_limit_array(ld)
+    return 1.0 / 120.0, w.num_bodies(), len(jd)

@@ -1,0 +1,156 @@
+"""Joints on the GPU: the reference's joint acceptance cases, and tick-by-tick bit parity with the CPU
+oracle on jointed scenes (pendulum chains, ragdolls on a heightfield, sleeping ragdolls hit by
+falling boxes, the per-island residual stop, batched worlds, rollback, the allocation-free hash)."""
+import numpy as np
+import pytest
+
+import joint_cases as J
+from conftest import rp, scenes
+from test_gpu_parity import run_pair
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", [n for n in dir(J) if n.startswith("case_")])
+def test_case(gpu, name):
+    getattr(J, name)(gpu)
+
+
+def _chain(rp_, w, n=6, hz=62.5):
+    """A pinned chain of rods: ball joints and limited hinges alternating, released horizontal."""
+    w.set_gravity((0.0, -9.81, 0.0))
+    pos = [(0.0, 12.0, 0.0)] + [(0.5 + 1.0 * k, 12.0, 0.0) for k in range(n)]
+    he = [(0.01, 0.01, 0.01)] + [(0.5, 0.04, 0.04)] * n
+    d = rp_.desc_array(np.array(pos), np.tile([0.0, 0.0, 0.0, 1.0], (n + 1, 1)), np.array(he), rp_.SHAPE_BOX,
+                       np.array([1.0] + [800.0] * n), np.array([0] + [1] * n, dtype=np.uint32))
+    first = w.add_bodies_array(d)
+    joints = []
+    for k in range(n):
+        fa = ((0.0, 0.0, 0.0), (0, 0, 0, 1)) if k == 0 else ((0.5, 0.0, 0.0), (0, 0, 0, 1))
+        joints.append((rp_.JOINT_BALL if k % 2 == 0 else rp_.JOINT_HINGE, first + k, first + k + 1, fa,
+                       ((-0.5, 0.0, 0.0), (0, 0, 0, 1)), 2))
+    j0 = w.add_joints(joints)
+    for k in range(n):
+        if k % 2:
+            w.set_joint_limit(j0 + k, True, 2, -1.2, 0.3)
+        else:
+            w.set_joint_limit(j0 + k, True, 1, -0.6, 0.6)
+    return 1.0 / hz, n + 1
+
+
+def _ragdolls(n, **kw):
+    def build(rp_, w):
+        dt, nb, _ = scenes.ragdolls(rp_, w, n_ragdolls=n, **kw)
+        return dt, nb
+    return build
+
+
+def test_pendulum_chain(oracle, gpu):
+    build = {"cap": (16, 16), "fn": lambda rp_, w: _chain(rp_, w)}
+    run_pair(oracle, gpu, build, 400)
+
+
+def test_ragdolls_on_terrain(oracle, gpu):
+    build = {"cap": (1024, 1024), "fn": _ragdolls(10)}
+    run_pair(oracle, gpu, build, 240, check_every=4)
+
+
+def test_ragdolls_residual_mode(oracle, gpu):
+    def build(rp_, w):
+        out = _ragdolls(8)(rp_, w)
+        w.set_residual_mode(1e-4, 96)
+        return out
+    run_pair(oracle, gpu, {"cap": (1024, 1024), "fn": build}, 200, check_every=4)
+
+
+def test_sleeping_ragdolls_hit_by_boxes(oracle, gpu):
+    """Ragdolls piled in a small area settle and fall asleep limb by limb; boxes dropped on them later
+    meet sleeping limbs whose joints still tie them to awake ones."""
+    def build(rp_, w):
+        dt, nb, _ = scenes.ragdolls(rp_, w, n_ragdolls=12, flat_area=8.0)
+        return dt, nb
+    wo, wg = oracle.world(2048, 2048), gpu.world(2048, 2048)
+    dt, _ = build(rp, wo)
+    build(rp, wg)
+    asleep = 0
+    for t in range(480):
+        wo.step(dt); wg.step(dt)
+        if t % 20 == 19:
+            assert wo.hash() == wg.hash(), f"tick {t}: hash differs"
+        asleep = max(asleep, wo.stats()["sleeping"])
+    assert asleep > 0, "nothing fell asleep: the case does not exercise sleeping jointed bodies"
+    rng = np.random.default_rng(4)
+    n = 24
+    pos = np.column_stack([rng.uniform(-3, 3, n), rng.uniform(3, 6, n), rng.uniform(-3, 3, n)])
+    d = rp.desc_array(pos, np.tile([0.0, 0.0, 0.0, 1.0], (n, 1)), np.full((n, 3), 0.3), rp.SHAPE_BOX,
+                      np.full(n, 2000.0), np.ones(n, dtype=np.uint32))
+    wo.add_bodies_array(d); wg.add_bodies_array(d)
+    for t in range(300):
+        wo.step(dt); wg.step(dt)
+        so, sg = wo.body_states(), wg.body_states()
+        assert np.array_equal(so.view(np.uint32), sg.view(np.uint32)), f"tick {t}: body bits differ"
+        assert wo.hash() == wg.hash(), f"tick {t}: hash differs"
+        for k in ("contacts", "islands", "levels", "max_batch", "sleeping", "rows_scheduled", "row_sweeps"):
+            assert wo.stats()[k] == wg.stats()[k], f"tick {t}: stat {k}"
+
+
+def test_batched_ragdoll_worlds(oracle, gpu):
+    """Worlds of ragdolls in one batched device world: each world's hash equals the oracle running
+    that world alone."""
+    k_worlds, per = 6, 3
+    h, origin = scenes.heightfield(64, 1.0, 5)
+    wg = gpu.world(4096, 4096)
+    wg.set_heightfield(h, 64, 64, 1.0, 1.0, origin, origin, material=4)
+    singles = []
+    for k in range(k_worlds):
+        first = wg.num_bodies() + 1
+        bd, jd, ld = scenes.ragdoll_arrays(rp, per, 100 + k, 40.0, base_id=first, y0=float(h.max()) + 1.0)
+        wg.add_world(bd)
+        j0 = wg.add_joint_array(jd)
+        ld[:, 0].view(np.uint32)[:] += j0
+        wg.set_joint_limit_array(ld)
+        bo, jo, lo = scenes.ragdoll_arrays(rp, per, 100 + k, 40.0, base_id=1, y0=float(h.max()) + 1.0)
+        wo = oracle.world(len(bo), len(bo))  # a world's hash covers its capacity: the batch's is its body count
+        wo.set_heightfield(h, 64, 64, 1.0, 1.0, origin, origin, material=4)
+        wo.add_bodies_array(bo)
+        wo.add_joint_array(jo)
+        wo.set_joint_limit_array(lo)
+        singles.append(wo)
+    for w in [wg] + singles:
+        w.set_pair_props(0, 0, 0.6, 0.5, 0.0, 0.08)
+        w.set_pair_props(0, 4, 0.883176, 0.724569, 0.0, 0.1)
+        w.set_iterations(24, 24)
+    dt = 1.0 / 120.0
+    for t in range(180):
+        wg.step(dt)
+        for wo in singles:
+            wo.step(dt)
+        if t % 30 == 29:
+            hs = wg.world_hashes()
+            for k, wo in enumerate(singles):
+                assert hs[k] == wo.hash(), f"tick {t}: world {k} hash differs"
+
+
+def test_ragdoll_rollback_replays_exactly(gpu):
+    w = gpu.world(1024, 1024)
+    dt, _, _ = scenes.ragdolls(rp, w, n_ragdolls=8)
+    for _ in range(60):
+        w.step(dt)
+    snap = w.snapshot()
+    for _ in range(30):
+        w.step(dt)
+    h1, s1 = w.hash(), w.body_states()
+    w.restore_exact(snap)
+    for _ in range(30):
+        w.step(dt)
+    assert w.hash() == h1
+    assert np.array_equal(w.body_states().view(np.uint32), s1.view(np.uint32))
+    w.free_snapshot(snap)
+
+
+def test_noalloc_hash_with_joints(gpu):
+    w = gpu.world(1024, 1024)
+    dt, _, _ = scenes.ragdolls(rp, w, n_ragdolls=6)
+    for _ in range(40):
+        w.step(dt)
+    assert w.hash_noalloc() == w.hash()
