@@ -10,6 +10,7 @@
 // Rows split into islands (connected through awake dynamic bodies); one warp owns an island and
 // walks its levels with __syncwarp between them, so no two warps ever touch the same body.
 #include <atomic>
+#include <type_traits>
 #include <cub/cub.cuh>
 
 #include "step_internal.cuh"
@@ -787,32 +788,48 @@ __device__ __forceinline__ void project_one(const BodiesV& B, const RowsV& R, ui
 // step's start poses spos / srot) rides on its first velocity row, which the schedule places before
 // every later row touching its bodies -- the reference's joints-then-contacts order; joints between
 // two frozen (static or sleeping) bodies are skipped. The shock projection has no joints.
-__global__ void k_pos_iterations(uint32_t nisl, uint32_t nc, Sched S, RowsV R, BodiesV B, int iters, int shock, f3 up,
-                                 const float4* __restrict__ c_pt, const float4* __restrict__ c_n,
-                                 const float4* __restrict__ lbv, float4* split_l, float4* split_a,
-                                 const JointGpu* __restrict__ J, float* jlam, const float4* __restrict__ spos,
-                                 const float4* __restrict__ srot, float dt) {
-  uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (warp >= nisl) return;
-  uint32_t off = S.lvl_off[warp], nl = S.nlev[warp];
+// G lanes per group (32 / G groups per warp): narrow groups (a few rows per level, as jointed
+// islands are) leave most of a warp idle with one group each. The warp walks the largest level count
+// of its groups, lanes of a group that has finished idle; groups never share a body.
+// skip: groups of these classes are left to another launch.
+template <int G>
+__global__ void __launch_bounds__(128) k_pos_iterations(uint32_t n_listed, const uint32_t* __restrict__ glist,
+                                                        uint32_t skip, const uint32_t* __restrict__ g_class,
+                                                        uint32_t nc, Sched S, RowsV R, BodiesV B, int iters, int shock,
+                                                        f3 up, const float4* __restrict__ c_pt,
+                                                        const float4* __restrict__ c_n, const float4* __restrict__ lbv,
+                                                        float4* split_l, float4* split_a,
+                                                        const JointGpu* __restrict__ J, float* jlam,
+                                                        const float4* __restrict__ spos, const float4* __restrict__ srot,
+                                                        float dt) {
+  const uint32_t lane = threadIdx.x & 31, sl = lane % (uint32_t)G;
+  const uint32_t slot = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32u / G) + lane / (uint32_t)G;
+  bool has = slot < n_listed;
+  const uint32_t g = has ? (glist ? glist[slot] : slot) : 0u;
+  if (has && skip && ((skip >> g_class[g]) & 1u)) has = false;
+  const uint32_t off = has ? S.lvl_off[g] : 0u, nl = has ? S.nlev[g] : 0u;
+  uint32_t nlw = nl;
+  for (int o = 16; o > 0; o >>= 1) nlw = max(nlw, __shfl_xor_sync(0xffffffffu, nlw, o));
   const bool joints_on = !shock && fin(dt) && dt > 0.0f;
   for (int it = 0; it < iters; ++it) {
-    for (uint32_t L = 0; L < nl; ++L) {
-      uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
-      for (uint32_t s = s0 + lane; s < s1; s += 32) {
-        uint32_t k = S.ord[s];
-        if (k >= nc) {
-          if (joints_on && (R.flags[k] & RF_JFIRST)) {
-            uint32_t j = __float_as_uint(R.la[k].x);
-            const JointGpu jt = J[j];
-            bool fa = !B.dyn[jt.a] || !B.awake[jt.a], fb = !B.dyn[jt.b] || !B.awake[jt.b];
-            if (!(fa && fb))
-              solve_d6_dev(jt, jlam + 6 * (size_t)j, B, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]), asq(srot[jt.b]));
+    for (uint32_t L = 0; L < nlw; ++L) {
+      if (L < nl) {
+        uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
+        for (uint32_t s = s0 + sl; s < s1; s += G) {
+          uint32_t k = S.ord[s];
+          if (k >= nc) {
+            if (joints_on && (R.flags[k] & RF_JFIRST)) {
+              uint32_t j = __float_as_uint(R.la[k].x);
+              const JointGpu jt = J[j];
+              bool fa = !B.dyn[jt.a] || !B.awake[jt.a], fb = !B.dyn[jt.b] || !B.awake[jt.b];
+              if (!(fa && fb))
+                solve_d6_dev(jt, jlam + 6 * (size_t)j, B, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]),
+                             asq(srot[jt.b]));
+            }
+            continue;
           }
-          continue;
+          project_one(B, R, k, shock != 0, up, c_pt, c_n, lbv, split_l, split_a);
         }
-        project_one(B, R, k, shock != 0, up, c_pt, c_n, lbv, split_l, split_a);
       }
       __syncwarp();
     }
@@ -1845,6 +1862,14 @@ __global__ void k_warm_merge_kept(uint32_t n, const uint4* __restrict__ kk, cons
   ok[p] = kk[j]; oa[p] = ka[j]; ob[p] = kb[j];
 }
 
+// Rows of the position-pass schedule: contacts, and each joint's first row.
+__global__ void k_pos_keep(uint32_t n, uint32_t nc, const uint32_t* __restrict__ rows, const uint32_t* __restrict__ flags,
+                           uint8_t* keep) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t r = rows[i];
+  keep[i] = (r < nc || (flags[r] & RF_JFIRST)) ? 1 : 0;
+}
 // Position i of the scheduled-row scan: joint rows (index nc .. nc + njr) first, then the contacts;
 // the row there and whether it is scheduled (a root was found for it).
 __global__ void k_joint_first_order(uint32_t n, uint32_t nc, uint32_t njr, const uint32_t* __restrict__ root,
@@ -1891,7 +1916,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   // joints: their rows follow the contact rows in the row arrays (index nc + r)
   const uint32_t nj = W.num_joints();
   const uint8_t* jointed = nj ? W.jointed_d.p : nullptr;
-  uint32_t njr = 0;
+  uint32_t njr = 0, npp = 0;  // joint rows; rows of the position-pass schedule (0: the main one)
+  uint32_t cls_n[32] = {};    // solve groups per class (class 3: g_small, not listed)
   S.constrained.ensure(nb + 1); S.loaded.ensure(nb + 1); S.ballistic.ensure(nb + 1); S.touching.ensure(nb + 1);
   S.uf.ensure(nb + 1); S.uf2.ensure(nb + 1); S.body_level.ensure(nb + 1); S.root_mark.ensure(nb + 1);
   S.Iw.ensure(9 * (size_t)nb + 9);
@@ -1975,7 +2001,6 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     }
     ctx.nsched = nsched;
     uint32_t nisl = 0, ng = 0, g_small = 0;
-    uint32_t cls_n[32] = {};  // groups per class (class 3: g_small, not listed)
     S.isl_start.ensure(nsched + 1); S.isl_cnt.ensure(nsched + 1);
     S.ord_main.ensure(nsched + 1); S.ord_vs.ensure(nsched + 1); S.ord_ps.ensure(nsched + 1);
     if (nsched > 0) {
@@ -2026,6 +2051,23 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       S.gb_list.ensure(nb + 1); S.gb_start.ensure(ng + 1); S.gb_cnt.ensure(ng + 1); S.body_local.ensure(nb + 1);
       RP_CUDA(cudaMemsetAsync(S.body_grp.p, 0xFF, sizeof(uint32_t) * (nb + 1), st));
       k_body_groups<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.r_ab.p, S.r_flags.p, S.body_grp.p); RP_COUNT_LAUNCH(1);
+      // ---- the position pass's own schedule when there are joints: the contacts and one unit per
+      // joint (its first row carries the joint's whole solve), in the same order -- without the
+      // joints' other velocity rows, which would only add levels
+      npp = 0;
+      if (njr) {
+        S.pp_rows.ensure(nsched + 1); S.pp_key.ensure(nsched + 1); S.pp_gs.ensure(ng + 1); S.pp_gc.ensure(ng + 1);
+        S.ord_pp.ensure(nsched + 1);  // build_schedule's order output (it sizes the level arrays itself)
+        S.flag8.ensure(nsched + 1);
+        k_pos_keep<<<nblk(nsched), T, 0, st>>>(nsched, nc, S.tmp32.p, S.r_flags.p, S.flag8.p); RP_COUNT_LAUNCH(1);
+        npp = select_flagged_u32(S, S.tmp32.p, S.flag8.p, S.pp_rows.p, nsched, st);
+        select_flagged_u32(S, S.g_key2.p, S.flag8.p, S.pp_key.p, nsched, st);
+        RP_CUDA(cudaMemsetAsync(S.pp_gs.p, 0, sizeof(uint32_t) * (ng + 1), st));
+        RP_CUDA(cudaMemsetAsync(S.pp_gc.p, 0, sizeof(uint32_t) * (ng + 1), st));
+        k_group_ranges<<<nblk(npp), T, 0, st>>>(npp, S.pp_key.p, S.pp_gs.p, S.pp_gc.p); RP_COUNT_LAUNCH(1);
+        build_schedule(S, stats + STAT_ERR, npp, ng, S.pp_rows.p, S.pp_gs.p, S.pp_gc.p, S.ord_pp.p, S.lvl_off_pp,
+                       S.lvl_start_pp, S.nlev_pp, nullptr, nullptr, st);
+      }
       k_flag_grouped<<<nblk(nb), T, 0, st>>>(nb, S.body_grp.p, S.gb_key.p); RP_COUNT_LAUNCH(1);
       select_flagged_iota(S, nb, S.gb_key.p, S.gb_tmp.p, S.counts.p + 0, st);
       uint32_t ngb = 0;
@@ -2272,9 +2314,24 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     S.pc_lb.ensure(nc + 1);
     k_pos_anchors<<<nblk(nc), T, 0, st>>>(nc, R, S.c_pt.p, S.orig_pos.p, S.orig_rot.p, S.pc_lb.p); RP_COUNT_LAUNCH(1);
     if (nj) RP_CUDA(cudaMemsetAsync(W.jlam.p, 0, sizeof(float) * 6 * (size_t)nj, st));  // Joints::begin_step
-    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, nc, SM, R, B, (int)W.iters_p_, 0, ctx.up, S.c_pt.p,
-                                                               S.c_n.p, S.pc_lb.p, S.split_l.p, S.split_a.p, W.joints_d.p,
-                                                               W.jlam.p, S.orig_pos.p, S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
+    Sched SPP = npp ? Sched{S.ord_pp.p, S.lvl_off_pp.p, S.lvl_start_pp.p, S.nlev_pp.p} : SM;
+    const uint32_t ngr = ctx.nisl;
+    auto pos_launch = [&](auto tag, uint32_t n, const uint32_t* list, uint32_t skip) {
+      constexpr int G = decltype(tag)::value;
+      if (!n) return;
+      uint32_t warps = (n + (32u / G) - 1) / (32u / G);
+      k_pos_iterations<G><<<nblk(warps * 32, 128), 128, 0, st>>>(
+          n, list, skip, S.g_class.p, nc, SPP, R, B, (int)W.iters_p_, 0, ctx.up, S.c_pt.p, S.c_n.p, S.pc_lb.p, S.split_l.p,
+          S.split_a.p, W.joints_d.p, W.jlam.p, S.orig_pos.p, S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
+    };
+    if (npp) {
+      // jointed islands of up to 128 / 256 rows (a ragdoll or two): 4 / 8 lanes each
+      pos_launch(std::integral_constant<int, 4>{}, cls_n[10], S.cls_list.p + 10 * (size_t)ngr, 0u);
+      pos_launch(std::integral_constant<int, 8>{}, cls_n[11], S.cls_list.p + 11 * (size_t)ngr, 0u);
+      pos_launch(std::integral_constant<int, 32>{}, ngr, nullptr, (1u << 10) | (1u << 11));
+    } else {
+      pos_launch(std::integral_constant<int, 32>{}, ngr, nullptr, 0u);
+    }
     P.end(PH_POS_ITER, st);
     P.begin(PH_POS_SHOCK, st);
     // shock projection in (height key, index) order at the poses the iterations left
@@ -2286,9 +2343,10 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     build_schedule(S, stats + STAT_ERR, nsched, ctx.nisl, S.rows_sched2.p, S.g_start.p, S.g_cnt.p, S.ord_ps.p, S.lvl_off_ps,
                    S.lvl_start_ps, S.nlev_ps, nullptr, nullptr, st);
     Sched SP{S.ord_ps.p, S.lvl_off_ps.p, S.lvl_start_ps.p, S.nlev_ps.p};
-    k_pos_iterations<<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, nc, SP, R, B, 1, 1, ctx.up, S.c_pt.p, S.c_n.p,
-                                                               S.pc_lb.p, S.split_l.p, S.split_a.p, W.joints_d.p,
-                                                               W.jlam.p, S.orig_pos.p, S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
+    k_pos_iterations<32><<<nblk(ctx.nisl * 32, 128), 128, 0, st>>>(ctx.nisl, nullptr, 0u, S.g_class.p, nc, SP, R, B, 1, 1,
+                                                                   ctx.up, S.c_pt.p, S.c_n.p, S.pc_lb.p, S.split_l.p,
+                                                                   S.split_a.p, W.joints_d.p, W.jlam.p, S.orig_pos.p,
+                                                                   S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
     P.end(PH_POS_SHOCK, st);
   }
   // ---- stages 6 and 7
