@@ -236,10 +236,10 @@ RPhysResult rphys_ext_num_joints(const RPhysWorld* world, uint32_t* out_count);
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:
  * cudaMalloc and cudaFree can wait for all work on the device and their memory use varies with the
- * world, while this call's scratch is one fixed array (about 15.5 MB per device) reserved when the
+ * world, while this call's scratch is one fixed array (about 16.5 MB per device) reserved when the
  * library is loaded. The digest is identical to rphys_world_get_step_hash's. Limits: a state
  * stream of at most 12 MiB (56 + 12 bytes per body, 3 bytes per body of capacity, up to 48 bytes
- * per warm-start entry) and at most 262144 warm-start entries; a larger world returns
+ * per warm-start entry), at most 262144 warm-start entries and 65536 joints; a larger world returns
  * RPHYS_ERR_CAPACITY with the sizes in rphys_last_error_message and runs nothing on the device.
  * The first call on each device looks up the array's address there (device setup): make it once
  * before the real-time loop. The array is shared by every world on a device, so calls are
