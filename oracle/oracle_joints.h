@@ -16,6 +16,7 @@ struct JRow {
   V3 u, ra, rb;
   float wa, wb, m_eff, target, lam_min, lam_max;
   uint8_t tag;
+  uint8_t idx = 0, cnt = 0;  // index in its joint's rows; the joint's row count (on its first row)
 };
 
 // d6_hinge_axis (bodies.rs:891-901) at the restated feature set: -1 for none.

@@ -1064,14 +1064,18 @@ void World::step(float dt) {
       uint32_t s = (uint32_t)jrows.size();
       d6_rows(*this, joints[jk], jk, dt, jrows);
       jrange[jk] = {s, (uint32_t)jrows.size()};
+      for (uint32_t k = s; k < (uint32_t)jrows.size(); ++k) jrows[k].idx = (uint8_t)(k - s);
+      if (jrows.size() > s) jrows[s].cnt = (uint8_t)(jrows.size() - s);
     }
     const uint32_t njr = (uint32_t)jrows.size();
     std::vector<float> jacc(njr, 0.0f);
     // 2a. one level schedule (:621-642, 666-683) over the joint rows, then the contact rows: entry
     // e < njr is joint row e, entry njr + k contact k. Every sweep then runs an island's joint rows
     // before its contacts, as the reference's joint batches run before its contact batches. A
-    // contact's side on a sleeping jointed body is read-only for the contact but moved by that
-    // body's joint rows, so the schedule and the solve islands count it as touched.
+    // joint's rows form one unit (its level, run in order by its first row), as a joint is one task
+    // of the reference's joint batches. A contact's side on a sleeping jointed body is read-only for
+    // the contact but moved by that body's joint rows, so the schedule and the solve islands count
+    // it as touched.
     auto ent = [&](uint32_t e, uint32_t* a, uint32_t* b, bool* ta, bool* tb) {
       if (e < njr) {
         const JRow& r = jrows[e];
@@ -1092,6 +1096,12 @@ void World::step(float dt) {
       for (uint32_t e = 0; e < nent; ++e) {
         uint32_t a, b; bool ta, tb;
         if (!ent(e, &a, &b, &ta, &tb)) continue;
+        if (e < njr && jrows[e].idx) {  // a joint's later row: with its first
+          uint32_t t = ent_level[e - jrows[e].idx];
+          batches[t].push_back(e);
+          ent_level[e] = t;
+          continue;
+        }
         uint32_t la = ta ? bl[a] : 0, lb = tb ? bl[b] : 0;
         uint32_t t = la > lb ? la : lb;
         if (t >= batches.size()) batches.emplace_back();
@@ -1260,9 +1270,13 @@ void World::step(float dt) {
     };
     // one entry: a joint row (solver.rs:821-830; residual |delta lambda| / m_eff) or a contact
     auto solve_ent = [&](uint32_t e, float* resid) {
-      if (e < njr) {
-        float d = joint_row_update(*this, jrows[e], jacc[e]);
-        *resid = rmax(*resid, std::fabs(d) / jrows[e].m_eff);
+      if (e < njr) {  // the first row of a joint runs the joint's rows in order
+        for (uint32_t q = 0; q < jrows[e].cnt; ++q) {
+          float d = joint_row_update(*this, jrows[e + q], jacc[e + q]);
+          float r = std::fabs(d) / jrows[e + q].m_eff;
+          if (q == 0) *resid = rmax(*resid, r);
+          else row_res[e + q] = r;
+        }
       } else {
         row(e - njr, resid);
       }
@@ -1277,14 +1291,14 @@ void World::step(float dt) {
 #pragma omp parallel for num_threads(threads)
           for (long q = 0; q < (long)b.size(); ++q) {
             uint32_t e = b[q];
-            if (isl_done[row_isl[e]]) continue;
+            if (isl_done[row_isl[e]] || (e < njr && jrows[e].idx)) continue;
             row_res[e] = 0.0f;
             solve_ent(e, &row_res[e]);
           }
         } else
 #endif
           for (uint32_t e : b) {
-            if (isl_done[row_isl[e]]) continue;
+            if (isl_done[row_isl[e]] || (e < njr && jrows[e].idx)) continue;
             row_res[e] = 0.0f;
             solve_ent(e, &row_res[e]);
           }

@@ -41,8 +41,9 @@ __global__ void k_joint_count(uint32_t nj, const JointGpu* __restrict__ J, Bodie
 }
 // Rows of joint j at R[base + off[j] + k]. Warm start (solver.rs:703-712): the previous rows'
 // impulses when the joint has an entry with the same row count and tags, each clamped to its
-// row's bounds. A joint row stores: ra.w = 1 / k, t1.w = target, t2.x = warm impulse, mu = (lam_min,
-// lam_max, 0, tag), la.x = the joint's index (bits).
+// row's bounds. A joint row stores: ra.w = 1 / k, t1 = (row count on the first row, index in the
+// joint, 0, target), t2.x = warm impulse, mu = (lam_min, lam_max, 0, tag), la.x = the joint's index
+// (bits).
 __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, BodiesV B, float dt,
                               const uint32_t* __restrict__ off, uint32_t base, RowsV R,
                               const uint32_t* __restrict__ jw_n, const uint8_t* __restrict__ jw_tag,
@@ -67,7 +68,8 @@ __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, Bodie
     R.ra[i] = f4(r.ra, r.m_eff);
     R.rb[i] = f4(r.rb, 0.0f);
     R.n[i] = f4(r.u, 0.0f);
-    R.t1[i] = make_float4(0.0f, 0.0f, 0.0f, r.target);
+    // t1.x: the joint's row count on its first row (the unit's length), t1.y: the row's index in it
+    R.t1[i] = make_float4(k == 0 ? (float)n : 0.0f, (float)k, 0.0f, r.target);
     R.t2[i] = make_float4(lam, 0.0f, 0.0f, 0.0f);
     R.mu[i] = make_float4(r.lo, r.hi, 0.0f, __uint_as_float(r.tag));
     R.la[i] = make_float4(__uint_as_float(j), 0.0f, 0.0f, 0.0f);

@@ -344,17 +344,23 @@ __global__ void k_warm_unscheduled(uint32_t nc, RowsV R, BodiesV B, const int* _
 // predecessor DAG, reached by monotone relaxation from 0 (after k passes every row whose longest
 // predecessor chain has length <= k is exact; an acyclic graph converges in depth + 1 passes).
 // Each row is one position s in ord_in; positions of one island are contiguous.
+// Joint units (t1 non-null): a joint's rows after its first are scheduled with it -- same level,
+// right after it (one thread runs them in order) -- so they take no body entries and lead[s] is the
+// distance back to the joint's first row (0 for every other row).
 __global__ void k_level_entries(uint32_t n, const uint32_t* __restrict__ ord_in, const uint2* __restrict__ ab,
-                                const uint32_t* __restrict__ flags, uint32_t* key, uint32_t* val) {
+                                const uint32_t* __restrict__ flags, const float4* __restrict__ t1, uint32_t* key,
+                                uint32_t* val, uint32_t* lead) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   uint32_t r = ord_in[s];
   uint2 x = ab[r];
   uint32_t f = flags[r];
-  key[2 * s] = (f & RF_TA) ? x.x : 0xFFFFFFFFu;
-  key[2 * s + 1] = (f & RF_TB) ? x.y : 0xFFFFFFFFu;
+  const bool tail = t1 && (f & RF_JOINT) && !(f & RF_JFIRST);
+  key[2 * s] = (!tail && (f & RF_TA)) ? x.x : 0xFFFFFFFFu;
+  key[2 * s + 1] = (!tail && (f & RF_TB)) ? x.y : 0xFFFFFFFFu;
   val[2 * s] = 2 * s;
   val[2 * s + 1] = 2 * s + 1;
+  if (lead) lead[s] = tail ? (uint32_t)t1[r].y : 0u;
 }
 // entries sorted by body (stable): the previous entry of the same body is the predecessor
 __global__ void k_level_preds(uint32_t m, const uint32_t* __restrict__ key, const uint32_t* __restrict__ val,
@@ -368,8 +374,9 @@ __global__ void k_level_preds(uint32_t m, const uint32_t* __restrict__ key, cons
 // One warp per island: lanes own contiguous chunks of the island's positions and sweep them in
 // order (so chains inside a chunk settle in one pass) until a pass changes nothing.
 __global__ void k_level_relax(uint32_t nisl, const uint32_t* __restrict__ isl_start, const uint32_t* __restrict__ isl_cnt,
-                              const uint32_t* __restrict__ ord_in, const uint32_t* __restrict__ pred, uint32_t* level,
-                              unsigned long long* key_out, uint32_t* nlev, uint32_t* row_level, uint32_t* err) {
+                              const uint32_t* __restrict__ ord_in, const uint32_t* __restrict__ pred,
+                              const uint32_t* __restrict__ lead, uint32_t* level, unsigned long long* key_out,
+                              uint32_t* nlev, uint32_t* row_level, uint32_t* err) {
   uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   uint32_t lane = threadIdx.x & 31;
   if (warp >= nisl) return;
@@ -386,6 +393,7 @@ __global__ void k_level_relax(uint32_t nisl, const uint32_t* __restrict__ isl_st
     for (uint32_t s = a; s < z; ++s) {
       uint32_t p0 = pred[2 * s], p1 = pred[2 * s + 1];
       uint32_t L = 0;
+      if (lead && lead[s]) L = vl[s - lead[s]];  // a joint's later row: its first row's level
       if (p0 != 0xFFFFFFFFu) { uint32_t v = vl[p0] + 1; if (v > L) L = v; }
       if (p1 != 0xFFFFFFFFu) { uint32_t v = vl[p1] + 1; if (v > L) L = v; }
       if (L != vl[s]) { vl[s] = L; changed = true; }
@@ -441,10 +449,14 @@ __global__ void k_joint_warm(uint32_t ng, uint32_t nc, Sched S, RowsV R, BodiesV
     uint32_t s0 = S.lvl_start[off + L], s1 = S.lvl_start[off + L + 1];
     for (uint32_t s = s0 + lane; s < s1; s += 32) {
       uint32_t k = S.ord[s];
-      if (k < nc || !(R.flags[k] & RF_JWARM)) continue;
-      Row r = ld_row(R, k);
-      acc_jn[k] = r.t2.x;
-      if (r.t2.x != 0.0f) joint_apply_glob(B, r, r.t2.x);
+      if (k < nc || (R.flags[k] & (RF_JWARM | RF_JFIRST)) != (RF_JWARM | RF_JFIRST)) continue;
+      const uint32_t cnt = (uint32_t)R.t1[k].x;  // the unit's rows follow its first, in order
+      for (uint32_t q = 0; q < cnt; ++q) {
+        uint32_t kq = S.ord[s + q];
+        Row r = ld_row(R, kq);
+        acc_jn[kq] = r.t2.x;
+        if (r.t2.x != 0.0f) joint_apply_glob(B, r, r.t2.x);
+      }
     }
     __syncwarp();
   }
@@ -486,7 +498,16 @@ __global__ void k_vel_solve(uint32_t nisl, uint32_t nc, Sched S, RowsV R, Bodies
       for (uint32_t s = s0 + lane; s < s1; s += 32) {
         uint32_t k = S.ord[s];
         Row r = ld_row(R, k);
-        resid = rmax(resid, k >= nc ? joint_row_glob(B, r, k, acc_jn) : pgs_row(B, r, k, acc_jn, acc_jt));
+        if (k >= nc) {  // a joint unit: its first row runs all its rows in order
+          if (!(r.flags & RF_JFIRST)) continue;
+          const uint32_t cnt = (uint32_t)r.t1.x;
+          for (uint32_t q = 0; q < cnt; ++q) {
+            uint32_t kq = S.ord[s + q];
+            resid = rmax(resid, joint_row_glob(B, q ? ld_row(R, kq) : r, kq, acc_jn));
+          }
+          continue;
+        }
+        resid = rmax(resid, pgs_row(B, r, k, acc_jn, acc_jt));
       }
       __syncwarp();
     }
@@ -1480,6 +1501,12 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
       for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1]; i += NT) {
         const SRow& r = W.rows[i];
         if (MULTI && W.isl_done[r.flags >> 16]) continue;
+        if (r.flags & RF_JOINT) {  // a joint is one unit: its first row runs all its rows in order
+          if (!(r.flags & RF_JFIRST)) continue;
+          const uint32_t cnt = (uint32_t)r.t1.x;
+          for (uint32_t q = 0; q < cnt; ++q) pgs_row_reg(B, W.rows[i + q], i + q, W.jn, W.jt, W.dres);
+          continue;
+        }
         pgs_row_reg(B, r, i, W.jn, W.jt, W.dres);
       }
       __syncthreads();
@@ -1638,6 +1665,20 @@ __device__ __forceinline__ SRow big_row(const BigStage<CH>& st, uint32_t i, m3* 
   *imb = q[21];
   return r;
 }
+// A row of the big-island stream read straight from global memory (a joint unit's later rows, which
+// may lie past the staged chunk).
+__device__ __forceinline__ SRow big_row_global(const SRowsV& R, const float4* __restrict__ X, uint32_t s, m3* qa, m3* qb,
+                                               float* ima, float* imb) {
+  SRow r = ld_srow(R, s);
+  const float4* x = X + 7 * (size_t)s;
+  float q[24];
+  for (int k = 0; k < 6; ++k) { float4 v = x[k]; q[4 * k] = v.x; q[4 * k + 1] = v.y; q[4 * k + 2] = v.z; q[4 * k + 3] = v.w; }
+  *qa = mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
+  *ima = q[9];
+  *qb = mcols(mk3(q[12], q[13], q[14]), mk3(q[15], q[16], q[17]), mk3(q[18], q[19], q[20]));
+  *imb = q[21];
+  return r;
+}
 template <int CH>
 __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, uint32_t want_class,
                                                       uint32_t n_listed, const uint32_t* __restrict__ glist,
@@ -1716,15 +1757,22 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
       BigStage<CH>& st = stg[buf];
       m3 qa, qb; float ima, imb;
       SRow r = big_row(st, tid, &qa, &qb, &ima, &imb);
-      float4 jj = st.j[tid];
-      float jn = jj.x; float2 jt = make_float2(jj.y, jj.z);
-      float d3[3];
-      pgs_row_core(lin, ang, r, qa, qb, ima, imb, jn, jt, d3);
-      J[c0 + tid] = make_float4(jn, jt.x, jt.y, 0.0f);
+      // a joint is one unit: its first row runs all its rows in order (the later ones from global)
+      const bool skip = (r.flags & RF_JOINT) && !(r.flags & RF_JFIRST);
+      const uint32_t cnt = (r.flags & RF_JOINT) ? (uint32_t)r.t1.x : 1u;
       float rr = 0.0f;
-      if (r.m_n > 0.0f) rr = rmax(rr, fabsf(d3[0]) / r.m_n);
-      if (r.m_t1 > 0.0f) rr = rmax(rr, fabsf(d3[1]) / r.m_t1);
-      if (r.m_t2 > 0.0f) rr = rmax(rr, fabsf(d3[2]) / r.m_t2);
+      for (uint32_t q = 0; q < cnt && !skip; ++q) {
+        const uint32_t sq = c0 + tid + q;
+        if (q) r = big_row_global(R, X, sq, &qa, &qb, &ima, &imb);
+        float4 jj = q ? J[sq] : st.j[tid];
+        float jn = jj.x; float2 jt = make_float2(jj.y, jj.z);
+        float d3[3];
+        pgs_row_core(lin, ang, r, qa, qb, ima, imb, jn, jt, d3);
+        J[sq] = make_float4(jn, jt.x, jt.y, 0.0f);
+        if (r.m_n > 0.0f) rr = rmax(rr, fabsf(d3[0]) / r.m_n);
+        if (r.m_t1 > 0.0f) rr = rmax(rr, fabsf(d3[1]) / r.m_t1);
+        if (r.m_t2 > 0.0f) rr = rmax(rr, fabsf(d3[2]) / r.m_t2);
+      }
       atomicMax(&res_bits, fbits(rr));  // non-negative floats: integer max, order-free
     }
     __threadfence_block();
@@ -1881,10 +1929,11 @@ __global__ void k_joint_first_order(uint32_t n, uint32_t nc, uint32_t njr, const
   fl[i] = root[r] != 0xFFFFFFFFu ? 1 : 0;
 }
 // ------------------------------------------------------------------ host driver
+// units: R.t1 of the rows when a joint's rows form one schedule unit (the velocity schedule), else null.
 static void build_schedule(WorldGpu::Scratch& S, uint32_t* W_err, uint32_t nsched, uint32_t nisl, const uint32_t* ord_in,
                            const uint32_t* isl_start, const uint32_t* isl_cnt, uint32_t* ord_out, DBuf<uint32_t>& lvl_off,
                            DBuf<uint32_t>& lvl_start, DBuf<uint32_t>& nlev, uint32_t* hist, uint32_t* row_level,
-                           cudaStream_t st) {
+                           cudaStream_t st, const float4* units = nullptr) {
   nlev.ensure(nisl + 1);
   lvl_off.ensure(nisl + 1);
   S.key64.ensure(nsched + 1); S.key64b.ensure(nsched + 1);
@@ -1892,11 +1941,13 @@ static void build_schedule(WorldGpu::Scratch& S, uint32_t* W_err, uint32_t nsche
   S.lv_key.ensure(2 * (size_t)nsched + 2); S.lv_key2.ensure(2 * (size_t)nsched + 2);
   S.lv_val.ensure(2 * (size_t)nsched + 2); S.lv_val2.ensure(2 * (size_t)nsched + 2);
   S.lv_pred.ensure(2 * (size_t)nsched + 2); S.lv_level.ensure(nsched + 1);
-  k_level_entries<<<nblk(nsched), T, 0, st>>>(nsched, ord_in, S.r_ab.p, S.r_flags.p, S.lv_key.p, S.lv_val.p); RP_COUNT_LAUNCH(1);
+  if (units) S.lv_lead.ensure(nsched + 1);
+  uint32_t* lead = units ? S.lv_lead.p : nullptr;
+  k_level_entries<<<nblk(nsched), T, 0, st>>>(nsched, ord_in, S.r_ab.p, S.r_flags.p, units, S.lv_key.p, S.lv_val.p, lead); RP_COUNT_LAUNCH(1);
   sort_pairs_u32(S, S.lv_key.p, S.lv_key2.p, S.lv_val.p, S.lv_val2.p, 2 * nsched, 0, 32, st);
   RP_CUDA(cudaMemsetAsync(S.lv_pred.p, 0xFF, sizeof(uint32_t) * 2 * (size_t)nsched, st));
   k_level_preds<<<nblk(2 * nsched), T, 0, st>>>(2 * nsched, S.lv_key2.p, S.lv_val2.p, S.lv_pred.p); RP_COUNT_LAUNCH(1);
-  k_level_relax<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, isl_start, isl_cnt, ord_in, S.lv_pred.p, S.lv_level.p,
+  k_level_relax<<<nblk(nisl * 32, 128), 128, 0, st>>>(nisl, isl_start, isl_cnt, ord_in, S.lv_pred.p, lead, S.lv_level.p,
                                                       S.key64.p, nlev.p, row_level, W_err); RP_COUNT_LAUNCH(1);
   sort_pairs_u64(S, S.key64.p, S.key64b.p, ord_in, ord_out, nsched, 0, 64, st);
   S.lv_np1.ensure(nisl + 1);
@@ -2045,7 +2096,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       S.lvl_hist.ensure(nsched + 1);
       RP_CUDA(cudaMemsetAsync(S.lvl_hist.p, 0, sizeof(uint32_t) * (nsched + 1), st));
       build_schedule(S, stats + STAT_ERR, nsched, ng, S.tmp32.p, S.g_start.p, S.g_cnt.p, S.ord_main.p, S.lvl_off, S.lvl_start,
-                     S.nlev, S.lvl_hist.p, S.row_level.p, st);
+                     S.nlev, S.lvl_hist.p, S.row_level.p, st, njr ? S.r_t1.p : nullptr);
       // ---- the bodies each group moves, with their index inside the group
       S.body_grp.ensure(nb + 1); S.gb_tmp.ensure(nb + 1); S.gb_key.ensure(nb + 1); S.gb_key2.ensure(nb + 1);
       S.gb_list.ensure(nb + 1); S.gb_start.ensure(ng + 1); S.gb_cnt.ensure(ng + 1); S.body_local.ensure(nb + 1);
