@@ -554,6 +554,16 @@ RPhysResult rphys_ext_set_joint_limits(RPhysWorld* W, const RPhysJointLimit* l, 
   for (uint32_t i = 0; i < n; ++i) W->w.set_d6_limit(l[i].joint, l[i].angular != 0, l[i].axis, l[i].enabled != 0, l[i].lo, l[i].hi);
   return RPHYS_OK;
 }
+// Test hook: f32 values d in [0.8, 1] where the restated turned test 2 acos(d) < 0.5 and the
+// threshold form d >= dstar disagree (the GPU evaluates the threshold form).
+uint32_t rphys_oracle_turned_threshold_mismatches(uint32_t dstar_bits) {
+  float dstar;
+  std::memcpy(&dstar, &dstar_bits, 4);
+  uint32_t bad = 0;
+  for (float d = 0.8f; d <= 1.0f; d = std::nextafter(d, 2.0f))
+    if ((2.0f * om::acosf_unit_rp(d) < 0.5f) != (d >= dstar)) bad++;
+  return bad;
+}
 RPhysResult rphys_ext_num_joints(const RPhysWorld* W, uint32_t* out) {
   clear_err();
   if (!W || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_num_joints: null arg");

@@ -108,10 +108,15 @@ __device__ __forceinline__ void apply_orientation_delta_dev(const BodiesV& B, ui
   q4 dq = qnormalize(mkq(d.x * 0.5f, d.y * 0.5f, d.z * 0.5f, 1.0f));
   B.rot[id] = f4q(fin_q(qnormalize(qmul(dq, asq(B.rot[id])))));
 }
-// turned (bodies.rs:486-490)
-__device__ __forceinline__ float turned_dev(q4 a, q4 b) {
+// turned(a, b) < SHAKE_MAX_TURN (bodies.rs:486-490, :477): 2 acos(d) < 0.5 with d = min(|w|, 1),
+// w the real part of a b*. acos is decreasing and the project's acos (one rounding of a double
+// evaluation) is monotone in d, so the test is d >= the least f32 that passes it, 0x3f780aa6
+// (0.968912482); tests/test_oracle_joints.py checks the two forms agree on every f32 in [0.8, 1]
+// (below that 2 acos(d) exceeds 1.28).
+#define RP_SHAKE_COS_BITS 0x3f780aa6u
+__device__ __forceinline__ bool turned_below_max(q4 a, q4 b) {
   float d = rmin(fabsf(qmul(a, qconj(b)).w), 1.0f);
-  return 2.0f * acos_unit_rp(d);
+  return d >= __uint_as_float(RP_SHAKE_COS_BITS);
 }
 // solve_d6 for locked and limited axes (compliance 0: alpha = 0; no drives, no rotors). lam: the
 // joint's six XPBD multipliers of this step (t0 t1 t2 r0 r1 r2). sa / sb: the step's start poses.
@@ -119,7 +124,7 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
                                              f3 sb_p, q4 sb_q) {
   const uint32_t A = j.a, Bb = j.b;
   const float wa = fin0(B.inv_mass[A]), wb = fin0(B.inv_mass[Bb]);
-  const bool shake = turned_dev(sa_q, asq(B.rot[A])) < 0.5f && turned_dev(sb_q, asq(B.rot[Bb])) < 0.5f;
+  const bool shake = turned_below_max(sa_q, asq(B.rot[A])) && turned_below_max(sb_q, asq(B.rot[Bb]));
   f3 ax0[3] = {mk3(0, 0, 0), mk3(0, 0, 0), mk3(0, 0, 0)}, la0 = mk3(0, 0, 0), lb0 = mk3(0, 0, 0);
   m3 ia0 = mzero(), ib0 = mzero();
   q4 fa_q = asq(j.fa_q), fb_q = asq(j.fb_q);

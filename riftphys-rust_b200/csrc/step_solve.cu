@@ -1245,6 +1245,43 @@ __device__ __noinline__ void joint_row_core(float4* lin, float4* ang, const SRow
   d3[1] = 0.0f;
   d3[2] = 0.0f;
 }
+// A joint unit on shared-memory bodies: the joint's rows in order, with both bodies' velocities,
+// inverse inertias and inverse masses held in registers across them (every row of a joint moves the
+// same two bodies) -- the same operations in the same order as one joint_row_core per row.
+__device__ __noinline__ void joint_unit_core(float4* lin, float4* ang, const SRow* rows, uint32_t cnt, const float* Iw,
+                                             const float* im, float* jn, float* dres) {
+  const SRow& r0 = rows[0];
+  const bool ha = r0.la != 0xFFFFFFFFu, hb = r0.lb != 0xFFFFFFFFu;
+  const bool ia = r0.inv_a > 0.0f, ib = r0.inv_b > 0.0f;
+  const m3 qa = load_iw(ia ? Iw + 9 * (size_t)r0.la : Iw), qb = load_iw(ib ? Iw + 9 * (size_t)r0.lb : Iw);
+  const float ima = ia ? im[r0.la] : 0.0f, imb = ib ? im[r0.lb] : 0.0f;
+  float4 LA = make_float4(0, 0, 0, 0), AA = LA, LB = LA, AB = LA;
+  if (ha) { LA = lin[r0.la]; AA = ang[r0.la]; }
+  if (hb) { LB = lin[r0.lb]; AB = ang[r0.lb]; }
+  f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
+  bool moved = false;
+  for (uint32_t q = 0; q < cnt; ++q) {
+    const SRow& r = rows[q];
+    f3 va, vb;
+    if (r.flags & RF_JANG) { va = ha ? aa : r.vfix; vb = hb ? ab : r.vfix; }
+    else { va = ha ? la + cross(aa, r.ra) : r.vfix; vb = hb ? lb + cross(ab, r.rb) : r.vfix; }
+    float v = dot(vb - va, r.n);
+    float old = jn[q];
+    float nw = clampf(old + (r.bias - v) * r.m_n, r.mu_s, r.mu_k);
+    jn[q] = nw;
+    if (nw != old) {
+      joint_apply_reg(la, aa, lb, ab, r, qa, qb, ima, imb, nw - old);
+      moved = true;
+    }
+    dres[3 * q] = nw - old;
+    dres[3 * q + 1] = 0.0f;
+    dres[3 * q + 2] = 0.0f;
+  }
+  if (moved) {
+    if (ia) { lin[r0.la] = f4(la, LA.w); ang[r0.la] = f4(aa, AA.w); }
+    if (ib) { lin[r0.lb] = f4(lb, LB.w); ang[r0.lb] = f4(ab, AB.w); }
+  }
+}
 // The row update on bodies whose velocities live in lin / ang (shared memory), with both bodies'
 // world inverse inertia and inverse mass passed in; jn / jt are the row's accumulators, d3
 // receives (new_jn - old_jn, friction deltas) for the residual.
@@ -1503,8 +1540,7 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
         if (MULTI && W.isl_done[r.flags >> 16]) continue;
         if (r.flags & RF_JOINT) {  // a joint is one unit: its first row runs all its rows in order
           if (!(r.flags & RF_JFIRST)) continue;
-          const uint32_t cnt = (uint32_t)r.t1.x;
-          for (uint32_t q = 0; q < cnt; ++q) pgs_row_reg(B, W.rows[i + q], i + q, W.jn, W.jt, W.dres);
+          joint_unit_core(B.lin, B.ang, &W.rows[i], (uint32_t)r.t1.x, B.Iw, B.im, &W.jn[i], &W.dres[3 * (size_t)i]);
           continue;
         }
         pgs_row_reg(B, r, i, W.jn, W.jt, W.dres);
