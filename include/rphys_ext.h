@@ -211,6 +211,7 @@ RPhysResult rphys_ext_get_row_predictions(const RPhysWorld* world, float* out4, 
  * descriptor adds none. */
 #define RPHYS_JOINT_BALL  0u
 #define RPHYS_JOINT_HINGE 1u
+#define RPHYS_JOINT_D6    2u   /* World::add_d6_joint with every axis enabled (locked), no stored hinge axis */
 typedef struct RPhysJointDesc {
     uint32_t kind;         /* RPHYS_JOINT_* */
     uint32_t hinge_axis;   /* RPHYS_JOINT_HINGE only */
@@ -232,6 +233,28 @@ typedef struct RPhysJointLimit {
 } RPhysJointLimit;
 RPhysResult rphys_ext_set_joint_limits(RPhysWorld* world, const RPhysJointLimit* limits, uint32_t n);
 RPhysResult rphys_ext_num_joints(const RPhysWorld* world, uint32_t* out_count);
+
+/* D6Axis.enabled and .compliance of one axis (m/N or rad/(N m); 0 = rigid), as a D6Joint built for
+ * World::add_d6_joint sets them (riftphys-articulation/src/bodies.rs:80-108). A compliant axis has
+ * no velocity row and acts as an XPBD spring at position level; a rotational axis whose compliance
+ * is at least 100x each other enabled one makes the joint a sprung hinge about it
+ * (d6_hinge_axis, bodies.rs:891-901). compliance finite and >= 0. */
+RPhysResult rphys_ext_set_joint_axis(RPhysWorld* world, uint32_t joint, uint32_t angular, uint32_t axis,
+                                     uint32_t enabled, float compliance);
+/* Joints::set_d6_drive_t / set_d6_drive_r (bodies.rs:354-366); drive = NULL clears it. A position
+ * drive (vel_mode 0) holds the axis at target (clamped into its limit) at position level; a
+ * velocity drive is a motor row driving the relative velocity to target with at most
+ * |max_impulse| per tick, and bodies of a joint with a rotational velocity drive keep the angular
+ * velocity the solve gave them (step.rs:352-366). Setting one enables the axis. Finite values. */
+typedef struct RPhysJointDrive { float target, kp, kd, max_impulse; uint32_t vel_mode; } RPhysJointDrive;
+RPhysResult rphys_ext_set_joint_drive(RPhysWorld* world, uint32_t joint, uint32_t angular, uint32_t axis,
+                                      const RPhysJointDrive* drive);
+/* Joints::set_d6_damping (bodies.rs:376-383): viscous damping (N m s/rad or N s/m; an implicit
+ * velocity row, or XPBD's damping term on a compliant unlimited row) and Coulomb friction (N m or
+ * N: at most friction x dt of impulse per tick) on one axis, free axes too. Negative or non-finite
+ * values become 0, as in the reference. */
+RPhysResult rphys_ext_set_joint_damping(RPhysWorld* world, uint32_t joint, uint32_t angular, uint32_t axis,
+                                        float damping, float friction);
 
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:

@@ -512,7 +512,7 @@ RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_
   std::lock_guard<std::mutex> g(W->mu);
   std::vector<std::pair<uint32_t, uint32_t>> ab(n);
   for (uint32_t i = 0; i < n; ++i) {
-    if (d[i].kind > RPHYS_JOINT_HINGE || (d[i].kind == RPHYS_JOINT_HINGE && d[i].hinge_axis > 2))
+    if (d[i].kind > RPHYS_JOINT_D6 || (d[i].kind == RPHYS_JOINT_HINGE && d[i].hinge_axis > 2))
       return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: bad kind or hinge axis");
     if (!fin_iso(d[i].frame_a) || !fin_iso(d[i].frame_b)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: frame contains NaN/Inf");
     RPhysResult r = live_id(W, d[i].body_a, "rphys_ext_add_joints", &ab[i].first);
@@ -525,7 +525,8 @@ RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_
   for (uint32_t i = 0; i < n; ++i) {
     Iso fa{v(d[i].frame_a.pos), q(d[i].frame_a.rot)}, fb{v(d[i].frame_b.pos), q(d[i].frame_b.rot)};
     if (d[i].kind == RPHYS_JOINT_BALL) W->w.add_ball_joint(ab[i].first, ab[i].second, fa, fb);
-    else W->w.add_hinge_joint(ab[i].first, ab[i].second, fa, fb, d[i].hinge_axis);
+    else if (d[i].kind == RPHYS_JOINT_HINGE) W->w.add_hinge_joint(ab[i].first, ab[i].second, fa, fb, d[i].hinge_axis);
+    else W->w.add_d6_joint(ab[i].first, ab[i].second, fa, fb);
   }
   return RPHYS_OK;
 }
@@ -563,6 +564,41 @@ uint32_t rphys_oracle_turned_threshold_mismatches(uint32_t dstar_bits) {
   for (float d = 0.8f; d <= 1.0f; d = std::nextafter(d, 2.0f))
     if ((2.0f * om::acosf_unit_rp(d) < 0.5f) != (d >= dstar)) bad++;
   return bad;
+}
+RPhysResult rphys_ext_set_joint_axis(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, uint32_t enabled,
+                                     float compliance) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_axis: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  if (joint >= W->w.joints.size()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_axis: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_axis: axis > 2");
+  if (!(std::isfinite(compliance) && compliance >= 0.0f))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_axis: compliance must be finite and >= 0");
+  W->w.set_d6_axis(joint, angular != 0, axis, enabled != 0, compliance);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_joint_drive(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis,
+                                      const RPhysJointDrive* d) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_drive: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  if (joint >= W->w.joints.size()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_drive: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_drive: axis > 2");
+  if (d && !(std::isfinite(d->target) && std::isfinite(d->kp) && std::isfinite(d->kd) && std::isfinite(d->max_impulse)))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_drive: non-finite drive value");
+  if (d) W->w.set_d6_drive(joint, angular != 0, axis, true, d->target, d->kp, d->kd, d->max_impulse, d->vel_mode != 0);
+  else W->w.set_d6_drive(joint, angular != 0, axis, false, 0.0f, 0.0f, 0.0f, 0.0f, false);
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_set_joint_damping(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, float damping,
+                                        float friction) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_damping: world is null");
+  std::lock_guard<std::mutex> g(W->mu);
+  if (joint >= W->w.joints.size()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_damping: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_damping: axis > 2");
+  W->w.set_d6_damping(joint, angular != 0, axis, damping, friction);
+  return RPHYS_OK;
 }
 RPhysResult rphys_ext_num_joints(const RPhysWorld* W, uint32_t* out) {
   clear_err();

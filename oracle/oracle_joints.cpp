@@ -54,14 +54,59 @@ void World::set_d6_limit(uint32_t id, bool angular, uint32_t axis, bool has, flo
     if (angular && j.hinge >= 0 && j.hinge != (int)axis) j.hinge = -1;
   }
 }
+uint32_t World::add_d6_joint(uint32_t a, uint32_t b, const Iso& fa, const Iso& fb) {
+  Joint j;
+  j.a = a; j.b = b; j.fa = fa; j.fb = fb;
+  for (int k = 0; k < 3; ++k) { j.t[k].enabled = true; j.r[k].enabled = true; }
+  j.hinge = -1;
+  joints.push_back(j);
+  return (uint32_t)joints.size() - 1;
+}
+void World::set_d6_axis(uint32_t id, bool angular, uint32_t axis, bool enabled, float compliance) {
+  if (id >= joints.size() || axis > 2) return;
+  D6Axis& x = angular ? joints[id].r[axis] : joints[id].t[axis];
+  x.enabled = enabled;
+  x.compliance = compliance;
+}
+// Joints::set_d6_drive_t / set_d6_drive_r (bodies.rs:354-366)
+void World::set_d6_drive(uint32_t id, bool angular, uint32_t axis, bool has, float target, float kp, float kd,
+                         float max_impulse, bool vel_mode) {
+  if (id >= joints.size() || axis > 2) return;
+  Joint& j = joints[id];
+  D6Axis& x = angular ? j.r[axis] : j.t[axis];
+  x.has_drive = has;
+  x.d_target = target; x.d_kp = kp; x.d_kd = kd; x.d_max = max_impulse; x.vel_mode = vel_mode;
+  if (has) {
+    x.enabled = true;
+    if (angular && j.hinge >= 0 && j.hinge != (int)axis) j.hinge = -1;
+  }
+}
+// Joints::set_d6_damping (bodies.rs:376-383): negative or non-finite values become 0
+void World::set_d6_damping(uint32_t id, bool angular, uint32_t axis, float damping, float friction) {
+  if (id >= joints.size() || axis > 2) return;
+  D6Axis& x = angular ? joints[id].r[axis] : joints[id].t[axis];
+  x.damping = rmax(fin0(damping), 0.0f);
+  x.friction = rmax(fin0(friction), 0.0f);
+}
+
+bool position_damped(const D6Axis& a) {
+  return a.enabled && a.compliance > 0.0f && a.damping > 0.0f && !a.has_limit && (!a.has_drive || !a.vel_mode);
+}
 
 int d6_hinge_axis(const Joint& j) {
   if (j.hinge >= 0) return j.hinge < 3 ? j.hinge : -1;
   int free_axis = -1, n = 0;
   for (int i = 0; i < 3; ++i)
-    if (!(j.r[i].enabled && !j.r[i].has_limit)) { free_axis = i; n++; }
+    if (!(j.r[i].enabled && !j.r[i].has_limit && !j.r[i].has_drive)) { free_axis = i; n++; }
   if (n == 1) return free_axis;
-  return -1;  // the compliance rule needs a compliant row; none is restated
+  auto c = [&](int i) { return j.r[i].enabled ? rmax(fin0(j.r[i].compliance), 0.0f) : 0.0f; };
+  for (int i = 0; i < 3; ++i) {
+    if (!(j.r[i].enabled && c(i) > 0.0f)) continue;
+    bool all = true;
+    for (int k = 0; k < 3; ++k) all = all && (k == i || c(i) >= 100.0f * c(k));
+    if (all) return i;
+  }
+  return -1;
 }
 
 float d6_row_angle(const Joint& j, Q4 rot_a, Q4 rot_b, int i) {
@@ -89,16 +134,50 @@ void d6_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vect
       const D6Axis& row = ang ? j.r[i] : j.t[i];
       V3 u = axes[i];
       uint8_t tag = (uint8_t)((ang << 5) | (i << 3));
-      if (!row.enabled) continue;
-      float k;
-      if (ang) k = dot(u, mvec(ia, u)) + dot(u, mvec(ib, u));
-      else {
-        V3 ca = cross(ra, u), cb = cross(rb, u);
-        k = ((wa + wb) + dot(ca, mvec(ia, ca))) + dot(cb, mvec(ib, cb));
+      auto keff = [&](V3 uu) {
+        if (ang) return dot(uu, mvec(ia, uu)) + dot(uu, mvec(ib, uu));
+        V3 ca = cross(ra, uu), cb = cross(rb, uu);
+        return ((wa + wb) + dot(ca, mvec(ia, ca))) + dot(cb, mvec(ib, cb));
+      };
+      // joint damping and Coulomb friction (W3a), on any axis; a compliant damped row's damping
+      // is in its position row instead
+      float damp = position_damped(row) ? 0.0f : row.damping;
+      if (damp > 0.0f || row.friction > 0.0f) {
+        float kk = keff(u);
+        if (kk > 1.0e-9f) {
+          JRow base{a, b, joint, ang != 0, u, ra, rb, wa, wb, 1.0f / kk, 0.0f, -INFINITY, INFINITY, tag};
+          if (damp > 0.0f) {
+            JRow dr = base;
+            dr.gamma = 1.0f / (damp * dt);
+            dr.m_eff = 1.0f / (kk + dr.gamma);
+            dr.tag = (uint8_t)(tag | 4);
+            out.push_back(dr);
+          }
+          if (row.friction > 0.0f) {
+            JRow fr = base;
+            float cap = row.friction * dt;
+            fr.lam_min = -cap; fr.lam_max = cap;
+            fr.tag = (uint8_t)(tag | 5);
+            out.push_back(fr);
+          }
+        }
       }
+      if (!row.enabled || row.compliance > 0.0f) continue;
+      if (row.has_drive && !row.vel_mode) continue;  // position drives stay at position level
+      float k = keff(u);
       if (k <= 1.0e-9f) continue;
       JRow base{a, b, joint, ang != 0, u, ra, rb, wa, wb, 1.0f / k, 0.0f, -INFINITY, INFINITY, tag};
-      if (!row.has_limit) { out.push_back(base); continue; }
+      if (row.has_drive) {  // velocity motor: the relative velocity to the target, at most max_impulse
+        JRow mr = base;
+        float cap = std::fabs(row.d_max);
+        mr.target = row.d_target; mr.lam_min = -cap; mr.lam_max = cap;
+        mr.tag = (uint8_t)(tag | 1);
+        out.push_back(mr);
+      }
+      if (!row.has_limit) {
+        if (!row.has_drive) out.push_back(base);
+        continue;
+      }
       float x = ang ? d6_row_angle(j, rot_a, rot_b, i) : dot(d, u);
       JRow lo = base, hi = base;
       lo.target = rmin((row.lo - x) / dt, 0.0f); lo.lam_min = 0.0f; lo.tag = (uint8_t)(tag | 2);
@@ -128,7 +207,9 @@ void joint_row_apply(World& w, const JRow& r, float lam) {
 float joint_row_update(World& w, const JRow& r, float& acc) {
   float v = joint_row_vel(w, r);
   float old = acc;
-  float nw = clampf(old + (r.target - v) * r.m_eff, r.lam_min, r.lam_max);
+  // rigid rows: v -> target; soft rows (dampers): v + gamma lam -> target
+  float nw = r.gamma == 0.0f ? old + (r.target - v) * r.m_eff : old + ((r.target - v) - r.gamma * old) * r.m_eff;
+  nw = clampf(nw, r.lam_min, r.lam_max);
   acc = nw;
   if (nw != old) joint_row_apply(w, r, nw - old);
   return nw - old;
@@ -163,11 +244,52 @@ static M3 inv_inertia_at(const World& w, uint32_t id, Q4 rot) {
   M3 r = mfrom_quat(rot);
   return mmul(mmul(r, w.inv_I[id]), mtranspose(r));
 }
+// alpha_dt2 (bodies.rs:438-441)
+static float alpha_dt2(float c, float dt2) {
+  c = rmax(fin0(c), 0.0f);
+  return c <= 0.0f ? 0.0f : fin0(c / dt2);
+}
+// The error a row acts on (bodies.rs:674-698, 786-810): locked at 0, a limit only while violated,
+// a position drive's target (clamped into the limit); a velocity drive leaves the axis free at
+// position level unless it is limited. False: nothing to correct.
+static bool row_error(const D6Axis& row, float coord, float* c) {
+  bool has = true;
+  *c = fin0(coord - 0.0f);
+  if (row.has_limit) {
+    float lo = fin0(row.lo), hi = fin0(row.hi);
+    if (coord < lo) *c = fin0(coord - lo);
+    else if (coord > hi) *c = fin0(coord - hi);
+    else has = false;
+  }
+  if (row.has_drive) {
+    if (!row.vel_mode) {
+      float target = fin0(row.d_target);
+      if (row.has_limit) target = clampf(target, fin0(row.lo), fin0(row.hi));
+      *c = fin0(coord - target);
+      has = true;
+    } else if (!row.has_limit) {
+      has = false;
+    }
+  }
+  return has;
+}
+// The measure of rotational row i at joint-frame rotations ra, rb (bodies.rs:796-803).
+static float row_angle(int hinge, Q4 ra, Q4 rb, int i, V3 u) {
+  Q4 q = qmul(qconj(ra), rb);
+  if (q.w < 0.0f) q = qneg(q);
+  V3 v{q.x, q.y, q.z};
+  if (hinge == i) return fin0(2.0f * atan2f_rp(comp(v, i), q.w));
+  if (hinge >= 0)
+    return fin0(dot(fin_v(cross(normalize_fin(qrot(ra, kUnit[hinge])), normalize_fin(qrot(rb, kUnit[hinge])))), u));
+  return fin0(dot(fin_v(qrot(ra, fin_v(mul(v, 2.0f)))), u));
+}
 
-// solve_d6 (bodies.rs:616-873) for locked and limited axes (no drive, compliance 0, so alpha = 0
-// and every row is the plain XPBD step).
+// solve_d6 (bodies.rs:616-873) without the rotor rows (no armature). sa / sb: the step's start
+// poses, for SHAKE's directions (when neither body turned too far) and for a damped compliant
+// row's change since the start.
 static void solve_d6(World& w, Joint& j, float dt, const Iso* sa, const Iso* sb) {
   const float wa = fin0(w.inv_mass[j.a]), wb = fin0(w.inv_mass[j.b]);
+  const float dt2 = rmax(dt * dt, 1.0e-12f);
   Q4 ra0_rot = w.rot[j.a], rb0_rot = w.rot[j.b];
   bool shake = sa && sb && turned(sa->rot, ra0_rot) < kShakeMaxTurn && turned(sb->rot, rb0_rot) < kShakeMaxTurn;
   V3 ax0[3] = {}, la0{}, lb0{};
@@ -180,17 +302,10 @@ static void solve_d6(World& w, Joint& j, float dt, const Iso* sa, const Iso* sb)
     ia0 = inv_inertia_at(w, j.a, sa->rot);
     ib0 = inv_inertia_at(w, j.b, sb->rot);
   }
-  const float alpha = 0.0f, bias_vel = 0.0f;
-  auto limit_err = [](const D6Axis& row, float coord, float* c) {
-    *c = fin0(coord - 0.0f);
-    if (!row.has_limit) return true;
-    float lo = fin0(row.lo), hi = fin0(row.hi);
-    if (coord < lo) { *c = fin0(coord - lo); return true; }
-    if (coord > hi) { *c = fin0(coord - hi); return true; }
-    return false;
-  };
+  const float bias_vel = 0.0f;
   for (int i = 0; i < 3; ++i) {
-    if (!j.t[i].enabled) continue;
+    const D6Axis& row = j.t[i];
+    if (!row.enabled) continue;
     Iso pa{w.pos[j.a], w.rot[j.a]}, pb{w.pos[j.b], w.rot[j.b]};
     V3 u = normalize_fin(qrot(qmul(pa.rot, j.fa.rot), kUnit[i]));
     if (vzero(u)) continue;
@@ -206,16 +321,26 @@ static void solve_d6(World& w, Joint& j, float dt, const Iso* sa, const Iso* sb)
     }
     float coord = fin0(dot(d, u));
     float c;
-    if (!limit_err(j.t[i], coord, &c)) continue;
+    if (!row_error(row, coord, &c)) continue;
     V3 ra_u = fin_v(cross(lever_a, un)), rb_u = fin_v(cross(lever_b, un));
     float w_rot_a = fin0(dot(ra_u, mvec(iaw, ra_u)));
     float w_rot_b = fin0(dot(rb_u, mvec(ibw, rb_u)));
     float ws = fin0(((wa + wb) + w_rot_a) + w_rot_b);
+    float alpha = alpha_dt2(row.compliance, dt2);
     float denom = fin0(ws + alpha);
     if (denom <= 0.0f) continue;
     c = fin0(c + fin0(bias_vel * dt));
     float lambda_old = fin0(j.lam_t[i]);
-    float dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    float dl;
+    if (position_damped(row) && sa && sb) {  // Kelvin-Voigt: spring and damper in one implicit row
+      V3 u0 = normalize_fin(qrot(qmul(sa->rot, j.fa.rot), kUnit[i]));
+      V3 d0 = fin_v(sub(add(sb->pos, qrot(sb->rot, j.fb.pos)), add(sa->pos, qrot(sa->rot, j.fa.pos))));
+      float gamma = fin0(row.compliance * row.damping / dt);
+      float dc = fin0(coord - dot(d0, u0));
+      dl = fin0(-((c + fin0(alpha * lambda_old)) + fin0(gamma * dc)) / fin0((1.0f + gamma) * ws + alpha));
+    } else {
+      dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    }
     j.lam_t[i] = fin0(lambda_old + dl);
     apply_position_delta(w, j.a, fin_v(mul(neg(un), fin0(dl * wa))));
     apply_position_delta(w, j.b, fin_v(mul(un, fin0(dl * wb))));
@@ -224,30 +349,35 @@ static void solve_d6(World& w, Joint& j, float dt, const Iso* sa, const Iso* sb)
   }
   const int hinge = d6_hinge_axis(j);
   for (int i = 0; i < 3; ++i) {
-    if (!j.r[i].enabled) continue;
+    const D6Axis& row = j.r[i];
+    if (!row.enabled) continue;
     Q4 ra = qmul(w.rot[j.a], j.fa.rot), rb = qmul(w.rot[j.b], j.fb.rot);
     V3 u = normalize_fin(qrot(ra, kUnit[i]));
     if (vzero(u)) continue;
-    Q4 q = qmul(qconj(ra), rb);
-    if (q.w < 0.0f) q = qneg(q);
-    V3 v{q.x, q.y, q.z};
-    float angle;
-    if (hinge == i) angle = fin0(2.0f * atan2f_rp(comp(v, i), q.w));
-    else if (hinge >= 0)
-      angle = fin0(dot(fin_v(cross(normalize_fin(qrot(ra, kUnit[hinge])), normalize_fin(qrot(rb, kUnit[hinge])))), u));
-    else angle = fin0(dot(fin_v(qrot(ra, fin_v(mul(v, 2.0f)))), u));
+    float angle = row_angle(hinge, ra, rb, i, u);
     V3 un;
     M3 iaw, ibw;
     if (shake) { un = ax0[i]; iaw = ia0; ibw = ib0; }
     else { un = u; iaw = w.inv_inertia_world(j.a); ibw = w.inv_inertia_world(j.b); }
     float c;
-    if (!limit_err(j.r[i], angle, &c)) continue;
+    if (!row_error(row, angle, &c)) continue;
     float ws = fin0(dot(un, mvec(iaw, un)) + dot(un, mvec(ibw, un)));
+    float alpha = alpha_dt2(row.compliance, dt2);
     float denom = fin0(ws + alpha);
     if (denom <= 0.0f) continue;
     c = fin0(c + fin0(bias_vel * dt));
     float lambda_old = fin0(j.lam_r[i]);
-    float dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    float dl;
+    if (position_damped(row) && sa && sb) {
+      Q4 ra0 = qmul(sa->rot, j.fa.rot), rb0 = qmul(sb->rot, j.fb.rot);
+      V3 u0 = normalize_fin(qrot(ra0, kUnit[i]));
+      float angle0 = row_angle(hinge, ra0, rb0, i, u0);
+      float gamma = fin0(row.compliance * row.damping / dt);
+      float dc = fin0(angle - angle0);
+      dl = fin0(-((c + fin0(alpha * lambda_old)) + fin0(gamma * dc)) / fin0((1.0f + gamma) * ws + alpha));
+    } else {
+      dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    }
     j.lam_r[i] = fin0(lambda_old + dl);
     apply_orientation_delta(w, j.a, fin_v(mul(neg(mvec(iaw, un)), dl)));
     apply_orientation_delta(w, j.b, fin_v(mul(mvec(ibw, un), dl)));

@@ -9,13 +9,14 @@
 
 namespace orc {
 
-// JointRow (solver.rs:264-288) with gamma = 0 (no damper rows are restated).
+// JointRow (solver.rs:264-288): gamma = 1 / (damping dt) on a damper row, 0 on the others.
 struct JRow {
   uint32_t a, b, joint;
   bool angular;
   V3 u, ra, rb;
   float wa, wb, m_eff, target, lam_min, lam_max;
   uint8_t tag;
+  float gamma = 0.0f;
   uint8_t idx = 0, cnt = 0;  // index in its joint's rows; the joint's row count (on its first row)
 };
 
@@ -28,6 +29,8 @@ void d6_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vect
 // joint_row_vel / joint_row_apply (solver.rs:291-307)
 float joint_row_vel(const World& w, const JRow& r);
 void joint_row_apply(World& w, const JRow& r, float lam);
+// position_damped (bodies.rs:58-61)
+bool position_damped(const D6Axis& a);
 // One Gauss-Seidel update of a joint row (solver.rs:821-830); returns new - old.
 float joint_row_update(World& w, const JRow& r, float& acc);
 // Joints::solve_step_with for one sweep (bodies.rs:422-471) with SHAKE directions from start

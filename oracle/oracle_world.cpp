@@ -1573,6 +1573,14 @@ void World::step(float dt) {
     if (c.depth - kMargin > -kPosSlop && pair_props(colliders[c.a_collider].mat, mb).stiffness <= 0.0f)
       touching[colliders[c.a_collider].body] = 1;
   }
+  // bodies of a joint with a velocity drive on a rotational axis keep the angular velocity the
+  // motor rows gave them (step.rs:352-366, the "motor overwrite")
+  std::vector<uint8_t> driven(count, 0);
+  for (auto& jt : joints) {
+    bool any = false;
+    for (int k = 0; k < 3; ++k) any = any || (jt.r[k].has_drive && jt.r[k].vel_mode);
+    if (any) { driven[jt.a] = 1; driven[jt.b] = 1; }
+  }
   for (uint32_t i = 0; i < count; ++i) {
     if (!dyn[i] || !awake[i]) continue;
     V3 vl = lin[i], va = ang[i];
@@ -1587,11 +1595,11 @@ void World::step(float dt) {
       np.pos.y = old.pos.y;
       set_pose(i, np);
     }
-    if (!qeq(np.rot, pred.rot)) {
+    if (!driven[i] && !qeq(np.rot, pred.rot)) {
       Q4 dq = qmul(np.rot, qconj(pred.rot));
       V3 d_ang = mul(V3{dq.x, dq.y, dq.z}, 2.0f);
       if (dq.w < 0.0f) d_ang = neg(d_ang);
-      va = add(va, divs(sub(d_ang, sa), dt));  // no velocity drives: never motor-driven
+      va = add(va, divs(sub(d_ang, sa), dt));
     }
     set_vel(i, vl, va);
   }

@@ -53,9 +53,17 @@ struct HeightField {
   uint32_t mat = 4;
 };
 
-// D6 joint (bodies.rs:55-137) at the restated feature set: an axis is enabled (locked) or free,
-// with an optional limit [lo, hi]; hinge is the stored hinge axis (add_hinge) or -1.
-struct D6Axis { bool enabled = false, has_limit = false; float lo = 0.0f, hi = 0.0f; };
+// D6 joint (bodies.rs:55-137) at the restated feature set: an axis is enabled or free, with an
+// optional limit [lo, hi], XPBD compliance, an optional drive (position target, or a velocity motor
+// with its impulse cap), viscous damping and Coulomb friction; hinge is the stored hinge axis
+// (add_hinge) or -1. Armature is not restated.
+struct D6Axis {
+  bool enabled = false, has_limit = false;
+  float lo = 0.0f, hi = 0.0f;
+  float compliance = 0.0f, damping = 0.0f, friction = 0.0f;
+  bool has_drive = false, vel_mode = false;
+  float d_target = 0.0f, d_kp = 0.0f, d_kd = 0.0f, d_max = 0.0f;
+};
 struct Joint {
   uint32_t a, b;
   Iso fa, fb;
@@ -151,6 +159,14 @@ struct World {
   uint32_t add_ball_joint(uint32_t a, uint32_t b, const Iso& fa, const Iso& fb);
   uint32_t add_hinge_joint(uint32_t a, uint32_t b, const Iso& fa, const Iso& fb, uint32_t axis);
   void set_d6_limit(uint32_t id, bool angular, uint32_t axis, bool has, float lo, float hi);
+  // World::add_d6_joint (world.rs:720-725) with every axis enabled (locked) and no stored hinge axis
+  uint32_t add_d6_joint(uint32_t a, uint32_t b, const Iso& fa, const Iso& fb);
+  // D6Axis.enabled / .compliance as add_d6_joint's struct sets them
+  void set_d6_axis(uint32_t id, bool angular, uint32_t axis, bool enabled, float compliance);
+  // set_d6_drive_t / set_d6_drive_r (bodies.rs:354-366) and set_d6_damping (:376-383)
+  void set_d6_drive(uint32_t id, bool angular, uint32_t axis, bool has, float target, float kp, float kd,
+                    float max_impulse, bool vel_mode);
+  void set_d6_damping(uint32_t id, bool angular, uint32_t axis, float damping, float friction);
   PairProps pair_props(uint32_t a, uint32_t b) const;
   void set_pair_props(uint32_t a, uint32_t b, const PairProps& p);
   void update_colliders_aabb();

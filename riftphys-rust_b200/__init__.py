@@ -125,6 +125,12 @@ class JointDesc(Structure):
 
 JOINT_BALL = 0
 JOINT_HINGE = 1
+JOINT_D6 = 2
+
+
+class JointDrive(Structure):
+    _fields_ = [("target", c_float), ("kp", c_float), ("kd", c_float), ("max_impulse", c_float),
+                ("vel_mode", c_uint32)]
 
 
 class JointLimit(Structure):
@@ -254,6 +260,9 @@ ABI = [
     ("rphys_ext_set_joint_limit", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float, c_float]),
     ("rphys_ext_num_joints", c_uint32, [c_void_p, POINTER(c_uint32)]),
     ("rphys_ext_set_joint_limits", c_uint32, [c_void_p, c_void_p, c_uint32]),
+    ("rphys_ext_set_joint_axis", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float]),
+    ("rphys_ext_set_joint_drive", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, POINTER(JointDrive)]),
+    ("rphys_ext_set_joint_damping", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_float, c_float]),
 ]
 
 
@@ -532,6 +541,17 @@ class World:
         on = lo is not None
         self.c("rphys_ext_set_joint_limit", joint, 1 if angular else 0, axis, 1 if on else 0,
                float(lo if on else 0.0), float(hi if on else 0.0))
+
+    def set_joint_axis(self, joint, angular, axis, enabled=True, compliance=0.0):
+        self.c("rphys_ext_set_joint_axis", joint, 1 if angular else 0, axis, 1 if enabled else 0, float(compliance))
+
+    def set_joint_drive(self, joint, angular, axis, target=None, kp=0.0, kd=0.0, max_impulse=0.0, velocity=False):
+        """A position drive (velocity=False) or a velocity motor on one axis; target=None clears it."""
+        d = None if target is None else byref(JointDrive(target, kp, kd, max_impulse, 1 if velocity else 0))
+        self.c("rphys_ext_set_joint_drive", joint, 1 if angular else 0, axis, d)
+
+    def set_joint_damping(self, joint, angular, axis, damping=0.0, friction=0.0):
+        self.c("rphys_ext_set_joint_damping", joint, 1 if angular else 0, axis, float(damping), float(friction))
 
     def num_joints(self):
         n = c_uint32(0)

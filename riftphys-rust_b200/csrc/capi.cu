@@ -603,7 +603,8 @@ RPhysResult rphys_ext_set_heightfield_f32(RPhysWorld* W, uint32_t nx, uint32_t n
     return set_hf(W, nx, nz, cx, cz, ox, oz, std::move(hh), mat);
   });
 }
-// World::add_ball_joint / add_hinge_joint (world.rs:718-719), all-or-nothing over the array.
+// World::add_ball_joint / add_hinge_joint (world.rs:718-719) and D6 joints with every axis locked,
+// all-or-nothing over the array.
 RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_t n, uint32_t* out_first) {
   clear_err();
   if (out_first) *out_first = 0;
@@ -612,7 +613,7 @@ RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_
   return guard("rphys_ext_add_joints", [&]() {
     std::vector<uint32_t> ab(2 * (size_t)n);
     for (uint32_t i = 0; i < n; ++i) {
-      if (d[i].kind > RPHYS_JOINT_HINGE || (d[i].kind == RPHYS_JOINT_HINGE && d[i].hinge_axis > 2))
+      if (d[i].kind > RPHYS_JOINT_D6 || (d[i].kind == RPHYS_JOINT_HINGE && d[i].hinge_axis > 2))
         return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: bad kind or hinge axis");
       if (!fin_iso(d[i].frame_a) || !fin_iso(d[i].frame_b))
         return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_joints: frame contains NaN/Inf");
@@ -668,6 +669,50 @@ RPhysResult rphys_ext_set_joint_limits(RPhysWorld* W, const RPhysJointLimit* l, 
   return guard("rphys_ext_set_joint_limits", [&]() {
     for (uint32_t i = 0; i < n; ++i)
       W->w->set_joint_limit(l[i].joint, l[i].angular != 0, l[i].axis, l[i].enabled != 0, l[i].lo, l[i].hi);
+    W->w->upload_joints();
+    return RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_set_joint_axis(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, uint32_t enabled,
+                                     float compliance) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_axis: world is null");
+  LOCK;
+  if (joint >= W->w->num_joints()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_axis: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_axis: axis > 2");
+  if (!(std::isfinite(compliance) && compliance >= 0.0f))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_axis: compliance must be finite and >= 0");
+  return guard("rphys_ext_set_joint_axis", [&]() {
+    W->w->set_joint_axis(joint, angular != 0, axis, enabled != 0, compliance);
+    W->w->upload_joints();
+    return RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_set_joint_drive(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis,
+                                      const RPhysJointDrive* d) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_drive: world is null");
+  LOCK;
+  if (joint >= W->w->num_joints()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_drive: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_drive: axis > 2");
+  if (d && !(std::isfinite(d->target) && std::isfinite(d->kp) && std::isfinite(d->kd) && std::isfinite(d->max_impulse)))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_drive: non-finite drive value");
+  return guard("rphys_ext_set_joint_drive", [&]() {
+    if (d) W->w->set_joint_drive(joint, angular != 0, axis, true, d->target, d->kp, d->kd, d->max_impulse, d->vel_mode != 0);
+    else W->w->set_joint_drive(joint, angular != 0, axis, false, 0.0f, 0.0f, 0.0f, 0.0f, false);
+    W->w->upload_joints();
+    return RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_set_joint_damping(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, float damping,
+                                        float friction) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_joint_damping: world is null");
+  LOCK;
+  if (joint >= W->w->num_joints()) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_set_joint_damping: joint out of range");
+  if (axis > 2) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_joint_damping: axis > 2");
+  return guard("rphys_ext_set_joint_damping", [&]() {
+    W->w->set_joint_damping(joint, angular != 0, axis, damping, friction);
     W->w->upload_joints();
     return RPHYS_OK;
   });

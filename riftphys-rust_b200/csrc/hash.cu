@@ -194,8 +194,8 @@ __global__ void k_hj_write(uint32_t n, const uint32_t* __restrict__ jw_n, const 
   put32(p, j);
   put32(p + 4, c);
   for (uint32_t k = 0; k < c; ++k) {
-    p[8 + 5 * k] = tag[12 * (size_t)j + k];
-    put32(p + 9 + 5 * k, canon_bits(lam[12 * (size_t)j + k]));
+    p[8 + 5 * k] = tag[kJointRows * (size_t)j + k];
+    put32(p + 9 + 5 * k, canon_bits(lam[kJointRows * (size_t)j + k]));
   }
 }
 // Sizes the joint section of joints [j0, j0 + n): bytes of its entries and their count.
@@ -211,7 +211,7 @@ static void joint_section(WorldGpu& W, uint32_t j0, uint32_t n, uint32_t* sz, ui
 static void joint_write(WorldGpu& W, uint32_t j0, uint32_t n, const uint32_t* off, uint8_t* out, cudaStream_t st) {
   if (!n) return;
   const int T = 256;
-  k_hj_write<<<(n + T - 1) / T, T, 0, st>>>(n, W.jw_n.p + j0, W.jw_tag.p + 12 * (size_t)j0, W.jw_lam.p + 12 * (size_t)j0,
+  k_hj_write<<<(n + T - 1) / T, T, 0, st>>>(n, W.jw_n.p + j0, W.jw_tag.p + kJointRows * (size_t)j0, W.jw_lam.p + kJointRows * (size_t)j0,
                                              off, out); RP_COUNT_LAUNCH(1);
 }
 
@@ -449,7 +449,7 @@ void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
   void* temp = base + NOALLOC_OFF_TEMP;
   // the stream length bound holds with every warm entry under its own key (the most bytes) and
   // every joint holding the most rows
-  uint64_t worst = 48 + 56ull * nb_ + 8 + 48ull * n_warm + 24 + (8 + 5ull * 12) * nj + 8 + 12ull * nb_ + 8 + cap + 8 +
+  uint64_t worst = 48 + 56ull * nb_ + 8 + 48ull * n_warm + 24 + (8 + 5ull * kJointRows) * nj + 8 + 12ull * nb_ + 8 + cap + 8 +
                    2ull * cap;
   if (worst > NOALLOC_STREAM_MAX)
     throw std::length_error("step_hash_noalloc: state stream of up to " + std::to_string(worst) + " bytes (" +

@@ -3,6 +3,7 @@
 // same row arrays as the contacts, their warm start and warm cache (solver.rs:699-712, 946-952),
 // and the World-level joint API (world.rs:718-720, 966-968).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <stdexcept>
 
@@ -36,48 +37,53 @@ __global__ void k_joint_marks(uint32_t nj, const JointGpu* __restrict__ J, const
 __global__ void k_joint_count(uint32_t nj, const JointGpu* __restrict__ J, BodiesV B, float dt, uint32_t* cnt) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nj) return;
-  JRowD rows[JMAX_ROWS];
-  cnt[j] = d6_rows_dev(J[j], B, dt, rows);
+  cnt[j] = d6_rows_dev(J[j], B, dt, [](const JRowD&, uint32_t) {});
 }
 // Rows of joint j at R[base + off[j] + k]. Warm start (solver.rs:703-712): the previous rows'
 // impulses when the joint has an entry with the same row count and tags, each clamped to its
 // row's bounds. A joint row stores: ra.w = 1 / k, t1 = (row count on the first row, index in the
-// joint, 0, target), t2.x = warm impulse, mu = (lam_min, lam_max, 0, tag), la.x = the joint's index
-// (bits).
+// joint, gamma, target), t2.x = warm impulse, mu = (lam_min, lam_max, 0, tag), la.x = the joint's
+// index (bits).
 __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, BodiesV B, float dt,
                               const uint32_t* __restrict__ off, uint32_t base, RowsV R,
                               const uint32_t* __restrict__ jw_n, const uint8_t* __restrict__ jw_tag,
                               const float* __restrict__ jw_lam, float* acc_jn, float2* acc_jt, uint32_t* uf) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nj) return;
-  JRowD rows[JMAX_ROWS];
   const JointGpu jt = J[j];
-  uint32_t n = d6_rows_dev(jt, B, dt, rows);
-  if (n == 0) return;
-  bool match = jw_n[j] == n;
-  for (uint32_t k = 0; k < n && match; ++k) match = jw_tag[JMAX_ROWS * (size_t)j + k] == (uint8_t)rows[k].tag;
-  for (uint32_t k = 0; k < n; ++k) {
-    const JRowD& r = rows[k];
-    uint32_t i = base + off[j] + k;
-    uint32_t f = RF_JOINT | (r.angular ? RF_JANG : 0u) | (r.wa > 0.0f ? RF_WA : 0u) | (r.wb > 0.0f ? RF_WB : 0u) |
-                 (k == 0 ? RF_JFIRST : 0u) | (match ? RF_JWARM : 0u);
-    float lam = match ? clampf(jw_lam[JMAX_ROWS * (size_t)j + k], r.lo, r.hi) : 0.0f;
+  const uint32_t r0 = base + off[j], wn = jw_n[j];
+  bool tags_match = true, dyn_a = false, dyn_b = false;
+  uint32_t n = d6_rows_dev(jt, B, dt, [&](const JRowD& r, uint32_t k) {
+    uint32_t i = r0 + k;
+    tags_match = tags_match && k < wn && jw_tag[JMAX_ROWS * (size_t)j + k] == (uint8_t)r.tag;
+    if (k == 0) { dyn_a = r.wa > 0.0f; dyn_b = r.wb > 0.0f; }
     R.ab[i] = make_uint2(jt.a, jt.b);
-    R.flags[i] = f;
+    R.flags[i] = RF_JOINT | (r.angular ? RF_JANG : 0u) | (r.wa > 0.0f ? RF_WA : 0u) | (r.wb > 0.0f ? RF_WB : 0u) |
+                 (k == 0 ? RF_JFIRST : 0u);
     R.inv[i] = make_float2(r.wa, r.wb);
     R.ra[i] = f4(r.ra, r.m_eff);
     R.rb[i] = f4(r.rb, 0.0f);
     R.n[i] = f4(r.u, 0.0f);
-    // t1.x: the joint's row count on its first row (the unit's length), t1.y: the row's index in it
-    R.t1[i] = make_float4(k == 0 ? (float)n : 0.0f, (float)k, 0.0f, r.target);
-    R.t2[i] = make_float4(lam, 0.0f, 0.0f, 0.0f);
+    // t1.x: the joint's row count on its first row (the unit's length, set below), t1.y: the row's index
+    R.t1[i] = make_float4(0.0f, (float)k, r.gamma, r.target);
+    R.t2[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     R.mu[i] = make_float4(r.lo, r.hi, 0.0f, __uint_as_float(r.tag));
     R.la[i] = make_float4(__uint_as_float(j), 0.0f, 0.0f, 0.0f);
     acc_jn[i] = 0.0f;
     acc_jt[i] = make_float2(0.0f, 0.0f);
+  });
+  if (n == 0) return;
+  R.t1[r0].x = (float)n;
+  if (tags_match && wn == n) {
+    for (uint32_t k = 0; k < n; ++k) {
+      const uint32_t i = r0 + k;
+      const float4 mu = R.mu[i];
+      R.flags[i] |= RF_JWARM;
+      R.t2[i].x = clampf(jw_lam[JMAX_ROWS * (size_t)j + k], mu.x, mu.y);
+    }
   }
   // the joint's rows join its two bodies' solve island when both can move
-  if (rows[0].wa > 0.0f && rows[0].wb > 0.0f) uf_union(uf, jt.a, jt.b);
+  if (dyn_a && dyn_b) uf_union(uf, jt.a, jt.b);
 }
 __global__ void k_joint_roots(uint32_t njr, uint32_t base, RowsV R, uint32_t* uf, uint32_t* row_root) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -164,13 +170,12 @@ uint32_t WorldGpu::world_of(uint32_t b) const {
   auto it = std::upper_bound(h_wb_start_.begin(), h_wb_start_.end(), b);
   return it == h_wb_start_.begin() ? 0u : (uint32_t)(it - h_wb_start_.begin()) - 1u;
 }
-// Joints::add_ball / add_hinge (bodies.rs:326-338)
+// Joints::add_ball / add_hinge (bodies.rs:326-338); kind 2: a D6 joint with every axis locked
 uint32_t WorldGpu::add_joint(uint32_t kind, uint32_t a, uint32_t b, const float fa[7], const float fb[7], uint32_t axis) {
   JointHost j{};
   j.a = a; j.b = b;
   for (int k = 0; k < 7; ++k) { j.fa[k] = fa[k]; j.fb[k] = fb[k]; }
-  for (int k = 0; k < 3; ++k) { j.en[k] = true; j.en[3 + k] = kind == 1 && (uint32_t)k != axis; }
-  for (int k = 0; k < 6; ++k) { j.lim[k] = false; j.lo[k] = 0.0f; j.hi[k] = 0.0f; }
+  for (int k = 0; k < 3; ++k) { j.en[k] = true; j.en[3 + k] = kind == 2 || (kind == 1 && (uint32_t)k != axis); }
   j.hinge = kind == 1 ? (int)axis : -1;
   if (batch_ && !h_wb_start_.empty()) {
     uint32_t wa = world_of(a), wb = world_of(b);
@@ -182,7 +187,12 @@ uint32_t WorldGpu::add_joint(uint32_t kind, uint32_t a, uint32_t b, const float 
   joints_dirty_ = true;
   return (uint32_t)h_joints_.size() - 1;
 }
-// Joints::set_d6_limit_t / set_d6_limit_r (bodies.rs:367-391) + leave_hinge (:876-878)
+// leave_hinge (bodies.rs:876-878): limiting or driving another rotational axis drops the stored
+// hinge axis
+static void leave_hinge(WorldGpu::JointHost& j, bool angular, uint32_t axis) {
+  if (angular && j.hinge >= 0 && j.hinge != (int)axis) j.hinge = -1;
+}
+// Joints::set_d6_limit_t / set_d6_limit_r (bodies.rs:367-391)
 void WorldGpu::set_joint_limit(uint32_t id, bool angular, uint32_t axis, bool on, float lo, float hi) {
   JointHost& j = h_joints_.at(id);
   uint32_t ax = (angular ? 3u : 0u) + axis;
@@ -190,17 +200,60 @@ void WorldGpu::set_joint_limit(uint32_t id, bool angular, uint32_t axis, bool on
   j.lo[ax] = lo; j.hi[ax] = hi;
   if (on) {
     j.en[ax] = true;
-    if (angular && j.hinge >= 0 && j.hinge != (int)axis) j.hinge = -1;
+    leave_hinge(j, angular, axis);
   }
   joints_dirty_ = true;
 }
-// d6_hinge_axis (bodies.rs:891-901) at the supported feature set (no compliant rows)
+// An axis locked (enabled) or free, and its XPBD compliance (0: rigid).
+void WorldGpu::set_joint_axis(uint32_t id, bool angular, uint32_t axis, bool enabled, float compliance) {
+  JointHost& j = h_joints_.at(id);
+  uint32_t ax = (angular ? 3u : 0u) + axis;
+  j.en[ax] = enabled;
+  j.comp[ax] = compliance;
+  joints_dirty_ = true;
+}
+// Joints::set_d6_drive_t / set_d6_drive_r (bodies.rs:354-366)
+void WorldGpu::set_joint_drive(uint32_t id, bool angular, uint32_t axis, bool on, float target, float kp, float kd,
+                               float max_impulse, bool vel_mode) {
+  JointHost& j = h_joints_.at(id);
+  uint32_t ax = (angular ? 3u : 0u) + axis;
+  j.drive[ax] = on;
+  j.dtarget[ax] = target; j.dkp[ax] = kp; j.dkd[ax] = kd; j.dmax[ax] = max_impulse; j.vel[ax] = vel_mode;
+  if (on) {
+    j.en[ax] = true;
+    leave_hinge(j, angular, axis);
+  }
+  joints_dirty_ = true;
+}
+// Joints::set_d6_damping (bodies.rs:376-383): negative or non-finite values become 0
+void WorldGpu::set_joint_damping(uint32_t id, bool angular, uint32_t axis, float damping, float friction) {
+  JointHost& j = h_joints_.at(id);
+  uint32_t ax = (angular ? 3u : 0u) + axis;
+  auto clean = [](float x) { return std::isfinite(x) && x > 0.0f ? x : 0.0f; };
+  j.damp[ax] = clean(damping);
+  j.fric[ax] = clean(friction);
+  joints_dirty_ = true;
+}
+// d6_hinge_axis (bodies.rs:891-901): the stored hinge axis; else the one free rotational axis
+// (neither locked, limited nor driven); else a compliant rotational axis at least 100x softer than
+// the other two.
 static int hinge_of(const WorldGpu::JointHost& j) {
   if (j.hinge >= 0) return j.hinge < 3 ? j.hinge : -1;
   int free_axis = -1, n = 0;
   for (int i = 0; i < 3; ++i)
-    if (!(j.en[3 + i] && !j.lim[3 + i])) { free_axis = i; n++; }
-  return n == 1 ? free_axis : -1;
+    if (!(j.en[3 + i] && !j.lim[3 + i] && !j.drive[3 + i])) { free_axis = i; n++; }
+  if (n == 1) return free_axis;
+  auto c = [&](int i) {
+    float x = j.comp[3 + i];
+    return j.en[3 + i] && std::isfinite(x) && x > 0.0f ? x : 0.0f;
+  };
+  for (int i = 0; i < 3; ++i) {
+    if (!(j.en[3 + i] && c(i) > 0.0f)) continue;
+    bool all = true;
+    for (int k = 0; k < 3; ++k) all = all && (k == i || c(i) >= 100.0f * c(k));
+    if (all) return i;
+  }
+  return -1;
 }
 template <class T>
 static void grow_keep(DBuf<T>& d, size_t old_n, size_t new_n, cudaStream_t st) {
@@ -215,8 +268,7 @@ static void grow_keep(DBuf<T>& d, size_t old_n, size_t new_n, cudaStream_t st) {
 void WorldGpu::upload_joints() {
   if (!joints_dirty_) return;
   const uint32_t nj = num_joints();
-  static_assert(sizeof(JointGpu) == 128, "JointGpu layout");
-  std::vector<JointGpu> h(nj ? nj : 1);
+    std::vector<JointGpu> h(nj ? nj : 1);
   std::vector<uint8_t> jointed(cap_b_ > nb_ ? cap_b_ : (nb_ ? nb_ : 1), 0);
   std::vector<unsigned long long> keys;
   for (uint32_t i = 0; i < nj; ++i) {
@@ -225,17 +277,25 @@ void WorldGpu::upload_joints() {
     std::memset(&g, 0, sizeof(g));
     g.a = s.a; g.b = s.b;
     uint32_t f = 0;
+    bool rdrive = false;
     for (int k = 0; k < 6; ++k) {
       if (s.en[k]) f |= 1u << k;
       if (s.lim[k]) f |= 1u << (JF_LIMIT_SHIFT + k);
+      if (s.drive[k]) f |= 1u << (JF_DRIVE_SHIFT + k);
+      if (s.vel[k]) f |= 1u << (JF_VEL_SHIFT + k);
       g.lo[k] = s.lo[k]; g.hi[k] = s.hi[k];
+      g.comp[k] = s.comp[k]; g.damp[k] = s.damp[k]; g.fric[k] = s.fric[k];
+      g.dtarget[k] = s.dtarget[k]; g.dmax[k] = s.dmax[k];
+      if (k >= 3 && s.drive[k] && s.vel[k]) rdrive = true;
     }
     f |= (uint32_t)(hinge_of(s) + 1) << JF_HINGE_SHIFT;
     g.flags = f;
     g.fa_p = make_float4(s.fa[0], s.fa[1], s.fa[2], 0.0f); g.fa_q = make_float4(s.fa[3], s.fa[4], s.fa[5], s.fa[6]);
     g.fb_p = make_float4(s.fb[0], s.fb[1], s.fb[2], 0.0f); g.fb_q = make_float4(s.fb[3], s.fb[4], s.fb[5], s.fb[6]);
-    jointed[s.a] = 1;
-    jointed[s.b] = 1;
+    // bit 0: in a joint; bit 1: in a joint with a rotational velocity drive (the motor overwrite)
+    const uint8_t mark = rdrive ? 3 : 1;
+    jointed[s.a] |= mark;
+    jointed[s.b] |= mark;
     keys.push_back(s.a < s.b ? (((unsigned long long)s.a << 32) | s.b) : (((unsigned long long)s.b << 32) | s.a));
   }
   std::sort(keys.begin(), keys.end());

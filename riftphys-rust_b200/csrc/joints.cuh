@@ -1,34 +1,49 @@
 // joints.cuh -- D6 joints on the GPU: the joint record the kernels read, its velocity rows
 // (d6_rows, riftphys-world/src/world/solver.rs:336-424) and its XPBD position solve with SHAKE
-// directions (solve_d6, riftphys-articulation/src/bodies.rs:616-873) for locked and limited axes.
+// directions (solve_d6, riftphys-articulation/src/bodies.rs:616-873): locked, limited, compliant
+// and driven axes, joint damping and friction (no armature rotors).
 // Every fin / normalize of the reference is kept where it stands: those sanitations change bits.
 #pragma once
 #include "step_rows.cuh"
 
 namespace rp {
 
-// One joint, 128 bytes. flags: bit i (i < 6) axis i enabled (t0 t1 t2 r0 r1 r2), bit 6 + i axis i
+// One joint, 256 bytes. flags: bit i (i < 6) axis i enabled (t0 t1 t2 r0 r1 r2), bit 6 + i axis i
 // limited to [lo[i], hi[i]], bits 12..14 the hinge axis + 1 (0: none; d6_hinge_axis, resolved on
-// the host whenever the joint changes).
+// the host whenever the joint changes), bit 16 + i axis i driven, bit 22 + i that drive a velocity
+// motor. Per axis: XPBD compliance, damping, friction, drive target and impulse cap.
 struct JointGpu {
   uint32_t a, b, flags, pad;
   float4 fa_p, fa_q, fb_p, fb_q;
   float lo[6], hi[6];
+  float comp[6], damp[6], fric[6], dtarget[6], dmax[6];
+  float pad2[2];
 };
-static_assert(sizeof(JointGpu) == 128, "JointGpu layout");
+static_assert(sizeof(JointGpu) == 256, "JointGpu layout");
 #define JF_LIMIT_SHIFT 6u
 #define JF_HINGE_SHIFT 12u
-#define JMAX_ROWS 12u  // 6 axes, 2 rows each when limited
+#define JF_DRIVE_SHIFT 16u
+#define JF_VEL_SHIFT 22u
+#define JMAX_ROWS kJointRows
 
 __host__ __device__ inline int joint_hinge(uint32_t flags) { return (int)((flags >> JF_HINGE_SHIFT) & 7u) - 1; }
 
-// A joint velocity row (JointRow, solver.rs:264-288; no damper rows, so gamma = 0).
+// A joint velocity row (JointRow, solver.rs:264-288); gamma = 1 / (damping dt) on a damper row.
 struct JRowD {
   f3 u, ra, rb;
-  float wa, wb, m_eff, target, lo, hi;
+  float wa, wb, m_eff, target, lo, hi, gamma;
   uint32_t tag;
   bool angular;
 };
+__host__ __device__ inline bool jaxis_on(uint32_t f, int ax) { return (f >> ax) & 1u; }
+__host__ __device__ inline bool jaxis_lim(uint32_t f, int ax) { return (f >> (JF_LIMIT_SHIFT + ax)) & 1u; }
+__host__ __device__ inline bool jaxis_drive(uint32_t f, int ax) { return (f >> (JF_DRIVE_SHIFT + ax)) & 1u; }
+__host__ __device__ inline bool jaxis_vel(uint32_t f, int ax) { return (f >> (JF_VEL_SHIFT + ax)) & 1u; }
+// position_damped (bodies.rs:58-61)
+__device__ __forceinline__ bool position_damped_dev(const JointGpu& j, int ax) {
+  return jaxis_on(j.flags, ax) && j.comp[ax] > 0.0f && j.damp[ax] > 0.0f && !jaxis_lim(j.flags, ax) &&
+         (!jaxis_drive(j.flags, ax) || !jaxis_vel(j.flags, ax));
+}
 
 __device__ __forceinline__ f3 unit_axis(int i) { return i == 0 ? mk3(1, 0, 0) : (i == 1 ? mk3(0, 1, 0) : mk3(0, 0, 1)); }
 __device__ __forceinline__ float comp3(f3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
@@ -53,9 +68,13 @@ __device__ __forceinline__ m3 inv_inertia_world_dev(const BodiesV& B, uint32_t i
   return world_inertia(rot, ld_m3(B.inv_I, id));
 }
 
-// d6_rows (solver.rs:336-424): the joint's rows in (linear x y z, angular x y z) order, limited
-// axes as a lower and an upper row. Returns the row count (0 when neither body is dynamic).
-__device__ __forceinline__ uint32_t d6_rows_dev(const JointGpu& j, const BodiesV& B, float dt, JRowD* out) {
+// d6_rows (solver.rs:336-424): per axis, in (linear x y z, angular x y z) order, a damper row and a
+// friction row when set (any axis; a compliant damped row's damping stays in its position row),
+// then for an enabled rigid axis without a position drive a motor row (velocity drive) and either
+// the equality row (no limit, no drive) or the two limit rows. Returns the row count (0 when
+// neither body is dynamic). Each row goes to emit(row, index in the joint) as it is made.
+template <class Emit>
+__device__ __forceinline__ uint32_t d6_rows_dev(const JointGpu& j, const BodiesV& B, float dt, Emit&& emit) {
   const uint32_t a = j.a, b = j.b;
   f3 pa = xyz(B.pos[a]), pb = xyz(B.pos[b]);
   q4 qa = asq(B.rot[a]), qb = asq(B.rot[b]);
@@ -70,27 +89,61 @@ __device__ __forceinline__ uint32_t d6_rows_dev(const JointGpu& j, const BodiesV
   for (int ang = 0; ang < 2; ++ang) {
     for (int i = 0; i < 3; ++i) {
       const int ax = 3 * ang + i;
-      if (!((j.flags >> ax) & 1u)) continue;
       f3 u = qrot(rot_a, unit_axis(i));
-      float k;
-      if (ang) k = dot(u, mvec(ia, u)) + dot(u, mvec(ib, u));
-      else {
+      auto keff = [&]() {
+        if (ang) return dot(u, mvec(ia, u)) + dot(u, mvec(ib, u));
         f3 ca = cross(ra, u), cb = cross(rb, u);
-        k = ((wa + wb) + dot(ca, mvec(ia, ca))) + dot(cb, mvec(ib, cb));
+        return ((wa + wb) + dot(ca, mvec(ia, ca))) + dot(cb, mvec(ib, cb));
+      };
+      JRowD base;
+      base.u = u; base.ra = ra; base.rb = rb; base.wa = wa; base.wb = wb;
+      base.target = 0.0f; base.lo = -INFINITY; base.hi = INFINITY; base.gamma = 0.0f;
+      base.tag = (uint32_t)((ang << 5) | (i << 3));
+      base.angular = ang != 0;
+      const float damp = position_damped_dev(j, ax) ? 0.0f : j.damp[ax];
+      if (damp > 0.0f || j.fric[ax] > 0.0f) {
+        float kk = keff();
+        if (kk > 1.0e-9f) {
+          if (damp > 0.0f) {
+            JRowD r = base;
+            r.gamma = 1.0f / (damp * dt);
+            r.m_eff = 1.0f / (kk + r.gamma);
+            r.tag = base.tag | 4u;
+            emit(r, n++);
+          }
+          if (j.fric[ax] > 0.0f) {
+            JRowD r = base;
+            r.m_eff = 1.0f / kk;
+            float cap = j.fric[ax] * dt;
+            r.lo = -cap; r.hi = cap;
+            r.tag = base.tag | 5u;
+            emit(r, n++);
+          }
+        }
       }
+      if (!jaxis_on(j.flags, ax) || j.comp[ax] > 0.0f) continue;
+      const bool drive = jaxis_drive(j.flags, ax), vel = jaxis_vel(j.flags, ax);
+      if (drive && !vel) continue;  // position drives stay at position level
+      float k = keff();
       if (k <= 1.0e-9f) continue;
-      JRowD r;
-      r.u = u; r.ra = ra; r.rb = rb; r.wa = wa; r.wb = wb; r.m_eff = 1.0f / k;
-      r.target = 0.0f; r.lo = -INFINITY; r.hi = INFINITY;
-      r.tag = (uint32_t)((ang << 5) | (i << 3));
-      r.angular = ang != 0;
-      if (!((j.flags >> (JF_LIMIT_SHIFT + ax)) & 1u)) { out[n++] = r; continue; }
+      base.m_eff = 1.0f / k;
+      if (drive) {  // velocity motor
+        JRowD r = base;
+        float cap = fabsf(j.dmax[ax]);
+        r.target = j.dtarget[ax]; r.lo = -cap; r.hi = cap;
+        r.tag = base.tag | 1u;
+        emit(r, n++);
+      }
+      if (!jaxis_lim(j.flags, ax)) {
+        if (!drive) emit(base, n++);
+        continue;
+      }
       float x = ang ? d6_row_angle_dev(hinge, rot_a, rot_b, i) : dot(d, u);
-      JRowD lo = r, hi = r;
-      lo.target = rmin((j.lo[ax] - x) / dt, 0.0f); lo.lo = 0.0f; lo.tag = r.tag | 2u;
-      hi.target = rmax((j.hi[ax] - x) / dt, 0.0f); hi.hi = 0.0f; hi.lo = -INFINITY; hi.tag = r.tag | 3u;
-      out[n++] = lo;
-      out[n++] = hi;
+      JRowD lo = base, hi = base;
+      lo.target = rmin((j.lo[ax] - x) / dt, 0.0f); lo.lo = 0.0f; lo.tag = base.tag | 2u;
+      hi.target = rmax((j.hi[ax] - x) / dt, 0.0f); hi.hi = 0.0f; hi.lo = -INFINITY; hi.tag = base.tag | 3u;
+      emit(lo, n++);
+      emit(hi, n++);
     }
   }
   return n;
@@ -118,12 +171,56 @@ __device__ __forceinline__ bool turned_below_max(q4 a, q4 b) {
   float d = rmin(fabsf(qmul(a, qconj(b)).w), 1.0f);
   return d >= __uint_as_float(RP_SHAKE_COS_BITS);
 }
-// solve_d6 for locked and limited axes (compliance 0: alpha = 0; no drives, no rotors). lam: the
-// joint's six XPBD multipliers of this step (t0 t1 t2 r0 r1 r2). sa / sb: the step's start poses.
-__device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, const BodiesV& B, f3 sa_p, q4 sa_q,
-                                             f3 sb_p, q4 sb_q) {
+// alpha_dt2 (bodies.rs:438-441)
+__device__ __forceinline__ float alpha_dt2_dev(float c, float dt2) {
+  c = rmax(fin0(c), 0.0f);
+  return c <= 0.0f ? 0.0f : fin0(c / dt2);
+}
+// The error axis ax acts on at coordinate coord (bodies.rs:674-698, 786-810): locked at 0, a limit
+// only while violated, a position drive's target clamped into the limit; a velocity drive leaves
+// an unlimited axis free at position level. False: nothing to correct.
+__device__ __forceinline__ bool row_error_dev(const JointGpu& j, int ax, float coord, float* c) {
+  bool has = true;
+  *c = fin0(coord - 0.0f);
+  const bool lim = jaxis_lim(j.flags, ax);
+  if (lim) {
+    float lo = fin0(j.lo[ax]), hi = fin0(j.hi[ax]);
+    if (coord < lo) *c = fin0(coord - lo);
+    else if (coord > hi) *c = fin0(coord - hi);
+    else has = false;
+  }
+  if (jaxis_drive(j.flags, ax)) {
+    if (!jaxis_vel(j.flags, ax)) {
+      float target = fin0(j.dtarget[ax]);
+      if (lim) target = clampf(target, fin0(j.lo[ax]), fin0(j.hi[ax]));
+      *c = fin0(coord - target);
+      has = true;
+    } else if (!lim) {
+      has = false;
+    }
+  }
+  return has;
+}
+// The measure of rotational axis i at joint-frame rotations ra, rb (bodies.rs:796-803).
+__device__ __forceinline__ float row_angle_dev(int hinge, q4 ra, q4 rb, int i, f3 u) {
+  q4 q = qmul(qconj(ra), rb);
+  if (q.w < 0.0f) q = qneg(q);
+  f3 v = mk3(q.x, q.y, q.z);
+  if (hinge == i) return fin0(2.0f * atan2_rp(comp3(v, i), q.w));
+  if (hinge >= 0)
+    return fin0(dot(fin_v(cross(normalize_fin(qrot(ra, unit_axis(hinge))), normalize_fin(qrot(rb, unit_axis(hinge))))), u));
+  return fin0(dot(fin_v(qrot(ra, fin_v(v * 2.0f))), u));
+}
+
+// solve_d6 (bodies.rs:616-873) without the rotor rows (no armature). lam: the joint's six XPBD
+// multipliers of this step (t0 t1 t2 r0 r1 r2). sa / sb: the step's start poses, for SHAKE's
+// directions (when neither body turned too far) and for a damped compliant axis's change since the
+// start (Kelvin-Voigt: spring and damper in one implicit row).
+__device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, const BodiesV& B, float dt, f3 sa_p,
+                                             q4 sa_q, f3 sb_p, q4 sb_q) {
   const uint32_t A = j.a, Bb = j.b;
   const float wa = fin0(B.inv_mass[A]), wb = fin0(B.inv_mass[Bb]);
+  const float dt2 = rmax(dt * dt, 1.0e-12f);
   const bool shake = turned_below_max(sa_q, asq(B.rot[A])) && turned_below_max(sb_q, asq(B.rot[Bb]));
   f3 ax0[3] = {mk3(0, 0, 0), mk3(0, 0, 0), mk3(0, 0, 0)}, la0 = mk3(0, 0, 0), lb0 = mk3(0, 0, 0);
   m3 ia0 = mzero(), ib0 = mzero();
@@ -137,9 +234,9 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
     ia0 = world_inertia(sa_q, ld_m3(B.inv_I, A));
     ib0 = world_inertia(sb_q, ld_m3(B.inv_I, Bb));
   }
-  const float alpha = 0.0f, bias_vel = 0.0f, dt_unused = 0.0f;
+  const float bias_vel = 0.0f;
   for (int i = 0; i < 3; ++i) {
-    if (!((j.flags >> i) & 1u)) continue;
+    if (!jaxis_on(j.flags, i)) continue;
     f3 pap = xyz(B.pos[A]), pbp = xyz(B.pos[Bb]);
     q4 paq = asq(B.rot[A]), pbq = asq(B.rot[Bb]);
     f3 u = normalize_fin(qrot(qmul(paq, fa_q), unit_axis(i)));
@@ -154,22 +251,27 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
       iaw = inv_inertia_world_dev(B, A, paq); ibw = inv_inertia_world_dev(B, Bb, pbq);
     }
     float coord = fin0(dot(d, u));
-    float c = fin0(coord - 0.0f);
-    if ((j.flags >> (JF_LIMIT_SHIFT + i)) & 1u) {
-      float lo = fin0(j.lo[i]), hi = fin0(j.hi[i]);
-      if (coord < lo) c = fin0(coord - lo);
-      else if (coord > hi) c = fin0(coord - hi);
-      else continue;
-    }
+    float c;
+    if (!row_error_dev(j, i, coord, &c)) continue;
     f3 ra_u = fin_v(cross(lever_a, un)), rb_u = fin_v(cross(lever_b, un));
     float w_rot_a = fin0(dot(ra_u, mvec(iaw, ra_u)));
     float w_rot_b = fin0(dot(rb_u, mvec(ibw, rb_u)));
     float ws = fin0(((wa + wb) + w_rot_a) + w_rot_b);
+    float alpha = alpha_dt2_dev(j.comp[i], dt2);
     float denom = fin0(ws + alpha);
     if (denom <= 0.0f) continue;
-    c = fin0(c + fin0(bias_vel * dt_unused));
+    c = fin0(c + fin0(bias_vel * dt));
     float lambda_old = fin0(lam[i]);
-    float dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    float dl;
+    if (position_damped_dev(j, i)) {
+      f3 u0 = normalize_fin(qrot(qmul(sa_q, fa_q), unit_axis(i)));
+      f3 d0 = fin_v((sb_p + qrot(sb_q, fb_p)) - (sa_p + qrot(sa_q, fa_p)));
+      float gamma = fin0(j.comp[i] * j.damp[i] / dt);
+      float dc = fin0(coord - dot(d0, u0));
+      dl = fin0(-((c + fin0(alpha * lambda_old)) + fin0(gamma * dc)) / fin0((1.0f + gamma) * ws + alpha));
+    } else {
+      dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    }
     lam[i] = fin0(lambda_old + dl);
     apply_position_delta_dev(B, A, fin_v((-un) * fin0(dl * wa)));
     apply_position_delta_dev(B, Bb, fin_v(un * fin0(dl * wb)));
@@ -178,37 +280,37 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
   }
   const int hinge = joint_hinge(j.flags);
   for (int i = 0; i < 3; ++i) {
-    if (!((j.flags >> (3 + i)) & 1u)) continue;
+    const int ax = 3 + i;
+    if (!jaxis_on(j.flags, ax)) continue;
     q4 paq = asq(B.rot[A]), pbq = asq(B.rot[Bb]);
     q4 ra = qmul(paq, fa_q), rb = qmul(pbq, fb_q);
     f3 u = normalize_fin(qrot(ra, unit_axis(i)));
     if (vzero(u)) continue;
-    q4 q = qmul(qconj(ra), rb);
-    if (q.w < 0.0f) q = qneg(q);
-    f3 v = mk3(q.x, q.y, q.z);
-    float angle;
-    if (hinge == i) angle = fin0(2.0f * atan2_rp(comp3(v, i), q.w));
-    else if (hinge >= 0)
-      angle = fin0(dot(fin_v(cross(normalize_fin(qrot(ra, unit_axis(hinge))), normalize_fin(qrot(rb, unit_axis(hinge))))), u));
-    else angle = fin0(dot(fin_v(qrot(ra, fin_v(v * 2.0f))), u));
+    float angle = row_angle_dev(hinge, ra, rb, i, u);
     f3 un;
     m3 iaw, ibw;
     if (shake) { un = ax0[i]; iaw = ia0; ibw = ib0; }
     else { un = u; iaw = inv_inertia_world_dev(B, A, paq); ibw = inv_inertia_world_dev(B, Bb, pbq); }
-    float c = fin0(angle - 0.0f);
-    if ((j.flags >> (JF_LIMIT_SHIFT + 3 + i)) & 1u) {
-      float lo = fin0(j.lo[3 + i]), hi = fin0(j.hi[3 + i]);
-      if (angle < lo) c = fin0(angle - lo);
-      else if (angle > hi) c = fin0(angle - hi);
-      else continue;
-    }
+    float c;
+    if (!row_error_dev(j, ax, angle, &c)) continue;
     float ws = fin0(dot(un, mvec(iaw, un)) + dot(un, mvec(ibw, un)));
+    float alpha = alpha_dt2_dev(j.comp[ax], dt2);
     float denom = fin0(ws + alpha);
     if (denom <= 0.0f) continue;
-    c = fin0(c + fin0(bias_vel * dt_unused));
-    float lambda_old = fin0(lam[3 + i]);
-    float dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
-    lam[3 + i] = fin0(lambda_old + dl);
+    c = fin0(c + fin0(bias_vel * dt));
+    float lambda_old = fin0(lam[ax]);
+    float dl;
+    if (position_damped_dev(j, ax)) {
+      q4 ra0 = qmul(sa_q, fa_q), rb0 = qmul(sb_q, fb_q);
+      f3 u0 = normalize_fin(qrot(ra0, unit_axis(i)));
+      float angle0 = row_angle_dev(hinge, ra0, rb0, i, u0);
+      float gamma = fin0(j.comp[ax] * j.damp[ax] / dt);
+      float dc = fin0(angle - angle0);
+      dl = fin0(-((c + fin0(alpha * lambda_old)) + fin0(gamma * dc)) / fin0((1.0f + gamma) * ws + alpha));
+    } else {
+      dl = fin0(-(c + fin0(alpha * lambda_old)) / denom);
+    }
+    lam[ax] = fin0(lambda_old + dl);
     apply_orientation_delta_dev(B, A, fin_v((-mvec(iaw, un)) * dl));
     apply_orientation_delta_dev(B, Bb, fin_v(mvec(ibw, un) * dl));
   }

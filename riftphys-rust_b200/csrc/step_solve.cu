@@ -235,6 +235,11 @@ __device__ __forceinline__ float pgs_row(const BodiesV& B, const Row& r, uint32_
   return res;
 }
 
+// The unclamped joint impulse (solver.rs:821-830): a rigid row drives v to the target, a damper row
+// (gamma = 1 / (damping dt) > 0) drives v + gamma lam to it.
+__device__ __forceinline__ float joint_lam(float old, float target, float v, float gamma, float m_eff) {
+  return gamma == 0.0f ? old + (target - v) * m_eff : old + ((target - v) - gamma * old) * m_eff;
+}
 // A joint velocity row on the global body arrays (the warp kernel of the largest islands).
 __device__ __forceinline__ void joint_apply_glob(const BodiesV& B, const Row& r, float lam) {
   f3 p = r.n * lam;
@@ -262,7 +267,7 @@ __device__ __forceinline__ float joint_row_glob(const BodiesV& B, const Row& r, 
   }
   float v = dot(vb - va, r.n);
   float old = acc_jn[k];
-  float nw = clampf(old + (r.bias - v) * r.m_n, r.mu_s, r.mu_k);
+  float nw = clampf(joint_lam(old, r.bias, v, r.t1.z, r.m_n), r.mu_s, r.mu_k);
   acc_jn[k] = nw;
   if (nw != old) joint_apply_glob(B, r, nw - old);
   return fabsf(nw - old) / r.m_n;
@@ -844,7 +849,7 @@ __global__ void __launch_bounds__(128) k_pos_iterations(uint32_t n_listed, const
               const JointGpu jt = J[j];
               bool fa = !B.dyn[jt.a] || !B.awake[jt.a], fb = !B.dyn[jt.b] || !B.awake[jt.b];
               if (!(fa && fb))
-                solve_d6_dev(jt, jlam + 6 * (size_t)j, B, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]),
+                solve_d6_dev(jt, jlam + 6 * (size_t)j, B, dt, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]),
                              asq(srot[jt.b]));
             }
             continue;
@@ -913,11 +918,14 @@ __global__ void k_stage6(uint32_t nb, BodiesV B, const float4* __restrict__ orig
       if (qfin(nr)) B.rot[i] = f4q(fin_q(nr));
     }
     q4 pr = asq(pred_rot[i]);
-    if (!qeq(nr, pr)) {
+    // a body of a joint with a rotational velocity drive keeps the angular velocity the motor rows
+    // gave it (step.rs:352-366, the motor overwrite): jointed bit 1
+    const bool driven = jointed && (jointed[i] & 2u);
+    if (!driven && !qeq(nr, pr)) {
       q4 dq = qmul(nr, qconj(pr));
       f3 d_ang = mk3(dq.x, dq.y, dq.z) * 2.0f;
       if (dq.w < 0.0f) d_ang = -d_ang;
-      va = va + (d_ang - sa) / dt;  // no velocity drives: no body is motor-driven
+      va = va + (d_ang - sa) / dt;
     }
     if (vfin(vl)) L = f4(fin_v(vl), L.w);
     if (vfin(va)) A = f4(fin_v(va), A.w);
@@ -1234,7 +1242,7 @@ __device__ __noinline__ void joint_row_core(float4* lin, float4* ang, const SRow
   else { va = ha ? la + cross(aa, r.ra) : r.vfix; vb = hb ? lb + cross(ab, r.rb) : r.vfix; }
   float v = dot(vb - va, r.n);
   float old = acc;
-  float nw = clampf(old + (r.bias - v) * r.m_n, r.mu_s, r.mu_k);
+  float nw = clampf(joint_lam(old, r.bias, v, r.t1.z, r.m_n), r.mu_s, r.mu_k);
   acc = nw;
   if (nw != old) {
     joint_apply_reg(la, aa, lb, ab, r, qa, qb, ima, imb, nw - old);
@@ -1267,7 +1275,7 @@ __device__ __noinline__ void joint_unit_core(float4* lin, float4* ang, const SRo
     else { va = ha ? la + cross(aa, r.ra) : r.vfix; vb = hb ? lb + cross(ab, r.rb) : r.vfix; }
     float v = dot(vb - va, r.n);
     float old = jn[q];
-    float nw = clampf(old + (r.bias - v) * r.m_n, r.mu_s, r.mu_k);
+    float nw = clampf(joint_lam(old, r.bias, v, r.t1.z, r.m_n), r.mu_s, r.mu_k);
     jn[q] = nw;
     if (nw != old) {
       joint_apply_reg(la, aa, lb, ab, r, qa, qb, ima, imb, nw - old);

@@ -588,10 +588,10 @@ SnapshotGpu* WorldGpu::snapshot_create() {  // lib.rs:1707-1752 + carried_state 
   cp(s->wb.p, warm_b.p, 16 * (size_t)n_warm);
   upload_joints();
   s->nj = num_joints();
-  s->jw_n.ensure(s->nj + 1); s->jw_tag.ensure(12 * (size_t)s->nj + 12); s->jw_lam.ensure(12 * (size_t)s->nj + 12);
+  s->jw_n.ensure(s->nj + 1); s->jw_tag.ensure(kJointRows * (size_t)s->nj + kJointRows); s->jw_lam.ensure(kJointRows * (size_t)s->nj + kJointRows);
   cp(s->jw_n.p, jw_n.p, 4 * (size_t)s->nj);
-  cp(s->jw_tag.p, jw_tag.p, 12 * (size_t)s->nj);
-  cp(s->jw_lam.p, jw_lam.p, 48 * (size_t)s->nj);
+  cp(s->jw_tag.p, jw_tag.p, kJointRows * (size_t)s->nj);
+  cp(s->jw_lam.p, jw_lam.p, 4 * kJointRows * (size_t)s->nj);
   RP_CUDA(cudaStreamSynchronize(stream_));
   return s;
 }
@@ -622,8 +622,8 @@ void WorldGpu::restore_joint_warm(const SnapshotGpu* s) {
   uint32_t nj = num_joints(), n = s->nj < nj ? s->nj : nj;
   if (n) {
     RP_CUDA(cudaMemcpyAsync(jw_n.p, s->jw_n.p, 4 * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
-    RP_CUDA(cudaMemcpyAsync(jw_tag.p, s->jw_tag.p, 12 * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
-    RP_CUDA(cudaMemcpyAsync(jw_lam.p, s->jw_lam.p, 48 * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
+    RP_CUDA(cudaMemcpyAsync(jw_tag.p, s->jw_tag.p, kJointRows * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
+    RP_CUDA(cudaMemcpyAsync(jw_lam.p, s->jw_lam.p, 4 * kJointRows * (size_t)n, cudaMemcpyDeviceToDevice, stream_));
   }
   if (nj > n) RP_CUDA(cudaMemsetAsync(jw_n.p + n, 0xFF, 4 * (size_t)(nj - n), stream_));
 }

@@ -23,6 +23,8 @@ namespace rp {
 
 class WarmModel;
 struct JointGpu;
+// Most velocity rows one D6 joint has: 6 axes x (damper, friction, motor, two limit rows), rounded up.
+constexpr uint32_t kJointRows = 32;
 
 struct StepStatsHost {
   uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
@@ -111,12 +113,19 @@ class WorldGpu {
     float fa[7], fb[7];            // frame in body A / B: pos xyz, quat xyzw
     bool en[6], lim[6];            // t0 t1 t2 r0 r1 r2
     float lo[6], hi[6];
+    float comp[6], damp[6], fric[6];  // XPBD compliance, damping, Coulomb friction
+    bool drive[6], vel[6];         // driven; the drive a velocity motor
+    float dtarget[6], dkp[6], dkd[6], dmax[6];
     int hinge;                     // stored hinge axis (add_hinge), -1 none
   };
   uint32_t num_joints() const { return (uint32_t)h_joints_.size(); }
   uint32_t world_of(uint32_t body) const;
   uint32_t add_joint(uint32_t kind, uint32_t a, uint32_t b, const float fa[7], const float fb[7], uint32_t axis);
   void set_joint_limit(uint32_t j, bool angular, uint32_t axis, bool on, float lo, float hi);
+  void set_joint_axis(uint32_t j, bool angular, uint32_t axis, bool enabled, float compliance);
+  void set_joint_drive(uint32_t j, bool angular, uint32_t axis, bool on, float target, float kp, float kd,
+                       float max_impulse, bool vel_mode);
+  void set_joint_damping(uint32_t j, bool angular, uint32_t axis, float damping, float friction);
   void upload_joints();            // the joint records, jointed bodies and jointed pairs, on change
   std::vector<JointHost> h_joints_;
   bool joints_dirty_ = false;

@@ -306,9 +306,32 @@ def ragdoll_arrays(rp, n, seed, area, base_id=1, y0=None, hf=None):
     return bd, jd, ld
 
 
-def ragdolls(rp, w, n_ragdolls=100, hf_n=128, seed=5, iterations=(24, 24), flat_area=None):
+def ragdoll_muscles(w, jd, j0):
+    """Drives, springs, dampers and friction on the joints of a ragdoll_arrays() joint array added
+    from joint id j0: each ball joint's twist a damped spring (compliance 0.05, damping 0.4; XPBD's
+    Kelvin-Voigt row) and its swing axes damped (0.3) with friction (0.05); elbows held by a position
+    drive at -0.5 rad, knees turned by a velocity motor (0.3 rad/s, at most 0.5 N m s a tick), ankles
+    damped with friction."""
+    u = jd.view(np.uint32)
+    for k in range(len(jd)):
+        j, kind, axis = j0 + k, int(u[k, 0]), int(u[k, 1])
+        if kind == 0:
+            w.set_joint_axis(j, True, 0, True, 0.05)
+            w.set_joint_damping(j, True, 0, 0.4, 0.0)
+            w.set_joint_damping(j, True, 1, 0.3, 0.05)
+            w.set_joint_damping(j, True, 2, 0.3, 0.05)
+        elif axis == 2:
+            w.set_joint_drive(j, True, 2, -0.5, max_impulse=1000.0)
+        elif k % 14 in (9, 12):  # shins (the joint of bone k + 1)
+            w.set_joint_drive(j, True, 0, 0.3, max_impulse=0.5, velocity=True)
+        else:
+            w.set_joint_damping(j, True, 0, 0.2, 0.02)
+
+
+def ragdolls(rp, w, n_ragdolls=100, hf_n=128, seed=5, iterations=(24, 24), flat_area=None, muscles=False):
     """Builds the ragdoll scene into World ``w``; returns (dt, body count, joint count). With
-    flat_area, the ragdolls fall in a square of that side onto a static ground box instead."""
+    flat_area, the ragdolls fall in a square of that side onto a static ground box instead; with
+    muscles, ragdoll_muscles() sets drives, springs and dampers on the joints."""
     w.set_pair_props(0, 0, 0.6, 0.5, 0.0, 0.08)
     w.set_pair_props(0, 4, 0.883176, 0.724569, 0.0, 0.1)
     w.set_iterations(*iterations)
@@ -328,4 +351,6 @@ def ragdolls(rp, w, n_ragdolls=100, hf_n=128, seed=5, iterations=(24, 24), flat_
     if j0:
         ld[:, 0].view(np.uint32)[:] += j0
     w.set_joint_limit_array(ld)
+    if muscles:
+        ragdoll_muscles(w, jd, j0)
     return 1.0 / 120.0, w.num_bodies(), len(jd)

@@ -1,9 +1,12 @@
 """Joint acceptance cases over any library exporting the C ABI (the CPU oracle in
 tests/test_oracle_joints.py, the CUDA library in tests/test_gpu_joints.py). Restated from the
-reference's riftphys-world/tests/joint_energy_test.rs:46-219 (SHAKE energy behaviour, limits,
-replay) and hinge_angle_test.rs:14-58 (hinge limits in radians), with the same bodies, rates and
-tolerances; the pin bodies carry a small collider here (the FFI gives every body one), which never
-touches the jointed rods."""
+reference's riftphys-world/tests: joint_energy_test.rs:46-219 (SHAKE energy behaviour, limits,
+replay), hinge_angle_test.rs:14-58 (hinge limits in radians), joint_damping_test.rs (viscous damping
+and Coulomb friction rows), compliant_joint_test.rs:20-75, 134-170 (torsional springs and sprung
+hinges), joint_conditioning_test.rs:22-66 (position drive, SHAKE projection) and
+world_robotics_test.rs:75-135 (velocity motor), with the same bodies, rates and tolerances; the pin
+bodies carry a small collider here (the FFI gives every body one), which never touches the jointed
+rods (jointed pairs make no contacts)."""
 import math
 
 import numpy as np
@@ -19,9 +22,11 @@ def _world(lib, cap=8):
     return w
 
 
-def _body(w, pos, he, density, dynamic=True, rot=(0.0, 0.0, 0.0, 1.0), lin=(0.0, 0.0, 0.0), ang=(0.0, 0.0, 0.0)):
+def _body(w, pos, he, density, dynamic=True, rot=(0.0, 0.0, 0.0, 1.0), lin=(0.0, 0.0, 0.0), ang=(0.0, 0.0, 0.0),
+          sleep=True):
     d = rp.desc_array(np.array([pos]), np.array([rot]), np.array([he]), rp.SHAPE_BOX, np.array([density]),
-                      np.array([1 if dynamic else 0], dtype=np.uint32), lin=np.array([lin]), ang=np.array([ang]))
+                      np.array([1 if dynamic else 0], dtype=np.uint32), sleep_allowed=1 if sleep else 0,
+                      lin=np.array([lin]), ang=np.array([ang]))
     return w.add_bodies_array(d)
 
 
@@ -236,4 +241,296 @@ def case_joint_api_errors(lib):
             raise AssertionError(f"accepted limit {args}")
     w.set_joint_limit(0, True, 1, -0.5, 0.5)
     w.set_joint_limit(0, True, 1)  # cleared
+    w.close()
+
+
+# ---- viscous damping and Coulomb friction on a hinge (joint_damping_test.rs)
+BAR = (0.5, 0.1, 0.1)
+BAR_MASS = 2.0
+BAR_I = BAR_MASS / 3.0 * (BAR[0] ** 2 + BAR[1] ** 2)  # about z
+
+
+def _spinner(lib, w0):
+    """joint_damping_test.rs:17-25: a 2 kg bar hinged about z through its centre to a static anchor,
+    spinning at w0 about z, no gravity, never asleep."""
+    w = lib.world(4, 4)
+    w.set_gravity((0.0, 0.0, 0.0))
+    p = _body(w, (0.0, 0.0, 0.0), PIN, 1.0, dynamic=False)
+    b = _body(w, (0.0, 0.0, 0.0), BAR, BAR_MASS / (8.0 * BAR[0] * BAR[1] * BAR[2]), ang=(0.0, 0.0, w0), sleep=False)
+    j = _hinge(w, p, b, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    return w, b, j
+
+
+class _Unwrap:
+    """Twist about z, unwrapped step to step (joint_damping_test.rs:28-41)."""
+
+    def __init__(self):
+        self.last = self.total = 0.0
+
+    def update(self, q):
+        a = 2.0 * math.atan2(q[2], q[3])
+        d = a - self.last
+        while d > math.pi:
+            d -= 2.0 * math.pi
+        while d < -math.pi:
+            d += 2.0 * math.pi
+        self.last = a
+        self.total += d
+        return self.total
+
+
+def case_damped_hinge_decays_at_the_closed_form_rate(lib):
+    """joint_damping_test.rs:43-66: the implicit damper's decay rate ln(1 + c dt / I) / dt within 0.5%,
+    c / I within 2%; the bar stays on its axis."""
+    for hz in (60.0, 240.0):
+        for rate in (0.5, 2.0):
+            w, b, j = _spinner(lib, 3.0)
+            w.set_joint_damping(j, True, 2, rate * BAR_I, 0.0)
+            t = 2.0
+            for _ in range(int(t * hz)):
+                w.step(1.0 / hz)
+            lin, ang = w.velocity(b)
+            measured = math.log(3.0 / ang[2]) / t
+            discrete = math.log(1.0 + rate / hz) * hz
+            assert abs(measured - discrete) < 0.005 * discrete, f"{hz} Hz, c/I {rate}: rate {measured:.4f}, discrete {discrete:.4f}"
+            assert abs(measured - rate) < 0.02 * rate, f"{hz} Hz, c/I {rate}: rate {measured:.4f}"
+            assert abs(ang[0]) < 1e-4 and abs(ang[1]) < 1e-4 and np.linalg.norm(lin) < 1e-4, f"off-axis motion {lin} {ang}"
+            w.close()
+
+
+def case_friction_only_with_zero_damping_is_finite(lib):
+    """joint_damping_test.rs:68-80: friction without damping is finite; NaN / negative coefficients
+    become 0 and act on nothing."""
+    w, b, j = _spinner(lib, 3.0)
+    w.set_joint_damping(j, True, 2, 0.0, 0.2)
+    for _ in range(60):
+        w.step(1.0 / 60.0)
+    wz = w.velocity(b)[1][2]
+    assert math.isfinite(wz) and wz < 3.0, f"w {wz}"
+    w.set_joint_damping(j, True, 2, float("nan"), -1.0)
+    before = w.velocity(b)[1][2]
+    w.step(1.0 / 60.0)
+    assert abs(w.velocity(b)[1][2] - before) < 1e-5, "a NaN / negative coefficient acted"
+    w.close()
+
+
+def case_friction_hinge_stops_at_the_closed_form_angle(lib):
+    """joint_damping_test.rs:82-99: Coulomb friction tau stops the bar after I w0^2 / (2 tau) (2%) and
+    holds it at rest."""
+    w0, tau = 3.0, 0.2
+    want = BAR_I * w0 * w0 / (2.0 * tau)
+    t_stop = BAR_I * w0 / tau
+    for hz in (60.0, 240.0):
+        w, b, j = _spinner(lib, w0)
+        w.set_joint_damping(j, True, 2, 0.0, tau)
+        u = _Unwrap()
+        angle = 0.0
+        for _ in range(int((t_stop + 2.0) * hz)):
+            w.step(1.0 / hz)
+            angle = u.update(w.pose(b)[1])
+        assert abs(angle - want) < 0.02 * want, f"{hz} Hz: stopped after {angle:.4f} rad, want {want:.4f}"
+        assert abs(w.velocity(b)[1][2]) < 1e-4, f"{hz} Hz: still turning"
+        w.close()
+
+
+def case_very_stiff_damping_is_stable(lib):
+    """joint_damping_test.rs:101-118: c dt / I far above 1 never reverses the spin."""
+    for hz in (60.0, 240.0):
+        w, b, j = _spinner(lib, 3.0)
+        w.set_joint_damping(j, True, 2, 1.0e4 * BAR_I, 0.0)
+        last = 3.0
+        for _ in range(int(hz)):
+            w.step(1.0 / hz)
+            wz = w.velocity(b)[1][2]
+            assert math.isfinite(wz) and wz >= -1e-6 and wz <= last + 1e-6, f"{hz} Hz: w went {last} -> {wz}"
+            last = wz
+        assert last < 1e-3, f"{hz} Hz: w still {last}"
+        w.close()
+
+
+def case_damping_on_a_limited_hinge_still_stops_at_the_limit(lib):
+    """joint_damping_test.rs:120-131: damping and a limit on one axis: the limit rows still hold."""
+    w, b, j = _spinner(lib, 3.0)
+    w.set_joint_damping(j, True, 2, 0.05, 0.0)
+    w.set_joint_limit(j, True, 2, -0.5, 0.5)
+    u = _Unwrap()
+    furthest = 0.0
+    for _ in range(480):
+        w.step(1.0 / 240.0)
+        furthest = max(furthest, u.update(w.pose(b)[1]))
+    assert furthest < 0.5 + 0.02, f"passed the limit: {furthest:.4f} rad"
+    w.close()
+
+
+# ---- compliant axes (compliant_joint_test.rs)
+def _quat_z(a):
+    return (0.0, 0.0, math.sin(0.5 * a), math.cos(0.5 * a))
+
+
+def _rotate(q, v):
+    return _rotm(q) @ np.asarray(v, dtype=np.float64)
+
+
+def _torsion_spring(lib, c, hz, secs):
+    """compliant_joint_test.rs:23-53: a 1 m, 2.5 kg rod held out by a torsional spring about z
+    (compliance c, rad per N m) on a D6 joint with every other axis rigid, started at its static sag;
+    returns the worst departure from the sag, relative to it."""
+    w = _world(lib, 4)
+    p = _body(w, (0.0, 10.0, 0.0), PIN, 1.0, dynamic=False)
+    m = 8.0 * ROD[0] * ROD[1] * ROD[2] * 1000.0
+    theta = 0.0
+    for _ in range(200):
+        theta = np.float32(0.5 * theta + 0.5 * c * m * G * 0.5 * math.cos(theta))
+    theta = float(theta)
+    q = _quat_z(-theta)
+    rod = _body(w, tuple(np.array([0.0, 10.0, 0.0]) + _rotate(q, (0.5, 0.0, 0.0))), ROD, 1000.0, rot=q, sleep=False)
+    j = w.add_joints([(rp.JOINT_D6, p, rod, ID, ((-0.5, 0.0, 0.0), (0, 0, 0, 1)), 0)])
+    w.set_joint_axis(j, True, 2, True, c)
+    worst = 0.0
+    for _ in range(int(secs * hz)):
+        w.step(1.0 / hz)
+        x, y, z, qw = w.pose(rod)[1]
+        s2 = 1.0 - qw * qw
+        if s2 >= 1e-8:
+            ang, az = 2.0 * math.acos(max(-1.0, min(1.0, qw))), z / math.sqrt(s2)
+        else:
+            ang, az = 0.0, 0.0
+        sag = -ang * math.copysign(1.0, az)
+        worst = max(worst, abs(sag - theta) / theta)
+    w.close()
+    return worst
+
+
+def case_torsional_spring_holds_its_static_sag(lib):
+    """compliant_joint_test.rs:55-61: within 3% of the static sag over 10 s (60 and 240 Hz)."""
+    for hz in (60.0, 240.0):
+        worst = _torsion_spring(lib, 0.008, hz, 10.0)
+        assert worst < 0.03, f"{hz} Hz: sag departed {100 * worst:.2f}% from static"
+
+
+def case_torsional_spring_large_sag_is_in_radians(lib):
+    """compliant_joint_test.rs:63-75: a soft spring sagging about 1 rad acts on the angle itself
+    (0.25% at 60 Hz, 0.5% at 240 Hz)."""
+    for hz, gate in ((60.0, 0.0025), (240.0, 0.005)):
+        worst = _torsion_spring(lib, 0.15, hz, 10.0)
+        assert worst < gate, f"{hz} Hz: sag departed {100 * worst:.3f}% from static"
+
+
+def _sprung_hinge_past_90(lib, align_c, hz):
+    """compliant_joint_test.rs:134-160: a 1 m rod hinged at its end about z by a spring (c = 0.15),
+    started 2.5 rad round and spinning 0.3 rad/s about x, no gravity; the x and y rows at compliance
+    align_c and no stored hinge axis. Returns (worst hinge-axis tilt in degrees, worst anchor gap)."""
+    w = lib.world(4, 4)
+    w.set_gravity((0.0, 0.0, 0.0))
+    p = _body(w, (0.0, 10.0, 0.0), PIN, 1.0, dynamic=False)
+    q = _quat_z(2.5)
+    rod = _body(w, tuple(np.array([0.0, 10.0, 0.0]) + _rotate(q, (0.5, 0.0, 0.0))), ROD, 1000.0, rot=q,
+                ang=(0.3, 0.0, 0.0), sleep=False)
+    j = w.add_joints([(rp.JOINT_D6, p, rod, ID, ((-0.5, 0.0, 0.0), (0, 0, 0, 1)), 0)])
+    w.set_joint_axis(j, True, 0, True, align_c)
+    w.set_joint_axis(j, True, 1, True, align_c)
+    w.set_joint_axis(j, True, 2, True, 0.15)
+    tilt = gap = 0.0
+    for _ in range(int(10.0 * hz)):
+        w.step(1.0 / hz)
+        pos, qq = w.pose(rod)
+        z = _rotate(qq, (0.0, 0.0, 1.0))
+        tilt = max(tilt, math.degrees(math.acos(max(-1.0, min(1.0, z[2])))))
+        gap = max(gap, float(np.linalg.norm(np.array(pos) + _rotate(qq, (-0.5, 0.0, 0.0)) - np.array([0.0, 10.0, 0.0]))))
+    w.close()
+    return tilt, gap
+
+
+def case_sprung_hinge_stays_aligned_past_90_degrees(lib):
+    """compliant_joint_test.rs:162-172: alignment rows rigid, 1e-9 and 1e-3, the hinge recognised from
+    its rows: tilt < 1 degree, gap < 1 mm."""
+    for align_c in (0.0, 1.0e-9, 1.0e-3):
+        for hz in (60.0, 240.0):
+            tilt, gap = _sprung_hinge_past_90(lib, align_c, hz)
+            assert tilt < 1.0 and gap < 0.001, f"c {align_c:g}, {hz} Hz: tilt {tilt:.2f} deg, gap {gap:.4f} m"
+
+
+# ---- drives
+def _hinge_angle_z(q):
+    x, y, z, qw = q
+    if qw < 0.0:
+        z, qw = -z, -qw
+    return 2.0 * math.atan2(z, qw)
+
+
+def case_hinge_position_drive_reaches_its_target(lib):
+    """joint_conditioning_test.rs:22-66 (the SHAKE projection): a 1 m, 2.5 kg rod hinged at its end
+    about z with a rigid position drive to 1 rad holds it within 0.1 degree after 0.1 s, joint apart
+    < 1 mm, at 60 / 240 Hz, with and without gravity, 20 and 21 position iterations."""
+    target = math.degrees(1.0)
+    for hz in (60.0, 240.0):
+        for gravity in (0.0, G):
+            for pos_iters in (20, 21):
+                w = lib.world(4, 4)
+                w.set_iterations(20, pos_iters)
+                w.set_gravity((0.0, -gravity, 0.0))
+                p = _body(w, (0.0, 10.0, 0.0), PIN, 1.0, dynamic=False)
+                r = _body(w, (0.5, 10.0, 0.0), ROD, 1000.0)
+                j = _hinge(w, p, r, (0.0, 0.0, 0.0), (-0.5, 0.0, 0.0))
+                w.set_joint_drive(j, True, 2, 1.0, kp=0.0, kd=0.0, max_impulse=1000.0, velocity=False)
+                worst = gap = 0.0
+                for k in range(int(hz)):
+                    w.step(1.0 / hz)
+                    if k / hz >= 0.1:
+                        pos, q = w.pose(r)
+                        worst = max(worst, abs(math.degrees(_hinge_angle_z(q)) - target))
+                        gap = max(gap, float(np.linalg.norm(np.array(pos) + _rotate(q, (-0.5, 0.0, 0.0)) - np.array([0.0, 10.0, 0.0]))))
+                assert worst < 0.1, f"{hz} Hz g {gravity} iters {pos_iters}: off target by {worst:.3f} deg"
+                assert gap < 0.001, f"{hz} Hz g {gravity} iters {pos_iters}: joint apart by {gap:.4f} m"
+                w.close()
+
+
+def case_hinge_velocity_motor_turns_the_leg(lib):
+    """world_robotics_test.rs:75-135: a 0.2 x 1 x 0.2 m leg hanging from a hinge about x, driven by a
+    velocity motor at 2 rad/s (max impulse 1000): after 30 ticks of 16 ms it turns at > 1.5 rad/s and
+    has swung to z < -0.7, y > 9.3."""
+    w = _world(lib, 32)
+    p = _body(w, (0.0, 10.0, 0.0), PIN, 1.0, dynamic=False)
+    leg = _body(w, (0.0, 9.0, 0.0), (0.1, 0.5, 0.1), 50.0)
+    j = w.add_joints([(rp.JOINT_HINGE, p, leg, ID, ((0.0, 1.0, 0.0), (0, 0, 0, 1)), 0)])
+    w.set_joint_drive(j, True, 0, 2.0, kp=0.0, kd=5.0, max_impulse=1000.0, velocity=True)
+    for _ in range(30):
+        w.step(0.016)
+    pos, _ = w.pose(leg)
+    ang = w.velocity(leg)[1]
+    assert ang[0] > 1.5, f"motor at {ang[0]:.3f} rad/s"
+    assert pos[2] < -0.7 and pos[1] > 9.3, f"leg at {pos}"
+    w.close()
+
+
+def case_d6_api_errors(lib):
+    """Argument checks of the D6 axis, drive and damping entry points."""
+    w = lib.world(4, 4)
+    a = _body(w, (0.0, 1.0, 0.0), (0.5, 0.5, 0.5), 1000.0)
+    b = _body(w, (2.0, 1.0, 0.0), (0.5, 0.5, 0.5), 1000.0)
+    j = w.add_joints([(rp.JOINT_D6, a, b, ID, ID, 0)])
+    calls = [
+        lambda: w.set_joint_axis(5, True, 0, True, 0.0),
+        lambda: w.set_joint_axis(j, True, 3, True, 0.0),
+        lambda: w.set_joint_axis(j, True, 0, True, -1.0),
+        lambda: w.set_joint_axis(j, True, 0, True, float("nan")),
+        lambda: w.set_joint_drive(j, True, 3, 1.0),
+        lambda: w.set_joint_drive(5, False, 0, 1.0),
+        lambda: w.set_joint_drive(j, True, 0, float("inf")),
+        lambda: w.set_joint_drive(j, True, 0, 1.0, max_impulse=float("nan")),
+        lambda: w.set_joint_damping(j, True, 3, 1.0, 0.0),
+        lambda: w.set_joint_damping(9, True, 0, 1.0, 0.0),
+    ]
+    for k, call in enumerate(calls):
+        try:
+            call()
+        except rp.RPhysError:
+            pass
+        else:
+            raise AssertionError(f"call {k} accepted")
+    w.set_joint_axis(j, False, 1, False, 0.0)
+    w.set_joint_drive(j, True, 0, 0.5, max_impulse=10.0, velocity=True)
+    w.set_joint_drive(j, True, 0)  # cleared
+    w.set_joint_damping(j, True, 1, 2.0, 0.5)
+    w.step(1.0 / 60.0)
     w.close()

@@ -38,6 +38,58 @@ def _chain(rp_, w, n=6, hz=62.5):
     return 1.0 / hz, n + 1
 
 
+def _d6_chain(rp_, w, hz=120.0):
+    """A pinned chain of six rods, one D6 feature per joint: a damped torsional spring (XPBD
+    Kelvin-Voigt row), a velocity motor, a translational spring with viscous damping, a limited
+    position drive, a ball joint with damping and friction on every axis, a limited axis with a
+    velocity drive; boxes dropped onto the chain add contacts on jointed bodies."""
+    w.set_gravity((0.0, -9.81, 0.0))
+    n = 6
+    pos = [(0.0, 6.0, 0.0)] + [(0.5 + 1.0 * k, 6.0, 0.0) for k in range(n)]
+    he = [(0.01, 0.01, 0.01)] + [(0.5, 0.06, 0.06)] * n
+    d = rp_.desc_array(np.array(pos), np.tile([0.0, 0.0, 0.0, 1.0], (n + 1, 1)), np.array(he), rp_.SHAPE_BOX,
+                       np.array([1.0] + [600.0] * n), np.array([0] + [1] * n, dtype=np.uint32), sleep_allowed=0)
+    first = w.add_bodies_array(d)
+    kinds = [rp_.JOINT_D6, rp_.JOINT_HINGE, rp_.JOINT_D6, rp_.JOINT_HINGE, rp_.JOINT_BALL, rp_.JOINT_D6]
+    joints = []
+    for k in range(n):
+        fa = ((0.0, 0.0, 0.0), (0, 0, 0, 1)) if k == 0 else ((0.5, 0.0, 0.0), (0, 0, 0, 1))
+        joints.append((kinds[k], first + k, first + k + 1, fa, ((-0.5, 0.0, 0.0), (0, 0, 0, 1)), 2))
+    j = w.add_joints(joints)
+    w.set_joint_axis(j, True, 2, True, 0.02)
+    w.set_joint_damping(j, True, 2, 0.5, 0.0)
+    w.set_joint_drive(j + 1, True, 2, 1.5, max_impulse=40.0, velocity=True)
+    w.set_joint_damping(j + 1, True, 0, 0.2, 0.1)
+    w.set_joint_axis(j + 2, False, 0, True, 2.0e-4)
+    w.set_joint_damping(j + 2, False, 0, 3.0, 0.0)
+    w.set_joint_damping(j + 2, True, 1, 0.0, 0.3)
+    w.set_joint_limit(j + 3, True, 2, -1.0, 0.6)
+    w.set_joint_drive(j + 3, True, 2, 0.4, max_impulse=1000.0)
+    for ax in range(3):
+        w.set_joint_damping(j + 4, True, ax, 0.25, 0.05)
+    w.set_joint_limit(j + 5, True, 1, -0.3, 0.3)
+    w.set_joint_drive(j + 5, True, 1, -0.8, max_impulse=5.0, velocity=True)
+    w.set_joint_axis(j + 5, True, 0, False)
+    g = rp_.desc_array(np.array([[3.0, -0.5, 0.0]]), np.array([[0.0, 0.0, 0.0, 1.0]]), np.array([[20.0, 0.5, 20.0]]),
+                       rp_.SHAPE_BOX, np.array([0.0]), np.array([0], dtype=np.uint32))
+    w.add_bodies_array(g)
+    rng = np.random.default_rng(9)
+    m = 10
+    bp = np.column_stack([rng.uniform(0.5, 6.0, m), rng.uniform(8.0, 11.0, m), rng.uniform(-0.3, 0.3, m)])
+    bd = rp_.desc_array(bp, np.tile([0.0, 0.0, 0.0, 1.0], (m, 1)), np.full((m, 3), 0.2), rp_.SHAPE_BOX,
+                        np.full(m, 500.0), np.ones(m, dtype=np.uint32))
+    w.add_bodies_array(bd)
+    return 1.0 / hz, w.num_bodies()
+
+
+def test_d6_feature_chain(oracle, gpu):
+    run_pair(oracle, gpu, {"cap": (32, 32), "fn": lambda rp_, w: _d6_chain(rp_, w)}, 600)
+
+
+def test_d6_feature_chain_60hz(oracle, gpu):
+    run_pair(oracle, gpu, {"cap": (32, 32), "fn": lambda rp_, w: _d6_chain(rp_, w, 60.0)}, 300)
+
+
 def _ragdolls(n, **kw):
     def build(rp_, w):
         dt, nb, _ = scenes.ragdolls(rp_, w, n_ragdolls=n, **kw)
@@ -52,6 +104,11 @@ def test_pendulum_chain(oracle, gpu):
 
 def test_ragdolls_on_terrain(oracle, gpu):
     build = {"cap": (1024, 1024), "fn": _ragdolls(10)}
+    run_pair(oracle, gpu, build, 240, check_every=4)
+
+
+def test_ragdolls_with_muscles_on_terrain(oracle, gpu):
+    build = {"cap": (1024, 1024), "fn": _ragdolls(10, muscles=True)}
     run_pair(oracle, gpu, build, 240, check_every=4)
 
 
