@@ -50,7 +50,7 @@ __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, Bodie
                               const float* __restrict__ jw_lam, float* acc_jn, float2* acc_jt, uint32_t* uf) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nj) return;
-  const JointGpu jt = J[j];
+  const JointGpu& jt = J[j];
   const uint32_t r0 = base + off[j], wn = jw_n[j];
   bool tags_match = true, dyn_a = false, dyn_b = false;
   uint32_t n = d6_rows_dev(jt, B, dt, [&](const JRowD& r, uint32_t k) {
@@ -287,6 +287,7 @@ void WorldGpu::upload_joints() {
       g.comp[k] = s.comp[k]; g.damp[k] = s.damp[k]; g.fric[k] = s.fric[k];
       g.dtarget[k] = s.dtarget[k]; g.dmax[k] = s.dmax[k];
       if (k >= 3 && s.drive[k] && s.vel[k]) rdrive = true;
+      if (s.drive[k] || s.comp[k] > 0.0f) f |= JF_FULL;
     }
     f |= (uint32_t)(hinge_of(s) + 1) << JF_HINGE_SHIFT;
     g.flags = f;

@@ -24,6 +24,7 @@ static_assert(sizeof(JointGpu) == 256, "JointGpu layout");
 #define JF_HINGE_SHIFT 12u
 #define JF_DRIVE_SHIFT 16u
 #define JF_VEL_SHIFT 22u
+#define JF_FULL (1u << 28)  // some axis compliant or driven: the position solve takes the full path
 #define JMAX_ROWS kJointRows
 
 __host__ __device__ inline int joint_hinge(uint32_t flags) { return (int)((flags >> JF_HINGE_SHIFT) & 7u) - 1; }
@@ -201,6 +202,17 @@ __device__ __forceinline__ bool row_error_dev(const JointGpu& j, int ax, float c
   }
   return has;
 }
+// row_error for an axis with no drive: 0 when locked, the violation when limited (false: inside).
+__device__ __forceinline__ bool limit_error_dev(const JointGpu& j, int ax, float coord, float* c) {
+  *c = fin0(coord - 0.0f);
+  if (jaxis_lim(j.flags, ax)) {
+    float lo = fin0(j.lo[ax]), hi = fin0(j.hi[ax]);
+    if (coord < lo) *c = fin0(coord - lo);
+    else if (coord > hi) *c = fin0(coord - hi);
+    else return false;
+  }
+  return true;
+}
 // The measure of rotational axis i at joint-frame rotations ra, rb (bodies.rs:796-803).
 __device__ __forceinline__ float row_angle_dev(int hinge, q4 ra, q4 rb, int i, f3 u) {
   q4 q = qmul(qconj(ra), rb);
@@ -215,20 +227,25 @@ __device__ __forceinline__ float row_angle_dev(int hinge, q4 ra, q4 rb, int i, f
 // solve_d6 (bodies.rs:616-873) without the rotor rows (no armature). lam: the joint's six XPBD
 // multipliers of this step (t0 t1 t2 r0 r1 r2). sa / sb: the step's start poses, for SHAKE's
 // directions (when neither body turned too far) and for a damped compliant axis's change since the
-// start (Kelvin-Voigt: spring and damper in one implicit row).
+// start (Kelvin-Voigt: spring and damper in one implicit row). kFull = false is the same solve for a
+// joint with no compliant and no driven axis (JF_FULL clear): every alpha is 0, no axis is
+// position-damped and row_error is the limit test alone -- the same operations, without the loads
+// and branches of the other cases (a shorter dependent chain in the position pass).
+template <bool kFull>
 __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, const BodiesV& B, float dt, f3 sa_p,
                                              q4 sa_q, f3 sb_p, q4 sb_q) {
   const uint32_t A = j.a, Bb = j.b;
   const float wa = fin0(B.inv_mass[A]), wb = fin0(B.inv_mass[Bb]);
-  const float dt2 = rmax(dt * dt, 1.0e-12f);
+  const float dt2 = kFull ? rmax(dt * dt, 1.0e-12f) : 0.0f;
   const bool shake = turned_below_max(sa_q, asq(B.rot[A])) && turned_below_max(sb_q, asq(B.rot[Bb]));
-  f3 ax0[3] = {mk3(0, 0, 0), mk3(0, 0, 0), mk3(0, 0, 0)}, la0 = mk3(0, 0, 0), lb0 = mk3(0, 0, 0);
+  // SHAKE's directions: axis i of the start frame, normalize_fin(qrot(r0, e_i)), made where used
+  f3 la0 = mk3(0, 0, 0), lb0 = mk3(0, 0, 0);
   m3 ia0 = mzero(), ib0 = mzero();
-  q4 fa_q = asq(j.fa_q), fb_q = asq(j.fb_q);
-  f3 fa_p = xyz(j.fa_p), fb_p = xyz(j.fb_p);
+  const uint32_t flags = j.flags;
+  const q4 fa_q = asq(j.fa_q), fb_q = asq(j.fb_q);
+  const f3 fa_p = xyz(j.fa_p), fb_p = xyz(j.fb_p);
+  const q4 r0 = qmul(sa_q, fa_q);
   if (shake) {
-    q4 r0 = qmul(sa_q, fa_q);
-    for (int i = 0; i < 3; ++i) ax0[i] = normalize_fin(qrot(r0, unit_axis(i)));
     la0 = fin_v(qrot(sa_q, fa_p));
     lb0 = fin_v(qrot(sb_q, fb_p));
     ia0 = world_inertia(sa_q, ld_m3(B.inv_I, A));
@@ -236,7 +253,7 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
   }
   const float bias_vel = 0.0f;
   for (int i = 0; i < 3; ++i) {
-    if (!jaxis_on(j.flags, i)) continue;
+    if (!jaxis_on(flags, i)) continue;
     f3 pap = xyz(B.pos[A]), pbp = xyz(B.pos[Bb]);
     q4 paq = asq(B.rot[A]), pbq = asq(B.rot[Bb]);
     f3 u = normalize_fin(qrot(qmul(paq, fa_q), unit_axis(i)));
@@ -245,25 +262,27 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
     f3 d = fin_v(xb - xa);
     f3 un, lever_a, lever_b;
     m3 iaw, ibw;
-    if (shake) { un = ax0[i]; lever_a = la0; lever_b = lb0; iaw = ia0; ibw = ib0; }
+    if (shake) { un = normalize_fin(qrot(r0, unit_axis(i))); lever_a = la0; lever_b = lb0; iaw = ia0; ibw = ib0; }
     else {
       un = u; lever_a = xa - pap; lever_b = xb - pbp;
       iaw = inv_inertia_world_dev(B, A, paq); ibw = inv_inertia_world_dev(B, Bb, pbq);
     }
     float coord = fin0(dot(d, u));
     float c;
-    if (!row_error_dev(j, i, coord, &c)) continue;
+    if (kFull) {
+      if (!row_error_dev(j, i, coord, &c)) continue;
+    } else if (!limit_error_dev(j, i, coord, &c)) continue;
     f3 ra_u = fin_v(cross(lever_a, un)), rb_u = fin_v(cross(lever_b, un));
     float w_rot_a = fin0(dot(ra_u, mvec(iaw, ra_u)));
     float w_rot_b = fin0(dot(rb_u, mvec(ibw, rb_u)));
     float ws = fin0(((wa + wb) + w_rot_a) + w_rot_b);
-    float alpha = alpha_dt2_dev(j.comp[i], dt2);
+    float alpha = kFull ? alpha_dt2_dev(j.comp[i], dt2) : 0.0f;
     float denom = fin0(ws + alpha);
     if (denom <= 0.0f) continue;
     c = fin0(c + fin0(bias_vel * dt));
     float lambda_old = fin0(lam[i]);
     float dl;
-    if (position_damped_dev(j, i)) {
+    if (kFull && position_damped_dev(j, i)) {
       f3 u0 = normalize_fin(qrot(qmul(sa_q, fa_q), unit_axis(i)));
       f3 d0 = fin_v((sb_p + qrot(sb_q, fb_p)) - (sa_p + qrot(sa_q, fa_p)));
       float gamma = fin0(j.comp[i] * j.damp[i] / dt);
@@ -278,10 +297,10 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
     apply_orientation_delta_dev(B, A, fin_v((-mvec(iaw, ra_u)) * dl));
     apply_orientation_delta_dev(B, Bb, fin_v(mvec(ibw, rb_u) * dl));
   }
-  const int hinge = joint_hinge(j.flags);
+  const int hinge = joint_hinge(flags);
   for (int i = 0; i < 3; ++i) {
     const int ax = 3 + i;
-    if (!jaxis_on(j.flags, ax)) continue;
+    if (!jaxis_on(flags, ax)) continue;
     q4 paq = asq(B.rot[A]), pbq = asq(B.rot[Bb]);
     q4 ra = qmul(paq, fa_q), rb = qmul(pbq, fb_q);
     f3 u = normalize_fin(qrot(ra, unit_axis(i)));
@@ -289,18 +308,20 @@ __device__ __forceinline__ void solve_d6_dev(const JointGpu& j, float* lam, cons
     float angle = row_angle_dev(hinge, ra, rb, i, u);
     f3 un;
     m3 iaw, ibw;
-    if (shake) { un = ax0[i]; iaw = ia0; ibw = ib0; }
+    if (shake) { un = normalize_fin(qrot(r0, unit_axis(i))); iaw = ia0; ibw = ib0; }
     else { un = u; iaw = inv_inertia_world_dev(B, A, paq); ibw = inv_inertia_world_dev(B, Bb, pbq); }
     float c;
-    if (!row_error_dev(j, ax, angle, &c)) continue;
+    if (kFull) {
+      if (!row_error_dev(j, ax, angle, &c)) continue;
+    } else if (!limit_error_dev(j, ax, angle, &c)) continue;
     float ws = fin0(dot(un, mvec(iaw, un)) + dot(un, mvec(ibw, un)));
-    float alpha = alpha_dt2_dev(j.comp[ax], dt2);
+    float alpha = kFull ? alpha_dt2_dev(j.comp[ax], dt2) : 0.0f;
     float denom = fin0(ws + alpha);
     if (denom <= 0.0f) continue;
     c = fin0(c + fin0(bias_vel * dt));
     float lambda_old = fin0(lam[ax]);
     float dl;
-    if (position_damped_dev(j, ax)) {
+    if (kFull && position_damped_dev(j, ax)) {
       q4 ra0 = qmul(sa_q, fa_q), rb0 = qmul(sb_q, fb_q);
       f3 u0 = normalize_fin(qrot(ra0, unit_axis(i)));
       float angle0 = row_angle_dev(hinge, ra0, rb0, i, u0);
@@ -333,5 +354,13 @@ void joints_row_roots(WorldGpu& W, const RowsV& R, uint32_t base, uint32_t njr, 
 void joints_store_warm(WorldGpu& W, const RowsV& R, uint32_t base, const float* acc_jn, cudaStream_t st);
 // Bodies in joints count as constrained (step.rs:160-170).
 void joints_mark_constrained(WorldGpu& W, uint8_t* constrained, cudaStream_t st);
+
+// The position solve of joint j: the full path for joints with a compliant or driven axis, the
+// locked-and-limited one for the rest.
+__device__ __forceinline__ void solve_d6_any(const JointGpu& j, float* lam, const BodiesV& B, float dt, f3 sa_p, q4 sa_q,
+                                             f3 sb_p, q4 sb_q) {
+  if (j.flags & JF_FULL) solve_d6_dev<true>(j, lam, B, dt, sa_p, sa_q, sb_p, sb_q);
+  else solve_d6_dev<false>(j, lam, B, dt, sa_p, sa_q, sb_p, sb_q);
+}
 
 }  // namespace rp

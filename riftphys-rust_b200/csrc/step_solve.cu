@@ -846,10 +846,10 @@ __global__ void __launch_bounds__(128) k_pos_iterations(uint32_t n_listed, const
           if (k >= nc) {
             if (joints_on && (R.flags[k] & RF_JFIRST)) {
               uint32_t j = __float_as_uint(R.la[k].x);
-              const JointGpu jt = J[j];
+              const JointGpu& jt = J[j];
               bool fa = !B.dyn[jt.a] || !B.awake[jt.a], fb = !B.dyn[jt.b] || !B.awake[jt.b];
               if (!(fa && fb))
-                solve_d6_dev(jt, jlam + 6 * (size_t)j, B, dt, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]),
+                solve_d6_any(jt, jlam + 6 * (size_t)j, B, dt, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]),
                              asq(srot[jt.b]));
             }
             continue;
