@@ -4,10 +4,11 @@
 //
 // The reference does its math through glam 0.27 (Vec3 / Mat3A / Quat, `libm` feature;
 // Cargo.lock:998-1000, Cargo.toml:37), a crate that is not vendored under the reference tree.
-// What is restated here is glam's published scalar formulas, in plain f32 with no FMA
-// contraction (build flag -ffp-contract=off): the operation order below is the order the
-// oracle and the CUDA kernels share, so the two agree bit for bit. Whether glam's SSE2 paths
-// round the same way is not pinned (no golden vector of the reference pins it).
+// What is restated here is glam's formulas, in plain f32 with no FMA contraction (build flag
+// -ffp-contract=off): Vec3 / Mat3 scalar, Quat in the lane order of its SSE2 paths (below). The
+// operation order is the one the oracle and the CUDA kernels share, so the two agree bit for bit,
+// and with these forms the oracle reproduces the reference's own golden bits for its
+// distance-joint scenes (distance_bits_test.rs:50-57).
 //
 // Transcendentals (sin, cos, exp) are the project's own: Cody-Waite argument reduction with
 // split constants derived from pi/2 and ln 2 to 80 digits, then Taylor polynomials evaluated
@@ -70,18 +71,26 @@ static inline V3 clamp_length_max(V3 a, float m) {
 }
 
 // ---- quaternions (x, y, z, w) ----
+// glam's Quat is an SSE2 type on x86_64, where the reference runs, so its product and norm follow
+// the lane order of glam's SSE2 paths (Quat::mul_quat after rtm's quat_mul, dot4, Vec4::normalize):
+// the Hamilton product lane-wise as (w0 b + x0 b1) + (y0 b2 + z0 b3), b1..b3 the signed lane
+// permutations of b; the 4-lane dot as (xx + zz) + (yy + ww); normalize as a division by the
+// length. These forms reproduce the reference's golden bits of distance_bits_test.rs:50-57
+// (tests/test_oracle_golden.py); the scalar forms do not.
 static inline Q4 qmul(Q4 a, Q4 b) {
-  return Q4{
-      ((a.w * b.x + a.x * b.w) + a.y * b.z) - a.z * b.y,
-      ((a.w * b.y - a.x * b.z) + a.y * b.w) + a.z * b.x,
-      ((a.w * b.z + a.x * b.y) - a.y * b.x) + a.z * b.w,
-      ((a.w * b.w - a.x * b.x) - a.y * b.y) - a.z * b.z};
+  return Q4{(a.w * b.x + a.x * b.w) + (a.y * b.z - a.z * b.y),
+            (a.w * b.y - a.x * b.z) + (a.y * b.w + a.z * b.x),
+            (a.w * b.z + a.x * b.y) + (-(a.y * b.x) + a.z * b.w),
+            (a.w * b.w - a.x * b.x) + (-(a.y * b.y) - a.z * b.z)};
 }
 static inline Q4 qconj(Q4 q) { return Q4{-q.x, -q.y, -q.z, q.w}; }
 static inline Q4 qneg(Q4 q) { return Q4{-q.x, -q.y, -q.z, -q.w}; }
-static inline float qdot(Q4 a, Q4 b) { return ((a.x * b.x + a.y * b.y) + a.z * b.z) + a.w * b.w; }
+static inline float qdot(Q4 a, Q4 b) { return (a.x * b.x + a.z * b.z) + (a.y * b.y + a.w * b.w); }
 static inline Q4 qscale(Q4 q, float s) { return Q4{q.x * s, q.y * s, q.z * s, q.w * s}; }
-static inline Q4 qnormalize(Q4 q) { float r = 1.0f / std::sqrt(qdot(q, q)); return qscale(q, r); }
+static inline Q4 qnormalize(Q4 q) {
+  float l = std::sqrt(qdot(q, q));
+  return Q4{q.x / l, q.y / l, q.z / l, q.w / l};
+}
 static inline bool qeq(Q4 a, Q4 b) { return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w; }
 // Quat * Vec3: v (w^2 - b.b) + b (2 v.b) + (b x v)(2 w)
 static inline V3 qrot(Q4 q, V3 v) {

@@ -565,6 +565,43 @@ uint32_t rphys_oracle_turned_threshold_mismatches(uint32_t dstar_bits) {
     if ((2.0f * om::acosf_unit_rp(d) < 0.5f) != (d >= dstar)) bad++;
   return bad;
 }
+// Test hook: the distance-joint scenes of the reference's golden bit test
+// (riftphys-world/tests/distance_bits_test.rs:11-48), built on the oracle World directly (no
+// colliders, as World::add_body makes none): a 0.2 x 0.1 x 0.16 m box of density 500 swinging on a
+// distance joint from a static pivot at (0, 5, 0), kind 0 rigid at its start length, kind 1 a
+// spring (compliance 2e-3 m/N) at 0.8 of it; 3 s at hz. Returns the FNV-1a fold of the box's
+// pose and velocity bits, the reference test's bits().
+uint64_t rphys_oracle_distance_bits(uint32_t kind, float hz) {
+  using namespace om;
+  orc::World w(8);
+  w.gravity = V3{0.0f, -9.81f, 0.0f};
+  uint32_t pivot = w.add_body(Iso{V3{0.0f, 5.0f, 0.0f}, Q4{0, 0, 0, 1}}, V3{0, 0, 0}, V3{0, 0, 0}, 0.0f, V3{0, 0, 0}, false);
+  const float he[3] = {0.1f, 0.05f, 0.08f};
+  float im;
+  V3 inertia;
+  orc::mass_from_density(orc::SH_BOX, he, 500.0f, &im, &inertia);
+  float sy, cy, sx, cx;
+  sincosf_rp(0.3f * 0.5f, &sy, &cy);  // Quat::from_rotation_y(0.3)
+  sincosf_rp(0.2f * 0.5f, &sx, &cx);  // Quat::from_rotation_x(0.2)
+  Q4 rot = qmul(Q4{0.0f, sy, 0.0f, cy}, Q4{sx, 0.0f, 0.0f, cx});
+  V3 start{0.7f, 4.3f, 0.2f};
+  uint32_t b = w.add_body(Iso{start, rot}, V3{0.0f, 0.5f, 1.5f}, V3{0.4f, -1.0f, 2.0f}, im, inertia, true);
+  w.sleep_allowed[b] = 0;
+  float rest = len(sub(start, V3{0.0f, 5.0f, 0.0f}));
+  if (kind == 0) w.add_distance_joint(pivot, b, rest, 0.0f);
+  else w.add_distance_joint(pivot, b, rest * 0.8f, 2.0e-3f);
+  const uint32_t n = (uint32_t)(3.0f * hz);
+  for (uint32_t t = 0; t < n; ++t) w.step(1.0f / hz);
+  uint64_t h = 0xcbf29ce484222325ull;
+  const float x[13] = {w.pos[b].x, w.pos[b].y, w.pos[b].z, w.rot[b].x, w.rot[b].y, w.rot[b].z, w.rot[b].w,
+                       w.lin[b].x, w.lin[b].y, w.lin[b].z, w.ang[b].x, w.ang[b].y, w.ang[b].z};
+  for (float f : x) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    h = (h ^ (uint64_t)u) * 0x100000001b3ull;
+  }
+  return h;
+}
 RPhysResult rphys_ext_set_joint_axis(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, uint32_t enabled,
                                      float compliance) {
   clear_err();

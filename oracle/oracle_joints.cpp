@@ -13,6 +13,13 @@ using namespace om;
 
 static const V3 kUnit[3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
 static const float kShakeMaxTurn = 0.5f;  // SHAKE_MAX_TURN (bodies.rs:477)
+// SHAKE_MAX_TURN.cos() (bodies.rs:520), through the project's cosine
+static float shake_max_turn_cos() {
+  float s, c;
+  om::sincosf_rp(kShakeMaxTurn, &s, &c);
+  return c;
+}
+static const float kShakeMaxTurnCos = shake_max_turn_cos();
 
 static inline float comp(V3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
 // normalize_fin (bodies.rs:19-27)
@@ -87,6 +94,28 @@ void World::set_d6_damping(uint32_t id, bool angular, uint32_t axis, float dampi
   D6Axis& x = angular ? joints[id].r[axis] : joints[id].t[axis];
   x.damping = rmax(fin0(damping), 0.0f);
   x.friction = rmax(fin0(friction), 0.0f);
+}
+
+// Joints::add_distance_joint (bodies.rs:273-285): rest and compliance sanitised (fin; compliance >= 0)
+uint32_t World::add_distance_joint(uint32_t a, uint32_t b, float rest, float compliance) {
+  Joint j;
+  j.a = a; j.b = b; j.kind = 1;
+  j.rest = fin0(rest);
+  j.compliance = rmax(fin0(compliance), 0.0f);
+  joints.push_back(j);
+  return (uint32_t)joints.size() - 1;
+}
+// Joints::add_distance_joint_at (bodies.rs:290-297)
+uint32_t World::add_distance_joint_at(uint32_t a, V3 la, uint32_t b, V3 lb, float rest, float compliance) {
+  uint32_t id = add_distance_joint(a, b, rest, compliance);
+  joints[id].la = fin_v(la);
+  joints[id].lb = fin_v(lb);
+  return id;
+}
+// Joints::set_distance_damping (bodies.rs:301-305)
+void World::set_distance_damping(uint32_t id, float damping) {
+  if (id >= joints.size() || joints[id].kind != 1) return;
+  joints[id].damping = rmax(fin0(damping), 0.0f);
 }
 
 bool position_damped(const D6Axis& a) {
@@ -188,6 +217,46 @@ void d6_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vect
   }
 }
 
+// distance_rows (solver.rs:309-330): an anchored rigid rod's equality row along the current
+// anchors' direction (a compliant rod has none: its damping is in its position row).
+static void distance_rows(const World& w, const Joint& j, uint32_t joint, std::vector<JRow>& out) {
+  const uint32_t a = j.a, b = j.b;
+  float wa = w.inv_mass[a], wb = w.inv_mass[b];
+  if (wa == 0.0f && wb == 0.0f) return;
+  V3 ra = qrot(w.rot[a], j.la), rb = qrot(w.rot[b], j.lb);
+  V3 d = sub(add(w.pos[b], rb), add(w.pos[a], ra));
+  float len = om::len(d);
+  if (!(len > 1e-6f)) return;
+  V3 u = divs(d, len);
+  M3 ia = w.inv_inertia_world(a), ib = w.inv_inertia_world(b);
+  V3 ca = cross(ra, u), cb = cross(rb, u);
+  float k = ((wa + wb) + dot(ca, mvec(ia, ca))) + dot(cb, mvec(ib, cb));
+  if (!(k > 1e-9f)) return;
+  if (j.compliance <= 0.0f) out.push_back(JRow{a, b, joint, false, u, ra, rb, wa, wb, 1.0f / k, 0.0f, -INFINITY, INFINITY, 0});
+}
+// The original distance row (solver.rs:793-817), made once per tick: positions do not move
+// during the velocity solve, so its direction and bias are the same at every sweep.
+static void legacy_distance_row(const World& w, const Joint& j, uint32_t joint, float dt, std::vector<JRow>& out) {
+  if (j.compliance > 0.0f) return;  // a spring acts at position level only
+  V3 dir = sub(w.pos[j.b], w.pos[j.a]);
+  float len = om::len(dir);
+  if (len < 1e-6f) return;
+  V3 n = divs(dir, len);
+  float inv_a = w.inv_mass[j.a], inv_b = w.inv_mass[j.b];
+  float inv_sum = inv_a + inv_b;
+  if (inv_sum < 1e-9f) return;
+  JRow r{j.a, j.b, joint, false, n, V3{0, 0, 0}, V3{0, 0, 0}, inv_a, inv_b, 1.0f / inv_sum, 0.0f, -INFINITY, INFINITY, 0};
+  r.legacy = true;
+  r.bias = (len - j.rest) * (0.1f / dt);
+  r.inv_sum = inv_sum;
+  out.push_back(r);
+}
+void joint_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vector<JRow>& out) {
+  if (j.kind == 0) d6_rows(w, j, joint, dt, out);
+  else if (j.anchored()) distance_rows(w, j, joint, out);
+  else legacy_distance_row(w, j, joint, dt, out);
+}
+
 float joint_row_vel(const World& w, const JRow& r) {
   if (r.angular) return dot(sub(w.ang[r.b], w.ang[r.a]), r.u);
   V3 vb = add(w.lin[r.b], cross(w.ang[r.b], r.rb));
@@ -205,6 +274,13 @@ void joint_row_apply(World& w, const JRow& r, float lam) {
   }
 }
 float joint_row_update(World& w, const JRow& r, float& acc) {
+  if (r.legacy) {
+    float v_rel = dot(sub(w.lin[r.b], w.lin[r.a]), r.u);
+    float j_mag = -(v_rel + r.bias) / r.inv_sum;
+    w.apply_impulse(r.a, mul(neg(r.u), j_mag));
+    w.apply_impulse(r.b, mul(r.u, j_mag));
+    return j_mag;
+  }
   float v = joint_row_vel(w, r);
   float old = acc;
   // rigid rows: v -> target; soft rows (dampers): v + gamma lam -> target
@@ -384,6 +460,93 @@ static void solve_d6(World& w, Joint& j, float dt, const Iso* sa, const Iso* sb)
   }
 }
 
+// solve_distance_row (bodies.rs:501-548): the original COM-to-COM rod, corrected along the
+// start-of-step direction when it is within SHAKE_MAX_TURN of the current one.
+static void solve_distance_row(World& w, Joint& j, float dt2, const Iso* sa, const Iso* sb) {
+  const uint32_t ia = j.a, ib = j.b;
+  float wa = w.inv_mass[ia], wb = w.inv_mass[ib];
+  float w_sum = fin0(wa + wb);
+  if (w_sum <= 0.0f) return;
+  V3 d = sub(w.pos[ib], w.pos[ia]);
+  float len2 = dot(d, d);
+  if (!fin(len2) || len2 <= 1.0e-20f) return;
+  float len = std::sqrt(len2);
+  if (len <= 1.0e-6f) return;
+  V3 n_cur = normalize_fin(divs(d, len));
+  if (vzero(n_cur)) return;
+  V3 n = n_cur;
+  if (sa && sb) {
+    V3 n0 = normalize_fin(sub(sb->pos, sa->pos));
+    if (!vzero(n0) && dot(n0, n_cur) > kShakeMaxTurnCos) n = n0;
+  }
+  float c_val = fin0(len - fin0(j.rest));
+  float alpha = j.compliance <= 0.0f ? 0.0f : fin0(rmax(fin0(j.compliance), 0.0f) / dt2);
+  float denom = fin0(w_sum + alpha);
+  if (denom <= 0.0f) return;
+  float lambda_old = fin0(j.lambda_acc);
+  float lambda = fin0(-(c_val + fin0(alpha * lambda_old)) / (denom * dot(n, n_cur)));
+  if (std::fabs(lambda) <= 1.0e-9f) return;
+  j.lambda_acc = fin0(lambda_old + lambda);
+  apply_position_delta(w, ia, fin_v(mul(neg(n), fin0(lambda * wa))));
+  apply_position_delta(w, ib, fin_v(mul(n, fin0(lambda * wb))));
+}
+// solve_distance_anchored (bodies.rs:557-614): C = |x_b - x_a| - rest on the current anchors,
+// along the start-of-step direction with start-of-step lever arms and inertias over the mixed
+// Jacobian product (current-iterate directions when a body turned too far or the mixed product
+// falls below half the start-of-step one); a damped compliant rod's spring and damper in one
+// implicit Kelvin-Voigt row.
+static void solve_distance_anchored(World& w, Joint& j, float dt, float dt2, const Iso* sa, const Iso* sb) {
+  const uint32_t ia = j.a, ib = j.b;
+  float wa = fin0(w.inv_mass[ia]), wb = fin0(w.inv_mass[ib]);
+  if (wa + wb <= 0.0f) return;
+  Iso pa{w.pos[ia], w.rot[ia]}, pb{w.pos[ib], w.rot[ib]};
+  V3 ra = fin_v(qrot(pa.rot, j.la)), rb = fin_v(qrot(pb.rot, j.lb));
+  V3 d = fin_v(sub(add(pb.pos, rb), add(pa.pos, ra)));
+  float len = om::len(d);
+  if (!fin(len) || len <= 1.0e-6f) return;
+  V3 n_cur = normalize_fin(divs(d, len));
+  if (vzero(n_cur)) return;
+  float c_val = fin0(len - fin0(j.rest));
+  float alpha = j.compliance <= 0.0f ? 0.0f : fin0(rmax(fin0(j.compliance), 0.0f) / dt2);
+  V3 n, ga, gb;
+  float wgen;
+  bool shake = false;
+  if (sa && sb && !(turned(sa->rot, pa.rot) >= kShakeMaxTurn) && !(turned(sb->rot, pb.rot) >= kShakeMaxTurn)) {
+    V3 ra0 = qrot(sa->rot, j.la), rb0 = qrot(sb->rot, j.lb);
+    V3 n0 = normalize_fin(sub(add(sb->pos, rb0), add(sa->pos, ra0)));
+    if (!vzero(n0)) {
+      M3 ia0 = inv_inertia_at(w, ia, sa->rot), ib0 = inv_inertia_at(w, ib, sb->rot);
+      V3 ga0 = mvec(ia0, cross(ra0, n0)), gb0 = mvec(ib0, cross(rb0, n0));
+      float w_sym = ((wa + wb) + dot(cross(ra0, n0), ga0)) + dot(cross(rb0, n0), gb0);
+      float w_mix = (((wa + wb) * dot(n_cur, n0)) + dot(cross(ra, n_cur), ga0)) + dot(cross(rb, n_cur), gb0);
+      if (fin(w_mix) && w_mix >= 0.5f * w_sym) { shake = true; n = n0; ga = ga0; gb = gb0; wgen = w_mix; }
+    }
+  }
+  if (!shake) {
+    M3 iaw = w.inv_inertia_world(ia), ibw = w.inv_inertia_world(ib);
+    V3 ca = cross(ra, n_cur), cb = cross(rb, n_cur);
+    wgen = ((wa + wb) + dot(ca, mvec(iaw, ca))) + dot(cb, mvec(ibw, cb));
+    n = n_cur; ga = mvec(iaw, ca); gb = mvec(ibw, cb);
+  }
+  float denom = fin0(wgen + alpha);
+  if (!(denom > 0.0f)) return;
+  float lambda_old = fin0(j.lambda_acc);
+  float dl;
+  if (j.compliance > 0.0f && j.damping > 0.0f && sa && sb) {
+    float len0 = om::len(sub(add(sb->pos, qrot(sb->rot, j.lb)), add(sa->pos, qrot(sa->rot, j.la))));
+    float gamma = fin0(j.compliance * j.damping / dt);
+    dl = fin0(-((c_val + fin0(alpha * lambda_old)) + fin0(gamma * fin0(len - len0))) / fin0((1.0f + gamma) * wgen + alpha));
+  } else {
+    dl = fin0(-(c_val + fin0(alpha * lambda_old)) / denom);
+  }
+  if (std::fabs(dl) <= 1.0e-12f) return;
+  j.lambda_acc = fin0(lambda_old + dl);
+  apply_position_delta(w, ia, fin_v(mul(neg(n), fin0(dl * wa))));
+  apply_position_delta(w, ib, fin_v(mul(n, fin0(dl * wb))));
+  apply_orientation_delta(w, ia, fin_v(mul(neg(ga), dl)));
+  apply_orientation_delta(w, ib, fin_v(mul(gb, dl)));
+}
+
 void solve_joints_pass(World& w, float dt, const std::vector<Iso>& start, const std::vector<uint8_t>& frozen) {
   dt = fin0(dt);
   if (!(dt > 0.0f)) return;
@@ -394,7 +557,9 @@ void solve_joints_pass(World& w, float dt, const std::vector<Iso>& start, const 
     const Iso* sa = j.a < start.size() ? &start[j.a] : nullptr;
     const Iso* sb = j.b < start.size() ? &start[j.b] : nullptr;
     Iso ca{w.pos[j.a], w.rot[j.a]}, cb{w.pos[j.b], w.rot[j.b]};
-    solve_d6(w, j, dt, sa ? sa : &ca, sb ? sb : &cb);
+    if (j.kind == 0) solve_d6(w, j, dt, sa ? sa : &ca, sb ? sb : &cb);
+    else if (j.anchored()) solve_distance_anchored(w, j, dt, rmax(dt * dt, 1.0e-12f), sa ? sa : &ca, sb ? sb : &cb);
+    else solve_distance_row(w, j, rmax(dt * dt, 1.0e-12f), sa ? sa : &ca, sb ? sb : &cb);
   }
 }
 

@@ -18,6 +18,10 @@ struct JRow {
   uint8_t tag;
   float gamma = 0.0f;
   uint8_t idx = 0, cnt = 0;  // index in its joint's rows; the joint's row count (on its first row)
+  // the original distance row (solver.rs:793-817): impulse -(v_rel + bias) / inv_sum along u on
+  // the linear velocities, bias = (len - rest) 0.1 / dt, no accumulation and no clamp
+  bool legacy = false;
+  float bias = 0.0f, inv_sum = 0.0f;
 };
 
 // d6_hinge_axis (bodies.rs:891-901) at the restated feature set: -1 for none.
@@ -26,6 +30,9 @@ int d6_hinge_axis(const Joint& j);
 float d6_row_angle(const Joint& j, Q4 rot_a, Q4 rot_b, int i);
 // d6_rows (solver.rs:336-424): the joint's velocity rows, appended to out.
 void d6_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vector<JRow>& out);
+// A joint's velocity rows whatever its kind (solver.rs:655-661): d6_rows, distance_rows
+// (solver.rs:309-330) for an anchored distance joint, the original row for the others.
+void joint_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vector<JRow>& out);
 // joint_row_vel / joint_row_apply (solver.rs:291-307)
 float joint_row_vel(const World& w, const JRow& r);
 void joint_row_apply(World& w, const JRow& r, float lam);

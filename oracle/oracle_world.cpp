@@ -1062,7 +1062,7 @@ void World::step(float dt) {
     std::vector<std::pair<uint32_t, uint32_t>> jrange(joints.size(), {0u, 0u});
     for (uint32_t jk : active_joints) {
       uint32_t s = (uint32_t)jrows.size();
-      d6_rows(*this, joints[jk], jk, dt, jrows);
+      joint_rows(*this, joints[jk], jk, dt, jrows);
       jrange[jk] = {s, (uint32_t)jrows.size()};
       for (uint32_t k = s; k < (uint32_t)jrows.size(); ++k) jrows[k].idx = (uint8_t)(k - s);
       if (jrows.size() > s) jrows[s].cnt = (uint8_t)(jrows.size() - s);
@@ -1114,10 +1114,11 @@ void World::step(float dt) {
     stats.levels = (uint32_t)batches.size();
     for (auto& b : batches) stats.max_batch = std::max<uint32_t>(stats.max_batch, (uint32_t)b.size());
     for (uint32_t k = 0; k < nc; ++k) levels_out[k] = ent_level[njr + k];
-    // warm start, joints (:699-712): serial in joint order, clamped to each row's bounds
+    // warm start, joints (:699-712): serial in joint order, clamped to each row's bounds; distance
+    // rows start cold (:704-705)
     for (uint32_t jk = 0; jk < (uint32_t)joints.size(); ++jk) {
       uint32_t s = jrange[jk].first, e = jrange[jk].second;
-      if (e == s) continue;
+      if (e == s || joints[jk].kind != 0) continue;
       auto it = warm_joints.find(jk);
       if (it == warm_joints.end()) continue;
       const WarmJointRows& prev = it->second;
@@ -1325,10 +1326,11 @@ void World::step(float dt) {
       stats.row_sweeps += isl_rows[i] * isl_sweeps[i];
       if (residual_mode && !isl_done[i]) stats.islands_capped++;
     }
-    // joints solved this tick replace their rows; the rest keep theirs (:946-952)
+    // joints solved this tick replace their rows; the rest keep theirs (:946-952); distance rows
+    // are not kept
     for (uint32_t jk = 0; jk < (uint32_t)joints.size(); ++jk) {
       uint32_t s = jrange[jk].first, e = jrange[jk].second;
-      if (e == s) continue;
+      if (e == s || joints[jk].kind != 0) continue;
       WarmJointRows rows;
       for (uint32_t k = s; k < e; ++k) rows.push_back({jrows[k].tag, jacc[k]});
       warm_joints[jk] = rows;
@@ -1555,8 +1557,10 @@ void World::step(float dt) {
       start_poses[i] = (dyn[i] && awake[i]) ? original[i] : Iso{pos[i], rot[i]};
       frozen[i] = (!dyn[i] || !awake[i]) ? 1 : 0;
     }
-    for (auto& jt : joints)  // Joints::begin_step (bodies.rs:290-300)
+    for (auto& jt : joints) {  // Joints::begin_step (bodies.rs:310-318)
       for (int k = 0; k < 3; ++k) { jt.lam_t[k] = 0.0f; jt.lam_r[k] = 0.0f; }
+      jt.lambda_acc = 0.0f;
+    }
   }
   if (has_joints || !pcs.empty()) {
     for (uint32_t it = 0; it < iters_p; ++it) {

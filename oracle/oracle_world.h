@@ -64,12 +64,23 @@ struct D6Axis {
   bool has_drive = false, vel_mode = false;
   float d_target = 0.0f, d_kp = 0.0f, d_kd = 0.0f, d_max = 0.0f;
 };
+// JointKind (bodies.rs:140-143): a D6 joint (kind 0) or a distance joint (kind 1,
+// DistanceJoint, bodies.rs:31-51: rest length, compliance, anchors la / lb in each body's frame,
+// damping along the rod; both anchors zero and no damping is the original COM-to-COM joint).
 struct Joint {
   uint32_t a, b;
+  int kind = 0;
   Iso fa, fb;
   D6Axis t[3], r[3];
   int hinge = -1;
   float lam_t[3] = {0, 0, 0}, lam_r[3] = {0, 0, 0};  // XPBD multipliers of the current step
+  float rest = 0.0f, compliance = 0.0f, damping = 0.0f, lambda_acc = 0.0f;
+  V3 la{0, 0, 0}, lb{0, 0, 0};
+  // DistanceJoint::anchored (bodies.rs:47-51)
+  bool anchored() const {
+    return !(la.x == 0.0f && la.y == 0.0f && la.z == 0.0f) || !(lb.x == 0.0f && lb.y == 0.0f && lb.z == 0.0f) ||
+           damping > 0.0f;
+  }
 };
 // warm_joints entry (solver.rs:946-952): per row, its tag and accumulated impulse
 using WarmJointRows = std::vector<std::pair<uint8_t, float>>;
@@ -167,6 +178,10 @@ struct World {
   void set_d6_drive(uint32_t id, bool angular, uint32_t axis, bool has, float target, float kp, float kd,
                     float max_impulse, bool vel_mode);
   void set_d6_damping(uint32_t id, bool angular, uint32_t axis, float damping, float friction);
+  // Joints::add_distance_joint / add_distance_joint_at / set_distance_damping (bodies.rs:273-305)
+  uint32_t add_distance_joint(uint32_t a, uint32_t b, float rest, float compliance);
+  uint32_t add_distance_joint_at(uint32_t a, V3 la, uint32_t b, V3 lb, float rest, float compliance);
+  void set_distance_damping(uint32_t id, float damping);
   PairProps pair_props(uint32_t a, uint32_t b) const;
   void set_pair_props(uint32_t a, uint32_t b, const PairProps& p);
   void update_colliders_aabb();

@@ -66,17 +66,25 @@ RP_HD f3 clamp_length_max(f3 a, float m) {
   return a;
 }
 
+// glam's Quat is an SSE2 type on x86_64, where the reference runs; its product and norm are
+// restated in the lane order of those SSE2 paths (pinned by the reference's golden bits of
+// distance_bits_test.rs): the Hamilton product lane-wise as (w0 b + x0 b1) + (y0 b2 + z0 b3), b1..b3
+// the signed lane permutations of b; the 4-lane dot as (xx + zz) + (yy + ww); normalize as a
+// division by the length.
 RP_HD q4 qmul(q4 a, q4 b) {
-  return mkq(((a.w * b.x + a.x * b.w) + a.y * b.z) - a.z * b.y,
-             ((a.w * b.y - a.x * b.z) + a.y * b.w) + a.z * b.x,
-             ((a.w * b.z + a.x * b.y) - a.y * b.x) + a.z * b.w,
-             ((a.w * b.w - a.x * b.x) - a.y * b.y) - a.z * b.z);
+  return mkq((a.w * b.x + a.x * b.w) + (a.y * b.z - a.z * b.y),
+             (a.w * b.y - a.x * b.z) + (a.y * b.w + a.z * b.x),
+             (a.w * b.z + a.x * b.y) + (-(a.y * b.x) + a.z * b.w),
+             (a.w * b.w - a.x * b.x) + (-(a.y * b.y) - a.z * b.z));
 }
 RP_HD q4 qconj(q4 q) { return mkq(-q.x, -q.y, -q.z, q.w); }
 RP_HD q4 qneg(q4 q) { return mkq(-q.x, -q.y, -q.z, -q.w); }
-RP_HD float qdot(q4 a, q4 b) { return ((a.x * b.x + a.y * b.y) + a.z * b.z) + a.w * b.w; }
+RP_HD float qdot(q4 a, q4 b) { return (a.x * b.x + a.z * b.z) + (a.y * b.y + a.w * b.w); }
 RP_HD q4 qscale(q4 q, float s) { return mkq(q.x * s, q.y * s, q.z * s, q.w * s); }
-RP_HD q4 qnormalize(q4 q) { float r = 1.0f / sqrtf(qdot(q, q)); return qscale(q, r); }
+RP_HD q4 qnormalize(q4 q) {
+  float l = sqrtf(qdot(q, q));
+  return mkq(q.x / l, q.y / l, q.z / l, q.w / l);
+}
 RP_HD bool qeq(q4 a, q4 b) { return a.x == b.x && a.y == b.y && a.z == b.z && a.w == b.w; }
 RP_HD f3 qrot(q4 q, f3 v) {
   f3 b = mk3(q.x, q.y, q.z);
