@@ -219,6 +219,20 @@ typedef struct RPhysJointDesc {
     RPhysIsometry frame_a, frame_b;
 } RPhysJointDesc;
 RPhysResult rphys_ext_add_joints(RPhysWorld* world, const RPhysJointDesc* descs, uint32_t n, uint32_t* out_first_id);
+/* World::add_distance_joint / add_distance_joint_at + set_distance_damping (world.rs:537-552;
+ * bodies.rs:273-305): body_b's anchor held at `rest` from body_a's (anchors in each body's frame),
+ * compliance in m/N (0 = rigid, else a spring at position level), damping in N s/m along the rod.
+ * Both anchors zero and no damping is the original centre-to-centre rod (its own velocity row,
+ * solver.rs:793-817); otherwise the anchored rows (the rod passes torque through its lever arms).
+ * Joint ids are shared with rphys_ext_add_joints; bodies so joined no longer collide. Finite
+ * values, compliance and damping >= 0; all-or-nothing over the array. */
+typedef struct RPhysDistanceJointDesc {
+    uint32_t body_a, body_b;
+    RPhysVec3 anchor_a, anchor_b;
+    float rest, compliance, damping;
+} RPhysDistanceJointDesc;
+RPhysResult rphys_ext_add_distance_joints(RPhysWorld* world, const RPhysDistanceJointDesc* descs, uint32_t n,
+                                          uint32_t* out_first_id);
 /* Joints::set_d6_limit_t (angular = 0) / set_d6_limit_r (angular = 1) (bodies.rs:367-391): with
  * enabled, the axis becomes a limited row on [lo, hi] (metres along frame A's axis, or radians:
  * the twist angle on a hinge's own axis, 2 sin(angle / 2) about the other axes); a limit on a

@@ -530,6 +530,33 @@ RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_
   }
   return RPHYS_OK;
 }
+RPhysResult rphys_ext_add_distance_joints(RPhysWorld* W, const RPhysDistanceJointDesc* d, uint32_t n,
+                                          uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_distance_joints: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  std::vector<std::pair<uint32_t, uint32_t>> ab(n);
+  auto fin3 = [](RPhysVec3 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!fin3(d[i].anchor_a) || !fin3(d[i].anchor_b) || !std::isfinite(d[i].rest) ||
+        !(std::isfinite(d[i].compliance) && d[i].compliance >= 0.0f) ||
+        !(std::isfinite(d[i].damping) && d[i].damping >= 0.0f))
+      return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_distance_joints: non-finite value or negative compliance / damping");
+    RPhysResult r = live_id(W, d[i].body_a, "rphys_ext_add_distance_joints", &ab[i].first);
+    if (r) return r;
+    r = live_id(W, d[i].body_b, "rphys_ext_add_distance_joints", &ab[i].second);
+    if (r) return r;
+    if (ab[i].first == ab[i].second) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_distance_joints: body_a == body_b");
+  }
+  *out_first = (uint32_t)W->w.joints.size();
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t id = W->w.add_distance_joint_at(ab[i].first, v(d[i].anchor_a), ab[i].second, v(d[i].anchor_b), d[i].rest,
+                                             d[i].compliance);
+    W->w.set_distance_damping(id, d[i].damping);
+  }
+  return RPHYS_OK;
+}
 RPhysResult rphys_ext_set_joint_limit(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, uint32_t enabled,
                                       float lo, float hi) {
   clear_err();
@@ -564,6 +591,15 @@ uint32_t rphys_oracle_turned_threshold_mismatches(uint32_t dstar_bits) {
   for (float d = 0.8f; d <= 1.0f; d = std::nextafter(d, 2.0f))
     if ((2.0f * om::acosf_unit_rp(d) < 0.5f) != (d >= dstar)) bad++;
   return bad;
+}
+// Test hook: SHAKE_MAX_TURN.cos() as the oracle computes it (its bits; the GPU carries them as a
+// constant).
+uint32_t rphys_oracle_shake_max_turn_cos_bits() {
+  float s, c;
+  om::sincosf_rp(0.5f, &s, &c);
+  uint32_t u;
+  std::memcpy(&u, &c, 4);
+  return u;
 }
 // Test hook: the distance-joint scenes of the reference's golden bit test
 // (riftphys-world/tests/distance_bits_test.rs:11-48), built on the oracle World directly (no

@@ -128,6 +128,11 @@ JOINT_HINGE = 1
 JOINT_D6 = 2
 
 
+class DistanceJointDesc(Structure):
+    _fields_ = [("body_a", c_uint32), ("body_b", c_uint32), ("anchor_a", Vec3), ("anchor_b", Vec3),
+                ("rest", c_float), ("compliance", c_float), ("damping", c_float)]
+
+
 class JointDrive(Structure):
     _fields_ = [("target", c_float), ("kp", c_float), ("kd", c_float), ("max_impulse", c_float),
                 ("vel_mode", c_uint32)]
@@ -260,6 +265,7 @@ ABI = [
     ("rphys_ext_set_joint_limit", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float, c_float]),
     ("rphys_ext_num_joints", c_uint32, [c_void_p, POINTER(c_uint32)]),
     ("rphys_ext_set_joint_limits", c_uint32, [c_void_p, c_void_p, c_uint32]),
+    ("rphys_ext_add_distance_joints", c_uint32, [c_void_p, POINTER(DistanceJointDesc), c_uint32, POINTER(c_uint32)]),
     ("rphys_ext_set_joint_axis", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float]),
     ("rphys_ext_set_joint_drive", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, POINTER(JointDrive)]),
     ("rphys_ext_set_joint_damping", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_float, c_float]),
@@ -526,6 +532,19 @@ class World:
             arr[i].frame_b = iso(*fb[0], q=tuple(fb[1]))
         first = c_uint32(0)
         self.c("rphys_ext_add_joints", arr, len(joints), byref(first))
+        return first.value
+
+    def add_distance_joints(self, joints):
+        """joints: iterable of (body_a, body_b, anchor_a, anchor_b, rest, compliance, damping), anchors
+        (x, y, z) in each body's frame. Returns the first joint id."""
+        joints = list(joints)
+        arr = (DistanceJointDesc * max(1, len(joints)))()
+        for i, (a, b, la, lb, rest, comp, damp) in enumerate(joints):
+            arr[i].body_a, arr[i].body_b = a, b
+            arr[i].anchor_a, arr[i].anchor_b = Vec3(*la), Vec3(*lb)
+            arr[i].rest, arr[i].compliance, arr[i].damping = rest, comp, damp
+        first = c_uint32(0)
+        self.c("rphys_ext_add_distance_joints", arr, len(joints), byref(first))
         return first.value
 
     def add_joint_array(self, arr):

@@ -641,6 +641,44 @@ RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_
     return RPHYS_OK;
   });
 }
+RPhysResult rphys_ext_add_distance_joints(RPhysWorld* W, const RPhysDistanceJointDesc* d, uint32_t n,
+                                          uint32_t* out_first) {
+  clear_err();
+  if (out_first) *out_first = 0;
+  if (!W || (!d && n) || !out_first) return fail(RPHYS_ERR_NULL, "rphys_ext_add_distance_joints: null arg");
+  LOCK;
+  return guard("rphys_ext_add_distance_joints", [&]() {
+    std::vector<uint32_t> ab(2 * (size_t)n);
+    auto fin3 = [](RPhysVec3 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+    for (uint32_t i = 0; i < n; ++i) {
+      if (!fin3(d[i].anchor_a) || !fin3(d[i].anchor_b) || !std::isfinite(d[i].rest) ||
+          !(std::isfinite(d[i].compliance) && d[i].compliance >= 0.0f) ||
+          !(std::isfinite(d[i].damping) && d[i].damping >= 0.0f))
+        return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_distance_joints: non-finite value or negative compliance / damping");
+      RPhysResult r = live_id(W, d[i].body_a, "rphys_ext_add_distance_joints", &ab[2 * i]);
+      if (r) return r;
+      r = live_id(W, d[i].body_b, "rphys_ext_add_distance_joints", &ab[2 * i + 1]);
+      if (r) return r;
+      if (ab[2 * i] == ab[2 * i + 1]) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_distance_joints: body_a == body_b");
+      if (W->w->batched() && W->w->num_worlds() > 0) {
+        uint32_t wa = W->w->world_of(ab[2 * i]), wb = W->w->world_of(ab[2 * i + 1]);
+        if (wa != wb)
+          return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_distance_joints: in a batch, a joint joins two bodies of one world");
+        uint32_t prev = i ? W->w->world_of(ab[2 * i - 2])
+                          : (W->w->num_joints() ? W->w->world_of(W->w->h_joints_.back().a) : 0u);
+        if (wa < prev) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_add_distance_joints: in a batch, joints come in world order");
+      }
+    }
+    *out_first = W->w->num_joints();
+    for (uint32_t i = 0; i < n; ++i) {
+      const float la[3] = {d[i].anchor_a.x, d[i].anchor_a.y, d[i].anchor_a.z};
+      const float lb[3] = {d[i].anchor_b.x, d[i].anchor_b.y, d[i].anchor_b.z};
+      W->w->add_distance_joint(ab[2 * i], ab[2 * i + 1], la, lb, d[i].rest, d[i].compliance, d[i].damping);
+    }
+    W->w->upload_joints();
+    return RPHYS_OK;
+  });
+}
 RPhysResult rphys_ext_set_joint_limit(RPhysWorld* W, uint32_t joint, uint32_t angular, uint32_t axis, uint32_t enabled,
                                       float lo, float hi) {
   clear_err();

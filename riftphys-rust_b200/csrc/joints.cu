@@ -37,7 +37,7 @@ __global__ void k_joint_marks(uint32_t nj, const JointGpu* __restrict__ J, const
 __global__ void k_joint_count(uint32_t nj, const JointGpu* __restrict__ J, BodiesV B, float dt, uint32_t* cnt) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nj) return;
-  cnt[j] = d6_rows_dev(J[j], B, dt, [](const JRowD&, uint32_t) {});
+  cnt[j] = joint_rows_dev(J[j], B, dt, [](const JRowD&, uint32_t) {});
 }
 // Rows of joint j at R[base + off[j] + k]. Warm start (solver.rs:703-712): the previous rows'
 // impulses when the joint has an entry with the same row count and tags, each clamped to its
@@ -53,19 +53,20 @@ __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, Bodie
   const JointGpu& jt = J[j];
   const uint32_t r0 = base + off[j], wn = jw_n[j];
   bool tags_match = true, dyn_a = false, dyn_b = false;
-  uint32_t n = d6_rows_dev(jt, B, dt, [&](const JRowD& r, uint32_t k) {
+  uint32_t n = joint_rows_dev(jt, B, dt, [&](const JRowD& r, uint32_t k) {
     uint32_t i = r0 + k;
     tags_match = tags_match && k < wn && jw_tag[JMAX_ROWS * (size_t)j + k] == (uint8_t)r.tag;
     if (k == 0) { dyn_a = r.wa > 0.0f; dyn_b = r.wb > 0.0f; }
     R.ab[i] = make_uint2(jt.a, jt.b);
     R.flags[i] = RF_JOINT | (r.angular ? RF_JANG : 0u) | (r.wa > 0.0f ? RF_WA : 0u) | (r.wb > 0.0f ? RF_WB : 0u) |
-                 (k == 0 ? RF_JFIRST : 0u);
+                 (k == 0 ? RF_JFIRST : 0u) | (r.legacy ? RF_JLEG : 0u);
     R.inv[i] = make_float2(r.wa, r.wb);
     R.ra[i] = f4(r.ra, r.m_eff);
-    R.rb[i] = f4(r.rb, 0.0f);
+    R.rb[i] = f4(r.rb, r.inv_sum);
     R.n[i] = f4(r.u, 0.0f);
-    // t1.x: the joint's row count on its first row (the unit's length, set below), t1.y: the row's index
-    R.t1[i] = make_float4(0.0f, (float)k, r.gamma, r.target);
+    // t1.x: the joint's row count on its first row (the unit's length, set below), t1.y: the row's
+    // index, t1.w: the target (the bias of an original distance row)
+    R.t1[i] = make_float4(0.0f, (float)k, r.gamma, r.legacy ? r.bias : r.target);
     R.t2[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     R.mu[i] = make_float4(r.lo, r.hi, 0.0f, __uint_as_float(r.tag));
     R.la[i] = make_float4(__uint_as_float(j), 0.0f, 0.0f, 0.0f);
@@ -74,7 +75,7 @@ __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, Bodie
   });
   if (n == 0) return;
   R.t1[r0].x = (float)n;
-  if (tags_match && wn == n) {
+  if (tags_match && wn == n && !(jt.flags & JF_DIST)) {  // distance rows start cold (solver.rs:704-705)
     for (uint32_t k = 0; k < n; ++k) {
       const uint32_t i = r0 + k;
       const float4 mu = R.mu[i];
@@ -93,13 +94,14 @@ __global__ void k_joint_roots(uint32_t njr, uint32_t base, RowsV R, uint32_t* uf
   row_root[r] = uf_find(uf, (R.flags[r] & RF_WA) ? ab.x : ab.y);
 }
 // Joints solved this tick replace their cache entry; the others keep theirs (solver.rs:946-952).
-__global__ void k_joint_store(uint32_t nj, const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ off,
+__global__ void k_joint_store(uint32_t nj, const JointGpu* __restrict__ J, const uint32_t* __restrict__ cnt,
+                              const uint32_t* __restrict__ off,
                               uint32_t base, RowsV R, const float* __restrict__ acc_jn, uint32_t* jw_n,
                               uint8_t* jw_tag, float* jw_lam) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nj) return;
   uint32_t n = cnt[j];
-  if (n == 0) return;
+  if (n == 0 || (J[j].flags & JF_DIST)) return;  // distance rows are not kept (solver.rs:945-947)
   jw_n[j] = n;
   for (uint32_t k = 0; k < n; ++k) {
     uint32_t r = base + off[j] + k;
@@ -155,7 +157,7 @@ void joints_row_roots(WorldGpu& W, const RowsV& R, uint32_t base, uint32_t njr, 
 void joints_store_warm(WorldGpu& W, const RowsV& R, uint32_t base, const float* acc_jn, cudaStream_t st) {
   uint32_t nj = W.num_joints();
   if (!nj || !W.njr_) return;
-  k_joint_store<<<nblk(nj), T, 0, st>>>(nj, W.jr_cnt.p, W.jr_off.p, base, R, acc_jn, W.jw_n.p, W.jw_tag.p, W.jw_lam.p);
+  k_joint_store<<<nblk(nj), T, 0, st>>>(nj, W.joints_d.p, W.jr_cnt.p, W.jr_off.p, base, R, acc_jn, W.jw_n.p, W.jw_tag.p, W.jw_lam.p);
   RP_COUNT_LAUNCH(1);
 }
 void joints_mark_constrained(WorldGpu& W, uint8_t* constrained, cudaStream_t st) {
@@ -177,6 +179,30 @@ uint32_t WorldGpu::add_joint(uint32_t kind, uint32_t a, uint32_t b, const float 
   for (int k = 0; k < 7; ++k) { j.fa[k] = fa[k]; j.fb[k] = fb[k]; }
   for (int k = 0; k < 3; ++k) { j.en[k] = true; j.en[3 + k] = kind == 2 || (kind == 1 && (uint32_t)k != axis); }
   j.hinge = kind == 1 ? (int)axis : -1;
+  if (batch_ && !h_wb_start_.empty()) {
+    uint32_t wa = world_of(a), wb = world_of(b);
+    if (wa != wb) throw std::invalid_argument("a joint in a batch joins two bodies of one world");
+    if (!h_joints_.empty() && wa < world_of(h_joints_.back().a))
+      throw std::invalid_argument("a batch's joints are added in world order");
+  }
+  h_joints_.push_back(j);
+  joints_dirty_ = true;
+  return (uint32_t)h_joints_.size() - 1;
+}
+// Joints::add_distance_joint_at + set_distance_damping (bodies.rs:273-305): rest and anchors made
+// finite, compliance and damping finite and >= 0.
+uint32_t WorldGpu::add_distance_joint(uint32_t a, uint32_t b, const float la[3], const float lb[3], float rest,
+                                      float compliance, float damping) {
+  JointHost j{};
+  j.a = a; j.b = b;
+  j.kind = 1;
+  j.hinge = -1;
+  auto fin0 = [](float x) { return std::isfinite(x) ? x : 0.0f; };
+  for (int k = 0; k < 3; ++k) { j.fa[k] = fin0(la[k]); j.fb[k] = fin0(lb[k]); }
+  j.fa[6] = 1.0f; j.fb[6] = 1.0f;
+  j.rest = fin0(rest);
+  j.dcomp = std::max(fin0(compliance), 0.0f);
+  j.ddamp = std::max(fin0(damping), 0.0f);
   if (batch_ && !h_wb_start_.empty()) {
     uint32_t wa = world_of(a), wb = world_of(b);
     if (wa != wb) throw std::invalid_argument("a joint in a batch joins two bodies of one world");
@@ -289,7 +315,17 @@ void WorldGpu::upload_joints() {
       if (k >= 3 && s.drive[k] && s.vel[k]) rdrive = true;
       if (s.drive[k] || s.comp[k] > 0.0f) f |= JF_FULL;
     }
-    f |= (uint32_t)(hinge_of(s) + 1) << JF_HINGE_SHIFT;
+    if (s.kind == 1) {  // a distance joint: rest lo[0], compliance comp[0], damping damp[0]
+      f = JF_DIST;
+      const bool anchored = !(s.fa[0] == 0.0f && s.fa[1] == 0.0f && s.fa[2] == 0.0f) ||
+                            !(s.fb[0] == 0.0f && s.fb[1] == 0.0f && s.fb[2] == 0.0f) || s.ddamp > 0.0f;
+      if (anchored) f |= JF_ANCH;
+      for (int k = 0; k < 6; ++k) { g.lo[k] = 0.0f; g.hi[k] = 0.0f; g.comp[k] = 0.0f; g.damp[k] = 0.0f; }
+      g.lo[0] = s.rest; g.comp[0] = s.dcomp; g.damp[0] = s.ddamp;
+      rdrive = false;
+    } else {
+      f |= (uint32_t)(hinge_of(s) + 1) << JF_HINGE_SHIFT;
+    }
     g.flags = f;
     g.fa_p = make_float4(s.fa[0], s.fa[1], s.fa[2], 0.0f); g.fa_q = make_float4(s.fa[3], s.fa[4], s.fa[5], s.fa[6]);
     g.fb_p = make_float4(s.fb[0], s.fb[1], s.fb[2], 0.0f); g.fb_q = make_float4(s.fb[3], s.fb[4], s.fb[5], s.fb[6]);

@@ -25,16 +25,25 @@ static_assert(sizeof(JointGpu) == 256, "JointGpu layout");
 #define JF_DRIVE_SHIFT 16u
 #define JF_VEL_SHIFT 22u
 #define JF_FULL (1u << 28)  // some axis compliant or driven: the position solve takes the full path
+// A distance joint (DistanceJoint, bodies.rs:31-51): rest length lo[0], compliance comp[0],
+// damping damp[0], anchors fa_p.xyz / fb_p.xyz in each body's frame; JF_ANCH: anchored (an anchor
+// or damping set), solved by the anchored rows, else by the original COM-to-COM ones.
+#define JF_DIST (1u << 29)
+#define JF_ANCH (1u << 30)
 #define JMAX_ROWS kJointRows
 
 __host__ __device__ inline int joint_hinge(uint32_t flags) { return (int)((flags >> JF_HINGE_SHIFT) & 7u) - 1; }
 
 // A joint velocity row (JointRow, solver.rs:264-288); gamma = 1 / (damping dt) on a damper row.
+// legacy: the original distance row (solver.rs:793-817), impulse -(v_rel + bias) / inv_sum along u
+// on the linear velocities, no accumulation and no clamp.
 struct JRowD {
   f3 u, ra, rb;
   float wa, wb, m_eff, target, lo, hi, gamma;
   uint32_t tag;
   bool angular;
+  bool legacy = false;
+  float bias = 0.0f, inv_sum = 0.0f;
 };
 __host__ __device__ inline bool jaxis_on(uint32_t f, int ax) { return (f >> ax) & 1u; }
 __host__ __device__ inline bool jaxis_lim(uint32_t f, int ax) { return (f >> (JF_LIMIT_SHIFT + ax)) & 1u; }
@@ -148,6 +157,57 @@ __device__ __forceinline__ uint32_t d6_rows_dev(const JointGpu& j, const BodiesV
     }
   }
   return n;
+}
+
+// distance_rows (solver.rs:309-330): an anchored rigid rod's equality row along the current
+// anchors' direction (a compliant rod has none); and the original COM-to-COM row (solver.rs:
+// 793-817), made once per tick since positions do not move during the velocity solve.
+template <class Emit>
+__device__ __forceinline__ uint32_t distance_rows_dev(const JointGpu& j, const BodiesV& B, float dt, Emit&& emit) {
+  const uint32_t a = j.a, b = j.b;
+  const float rest = j.lo[0], compliance = j.comp[0];
+  if (j.flags & JF_ANCH) {
+    float wa = B.inv_mass[a], wb = B.inv_mass[b];
+    if (wa == 0.0f && wb == 0.0f) return 0;
+    q4 qa = asq(B.rot[a]), qb = asq(B.rot[b]);
+    f3 ra = qrot(qa, xyz(j.fa_p)), rb = qrot(qb, xyz(j.fb_p));
+    f3 d = (xyz(B.pos[b]) + rb) - (xyz(B.pos[a]) + ra);
+    float len = sqrtf(len2(d));
+    if (!(len > 1e-6f)) return 0;
+    f3 u = d / len;
+    m3 ia = inv_inertia_world_dev(B, a, qa), ib = inv_inertia_world_dev(B, b, qb);
+    f3 ca = cross(ra, u), cb = cross(rb, u);
+    float k = ((wa + wb) + dot(ca, mvec(ia, ca))) + dot(cb, mvec(ib, cb));
+    if (!(k > 1e-9f)) return 0;
+    if (compliance > 0.0f) return 0;
+    JRowD r;
+    r.u = u; r.ra = ra; r.rb = rb; r.wa = wa; r.wb = wb; r.m_eff = 1.0f / k;
+    r.target = 0.0f; r.lo = -INFINITY; r.hi = INFINITY; r.gamma = 0.0f; r.tag = 0; r.angular = false;
+    emit(r, 0u);
+    return 1;
+  }
+  if (compliance > 0.0f) return 0;  // a spring acts at position level only
+  f3 dir = xyz(B.pos[b]) - xyz(B.pos[a]);
+  float len = sqrtf(len2(dir));
+  if (len < 1e-6f) return 0;
+  f3 n = dir / len;
+  float inv_a = B.inv_mass[a], inv_b = B.inv_mass[b];
+  float inv_sum = inv_a + inv_b;
+  if (inv_sum < 1e-9f) return 0;
+  JRowD r;
+  r.u = n; r.ra = mk3(0, 0, 0); r.rb = mk3(0, 0, 0); r.wa = inv_a; r.wb = inv_b; r.m_eff = 1.0f / inv_sum;
+  r.target = 0.0f; r.lo = -INFINITY; r.hi = INFINITY; r.gamma = 0.0f; r.tag = 0; r.angular = false;
+  r.legacy = true;
+  r.bias = (len - rest) * (0.1f / dt);
+  r.inv_sum = inv_sum;
+  emit(r, 0u);
+  return 1;
+}
+// A joint's velocity rows whatever its kind (solver.rs:655-661).
+template <class Emit>
+__device__ __forceinline__ uint32_t joint_rows_dev(const JointGpu& j, const BodiesV& B, float dt, Emit&& emit) {
+  if (j.flags & JF_DIST) return distance_rows_dev(j, B, dt, emit);
+  return d6_rows_dev(j, B, dt, emit);
 }
 
 // ---- the position solve (bodies.rs:616-873) on the bodies' global pose arrays
@@ -355,12 +415,111 @@ void joints_store_warm(WorldGpu& W, const RowsV& R, uint32_t base, const float* 
 // Bodies in joints count as constrained (step.rs:160-170).
 void joints_mark_constrained(WorldGpu& W, uint8_t* constrained, cudaStream_t st);
 
-// The position solve of joint j: the full path for joints with a compliant or driven axis, the
-// locked-and-limited one for the rest.
-__device__ __forceinline__ void solve_d6_any(const JointGpu& j, float* lam, const BodiesV& B, float dt, f3 sa_p, q4 sa_q,
-                                             f3 sb_p, q4 sb_q) {
-  if (j.flags & JF_FULL) solve_d6_dev<true>(j, lam, B, dt, sa_p, sa_q, sb_p, sb_q);
-  else solve_d6_dev<false>(j, lam, B, dt, sa_p, sa_q, sb_p, sb_q);
+// SHAKE_MAX_TURN.cos() (bodies.rs:520) as the project's cosine gives it: 0.87758255
+// (tests/test_oracle_joints.py checks the oracle's value has these bits).
+#define RP_SHAKE_MAX_TURN_COS_BITS 0x3f60a940u
+// solve_distance_row (bodies.rs:501-548): the original COM-to-COM rod, corrected along the
+// start-of-step direction when it is within SHAKE_MAX_TURN of the current one. lam: its multiplier.
+__device__ __forceinline__ void solve_distance_row_dev(const JointGpu& j, float* lam, const BodiesV& B, float dt2,
+                                                       f3 sa_p, f3 sb_p) {
+  const uint32_t ia = j.a, ib = j.b;
+  const float wa = B.inv_mass[ia], wb = B.inv_mass[ib];
+  const float w_sum = fin0(wa + wb);
+  if (w_sum <= 0.0f) return;
+  f3 d = xyz(B.pos[ib]) - xyz(B.pos[ia]);
+  float l2 = len2(d);
+  if (!fin(l2) || l2 <= 1.0e-20f) return;
+  float len = sqrtf(l2);
+  if (len <= 1.0e-6f) return;
+  f3 n_cur = normalize_fin(d / len);
+  if (vzero(n_cur)) return;
+  f3 n = n_cur;
+  f3 n0 = normalize_fin(sb_p - sa_p);
+  if (!vzero(n0) && dot(n0, n_cur) > __uint_as_float(RP_SHAKE_MAX_TURN_COS_BITS)) n = n0;
+  const float compliance = j.comp[0];
+  float c_val = fin0(len - fin0(j.lo[0]));
+  float alpha = compliance <= 0.0f ? 0.0f : fin0(rmax(fin0(compliance), 0.0f) / dt2);
+  float denom = fin0(w_sum + alpha);
+  if (denom <= 0.0f) return;
+  float lambda_old = fin0(lam[0]);
+  float lambda = fin0(-(c_val + fin0(alpha * lambda_old)) / (denom * dot(n, n_cur)));
+  if (fabsf(lambda) <= 1.0e-9f) return;
+  lam[0] = fin0(lambda_old + lambda);
+  apply_position_delta_dev(B, ia, fin_v((-n) * fin0(lambda * wa)));
+  apply_position_delta_dev(B, ib, fin_v(n * fin0(lambda * wb)));
+}
+// solve_distance_anchored (bodies.rs:557-614): C = |x_b - x_a| - rest on the current anchors, along
+// the start-of-step direction with start-of-step lever arms and inertias over the mixed Jacobian
+// product (current-iterate directions when a body turned too far or the mixed product falls below
+// half the start-of-step one); a damped compliant rod's spring and damper in one Kelvin-Voigt row.
+__device__ __forceinline__ void solve_distance_anchored_dev(const JointGpu& j, float* lam, const BodiesV& B, float dt,
+                                                            float dt2, f3 sa_p, q4 sa_q, f3 sb_p, q4 sb_q) {
+  const uint32_t ia = j.a, ib = j.b;
+  const float wa = fin0(B.inv_mass[ia]), wb = fin0(B.inv_mass[ib]);
+  if (wa + wb <= 0.0f) return;
+  const f3 la = xyz(j.fa_p), lb = xyz(j.fb_p);
+  const float rest = j.lo[0], compliance = j.comp[0], damping = j.damp[0];
+  f3 pap = xyz(B.pos[ia]), pbp = xyz(B.pos[ib]);
+  q4 paq = asq(B.rot[ia]), pbq = asq(B.rot[ib]);
+  f3 ra = fin_v(qrot(paq, la)), rb = fin_v(qrot(pbq, lb));
+  f3 d = fin_v((pbp + rb) - (pap + ra));
+  float len = sqrtf(len2(d));
+  if (!fin(len) || len <= 1.0e-6f) return;
+  f3 n_cur = normalize_fin(d / len);
+  if (vzero(n_cur)) return;
+  float c_val = fin0(len - fin0(rest));
+  float alpha = compliance <= 0.0f ? 0.0f : fin0(rmax(fin0(compliance), 0.0f) / dt2);
+  f3 n = n_cur, ga, gb;
+  float wgen = 0.0f;
+  bool shake = false;
+  if (turned_below_max(sa_q, paq) && turned_below_max(sb_q, pbq)) {
+    f3 ra0 = qrot(sa_q, la), rb0 = qrot(sb_q, lb);
+    f3 n0 = normalize_fin((sb_p + rb0) - (sa_p + ra0));
+    if (!vzero(n0)) {
+      m3 ia0 = world_inertia(sa_q, ld_m3(B.inv_I, ia)), ib0 = world_inertia(sb_q, ld_m3(B.inv_I, ib));
+      f3 ga0 = mvec(ia0, cross(ra0, n0)), gb0 = mvec(ib0, cross(rb0, n0));
+      float w_sym = ((wa + wb) + dot(cross(ra0, n0), ga0)) + dot(cross(rb0, n0), gb0);
+      float w_mix = (((wa + wb) * dot(n_cur, n0)) + dot(cross(ra, n_cur), ga0)) + dot(cross(rb, n_cur), gb0);
+      if (fin(w_mix) && w_mix >= 0.5f * w_sym) { shake = true; n = n0; ga = ga0; gb = gb0; wgen = w_mix; }
+    }
+  }
+  if (!shake) {
+    m3 iaw = inv_inertia_world_dev(B, ia, paq), ibw = inv_inertia_world_dev(B, ib, pbq);
+    f3 ca = cross(ra, n_cur), cb = cross(rb, n_cur);
+    wgen = ((wa + wb) + dot(ca, mvec(iaw, ca))) + dot(cb, mvec(ibw, cb));
+    n = n_cur; ga = mvec(iaw, ca); gb = mvec(ibw, cb);
+  }
+  float denom = fin0(wgen + alpha);
+  if (!(denom > 0.0f)) return;
+  float lambda_old = fin0(lam[0]);
+  float dl;
+  if (compliance > 0.0f && damping > 0.0f) {
+    float len0 = sqrtf(len2((sb_p + qrot(sb_q, lb)) - (sa_p + qrot(sa_q, la))));
+    float gamma = fin0(compliance * damping / dt);
+    dl = fin0(-((c_val + fin0(alpha * lambda_old)) + fin0(gamma * fin0(len - len0))) / fin0((1.0f + gamma) * wgen + alpha));
+  } else {
+    dl = fin0(-(c_val + fin0(alpha * lambda_old)) / denom);
+  }
+  if (fabsf(dl) <= 1.0e-12f) return;
+  lam[0] = fin0(lambda_old + dl);
+  apply_position_delta_dev(B, ia, fin_v((-n) * fin0(dl * wa)));
+  apply_position_delta_dev(B, ib, fin_v(n * fin0(dl * wb)));
+  apply_orientation_delta_dev(B, ia, fin_v((-ga) * dl));
+  apply_orientation_delta_dev(B, ib, fin_v(gb * dl));
+}
+// The position solve of joint j: a distance joint's row; for a D6 joint the full path when it has
+// a compliant or driven axis, the locked-and-limited one otherwise.
+__device__ __forceinline__ void solve_joint_pos(const JointGpu& j, float* lam, const BodiesV& B, float dt, f3 sa_p,
+                                                q4 sa_q, f3 sb_p, q4 sb_q) {
+  if (j.flags & JF_DIST) {
+    const float dt2 = rmax(dt * dt, 1.0e-12f);
+    if (j.flags & JF_ANCH) solve_distance_anchored_dev(j, lam, B, dt, dt2, sa_p, sa_q, sb_p, sb_q);
+    else solve_distance_row_dev(j, lam, B, dt2, sa_p, sb_p);
+  } else if (j.flags & JF_FULL) {
+    solve_d6_dev<true>(j, lam, B, dt, sa_p, sa_q, sb_p, sb_q);
+  } else {
+    solve_d6_dev<false>(j, lam, B, dt, sa_p, sa_q, sb_p, sb_q);
+  }
 }
 
 }  // namespace rp

@@ -176,6 +176,11 @@ __device__ __forceinline__ f3 rel_vel(const BodiesV& B, const Row& r) {
   f3 vb = (r.flags & RF_TERRAIN) ? mk3(0, 0, 0) : xyz(B.lin[r.bi]) + cross(xyz(B.ang[r.bi]), r.rb);
   return vb - va;
 }
+// Bodies::apply_impulse alone (dynamics.rs:193-197): the linear part
+__device__ __forceinline__ void lin_impulse(const BodiesV& B, uint32_t i, f3 j) {
+  float im = B.inv_mass[i];
+  if (im > 0.0f && vfin(j)) { float4 l = B.lin[i]; B.lin[i] = f4(fin_v(xyz(l) + j * im), l.w); }
+}
 // Bodies::apply_impulse / apply_angular_impulse (dynamics.rs:193-205) with the tick's R I^-1 R^T
 __device__ __forceinline__ void body_impulse(const BodiesV& B, uint32_t i, f3 j, f3 tau) {
   float im = B.inv_mass[i];
@@ -258,7 +263,16 @@ __device__ __forceinline__ void joint_apply_glob(const BodiesV& B, const Row& r,
     if (r.inv_b > 0.0f) body_impulse(B, r.bi, p, cross(r.rb, p));
   }
 }
+// The original distance row (solver.rs:793-817) on the global arrays: returns the impulse.
+__device__ __forceinline__ float legacy_row_glob(const BodiesV& B, const Row& r) {
+  float v_rel = dot(xyz(B.lin[r.bi]) - xyz(B.lin[r.ai]), r.n);
+  float j_mag = -(v_rel + r.bias) / r.m_t1;
+  lin_impulse(B, r.ai, (-r.n) * j_mag);
+  lin_impulse(B, r.bi, r.n * j_mag);
+  return j_mag;
+}
 __device__ __forceinline__ float joint_row_glob(const BodiesV& B, const Row& r, uint32_t k, float* acc_jn) {
+  if (r.flags & RF_JLEG) return fabsf(legacy_row_glob(B, r)) / r.m_n;
   f3 va, vb;
   if (r.flags & RF_JANG) { va = xyz(B.ang[r.ai]); vb = xyz(B.ang[r.bi]); }
   else {
@@ -849,7 +863,7 @@ __global__ void __launch_bounds__(128) k_pos_iterations(uint32_t n_listed, const
               const JointGpu& jt = J[j];
               bool fa = !B.dyn[jt.a] || !B.awake[jt.a], fb = !B.dyn[jt.b] || !B.awake[jt.b];
               if (!(fa && fb))
-                solve_d6_any(jt, jlam + 6 * (size_t)j, B, dt, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]),
+                solve_joint_pos(jt, jlam + 6 * (size_t)j, B, dt, xyz(spos[jt.a]), asq(srot[jt.a]), xyz(spos[jt.b]),
                              asq(srot[jt.b]));
             }
             continue;
@@ -1104,8 +1118,11 @@ __global__ void k_permute_rows(uint32_t n, uint32_t nc, const uint32_t* __restri
   O.ra[s] = ra; O.rb[s] = rb; O.n[s] = R.n[r]; O.t1[s] = R.t1[r]; O.t2[s] = R.t2[r]; O.mu[s] = R.mu[r];
   f3 va = mk3(0, 0, 0), vb = mk3(0, 0, 0);
   const bool jang = (f & RF_JANG) != 0;
-  if (!(f & RF_TA)) va = jang ? xyz(B.ang[x.x]) : xyz(B.lin[x.x]) + cross(xyz(B.ang[x.x]), xyz(ra));
-  if (!(f & RF_TERRAIN) && !(f & RF_TB)) vb = jang ? xyz(B.ang[x.y]) : xyz(B.lin[x.y]) + cross(xyz(B.ang[x.y]), xyz(rb));
+  const bool jleg = (f & RF_JLEG) != 0;  // the original distance row reads linear velocities alone
+  if (!(f & RF_TA))
+    va = jang ? xyz(B.ang[x.x]) : (jleg ? xyz(B.lin[x.x]) : xyz(B.lin[x.x]) + cross(xyz(B.ang[x.x]), xyz(ra)));
+  if (!(f & RF_TERRAIN) && !(f & RF_TB))
+    vb = jang ? xyz(B.ang[x.y]) : (jleg ? xyz(B.lin[x.y]) : xyz(B.lin[x.y]) + cross(xyz(B.ang[x.y]), xyz(rb)));
   O.va[s] = f4(va);
   O.vb[s] = f4(vb);
   O.jn[s] = 0.0f;
@@ -1229,6 +1246,16 @@ __device__ __forceinline__ void joint_apply_reg(f3& la, f3& aa, f3& lb, f3& ab, 
     if (ib) impulse_reg(lb, ab, imb, qb, p, cross(r.rb, p));
   }
 }
+// The original distance row (solver.rs:793-817) on register copies of the two linear velocities
+// (a side outside the group reads vfix, its linear velocity): returns the impulse.
+__device__ __forceinline__ float legacy_row_reg(f3& la, f3& lb, bool ha, bool hb, const SRow& r, float ima, float imb) {
+  float v_rel = dot((hb ? lb : r.vfix) - (ha ? la : r.vfix), r.n);
+  float j_mag = -(v_rel + r.bias) / r.m_t1;
+  f3 pa = (-r.n) * j_mag, pb = r.n * j_mag;
+  if (r.inv_a > 0.0f && ima > 0.0f && vfin(pa)) la = fin_v(la + pa * ima);
+  if (r.inv_b > 0.0f && imb > 0.0f && vfin(pb)) lb = fin_v(lb + pb * imb);
+  return j_mag;
+}
 __device__ __noinline__ void joint_row_core(float4* lin, float4* ang, const SRow& r, const m3& qa, const m3& qb,
                                                float ima, float imb, float& acc, float* d3) {
   const bool ha = r.la != 0xFFFFFFFFu, hb = r.lb != 0xFFFFFFFFu;
@@ -1237,6 +1264,14 @@ __device__ __noinline__ void joint_row_core(float4* lin, float4* ang, const SRow
   if (ha) { LA = lin[r.la]; AA = ang[r.la]; }
   if (hb) { LB = lin[r.lb]; AB = ang[r.lb]; }
   f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
+  if (r.flags & RF_JLEG) {
+    d3[0] = legacy_row_reg(la, lb, ha, hb, r, ima, imb);
+    d3[1] = 0.0f;
+    d3[2] = 0.0f;
+    if (ia) lin[r.la] = f4(la, LA.w);
+    if (ib) lin[r.lb] = f4(lb, LB.w);
+    return;
+  }
   f3 va, vb;
   if (r.flags & RF_JANG) { va = ha ? aa : r.vfix; vb = hb ? ab : r.vfix; }
   else { va = ha ? la + cross(aa, r.ra) : r.vfix; vb = hb ? lb + cross(ab, r.rb) : r.vfix; }
@@ -1270,6 +1305,13 @@ __device__ __noinline__ void joint_unit_core(float4* lin, float4* ang, const SRo
   bool moved = false;
   for (uint32_t q = 0; q < cnt; ++q) {
     const SRow& r = rows[q];
+    if (r.flags & RF_JLEG) {
+      dres[3 * q] = legacy_row_reg(la, lb, ha, hb, r, ima, imb);
+      dres[3 * q + 1] = 0.0f;
+      dres[3 * q + 2] = 0.0f;
+      moved = true;
+      continue;
+    }
     f3 va, vb;
     if (r.flags & RF_JANG) { va = ha ? aa : r.vfix; vb = hb ? ab : r.vfix; }
     else { va = ha ? la + cross(aa, r.ra) : r.vfix; vb = hb ? lb + cross(ab, r.rb) : r.vfix; }

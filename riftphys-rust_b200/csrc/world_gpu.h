@@ -117,6 +117,9 @@ class WorldGpu {
     bool drive[6], vel[6];         // driven; the drive a velocity motor
     float dtarget[6], dkp[6], dkd[6], dmax[6];
     int hinge;                     // stored hinge axis (add_hinge), -1 none
+    // kind 1, a distance joint: rest length, compliance, damping along the rod; anchors in fa / fb
+    int kind;
+    float rest, dcomp, ddamp;
   };
   uint32_t num_joints() const { return (uint32_t)h_joints_.size(); }
   uint32_t world_of(uint32_t body) const;
@@ -126,6 +129,8 @@ class WorldGpu {
   void set_joint_drive(uint32_t j, bool angular, uint32_t axis, bool on, float target, float kp, float kd,
                        float max_impulse, bool vel_mode);
   void set_joint_damping(uint32_t j, bool angular, uint32_t axis, float damping, float friction);
+  uint32_t add_distance_joint(uint32_t a, uint32_t b, const float la[3], const float lb[3], float rest, float compliance,
+                              float damping);
   void upload_joints();            // the joint records, jointed bodies and jointed pairs, on change
   std::vector<JointHost> h_joints_;
   bool joints_dirty_ = false;

@@ -4,7 +4,8 @@ reference's riftphys-world/tests: joint_energy_test.rs:46-219 (SHAKE energy beha
 replay), hinge_angle_test.rs:14-58 (hinge limits in radians), joint_damping_test.rs (viscous damping
 and Coulomb friction rows), compliant_joint_test.rs:20-75, 134-170 (torsional springs and sprung
 hinges), joint_conditioning_test.rs:22-66 (position drive, SHAKE projection) and
-world_robotics_test.rs:75-135 (velocity motor), with the same bodies, rates and tolerances; the pin
+world_robotics_test.rs:75-135 (velocity motor), distance joints from compliant_joint_test.rs:77-131
+and the golden bits of distance_bits_test.rs, with the same bodies, rates and tolerances; the pin
 bodies carry a small collider here (the FFI gives every body one), which never touches the jointed
 rods (jointed pairs make no contacts)."""
 import math
@@ -532,5 +533,127 @@ def case_d6_api_errors(lib):
     w.set_joint_drive(j, True, 0, 0.5, max_impulse=10.0, velocity=True)
     w.set_joint_drive(j, True, 0)  # cleared
     w.set_joint_damping(j, True, 1, 2.0, 0.5)
+    w.step(1.0 / 60.0)
+    w.close()
+
+
+# ---- distance joints
+def case_compliant_distance_joint_holds_its_static_stretch(lib):
+    """compliant_joint_test.rs:77-112: a 2 kg weight on a compliant distance joint (0.0005 m/N),
+    started at its static stretch c m g, stays within 3% of it for 10 s at 60 Hz / 20 iterations,
+    240 Hz / 20 and 240 Hz / 4."""
+    c, m = 0.0005, 2.0
+    stretch = c * m * G
+    for hz, iters in ((60.0, 20), (240.0, 20), (240.0, 4)):
+        w = _world(lib, 4)
+        w.set_iterations(iters, iters)
+        p = _body(w, (0.0, 10.0, 0.0), PIN, 1.0, dynamic=False)
+        bob = _body(w, (0.0, 9.0 - stretch, 0.0), (0.05, 0.05, 0.05), m / 0.001, sleep=False)
+        w.add_distance_joints([(p, bob, (0, 0, 0), (0, 0, 0), 1.0, c, 0.0)])
+        worst = 0.0
+        for _ in range(int(10.0 * hz)):
+            w.step(1.0 / hz)
+            s = (10.0 - w.pose(bob)[0][1]) - 1.0
+            worst = max(worst, abs(s - stretch) / stretch)
+        assert worst < 0.03, f"{hz} Hz, {iters} iterations: stretch departed {100 * worst:.2f}%"
+        w.close()
+
+
+def case_rigid_distance_joint_stays_rigid(lib):
+    """compliant_joint_test.rs:114-131: compliance 0 holds a 1 m rod within 2 mm for 10 s."""
+    w = _world(lib, 4)
+    p = _body(w, (0.0, 10.0, 0.0), PIN, 1.0, dynamic=False)
+    bob = _body(w, (1.0, 10.0, 0.0), (0.05, 0.05, 0.05), 1000.0)
+    w.add_distance_joints([(p, bob, (0, 0, 0), (0, 0, 0), 1.0, 0.0, 0.0)])
+    worst = 0.0
+    for _ in range(600):
+        w.step(1.0 / 60.0)
+        worst = max(worst, abs(float(np.linalg.norm(np.array(w.pose(bob)[0]) - np.array([0.0, 10.0, 0.0]))) - 1.0))
+    assert worst < 0.002, f"rigid distance joint stretched {worst:.4f} m"
+    w.close()
+
+
+def _f32(x):
+    return np.float32(x)
+
+
+def _glam_qmul(a, b):
+    """glam's SSE2 Quat product (lane order (w0 b + x0 b1) + (y0 b2 + z0 b3)) in f32."""
+    ax, ay, az, aw = (_f32(v) for v in a)
+    bx, by, bz, bw = (_f32(v) for v in b)
+    return ((aw * bx + ax * bw) + (ay * bz - az * by),
+            (aw * by - ax * bz) + (ay * bw + az * bx),
+            (aw * bz + ax * by) + (-(ay * bx) + az * bw),
+            (aw * bw - ax * bx) + (-(ay * by) - az * bz))
+
+
+DISTANCE_GOLDEN = {  # distance_bits_test.rs:52-55, recorded from the reference binary
+    (0, 60.0): 0x87F81A83F9615530, (0, 240.0): 0xE7411745726C1915,
+    (1, 60.0): 0x6F111D612DA3E10F, (1, 240.0): 0xED532E5E87913E18,
+}
+
+
+def distance_golden_scene(lib, kind, hz):
+    """distance_bits_test.rs:21-48 through the C ABI: a 0.2 x 0.1 x 0.16 m box of density 500 on a
+    distance joint from a static pivot at (0, 5, 0) (a 2 cm box here: the FFI gives every body a
+    collider; a jointed pair makes no contact), kind 0 rigid at its start length, kind 1 a spring
+    (2e-3 m/N) at 0.8 of it; 3 s at hz. Returns bits(): the FNV-1a fold of the box's pose and
+    velocity bits."""
+    w = lib.world(8, 8)
+    w.set_gravity((0.0, -9.81, 0.0))
+    w.set_iterations(20, 20)
+    p = _body(w, (0.0, 5.0, 0.0), PIN, 1.0, dynamic=False)
+    h = _f32(0.3) * _f32(0.5), _f32(0.2) * _f32(0.5)
+    qy = (0.0, _f32(math.sin(float(h[0]))), 0.0, _f32(math.cos(float(h[0]))))
+    qx = (_f32(math.sin(float(h[1]))), 0.0, 0.0, _f32(math.cos(float(h[1]))))
+    rot = tuple(float(v) for v in _glam_qmul(qy, qx))
+    start = (0.7, 4.3, 0.2)
+    b = _body(w, start, (0.1, 0.05, 0.08), 500.0, rot=rot, lin=(0.0, 0.5, 1.5), ang=(0.4, -1.0, 2.0), sleep=False)
+    d = np.array(start, dtype=np.float32) - np.array([0.0, 5.0, 0.0], dtype=np.float32)
+    rest = np.sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2])
+    if kind == 0:
+        w.add_distance_joints([(p, b, (0, 0, 0), (0, 0, 0), float(rest), 0.0, 0.0)])
+    else:
+        w.add_distance_joints([(p, b, (0, 0, 0), (0, 0, 0), float(rest * _f32(0.8)), 2.0e-3, 0.0)])
+    dt = float(_f32(1.0) / _f32(hz))
+    for _ in range(int(3.0 * hz)):
+        w.step(dt)
+    (pos, q), (lin, ang) = w.pose(b), w.velocity(b)
+    hsh = 0xCBF29CE484222325
+    for x in list(pos) + list(q) + list(lin) + list(ang):
+        hsh = ((hsh ^ int(np.float32(x).view(np.uint32))) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    w.close()
+    return hsh
+
+
+def case_distance_joint_scenes_keep_the_reference_bits(lib):
+    """distance_bits_test.rs:48-63: the reference binary's golden bits, through the C ABI."""
+    for (kind, hz), want in sorted(DISTANCE_GOLDEN.items()):
+        got = distance_golden_scene(lib, kind, hz)
+        assert got == want, f"kind {kind} {hz} Hz: {got:016x}, reference {want:016x}"
+
+
+def case_distance_joint_api_errors(lib):
+    """Argument checks of rphys_ext_add_distance_joints (all-or-nothing)."""
+    w = lib.world(4, 4)
+    a = _body(w, (0.0, 1.0, 0.0), (0.5, 0.5, 0.5), 1000.0)
+    b = _body(w, (2.0, 1.0, 0.0), (0.5, 0.5, 0.5), 1000.0)
+    bad = [
+        (a, a, (0, 0, 0), (0, 0, 0), 1.0, 0.0, 0.0),
+        (a, 99, (0, 0, 0), (0, 0, 0), 1.0, 0.0, 0.0),
+        (a, b, (float("nan"), 0, 0), (0, 0, 0), 1.0, 0.0, 0.0),
+        (a, b, (0, 0, 0), (0, 0, 0), float("inf"), 0.0, 0.0),
+        (a, b, (0, 0, 0), (0, 0, 0), 1.0, -1.0, 0.0),
+        (a, b, (0, 0, 0), (0, 0, 0), 1.0, 0.0, -2.0),
+    ]
+    for j in bad:
+        try:
+            w.add_distance_joints([(a, b, (0, 0, 0), (0, 0, 0), 2.0, 0.0, 0.0), j])
+        except rp.RPhysError:
+            pass
+        else:
+            raise AssertionError(f"accepted {j}")
+    assert w.num_joints() == 0
+    assert w.add_distance_joints([(a, b, (0.1, 0, 0), (0, 0, 0), 2.0, 1e-3, 5.0)]) == 0
     w.step(1.0 / 60.0)
     w.close()

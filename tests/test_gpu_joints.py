@@ -82,6 +82,57 @@ def _d6_chain(rp_, w, hz=120.0):
     return 1.0 / hz, w.num_bodies()
 
 
+def _distance_scene(rp_, w, hz=120.0):
+    """Distance joints of every kind under falling boxes: a rigid centre-to-centre rod, a sprung
+    one, an anchored rigid rod (torque through its lever arms), an anchored damped spring, and a
+    chain mixing them with a ball joint."""
+    w.set_gravity((0.0, -9.81, 0.0))
+    pins = [(-6.0, 8.0, 0.0), (-3.0, 8.0, 0.0), (0.0, 8.0, 0.0), (3.0, 8.0, 0.0), (6.0, 8.0, 0.0)]
+    d = rp_.desc_array(np.array(pins), np.tile([0.0, 0.0, 0.0, 1.0], (5, 1)), np.full((5, 3), 0.02), rp_.SHAPE_BOX,
+                       np.ones(5), np.zeros(5, dtype=np.uint32))
+    p0 = w.add_bodies_array(d)
+    rng = np.random.default_rng(3)
+    bobs = []
+    for k in range(5):
+        x, y, z = pins[k]
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        bd = rp_.desc_array(np.array([[x + 0.6, y - 0.8, 0.3]]), q[None, :], np.array([[0.15, 0.1, 0.2]]), rp_.SHAPE_BOX,
+                            np.array([600.0]), np.ones(1, dtype=np.uint32), sleep_allowed=0,
+                            lin=np.array([[0.0, 0.0, 1.0]]), ang=np.array([[0.5, -1.0, 1.5]]))
+        bobs.append(w.add_bodies_array(bd))
+    w.add_distance_joints([
+        (p0, bobs[0], (0, 0, 0), (0, 0, 0), 1.0, 0.0, 0.0),
+        (p0 + 1, bobs[1], (0, 0, 0), (0, 0, 0), 0.9, 4.0e-3, 0.0),
+        (p0 + 2, bobs[2], (0, 0, 0), (0.1, 0.05, -0.1), 1.1, 0.0, 0.0),
+        (p0 + 3, bobs[3], (0.0, -0.01, 0.0), (-0.1, 0.1, 0.0), 0.8, 2.0e-3, 3.0),
+        (p0 + 4, bobs[4], (0, 0, 0), (0, 0, 0), 1.0, 0.0, 0.0),
+    ])
+    # a second link below the last bob: a ball joint then a sprung rod
+    bd = rp_.desc_array(np.array([[6.6, 6.2, 0.3], [6.6, 5.0, 0.3]]), np.tile([0.0, 0.0, 0.0, 1.0], (2, 1)),
+                        np.full((2, 3), 0.12), rp_.SHAPE_BOX, np.full(2, 700.0), np.ones(2, dtype=np.uint32))
+    c0 = w.add_bodies_array(bd)
+    w.add_joints([(rp_.JOINT_BALL, bobs[4], c0, ((0.0, -0.3, 0.0), (0, 0, 0, 1)), ((0.0, 0.3, 0.0), (0, 0, 0, 1)), 0)])
+    w.add_distance_joints([(c0, c0 + 1, (0, -0.1, 0), (0, 0.1, 0), 1.0, 1.0e-3, 0.0)])
+    g = rp_.desc_array(np.array([[0.0, -0.5, 0.0]]), np.array([[0.0, 0.0, 0.0, 1.0]]), np.array([[20.0, 0.5, 20.0]]),
+                       rp_.SHAPE_BOX, np.array([0.0]), np.array([0], dtype=np.uint32))
+    w.add_bodies_array(g)
+    m = 8
+    bp = np.column_stack([rng.uniform(-6.0, 6.0, m), rng.uniform(9.0, 12.0, m), rng.uniform(-0.2, 0.6, m)])
+    bd = rp_.desc_array(bp, np.tile([0.0, 0.0, 0.0, 1.0], (m, 1)), np.full((m, 3), 0.2), rp_.SHAPE_BOX,
+                        np.full(m, 500.0), np.ones(m, dtype=np.uint32))
+    w.add_bodies_array(bd)
+    return 1.0 / hz, w.num_bodies()
+
+
+def test_distance_joints(oracle, gpu):
+    run_pair(oracle, gpu, {"cap": (32, 32), "fn": lambda rp_, w: _distance_scene(rp_, w)}, 600)
+
+
+def test_distance_joints_60hz(oracle, gpu):
+    run_pair(oracle, gpu, {"cap": (32, 32), "fn": lambda rp_, w: _distance_scene(rp_, w, 60.0)}, 300)
+
+
 def test_d6_feature_chain(oracle, gpu):
     run_pair(oracle, gpu, {"cap": (32, 32), "fn": lambda rp_, w: _d6_chain(rp_, w)}, 600)
 

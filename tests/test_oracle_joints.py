@@ -19,3 +19,12 @@ def test_shake_turned_threshold(oracle):
     f.restype, f.argtypes = ctypes.c_uint32, [ctypes.c_uint32]
     assert f(0x3F780AA6) == 0
     assert f(0x3F780AA5) > 0 and f(0x3F780AA7) > 0  # the neighbours of the threshold do not agree
+
+
+def test_shake_max_turn_cos_bits(oracle):
+    """The GPU's distance-joint position solve compares against SHAKE_MAX_TURN.cos() (bodies.rs:520)
+    as the constant 0x3f60a940; the oracle computes it with the project's cosine."""
+    import ctypes
+    f = oracle.dll.rphys_oracle_shake_max_turn_cos_bits
+    f.restype, f.argtypes = ctypes.c_uint32, []
+    assert f() == 0x3F60A940
