@@ -252,9 +252,16 @@ static void legacy_distance_row(const World& w, const Joint& j, uint32_t joint, 
   out.push_back(r);
 }
 void joint_rows(const World& w, const Joint& j, uint32_t joint, float dt, std::vector<JRow>& out) {
+  const size_t s0 = out.size();
   if (j.kind == 0) d6_rows(w, j, joint, dt, out);
   else if (j.anchored()) distance_rows(w, j, joint, out);
   else legacy_distance_row(w, j, joint, dt, out);
+  float wa = w.inv_mass[j.a], wb = w.inv_mass[j.b];
+  if (out.size() == s0 && (wa > 0.0f || wb > 0.0f)) {
+    JRow r{j.a, j.b, joint, false, V3{0, 0, 0}, V3{0, 0, 0}, V3{0, 0, 0}, wa, wb, 1.0f, 0.0f, -INFINITY, INFINITY, 0};
+    r.carrier = true;
+    out.push_back(r);
+  }
 }
 
 float joint_row_vel(const World& w, const JRow& r) {
@@ -274,6 +281,7 @@ void joint_row_apply(World& w, const JRow& r, float lam) {
   }
 }
 float joint_row_update(World& w, const JRow& r, float& acc) {
+  if (r.carrier) return 0.0f;
   if (r.legacy) {
     float v_rel = dot(sub(w.lin[r.b], w.lin[r.a]), r.u);
     float j_mag = -(v_rel + r.bias) / r.inv_sum;

@@ -22,6 +22,10 @@ struct JRow {
   // the linear velocities, bias = (len - rest) 0.1 / dt, no accumulation and no clamp
   bool legacy = false;
   float bias = 0.0f, inv_sum = 0.0f;
+  // a joint with no velocity row (a spring, or every row skipped) still solves at position level:
+  // its one carrier row puts it in the schedule (a task of the reference's joint batches, which
+  // hold every active joint, solver.rs:666-679) and does nothing in the velocity solve
+  bool carrier = false;
 };
 
 // d6_hinge_axis (bodies.rs:891-901) at the restated feature set: -1 for none.

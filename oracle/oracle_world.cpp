@@ -1118,7 +1118,7 @@ void World::step(float dt) {
     // rows start cold (:704-705)
     for (uint32_t jk = 0; jk < (uint32_t)joints.size(); ++jk) {
       uint32_t s = jrange[jk].first, e = jrange[jk].second;
-      if (e == s || joints[jk].kind != 0) continue;
+      if (e == s || joints[jk].kind != 0 || jrows[s].carrier) continue;
       auto it = warm_joints.find(jk);
       if (it == warm_joints.end()) continue;
       const WarmJointRows& prev = it->second;
@@ -1330,7 +1330,7 @@ void World::step(float dt) {
     // are not kept
     for (uint32_t jk = 0; jk < (uint32_t)joints.size(); ++jk) {
       uint32_t s = jrange[jk].first, e = jrange[jk].second;
-      if (e == s || joints[jk].kind != 0) continue;
+      if (e == s || joints[jk].kind != 0 || jrows[s].carrier) continue;
       WarmJointRows rows;
       for (uint32_t k = s; k < e; ++k) rows.push_back({jrows[k].tag, jacc[k]});
       warm_joints[jk] = rows;

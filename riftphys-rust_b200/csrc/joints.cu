@@ -59,7 +59,7 @@ __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, Bodie
     if (k == 0) { dyn_a = r.wa > 0.0f; dyn_b = r.wb > 0.0f; }
     R.ab[i] = make_uint2(jt.a, jt.b);
     R.flags[i] = RF_JOINT | (r.angular ? RF_JANG : 0u) | (r.wa > 0.0f ? RF_WA : 0u) | (r.wb > 0.0f ? RF_WB : 0u) |
-                 (k == 0 ? RF_JFIRST : 0u) | (r.legacy ? RF_JLEG : 0u);
+                 (k == 0 ? RF_JFIRST : 0u) | (r.legacy ? RF_JLEG : 0u) | (r.carrier ? RF_JNULL : 0u);
     R.inv[i] = make_float2(r.wa, r.wb);
     R.ra[i] = f4(r.ra, r.m_eff);
     R.rb[i] = f4(r.rb, r.inv_sum);
@@ -75,7 +75,8 @@ __global__ void k_joint_build(uint32_t nj, const JointGpu* __restrict__ J, Bodie
   });
   if (n == 0) return;
   R.t1[r0].x = (float)n;
-  if (tags_match && wn == n && !(jt.flags & JF_DIST)) {  // distance rows start cold (solver.rs:704-705)
+  // distance rows start cold (solver.rs:704-705); a carrier row is no row
+  if (tags_match && wn == n && !(jt.flags & JF_DIST) && !(R.flags[r0] & RF_JNULL)) {
     for (uint32_t k = 0; k < n; ++k) {
       const uint32_t i = r0 + k;
       const float4 mu = R.mu[i];
@@ -101,7 +102,8 @@ __global__ void k_joint_store(uint32_t nj, const JointGpu* __restrict__ J, const
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nj) return;
   uint32_t n = cnt[j];
-  if (n == 0 || (J[j].flags & JF_DIST)) return;  // distance rows are not kept (solver.rs:945-947)
+  // distance rows are not kept (solver.rs:945-947); a carrier row is no row
+  if (n == 0 || (J[j].flags & JF_DIST) || (R.flags[base + off[j]] & RF_JNULL)) return;
   jw_n[j] = n;
   for (uint32_t k = 0; k < n; ++k) {
     uint32_t r = base + off[j] + k;

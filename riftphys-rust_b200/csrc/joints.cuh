@@ -44,6 +44,7 @@ struct JRowD {
   bool angular;
   bool legacy = false;
   float bias = 0.0f, inv_sum = 0.0f;
+  bool carrier = false;  // a joint's one row when it has no velocity row (RF_JNULL)
 };
 __host__ __device__ inline bool jaxis_on(uint32_t f, int ax) { return (f >> ax) & 1u; }
 __host__ __device__ inline bool jaxis_lim(uint32_t f, int ax) { return (f >> (JF_LIMIT_SHIFT + ax)) & 1u; }
@@ -203,11 +204,22 @@ __device__ __forceinline__ uint32_t distance_rows_dev(const JointGpu& j, const B
   emit(r, 0u);
   return 1;
 }
-// A joint's velocity rows whatever its kind (solver.rs:655-661).
+// A joint's velocity rows whatever its kind (solver.rs:655-661); a joint with a dynamic body and
+// no row gets one carrier row, which puts it in the schedules for its position solve (a task of
+// the reference's joint batches, which hold every active joint) and does nothing at velocity level.
 template <class Emit>
 __device__ __forceinline__ uint32_t joint_rows_dev(const JointGpu& j, const BodiesV& B, float dt, Emit&& emit) {
-  if (j.flags & JF_DIST) return distance_rows_dev(j, B, dt, emit);
-  return d6_rows_dev(j, B, dt, emit);
+  uint32_t n = (j.flags & JF_DIST) ? distance_rows_dev(j, B, dt, emit) : d6_rows_dev(j, B, dt, emit);
+  const float wa = B.inv_mass[j.a], wb = B.inv_mass[j.b];
+  if (n == 0 && (wa > 0.0f || wb > 0.0f)) {
+    JRowD r;
+    r.u = mk3(0, 0, 0); r.ra = mk3(0, 0, 0); r.rb = mk3(0, 0, 0); r.wa = wa; r.wb = wb; r.m_eff = 1.0f;
+    r.target = 0.0f; r.lo = -INFINITY; r.hi = INFINITY; r.gamma = 0.0f; r.tag = 0; r.angular = false;
+    r.carrier = true;
+    emit(r, 0u);
+    n = 1;
+  }
+  return n;
 }
 
 // ---- the position solve (bodies.rs:616-873) on the bodies' global pose arrays

@@ -11,10 +11,12 @@ namespace rp {
 // (levels, solve islands) without receiving impulses. RF_JOINT: a joint velocity row (RF_JANG:
 // angular; RF_JWARM: warm-started from the previous tick; RF_JFIRST: the joint's first row, which
 // carries the joint's position solve in the position pass; RF_JLEG: the original distance row,
-// impulse -(v_rel + bias) / inv_sum on the linear velocities, bias in t1.w, inv_sum in rb.w).
+// impulse -(v_rel + bias) / inv_sum on the linear velocities, bias in t1.w, inv_sum in rb.w;
+// RF_JNULL: the carrier row of a joint with no velocity row, which puts the joint in the schedules
+// for its position solve and does nothing in the velocity solve).
 enum : uint32_t {
   RF_TERRAIN = 1, RF_TOI = 4, RF_WA = 8, RF_WB = 16, RF_RA = 32, RF_RB = 64,
-  RF_JOINT = 128, RF_JANG = 256, RF_JWARM = 512, RF_JFIRST = 1024, RF_JLEG = 2048
+  RF_JOINT = 128, RF_JANG = 256, RF_JWARM = 512, RF_JFIRST = 1024, RF_JLEG = 2048, RF_JNULL = 4096
 };
 #define RF_TA (RF_WA | RF_RA)
 #define RF_TB (RF_WB | RF_RB)

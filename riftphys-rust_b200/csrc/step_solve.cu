@@ -272,6 +272,7 @@ __device__ __forceinline__ float legacy_row_glob(const BodiesV& B, const Row& r)
   return j_mag;
 }
 __device__ __forceinline__ float joint_row_glob(const BodiesV& B, const Row& r, uint32_t k, float* acc_jn) {
+  if (r.flags & RF_JNULL) return 0.0f;
   if (r.flags & RF_JLEG) return fabsf(legacy_row_glob(B, r)) / r.m_n;
   f3 va, vb;
   if (r.flags & RF_JANG) { va = xyz(B.ang[r.ai]); vb = xyz(B.ang[r.bi]); }
@@ -1264,6 +1265,12 @@ __device__ __noinline__ void joint_row_core(float4* lin, float4* ang, const SRow
   if (ha) { LA = lin[r.la]; AA = ang[r.la]; }
   if (hb) { LB = lin[r.lb]; AB = ang[r.lb]; }
   f3 la = xyz(LA), aa = xyz(AA), lb = xyz(LB), ab = xyz(AB);
+  if (r.flags & RF_JNULL) {
+    d3[0] = 0.0f;
+    d3[1] = 0.0f;
+    d3[2] = 0.0f;
+    return;
+  }
   if (r.flags & RF_JLEG) {
     d3[0] = legacy_row_reg(la, lb, ha, hb, r, ima, imb);
     d3[1] = 0.0f;
@@ -1305,6 +1312,12 @@ __device__ __noinline__ void joint_unit_core(float4* lin, float4* ang, const SRo
   bool moved = false;
   for (uint32_t q = 0; q < cnt; ++q) {
     const SRow& r = rows[q];
+    if (r.flags & RF_JNULL) {
+      dres[3 * q] = 0.0f;
+      dres[3 * q + 1] = 0.0f;
+      dres[3 * q + 2] = 0.0f;
+      continue;
+    }
     if (r.flags & RF_JLEG) {
       dres[3 * q] = legacy_row_reg(la, lb, ha, hb, r, ima, imb);
       dres[3 * q + 1] = 0.0f;
