@@ -75,7 +75,7 @@ typedef struct RPhysStepStats {
     uint32_t max_batch;      /* largest level (World::last_max_batch().0 without joints) */
     uint32_t warm_matched;   /* contacts started warm (World::warm_matched) */
     uint32_t sweeps;         /* velocity sweeps run in the last tick */
-    uint32_t bounce_skipped; /* rows that would take the W6 bounce passes (solved inelastic here) */
+    uint32_t bounce_rows;    /* rows the W6 bounce pass solved at their time of impact (BounceStats::toi_rows) */
     uint32_t warm_entries;   /* entries in the warm-start cache (World::warm_contacts) */
     uint32_t sleeping;       /* bodies asleep (World::num_sleeping) */
     uint32_t error_flags;    /* RPHYS_STATERR_* */

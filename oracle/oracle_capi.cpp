@@ -696,7 +696,7 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
   std::memset(o, 0, sizeof(*o));
   o->pairs = s.pairs; o->contacts = s.contacts; o->islands = s.islands; o->levels = s.levels;
   o->max_batch = s.max_batch; o->warm_matched = s.warm_matched; o->sweeps = s.sweeps;
-  o->bounce_skipped = s.bounce_skipped; o->residual = s.residual;
+  o->bounce_rows = s.bounce_rows; o->residual = s.residual;
   o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
   o->islands_capped = s.islands_capped;
   o->pred_used = s.pred_used;

@@ -2,6 +2,7 @@
 // reference's World::step; see oracle_world.h for scope. Every function cites the reference
 // lines it follows (paths relative to the reference's crates/ directory).
 #include "oracle_world.h"
+#include "oracle_bounce.h"
 #include "oracle_joints.h"
 
 #include <algorithm>
@@ -781,6 +782,9 @@ struct CC {
   float mu_s, mu_k, sv;
   float depth_bias, restitution_bias;
   bool soft, toi;
+  // W6 (solver.rs:575-587): the gap at the step's start, the pair's restitution, and each side's
+  // normal velocity at the contact from the start velocities and after this step's forces
+  float toi_s0, toi_e, toi_va0, toi_va1, toi_vb0, toi_vb1;
 };
 // orthonormal_basis (riftphys-world/src/world/geom.rs:30-38)
 static void orthonormal_basis(V3 n, V3* t1, V3* t2) {
@@ -835,6 +839,273 @@ static uint32_t level_schedule(const std::vector<CC>& cs, const std::vector<uint
 }
 
 // ------------------------------------------------------------------ the tick
+// ------------------------------------------------------------------ W6 bounce passes
+// toi_bounce (solver.rs:203-219): the end-of-step normal velocity of a bounce found at its time of
+// impact inside the step and, when the pair started apart, the pseudo-velocity that moves it to
+// where the bounce leaves it.
+static void toi_bounce(float s0, float v0, float a, float e, float dt, float* v_end_out, bool* has_pseudo, float* pseudo) {
+  float t_c;
+  if (s0 <= 0.0f) {
+    t_c = 0.0f;
+  } else {
+    float disc = v0 * v0 - 2.0f * a * s0;
+    float den = disc >= 0.0f ? -v0 + std::sqrt(disc) : 0.0f;
+    t_c = den > 0.0f ? rmin(2.0f * s0 / den, dt) : dt;
+  }
+  float v_out = rmax(-e * (v0 + a * t_c), 0.0f);
+  float tau = dt - t_c;
+  float rise = v_out * tau + 0.5f * a * tau * tau;
+  float v_end, s_end;
+  if (rise < 0.0f) { v_end = 0.0f; s_end = 0.0f; }
+  else { v_end = rmax(v_out + a * tau, 0.0f); s_end = rise; }
+  *v_end_out = v_end;
+  *has_pseudo = s0 > 0.0f;
+  *pseudo = (s_end - s0) / dt - v_end;
+}
+// row_sides (solver.rs:117-134): a side that cannot move (no inverse mass, zero inverse inertia)
+// is none; the world inverse inertia symmetrised in f64.
+static std::array<bounce::RowSide, 2> row_sides(const CC& cs) {
+  using namespace bounce;
+  const D3 n{cs.n.x, cs.n.y, cs.n.z};
+  auto side = [&](uint32_t body, double sign, V3 r, float inv, const M3& ii) {
+    RowSide s{};
+    if (inv <= 0.0f && mis_zero(ii)) { s.body = kNone; return s; }
+    s.body = body;
+    s.jl = dmul(n, sign);
+    s.ja = dmul(dcross(D3{r.x, r.y, r.z}, n), sign);
+    auto c = [](V3 v) { return D3{v.x, v.y, v.z}; };
+    DM3 m{c(ii.c0), c(ii.c1), c(ii.c2)};
+    DM3 mt{D3{m.c0.x, m.c1.x, m.c2.x}, D3{m.c0.y, m.c1.y, m.c2.y}, D3{m.c0.z, m.c1.z, m.c2.z}};
+    DM3 ms{dmul(dadd(m.c0, mt.c0), 0.5), dmul(dadd(m.c1, mt.c1), 0.5), dmul(dadd(m.c2, mt.c2), 0.5)};
+    s.mjl = dmul(s.jl, (double)inv);
+    s.mja = dmvec(ms, s.ja);
+    return s;
+  };
+  return {side(cs.ai, -1.0, cs.ra, cs.inv_a, cs.ii_a), side(cs.terrain ? kNone : cs.bi, 1.0, cs.rb, cs.inv_b, cs.ii_b)};
+}
+// The W6 bounce passes (solver.rs:1009-1241) for free bodies' contacts approaching faster than
+// 1 m/s with restitution: each bounces at its time of impact (its end-of-step velocity target from
+// toi_bounce), with the bounced bodies' other loaded contacts as push-only supports, solved per
+// connected component by the interior-point LCP (up to 250 rows) or swept; then the pseudo pass
+// moves the bounced pairs to where the bounce leaves them (pseudo-velocities for the integration).
+static constexpr size_t kDirectMax = 250, kBounceSweeps = 256, kBounceSolves = 64;
+static constexpr float kBounceTol = 1e-6f;
+static void w6_bounce(World& w, const std::vector<CC>& cons, std::vector<float>& acc_jn, const std::vector<float>& acc_jt,
+                      const std::vector<uint8_t>& jointed, float dt, uint32_t num_bodies,
+                      std::vector<std::pair<V3, V3>>& pseudo_out, uint32_t* n_toi) {
+  using namespace bounce;
+  const size_t nc = cons.size();
+  auto loaded_at = [&](size_t c, const std::vector<float>& jn) {
+    return jn[c] > 0.0f || acc_jt[2 * c] != 0.0f || acc_jt[2 * c + 1] != 0.0f;
+  };
+  auto grow = [&](std::vector<uint8_t>& involved, const std::vector<float>& jn) {
+    for (;;) {
+      bool changed = false;
+      for (size_t c = 0; c < nc; ++c) {
+        const CC& cs = cons[c];
+        if (cs.soft || cs.terrain || !loaded_at(c, jn)) continue;
+        const uint32_t xs[2] = {cs.ai, cs.bi}, ys[2] = {cs.bi, cs.ai};
+        const float invy[2] = {cs.inv_b, cs.inv_a};
+        for (int k = 0; k < 2; ++k)
+          if (involved[xs[k]] && !involved[ys[k]] && invy[k] > 0.0f && !jointed[ys[k]]) {
+            involved[ys[k]] = 1;
+            changed = true;
+          }
+      }
+      if (!changed) break;
+    }
+  };
+  auto partner = [&](const CC& cs, uint32_t id) { return cs.terrain ? 0xFFFFFFFFu : (id == cs.ai ? cs.bi : cs.ai); };
+  // cs with jointed bodies immovable and its normal effective mass; false if neither side moves
+  auto free_only = [&](const CC& in, CC* out) {
+    CC cs = in;
+    if (jointed[cs.ai]) { cs.inv_a = 0.0f; cs.ii_a = mzero(); }
+    if (cs.terrain || jointed[cs.bi]) { cs.inv_b = 0.0f; cs.ii_b = mzero(); }
+    V3 ca = cross(cs.ra, cs.n), cb = cross(cs.rb, cs.n);
+    float k = ((cs.inv_a + cs.inv_b) + dot(ca, mvec(cs.ii_a, ca))) + dot(cb, mvec(cs.ii_b, cb));
+    if (!(k > 1e-9f)) return false;
+    cs.m_n = 1.0f / k;
+    *out = cs;
+    return true;
+  };
+  std::vector<uint8_t> toi_set(nc, 0);
+  bool any = false;
+  for (size_t c = 0; c < nc; ++c) {
+    toi_set[c] = cons[c].toi && cons[c].restitution_bias > 0.0f && acc_jn[c] > 0.0f;
+    any = any || toi_set[c];
+  }
+  std::vector<std::pair<size_t, float>> toi_rows, pseudo_rows;
+  if (any) {
+    std::vector<std::vector<uint32_t>> rests_on(num_bodies);
+    for (size_t c = 0; c < nc; ++c) {
+      const CC& cs = cons[c];
+      if (toi_set[c] || !loaded_at(c, acc_jn)) continue;
+      rests_on[cs.ai].push_back(partner(cs, cs.ai));
+      if (!cs.terrain) rests_on[cs.bi].push_back(partner(cs, cs.bi));
+    }
+    for (size_t c = 0; c < nc; ++c) {
+      if (!toi_set[c]) continue;
+      const CC& cs = cons[c];
+      // a side resting on something other than its partner is struck from its start velocity
+      auto side = [&](uint32_t id, float start, float after, float* s0, float* s1) {
+        uint32_t other = partner(cs, id);
+        bool rests = false;
+        for (uint32_t p : rests_on[id]) rests = rests || p != other;
+        *s0 = start;
+        *s1 = rests ? start : after;
+      };
+      float a0, a1, b0 = 0.0f, b1 = 0.0f;
+      side(cs.ai, cs.toi_va0, cs.toi_va1, &a0, &a1);
+      if (!cs.terrain) side(cs.bi, cs.toi_vb0, cs.toi_vb1, &b0, &b1);
+      float v0 = b0 - a0;
+      float acc = ((b1 - a1) - v0) / dt;
+      float v_end, u;
+      bool hp;
+      toi_bounce(cs.toi_s0, v0, acc, cs.toi_e, dt, &v_end, &hp, &u);
+      toi_rows.push_back({c, v_end});
+      if (hp) pseudo_rows.push_back({c, u});
+    }
+    std::vector<uint8_t> involved(num_bodies, 0);
+    for (auto& tr : toi_rows) {
+      const CC& cs = cons[tr.first];
+      involved[cs.ai] = 1;
+      if (!cs.terrain) involved[cs.bi] = 1;
+    }
+    grow(involved, acc_jn);
+    // one list: the bounces (accumulating into acc_jn), then the supports (fresh accumulators)
+    struct BRow { CC cs; float target; long c; };
+    std::vector<BRow> rows;
+    for (auto& tr : toi_rows) rows.push_back(BRow{cons[tr.first], tr.second, (long)tr.first});
+    for (size_t c = 0; c < nc; ++c) {
+      const CC& cs = cons[c];
+      if (toi_set[c] || cs.soft || acc_jn[c] <= 0.0f) continue;
+      if (!involved[cs.ai] && (cs.terrain || !involved[cs.bi])) continue;
+      CC row;
+      if (!free_only(cs, &row)) continue;
+      rows.push_back(BRow{row, rmin(cs.depth_bias, 0.0f), -1});
+    }
+    std::vector<float> sup_acc(rows.size(), 0.0f);
+    std::vector<std::array<RowSide, 2>> sides_all;
+    for (auto& r : rows) sides_all.push_back(row_sides(r.cs));
+    for (auto& comp : row_components(sides_all, num_bodies)) {
+      const size_t n = comp.size();
+      bool sweep = n > kDirectMax;
+      auto acc_of = [&](size_t i) -> float& { return rows[i].c >= 0 ? acc_jn[(size_t)rows[i].c] : sup_acc[i]; };
+      if (!sweep) {
+        std::vector<std::array<RowSide, 2>> sides;
+        for (size_t i : comp) sides.push_back(sides_all[i]);
+        Csr k = contact_csr(sides);
+        std::vector<double> b, acc0;
+        for (size_t i : comp) {
+          b.push_back((double)(rows[i].target - dot(contact_rel_vel(w, rows[i].cs), rows[i].cs.n)));
+          acc0.push_back((double)acc_of(i));
+        }
+        QpResult qr = bounce_qp(k, b, acc0, kBounceSolves);
+        sweep = !qr.converged;
+        for (size_t q = 0; q < n; ++q) {
+          size_t i = comp[q];
+          float old = acc_of(i);
+          float nw = rmax((float)((double)old + qr.x[q]), 0.0f);
+          acc_of(i) = nw;
+          apply_contact_impulse(w, rows[i].cs, mul(rows[i].cs.n, nw - old));
+        }
+      }
+      if (!sweep) continue;
+      for (size_t it = 0; it < kBounceSweeps; ++it) {
+        float change = 0.0f;
+        for (size_t m = 0; m < n; ++m) {
+          size_t i = comp[it % 2 == 0 ? m : n - 1 - m];
+          const CC& row = rows[i].cs;
+          float v = dot(contact_rel_vel(w, row), row.n);
+          float old = acc_of(i);
+          float nw = rmax(old + (rows[i].target - v) * row.m_n, 0.0f);
+          acc_of(i) = nw;
+          apply_contact_impulse(w, row, mul(row.n, nw - old));
+          change = rmax(change, std::fabs(nw - old) / row.m_n / (1.0f + std::fabs(rows[i].target)));
+        }
+        if (change < kBounceTol) break;
+      }
+    }
+  }
+  *n_toi = (uint32_t)toi_rows.size();
+  // 3c. the pseudo pass (:1161-1241)
+  if (pseudo_rows.empty()) return;
+  std::vector<uint8_t> in_set(nc, 0), involved(num_bodies, 0);
+  for (auto& pr : pseudo_rows) {
+    in_set[pr.first] = 1;
+    const CC& cs = cons[pr.first];
+    involved[cs.ai] = 1;
+    if (!cs.terrain) involved[cs.bi] = 1;
+  }
+  grow(involved, acc_jn);
+  std::vector<std::pair<CC, float>> rows;
+  for (auto& pr : pseudo_rows) {
+    CC row;
+    if (free_only(cons[pr.first], &row)) rows.push_back({row, pr.second});
+  }
+  for (size_t c = 0; c < nc; ++c) {
+    const CC& cs = cons[c];
+    if (in_set[c] || cs.soft || !loaded_at(c, acc_jn)) continue;
+    if (!involved[cs.ai] && (cs.terrain || !involved[cs.bi])) continue;
+    CC row;
+    if (free_only(cs, &row)) rows.push_back({row, 0.0f});
+  }
+  std::vector<std::pair<V3, V3>> pseudo(num_bodies, {V3{0, 0, 0}, V3{0, 0, 0}});
+  auto rel = [&](const CC& cs) {
+    V3 la = pseudo[cs.ai].first, wa = pseudo[cs.ai].second;
+    V3 lb = cs.terrain ? V3{0, 0, 0} : pseudo[cs.bi].first, wb = cs.terrain ? V3{0, 0, 0} : pseudo[cs.bi].second;
+    return dot(sub(add(lb, cross(wb, cs.rb)), add(la, cross(wa, cs.ra))), cs.n);
+  };
+  std::vector<std::array<RowSide, 2>> sides_all;
+  for (auto& r : rows) sides_all.push_back(row_sides(r.first));
+  std::vector<std::pair<D3, D3>> acc(num_bodies, {D3{0, 0, 0}, D3{0, 0, 0}});
+  std::vector<uint8_t> direct(num_bodies, 0);
+  for (auto& comp : row_components(sides_all, num_bodies)) {
+    const size_t n = comp.size();
+    if (n <= kDirectMax) {
+      std::vector<std::array<RowSide, 2>> sides;
+      for (size_t i : comp) sides.push_back(sides_all[i]);
+      Csr k = contact_csr(sides);
+      std::vector<double> u;
+      for (size_t i : comp) u.push_back((double)rows[i].second);
+      std::vector<double> x = pseudo_solve(k, u);
+      for (size_t q = 0; q < n; ++q)
+        for (auto& sd : sides[q]) {
+          if (sd.body == kNone) continue;
+          acc[sd.body].first = dadd(acc[sd.body].first, dmul(sd.mjl, x[q]));
+          acc[sd.body].second = dadd(acc[sd.body].second, dmul(sd.mja, x[q]));
+          direct[sd.body] = 1;
+        }
+      continue;
+    }
+    for (size_t it = 0; it < kBounceSweeps; ++it) {
+      float change = 0.0f;
+      for (size_t m = 0; m < n; ++m) {
+        const CC& cs = rows[comp[it % 2 == 0 ? m : n - 1 - m]].first;
+        float u = rows[comp[it % 2 == 0 ? m : n - 1 - m]].second;
+        float d = u - rel(cs);
+        change = rmax(change, std::fabs(d) / (1.0f + std::fabs(u)));
+        V3 j = mul(cs.n, d * cs.m_n);
+        if (cs.inv_a > 0.0f) {
+          pseudo[cs.ai].first = sub(pseudo[cs.ai].first, mul(j, cs.inv_a));
+          pseudo[cs.ai].second = sub(pseudo[cs.ai].second, mvec(cs.ii_a, cross(cs.ra, j)));
+        }
+        if (cs.inv_b > 0.0f) {
+          pseudo[cs.bi].first = add(pseudo[cs.bi].first, mul(j, cs.inv_b));
+          pseudo[cs.bi].second = add(pseudo[cs.bi].second, mvec(cs.ii_b, cross(cs.rb, j)));
+        }
+      }
+      if (change < kBounceTol) break;
+    }
+  }
+  for (uint32_t b = 0; b < num_bodies; ++b)
+    if (direct[b]) {
+      const D3 l = acc[b].first, a = acc[b].second;
+      pseudo[b] = {V3{(float)l.x, (float)l.y, (float)l.z}, V3{(float)a.x, (float)a.y, (float)a.z}};
+    }
+  pseudo_out = std::move(pseudo);
+}
+
 void World::step(float dt) {
   const uint32_t count = num_bodies();
   tick += 1;
@@ -1012,6 +1283,7 @@ void World::step(float dt) {
   }
   stats.islands = n_islands;
   std::vector<uint8_t> contact_loaded(count, 0);
+  std::vector<std::pair<V3, V3>> bounce_pseudo;  // W6 pseudo-velocities (empty: none this tick)
   std::vector<uint32_t> levels_out(nc, 0xFFFFFFFFu);
   const V3 up = len2(gravity) > 0.0f ? neg(normalize(gravity)) : V3{0, 1, 0};
   std::vector<CC> cons;
@@ -1051,9 +1323,24 @@ void World::step(float dt) {
       V3 vb_l = cs.terrain ? V3{0, 0, 0} : pre_lin[cs.bi], vb_a = cs.terrain ? V3{0, 0, 0} : pre_ang[cs.bi];
       float v_pre = dot(sub(add(vb_l, cross(vb_a, cs.rb)), add(va_l, cross(va_a, cs.ra))), cs.n);
       float v_rel_n = 0.5f * (v_pre + dot(contact_rel_vel(*this, cs), cs.n));
+      cs.toi_s0 = cs.toi_e = cs.toi_va0 = cs.toi_va1 = cs.toi_vb0 = cs.toi_vb1 = 0.0f;
       if (v_rel_n < -1.0f) {
         cs.restitution_bias = (-pp.restitution) * v_rel_n;
         cs.toi = !jointed[cs.ai] && (cs.terrain || !jointed[cs.bi]);  // W6: free bodies only
+        if (cs.toi) {
+          // the integrator's motion model: linear velocity from the end of last step (solver.rs:575-587)
+          auto at = [&](V3 l, V3 a, V3 r) { return dot(add(l, cross(a, r)), cs.n); };
+          V3 sl_a = cs.ai < last_lin_vel.size() ? last_lin_vel[cs.ai] : pre_lin[cs.ai];
+          cs.toi_va0 = at(sl_a, pre_ang[cs.ai], cs.ra);
+          cs.toi_va1 = at(lin[cs.ai], ang[cs.ai], cs.ra);
+          if (!cs.terrain) {
+            V3 sl_b = cs.bi < last_lin_vel.size() ? last_lin_vel[cs.bi] : pre_lin[cs.bi];
+            cs.toi_vb0 = at(sl_b, pre_ang[cs.bi], cs.rb);
+            cs.toi_vb1 = at(lin[cs.bi], ang[cs.bi], cs.rb);
+          }
+          cs.toi_s0 = -pen;
+          cs.toi_e = pp.restitution;
+        }
       }
     }
     // 2a. level schedule (:621-642)
@@ -1386,9 +1673,8 @@ void World::step(float dt) {
       acc_jn[k] = nw2;
       apply_contact_impulse(*this, cs, mul(cs.n, nw2 - old));
     }
-    // W6 bounce passes (:1047-1241): counted, not run
-    for (uint32_t k = 0; k < nc; ++k)
-      if (cons[k].toi && cons[k].restitution_bias > 0.0f && acc_jn[k] > 0.0f) stats.bounce_skipped++;
+    // W6 bounce passes (:1009-1241)
+    w6_bounce(*this, cons, acc_jn, acc_jt, jointed, dt, count, bounce_pseudo, &stats.bounce_rows);
     // contact_loaded (:1248-1256) and impulse write-back (:1268-1270)
     for (uint32_t k = 0; k < nc; ++k) {
       const CC& cs = cons[k];
@@ -1470,6 +1756,12 @@ void World::step(float dt) {
         va = w;
         set_vel(i, vl, va);
       }
+    }
+    // a bounced free body's pseudo-velocity (W6, step.rs:271-277): moves it, never enters its velocity
+    if (i < bounce_pseudo.size()) {
+      V3 pl = bounce_pseudo[i].first, pa = bounce_pseudo[i].second;
+      pose.pos = add(pose.pos, mul(pl, dt));
+      if (len2(pa) > 0.0f) pose.rot = qnormalize(qmul(qfrom_axis_angle(normalize(pa), len(pa) * dt), pose.rot));
     }
     set_pose(i, pose);
     predicted[i] = Iso{pos[i], rot[i]};

@@ -102,7 +102,7 @@ struct Snapshot {
 
 struct Stats {
   uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
-  uint32_t sweeps = 0, bounce_skipped = 0, row_sweeps = 0, rows_scheduled = 0;
+  uint32_t sweeps = 0, bounce_rows = 0, row_sweeps = 0, rows_scheduled = 0;
   uint32_t islands_capped = 0;  // residual mode: solve islands still above the tolerance at the cap
   uint32_t pred_used = 0;       // rows started from an offered prediction
   float residual = 0;

@@ -179,7 +179,7 @@ def limit_array(joint, angular, axis, lo, hi):
 
 class StepStats(Structure):
     _fields_ = [(n, c_uint32) for n in ("pairs", "contacts", "islands", "levels", "max_batch", "warm_matched",
-                                        "sweeps", "bounce_skipped", "warm_entries", "sleeping", "error_flags")] + \
+                                        "sweeps", "bounce_rows", "warm_entries", "sleeping", "error_flags")] + \
                [("residual", c_float), ("row_sweeps", c_uint32), ("rows_scheduled", c_uint32)] + \
                [(n, c_uint32) for n in ("groups_shared", "groups_global", "max_group_rows", "max_group_bodies",
                                         "islands_capped", "pred_used")]

@@ -789,7 +789,7 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
     const rp::StepStatsHost& s = W->w->stats();
     o->pairs = s.pairs; o->contacts = s.contacts; o->islands = s.islands; o->levels = s.levels;
     o->max_batch = s.max_batch; o->warm_matched = s.warm_matched; o->sweeps = s.sweeps;
-    o->bounce_skipped = s.bounce_skipped; o->warm_entries = s.warm_entries; o->sleeping = s.sleeping;
+    o->bounce_rows = s.bounce_rows; o->warm_entries = s.warm_entries; o->sleeping = s.sleeping;
     o->error_flags = s.error_flags; o->residual = s.residual;
     o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
     o->groups_shared = s.groups_shared; o->groups_global = s.groups_global;

@@ -524,7 +524,7 @@ const StepStatsHost& WorldGpu::stats() {
     RP_CUDA(cudaStreamSynchronize(stream_));
     st_.error_flags = h[STAT_ERR];
     st_.warm_matched = h[STAT_WARM_MATCHED];
-    st_.bounce_skipped = h[STAT_BOUNCE];
+    st_.bounce_rows = h[STAT_BOUNCE];
     st_.sweeps = h[STAT_SWEEPS];
     float r; std::memcpy(&r, &h[STAT_RESID], 4); st_.residual = r;
     st_.sleeping = h[STAT_SLEEPING];

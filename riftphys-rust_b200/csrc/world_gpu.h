@@ -28,7 +28,7 @@ constexpr uint32_t kJointRows = 32;
 
 struct StepStatsHost {
   uint32_t pairs = 0, contacts = 0, islands = 0, levels = 0, max_batch = 0, warm_matched = 0;
-  uint32_t sweeps = 0, bounce_skipped = 0, warm_entries = 0, sleeping = 0, error_flags = 0;
+  uint32_t sweeps = 0, bounce_rows = 0, warm_entries = 0, sleeping = 0, error_flags = 0;
   float residual = 0.0f;
   uint32_t row_sweeps = 0, rows_scheduled = 0;
   uint32_t groups_shared = 0, groups_global = 0, max_group_rows = 0, max_group_bodies = 0;

@@ -42,7 +42,7 @@ def run_pair(oracle, gpu, build, ticks, check_every=1):
         assert wo.hash() == wg.hash(), f"tick {t}: tick hash differs"
         sto, stg = wo.stats(), wg.stats()
         for k in ("pairs", "contacts", "islands", "levels", "max_batch", "warm_matched", "warm_entries", "sleeping",
-                  "bounce_skipped", "sweeps", "row_sweeps", "rows_scheduled", "islands_capped", "residual"):
+                  "bounce_rows", "sweeps", "row_sweeps", "rows_scheduled", "islands_capped", "residual"):
             assert sto[k] == stg[k], f"tick {t}: stat {k} {sto[k]} vs {stg[k]}"
     return wo, wg
 
