@@ -173,6 +173,15 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> sap_w, gp_cnt, gp_off;
   DBuf<float4> big_x, big_j;                                                   // big-island row stream
   DBuf<float> feat, pred3, targets;                                            // learned warm start
+  // W6 bounce passes: per contact the time-of-impact data, then the passes' scratch
+  DBuf<float4> toi_a;
+  DBuf<float2> toi_b;
+  DBuf<uint32_t> w6_rest_cnt, w6_rest_min, w6_rest_max, w6_parent, w6_slot, w6_rows, w6_comp_rows, w6_comp_start,
+      w6_row_comp, w6_cur, w6_ctr;
+  DBuf<uint8_t> w6_involved, w6_direct, w6_in_set, w6_has_pseudo, w6_pool;
+  DBuf<double> w6_acc;
+  DBuf<float4> w6_pl, w6_pa;
+  DBuf<float> w6_target, w6_sup_acc, w6_pseudo_u;
   DBuf<uint8_t> feat_valid;
   DBuf<float4> pred_used, s_pred;
   // solve groups (islands packed for one CTA each) and their shared-memory residents

@@ -94,7 +94,8 @@ __global__ void k_build_rows(uint32_t nc, float dt, const uint32_t* __restrict__
                              const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ cmat, uint32_t hf_mat,
                              const float* __restrict__ ptab, BodiesV B, const float4* __restrict__ pre_lin,
                              const float4* __restrict__ pre_ang, RowsV R, float* acc_jn, float2* acc_jt,
-                             const uint32_t* __restrict__ uf, uint32_t* row_root, const uint8_t* __restrict__ jointed) {
+                             const uint32_t* __restrict__ uf, uint32_t* row_root, const uint8_t* __restrict__ jointed,
+                             const float4* __restrict__ last_lin, float4* toi_a, float2* toi_b) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nc) return;
   bool terrain = c_b[k] == 0xFFFFFFFFu;
@@ -130,7 +131,19 @@ __global__ void k_build_rows(uint32_t nc, float dt, const uint32_t* __restrict__
   const bool ja = jointed && jointed[ai], jb = jointed && !terrain && jointed[bi];
   if (v_rel_n < -1.0f) {
     rbias = (-rest) * v_rel_n;
-    if (!ja && !jb) flags |= RF_TOI;  // W6: free bodies only (solver.rs:571-573)
+    if (!ja && !jb) {  // W6: free bodies bounce at their time of impact (solver.rs:571-587)
+      flags |= RF_TOI;
+      // each side's normal velocity at the contact from the integrator's start velocities (last
+      // step's linear, the start angular) and after this step's forces
+      auto at = [&](f3 l, f3 a, f3 r) { return dot(l + cross(a, r), n); };
+      float vb0 = 0.0f, vb1 = 0.0f;
+      if (!terrain) {
+        vb0 = at(xyz(last_lin[bi]), vba, rb);
+        vb1 = at(xyz(B.lin[bi]), xyz(B.ang[bi]), rb);
+      }
+      toi_a[k] = make_float4(-pen, rest, at(xyz(last_lin[ai]), vaa, ra), at(xyz(B.lin[ai]), xyz(B.ang[ai]), ra));
+      toi_b[k] = make_float2(vb0, vb1);
+    }
   }
   bool wa = inv_a > 0.0f, wb = !terrain && inv_b > 0.0f;
   if (wa) flags |= RF_WA;
@@ -196,6 +209,7 @@ __device__ __forceinline__ void contact_impulse(const BodiesV& B, const Row& r, 
   if (r.inv_a > 0.0f) { f3 nj = -j; body_impulse(B, r.ai, nj, cross(r.ra, nj)); }
   if (r.inv_b > 0.0f) body_impulse(B, r.bi, j, cross(r.rb, j));
 }
+#include "bounce.cuh"
 __device__ __forceinline__ float mu_dynamic(const Row& r, float slip) {  // solver.rs:429-431
   float t = slip / r.sv;
   return r.mu_k + (r.mu_s - r.mu_k) * exp_rp(-(t * t));
@@ -598,7 +612,7 @@ __global__ void k_after_solve(uint32_t nc, RowsV R, const float* __restrict__ ac
     if (!(f & RF_TERRAIN)) loaded[x.y] = 1;
   }
   c_n[k].w = jn;
-  if ((f & RF_TOI) && R.t2[k].w > 0.0f && jn > 0.0f) atomicAdd(&stats[STAT_BOUNCE], 1u);
+  (void)stats;
 }
 
 // ------------------------------------------------------------------ warm cache rebuild
@@ -702,7 +716,8 @@ __global__ void k_ballistic(uint32_t nisl, Sched S, RowsV R, BodiesV B, const fl
 // Position integration with the gyroscopic midpoint turn (step.rs:208-280), one thread per body.
 __global__ void k_integrate(uint32_t nb, BodiesV B, const uint8_t* __restrict__ ballistic,
                             const float4* __restrict__ last_lin, float dt, float4* orig_pos, float4* orig_rot,
-                            float4* pred_pos, float4* pred_rot) {
+                            float4* pred_pos, float4* pred_rot, const uint32_t* __restrict__ w6_ctr,
+                            const float4* __restrict__ w6_pl, const float4* __restrict__ w6_pa) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nb) return;
   float4 P = B.pos[i], Q = B.rot[i];
@@ -753,6 +768,12 @@ __global__ void k_integrate(uint32_t nb, BodiesV B, const uint8_t* __restrict__ 
       if (vfin(vl)) B.lin[i] = f4(fin_v(vl), L.w);  // Bodies::set_vel
       if (vfin(va)) B.ang[i] = f4(fin_v(va), A.w);
     }
+  }
+  // a bounced free body's pseudo-velocity (W6, step.rs:271-277): moves it, never enters its velocity
+  if (w6_ctr[w6::C_PON]) {
+    const f3 pl = xyz(w6_pl[i]), pa = xyz(w6_pa[i]);
+    pos = pos + pl * dt;
+    if (len2(pa) > 0.0f) rot = qnormalize(qmul(qfrom_axis_angle(normalize(pa), len(pa) * dt), rot));
   }
   // Bodies::set_pose (dynamics.rs:130-134)
   if (vfin(pos)) P = f4(fin_v(pos), P.w);
@@ -2057,6 +2078,23 @@ static void build_schedule(WorldGpu::Scratch& S, uint32_t* W_err, uint32_t nsche
                                              hist); RP_COUNT_LAUNCH(1);
 }
 
+// The W6 passes' scratch: per body, per contact, and a fixed pool for the direct solves.
+static w6::W6V w6_view(WorldGpu::Scratch& S) {
+  w6::W6V V;
+  V.rest_cnt = S.w6_rest_cnt.p; V.rest_min = S.w6_rest_min.p; V.rest_max = S.w6_rest_max.p;
+  V.parent = S.w6_parent.p; V.slot = S.w6_slot.p;
+  V.involved = S.w6_involved.p; V.direct = S.w6_direct.p; V.in_set = S.w6_in_set.p; V.has_pseudo = S.w6_has_pseudo.p;
+  V.acc = S.w6_acc.p; V.pl = S.w6_pl.p; V.pa = S.w6_pa.p;
+  V.rows = S.w6_rows.p; V.target = S.w6_target.p; V.sup_acc = S.w6_sup_acc.p; V.pseudo_u = S.w6_pseudo_u.p;
+  V.comp_rows = S.w6_comp_rows.p; V.comp_start = S.w6_comp_start.p; V.row_comp = S.w6_row_comp.p; V.cur = S.w6_cur.p;
+  V.ctr = S.w6_ctr.p;
+  V.pool = S.w6_pool.p;
+  V.pool_bytes = S.w6_pool.cap;
+  V.toi_a = S.toi_a.p; V.toi_b = S.toi_b.p;
+  return V;
+}
+static constexpr size_t kW6Pool = 48ull << 20;  // direct-solve scratch: about eleven 250-row components at once
+
 void run_solve(WorldGpu& W, StepCtx& ctx) {
   auto& S = *W.s_;
   cudaStream_t st = W.stream();
@@ -2073,6 +2111,15 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   S.Iw.ensure(9 * (size_t)nb + 9);
   S.orig_pos.ensure(nb + 1); S.orig_rot.ensure(nb + 1); S.pred_pos.ensure(nb + 1); S.pred_rot.ensure(nb + 1);
   S.split_l.ensure(nb + 1); S.split_a.ensure(nb + 1);
+  S.toi_a.ensure(nc + 1); S.toi_b.ensure(nc + 1);
+  S.w6_rest_cnt.ensure(nb + 1); S.w6_rest_min.ensure(nb + 1); S.w6_rest_max.ensure(nb + 1); S.w6_parent.ensure(nb + 1);
+  S.w6_slot.ensure(nb + 1); S.w6_involved.ensure(nb + 1); S.w6_direct.ensure(nb + 1); S.w6_acc.ensure(6 * (size_t)nb + 6);
+  S.w6_pl.ensure(nb + 1); S.w6_pa.ensure(nb + 1);
+  S.w6_rows.ensure(nc + 1); S.w6_target.ensure(nc + 1); S.w6_sup_acc.ensure(nc + 1); S.w6_pseudo_u.ensure(nc + 1);
+  S.w6_in_set.ensure(nc + 1); S.w6_has_pseudo.ensure(nc + 1); S.w6_comp_rows.ensure(nc + 1);
+  S.w6_comp_start.ensure(nc + 2); S.w6_row_comp.ensure(nc + 1); S.w6_cur.ensure(nc + 1);
+  S.w6_ctr.ensure(w6::C_N); S.w6_pool.ensure(kW6Pool);
+  RP_CUDA(cudaMemsetAsync(S.w6_ctr.p, 0, sizeof(uint32_t) * w6::C_N, st));  // no bounce until the count says so
   RP_CUDA(cudaMemsetAsync(S.loaded.p, 0, nb + 1, st));
   RP_CUDA(cudaMemsetAsync(S.constrained.p, 0, nb + 1, st));
   RP_CUDA(cudaMemsetAsync(S.touching.p, 0, nb + 1, st));
@@ -2127,7 +2174,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                                                S.uf.p); RP_COUNT_LAUNCH(1);
       k_build_rows<<<nblk(nc), T, 0, st>>>(nc, ctx.dt, S.c_a.p, S.c_b.p, S.c_pt.p, S.c_n.p, W.col_body.p, W.col_mat.p,
                                            ctx.hf_mat, W.pair_table.p, B, S.pre_lin.p, S.pre_ang.p, R, S.acc_jn.p,
-                                           S.acc_jt.p, S.uf.p, S.row_isl.p, jointed); RP_COUNT_LAUNCH(1);
+                                           S.acc_jt.p, S.uf.p, S.row_isl.p, jointed, W.last_lin.p, S.toi_a.p,
+                                           S.toi_b.p); RP_COUNT_LAUNCH(1);
     }
     joints_row_roots(W, R, nc, njr, S.uf.p, S.row_isl.p, st);
     P.end(PH_ROWS, st);
@@ -2437,6 +2485,15 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       k_vel_shock<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, SV, R, B, ctx.up, S.acc_jn.p); RP_COUNT_LAUNCH(1);
       // restitution for the contacts W6 leaves alone (jointed bodies); without joints there are none
       if (nj) { k_restitution<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, nc, SM, R, B, S.acc_jn.p); RP_COUNT_LAUNCH(1); }
+      // the W6 bounce passes (solver.rs:1009-1241); every kernel after the count returns at once
+      // when no row bounces
+      w6::W6V V6 = w6_view(S);
+      w6::k_w6_count<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, V6, stats); RP_COUNT_LAUNCH(1);
+      w6::k_w6_setup<<<1, w6::kBT, 0, st>>>(nc, nb, R, B, S.acc_jn.p, S.acc_jt.p, jointed, ctx.dt, V6); RP_COUNT_LAUNCH(1);
+      w6::k_w6_solve<<<4, 64, 0, st>>>(R, B, S.acc_jn.p, jointed, V6, stats); RP_COUNT_LAUNCH(1);
+      w6::k_w6_pseudo_setup<<<1, w6::kBT, 0, st>>>(nc, nb, R, B, S.acc_jn.p, S.acc_jt.p, jointed, V6); RP_COUNT_LAUNCH(1);
+      w6::k_w6_pseudo_solve<<<4, 64, 0, st>>>(R, B, jointed, V6, stats); RP_COUNT_LAUNCH(1);
+      w6::k_w6_pseudo_finish<<<nblk(nb), T, 0, st>>>(nb, V6); RP_COUNT_LAUNCH(1);
     }
     P.end(PH_VEL_SHOCK, st);
     k_after_solve<<<nblk(nc), T, 0, st>>>(nc, R, S.acc_jn.p, S.acc_jt.p, S.loaded.p, S.c_n.p, stats); RP_COUNT_LAUNCH(1);
@@ -2455,7 +2512,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
   P.begin(PH_INTEGRATE, st);
   if (nb > 0) {
     k_integrate<<<nblk(nb, 128), 128, 0, st>>>(nb, B, S.ballistic.p, W.last_lin.p, ctx.dt, S.orig_pos.p, S.orig_rot.p,
-                                               S.pred_pos.p, S.pred_rot.p); RP_COUNT_LAUNCH(1);
+                                               S.pred_pos.p, S.pred_rot.p, S.w6_ctr.p, S.w6_pl.p, S.w6_pa.p);
+    RP_COUNT_LAUNCH(1);
   }
   P.end(PH_INTEGRATE, st);
   // ---- stage 5: position pass (step.rs:284-309); its contacts are the scheduled rows
