@@ -455,6 +455,20 @@ def main():
         rollback = {"ticks": 8, "ms": r0.elapsed_time(r1), "worlds": w.num_worlds(),
                     "hashes_match": h_first == h_again}
 
+    # the riftnet wire snapshot of the final state (riftphys-riftnet/src/wire.rs): packed on the
+    # device and copied to the host, as a server does every tick; host-timed over a few calls
+    wire = None
+    if args.config == "terrain":
+        import time as _time
+        w.pack_snapshot(0, 0)
+        t0 = _time.perf_counter()
+        reps = 10
+        for k in range(reps):
+            data, chunks = w.pack_snapshot(k, 0)
+        wire_ms = (_time.perf_counter() - t0) * 1000.0 / reps
+        wire = {"bodies": nb, "chunks": chunks, "bytes": len(data), "ms": wire_ms,
+                "gb_per_s": len(data) / (wire_ms * 1e-3) / 1e9, "note": "host-timed, device pack + copy to pageable memory"}
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "body-ticks/s", "n_gpus": world_size, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -476,6 +490,8 @@ def main():
             line["rollback"] = rollback
         if learned is not None:
             line["learned_warm_start"] = learned
+        if wire is not None:
+            line["wire_snapshot"] = wire
         print(json.dumps(line), flush=True)
     w.free_snapshot(snap)
     w.close()

@@ -270,6 +270,22 @@ RPhysResult rphys_ext_set_joint_drive(RPhysWorld* world, uint32_t joint, uint32_
 RPhysResult rphys_ext_set_joint_damping(RPhysWorld* world, uint32_t joint, uint32_t angular, uint32_t axis,
                                         float damping, float friction);
 
+/* The riftnet wire snapshot (riftphys-riftnet/src/wire.rs:1-53): every live body, in id order, as
+ * a NetEnt {u32 id (the FFI body id); f32 px py pz, qx qy qz qw, sx sy sz; u32 kind} of 48 bytes
+ * -- kind 1 sphere (scale r r r), 2 box (the half extents), 3 capsule along y (r, (hh + r) / 2, r)
+ * as wire.rs:22-23 defines -- 25 to a chunk (MAX_PAYLOAD 1200 bytes) behind a 32-byte NetHdr
+ * {u32 magic 0x30535052; u16 ver 2; u8 kind 1; u8 flags 0; u64 tick; u64 epoch; u16 total;
+ * u16 index; u32 payload_len}, the chunks back to back in out (chunk c at c x 1232 bytes): what
+ * pack_snapshot(tick, epoch, ents) returns, one datagram per chunk. Packed on the device; out
+ * NULL only reports the sizes (out_bytes, out_chunks). total is the chunk count as u16, as in the
+ * reference. RPHYS_ERR_CAPACITY when out_cap is smaller than the snapshot. */
+#define RPHYS_WIRE_MAGIC 0x30535052u
+#define RPHYS_WIRE_HEADER_BYTES 32u
+#define RPHYS_WIRE_ENTITY_BYTES 48u
+#define RPHYS_WIRE_ENTITIES_PER_CHUNK 25u
+RPhysResult rphys_ext_pack_snapshot(RPhysWorld* world, uint64_t tick, uint64_t epoch, uint8_t* out, uint64_t out_cap,
+                                    uint64_t* out_bytes, uint32_t* out_chunks);
+
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:
  * cudaMalloc and cudaFree can wait for all work on the device and their memory use varies with the

@@ -363,6 +363,56 @@ RPhysResult rphys_world_clear_heightfield(RPhysWorld* W) {
   return RPHYS_OK;
 }
 
+// pack_snapshot (riftphys-riftnet/src/wire.rs:36-53) over every live body in id order; the entity
+// scale from the body's collider as wire.rs:22-23 defines it.
+RPhysResult rphys_ext_pack_snapshot(RPhysWorld* W, uint64_t tick, uint64_t epoch, uint8_t* out, uint64_t out_cap,
+                                    uint64_t* out_bytes, uint32_t* out_chunks) {
+  clear_err();
+  if (out_bytes) *out_bytes = 0;
+  if (out_chunks) *out_chunks = 0;
+  if (!W || !out_bytes || !out_chunks) return fail(RPHYS_ERR_NULL, "rphys_ext_pack_snapshot: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  const uint32_t per = 1200u / 48u;
+  std::vector<uint32_t> live;
+  for (uint32_t i = 0; i < W->w.num_bodies(); ++i)
+    if (W->w.alive[i]) live.push_back(i);
+  const uint32_t n = (uint32_t)live.size(), chunks = (n + per - 1) / per;
+  const uint64_t bytes = (uint64_t)chunks * 32u + (uint64_t)n * 48u;
+  *out_bytes = bytes;
+  *out_chunks = chunks;
+  if (!out) return RPHYS_OK;
+  if (out_cap < bytes) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_pack_snapshot: buffer smaller than the snapshot");
+  uint8_t* p = out;
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t k = std::min(per, n - c * per);
+    uint8_t hdr[32] = {};
+    const uint32_t magic = 0x30535052u, plen = k * 48u;
+    const uint16_t ver = 2, total = (uint16_t)chunks, index = (uint16_t)c;
+    std::memcpy(hdr + 0, &magic, 4); std::memcpy(hdr + 4, &ver, 2); hdr[6] = 1; hdr[7] = 0;
+    std::memcpy(hdr + 8, &tick, 8); std::memcpy(hdr + 16, &epoch, 8);
+    std::memcpy(hdr + 24, &total, 2); std::memcpy(hdr + 26, &index, 2); std::memcpy(hdr + 28, &plen, 4);
+    std::memcpy(p, hdr, 32);
+    p += 32;
+    for (uint32_t e = c * per; e < c * per + k; ++e) {
+      const uint32_t b = live[e];
+      const orc::Shape& sh = W->w.colliders[b].shape;
+      float ent[12];
+      uint32_t id = b + 1, kind;
+      float sx, sy, sz;
+      if (sh.kind == SH_SPHERE) { sx = sy = sz = sh.a; kind = 1; }
+      else if (sh.kind == SH_BOX) { sx = sh.a; sy = sh.b; sz = sh.c; kind = 2; }
+      else { sx = sh.a; sy = (sh.b + sh.a) * 0.5f; sz = sh.a; kind = 3; }
+      std::memcpy(ent + 0, &id, 4);
+      ent[1] = W->w.pos[b].x; ent[2] = W->w.pos[b].y; ent[3] = W->w.pos[b].z;
+      ent[4] = W->w.rot[b].x; ent[5] = W->w.rot[b].y; ent[6] = W->w.rot[b].z; ent[7] = W->w.rot[b].w;
+      ent[8] = sx; ent[9] = sy; ent[10] = sz;
+      std::memcpy(ent + 11, &kind, 4);
+      std::memcpy(p, ent, 48);
+      p += 48;
+    }
+  }
+  return RPHYS_OK;
+}
 RPhysResult rphys_world_get_contacts(const RPhysWorld* Wc, RPhysContactEvent* out, uint32_t cap, uint32_t* out_count) {
   clear_err();
   if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_world_get_contacts: null arg");

@@ -265,6 +265,8 @@ ABI = [
     ("rphys_ext_set_joint_limit", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float, c_float]),
     ("rphys_ext_num_joints", c_uint32, [c_void_p, POINTER(c_uint32)]),
     ("rphys_ext_set_joint_limits", c_uint32, [c_void_p, c_void_p, c_uint32]),
+    ("rphys_ext_pack_snapshot", c_uint32, [c_void_p, c_uint64, c_uint64, c_void_p, c_uint64, POINTER(c_uint64),
+                                           POINTER(c_uint32)]),
     ("rphys_ext_add_distance_joints", c_uint32, [c_void_p, POINTER(DistanceJointDesc), c_uint32, POINTER(c_uint32)]),
     ("rphys_ext_set_joint_axis", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float]),
     ("rphys_ext_set_joint_drive", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, POINTER(JointDrive)]),
@@ -426,6 +428,9 @@ class World:
     def free_snapshot(self, snap):
         self.lib.dll.rphys_world_snapshot_free(c_void_p(snap))
 
+    def remove_body(self, bid):
+        self.c("rphys_body_remove", bid)
+
     def apply_impulse(self, bid, j):
         self.c("rphys_body_apply_impulse", bid, Vec3(*j))
 
@@ -533,6 +538,14 @@ class World:
         first = c_uint32(0)
         self.c("rphys_ext_add_joints", arr, len(joints), byref(first))
         return first.value
+
+    def pack_snapshot(self, tick, epoch):
+        """The riftnet wire snapshot of the live bodies: (bytes, chunk count)."""
+        n, c = c_uint64(0), c_uint32(0)
+        self.c("rphys_ext_pack_snapshot", tick, epoch, None, 0, byref(n), byref(c))
+        buf = ctypes.create_string_buffer(max(1, n.value))
+        self.c("rphys_ext_pack_snapshot", tick, epoch, buf, n.value, byref(n), byref(c))
+        return buf.raw[: n.value], c.value
 
     def add_distance_joints(self, joints):
         """joints: iterable of (body_a, body_b, anchor_a, anchor_b, rest, compliance, damping), anchors

@@ -423,6 +423,25 @@ RPhysResult rphys_world_get_contacts(const RPhysWorld* Wc, RPhysContactEvent* ou
     return (RPhysResult)RPHYS_OK;
   });
 }
+RPhysResult rphys_ext_pack_snapshot(RPhysWorld* W, uint64_t tick, uint64_t epoch, uint8_t* out, uint64_t out_cap,
+                                    uint64_t* out_bytes, uint32_t* out_chunks) {
+  clear_err();
+  if (out_bytes) *out_bytes = 0;
+  if (out_chunks) *out_chunks = 0;
+  if (!W || !out_bytes || !out_chunks) return fail(RPHYS_ERR_NULL, "rphys_ext_pack_snapshot: null arg");
+  return guard("rphys_ext_pack_snapshot", [&]() {
+    LOCK;
+    size_t bytes = 0;
+    uint32_t chunks = 0;
+    W->w->pack_snapshot(tick, epoch, nullptr, 0, &bytes, &chunks);
+    *out_bytes = bytes;
+    *out_chunks = chunks;
+    if (!out) return (RPhysResult)RPHYS_OK;
+    if (out_cap < bytes) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_pack_snapshot: buffer smaller than the snapshot");
+    W->w->pack_snapshot(tick, epoch, out, (size_t)out_cap, &bytes, &chunks);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
 RPhysWorldSnapshot* rphys_world_snapshot_create(const RPhysWorld* Wc) {
   clear_err();
   if (!Wc) { fail(RPHYS_ERR_NULL, "rphys_world_snapshot_create: world is null"); return nullptr; }

@@ -182,6 +182,9 @@ struct WorldGpu::Scratch {
   DBuf<double> w6_acc;
   DBuf<float4> w6_pl, w6_pa;
   DBuf<float> w6_target, w6_sup_acc, w6_pseudo_u;
+  // the wire snapshot
+  DBuf<uint32_t> wire_flag, wire_off;
+  DBuf<uint8_t> wire_buf;
   DBuf<uint8_t> feat_valid;
   DBuf<float4> pred_used, s_pred;
   // solve groups (islands packed for one CTA each) and their shared-memory residents

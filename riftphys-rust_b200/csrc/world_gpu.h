@@ -157,6 +157,10 @@ class WorldGpu {
   void get_pairs(std::vector<uint64_t>& out);
   struct ContactOut { uint32_t a, b; float p[3], n[3]; float depth, impulse; uint32_t level; };
   void get_contacts(std::vector<ContactOut>& out);
+  // The riftnet wire snapshot of the live bodies (riftphys-riftnet/src/wire.rs:36-53): sizes, and
+  // the chunks packed into host_out when it is given (throws std::length_error past cap).
+  void pack_snapshot(unsigned long long tick, unsigned long long epoch, uint8_t* host_out, size_t cap, size_t* bytes,
+                     uint32_t* chunks);
   uint32_t body_of_collider(uint32_t c) const { return h_col_body_[c]; }
 
   // ---- rollback
