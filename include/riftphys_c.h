@@ -7,8 +7,8 @@
  * declares; its layout is the Rust definition at crates/riftphys-ffi/src/lib.rs:107-115.
  *
  * Each entry point below cites the reference function it replaces (file:line in
- * crates/riftphys-ffi/src/lib.rs). Ray and capsule-sweep queries and the kinematic player
- * controller are outside the GPU step and are not exported.
+ * crates/riftphys-ffi/src/lib.rs). Ray casts are exported (run on the device); capsule sweeps and
+ * the kinematic player controller are not.
  */
 #pragma once
 
@@ -100,6 +100,25 @@ typedef struct RPhysHeightfieldDesc {
     float height_scale; float height_offset;
     const int16_t* heights;
 } RPhysHeightfieldDesc;
+
+/* ===================== QUERIES ===================== */
+typedef struct RPhysRayQuery {
+    RPhysVec3 origin;
+    RPhysVec3 dir;          /* need not be normalised; zero is a miss */
+    float max_distance;     /* <= 0: a miss */
+    uint32_t ignore_body;   /* 1-based; 0 = none; the terrain sentinel is invalid here */
+} RPhysRayQuery;
+typedef struct RPhysRayHit {
+    RPhysBool hit;
+    uint32_t  body_id;      /* 1-based; 0 = none; RPHYS_TERRAIN_BODY_ID for the heightfield */
+    float     fraction;     /* distance / max_distance, in [0, 1] */
+    RPhysVec3 point;
+    RPhysVec3 normal;
+} RPhysRayHit;
+/* World::raycast (riftphys-world/src/world/queries.rs:50-116; lib.rs:1271-1346): the nearest of the
+ * colliders' AABBs and the heightfield's triangles along the ray; a miss is hit 0, body 0, fraction
+ * 1, point 0, normal +Y. */
+RPhysResult rphys_world_raycast(const RPhysWorld* world, const RPhysRayQuery* query, RPhysRayHit* out_hit);
 
 /* ===================== API ===================== */
 RPhysResult rphys_world_set_heightfield_i16(RPhysWorld* world, const RPhysHeightfieldDesc* hf,

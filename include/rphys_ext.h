@@ -286,6 +286,11 @@ RPhysResult rphys_ext_set_joint_damping(RPhysWorld* world, uint32_t joint, uint3
 RPhysResult rphys_ext_pack_snapshot(RPhysWorld* world, uint64_t tick, uint64_t epoch, uint8_t* out, uint64_t out_cap,
                                     uint64_t* out_bytes, uint32_t* out_chunks);
 
+/* rphys_world_raycast for n rays at once, one device block per ray; every query checked first
+ * (all-or-nothing), then out[i] as rphys_world_raycast would write it for queries[i]. */
+RPhysResult rphys_ext_raycast_batch(const RPhysWorld* world, const RPhysRayQuery* queries, uint32_t n,
+                                    RPhysRayHit* out);
+
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:
  * cudaMalloc and cudaFree can wait for all work on the device and their memory use varies with the

@@ -413,6 +413,66 @@ RPhysResult rphys_ext_pack_snapshot(RPhysWorld* W, uint64_t tick, uint64_t epoch
   }
   return RPHYS_OK;
 }
+// rphys_world_raycast (riftphys-ffi/src/lib.rs:1271-1346, 470-479)
+static void write_raycast_miss(RPhysRayHit* h) {
+  h->hit = RPHYS_FALSE;
+  h->body_id = RPHYS_INVALID_BODY_ID;
+  h->fraction = 1.0f;
+  h->point = RPhysVec3{0.0f, 0.0f, 0.0f};
+  h->normal = RPhysVec3{0.0f, 1.0f, 0.0f};
+}
+static RPhysResult raycast_one(RPhysWorld* W, const RPhysRayQuery& q, const char* ctx, RPhysRayHit* out) {
+  write_raycast_miss(out);
+  auto fin3 = [](RPhysVec3 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+  if (!fin3(q.origin)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": origin contains NaN/Inf");
+  if (!fin3(q.dir)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": dir contains NaN/Inf");
+  if (!std::isfinite(q.max_distance)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": max_distance is not finite");
+  uint32_t ignore = 0xFFFFFFFFu;
+  if (q.ignore_body != 0) {
+    const std::string ictx = std::string(ctx) + ".ignore_body";
+    RPhysResult r = live_id(W, q.ignore_body, ictx.c_str(), &ignore);
+    if (r) return r;
+  }
+  if (q.max_distance <= 0.0f) return RPHYS_OK;
+  V3 d = v(q.dir);
+  const float len2 = om::dot(d, d);
+  if (!std::isfinite(len2)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": dir length overflow/invalid");
+  if (len2 <= 1.0e-20f) return RPHYS_OK;
+  d = om::divs(d, std::sqrt(len2));
+  uint32_t body;
+  float toi;
+  V3 p, n;
+  if (!W->w.raycast(v(q.origin), d, q.max_distance, ignore, &body, &toi, &p, &n)) return RPHYS_OK;
+  out->hit = RPHYS_TRUE;
+  out->body_id = body == 0xFFFFFFFFu ? RPHYS_TERRAIN_BODY_ID : body + 1;
+  out->fraction = om::clampf(toi, 0.0f, 1.0f);
+  out->point = RPhysVec3{p.x, p.y, p.z};
+  out->normal = RPhysVec3{n.x, n.y, n.z};
+  return RPHYS_OK;
+}
+RPhysResult rphys_world_raycast(const RPhysWorld* Wc, const RPhysRayQuery* q, RPhysRayHit* out) {
+  clear_err();
+  if (out) write_raycast_miss(out);
+  if (!Wc || !q || !out) return fail(RPHYS_ERR_NULL, "rphys_world_raycast: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  return raycast_one(W, *q, "rphys_world_raycast", out);
+}
+RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q, uint32_t n, RPhysRayHit* out) {
+  clear_err();
+  if (!Wc || ((!q || !out) && n)) return fail(RPHYS_ERR_NULL, "rphys_ext_raycast_batch: null arg");
+  for (uint32_t i = 0; i < n; ++i) write_raycast_miss(out + i);
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  for (uint32_t i = 0; i < n; ++i) {
+    RPhysResult r = raycast_one(W, q[i], "rphys_ext_raycast_batch", out + i);
+    if (r) {
+      for (uint32_t k = 0; k < n; ++k) write_raycast_miss(out + k);
+      return r;
+    }
+  }
+  return RPHYS_OK;
+}
 RPhysResult rphys_world_get_contacts(const RPhysWorld* Wc, RPhysContactEvent* out, uint32_t cap, uint32_t* out_count) {
   clear_err();
   if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_world_get_contacts: null arg");

@@ -769,6 +769,134 @@ static void hf_query(const HeightField& hf, const Aabb& a, std::vector<Shape>& o
     }
 }
 
+// ------------------------------------------------------------------ queries
+// normal_from_aabb_point / ray_aabb (riftphys-world/src/world/geom.rs:40-93)
+static V3 normal_from_aabb_point(const Aabb& b, V3 p) {
+  const float eps = 1.0e-4f;
+  if (std::fabs(p.x - b.min.x) < eps) return V3{-1, 0, 0};
+  if (std::fabs(p.x - b.max.x) < eps) return V3{1, 0, 0};
+  if (std::fabs(p.y - b.min.y) < eps) return V3{0, -1, 0};
+  if (std::fabs(p.y - b.max.y) < eps) return V3{0, 1, 0};
+  if (std::fabs(p.z - b.min.z) < eps) return V3{0, 0, -1};
+  if (std::fabs(p.z - b.max.z) < eps) return V3{0, 0, 1};
+  V3 c = mul(add(b.min, b.max), 0.5f);
+  V3 n = sub(p, c);
+  float l2 = dot(n, n);
+  if (l2 > 1.0e-20f) n = divs(n, std::sqrt(l2));
+  else n = V3{0, 1, 0};
+  return n;
+}
+static bool ray_aabb(V3 o, V3 d, const Aabb& b, float max_d, float* t_out, V3* p_out, V3* n_out) {
+  const float eps = 1.0e-8f;
+  float tmin = 0.0f, tmax = max_d;
+  const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+  const float lo[3] = {b.min.x, b.min.y, b.min.z}, hi[3] = {b.max.x, b.max.y, b.max.z};
+  for (int a = 0; a < 3; ++a) {
+    if (std::fabs(dd[a]) < eps) {
+      if (oo[a] < lo[a] || oo[a] > hi[a]) return false;
+    } else {
+      float inv = 1.0f / dd[a];
+      float t1 = (lo[a] - oo[a]) * inv, t2 = (hi[a] - oo[a]) * inv;
+      if (t1 > t2) std::swap(t1, t2);
+      if (t1 > tmin) tmin = t1;
+      if (t2 < tmax) tmax = t2;
+      if (tmin > tmax) return false;
+    }
+  }
+  if (tmin < 0.0f || tmin > max_d) return false;
+  V3 p = add(o, mul(d, tmin));
+  *t_out = tmin;
+  *p_out = p;
+  *n_out = normal_from_aabb_point(b, p);
+  return true;
+}
+// Triangle::intersect_ray (riftphys-geom/src/triangle.rs:215-235) with Plane::from_points /
+// from_point_normal / intersect_ray (plane.rs:16-86) and Triangle::barycentric (triangle.rs:74-113)
+static bool ray_triangle(V3 o, V3 d, float max_d, V3 a, V3 b, V3 c, float* t_out) {
+  V3 n = cross(sub(b, a), sub(c, a));
+  float a2 = dot(n, n);
+  if (!fin(a2) || a2 <= 1.0e-16f) return false;
+  if (!(vfin(a) && vfin(b) && vfin(c))) return false;
+  float l2 = dot(n, n);
+  if (!fin(l2) || l2 <= 1.0e-6f * 1.0e-6f) return false;
+  float inv_len = 1.0f / std::sqrt(l2);
+  V3 nu = mul(n, inv_len);
+  float pd = -dot(nu, a);
+  if (!(vfin(nu) && fin(pd))) return false;
+  if (!(vfin(o) && vfin(d))) return false;
+  float denom = dot(nu, d);
+  if (!fin(denom) || std::fabs(denom) < 1.0e-6f) return false;
+  float numer = -(dot(nu, o) + pd);
+  if (!fin(numer)) return false;
+  float t = numer / denom;
+  if (!fin(t)) return false;
+  if (!(t >= 0.0f && t <= max_d)) return false;
+  V3 p = add(o, mul(d, t));
+  V3 v0 = sub(b, a), v1 = sub(c, a), v2 = sub(p, a);
+  float d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
+  float den = d00 * d11 - d01 * d01;
+  float scale = rmax(std::fabs(d00 * d11), 1.0f);
+  if (!fin(den) || std::fabs(den) <= 1.0e-12f * scale) return false;
+  float inv = 1.0f / den;
+  float v = (d11 * d20 - d01 * d21) * inv;
+  float w = (d00 * d21 - d01 * d20) * inv;
+  float u = 1.0f - v - w;
+  if (!(fin(u) && fin(v) && fin(w) && u >= -1.0e-5f && v >= -1.0e-5f && w >= -1.0e-5f)) return false;
+  *t_out = t;
+  return true;
+}
+// Triangle::normal (triangle.rs:26-31)
+static V3 tri_normal(V3 a, V3 b, V3 c) {
+  V3 n = cross(sub(b, a), sub(c, a));
+  if (!vfin(n)) return V3{0, 0, 0};
+  float rcp = 1.0f / std::sqrt(dot(n, n));
+  return (fin(rcp) && rcp > 0.0f) ? mul(n, rcp) : V3{0, 0, 0};
+}
+bool World::raycast(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t* body, float* toi, V3* point,
+                    V3* normal) const {
+  const float max_d = rmax(max_dist, 0.0f);
+  if (max_d <= 0.0f) return false;
+  const float l = std::sqrt(dot(dir, dir));
+  if (!fin(l) || l < 1.0e-12f) return false;
+  dir = divs(dir, l);
+  bool have = false;
+  float bt = 0.0f;
+  size_t bci = 0;
+  V3 bp{0, 0, 0}, bn{0, 0, 0};
+  const size_t kEnv = (size_t)-1;
+  for (size_t ci = 0; ci < colliders.size(); ++ci) {
+    const Collider& c = colliders[ci];
+    if (c.body == ignore) continue;
+    float t;
+    V3 p, n;
+    if (!ray_aabb(origin, dir, c.aabb, max_d, &t, &p, &n)) continue;
+    if (!have || (t < bt - 1.0e-9f) || (std::fabs(t - bt) <= 1.0e-9f && ci < bci)) {
+      have = true; bt = t; bci = ci; bp = p; bn = n;
+    }
+  }
+  if (has_hf) {
+    V3 end = add(origin, mul(dir, max_d));
+    Aabb q = aabb_new(vmin(origin, end), vmax(origin, end));
+    std::vector<Shape> tris;
+    hf_query(hf, q, tris);
+    for (const Shape& tr : tris) {
+      float t;
+      if (!ray_triangle(origin, dir, max_d, tr.ta, tr.tb, tr.tc, &t)) continue;
+      if (!have || t < bt - 1.0e-9f) {
+        have = true; bt = t; bci = kEnv;
+        bp = fin(t) ? add(origin, mul(dir, t)) : origin;
+        bn = tri_normal(tr.ta, tr.tb, tr.tc);
+      }
+    }
+  }
+  if (!have) return false;
+  *body = bci == kEnv ? 0xFFFFFFFFu : colliders[bci].body;
+  *toi = clampf(bt / max_d, 0.0f, 1.0f);
+  *point = bp;
+  *normal = bn;
+  return true;
+}
+
 // ------------------------------------------------------------------ solver
 // ContactConstraint (solver.rs:47-87), the fields the configured path reads.
 struct CC {

@@ -187,6 +187,10 @@ struct World {
   void update_colliders_aabb();
   CarriedState carried_state() const;
   void restore_carried_state(const CarriedState& s);
+  // World::raycast (queries.rs:50-116): dir normalised here again; ignore a body index or
+  // 0xFFFFFFFF. Returns false on a miss; body 0xFFFFFFFF is the terrain.
+  bool raycast(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t* body, float* toi, V3* point,
+               V3* normal) const;
   // step.rs / provenance.rs
   void step(float dt);
   void step_hash(uint8_t out[32]) const;

@@ -128,6 +128,14 @@ JOINT_HINGE = 1
 JOINT_D6 = 2
 
 
+class RayQuery(Structure):
+    _fields_ = [("origin", Vec3), ("dir", Vec3), ("max_distance", c_float), ("ignore_body", c_uint32)]
+
+
+class RayHit(Structure):
+    _fields_ = [("hit", c_uint32), ("body_id", c_uint32), ("fraction", c_float), ("point", Vec3), ("normal", Vec3)]
+
+
 class DistanceJointDesc(Structure):
     _fields_ = [("body_a", c_uint32), ("body_b", c_uint32), ("anchor_a", Vec3), ("anchor_b", Vec3),
                 ("rest", c_float), ("compliance", c_float), ("damping", c_float)]
@@ -265,6 +273,8 @@ ABI = [
     ("rphys_ext_set_joint_limit", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float, c_float]),
     ("rphys_ext_num_joints", c_uint32, [c_void_p, POINTER(c_uint32)]),
     ("rphys_ext_set_joint_limits", c_uint32, [c_void_p, c_void_p, c_uint32]),
+    ("rphys_world_raycast", c_uint32, [c_void_p, POINTER(RayQuery), POINTER(RayHit)]),
+    ("rphys_ext_raycast_batch", c_uint32, [c_void_p, POINTER(RayQuery), c_uint32, POINTER(RayHit)]),
     ("rphys_ext_pack_snapshot", c_uint32, [c_void_p, c_uint64, c_uint64, c_void_p, c_uint64, POINTER(c_uint64),
                                            POINTER(c_uint32)]),
     ("rphys_ext_add_distance_joints", c_uint32, [c_void_p, POINTER(DistanceJointDesc), c_uint32, POINTER(c_uint32)]),
@@ -538,6 +548,31 @@ class World:
         first = c_uint32(0)
         self.c("rphys_ext_add_joints", arr, len(joints), byref(first))
         return first.value
+
+    def raycast(self, origin, d, max_distance, ignore=0):
+        """rphys_world_raycast: (hit, body_id, fraction, point, normal)."""
+        q = RayQuery(Vec3(*origin), Vec3(*d), max_distance, ignore)
+        h = RayHit()
+        self.c("rphys_world_raycast", byref(q), byref(h))
+        return (bool(h.hit), h.body_id, h.fraction, (h.point.x, h.point.y, h.point.z), (h.normal.x, h.normal.y, h.normal.z))
+
+    def raycast_batch(self, origins, dirs, max_distance, ignore=None):
+        """rphys_ext_raycast_batch over arrays of origins and directions: the hits as a numpy
+        array of 10 float32 columns per ray (hit and body id as uint32 bits, fraction, point, normal)."""
+        import numpy as np
+        n = len(origins)
+        q = np.zeros((n, 8), dtype=np.float32)
+        q[:, 0:3] = origins
+        q[:, 3:6] = dirs
+        q[:, 6] = max_distance
+        if ignore is not None:
+            q[:, 7].view(np.uint32)[:] = ignore
+        assert q.strides[0] == ctypes.sizeof(RayQuery)
+        out = np.zeros((n, 9), dtype=np.float32)
+        assert out.strides[0] == ctypes.sizeof(RayHit)
+        self.c("rphys_ext_raycast_batch", ctypes.cast(q.ctypes.data, POINTER(RayQuery)), n,
+               ctypes.cast(out.ctypes.data, POINTER(RayHit)))
+        return out
 
     def pack_snapshot(self, tick, epoch):
         """The riftnet wire snapshot of the live bodies: (bytes, chunk count)."""

@@ -442,6 +442,95 @@ RPhysResult rphys_ext_pack_snapshot(RPhysWorld* W, uint64_t tick, uint64_t epoch
     return (RPhysResult)RPHYS_OK;
   });
 }
+// lib.rs:470-479
+static void write_raycast_miss(RPhysRayHit* h) {
+  h->hit = RPHYS_FALSE;
+  h->body_id = RPHYS_INVALID_BODY_ID;
+  h->fraction = 1.0f;
+  h->point = RPhysVec3{0.0f, 0.0f, 0.0f};
+  h->normal = RPhysVec3{0.0f, 1.0f, 0.0f};
+}
+// The checks and the direction normalisation of rphys_world_raycast (lib.rs:1286-1322) and of
+// World::raycast (queries.rs:51-56); *cast = 1 when the ray is cast (ray8 filled), 0 for a miss.
+static RPhysResult ray_prepare(RPhysWorld* W, const RPhysRayQuery& q, const char* ctx, float ray8[8], int* cast) {
+  *cast = 0;
+  auto fin3 = [](RPhysVec3 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+  if (!fin3(q.origin)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": origin contains NaN/Inf");
+  if (!fin3(q.dir)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": dir contains NaN/Inf");
+  if (!std::isfinite(q.max_distance)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": max_distance is not finite");
+  uint32_t ignore = 0xFFFFFFFFu;
+  if (q.ignore_body != 0) {
+    RPhysResult r = live_id(W, q.ignore_body, std::string(ctx) + ".ignore_body", &ignore);
+    if (r) return r;
+  }
+  if (q.max_distance <= 0.0f) return RPHYS_OK;
+  const float len2 = (q.dir.x * q.dir.x + q.dir.y * q.dir.y) + q.dir.z * q.dir.z;
+  if (!std::isfinite(len2)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": dir length overflow/invalid");
+  if (len2 <= 1.0e-20f) return RPHYS_OK;
+  const float l = std::sqrt(len2);
+  float dx = q.dir.x / l, dy = q.dir.y / l, dz = q.dir.z / l;
+  const float len = std::sqrt((dx * dx + dy * dy) + dz * dz);  // World::raycast normalises again
+  if (!std::isfinite(len) || len < 1.0e-12f) return RPHYS_OK;
+  dx /= len; dy /= len; dz /= len;
+  ray8[0] = q.origin.x; ray8[1] = q.origin.y; ray8[2] = q.origin.z;
+  ray8[3] = dx; ray8[4] = dy; ray8[5] = dz;
+  ray8[6] = q.max_distance;
+  std::memcpy(ray8 + 7, &ignore, 4);
+  *cast = 1;
+  return RPHYS_OK;
+}
+static void ray_result(const float4& pt, const float4& n, RPhysRayHit* h) {
+  uint32_t code;
+  std::memcpy(&code, &pt.w, 4);
+  if (code == 0) { write_raycast_miss(h); return; }
+  h->hit = RPHYS_TRUE;
+  h->body_id = code;  // id + 1, or RPHYS_TERRAIN_BODY_ID
+  h->fraction = n.w;
+  h->point = RPhysVec3{pt.x, pt.y, pt.z};
+  h->normal = RPhysVec3{n.x, n.y, n.z};
+}
+RPhysResult rphys_world_raycast(const RPhysWorld* Wc, const RPhysRayQuery* q, RPhysRayHit* out) {
+  clear_err();
+  if (out) write_raycast_miss(out);
+  if (!Wc || !q || !out) return fail(RPHYS_ERR_NULL, "rphys_world_raycast: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_world_raycast", [&]() {
+    LOCK;
+    float ray8[8];
+    int cast = 0;
+    RPhysResult r = ray_prepare(W, *q, "rphys_world_raycast", ray8, &cast);
+    if (r || !cast) return r;
+    float4 pt, n;
+    W->w->raycast_batch(1, ray8, &pt, &n);
+    ray_result(pt, n, out);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q, uint32_t n, RPhysRayHit* out) {
+  clear_err();
+  if (!Wc || ((!q || !out) && n)) return fail(RPHYS_ERR_NULL, "rphys_ext_raycast_batch: null arg");
+  for (uint32_t i = 0; i < n; ++i) write_raycast_miss(out + i);
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_raycast_batch", [&]() {
+    LOCK;
+    std::vector<float> rays;
+    std::vector<uint32_t> which;
+    rays.reserve(8 * (size_t)n);
+    for (uint32_t i = 0; i < n; ++i) {
+      float ray8[8];
+      int cast = 0;
+      RPhysResult r = ray_prepare(W, q[i], "rphys_ext_raycast_batch", ray8, &cast);
+      if (r) return r;
+      if (cast) { rays.insert(rays.end(), ray8, ray8 + 8); which.push_back(i); }
+    }
+    const uint32_t m = (uint32_t)which.size();
+    if (!m) return (RPhysResult)RPHYS_OK;
+    std::vector<float4> pt(m), nn(m);
+    W->w->raycast_batch(m, rays.data(), pt.data(), nn.data());
+    for (uint32_t k = 0; k < m; ++k) ray_result(pt[k], nn[k], out + which[k]);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
 RPhysWorldSnapshot* rphys_world_snapshot_create(const RPhysWorld* Wc) {
   clear_err();
   if (!Wc) { fail(RPHYS_ERR_NULL, "rphys_world_snapshot_create: world is null"); return nullptr; }

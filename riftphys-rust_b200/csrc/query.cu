@@ -1,0 +1,240 @@
+// query.cu -- ray casts on the device (riftphys-world/src/world/queries.rs:50-116): against every
+// collider's stored AABB (geom.rs:40-93), then against the heightfield's triangles in the ray's
+// box (terrain.rs:300-358, triangle.rs:215-235). One block per ray: its threads test a chunk of
+// colliders (or triangles) at once, then one thread takes the chunk's hits in index order with
+// the reference's replacement rule, so the result is the sequential scan's exactly.
+#include "shape_aabb.cuh"
+#include "step_internal.cuh"
+
+namespace rp {
+
+namespace {
+constexpr int QT = 256;  // threads per ray
+}
+
+struct RayIn { f3 o, d; float max_d; uint32_t ignore; };  // d normalised; ignore: body index or kNoBody
+constexpr uint32_t kNoBody = 0xFFFFFFFFu;
+static_assert(sizeof(RayIn) == 32, "RayIn: 8 words per ray");
+
+// normal_from_aabb_point (geom.rs:40-57)
+__device__ f3 normal_from_aabb_point(f3 mn, f3 mx, f3 p) {
+  const float eps = 1.0e-4f;
+  if (fabsf(p.x - mn.x) < eps) return mk3(-1, 0, 0);
+  if (fabsf(p.x - mx.x) < eps) return mk3(1, 0, 0);
+  if (fabsf(p.y - mn.y) < eps) return mk3(0, -1, 0);
+  if (fabsf(p.y - mx.y) < eps) return mk3(0, 1, 0);
+  if (fabsf(p.z - mn.z) < eps) return mk3(0, 0, -1);
+  if (fabsf(p.z - mx.z) < eps) return mk3(0, 0, 1);
+  f3 c = (mn + mx) * 0.5f;
+  f3 n = p - c;
+  float l2 = len2(n);
+  if (l2 > 1.0e-20f) { float l = sqrtf(l2); n = mk3(n.x / l, n.y / l, n.z / l); }
+  else n = mk3(0, 1, 0);
+  return n;
+}
+// ray_aabb (geom.rs:59-93): the slab test from t = 0 to max_dist
+__device__ bool ray_aabb(f3 o, f3 d, f3 mn, f3 mx, float max_d, float* t_out, f3* p_out, f3* n_out) {
+  const float eps = 1.0e-8f;
+  float tmin = 0.0f, tmax = max_d;
+  const float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z}, lo[3] = {mn.x, mn.y, mn.z}, hi[3] = {mx.x, mx.y, mx.z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (fabsf(dd[a]) < eps) {
+      if (oo[a] < lo[a] || oo[a] > hi[a]) return false;
+    } else {
+      float inv = 1.0f / dd[a];
+      float t1 = (lo[a] - oo[a]) * inv, t2 = (hi[a] - oo[a]) * inv;
+      if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+      if (t1 > tmin) tmin = t1;
+      if (t2 < tmax) tmax = t2;
+      if (tmin > tmax) return false;
+    }
+  }
+  if (tmin < 0.0f || tmin > max_d) return false;
+  f3 p = o + d * tmin;
+  *t_out = tmin;
+  *p_out = p;
+  *n_out = normal_from_aabb_point(mn, mx, p);
+  return true;
+}
+// Triangle::intersect_ray (triangle.rs:215-235) with Plane::from_points / intersect_ray
+// (plane.rs:16-86) and Triangle::barycentric (triangle.rs:74-113); t in [0, max_d].
+__device__ bool ray_triangle(f3 o, f3 d, float max_d, f3 a, f3 b, f3 c, float* t_out) {
+  f3 n = cross(b - a, c - a);
+  float a2 = dot(n, n);
+  if (!fin(a2) || a2 <= 1.0e-16f) return false;  // degenerate
+  if (!(vfin(a) && vfin(b) && vfin(c))) return false;
+  float l2 = dot(n, n);
+  if (!fin(l2) || l2 <= 1.0e-6f * 1.0e-6f) return false;
+  float inv_len = 1.0f / sqrtf(l2);
+  f3 nu = n * inv_len;
+  float pd = -dot(nu, a);
+  if (!(vfin(nu) && fin(pd))) return false;
+  if (!(vfin(o) && vfin(d))) return false;
+  float denom = dot(nu, d);
+  if (!fin(denom) || fabsf(denom) < 1.0e-6f) return false;
+  float numer = -(dot(nu, o) + pd);
+  if (!fin(numer)) return false;
+  float t = numer / denom;
+  if (!fin(t)) return false;
+  if (!(t >= 0.0f && t <= max_d)) return false;
+  f3 p = o + d * t;
+  f3 v0 = b - a, v1 = c - a, v2 = p - a;
+  float d00 = dot(v0, v0), d01 = dot(v0, v1), d11 = dot(v1, v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
+  float den = d00 * d11 - d01 * d01;
+  float scale = rmax(fabsf(d00 * d11), 1.0f);
+  if (!fin(den) || fabsf(den) <= 1.0e-12f * scale) return false;
+  float inv = 1.0f / den;
+  float v = (d11 * d20 - d01 * d21) * inv;
+  float w = (d00 * d21 - d01 * d20) * inv;
+  float u = 1.0f - v - w;
+  if (!(fin(u) && fin(v) && fin(w) && u >= -1.0e-5f && v >= -1.0e-5f && w >= -1.0e-5f)) return false;
+  *t_out = t;
+  return true;
+}
+// Triangle::normal (triangle.rs:26-31): normalize_or_zero of the unnormalised normal
+__device__ f3 tri_normal(f3 a, f3 b, f3 c) {
+  f3 n = cross(b - a, c - a);
+  if (!vfin(n)) return mk3(0, 0, 0);
+  float rcp = 1.0f / sqrtf(dot(n, n));
+  return (fin(rcp) && rcp > 0.0f) ? n * rcp : mk3(0, 0, 0);
+}
+
+struct HfDev { const float* h; uint32_t nx, nz; float sx, sz, ox, oz, min_y, max_y; };
+
+__global__ void __launch_bounds__(QT) k_raycast(uint32_t nrays, const RayIn* __restrict__ rays, uint32_t ncol,
+                                                const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ ckind,
+                                                const float4* __restrict__ cdims, const float4* __restrict__ pos,
+                                                const float4* __restrict__ rot, const uint8_t* __restrict__ alive,
+                                                bool has_hf, HfDev hf, float4* out_pt, float4* out_n) {
+  const uint32_t r = blockIdx.x;
+  if (r >= nrays) return;
+  const int tid = threadIdx.x;
+  const RayIn ray = rays[r];
+  __shared__ float s_t[QT];
+  __shared__ float4 s_p[QT], s_n[QT];
+  __shared__ uint8_t s_hit[QT];
+  __shared__ float b_t;
+  __shared__ uint32_t b_ci;
+  __shared__ f3 b_p, b_n;
+  __shared__ int have;
+  if (tid == 0) { have = 0; b_t = 0.0f; b_ci = 0; }
+  __syncthreads();
+  // 1. colliders, in index order: take a hit when it is the first, or nearer by more than 1e-9
+  //    (or as near and of a lower index, which a scan in index order never sees)
+  for (uint32_t base = 0; base < ncol; base += QT) {
+    const uint32_t ci = base + tid;
+    bool hit = false;
+    if (ci < ncol) {
+      const uint32_t bd = cbody[ci];
+      if (alive[bd] && bd != ray.ignore) {
+        f3 mn, mx;
+        aabb_of(ckind[ci], cdims[ci], xyz(pos[bd]), asq(rot[bd]), &mn, &mx);
+        float t;
+        f3 p, n;
+        hit = ray_aabb(ray.o, ray.d, mn, mx, ray.max_d, &t, &p, &n);
+        if (hit) { s_t[tid] = t; s_p[tid] = f4(p); s_n[tid] = f4(n); }
+      }
+    }
+    s_hit[tid] = hit ? 1 : 0;
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 0; k < QT; ++k) {
+        if (!s_hit[k]) continue;
+        const float t = s_t[k];
+        const uint32_t ci2 = base + k;
+        if (!have || (t < b_t - 1.0e-9f) || (fabsf(t - b_t) <= 1.0e-9f && ci2 < b_ci)) {
+          have = 1; b_t = t; b_ci = ci2; b_p = xyz(s_p[k]); b_n = xyz(s_n[k]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // 2. the heightfield's triangles in the ray's box, cell by cell: nearer by more than 1e-9 wins
+  if (has_hf) {
+    const f3 end = ray.o + ray.d * ray.max_d;
+    f3 qa = vmin(ray.o, end), qb = vmax(ray.o, end);
+    qa = mk3(qf32(qa.x), qf32(qa.y), qf32(qa.z));
+    qb = mk3(qf32(qb.x), qf32(qb.y), qf32(qb.z));
+    const f3 qmn = vmin(qa, qb), qmx = vmax(qa, qb);
+    const int nx = (int)hf.nx, nz = (int)hf.nz;
+    if (nx >= 2 && nz >= 2 && !(qmn.y > hf.max_y + 1.0f || qmx.y < hf.min_y - 1.0f)) {
+      auto toi = [](float f) -> long long {
+        if (isnan(f)) return 0;
+        if (f >= 2147483647.0f) return 2147483647;
+        if (f <= -2147483648.0f) return -2147483648LL;
+        return (long long)f;
+      };
+      auto cl = [](long long v, long long lo, long long hi) { return v < lo ? lo : (v > hi ? hi : v); };
+      const long long gx0 = cl(toi(floorf((qmn.x - hf.ox) / hf.sx)) - 1, 0, nx - 2);
+      const long long gx1 = cl(toi(ceilf((qmx.x - hf.ox) / hf.sx)) + 1, 0, nx - 2);
+      const long long gz0 = cl(toi(floorf((qmn.z - hf.oz) / hf.sz)) - 1, 0, nz - 2);
+      const long long gz1 = cl(toi(ceilf((qmx.z - hf.oz) / hf.sz)) + 1, 0, nz - 2);
+      const unsigned long long wx = (unsigned long long)(gx1 - gx0 + 1), ntri = 2ull * wx * (unsigned long long)(gz1 - gz0 + 1);
+      for (unsigned long long base = 0; base < ntri; base += QT) {
+        const unsigned long long k = base + tid;
+        bool hit = false;
+        if (k < ntri) {
+          const unsigned long long cell = k >> 1;
+          const long long gz = gz0 + (long long)(cell / wx), gx = gx0 + (long long)(cell % wx);
+          auto H = [&](long long x, long long z) { return hf.h[(size_t)x + (size_t)z * hf.nx]; };
+          const float x0 = (float)gx * hf.sx + hf.ox, x1 = x0 + hf.sx;
+          const float z0 = (float)gz * hf.sz + hf.oz, z1 = z0 + hf.sz;
+          const f3 p00 = mk3(x0, H(gx, gz), z0), p10 = mk3(x1, H(gx + 1, gz), z0);
+          const f3 p01 = mk3(x0, H(gx, gz + 1), z1), p11 = mk3(x1, H(gx + 1, gz + 1), z1);
+          f3 a = p00, b = p01, c = p10;  // tri1 = (p00, p01, p10), tri2 = (p10, p01, p11)
+          if (k & 1ull) { a = p10; b = p01; c = p11; }
+          float t;
+          hit = ray_triangle(ray.o, ray.d, ray.max_d, a, b, c, &t);
+          if (hit) {
+            s_t[tid] = t;
+            s_p[tid] = f4(ray.o + ray.d * t);
+            s_n[tid] = f4(tri_normal(a, b, c));
+          }
+        }
+        s_hit[tid] = hit ? 1 : 0;
+        __syncthreads();
+        if (tid == 0) {
+          for (int q = 0; q < QT; ++q) {
+            if (!s_hit[q]) continue;
+            const float t = s_t[q];
+            if (!have || t < b_t - 1.0e-9f) { have = 1; b_t = t; b_ci = kNoBody; b_p = xyz(s_p[q]); b_n = xyz(s_n[q]); }
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  if (tid == 0) {
+    if (!have) {
+      out_pt[r] = make_float4(0, 0, 0, __uint_as_float(0u));
+      out_n[r] = make_float4(0, 1, 0, 1.0f);
+    } else {
+      const uint32_t body = b_ci == kNoBody ? kNoBody : cbody[b_ci];
+      out_pt[r] = make_float4(b_p.x, b_p.y, b_p.z, __uint_as_float(body == kNoBody ? kNoBody : body + 1u));
+      out_n[r] = make_float4(b_n.x, b_n.y, b_n.z, clampf(b_t / ray.max_d, 0.0f, 1.0f));
+    }
+  }
+}
+
+// World::raycast over a batch (queries.rs:50-116): n rays with origin, direction (unit) and max
+// distance; out per ray (x y z, body id + 1 bits or 0 for none or 0xFFFFFFFF for the terrain)
+// and (normal, fraction).
+void WorldGpu::raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, float4* hit_n) {
+  auto& S = *s_;
+  cudaStream_t st = stream_;
+  if (n == 0) return;
+  S.ray_in.ensure(2ull * n + 2);
+  S.ray_pt.ensure(n + 1);
+  S.ray_n.ensure(n + 1);
+  RP_CUDA(cudaMemcpyAsync(S.ray_in.p, rays8, sizeof(RayIn) * n, cudaMemcpyHostToDevice, st));
+  HfDev hf{hf_h_.p, hf_nx_, hf_nz_, hf_sx_, hf_sz_, hf_ox_, hf_oz_, hf_min_, hf_max_};
+  k_raycast<<<n, QT, 0, st>>>(n, reinterpret_cast<const RayIn*>(S.ray_in.p), ncol_, col_body.p, col_kind.p, col_dims.p,
+                               pos.p, rot.p, alive_d.p, has_hf_, hf, S.ray_pt.p, S.ray_n.p);
+  RP_COUNT_LAUNCH(1);
+  RP_CUDA(cudaMemcpyAsync(hit_pt, S.ray_pt.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaMemcpyAsync(hit_n, S.ray_n.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace rp

@@ -5,6 +5,7 @@
 #include <cub/cub.cuh>
 
 #include "rp_narrow.cuh"
+#include "shape_aabb.cuh"
 #include "step_internal.cuh"
 
 namespace rp {
@@ -23,25 +24,6 @@ __global__ void k_forces(int nb, const float4* lin, const float4* __restrict__ a
   if (!dyn[i] || !awake[i]) return;
   f3 nl = xyz(l) + g * dt;
   if (vfin(nl)) lin_out[i] = f4(fin_v(nl), l.w);  // Bodies::set_vel (dynamics.rs:141-145)
-}
-
-// aabb_of (shape.rs:7-56) with Aabb::new's 1e-6 quantisation (aabb.rs:21-26)
-__device__ __forceinline__ void aabb_of(uint32_t kind, float4 d, f3 p, q4 q, f3* mn, f3* mx) {
-  f3 he;
-  if (kind == SH_SPHERE) he = splat(fabsf(d.x));
-  else if (kind == SH_BOX) {
-    m3 r = mfrom_quat(q);
-    m3 ar = mcols(vabs(r.c0), vabs(r.c1), vabs(r.c2));
-    he = mvec(ar, mk3(fabsf(d.x), fabsf(d.y), fabsf(d.z)));
-  } else {
-    f3 axis = qrot(q, mk3(0, 1, 0)) * fabsf(d.y);
-    he = vabs(axis) + splat(fabsf(d.x));
-  }
-  f3 a = p - he, b = p + he;
-  a = mk3(qf32(a.x), qf32(a.y), qf32(a.z));
-  b = mk3(qf32(b.x), qf32(b.y), qf32(b.z));
-  *mn = vmin(a, b);
-  *mx = vmax(a, b);
 }
 
 // update_colliders_aabb (world.rs:793-798) + the swept, margin-inflated box (step.rs:75-81):

@@ -185,6 +185,8 @@ struct WorldGpu::Scratch {
   // the wire snapshot
   DBuf<uint32_t> wire_flag, wire_off;
   DBuf<uint8_t> wire_buf;
+  // ray casts
+  DBuf<float4> ray_in, ray_pt, ray_n;
   DBuf<uint8_t> feat_valid;
   DBuf<float4> pred_used, s_pred;
   // solve groups (islands packed for one CTA each) and their shared-memory residents

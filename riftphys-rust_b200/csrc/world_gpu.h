@@ -161,6 +161,10 @@ class WorldGpu {
   // the chunks packed into host_out when it is given (throws std::length_error past cap).
   void pack_snapshot(unsigned long long tick, unsigned long long epoch, uint8_t* host_out, size_t cap, size_t* bytes,
                      uint32_t* chunks);
+  // World::raycast for n rays (queries.rs:50-116): rays8 per ray origin xyz, unit direction xyz,
+  // max distance, ignored body index bits (0xFFFFFFFF: none); per ray hit point xyz with w the hit
+  // body's id + 1 (0: no hit, 0xFFFFFFFF: the terrain) as bits, and normal xyz with w the fraction.
+  void raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, float4* hit_n);
   uint32_t body_of_collider(uint32_t c) const { return h_col_body_[c]; }
 
   // ---- rollback
