@@ -7,8 +7,8 @@
  * declares; its layout is the Rust definition at crates/riftphys-ffi/src/lib.rs:107-115.
  *
  * Each entry point below cites the reference function it replaces (file:line in
- * crates/riftphys-ffi/src/lib.rs). Ray casts are exported (run on the device); capsule sweeps and
- * the kinematic player controller are not.
+ * crates/riftphys-ffi/src/lib.rs). Ray casts and capsule sweeps are exported (run on the device);
+ * the kinematic player controller is not.
  */
 #pragma once
 
@@ -119,6 +119,26 @@ typedef struct RPhysRayHit {
  * colliders' AABBs and the heightfield's triangles along the ray; a miss is hit 0, body 0, fraction
  * 1, point 0, normal +Y. */
 RPhysResult rphys_world_raycast(const RPhysWorld* world, const RPhysRayQuery* query, RPhysRayHit* out_hit);
+typedef struct RPhysCapsuleSweepQuery {
+    RPhysVec3 from;
+    RPhysVec3 to;
+    float radius;           /* finite, > 0 */
+    float half_height;      /* finite, >= 0; the capsule is upright (local y) */
+    uint32_t ignore_body;   /* 1-based; 0 = none; the terrain sentinel is invalid here */
+} RPhysCapsuleSweepQuery;
+typedef struct RPhysCapsuleSweepHit {
+    RPhysBool hit;
+    uint32_t  body_id;      /* 1-based; 0 = none; RPHYS_TERRAIN_BODY_ID for the heightfield */
+    float     fraction;     /* of the way from -> to, in [0, 1]; 0 when it started overlapping */
+    RPhysBool started_overlapping;
+    RPhysVec3 point;
+    RPhysVec3 normal;
+} RPhysCapsuleSweepHit;
+/* World::sweep_capsule (queries.rs:118-249; lib.rs:1349-1411): overlap at from first (the
+ * narrowphase against colliders, then terrain triangles), else the capsule's tip and base spheres
+ * swept against the colliders' and the terrain triangles' AABBs. */
+RPhysResult rphys_world_capsule_sweep(const RPhysWorld* world, const RPhysCapsuleSweepQuery* query,
+                                      RPhysCapsuleSweepHit* out_hit);
 
 /* ===================== API ===================== */
 RPhysResult rphys_world_set_heightfield_i16(RPhysWorld* world, const RPhysHeightfieldDesc* hf,

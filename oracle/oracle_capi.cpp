@@ -473,6 +473,42 @@ RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q
   }
   return RPHYS_OK;
 }
+// rphys_world_capsule_sweep (riftphys-ffi/src/lib.rs:1349-1411, 482-492)
+RPhysResult rphys_world_capsule_sweep(const RPhysWorld* Wc, const RPhysCapsuleSweepQuery* q, RPhysCapsuleSweepHit* out) {
+  clear_err();
+  if (out) {
+    out->hit = RPHYS_FALSE; out->body_id = RPHYS_INVALID_BODY_ID; out->fraction = 1.0f; out->started_overlapping = RPHYS_FALSE;
+    out->point = RPhysVec3{0.0f, 0.0f, 0.0f}; out->normal = RPhysVec3{0.0f, 1.0f, 0.0f};
+  }
+  if (!Wc || !q || !out) return fail(RPHYS_ERR_NULL, "rphys_world_capsule_sweep: null arg");
+  auto fin3 = [](RPhysVec3 a) { return std::isfinite(a.x) && std::isfinite(a.y) && std::isfinite(a.z); };
+  if (!fin3(q->from)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: from contains NaN/Inf");
+  if (!fin3(q->to)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: to contains NaN/Inf");
+  if (!(std::isfinite(q->radius) && q->radius > 0.0f))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: radius must be finite and > 0");
+  if (!(std::isfinite(q->half_height) && q->half_height >= 0.0f))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: half_height must be finite and >= 0");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  uint32_t ignore = 0xFFFFFFFFu;
+  if (q->ignore_body != 0) {
+    RPhysResult r = live_id(W, q->ignore_body, "rphys_world_capsule_sweep.ignore_body", &ignore);
+    if (r) return r;
+  }
+  uint32_t body;
+  float toi;
+  bool overlap;
+  V3 p, n;
+  if (!W->w.sweep_capsule(v(q->from), v(q->to), q->radius, q->half_height, ignore, &body, &toi, &overlap, &p, &n))
+    return RPHYS_OK;
+  out->hit = RPHYS_TRUE;
+  out->body_id = body == 0xFFFFFFFFu ? RPHYS_TERRAIN_BODY_ID : body + 1;
+  out->fraction = om::clampf(toi, 0.0f, 1.0f);
+  out->started_overlapping = overlap ? RPHYS_TRUE : RPHYS_FALSE;
+  out->point = RPhysVec3{p.x, p.y, p.z};
+  out->normal = RPhysVec3{n.x, n.y, n.z};
+  return RPHYS_OK;
+}
 RPhysResult rphys_world_get_contacts(const RPhysWorld* Wc, RPhysContactEvent* out, uint32_t cap, uint32_t* out_count) {
   clear_err();
   if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_world_get_contacts: null arg");

@@ -897,6 +897,117 @@ bool World::raycast(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t
   return true;
 }
 
+// ---- capsule sweeps: riftphys-query/src/lib.rs:1-134 (sphere sweeps against AABBs)
+static const float kToiEps = 1e-9f;
+static bool ray_aabb_slab_unit(V3 o, V3 d, const Aabb& b, float* t_out, V3* n_out) {  // lib.rs:42-79
+  V3 inv{(o.x == o.x && std::fabs(d.x) > 1e-9f) ? 1.0f / d.x : 1.0e9f,
+         (o.y == o.y && std::fabs(d.y) > 1e-9f) ? 1.0f / d.y : 1.0e9f,
+         (o.z == o.z && std::fabs(d.z) > 1e-9f) ? 1.0f / d.z : 1.0e9f};
+  V3 t1{(b.min.x - o.x) * inv.x, (b.min.y - o.y) * inv.y, (b.min.z - o.z) * inv.z};
+  V3 t2{(b.max.x - o.x) * inv.x, (b.max.y - o.y) * inv.y, (b.max.z - o.z) * inv.z};
+  V3 tmin = vmin(t1, t2), tmax = vmax(t1, t2);
+  float t_enter = tmin.x;
+  V3 n{t1.x > t2.x ? 1.0f : -1.0f, 0.0f, 0.0f};
+  if (tmin.y > t_enter) { t_enter = tmin.y; n = V3{0.0f, t1.y > t2.y ? 1.0f : -1.0f, 0.0f}; }
+  if (tmin.z > t_enter) { t_enter = tmin.z; n = V3{0.0f, 0.0f, t1.z > t2.z ? 1.0f : -1.0f}; }
+  float t_exit = rmin(rmin(tmax.x, tmax.y), tmax.z);
+  if (t_enter <= t_exit && t_exit >= 0.0f && t_enter >= 0.0f && t_enter <= 1.0f) { *t_out = t_enter; *n_out = n; return true; }
+  return false;
+}
+static bool sweep_sphere_aabb(V3 p0, V3 v, float r, const Aabb& a, float* t, V3* n) {  // lib.rs:81-104, dt 1
+  V3 dir = mul(v, 1.0f);
+  Aabb e{sub(a.min, splat(r)), add(a.max, splat(r))};
+  if (dot(dir, dir) < 1e-12f) {
+    bool inside = p0.x >= e.min.x && p0.x <= e.max.x && p0.y >= e.min.y && p0.y <= e.max.y && p0.z >= e.min.z && p0.z <= e.max.z;
+    if (inside) { *t = 0.0f; *n = V3{0, 1, 0}; }
+    return inside;
+  }
+  return ray_aabb_slab_unit(p0, dir, e, t, n);
+}
+// sweep_two_spheres_aabbs over one AABB (lib.rs:118-134) with pick_better (lib.rs:14-33)
+static bool sweep_two(V3 tip0, V3 base0, V3 v, float r, const Aabb& a, float* t, V3* n, int* kind) {
+  bool have = false;
+  float tt;
+  V3 nn;
+  if (sweep_sphere_aabb(tip0, v, r, a, &tt, &nn)) { have = true; *t = tt; *n = nn; *kind = 0; }
+  if (sweep_sphere_aabb(base0, v, r, a, &tt, &nn)) {
+    if (!have || tt < *t - kToiEps) { have = true; *t = tt; *n = nn; *kind = 1; }
+  }
+  return have;
+}
+bool World::sweep_capsule(V3 from, V3 to, float radius, float half_height, uint32_t ignore, uint32_t* body,
+                          float* toi, bool* overlap, V3* point, V3* normal) const {
+  const V3 v = sub(to, from);
+  const float dist_sq = dot(v, v);
+  const Shape cap{SH_CAPSULE, radius, half_height, 0.0f, V3{0, 0, 0}, V3{0, 0, 0}, V3{0, 0, 0}};
+  const Iso cx{from, Q4{0, 0, 0, 1}};
+  *overlap = false;
+  for (size_t ci = 0; ci < colliders.size(); ++ci) {  // 1. overlap at t = 0
+    const Collider& c = colliders[ci];
+    if (c.body == ignore) continue;
+    Manifold m;
+    if (collide_shapes(cap, cx, c.shape, Iso{pos[c.body], rot[c.body]}, 0.0f, &m) && m.len > 0) {
+      *body = c.body; *toi = 0.0f; *overlap = true; *point = m.pts[0].position; *normal = m.normal;
+      return true;
+    }
+  }
+  std::vector<Shape> tris;
+  if (has_hf) {
+    hf_query(hf, aabb_of(cap, cx), tris);
+    for (const Shape& tr : tris) {
+      Manifold m;
+      if (collide_shapes(cap, cx, tr, Iso{V3{0, 0, 0}, Q4{0, 0, 0, 1}}, 0.0f, &m) && m.len > 0) {
+        *body = 0xFFFFFFFFu; *toi = 0.0f; *overlap = true; *point = m.pts[0].position; *normal = m.normal;
+        return true;
+      }
+    }
+  }
+  if (dist_sq < 1.0e-12f) return false;  // 2. stationary
+  const V3 tip0 = add(from, V3{0.0f, half_height, 0.0f}), base0 = add(from, V3{0.0f, -half_height, 0.0f});
+  bool have = false;
+  float bt = 0.0f;
+  size_t bci = 0;
+  const size_t kEnv = (size_t)-1;
+  V3 bp{0, 0, 0}, bn{0, 0, 0};
+  for (size_t ci = 0; ci < colliders.size(); ++ci) {  // 3. swept spheres against AABBs
+    const Collider& c = colliders[ci];
+    if (c.body == ignore) continue;
+    float t;
+    V3 n;
+    int kind;
+    if (!sweep_two(tip0, base0, v, radius, c.aabb, &t, &n, &kind)) continue;
+    t = clampf(t, 0.0f, 1.0f);
+    V3 c0 = kind == 0 ? tip0 : base0;
+    V3 p = sub(add(c0, mul(v, t)), mul(n, radius));
+    if (!have || (t < bt - kToiEps) || (std::fabs(t - bt) <= kToiEps && ci < bci)) { have = true; bt = t; bci = ci; bp = p; bn = n; }
+  }
+  if (has_hf) {
+    V3 ext = splat(radius + half_height);
+    Aabb sb = aabb_new(sub(vmin(from, to), ext), add(vmax(from, to), ext));
+    tris.clear();
+    hf_query(hf, sb, tris);
+    const Q4 id{0, 0, 0, 1};
+    for (const Shape& tr : tris) {
+      V3 wa = add(V3{0, 0, 0}, qrot(id, tr.ta)), wb = add(V3{0, 0, 0}, qrot(id, tr.tb)), wc = add(V3{0, 0, 0}, qrot(id, tr.tc));
+      Aabb ea = aabb_new(vmin(vmin(wa, wb), wc), vmax(vmax(wa, wb), wc));
+      float t;
+      V3 n;
+      int kind;
+      if (!sweep_two(tip0, base0, v, radius, ea, &t, &n, &kind)) continue;
+      t = clampf(t, 0.0f, 1.0f);
+      V3 c0 = kind == 0 ? tip0 : base0;
+      V3 p = sub(add(c0, mul(v, t)), mul(n, radius));
+      if (!have || t < bt - kToiEps) { have = true; bt = t; bci = kEnv; bp = p; bn = n; }
+    }
+  }
+  if (!have) return false;
+  *body = bci == kEnv ? 0xFFFFFFFFu : colliders[bci].body;
+  *toi = bt;
+  *point = bp;
+  *normal = bn;
+  return true;
+}
+
 // ------------------------------------------------------------------ solver
 // ContactConstraint (solver.rs:47-87), the fields the configured path reads.
 struct CC {

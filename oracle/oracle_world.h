@@ -191,6 +191,10 @@ struct World {
   // 0xFFFFFFFF. Returns false on a miss; body 0xFFFFFFFF is the terrain.
   bool raycast(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t* body, float* toi, V3* point,
                V3* normal) const;
+  // World::sweep_capsule (queries.rs:118-249): a y-axis capsule from -> to. Returns false on a
+  // miss; body 0xFFFFFFFF is the terrain; *overlap when it started overlapping (toi 0).
+  bool sweep_capsule(V3 from, V3 to, float radius, float half_height, uint32_t ignore, uint32_t* body, float* toi,
+                     bool* overlap, V3* point, V3* normal) const;
   // step.rs / provenance.rs
   void step(float dt);
   void step_hash(uint8_t out[32]) const;

@@ -136,6 +136,15 @@ class RayHit(Structure):
     _fields_ = [("hit", c_uint32), ("body_id", c_uint32), ("fraction", c_float), ("point", Vec3), ("normal", Vec3)]
 
 
+class CapsuleSweepQuery(Structure):
+    _fields_ = [("from_", Vec3), ("to", Vec3), ("radius", c_float), ("half_height", c_float), ("ignore_body", c_uint32)]
+
+
+class CapsuleSweepHit(Structure):
+    _fields_ = [("hit", c_uint32), ("body_id", c_uint32), ("fraction", c_float), ("started_overlapping", c_uint32),
+                ("point", Vec3), ("normal", Vec3)]
+
+
 class DistanceJointDesc(Structure):
     _fields_ = [("body_a", c_uint32), ("body_b", c_uint32), ("anchor_a", Vec3), ("anchor_b", Vec3),
                 ("rest", c_float), ("compliance", c_float), ("damping", c_float)]
@@ -273,6 +282,7 @@ ABI = [
     ("rphys_ext_set_joint_limit", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float, c_float]),
     ("rphys_ext_num_joints", c_uint32, [c_void_p, POINTER(c_uint32)]),
     ("rphys_ext_set_joint_limits", c_uint32, [c_void_p, c_void_p, c_uint32]),
+    ("rphys_world_capsule_sweep", c_uint32, [c_void_p, POINTER(CapsuleSweepQuery), POINTER(CapsuleSweepHit)]),
     ("rphys_world_raycast", c_uint32, [c_void_p, POINTER(RayQuery), POINTER(RayHit)]),
     ("rphys_ext_raycast_batch", c_uint32, [c_void_p, POINTER(RayQuery), c_uint32, POINTER(RayHit)]),
     ("rphys_ext_pack_snapshot", c_uint32, [c_void_p, c_uint64, c_uint64, c_void_p, c_uint64, POINTER(c_uint64),
@@ -555,6 +565,14 @@ class World:
         h = RayHit()
         self.c("rphys_world_raycast", byref(q), byref(h))
         return (bool(h.hit), h.body_id, h.fraction, (h.point.x, h.point.y, h.point.z), (h.normal.x, h.normal.y, h.normal.z))
+
+    def capsule_sweep(self, frm, to, radius, half_height, ignore=0):
+        """rphys_world_capsule_sweep: (hit, body_id, fraction, started_overlapping, point, normal)."""
+        q = CapsuleSweepQuery(Vec3(*frm), Vec3(*to), radius, half_height, ignore)
+        h = CapsuleSweepHit()
+        self.c("rphys_world_capsule_sweep", byref(q), byref(h))
+        return (bool(h.hit), h.body_id, h.fraction, bool(h.started_overlapping), (h.point.x, h.point.y, h.point.z),
+                (h.normal.x, h.normal.y, h.normal.z))
 
     def raycast_batch(self, origins, dirs, max_distance, ignore=None):
         """rphys_ext_raycast_batch over arrays of origins and directions: the hits as a numpy

@@ -531,6 +531,51 @@ RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q
     return (RPhysResult)RPHYS_OK;
   });
 }
+// lib.rs:482-492
+static void write_sweep_miss(RPhysCapsuleSweepHit* h) {
+  h->hit = RPHYS_FALSE;
+  h->body_id = RPHYS_INVALID_BODY_ID;
+  h->fraction = 1.0f;
+  h->started_overlapping = RPHYS_FALSE;
+  h->point = RPhysVec3{0.0f, 0.0f, 0.0f};
+  h->normal = RPhysVec3{0.0f, 1.0f, 0.0f};
+}
+RPhysResult rphys_world_capsule_sweep(const RPhysWorld* Wc, const RPhysCapsuleSweepQuery* q, RPhysCapsuleSweepHit* out) {
+  clear_err();
+  if (out) write_sweep_miss(out);
+  if (!Wc || !q || !out) return fail(RPHYS_ERR_NULL, "rphys_world_capsule_sweep: null arg");
+  auto fin3 = [](RPhysVec3 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+  if (!fin3(q->from)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: from contains NaN/Inf");
+  if (!fin3(q->to)) return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: to contains NaN/Inf");
+  if (!(std::isfinite(q->radius) && q->radius > 0.0f))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: radius must be finite and > 0");
+  if (!(std::isfinite(q->half_height) && q->half_height >= 0.0f))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_world_capsule_sweep: half_height must be finite and >= 0");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_world_capsule_sweep", [&]() {
+    LOCK;
+    uint32_t ignore = 0xFFFFFFFFu;
+    if (q->ignore_body != 0) {
+      RPhysResult r = live_id(W, q->ignore_body, "rphys_world_capsule_sweep.ignore_body", &ignore);
+      if (r) return r;
+    }
+    float q12[12] = {q->from.x, q->from.y, q->from.z, q->to.x, q->to.y, q->to.z, q->radius, q->half_height, 0, 0, 0, 0};
+    std::memcpy(q12 + 8, &ignore, 4);
+    float4 pt, n;
+    W->w->sweep_batch(1, q12, &pt, &n);
+    uint32_t code;
+    std::memcpy(&code, &pt.w, 4);
+    if (code == 0) return (RPhysResult)RPHYS_OK;
+    const bool overlap = n.w == 0.0f && std::signbit(n.w);
+    out->hit = RPHYS_TRUE;
+    out->body_id = code;
+    out->fraction = overlap ? 0.0f : n.w;
+    out->started_overlapping = overlap ? RPHYS_TRUE : RPHYS_FALSE;
+    out->point = RPhysVec3{pt.x, pt.y, pt.z};
+    out->normal = RPhysVec3{n.x, n.y, n.z};
+    return (RPhysResult)RPHYS_OK;
+  });
+}
 RPhysWorldSnapshot* rphys_world_snapshot_create(const RPhysWorld* Wc) {
   clear_err();
   if (!Wc) { fail(RPHYS_ERR_NULL, "rphys_world_snapshot_create: world is null"); return nullptr; }

@@ -3,6 +3,7 @@
 // box (terrain.rs:300-358, triangle.rs:215-235). One block per ray: its threads test a chunk of
 // colliders (or triangles) at once, then one thread takes the chunk's hits in index order with
 // the reference's replacement rule, so the result is the sequential scan's exactly.
+#include "rp_narrow.cuh"
 #include "shape_aabb.cuh"
 #include "step_internal.cuh"
 
@@ -215,6 +216,281 @@ __global__ void __launch_bounds__(QT) k_raycast(uint32_t nrays, const RayIn* __r
       out_n[r] = make_float4(b_n.x, b_n.y, b_n.z, clampf(b_t / ray.max_d, 0.0f, 1.0f));
     }
   }
+}
+
+// ---- capsule sweeps (queries.rs:118-249): a y-axis capsule at from, overlap at t = 0 first, then
+// its tip and base spheres swept along to - from against the colliders' and the terrain
+// triangles' AABBs (riftphys-query/src/lib.rs:1-134).
+struct SweepIn { f3 from, to; float r, hh; uint32_t ignore; uint32_t pad[3]; };
+static_assert(sizeof(SweepIn) == 48, "SweepIn: 12 words per sweep");
+constexpr float kToiEps = 1e-9f;  // TOI_EPS (lib.rs:4) and the sweep's eps (queries.rs:185)
+// ray_aabb_slab_unit (lib.rs:42-79)
+__device__ bool ray_aabb_slab_unit(f3 o, f3 d, f3 mn, f3 mx, float* t_out, f3* n_out) {
+  const f3 inv = mk3((o.x == o.x && fabsf(d.x) > 1e-9f) ? 1.0f / d.x : 1.0e9f,
+                     (o.y == o.y && fabsf(d.y) > 1e-9f) ? 1.0f / d.y : 1.0e9f,
+                     (o.z == o.z && fabsf(d.z) > 1e-9f) ? 1.0f / d.z : 1.0e9f);
+  const f3 t1 = mk3((mn.x - o.x) * inv.x, (mn.y - o.y) * inv.y, (mn.z - o.z) * inv.z);
+  const f3 t2 = mk3((mx.x - o.x) * inv.x, (mx.y - o.y) * inv.y, (mx.z - o.z) * inv.z);
+  const f3 tmin = vmin(t1, t2), tmax = vmax(t1, t2);
+  float t_enter = tmin.x;
+  f3 n = mk3(t1.x > t2.x ? 1.0f : -1.0f, 0.0f, 0.0f);
+  if (tmin.y > t_enter) { t_enter = tmin.y; n = mk3(0.0f, t1.y > t2.y ? 1.0f : -1.0f, 0.0f); }
+  if (tmin.z > t_enter) { t_enter = tmin.z; n = mk3(0.0f, 0.0f, t1.z > t2.z ? 1.0f : -1.0f); }
+  const float t_exit = rmin(rmin(tmax.x, tmax.y), tmax.z);
+  if (t_enter <= t_exit && t_exit >= 0.0f && t_enter >= 0.0f && t_enter <= 1.0f) { *t_out = t_enter; *n_out = n; return true; }
+  return false;
+}
+// sweep_sphere_aabb (lib.rs:81-104) with dt = 1
+__device__ bool sweep_sphere_aabb(f3 p0, f3 v, float r, f3 mn, f3 mx, float* t, f3* n) {
+  const f3 dir = v * 1.0f;
+  const f3 e = splat(r);
+  const f3 emn = mn - e, emx = mx + e;
+  if (len2(dir) < 1e-12f) {
+    const bool inside = p0.x >= emn.x && p0.x <= emx.x && p0.y >= emn.y && p0.y <= emx.y && p0.z >= emn.z && p0.z <= emx.z;
+    if (inside) { *t = 0.0f; *n = mk3(0, 1, 0); }
+    return inside;
+  }
+  return ray_aabb_slab_unit(p0, dir, emn, emx, t, n);
+}
+// sweep_two_spheres_aabbs for one AABB (lib.rs:118-134): the tip's hit, then the base's, by pick_better
+__device__ bool sweep_two(f3 tip0, f3 base0, f3 v, float r, f3 mn, f3 mx, float* t, f3* n, int* kind) {
+  bool have = false;
+  float tt;
+  f3 nn;
+  if (sweep_sphere_aabb(tip0, v, r, mn, mx, &tt, &nn)) { have = true; *t = tt; *n = nn; *kind = 0; }
+  if (sweep_sphere_aabb(base0, v, r, mn, mx, &tt, &nn)) {
+    // pick_better: nearer by more than TOI_EPS, or as near with the same target and a lower kind
+    // (never: the base is kind 1)
+    if (!have || tt < *t - kToiEps) { have = true; *t = tt; *n = nn; *kind = 1; }
+  }
+  return have;
+}
+
+__global__ void __launch_bounds__(QT) k_sweep(uint32_t nq, const SweepIn* __restrict__ qs, uint32_t ncol,
+                                              const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ ckind,
+                                              const float4* __restrict__ cdims, const float4* __restrict__ pos,
+                                              const float4* __restrict__ rot, const uint8_t* __restrict__ alive,
+                                              bool has_hf, HfDev hf, float4* out_pt, float4* out_n) {
+  const uint32_t r = blockIdx.x;
+  if (r >= nq) return;
+  const int tid = threadIdx.x;
+  const SweepIn q = qs[r];
+  __shared__ float s_t[QT];
+  __shared__ float4 s_p[QT], s_n[QT];
+  __shared__ uint8_t s_hit[QT];
+  __shared__ int done, have;
+  __shared__ float b_t;
+  __shared__ uint32_t b_code;  // id + 1 or 0xFFFFFFFF (terrain)
+  __shared__ f3 b_p, b_n;
+  __shared__ int b_over;
+  if (tid == 0) { done = 0; have = 0; b_t = 0.0f; b_code = 0; b_over = 0; }
+  __syncthreads();
+  Shape cap;
+  cap.kind = SH_CAPSULE; cap.a = q.r; cap.b = q.hh; cap.c = 0.0f;
+  Iso cx;
+  cx.pos = q.from; cx.rot = mkq(0, 0, 0, 1);
+  // 1. overlap at t = 0 (queries.rs:133-152): the first collider in order that touches
+  for (uint32_t base = 0; base < ncol && !done; base += QT) {
+    const uint32_t ci = base + tid;
+    bool hit = false;
+    if (ci < ncol) {
+      const uint32_t bd = cbody[ci];
+      if (alive[bd] && bd != q.ignore) {
+        const float4 d = cdims[ci];
+        Shape sh; sh.kind = ckind[ci]; sh.a = d.x; sh.b = d.y; sh.c = d.z;
+        Iso bx; bx.pos = xyz(pos[bd]); bx.rot = asq(rot[bd]);
+        Manifold m;
+        if (collide_pair(cap, cx, sh, bx, 0.0f, &m) && m.len > 0) {
+          hit = true;
+          s_p[tid] = f4(m.pts[0].position);
+          s_n[tid] = f4(m.normal);
+        }
+      }
+    }
+    s_hit[tid] = hit ? 1 : 0;
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 0; k < QT; ++k)
+        if (s_hit[k]) {
+          done = 1; have = 1; b_over = 1; b_t = 0.0f; b_code = cbody[base + k] + 1u;
+          b_p = xyz(s_p[k]); b_n = xyz(s_n[k]);
+          break;
+        }
+    }
+    __syncthreads();
+  }
+  // terrain triangles at t = 0 (queries.rs:154-175): the capsule's AABB window, first overlap
+  auto window = [&](f3 qmn, f3 qmx, long long* gx0, long long* gx1, long long* gz0, long long* gz1) {
+    const int nx = (int)hf.nx, nz = (int)hf.nz;
+    if (nx < 2 || nz < 2 || qmn.y > hf.max_y + 1.0f || qmx.y < hf.min_y - 1.0f) return false;
+    auto toi = [](float f) -> long long {
+      if (isnan(f)) return 0;
+      if (f >= 2147483647.0f) return 2147483647;
+      if (f <= -2147483648.0f) return -2147483648LL;
+      return (long long)f;
+    };
+    auto cl = [](long long v, long long lo, long long hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    *gx0 = cl(toi(floorf((qmn.x - hf.ox) / hf.sx)) - 1, 0, nx - 2);
+    *gx1 = cl(toi(ceilf((qmx.x - hf.ox) / hf.sx)) + 1, 0, nx - 2);
+    *gz0 = cl(toi(floorf((qmn.z - hf.oz) / hf.sz)) - 1, 0, nz - 2);
+    *gz1 = cl(toi(ceilf((qmx.z - hf.oz) / hf.sz)) + 1, 0, nz - 2);
+    return true;
+  };
+  auto tri_of = [&](long long gx0, unsigned long long wx, long long gz0, unsigned long long k, Tri* t) {
+    const unsigned long long cell = k >> 1;
+    const long long gz = gz0 + (long long)(cell / wx), gx = gx0 + (long long)(cell % wx);
+    auto H = [&](long long x, long long z) { return hf.h[(size_t)x + (size_t)z * hf.nx]; };
+    const float x0 = (float)gx * hf.sx + hf.ox, x1 = x0 + hf.sx;
+    const float z0 = (float)gz * hf.sz + hf.oz, z1 = z0 + hf.sz;
+    const f3 p00 = mk3(x0, H(gx, gz), z0), p10 = mk3(x1, H(gx + 1, gz), z0);
+    const f3 p01 = mk3(x0, H(gx, gz + 1), z1), p11 = mk3(x1, H(gx + 1, gz + 1), z1);
+    if (k & 1ull) { t->a = p10; t->b = p01; t->c = p11; }
+    else { t->a = p00; t->b = p01; t->c = p10; }
+  };
+  if (has_hf && !done) {
+    f3 mn, mx;
+    aabb_of(SH_CAPSULE, make_float4(q.r, q.hh, 0.0f, 0.0f), q.from, mkq(0, 0, 0, 1), &mn, &mx);
+    long long gx0, gx1, gz0, gz1;
+    if (window(mn, mx, &gx0, &gx1, &gz0, &gz1)) {
+      const unsigned long long wx = (unsigned long long)(gx1 - gx0 + 1), ntri = 2ull * wx * (unsigned long long)(gz1 - gz0 + 1);
+      for (unsigned long long base = 0; base < ntri && !done; base += QT) {
+        const unsigned long long k = base + tid;
+        bool hit = false;
+        if (k < ntri) {
+          Tri t;
+          tri_of(gx0, wx, gz0, k, &t);
+          Manifold m;
+          if (collide_tri(cap, cx, t, 0.0f, &m) && m.len > 0) { hit = true; s_p[tid] = f4(m.pts[0].position); s_n[tid] = f4(m.normal); }
+        }
+        s_hit[tid] = hit ? 1 : 0;
+        __syncthreads();
+        if (tid == 0) {
+          for (int k2 = 0; k2 < QT; ++k2)
+            if (s_hit[k2]) {
+              done = 1; have = 1; b_over = 1; b_t = 0.0f; b_code = 0xFFFFFFFFu;
+              b_p = xyz(s_p[k2]); b_n = xyz(s_n[k2]);
+              break;
+            }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  const f3 v = q.to - q.from;
+  if (!done && !(len2(v) < 1.0e-12f)) {
+    // 2. the swept tip and base spheres against the colliders' AABBs (queries.rs:179-212)
+    const f3 tip0 = q.from + mk3(0.0f, q.hh, 0.0f), base0 = q.from + mk3(0.0f, -q.hh, 0.0f);
+    __shared__ uint32_t b_ci;
+    __shared__ int s_kind[QT];
+    if (tid == 0) b_ci = 0;
+    for (uint32_t base = 0; base < ncol; base += QT) {
+      const uint32_t ci = base + tid;
+      bool hit = false;
+      if (ci < ncol) {
+        const uint32_t bd = cbody[ci];
+        if (alive[bd] && bd != q.ignore) {
+          f3 mn, mx;
+          aabb_of(ckind[ci], cdims[ci], xyz(pos[bd]), asq(rot[bd]), &mn, &mx);
+          float t;
+          f3 n;
+          int kind;
+          if (sweep_two(tip0, base0, v, q.r, mn, mx, &t, &n, &kind)) {
+            t = clampf(t, 0.0f, 1.0f);
+            const f3 c0 = kind == 0 ? tip0 : base0;
+            hit = true;
+            s_t[tid] = t; s_n[tid] = f4(n); s_p[tid] = f4((c0 + v * t) - n * q.r); s_kind[tid] = kind;
+          }
+        }
+      }
+      s_hit[tid] = hit ? 1 : 0;
+      __syncthreads();
+      if (tid == 0) {
+        for (int k = 0; k < QT; ++k) {
+          if (!s_hit[k]) continue;
+          const float t = s_t[k];
+          const uint32_t ci2 = base + k;
+          if (!have || (t < b_t - kToiEps) || (fabsf(t - b_t) <= kToiEps && ci2 < b_ci)) {
+            have = 1; b_t = t; b_ci = ci2; b_code = cbody[ci2] + 1u; b_p = xyz(s_p[k]); b_n = xyz(s_n[k]);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // the terrain triangles' AABBs in the swept box (queries.rs:214-236)
+    if (has_hf) {
+      const f3 ext = splat(q.r + q.hh);
+      f3 qa = vmin(q.from, q.to) - ext, qb = vmax(q.from, q.to) + ext;
+      qa = mk3(qf32(qa.x), qf32(qa.y), qf32(qa.z));
+      qb = mk3(qf32(qb.x), qf32(qb.y), qf32(qb.z));
+      long long gx0, gx1, gz0, gz1;
+      if (window(vmin(qa, qb), vmax(qa, qb), &gx0, &gx1, &gz0, &gz1)) {
+        const unsigned long long wx = (unsigned long long)(gx1 - gx0 + 1), ntri = 2ull * wx * (unsigned long long)(gz1 - gz0 + 1);
+        for (unsigned long long base = 0; base < ntri; base += QT) {
+          const unsigned long long k = base + tid;
+          bool hit = false;
+          if (k < ntri) {
+            Tri tr;
+            tri_of(gx0, wx, gz0, k, &tr);
+            // aabb_of(Triangle, identity) (shape.rs:60-70): the vertices through the identity pose
+            const q4 id = mkq(0, 0, 0, 1);
+            const f3 wa = mk3(0, 0, 0) + qrot(id, tr.a), wb = mk3(0, 0, 0) + qrot(id, tr.b), wc = mk3(0, 0, 0) + qrot(id, tr.c);
+            f3 a = vmin(vmin(wa, wb), wc), b = vmax(vmax(wa, wb), wc);
+            a = mk3(qf32(a.x), qf32(a.y), qf32(a.z));
+            b = mk3(qf32(b.x), qf32(b.y), qf32(b.z));
+            const f3 mn = vmin(a, b), mx = vmax(a, b);
+            float t;
+            f3 n;
+            int kind;
+            if (sweep_two(tip0, base0, v, q.r, mn, mx, &t, &n, &kind)) {
+              t = clampf(t, 0.0f, 1.0f);
+              const f3 c0 = kind == 0 ? tip0 : base0;
+              hit = true;
+              s_t[tid] = t; s_n[tid] = f4(n); s_p[tid] = f4((c0 + v * t) - n * q.r);
+            }
+          }
+          s_hit[tid] = hit ? 1 : 0;
+          __syncthreads();
+          if (tid == 0) {
+            for (int k2 = 0; k2 < QT; ++k2) {
+              if (!s_hit[k2]) continue;
+              const float t = s_t[k2];
+              if (!have || t < b_t - kToiEps) { have = 1; b_t = t; b_code = 0xFFFFFFFFu; b_p = xyz(s_p[k2]); b_n = xyz(s_n[k2]); }
+            }
+          }
+          __syncthreads();
+        }
+      }
+    }
+  }
+  if (tid == 0) {
+    if (!have) {
+      out_pt[r] = make_float4(0, 0, 0, __uint_as_float(0u));
+      out_n[r] = make_float4(0, 1, 0, 1.0f);
+    } else {
+      out_pt[r] = make_float4(b_p.x, b_p.y, b_p.z, __uint_as_float(b_code));
+      out_n[r] = make_float4(b_n.x, b_n.y, b_n.z, b_over ? -0.0f : clampf(b_t, 0.0f, 1.0f));
+    }
+  }
+}
+
+// World::sweep_capsule over a batch: per query from xyz, to xyz, radius, half height, ignored body
+// index bits (0xFFFFFFFF: none) and 3 words of padding; out as raycast_batch's, with the normal's
+// w = -0.0 when the capsule started overlapping (toi 0).
+void WorldGpu::sweep_batch(uint32_t n, const float* q12, float4* hit_pt, float4* hit_n) {
+  auto& S = *s_;
+  cudaStream_t st = stream_;
+  if (n == 0) return;
+  S.ray_in.ensure(3ull * n + 3);
+  S.ray_pt.ensure(n + 1);
+  S.ray_n.ensure(n + 1);
+  RP_CUDA(cudaMemcpyAsync(S.ray_in.p, q12, sizeof(SweepIn) * n, cudaMemcpyHostToDevice, st));
+  HfDev hf{hf_h_.p, hf_nx_, hf_nz_, hf_sx_, hf_sz_, hf_ox_, hf_oz_, hf_min_, hf_max_};
+  k_sweep<<<n, QT, 0, st>>>(n, reinterpret_cast<const SweepIn*>(S.ray_in.p), ncol_, col_body.p, col_kind.p, col_dims.p,
+                             pos.p, rot.p, alive_d.p, has_hf_, hf, S.ray_pt.p, S.ray_n.p);
+  RP_COUNT_LAUNCH(1);
+  RP_CUDA(cudaMemcpyAsync(hit_pt, S.ray_pt.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaMemcpyAsync(hit_n, S.ray_n.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaStreamSynchronize(st));
 }
 
 // World::raycast over a batch (queries.rs:50-116): n rays with origin, direction (unit) and max

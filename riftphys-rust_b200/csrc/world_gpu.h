@@ -165,6 +165,10 @@ class WorldGpu {
   // max distance, ignored body index bits (0xFFFFFFFF: none); per ray hit point xyz with w the hit
   // body's id + 1 (0: no hit, 0xFFFFFFFF: the terrain) as bits, and normal xyz with w the fraction.
   void raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, float4* hit_n);
+  // World::sweep_capsule for n queries (queries.rs:118-249): q12 per query from xyz, to xyz,
+  // radius, half height, ignored body index bits, 3 words unused; out as raycast_batch's, the
+  // normal's w -0.0 when the capsule started overlapping.
+  void sweep_batch(uint32_t n, const float* q12, float4* hit_pt, float4* hit_n);
   uint32_t body_of_collider(uint32_t c) const { return h_col_body_[c]; }
 
   // ---- rollback

@@ -99,3 +99,59 @@ def case_batched_rays_equal_single_calls(lib):
         assert np.array_equal(np.float32([frac, *point, *normal]), row[2:9]), (i, row, frac, point, normal)
     assert out[:, 0].view(np.uint32).sum() > 100  # most rays hit something
     w.close()
+
+
+# ---- capsule sweeps (World::sweep_capsule, queries.rs:118-249, through rphys_world_capsule_sweep)
+def case_capsule_sweep_hits_wall_and_ignore_works(lib):
+    """tests.rs:282-330"""
+    w = lib.world(8, 8)
+    wall = w.add_box((3.0, 1.0, 0.0), (0.125, 2.0, 2.0), dynamic=False)
+    hit, body, frac, over, point, normal = w.capsule_sweep((0.0, 1.0, 0.0), (6.0, 1.0, 0.0), 0.5, 0.5)
+    assert hit and body == wall and 0.0 <= frac <= 1.0 and not over
+    hit2, body2, frac2, _, _, _ = w.capsule_sweep((0.0, 1.0, 0.0), (6.0, 1.0, 0.0), 0.5, 0.5, ignore=wall)
+    assert not hit2 and body2 == 0 and frac2 == 1.0
+    w.close()
+
+
+def case_capsule_sweep_invalid_ignore_returns_invalid_id(lib):
+    """tests.rs:829-860"""
+    w = lib.world(8, 8)
+    try:
+        w.capsule_sweep((0.0, 1.0, 0.0), (6.0, 1.0, 0.0), 0.5, 0.5, ignore=999999)
+    except rp.RPhysError as e:
+        assert "0x2" in str(e), str(e)
+    else:
+        raise AssertionError("an invalid ignore_body was accepted")
+    w.close()
+
+
+def case_capsule_sweep_started_overlapping_sets_flag(lib):
+    """tests.rs:1344-1380"""
+    w = lib.world(8, 8)
+    wall = w.add_box((0.0, 1.0, 0.0), (1.0, 1.0, 1.0), dynamic=False)
+    hit, body, frac, over, _, _ = w.capsule_sweep((0.0, 1.0, 0.0), (0.0, 1.0, 0.0), 0.75, 0.5)
+    assert hit and body == wall and over and 0.0 <= frac <= 1.0
+    w.close()
+
+
+def case_capsule_sweep_argument_checks(lib):
+    w = lib.world(8, 8)
+    for args in (((float("nan"), 0, 0), (1, 0, 0), 0.5, 0.5), ((0, 0, 0), (1, 0, 0), 0.0, 0.5),
+                 ((0, 0, 0), (1, 0, 0), 0.5, -1.0)):
+        try:
+            w.capsule_sweep(*args)
+        except rp.RPhysError:
+            pass
+        else:
+            raise AssertionError(f"accepted {args}")
+    w.close()
+
+
+def random_sweeps(n, seed):
+    rng = np.random.default_rng(seed)
+    frm = np.column_stack([rng.uniform(-40, 40, n), rng.uniform(2, 20, n), rng.uniform(-40, 40, n)])
+    to = frm + np.column_stack([rng.normal(size=n) * 6, -np.abs(rng.normal(size=n)) * 10, rng.normal(size=n) * 6])
+    to[::13] = frm[::13]  # stationary
+    r = rng.uniform(0.1, 0.6, n)
+    hh = rng.uniform(0.0, 0.8, n)
+    return frm, to, r, hh

@@ -21,3 +21,17 @@ def test_rays_equal_the_oracle(oracle, gpu):
     rg = wg.raycast_batch(o, d, 90.0, ignore=5)
     assert np.array_equal(ro.view(np.uint32), rg.view(np.uint32))
     assert ro[:, 0].view(np.uint32).sum() > 1000
+
+
+def test_capsule_sweeps_equal_the_oracle(oracle, gpu):
+    wo, wg = RC.stepped_terrain(oracle), RC.stepped_terrain(gpu)
+    frm, to, r, hh = RC.random_sweeps(400, 12)
+    hits = 0
+    for i in range(400):
+        a = wo.capsule_sweep(tuple(frm[i]), tuple(to[i]), float(r[i]), float(hh[i]), ignore=3)
+        b = wg.capsule_sweep(tuple(frm[i]), tuple(to[i]), float(r[i]), float(hh[i]), ignore=3)
+        fa = np.float32([a[2], *a[4], *a[5]]).view(np.uint32)
+        fb = np.float32([b[2], *b[4], *b[5]]).view(np.uint32)
+        assert a[:2] == b[:2] and a[3] == b[3] and np.array_equal(fa, fb), (i, a, b)
+        hits += a[0]
+    assert hits > 100
