@@ -7,8 +7,8 @@
  * declares; its layout is the Rust definition at crates/riftphys-ffi/src/lib.rs:107-115.
  *
  * Each entry point below cites the reference function it replaces (file:line in
- * crates/riftphys-ffi/src/lib.rs). Ray casts and capsule sweeps are exported (run on the device);
- * the kinematic player controller is not.
+ * crates/riftphys-ffi/src/lib.rs). Ray casts, capsule sweeps and the kinematic player controller
+ * are exported and run on the device.
  */
 #pragma once
 
@@ -139,6 +139,24 @@ typedef struct RPhysCapsuleSweepHit {
  * swept against the colliders' and the terrain triangles' AABBs. */
 RPhysResult rphys_world_capsule_sweep(const RPhysWorld* world, const RPhysCapsuleSweepQuery* query,
                                       RPhysCapsuleSweepHit* out_hit);
+
+/* ===================== KINEMATIC PLAYER CONTROLLER ===================== */
+typedef struct RPhysPlayerDesc {
+    RPhysIsometry start_pose;
+    float radius;           /* finite, > 0 */
+    float height;           /* finite, > 0; the capsule's half height is height / 2 */
+    float speed;
+} RPhysPlayerDesc;
+/* World::add_player (world.rs:466-475; lib.rs:1580-1627): a static body with a capsule collider of
+ * radius 0.4 and half height 0.9, whatever the desc's size, which the controller's sweeps use.
+ * Takes one body and one collider of the world's capacity. Returns a 0-based player index. */
+RPhysResult rphys_add_player(RPhysWorld* world, const RPhysPlayerDesc* desc, uint32_t* out_player_idx);
+/* The player's move direction for the next ticks (lib.rs:1668-1693); any length, normalised by the
+ * step. */
+RPhysResult rphys_player_set_input(RPhysWorld* world, uint32_t player_idx, RPhysVec3 move_dir);
+/* The player body's pose and whether the last tick's slide found a floor (lib.rs:1629-1666). */
+RPhysResult rphys_player_get_pose(const RPhysWorld* world, uint32_t player_idx, RPhysIsometry* out_pose,
+                                  RPhysBool* out_grounded);
 
 /* ===================== API ===================== */
 RPhysResult rphys_world_set_heightfield_i16(RPhysWorld* world, const RPhysHeightfieldDesc* hf,

@@ -27,7 +27,7 @@ struct RPhysWorld {
   uint32_t bodies_created = 0, colliders_created = 0, max_bodies, max_colliders;
   RPhysWorld(uint32_t mb, uint32_t mc) : w(mb), max_bodies(mb), max_colliders(mc) {}
 };
-struct RPhysWorldSnapshot { Snapshot s; };
+struct RPhysWorldSnapshot { Snapshot s; std::vector<World::Player> players; };  // lib.rs:1696-1702
 
 static V3 v(const RPhysVec3& a) { return V3{a.x, a.y, a.z}; }
 static Q4 q(const RPhysQuat& a) { return Q4{a.x, a.y, a.z, a.w}; }
@@ -509,6 +509,53 @@ RPhysResult rphys_world_capsule_sweep(const RPhysWorld* Wc, const RPhysCapsuleSw
   out->normal = RPhysVec3{n.x, n.y, n.z};
   return RPHYS_OK;
 }
+
+// rphys_add_player (lib.rs:1580-1627): the desc is checked before the lock, then one body and one
+// collider of capacity; the controller gets the desc's size and speed after World::add_player.
+RPhysResult rphys_add_player(RPhysWorld* W, const RPhysPlayerDesc* d, uint32_t* out) {
+  clear_err();
+  if (out) *out = 0xFFFFFFFFu;
+  if (!W || !d || !out) return fail(RPHYS_ERR_NULL, "rphys_add_player: null arg");
+  if (!fin_iso(d->start_pose)) return fail(RPHYS_ERR_BAD_ARG, "rphys_add_player: pose contains NaN/Inf");
+  if (!(std::isfinite(d->radius) && d->radius > 0.0f)) return fail(RPHYS_ERR_BAD_ARG, "rphys_add_player: radius must be > 0");
+  if (!(std::isfinite(d->height) && d->height > 0.0f)) return fail(RPHYS_ERR_BAD_ARG, "rphys_add_player: height must be > 0");
+  std::lock_guard<std::mutex> g(W->mu);
+  if (W->bodies_created + 1ull > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, "rphys_add_player: body capacity exceeded");
+  if (W->colliders_created + 1ull > W->max_colliders) return fail(RPHYS_ERR_CAPACITY, "rphys_add_player: collider capacity exceeded");
+  const uint32_t idx = W->w.add_player(Iso{v(d->start_pose.pos), q(d->start_pose.rot)});
+  W->bodies_created++;
+  W->colliders_created++;
+  World::Player& p = W->w.players[idx];
+  p.radius = d->radius; p.height = d->height; p.speed = d->speed;
+  *out = idx;
+  return RPHYS_OK;
+}
+// rphys_player_get_pose (lib.rs:1629-1666): identity and false written first
+RPhysResult rphys_player_get_pose(const RPhysWorld* Wc, uint32_t idx, RPhysIsometry* out, RPhysBool* grounded) {
+  clear_err();
+  if (out) *out = RPhysIsometry{RPhysVec3{0, 0, 0}, RPhysQuat{0, 0, 0, 1}};
+  if (grounded) *grounded = RPHYS_FALSE;
+  if (!Wc || !out) return RPHYS_ERR_NULL;
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  if (idx >= W->w.players.size()) return fail(RPHYS_ERR_BAD_ARG, "rphys_player_get_pose: player_idx out of bounds");
+  const World::Player& p = W->w.players[idx];
+  const V3 pp = W->w.pos[p.body];
+  const Q4 qq = W->w.rot[p.body];
+  *out = RPhysIsometry{RPhysVec3{pp.x, pp.y, pp.z}, RPhysQuat{qq.x, qq.y, qq.z, qq.w}};
+  if (grounded) *grounded = p.grounded ? RPHYS_TRUE : RPHYS_FALSE;
+  return RPHYS_OK;
+}
+// rphys_player_set_input (lib.rs:1668-1693)
+RPhysResult rphys_player_set_input(RPhysWorld* W, uint32_t idx, RPhysVec3 dir) {
+  clear_err();
+  if (!W) return RPHYS_ERR_NULL;
+  if (!fin3(dir)) return fail(RPHYS_ERR_BAD_ARG, "rphys_player_set_input: move_dir NaN/Inf");
+  std::lock_guard<std::mutex> g(W->mu);
+  if (idx >= W->w.players.size()) return fail(RPHYS_ERR_BAD_ARG, "rphys_player_set_input: player_idx out of bounds");
+  W->w.players[idx].input = v(dir);
+  return RPHYS_OK;
+}
 RPhysResult rphys_world_get_contacts(const RPhysWorld* Wc, RPhysContactEvent* out, uint32_t cap, uint32_t* out_count) {
   clear_err();
   if (!Wc || !out_count) return fail(RPHYS_ERR_NULL, "rphys_world_get_contacts: null arg");
@@ -544,6 +591,7 @@ RPhysWorldSnapshot* rphys_world_snapshot_create(const RPhysWorld* Wc) {
     else { s->s.poses.push_back(Iso{V3{0, 0, 0}, Q4{0, 0, 0, 1}}); s->s.lin.push_back(V3{0, 0, 0}); s->s.ang.push_back(V3{0, 0, 0}); }
   }
   s->s.carried = w.carried_state();
+  s->players = w.players;
   return s;
 }
 RPhysResult rphys_world_snapshot_restore(RPhysWorld* W, const RPhysWorldSnapshot* s) {
@@ -552,6 +600,7 @@ RPhysResult rphys_world_snapshot_restore(RPhysWorld* W, const RPhysWorldSnapshot
   std::lock_guard<std::mutex> g(W->mu);
   World& w = W->w;
   w.tick = s->s.tick;
+  w.players = s->players;  // lib.rs:1775
   for (uint32_t i = 0; i < s->s.poses.size(); ++i) {
     if (i < w.alive.size() && w.alive[i] && i < w.num_bodies()) {
       w.set_body_pose(i, s->s.poses[i]);
@@ -576,6 +625,8 @@ RPhysResult rphys_ext_snapshot_restore_exact(RPhysWorld* W, const RPhysWorldSnap
     w.lin[i] = s->s.lin[i];
     w.ang[i] = s->s.ang[i];
   }
+  w.players = s->players;
+  w.update_colliders_aabb();  // a world clone holds the AABBs of the stored poses
   w.restore_carried_state(s->s.carried);
   return RPHYS_OK;
 }

@@ -1008,6 +1008,80 @@ bool World::sweep_capsule(V3 from, V3 to, float radius, float half_height, uint3
   return true;
 }
 
+// ---- the kinematic player controller
+uint32_t World::add_player(const Iso& pose) {
+  uint32_t id = add_body(pose, V3{0, 0, 0}, V3{0, 0, 0}, 0.0f, V3{0, 0, 0}, false);
+  Player p;
+  p.body = id;
+  add_collider(id, Shape{SH_CAPSULE, p.radius, p.height * 0.5f, 0.0f, V3{0, 0, 0}, V3{0, 0, 0}, V3{0, 0, 0}}, 0);
+  players.push_back(p);
+  return (uint32_t)players.size() - 1;
+}
+static bool aabb_intersects(const Aabb& a, const Aabb& b) {  // Aabb::intersects (aabb.rs:75-79)
+  return a.min.x <= b.max.x && a.max.x >= b.min.x && a.min.y <= b.max.y && a.max.y >= b.min.y && a.min.z <= b.max.z &&
+         a.max.z >= b.min.z;
+}
+// World::update_players (step.rs:544-639): gravity or the sticky floor, the input direction at the
+// player's speed, then up to four sweep-and-slide passes: the first terrain triangle, else the first
+// collider, within 5 cm of the moved capsule pushes it out and kills the motion into it (a floor
+// grounds it; a dynamic body is woken and kicked). Poses move through Bodies::set_pose, so the
+// colliders' stored AABBs stay those of the step's start until the tick updates them.
+void World::update_players(float dt) {
+  for (size_t pi = 0; pi < players.size(); ++pi) {
+    Player pl = players[pi];
+    V3 p = pos[pl.body];
+    if (!pl.grounded) pl.vertical_vel -= 9.81f * dt;
+    else if (pl.vertical_vel <= 0.0f) pl.vertical_vel = -0.5f;
+    const float im2 = dot(pl.input, pl.input);
+    V3 move_dir = im2 > 1e-6f ? divs(pl.input, std::sqrt(im2)) : V3{0, 0, 0};
+    V3 desired = add(mul(mul(move_dir, pl.speed), dt), V3{0.0f, pl.vertical_vel * dt, 0.0f});
+    pl.grounded = false;
+    for (int it = 0; it < 4; ++it) {
+      if (dot(desired, desired) < 1e-6f) break;
+      const Iso xf{add(p, desired), Q4{0, 0, 0, 1}};
+      const Shape sh{SH_CAPSULE, pl.radius, pl.height * 0.5f, 0.0f, V3{0, 0, 0}, V3{0, 0, 0}, V3{0, 0, 0}};
+      const Aabb box = aabb_of(sh, xf);
+      bool have = false;
+      V3 hn{0, 0, 0};
+      float hpen = 0.0f;
+      long hbody = -1;
+      if (has_hf) {
+        std::vector<Shape> tris;
+        hf_query(hf, box, tris);
+        for (const Shape& tr : tris) {
+          Manifold m{};
+          if (collide_shapes(sh, xf, tr, Iso{V3{0, 0, 0}, Q4{0, 0, 0, 1}}, 0.05f, &m)) {
+            have = true; hn = m.pts[0].normal; hpen = m.pts[0].penetration;
+            break;
+          }
+        }
+      }
+      if (!have) {
+        for (const Collider& c : colliders) {
+          if (c.body == pl.body || !aabb_intersects(box, c.aabb)) continue;
+          Manifold m{};
+          if (collide_shapes(sh, xf, c.shape, Iso{pos[c.body], rot[c.body]}, 0.05f, &m)) {
+            have = true; hn = m.pts[0].normal; hpen = m.pts[0].penetration; hbody = (long)c.body;
+            break;
+          }
+        }
+      }
+      if (!have) break;
+      if (hn.y > 0.6f) { pl.grounded = true; pl.vertical_vel = 0.0f; }
+      desired = add(desired, mul(hn, hpen + 0.001f));
+      const float d = dot(desired, hn);
+      if (d < 0.0f) desired = sub(desired, mul(hn, d));
+      if (hbody >= 0 && dyn[(size_t)hbody]) {
+        wake((uint32_t)hbody);
+        apply_impulse((uint32_t)hbody, mul(neg(hn), 10.0f));
+      }
+    }
+    p = add(p, desired);
+    set_pose(pl.body, Iso{p, Q4{0, 0, 0, 1}});
+    players[pi] = pl;
+  }
+}
+
 // ------------------------------------------------------------------ solver
 // ContactConstraint (solver.rs:47-87), the fields the configured path reads.
 struct CC {
@@ -1349,6 +1423,7 @@ void World::step(float dt) {
   const uint32_t count = num_bodies();
   tick += 1;
   stats = Stats{};
+  update_players(dt);  // step.rs:51
   // --- Stage 1: forces (step.rs:53-68)
   std::vector<V3> pre_lin(lin.begin(), lin.end()), pre_ang(ang.begin(), ang.end());
   V3 g{q6(gravity.x), q6(gravity.y), q6(gravity.z)};  // grav_eval Uniform (gravity.rs:79-87)

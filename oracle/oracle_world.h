@@ -187,6 +187,14 @@ struct World {
   void update_colliders_aabb();
   CarriedState carried_state() const;
   void restore_carried_state(const CarriedState& s);
+  // PlayerController (world.rs:45-70) and World::add_player (world.rs:466-475): a static body with a
+  // capsule collider of the controller's default size (radius 0.4, half height 0.9), whatever size
+  // the controller is given afterwards.
+  struct Player { uint32_t body; float radius = 0.4f, height = 1.8f, speed = 5.0f; bool grounded = false;
+                  float vertical_vel = 0.0f; V3 input{0, 0, 0}; };
+  std::vector<Player> players;
+  uint32_t add_player(const Iso& pose);
+  void update_players(float dt);  // step.rs:544-639
   // World::raycast (queries.rs:50-116): dir normalised here again; ignore a body index or
   // 0xFFFFFFFF. Returns false on a miss; body 0xFFFFFFFF is the terrain.
   bool raycast(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t* body, float* toi, V3* point,

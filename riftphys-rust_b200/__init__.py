@@ -145,6 +145,10 @@ class CapsuleSweepHit(Structure):
                 ("point", Vec3), ("normal", Vec3)]
 
 
+class PlayerDesc(Structure):
+    _fields_ = [("start_pose", Isometry), ("radius", c_float), ("height", c_float), ("speed", c_float)]
+
+
 class DistanceJointDesc(Structure):
     _fields_ = [("body_a", c_uint32), ("body_b", c_uint32), ("anchor_a", Vec3), ("anchor_b", Vec3),
                 ("rest", c_float), ("compliance", c_float), ("damping", c_float)]
@@ -284,6 +288,9 @@ ABI = [
     ("rphys_ext_set_joint_limits", c_uint32, [c_void_p, c_void_p, c_uint32]),
     ("rphys_world_capsule_sweep", c_uint32, [c_void_p, POINTER(CapsuleSweepQuery), POINTER(CapsuleSweepHit)]),
     ("rphys_world_raycast", c_uint32, [c_void_p, POINTER(RayQuery), POINTER(RayHit)]),
+    ("rphys_add_player", c_uint32, [c_void_p, POINTER(PlayerDesc), POINTER(c_uint32)]),
+    ("rphys_player_set_input", c_uint32, [c_void_p, c_uint32, Vec3]),
+    ("rphys_player_get_pose", c_uint32, [c_void_p, c_uint32, POINTER(Isometry), POINTER(c_uint32)]),
     ("rphys_ext_raycast_batch", c_uint32, [c_void_p, POINTER(RayQuery), c_uint32, POINTER(RayHit)]),
     ("rphys_ext_pack_snapshot", c_uint32, [c_void_p, c_uint64, c_uint64, c_void_p, c_uint64, POINTER(c_uint64),
                                            POINTER(c_uint32)]),
@@ -573,6 +580,23 @@ class World:
         self.c("rphys_world_capsule_sweep", byref(q), byref(h))
         return (bool(h.hit), h.body_id, h.fraction, bool(h.started_overlapping), (h.point.x, h.point.y, h.point.z),
                 (h.normal.x, h.normal.y, h.normal.z))
+
+    def add_player(self, pose, radius=0.4, height=1.8, speed=5.0):
+        """rphys_add_player: a kinematic capsule controller; returns its 0-based index."""
+        d = PlayerDesc(pose, radius, height, speed)
+        out = c_uint32(0)
+        self.c("rphys_add_player", byref(d), byref(out))
+        return out.value
+
+    def player_set_input(self, idx, move_dir):
+        self.c("rphys_player_set_input", idx, Vec3(*move_dir))
+
+    def player_pose(self, idx):
+        """rphys_player_get_pose: ((x, y, z), (qx, qy, qz, qw), grounded)."""
+        p = Isometry()
+        g = c_uint32(0)
+        self.c("rphys_player_get_pose", idx, byref(p), byref(g))
+        return (p.pos.x, p.pos.y, p.pos.z), (p.rot.x, p.rot.y, p.rot.z, p.rot.w), bool(g.value)
 
     def raycast_batch(self, origins, dirs, max_distance, ignore=None):
         """rphys_ext_raycast_batch over arrays of origins and directions: the hits as a numpy

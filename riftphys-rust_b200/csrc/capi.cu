@@ -576,6 +576,60 @@ RPhysResult rphys_world_capsule_sweep(const RPhysWorld* Wc, const RPhysCapsuleSw
     return (RPhysResult)RPHYS_OK;
   });
 }
+// rphys_add_player (lib.rs:1580-1627): the desc checked, then one body and one collider of
+// capacity; World::add_player's body and capsule, the desc's size and speed on the controller.
+RPhysResult rphys_add_player(RPhysWorld* W, const RPhysPlayerDesc* d, uint32_t* out) {
+  clear_err();
+  if (out) *out = 0xFFFFFFFFu;
+  if (!W || !d || !out) return fail(RPHYS_ERR_NULL, "rphys_add_player: null arg");
+  if (!fin_iso(d->start_pose)) return fail(RPHYS_ERR_BAD_ARG, "rphys_add_player: pose contains NaN/Inf");
+  if (!(std::isfinite(d->radius) && d->radius > 0.0f)) return fail(RPHYS_ERR_BAD_ARG, "rphys_add_player: radius must be > 0");
+  if (!(std::isfinite(d->height) && d->height > 0.0f)) return fail(RPHYS_ERR_BAD_ARG, "rphys_add_player: height must be > 0");
+  return guard("rphys_add_player", [&]() {
+    LOCK;
+    if (W->bodies_created + 1ull > W->max_bodies) return fail(RPHYS_ERR_CAPACITY, "rphys_add_player: body capacity exceeded");
+    if (W->colliders_created + 1ull > W->max_colliders)
+      return fail(RPHYS_ERR_CAPACITY, "rphys_add_player: collider capacity exceeded");
+    float p[7];
+    pose7(d->start_pose, p);
+    const uint32_t idx = W->w->add_player(p, d->radius, d->height, d->speed);
+    W->bodies_created++;
+    W->colliders_created++;
+    *out = idx;
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+// rphys_player_get_pose (lib.rs:1629-1666): identity and false written first
+RPhysResult rphys_player_get_pose(const RPhysWorld* Wc, uint32_t idx, RPhysIsometry* out, RPhysBool* grounded) {
+  clear_err();
+  if (out) *out = RPhysIsometry{RPhysVec3{0, 0, 0}, RPhysQuat{0, 0, 0, 1}};
+  if (grounded) *grounded = RPHYS_FALSE;
+  if (!Wc || !out) return RPHYS_ERR_NULL;
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_player_get_pose", [&]() {
+    LOCK;
+    if (idx >= W->w->num_players()) return fail(RPHYS_ERR_BAD_ARG, "rphys_player_get_pose: player_idx out of bounds");
+    float p[7];
+    bool g = false;
+    W->w->get_player(idx, p, &g);
+    *out = RPhysIsometry{RPhysVec3{p[0], p[1], p[2]}, RPhysQuat{p[3], p[4], p[5], p[6]}};
+    if (grounded) *grounded = g ? RPHYS_TRUE : RPHYS_FALSE;
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+// rphys_player_set_input (lib.rs:1668-1693)
+RPhysResult rphys_player_set_input(RPhysWorld* W, uint32_t idx, RPhysVec3 dir) {
+  clear_err();
+  if (!W) return RPHYS_ERR_NULL;
+  if (!fin3(dir)) return fail(RPHYS_ERR_BAD_ARG, "rphys_player_set_input: move_dir NaN/Inf");
+  return guard("rphys_player_set_input", [&]() {
+    LOCK;
+    if (idx >= W->w->num_players()) return fail(RPHYS_ERR_BAD_ARG, "rphys_player_set_input: player_idx out of bounds");
+    const float v3[3] = {dir.x, dir.y, dir.z};
+    W->w->set_player_input(idx, v3);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
 RPhysWorldSnapshot* rphys_world_snapshot_create(const RPhysWorld* Wc) {
   clear_err();
   if (!Wc) { fail(RPHYS_ERR_NULL, "rphys_world_snapshot_create: world is null"); return nullptr; }

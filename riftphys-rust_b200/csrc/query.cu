@@ -3,6 +3,7 @@
 // box (terrain.rs:300-358, triangle.rs:215-235). One block per ray: its threads test a chunk of
 // colliders (or triangles) at once, then one thread takes the chunk's hits in index order with
 // the reference's replacement rule, so the result is the sequential scan's exactly.
+#include "hf_cells.cuh"
 #include "rp_narrow.cuh"
 #include "shape_aabb.cuh"
 #include "step_internal.cuh"
@@ -100,8 +101,6 @@ __device__ f3 tri_normal(f3 a, f3 b, f3 c) {
   float rcp = 1.0f / sqrtf(dot(n, n));
   return (fin(rcp) && rcp > 0.0f) ? n * rcp : mk3(0, 0, 0);
 }
-
-struct HfDev { const float* h; uint32_t nx, nz; float sx, sz, ox, oz, min_y, max_y; };
 
 __global__ void __launch_bounds__(QT) k_raycast(uint32_t nrays, const RayIn* __restrict__ rays, uint32_t ncol,
                                                 const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ ckind,
@@ -321,31 +320,10 @@ __global__ void __launch_bounds__(QT) k_sweep(uint32_t nq, const SweepIn* __rest
   }
   // terrain triangles at t = 0 (queries.rs:154-175): the capsule's AABB window, first overlap
   auto window = [&](f3 qmn, f3 qmx, long long* gx0, long long* gx1, long long* gz0, long long* gz1) {
-    const int nx = (int)hf.nx, nz = (int)hf.nz;
-    if (nx < 2 || nz < 2 || qmn.y > hf.max_y + 1.0f || qmx.y < hf.min_y - 1.0f) return false;
-    auto toi = [](float f) -> long long {
-      if (isnan(f)) return 0;
-      if (f >= 2147483647.0f) return 2147483647;
-      if (f <= -2147483648.0f) return -2147483648LL;
-      return (long long)f;
-    };
-    auto cl = [](long long v, long long lo, long long hi) { return v < lo ? lo : (v > hi ? hi : v); };
-    *gx0 = cl(toi(floorf((qmn.x - hf.ox) / hf.sx)) - 1, 0, nx - 2);
-    *gx1 = cl(toi(ceilf((qmx.x - hf.ox) / hf.sx)) + 1, 0, nx - 2);
-    *gz0 = cl(toi(floorf((qmn.z - hf.oz) / hf.sz)) - 1, 0, nz - 2);
-    *gz1 = cl(toi(ceilf((qmx.z - hf.oz) / hf.sz)) + 1, 0, nz - 2);
-    return true;
+    return hf_window(hf, qmn, qmx, gx0, gx1, gz0, gz1);
   };
   auto tri_of = [&](long long gx0, unsigned long long wx, long long gz0, unsigned long long k, Tri* t) {
-    const unsigned long long cell = k >> 1;
-    const long long gz = gz0 + (long long)(cell / wx), gx = gx0 + (long long)(cell % wx);
-    auto H = [&](long long x, long long z) { return hf.h[(size_t)x + (size_t)z * hf.nx]; };
-    const float x0 = (float)gx * hf.sx + hf.ox, x1 = x0 + hf.sx;
-    const float z0 = (float)gz * hf.sz + hf.oz, z1 = z0 + hf.sz;
-    const f3 p00 = mk3(x0, H(gx, gz), z0), p10 = mk3(x1, H(gx + 1, gz), z0);
-    const f3 p01 = mk3(x0, H(gx, gz + 1), z1), p11 = mk3(x1, H(gx + 1, gz + 1), z1);
-    if (k & 1ull) { t->a = p10; t->b = p01; t->c = p11; }
-    else { t->a = p00; t->b = p01; t->c = p10; }
+    hf_tri(hf, gx0, wx, gz0, k, t);
   };
   if (has_hf && !done) {
     f3 mn, mx;

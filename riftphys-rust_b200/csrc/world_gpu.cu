@@ -347,6 +347,7 @@ void WorldGpu::get_row_predictions(std::vector<float>& pred4) {
 }
 
 void WorldGpu::begin_world() {
+  if (!h_players_.empty()) throw std::invalid_argument("a world with players cannot become a batch");
   batch_ = true;
   h_wb_start_.push_back(nb_);
   h_wc_start_.push_back(ncol_);
@@ -484,6 +485,7 @@ void WorldGpu::step(float dt) {
   AllocStreamScope alloc_scope(stream_);
   tick_ += 1;
   RP_CUDA(cudaMemsetAsync(d_stats.p, 0, STAT_COUNT * 4, stream_));
+  run_players(dt);  // step.rs:51
   StepCtx ctx;
   ctx.dt = dt;
   ctx.g = mk3(q6(gravity_.x), q6(gravity_.y), q6(gravity_.z));
@@ -593,6 +595,7 @@ SnapshotGpu* WorldGpu::snapshot_create() {  // lib.rs:1707-1752 + carried_state 
   cp(s->jw_tag.p, jw_tag.p, kJointRows * (size_t)s->nj);
   cp(s->jw_lam.p, jw_lam.p, 4 * kJointRows * (size_t)s->nj);
   RP_CUDA(cudaStreamSynchronize(stream_));
+  s->players = players();
   return s;
 }
 // Every stored bit back (a World clone, not the FFI's pose injection): for rollback that must
@@ -615,6 +618,7 @@ void WorldGpu::snapshot_restore_exact(const SnapshotGpu* s) {
   n_warm = s->n_warm;
   restore_joint_warm(s);
   RP_CUDA(cudaStreamSynchronize(stream_));
+  set_players(s->players);
 }
 // The joint cache as the snapshot held it; joints added since have no entry.
 void WorldGpu::restore_joint_warm(const SnapshotGpu* s) {
@@ -651,6 +655,7 @@ void WorldGpu::snapshot_restore(const SnapshotGpu* s) {  // lib.rs:1754-1793 + r
   restore_joint_warm(s);
   filter_joint_warm_alive();
   RP_CUDA(cudaStreamSynchronize(stream_));
+  set_players(s->players);  // lib.rs:1775
 }
 void WorldGpu::snapshot_free(SnapshotGpu* s) { delete s; }
 

@@ -47,6 +47,18 @@ struct DBuf {
   ~DBuf() { release(); }
 };
 
+// PlayerController (world.rs:45-70) as the device keeps it, 16 words: the controller's state, its
+// input, and the pose its body had when the tick's player pass began.
+struct PlayerGpu {
+  uint32_t body;
+  float radius, height, speed;
+  float vvel;
+  uint32_t grounded;
+  float in[3];
+  float p0[3], q0[4];
+};
+static_assert(sizeof(PlayerGpu) == 64, "PlayerGpu: 16 words");
+
 struct SnapshotGpu;
 
 class WorldGpu {
@@ -171,6 +183,20 @@ class WorldGpu {
   void sweep_batch(uint32_t n, const float* q12, float4* hit_pt, float4* hit_n);
   uint32_t body_of_collider(uint32_t c) const { return h_col_body_[c]; }
 
+  // ---- the kinematic player controller (world.rs:466-475; step.rs:544-639). The device holds
+  // the controllers between ticks; the host copy is refreshed when the host reads or changes one.
+  uint32_t add_player(const float pose[7], float radius, float height, float speed);
+  uint32_t num_players() const { return (uint32_t)h_players_.size(); }
+  void set_player_input(uint32_t i, const float dir[3]);
+  void get_player(uint32_t i, float pose[7], bool* grounded);
+  const std::vector<PlayerGpu>& players();   // the controllers as the device has them
+  void set_players(const std::vector<PlayerGpu>& v);
+  void run_players(float dt);                // World::update_players, at the start of a tick
+  std::vector<PlayerGpu> h_players_;
+  bool players_dev_newer_ = false;
+  DBuf<PlayerGpu> players_d;
+  DBuf<uint32_t> player_of_d;                // per body: its controller's index, or 0xFFFFFFFF
+
   // ---- rollback
   SnapshotGpu* snapshot_create();
   void snapshot_restore(const SnapshotGpu* s);
@@ -253,6 +279,7 @@ struct SnapshotGpu {
   DBuf<uint32_t> jw_n;
   DBuf<uint8_t> jw_tag;
   DBuf<float> jw_lam;
+  std::vector<PlayerGpu> players;  // lib.rs:1696-1702
 };
 
 // MassProps::from_*_density (riftphys-geom/src/mass.rs:75-145); host side.
