@@ -290,6 +290,13 @@ RPhysResult rphys_ext_pack_snapshot(RPhysWorld* world, uint64_t tick, uint64_t e
  * (all-or-nothing), then out[i] as rphys_world_raycast would write it for queries[i]. */
 RPhysResult rphys_ext_raycast_batch(const RPhysWorld* world, const RPhysRayQuery* queries, uint32_t n,
                                     RPhysRayHit* out);
+/* World::raycast_exact (crates/riftphys-world/src/world/queries.rs:18-48; ray_shape,
+ * crates/riftphys-geom/src/raycast.rs:13-130) for n rays: the true shapes (rotated boxes, spheres,
+ * capsules, terrain triangles) instead of the colliders' AABBs. Skips ignore_body (the reference's
+ * skip predicate, for one body). Checked and normalised as rphys_world_raycast; normals face the
+ * ray, and a ray starting inside a solid hits at fraction 0 with normal -dir. */
+RPhysResult rphys_ext_raycast_exact_batch(const RPhysWorld* world, const RPhysRayQuery* queries, uint32_t n,
+                                          RPhysRayHit* out);
 
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:

@@ -421,7 +421,7 @@ static void write_raycast_miss(RPhysRayHit* h) {
   h->point = RPhysVec3{0.0f, 0.0f, 0.0f};
   h->normal = RPhysVec3{0.0f, 1.0f, 0.0f};
 }
-static RPhysResult raycast_one(RPhysWorld* W, const RPhysRayQuery& q, const char* ctx, RPhysRayHit* out) {
+static RPhysResult raycast_one(RPhysWorld* W, const RPhysRayQuery& q, const char* ctx, RPhysRayHit* out, bool exact = false) {
   write_raycast_miss(out);
   auto fin3 = [](RPhysVec3 v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
   if (!fin3(q.origin)) return fail(RPHYS_ERR_BAD_ARG, std::string(ctx) + ": origin contains NaN/Inf");
@@ -442,7 +442,9 @@ static RPhysResult raycast_one(RPhysWorld* W, const RPhysRayQuery& q, const char
   uint32_t body;
   float toi;
   V3 p, n;
-  if (!W->w.raycast(v(q.origin), d, q.max_distance, ignore, &body, &toi, &p, &n)) return RPHYS_OK;
+  const bool hit = exact ? W->w.raycast_exact(v(q.origin), d, q.max_distance, ignore, &body, &toi, &p, &n)
+                         : W->w.raycast(v(q.origin), d, q.max_distance, ignore, &body, &toi, &p, &n);
+  if (!hit) return RPHYS_OK;
   out->hit = RPHYS_TRUE;
   out->body_id = body == 0xFFFFFFFFu ? RPHYS_TERRAIN_BODY_ID : body + 1;
   out->fraction = om::clampf(toi, 0.0f, 1.0f);
@@ -474,6 +476,22 @@ RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q
   return RPHYS_OK;
 }
 // rphys_world_capsule_sweep (riftphys-ffi/src/lib.rs:1349-1411, 482-492)
+// World::raycast_exact (queries.rs:18-48) for n rays, checked and normalised as rphys_world_raycast
+RPhysResult rphys_ext_raycast_exact_batch(const RPhysWorld* Wc, const RPhysRayQuery* q, uint32_t n, RPhysRayHit* out) {
+  clear_err();
+  if (!Wc || ((!q || !out) && n)) return fail(RPHYS_ERR_NULL, "rphys_ext_raycast_exact_batch: null arg");
+  for (uint32_t i = 0; i < n; ++i) write_raycast_miss(out + i);
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  for (uint32_t i = 0; i < n; ++i) {
+    RPhysResult r = raycast_one(W, q[i], "rphys_ext_raycast_exact_batch", out + i, true);
+    if (r) {
+      for (uint32_t k = 0; k < n; ++k) write_raycast_miss(out + k);
+      return r;
+    }
+  }
+  return RPHYS_OK;
+}
 RPhysResult rphys_world_capsule_sweep(const RPhysWorld* Wc, const RPhysCapsuleSweepQuery* q, RPhysCapsuleSweepHit* out) {
   clear_err();
   if (out) {

@@ -897,6 +897,151 @@ bool World::raycast(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t
   return true;
 }
 
+// ---- exact ray casts: ray_shape (riftphys-geom/src/raycast.rs:13-130) against true shapes
+static bool ray_sphere_local(V3 o, V3 d, V3 c, float r, float* t_out, V3* n_out) {  // raycast.rs:42-53
+  const V3 m = sub(o, c);
+  const float b = dot(m, d);
+  const float cc = dot(m, m) - r * r;
+  if (cc <= 0.0f) { *t_out = 0.0f; *n_out = neg(d); return true; }
+  if (b > 0.0f) return false;
+  const float disc = b * b - cc;
+  if (disc < 0.0f) return false;
+  float t = -b - std::sqrt(disc);
+  t = rmax(t, 0.0f);
+  *t_out = t;
+  *n_out = normalize_or_zero(add(m, mul(d, t)));
+  return true;
+}
+static bool ray_box_local(V3 o, V3 d, V3 he, float* t_out, V3* n_out) {  // raycast.rs:55-82
+  float tmin = 0.0f, tmax = INFINITY;
+  V3 normal = neg(d);
+  const float oa[3] = {o.x, o.y, o.z}, da[3] = {d.x, d.y, d.z}, ha[3] = {he.x, he.y, he.z};
+  for (int ax = 0; ax < 3; ++ax) {
+    if (std::fabs(da[ax]) < 1.0e-9f) {
+      if (oa[ax] < -ha[ax] || oa[ax] > ha[ax]) return false;
+      continue;
+    }
+    const float inv = 1.0f / da[ax];
+    float t1 = (-ha[ax] - oa[ax]) * inv, t2 = (ha[ax] - oa[ax]) * inv;
+    float sign = -1.0f;
+    if (t1 > t2) { std::swap(t1, t2); sign = 1.0f; }
+    if (t1 > tmin) {
+      tmin = t1;
+      float n[3] = {0.0f, 0.0f, 0.0f};
+      n[ax] = sign;
+      normal = V3{n[0], n[1], n[2]};
+    }
+    tmax = rmin(tmax, t2);
+    if (tmin > tmax) return false;
+  }
+  *t_out = tmin;
+  *n_out = normal;
+  return true;
+}
+static bool ray_tube_local(V3 o, V3 d, float r, float hh, float* t_out, V3* n_out) {  // raycast.rs:84-96
+  const float a = d.x * d.x + d.z * d.z;
+  if (a < 1.0e-9f) return false;
+  const float b = o.x * d.x + o.z * d.z;
+  const float c = o.x * o.x + o.z * o.z - r * r;
+  const float disc = b * b - a * c;
+  if (disc < 0.0f) return false;
+  const float t = (-b - std::sqrt(disc)) / a;
+  if (t < 0.0f) return false;
+  const V3 p = add(o, mul(d, t));
+  if (std::fabs(p.y) > hh) return false;
+  *t_out = t;
+  *n_out = normalize_or_zero(V3{p.x, 0.0f, p.z});
+  return true;
+}
+static bool ray_capsule_local(V3 o, V3 d, float r, float hh, float* t_out, V3* n_out) {  // raycast.rs:98-109
+  const V3 core{0.0f, clampf(o.y, -hh, hh), 0.0f};
+  const V3 oc = sub(o, core);
+  if (dot(oc, oc) <= r * r) { *t_out = 0.0f; *n_out = neg(d); return true; }
+  bool have = ray_tube_local(o, d, r, hh, t_out, n_out);
+  const float cys[2] = {hh, -hh};
+  for (float cy : cys) {
+    float t;
+    V3 n;
+    if (ray_sphere_local(o, d, V3{0.0f, cy, 0.0f}, r, &t, &n) && (!have || t < *t_out)) {
+      have = true; *t_out = t; *n_out = n;
+    }
+  }
+  return have;
+}
+// ray_shape for the colliders' shapes and terrain triangles: (t, world normal facing the ray)
+static bool ray_shape(const Shape& s, const Iso& xf, V3 origin, V3 dir, float max_t, float* t_out, V3* n_out) {
+  if (!(max_t >= 0.0f) || !vfin(origin) || !vfin(dir)) return false;
+  const Q4 inv = qconj(xf.rot);
+  const V3 o = qrot(inv, sub(origin, xf.pos));
+  const V3 d = qrot(inv, dir);
+  float t;
+  V3 n;
+  bool hit;
+  if (s.kind == SH_SPHERE) hit = ray_sphere_local(o, d, V3{0, 0, 0}, std::fabs(s.a), &t, &n);
+  else if (s.kind == SH_BOX) hit = ray_box_local(o, d, V3{std::fabs(s.a), std::fabs(s.b), std::fabs(s.c)}, &t, &n);
+  else if (s.kind == SH_CAPSULE) hit = ray_capsule_local(o, d, std::fabs(s.a), std::fabs(s.b), &t, &n);
+  else {  // a triangle (triangle.rs:215-235 and :26-31)
+    hit = ray_triangle(o, d, max_t, s.ta, s.tb, s.tc, &t);
+    if (hit) {
+      const V3 tn = tri_normal(s.ta, s.tb, s.tc);
+      n = dot(tn, d) > 0.0f ? neg(tn) : tn;
+    }
+  }
+  if (!hit || !(t <= max_t && fin(t))) return false;
+  *t_out = t;
+  *n_out = qrot(xf.rot, n);
+  return true;
+}
+// World::raycast_exact (queries.rs:18-48), skipping one body index (0xFFFFFFFF: none): colliders
+// whose fresh AABB the ray meets, then the terrain triangles in the ray's box; a hit replaces the
+// best only when strictly nearer.
+bool World::raycast_exact(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t* body, float* toi, V3* point,
+                          V3* normal) const {
+  const float max_d = rmax(max_dist, 0.0f);
+  if (max_d <= 0.0f) return false;
+  const float l = std::sqrt(dot(dir, dir));
+  if (!fin(l) || l < 1.0e-12f) return false;
+  dir = divs(dir, l);
+  bool have = false;
+  float bt = 0.0f;
+  size_t bci = 0;
+  V3 bn{0, 0, 0};
+  const size_t kEnv = (size_t)-1;
+  for (size_t ci = 0; ci < colliders.size(); ++ci) {
+    const Collider& c = colliders[ci];
+    if (c.body == ignore) continue;
+    const Iso pose{pos[c.body], rot[c.body]};
+    float t0;
+    V3 p0, n0;
+    if (!ray_aabb(origin, dir, aabb_of(c.shape, pose), max_d, &t0, &p0, &n0)) continue;
+    float t;
+    V3 n;
+    if (ray_shape(c.shape, pose, origin, dir, max_d, &t, &n) && (!have || t < bt)) {
+      have = true; bt = t; bci = ci; bn = n;
+    }
+  }
+  if (has_hf) {
+    const V3 end = add(origin, mul(dir, max_d));
+    const Aabb q = aabb_new(vmin(origin, end), vmax(origin, end));
+    std::vector<Shape> tris;
+    hf_query(hf, q, tris);
+    const Iso id{V3{0, 0, 0}, Q4{0, 0, 0, 1}};
+    for (const Shape& tr : tris) {
+      float t;
+      V3 n;
+      if (ray_shape(tr, id, origin, dir, max_d, &t, &n) && (!have || t < bt)) {
+        have = true; bt = t; bci = kEnv; bn = n;
+      }
+    }
+  }
+  if (!have) return false;
+  *body = bci == kEnv ? 0xFFFFFFFFu : colliders[bci].body;
+  *toi = clampf(bt / max_d, 0.0f, 1.0f);
+  *point = add(origin, mul(dir, bt));
+  *normal = bn;
+  return true;
+}
+
 // ---- capsule sweeps: riftphys-query/src/lib.rs:1-134 (sphere sweeps against AABBs)
 static const float kToiEps = 1e-9f;
 static bool ray_aabb_slab_unit(V3 o, V3 d, const Aabb& b, float* t_out, V3* n_out) {  // lib.rs:42-79

@@ -199,6 +199,9 @@ struct World {
   // 0xFFFFFFFF. Returns false on a miss; body 0xFFFFFFFF is the terrain.
   bool raycast(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t* body, float* toi, V3* point,
                V3* normal) const;
+  // World::raycast_exact (queries.rs:18-48) with the skip set to one body index (0xFFFFFFFF: none)
+  bool raycast_exact(V3 origin, V3 dir, float max_dist, uint32_t ignore, uint32_t* body, float* toi, V3* point,
+                     V3* normal) const;
   // World::sweep_capsule (queries.rs:118-249): a y-axis capsule from -> to. Returns false on a
   // miss; body 0xFFFFFFFF is the terrain; *overlap when it started overlapping (toi 0).
   bool sweep_capsule(V3 from, V3 to, float radius, float half_height, uint32_t ignore, uint32_t* body, float* toi,

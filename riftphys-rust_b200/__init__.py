@@ -292,6 +292,7 @@ ABI = [
     ("rphys_player_set_input", c_uint32, [c_void_p, c_uint32, Vec3]),
     ("rphys_player_get_pose", c_uint32, [c_void_p, c_uint32, POINTER(Isometry), POINTER(c_uint32)]),
     ("rphys_ext_raycast_batch", c_uint32, [c_void_p, POINTER(RayQuery), c_uint32, POINTER(RayHit)]),
+    ("rphys_ext_raycast_exact_batch", c_uint32, [c_void_p, POINTER(RayQuery), c_uint32, POINTER(RayHit)]),
     ("rphys_ext_pack_snapshot", c_uint32, [c_void_p, c_uint64, c_uint64, c_void_p, c_uint64, POINTER(c_uint64),
                                            POINTER(c_uint32)]),
     ("rphys_ext_add_distance_joints", c_uint32, [c_void_p, POINTER(DistanceJointDesc), c_uint32, POINTER(c_uint32)]),
@@ -598,9 +599,10 @@ class World:
         self.c("rphys_player_get_pose", idx, byref(p), byref(g))
         return (p.pos.x, p.pos.y, p.pos.z), (p.rot.x, p.rot.y, p.rot.z, p.rot.w), bool(g.value)
 
-    def raycast_batch(self, origins, dirs, max_distance, ignore=None):
-        """rphys_ext_raycast_batch over arrays of origins and directions: the hits as a numpy
-        array of 10 float32 columns per ray (hit and body id as uint32 bits, fraction, point, normal)."""
+    def raycast_batch(self, origins, dirs, max_distance, ignore=None, exact=False):
+        """rphys_ext_raycast_batch (or, with exact, rphys_ext_raycast_exact_batch: true shapes) over
+        arrays of origins and directions: the hits as a numpy array of 9 float32 columns per ray (hit
+        and body id as uint32 bits, fraction, point, normal)."""
         import numpy as np
         n = len(origins)
         q = np.zeros((n, 8), dtype=np.float32)
@@ -612,7 +614,8 @@ class World:
         assert q.strides[0] == ctypes.sizeof(RayQuery)
         out = np.zeros((n, 9), dtype=np.float32)
         assert out.strides[0] == ctypes.sizeof(RayHit)
-        self.c("rphys_ext_raycast_batch", ctypes.cast(q.ctypes.data, POINTER(RayQuery)), n,
+        self.c("rphys_ext_raycast_exact_batch" if exact else "rphys_ext_raycast_batch",
+               ctypes.cast(q.ctypes.data, POINTER(RayQuery)), n,
                ctypes.cast(out.ctypes.data, POINTER(RayHit)))
         return out
 

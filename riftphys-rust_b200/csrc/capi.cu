@@ -506,12 +506,13 @@ RPhysResult rphys_world_raycast(const RPhysWorld* Wc, const RPhysRayQuery* q, RP
     return (RPhysResult)RPHYS_OK;
   });
 }
-RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q, uint32_t n, RPhysRayHit* out) {
+static RPhysResult raycast_many(const RPhysWorld* Wc, const RPhysRayQuery* q, uint32_t n, RPhysRayHit* out, const char* ctx,
+                                bool exact) {
   clear_err();
-  if (!Wc || ((!q || !out) && n)) return fail(RPHYS_ERR_NULL, "rphys_ext_raycast_batch: null arg");
+  if (!Wc || ((!q || !out) && n)) return fail(RPHYS_ERR_NULL, std::string(ctx) + ": null arg");
   for (uint32_t i = 0; i < n; ++i) write_raycast_miss(out + i);
   RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
-  return guard("rphys_ext_raycast_batch", [&]() {
+  return guard(ctx, [&]() {
     LOCK;
     std::vector<float> rays;
     std::vector<uint32_t> which;
@@ -519,17 +520,24 @@ RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q
     for (uint32_t i = 0; i < n; ++i) {
       float ray8[8];
       int cast = 0;
-      RPhysResult r = ray_prepare(W, q[i], "rphys_ext_raycast_batch", ray8, &cast);
+      RPhysResult r = ray_prepare(W, q[i], ctx, ray8, &cast);
       if (r) return r;
       if (cast) { rays.insert(rays.end(), ray8, ray8 + 8); which.push_back(i); }
     }
     const uint32_t m = (uint32_t)which.size();
     if (!m) return (RPhysResult)RPHYS_OK;
     std::vector<float4> pt(m), nn(m);
-    W->w->raycast_batch(m, rays.data(), pt.data(), nn.data());
+    W->w->raycast_batch(m, rays.data(), pt.data(), nn.data(), exact);
     for (uint32_t k = 0; k < m; ++k) ray_result(pt[k], nn[k], out + which[k]);
     return (RPhysResult)RPHYS_OK;
   });
+}
+RPhysResult rphys_ext_raycast_batch(const RPhysWorld* Wc, const RPhysRayQuery* q, uint32_t n, RPhysRayHit* out) {
+  return raycast_many(Wc, q, n, out, "rphys_ext_raycast_batch", false);
+}
+// World::raycast_exact (queries.rs:18-48) for n rays, checked and normalised as rphys_world_raycast
+RPhysResult rphys_ext_raycast_exact_batch(const RPhysWorld* Wc, const RPhysRayQuery* q, uint32_t n, RPhysRayHit* out) {
+  return raycast_many(Wc, q, n, out, "rphys_ext_raycast_exact_batch", true);
 }
 // lib.rs:482-492
 static void write_sweep_miss(RPhysCapsuleSweepHit* h) {

@@ -451,6 +451,195 @@ __global__ void __launch_bounds__(QT) k_sweep(uint32_t nq, const SweepIn* __rest
   }
 }
 
+
+// ---- exact ray casts: ray_shape (riftphys-geom/src/raycast.rs:13-130), in the shape's frame
+__device__ bool ray_sphere_local(f3 o, f3 d, f3 c, float r, float* t_out, f3* n_out) {  // raycast.rs:42-53
+  const f3 m = o - c;
+  const float b = dot(m, d);
+  const float cc = dot(m, m) - r * r;
+  if (cc <= 0.0f) { *t_out = 0.0f; *n_out = mk3(-d.x, -d.y, -d.z); return true; }
+  if (b > 0.0f) return false;
+  const float disc = b * b - cc;
+  if (disc < 0.0f) return false;
+  const float t = rmax(-b - sqrtf(disc), 0.0f);
+  *t_out = t;
+  *n_out = normalize_or_zero(m + d * t);
+  return true;
+}
+__device__ bool ray_box_local(f3 o, f3 d, f3 he, float* t_out, f3* n_out) {  // raycast.rs:55-82
+  float tmin = 0.0f, tmax = __int_as_float(0x7f800000);
+  f3 normal = mk3(-d.x, -d.y, -d.z);
+  const float oa[3] = {o.x, o.y, o.z}, da[3] = {d.x, d.y, d.z}, ha[3] = {he.x, he.y, he.z};
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    if (fabsf(da[ax]) < 1.0e-9f) {
+      if (oa[ax] < -ha[ax] || oa[ax] > ha[ax]) return false;
+      continue;
+    }
+    const float inv = 1.0f / da[ax];
+    float t1 = (-ha[ax] - oa[ax]) * inv, t2 = (ha[ax] - oa[ax]) * inv;
+    float sign = -1.0f;
+    if (t1 > t2) { const float sw = t1; t1 = t2; t2 = sw; sign = 1.0f; }
+    if (t1 > tmin) {
+      tmin = t1;
+      normal = mk3(ax == 0 ? sign : 0.0f, ax == 1 ? sign : 0.0f, ax == 2 ? sign : 0.0f);
+    }
+    tmax = rmin(tmax, t2);
+    if (tmin > tmax) return false;
+  }
+  *t_out = tmin;
+  *n_out = normal;
+  return true;
+}
+__device__ bool ray_tube_local(f3 o, f3 d, float r, float hh, float* t_out, f3* n_out) {  // raycast.rs:84-96
+  const float a = d.x * d.x + d.z * d.z;
+  if (a < 1.0e-9f) return false;
+  const float b = o.x * d.x + o.z * d.z;
+  const float c = o.x * o.x + o.z * o.z - r * r;
+  const float disc = b * b - a * c;
+  if (disc < 0.0f) return false;
+  const float t = (-b - sqrtf(disc)) / a;
+  if (t < 0.0f) return false;
+  const f3 p = o + d * t;
+  if (fabsf(p.y) > hh) return false;
+  *t_out = t;
+  *n_out = normalize_or_zero(mk3(p.x, 0.0f, p.z));
+  return true;
+}
+__device__ bool ray_capsule_local(f3 o, f3 d, float r, float hh, float* t_out, f3* n_out) {  // raycast.rs:98-109
+  const f3 oc = o - mk3(0.0f, clampf(o.y, -hh, hh), 0.0f);
+  if (dot(oc, oc) <= r * r) { *t_out = 0.0f; *n_out = mk3(-d.x, -d.y, -d.z); return true; }
+  bool have = ray_tube_local(o, d, r, hh, t_out, n_out);
+#pragma unroll
+  for (int e = 0; e < 2; ++e) {
+    float t;
+    f3 n;
+    if (ray_sphere_local(o, d, mk3(0.0f, e == 0 ? hh : -hh, 0.0f), r, &t, &n) && (!have || t < *t_out)) {
+      have = true; *t_out = t; *n_out = n;
+    }
+  }
+  return have;
+}
+// ray_shape: kind 0 sphere, 1 box, 2 capsule (dims as the colliders'), 3 the triangle tri
+__device__ bool ray_shape_dev(uint32_t kind, float4 dims, const Tri& tri, f3 xp, q4 xq, f3 origin, f3 dir, float max_t,
+                              float* t_out, f3* n_out) {
+  if (!(max_t >= 0.0f) || !vfin(origin) || !vfin(dir)) return false;
+  const q4 inv = qconj(xq);
+  const f3 o = qrot(inv, origin - xp), d = qrot(inv, dir);
+  float t = 0.0f;
+  f3 n = mk3(0, 0, 0);
+  bool hit;
+  if (kind == SH_SPHERE) hit = ray_sphere_local(o, d, mk3(0, 0, 0), fabsf(dims.x), &t, &n);
+  else if (kind == SH_BOX) hit = ray_box_local(o, d, mk3(fabsf(dims.x), fabsf(dims.y), fabsf(dims.z)), &t, &n);
+  else if (kind == SH_CAPSULE) hit = ray_capsule_local(o, d, fabsf(dims.x), fabsf(dims.y), &t, &n);
+  else {
+    hit = ray_triangle(o, d, max_t, tri.a, tri.b, tri.c, &t);
+    if (hit) {
+      const f3 tn = tri_normal(tri.a, tri.b, tri.c);
+      n = dot(tn, d) > 0.0f ? mk3(-tn.x, -tn.y, -tn.z) : tn;
+    }
+  }
+  if (!hit || !(t <= max_t && fin(t))) return false;
+  *t_out = t;
+  *n_out = qrot(xq, n);
+  return true;
+}
+
+// World::raycast_exact (queries.rs:18-48): colliders whose fresh AABB the ray meets, tested against
+// their true shape, then the heightfield's triangles in the ray's box; a hit replaces the best only
+// when strictly nearer, so the first of equals (lowest collider, colliders before terrain) stays.
+__global__ void __launch_bounds__(QT) k_raycast_exact(uint32_t nrays, const RayIn* __restrict__ rays, uint32_t ncol,
+                                                      const uint32_t* __restrict__ cbody, const uint32_t* __restrict__ ckind,
+                                                      const float4* __restrict__ cdims, const float4* __restrict__ pos,
+                                                      const float4* __restrict__ rot, const uint8_t* __restrict__ alive,
+                                                      bool has_hf, HfDev hf, float4* out_pt, float4* out_n) {
+  const uint32_t r = blockIdx.x;
+  if (r >= nrays) return;
+  const int tid = threadIdx.x;
+  const RayIn ray = rays[r];
+  __shared__ float s_t[QT];
+  __shared__ float4 s_n[QT];
+  __shared__ uint8_t s_hit[QT];
+  __shared__ float b_t;
+  __shared__ uint32_t b_code;
+  __shared__ f3 b_n;
+  __shared__ int have;
+  if (tid == 0) { have = 0; b_t = 0.0f; b_code = 0; }
+  __syncthreads();
+  const Tri none{};
+  for (uint32_t base = 0; base < ncol; base += QT) {
+    const uint32_t ci = base + tid;
+    bool hit = false;
+    if (ci < ncol) {
+      const uint32_t bd = cbody[ci];
+      if (alive[bd] && bd != ray.ignore) {
+        const f3 bp = xyz(pos[bd]);
+        const q4 bq = asq(rot[bd]);
+        f3 mn, mx, p0, n0;
+        float t0;
+        aabb_of(ckind[ci], cdims[ci], bp, bq, &mn, &mx);
+        if (ray_aabb(ray.o, ray.d, mn, mx, ray.max_d, &t0, &p0, &n0)) {
+          float t;
+          f3 n;
+          hit = ray_shape_dev(ckind[ci], cdims[ci], none, bp, bq, ray.o, ray.d, ray.max_d, &t, &n);
+          if (hit) { s_t[tid] = t; s_n[tid] = f4(n); }
+        }
+      }
+    }
+    s_hit[tid] = hit ? 1 : 0;
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 0; k < QT; ++k) {
+        if (!s_hit[k] || (have && !(s_t[k] < b_t))) continue;
+        have = 1; b_t = s_t[k]; b_code = cbody[base + k] + 1u; b_n = xyz(s_n[k]);
+      }
+    }
+    __syncthreads();
+  }
+  if (has_hf) {
+    const f3 end = ray.o + ray.d * ray.max_d;
+    f3 qa = vmin(ray.o, end), qb = vmax(ray.o, end);
+    qa = mk3(qf32(qa.x), qf32(qa.y), qf32(qa.z));
+    qb = mk3(qf32(qb.x), qf32(qb.y), qf32(qb.z));
+    long long gx0, gx1, gz0, gz1;
+    if (hf_window(hf, vmin(qa, qb), vmax(qa, qb), &gx0, &gx1, &gz0, &gz1)) {
+      const unsigned long long wx = (unsigned long long)(gx1 - gx0 + 1), ntri = 2ull * wx * (unsigned long long)(gz1 - gz0 + 1);
+      const q4 qid = mkq(0, 0, 0, 1);
+      for (unsigned long long base = 0; base < ntri; base += QT) {
+        const unsigned long long k = base + tid;
+        bool hit = false;
+        if (k < ntri) {
+          Tri tr;
+          hf_tri(hf, gx0, wx, gz0, k, &tr);
+          float t;
+          f3 n;
+          hit = ray_shape_dev(3u, make_float4(0, 0, 0, 0), tr, mk3(0, 0, 0), qid, ray.o, ray.d, ray.max_d, &t, &n);
+          if (hit) { s_t[tid] = t; s_n[tid] = f4(n); }
+        }
+        s_hit[tid] = hit ? 1 : 0;
+        __syncthreads();
+        if (tid == 0) {
+          for (int q = 0; q < QT; ++q) {
+            if (!s_hit[q] || (have && !(s_t[q] < b_t))) continue;
+            have = 1; b_t = s_t[q]; b_code = 0xFFFFFFFFu; b_n = xyz(s_n[q]);
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+  if (tid == 0) {
+    if (!have) {
+      out_pt[r] = make_float4(0, 0, 0, __uint_as_float(0u));
+      out_n[r] = make_float4(0, 1, 0, 1.0f);
+    } else {
+      const f3 p = ray.o + ray.d * b_t;
+      out_pt[r] = make_float4(p.x, p.y, p.z, __uint_as_float(b_code));
+      out_n[r] = make_float4(b_n.x, b_n.y, b_n.z, clampf(b_t / ray.max_d, 0.0f, 1.0f));
+    }
+  }
+}
+
 // World::sweep_capsule over a batch: per query from xyz, to xyz, radius, half height, ignored body
 // index bits (0xFFFFFFFF: none) and 3 words of padding; out as raycast_batch's, with the normal's
 // w = -0.0 when the capsule started overlapping (toi 0).
@@ -474,7 +663,7 @@ void WorldGpu::sweep_batch(uint32_t n, const float* q12, float4* hit_pt, float4*
 // World::raycast over a batch (queries.rs:50-116): n rays with origin, direction (unit) and max
 // distance; out per ray (x y z, body id + 1 bits or 0 for none or 0xFFFFFFFF for the terrain)
 // and (normal, fraction).
-void WorldGpu::raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, float4* hit_n) {
+void WorldGpu::raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, float4* hit_n, bool exact) {
   auto& S = *s_;
   cudaStream_t st = stream_;
   if (n == 0) return;
@@ -483,8 +672,12 @@ void WorldGpu::raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, flo
   S.ray_n.ensure(n + 1);
   RP_CUDA(cudaMemcpyAsync(S.ray_in.p, rays8, sizeof(RayIn) * n, cudaMemcpyHostToDevice, st));
   HfDev hf{hf_h_.p, hf_nx_, hf_nz_, hf_sx_, hf_sz_, hf_ox_, hf_oz_, hf_min_, hf_max_};
-  k_raycast<<<n, QT, 0, st>>>(n, reinterpret_cast<const RayIn*>(S.ray_in.p), ncol_, col_body.p, col_kind.p, col_dims.p,
-                               pos.p, rot.p, alive_d.p, has_hf_, hf, S.ray_pt.p, S.ray_n.p);
+  if (exact)
+    k_raycast_exact<<<n, QT, 0, st>>>(n, reinterpret_cast<const RayIn*>(S.ray_in.p), ncol_, col_body.p, col_kind.p,
+                                       col_dims.p, pos.p, rot.p, alive_d.p, has_hf_, hf, S.ray_pt.p, S.ray_n.p);
+  else
+    k_raycast<<<n, QT, 0, st>>>(n, reinterpret_cast<const RayIn*>(S.ray_in.p), ncol_, col_body.p, col_kind.p, col_dims.p,
+                                 pos.p, rot.p, alive_d.p, has_hf_, hf, S.ray_pt.p, S.ray_n.p);
   RP_COUNT_LAUNCH(1);
   RP_CUDA(cudaMemcpyAsync(hit_pt, S.ray_pt.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
   RP_CUDA(cudaMemcpyAsync(hit_n, S.ray_n.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));

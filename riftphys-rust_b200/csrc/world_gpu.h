@@ -176,7 +176,8 @@ class WorldGpu {
   // World::raycast for n rays (queries.rs:50-116): rays8 per ray origin xyz, unit direction xyz,
   // max distance, ignored body index bits (0xFFFFFFFF: none); per ray hit point xyz with w the hit
   // body's id + 1 (0: no hit, 0xFFFFFFFF: the terrain) as bits, and normal xyz with w the fraction.
-  void raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, float4* hit_n);
+  // exact: World::raycast_exact (queries.rs:18-48), the true shapes instead of their AABBs
+  void raycast_batch(uint32_t n, const float* rays8, float4* hit_pt, float4* hit_n, bool exact = false);
   // World::sweep_capsule for n queries (queries.rs:118-249): q12 per query from xyz, to xyz,
   // radius, half height, ignored body index bits, 3 words unused; out as raycast_batch's, the
   // normal's w -0.0 when the capsule started overlapping.

@@ -1,6 +1,8 @@
 """Ray casts (World::raycast, riftphys-world/src/world/queries.rs:50-116, through rphys_world_raycast)
 over any library exporting the C ABI: the reference's FFI ray tests (riftphys-ffi/src/tests.rs:178-280,
 488-530, 1201-1240, 1317-1345) restated, and the batched entry point agreeing with single calls."""
+import math
+
 import numpy as np
 
 from conftest import rp, scenes
@@ -69,6 +71,88 @@ def case_raycast_negative_max_distance_is_safe_and_misses(lib):
     _ground(w)
     hit, body, frac, _, _ = w.raycast((0.0, 5.0, 0.0), (0.0, -1.0, 0.0), -3.0)
     assert not hit and body == 0 and frac == 1.0
+    w.close()
+
+
+# ---- exact rays (World::raycast_exact, queries.rs:18-48, through rphys_ext_raycast_exact_batch)
+def _exact(w, o, d, max_d, ignore=None):
+    row = w.raycast_batch(np.float32([o]), np.float32([d]), max_d, ignore=ignore, exact=True)[0]
+    hit = bool(row[0:1].view(np.uint32)[0])
+    return hit, int(row[1:2].view(np.uint32)[0]), float(row[2]), tuple(map(float, row[3:6])), tuple(map(float, row[6:9]))
+
+
+def _qz(deg):
+    h = math.radians(deg) / 2.0
+    return (0.0, 0.0, math.sin(h), math.cos(h))
+
+
+def case_exact_tilted_plate_reads_its_slope_not_its_bounds(lib):
+    """raycast_exact_test.rs:15-30: a 10 mm plate tilted 30 degrees; the exact ray reads the top face
+    at y = x tan30 + 0.005 / cos30, the AABB ray the top of the bounds."""
+    w = lib.world(8, 8)
+    w.add_box((0.0, 0.0, 0.0), (0.1, 0.005, 0.1), dynamic=False, q=_qz(30.0))
+    for x in (-0.05, 0.0, 0.05):
+        hit, _, _, point, _ = _exact(w, (x, 0.5, 0.0), (0.0, -1.0, 0.0), 1.0)
+        want = x * math.tan(math.radians(30.0)) + 0.005 / math.cos(math.radians(30.0))
+        assert hit and abs(point[1] - want) < 1e-5, (x, point, want)
+        ahit, _, _, apoint, _ = w.raycast((x, 0.5, 0.0), (0.0, -1.0, 0.0), 1.0)
+        assert ahit and apoint[1] > want - 1e-6
+    w.close()
+
+
+def case_exact_ray_passes_through_a_gap_between_plates(lib):
+    """raycast_exact_test.rs:32-48: two plates with a 2 mm gap over a table; the ray through the gap
+    hits the table, one beside it the plate, and skipping the table sees through it."""
+    w = lib.world(8, 8)
+    w.add_box((-0.051, -0.005, 0.0), (0.05, 0.005, 0.1), dynamic=False)
+    w.add_box((0.051, -0.005, 0.0), (0.05, 0.005, 0.1), dynamic=False)
+    table = w.add_box((0.0, -0.02, 0.0), (0.2, 0.01, 0.2), dynamic=False)
+    hit, body, _, point, _ = _exact(w, (0.0, 0.2, 0.0), (0.0, -1.0, 0.0), 1.0)
+    assert hit and body == table and abs(point[1] + 0.01) < 1e-6, (body, point)
+    hit, _, _, point, _ = _exact(w, (0.0015, 0.2, 0.0), (0.0, -1.0, 0.0), 1.0)
+    assert hit and abs(point[1]) < 1e-6
+    hit, _, _, _, _ = _exact(w, (0.0, -0.015, 0.0), (0.0, -1.0, 0.0), 1.0, ignore=table)
+    assert not hit
+    w.close()
+
+
+def case_exact_capsule_and_sphere_hit_their_surface(lib):
+    """raycast_exact_test.rs:50-60 and raycast.rs:153-172: the sphere's surface, not its bounds; a
+    capsule's side, its cap from above, and a miss past the cap."""
+    w = lib.world(8, 8)
+    w.add_sphere((0.0, 0.0, 0.0), 0.1, dynamic=False)
+    hit, _, _, point, _ = _exact(w, (0.08, 1.0, 0.0), (0.0, -1.0, 0.0), 2.0)
+    assert hit and abs(point[1] - 0.06) < 1e-5, point
+    assert not _exact(w, (0.09, 1.0, 0.09), (0.0, -1.0, 0.0), 2.0)[0]
+    assert w.raycast((0.09, 1.0, 0.09), (0.0, -1.0, 0.0), 2.0)[0]
+    w.close()
+    w = lib.world(8, 8)
+    w.add_capsule((0.0, 0.0, 0.0), 0.2, 0.5, dynamic=False)
+    hit, _, frac, _, _ = _exact(w, (-1.0, 0.3, 0.0), (1.0, 0.0, 0.0), 10.0)
+    assert hit and abs(frac * 10.0 - 0.8) < 1e-5
+    hit, _, frac, _, normal = _exact(w, (0.0, 2.0, 0.0), (0.0, -1.0, 0.0), 10.0)
+    assert hit and abs(frac * 10.0 - 1.3) < 1e-5 and abs(normal[1] - 1.0) < 1e-5
+    assert not _exact(w, (-1.0, 0.71, 0.0), (1.0, 0.0, 0.0), 10.0)[0]
+    w.close()
+
+
+def case_exact_starting_inside_hits_at_zero(lib):
+    """raycast.rs:174-179: a ray from inside a box hits at t = 0 with normal -dir."""
+    w = lib.world(8, 8)
+    w.add_box((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), dynamic=False)
+    hit, _, frac, point, normal = _exact(w, (0.0, 0.0, 0.0), (1.0, 0.0, 0.0), 5.0)
+    assert hit and frac == 0.0 and point == (0.0, 0.0, 0.0) and normal == (-1.0, -0.0, -0.0), (frac, normal)
+    w.close()
+
+
+def case_exact_hits_terrain_with_normal_facing_the_ray(lib):
+    """queries.rs:33-41: terrain triangles through ray_shape; the normal faces the ray."""
+    w = lib.world(8, 8)
+    w.set_heightfield(np.zeros(4, dtype=np.float32), 2, 2, 10.0, 10.0, 0.0, 0.0)
+    hit, body, _, point, normal = _exact(w, (1.0, 5.0, 1.0), (0.0, -1.0, 0.0), 50.0)
+    assert hit and body == 0xFFFFFFFF and abs(point[1]) < 1e-6 and normal[1] > 0.99, (body, point, normal)
+    hit, body, _, _, normal = _exact(w, (1.0, -5.0, 1.0), (0.0, 1.0, 0.0), 50.0)
+    assert hit and body == 0xFFFFFFFF and normal[1] < -0.99, normal
     w.close()
 
 

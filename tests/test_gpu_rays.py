@@ -35,3 +35,15 @@ def test_capsule_sweeps_equal_the_oracle(oracle, gpu):
         assert a[:2] == b[:2] and a[3] == b[3] and np.array_equal(fa, fb), (i, a, b)
         hits += a[0]
     assert hits > 100
+
+
+def test_exact_rays_equal_the_oracle(oracle, gpu):
+    wo, wg = RC.stepped_terrain(oracle), RC.stepped_terrain(gpu)
+    o, d = RC.random_rays(2000, 13)
+    ro = wo.raycast_batch(o, d, 90.0, ignore=5, exact=True)
+    rg = wg.raycast_batch(o, d, 90.0, ignore=5, exact=True)
+    assert np.array_equal(ro.view(np.uint32), rg.view(np.uint32))
+    hits = ro[:, 0].view(np.uint32)
+    assert hits.sum() > 1000
+    # some rays end on bodies, not only on the terrain
+    assert (ro[:, 1].view(np.uint32)[hits == 1] != 0xFFFFFFFF).sum() > 50
