@@ -468,6 +468,24 @@ def main():
         wire_ms = (_time.perf_counter() - t0) * 1000.0 / reps
         wire = {"bodies": nb, "chunks": chunks, "bytes": len(data), "ms": wire_ms,
                 "gb_per_s": len(data) / (wire_ms * 1e-3) / 1e9, "note": "host-timed, device pack + copy to pageable memory"}
+        # batched scene queries on the same state (queries.rs:18-116): 16,384 seeded rays down onto
+        # the scene, AABB and exact, through the C ABI; host-timed, rays/s
+        qrng = np.random.default_rng(5)
+        nq = 16384
+        qo = np.column_stack([qrng.uniform(-190, 190, nq), qrng.uniform(20, 70, nq), qrng.uniform(-190, 190, nq)])
+        qd = np.column_stack([qrng.normal(size=nq) * 0.3, -np.ones(nq), qrng.normal(size=nq) * 0.3])
+        qo, qd = qo.astype(np.float32), qd.astype(np.float32)
+        rays = {}
+        for name, exact in (("aabb", False), ("exact", True)):
+            w.raycast_batch(qo, qd, 120.0, exact=exact)
+            t0 = _time.perf_counter()
+            for _ in range(3):
+                hits = w.raycast_batch(qo, qd, 120.0, exact=exact)
+            ms = (_time.perf_counter() - t0) * 1000.0 / 3
+            rays[name] = {"rays": nq, "ms": ms, "rays_per_s": nq / (ms * 1e-3),
+                          "hits": int(hits[:, 0].view(np.uint32).sum())}
+        wire["ray_batch"] = dict(rays, note="host-timed through rphys_ext_raycast_batch / _exact_batch, "
+                                             "one 256-thread block per ray over every collider")
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "body-ticks/s", "n_gpus": world_size, "steps": args.steps,
