@@ -306,6 +306,9 @@ RPhysResult rphys_ext_raycast_exact_batch(const RPhysWorld* world, const RPhysRa
  * stream of at most 12 MiB (56 + 12 bytes per body, 3 bytes per body of capacity, up to 48 bytes
  * per warm-start entry), at most 262144 warm-start entries and 65536 joints; a larger world returns
  * RPHYS_ERR_CAPACITY with the sizes in rphys_last_error_message and runs nothing on the device.
+ * Joints added or changed since the last step are not uploaded by this call (the next step does
+ * that): their warm-cache entries do not exist yet, so the digest is unchanged by them. The call
+ * runs on the device the world was created on, whatever device the calling thread has current.
  * The first call on each device looks up the array's address there (device setup): make it once
  * before the real-time loop. The array is shared by every world on a device, so calls are
  * serialised inside the library; each returns after its device work finished. */

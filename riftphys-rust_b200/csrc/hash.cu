@@ -413,10 +413,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 static std::mutex g_noalloc_mu;
 static unsigned char* g_noalloc_ptr[64];  // per device ordinal, set by the first call on that device
 
-// The device address of g_noalloc_scratch on the current device, looked up on the first call there.
-static unsigned char* noalloc_scratch() {
-  int dev = 0;
-  RP_CUDA(cudaGetDevice(&dev));
+// The device address of g_noalloc_scratch on device dev (the current device), looked up on the
+// first call there.
+static unsigned char* noalloc_scratch(int dev) {
   if (dev < 0 || dev >= 64) throw std::runtime_error("step_hash_noalloc: device ordinal above 63");
   if (!g_noalloc_ptr[dev]) {
     void* p = nullptr;
@@ -425,28 +424,32 @@ static unsigned char* noalloc_scratch() {
   }
   return g_noalloc_ptr[dev];
 }
+// Makes the world's device current for the call and puts the caller's back on return.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {
+    RP_CUDA(cudaGetDevice(&prev));
+    if (prev != dev) RP_CUDA(cudaSetDevice(dev));
+    else prev = -1;
+  }
+  ~DeviceScope() { if (prev >= 0) cudaSetDevice(prev); }
+};
 
 void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  unsigned char* base = noalloc_scratch();
-  cudaStream_t st = stream_;
   const int T = 256;
   uint32_t cap = cap_b_ > nb_ ? cap_b_ : nb_;
+  // Every limit is checked before any device work. Joints added or changed since the last tick
+  // are not uploaded here (that would allocate): the warm cache holds entries for the first
+  // jw_init_ joints only, and a joint without an entry adds no byte to the stream, so hashing
+  // those jw_init_ slots gives the digest step_hash gives after its upload.
+  if (num_joints() > NOALLOC_JOINT_MAX)
+    throw std::length_error("step_hash_noalloc: " + std::to_string(num_joints()) + " joints, at most " +
+                            std::to_string(NOALLOC_JOINT_MAX));
   if (n_warm > NOALLOC_WARM_MAX)
     throw std::length_error("step_hash_noalloc: " + std::to_string(n_warm) + " warm-start entries, at most " +
                             std::to_string(NOALLOC_WARM_MAX));
-  upload_joints();
-  const uint32_t nj = num_joints();
-  if (nj > NOALLOC_JOINT_MAX)
-    throw std::length_error("step_hash_noalloc: " + std::to_string(nj) + " joints, at most " +
-                            std::to_string(NOALLOC_JOINT_MAX));
-  uint32_t* woff = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WOFF);
-  uint32_t* wpos = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WPOS);
-  uint32_t* jsz = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JSZ);
-  uint32_t* joff = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JOFF);
-  uint32_t* jhas = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JHAS);
-  uint32_t* jpos = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JPOS);
-  void* temp = base + NOALLOC_OFF_TEMP;
+  const uint32_t nj = jw_n.p ? jw_init_ : 0u;
   // the stream length bound holds with every warm entry under its own key (the most bytes) and
   // every joint holding the most rows
   uint64_t worst = 48 + 56ull * nb_ + 8 + 48ull * n_warm + 24 + (8 + 5ull * kJointRows) * nj + 8 + 12ull * nb_ + 8 + cap + 8 +
@@ -455,11 +458,25 @@ void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
     throw std::length_error("step_hash_noalloc: state stream of up to " + std::to_string(worst) + " bytes (" +
                             std::to_string(nb_) + " bodies, capacity " + std::to_string(cap) + ", " +
                             std::to_string(n_warm) + " warm entries), at most " + std::to_string(NOALLOC_STREAM_MAX));
+  // the scans' temporary bytes (cub's size query launches nothing)
+  size_t wtemp = 0, jtemp = 0;
+  if (n_warm) RP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, wtemp, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n_warm, stream_));
+  if (nj) RP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, jtemp, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)nj, stream_));
+  if (wtemp > NOALLOC_TEMP_BYTES || jtemp > NOALLOC_TEMP_BYTES)
+    throw std::length_error("step_hash_noalloc: scan needs more temporary bytes than reserved");
+  DeviceScope on_device(dev_);
+  unsigned char* base = noalloc_scratch(dev_);
+  cudaStream_t st = stream_;
+  uint32_t* woff = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WOFF);
+  uint32_t* wpos = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_WPOS);
+  uint32_t* jsz = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JSZ);
+  uint32_t* joff = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JOFF);
+  uint32_t* jhas = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JHAS);
+  uint32_t* jpos = reinterpret_cast<uint32_t*>(base + NOALLOC_OFF_JPOS);
+  void* temp = base + NOALLOC_OFF_TEMP;
   uint32_t nkeys = 0;
   if (n_warm) {
-    size_t bytes = 0;
-    RP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, woff, wpos, (int)n_warm, st));
-    if (bytes > NOALLOC_TEMP_BYTES) throw std::length_error("step_hash_noalloc: scan needs more temporary bytes than reserved");
+    size_t bytes = wtemp;
     k_h_warm_flags<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, woff); RP_COUNT_LAUNCH(1);
     RP_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, woff, wpos, (int)n_warm, st));
     RP_COUNT_LAUNCH(2);
@@ -471,9 +488,7 @@ void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
   }
   uint64_t jbytes = 0, jcount = 0;
   if (nj) {
-    size_t bytes = 0;
-    RP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, jsz, joff, (int)nj, st));
-    if (bytes > NOALLOC_TEMP_BYTES) throw std::length_error("step_hash_noalloc: scan needs more temporary bytes than reserved");
+    size_t bytes = jtemp;
     k_hj_sizes<<<(nj + T - 1) / T, T, 0, st>>>(nj, jw_n.p, jsz, jhas); RP_COUNT_LAUNCH(1);
     RP_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, jsz, joff, (int)nj, st));
     RP_COUNT_LAUNCH(2);

@@ -161,6 +161,7 @@ __global__ void k_restore_bodies(uint32_t n, const float4* __restrict__ sp, cons
 
 // ------------------------------------------------------------------ WorldGpu
 WorldGpu::WorldGpu(uint32_t max_bodies, uint32_t max_colliders) : cap_b_(max_bodies), cap_c_(max_colliders) {
+  RP_CUDA(cudaGetDevice(&dev_));
   RP_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   // the side streams carry the long single-island solves: highest priority, so the block
   // scheduler places them before the many short packed groups queued on the main stream

@@ -205,6 +205,7 @@ class WorldGpu {
   static void snapshot_free(SnapshotGpu* s);
 
   cudaStream_t stream() const { return stream_; }
+  int device() const { return dev_; }  // the device the world was created on (its stream's)
   // learned warm start: a model (owned by the caller) predicting each row's start, and logging of
   // the rows' features and converged impulses (its training data)
   WarmModel* model_ = nullptr;
@@ -228,6 +229,7 @@ class WorldGpu {
 
   // capacities and counts
   uint32_t cap_b_, cap_c_, nb_ = 0, ncol_ = 0;
+  int dev_ = 0;
   cudaStream_t stream_ = nullptr;
   // host mirrors of static data
   std::vector<uint8_t> h_alive_;

@@ -68,3 +68,27 @@ def test_noalloc_hash_refuses_oversized_world(gpu):
     dt, _ = scenes.box_drop(rp, w, n_side=3)
     w.step(dt)
     _check_two_in_a_row(w)
+
+
+def test_noalloc_hash_with_new_joints_allocates_nothing(gpu):
+    """Joints added since the last step (D6 and distance joints) are hashed without being uploaded:
+    the call allocates nothing and still gives step_hash's digest, before and after stepping."""
+    w = gpu.world(1024, 1024)
+    dt, _, _ = scenes.ragdolls(rp, w, n_ragdolls=3)
+    for _ in range(20):
+        w.step(dt)
+    w.hash_noalloc()                        # device setup
+    a, b = w.add_box((0.0, 9.0, 0.0), (0.3, 0.3, 0.3)), w.add_box((0.0, 10.0, 0.0), (0.3, 0.3, 0.3))
+    j = w.add_joints([(0, a, b, ((0.0, 0.5, 0.0), (0.0, 0.0, 0.0, 1.0)), ((0.0, -0.5, 0.0), (0.0, 0.0, 0.0, 1.0)), 0)])
+    w.add_distance_joints([(a, b, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 1.0, 0.0, 0.0)])
+    w.set_joint_limit(j, True, 1, -0.5, 0.5)
+    before = _free_bytes()
+    h_new = w.hash_noalloc()                # joints dirty: nothing uploaded, nothing allocated
+    assert _free_bytes() == before
+    assert h_new == w.hash()                # step_hash uploads them and gives the same digest
+    for _ in range(5):
+        w.step(dt)
+        before = _free_bytes()
+        h = w.hash_noalloc()
+        assert _free_bytes() == before
+        assert h == w.hash()
