@@ -1,13 +1,14 @@
-"""Benchmark: body-ticks/s of the rigid-body tick at PGS residual <= 1e-4 on one B200.
+"""Benchmark: body-ticks/s of the rigid-body tick at PGS residual <= 1e-4 (or the sweep cap) on one B200.
 
 Workload (default ``--config terrain``): 100,000 bodies (40% spheres, 30% capsules, 30% boxes,
-density 1000) falling onto a 512x512 heightfield (1 m spacing), dt 1/60, 20 iterations; the
-velocity solve sweeps until its residual (largest |delta impulse| / effective mass over all rows,
-m/s) is <= 1e-4, at most 80 sweeps. Seeded synthetic scene (no dataset). A "step" is one tick of
-the whole world. The scene is first advanced ``--settle`` ticks (untimed) so the timed ticks sit
-in the contact-rich part of the 600-tick run; then W warm-up ticks, then exactly K timed ticks,
-bracketed by a barrier + device synchronize, timed with CUDA events recorded on the world's own
-stream. ``--config box_drop`` is the 1,000-box drop (8 iterations).
+density 1000) falling onto a 512x512 heightfield (1 m spacing), dt 1/60, 20 iterations; each solve
+island sweeps until its residual (largest |delta impulse| / effective mass over its rows in a
+sweep, m/s) is <= 1e-4, or 80 sweeps (4x the iteration count). Seeded synthetic scene (no
+dataset). A "step" is one tick of the whole world. The scene is first advanced ``--settle`` ticks
+(untimed) so the timed ticks sit in the contact-rich part of the 600-tick run; then W warm-up
+ticks, then exactly K timed ticks, bracketed by a barrier + device synchronize, timed with CUDA
+events recorded on the world's own stream. ``--config box_drop`` is the 1,000-box drop
+(8 iterations).
 
 value   whole-job body-ticks/s (bodies x K summed over ranks / max over ranks of the timed span).
 e2e     the same metric through the C ABI's rphys_world_step_ex with the tick's state read back to
@@ -16,12 +17,17 @@ e2e     the same metric through the C ABI's rphys_world_step_ex with the tick's 
 roofline  the stage with the most device time in a profiled replay of the same K ticks (CUDA events
         around each stage on the world's stream): its algorithmic bytes per launch / its mean
         duration, against the measured HBM copy bandwidth in MEASURED_PEAKS.json.
-cpu_baseline  the CPU restatement of the reference step (C++, OpenMP) on a bounded sample of the
-        same workload: a 50x50 m patch at the same body density and shape mix, settled, then timed.
+cpu_baseline  the CPU restatement of the reference step (C++, OpenMP, all host threads) on the
+        benchmark's own state: it loads the GPU world's state blob from the timed region's start
+        and steps --cpu-ticks ticks of the full workload.
+parity  those ticks' hashes and the final body states, GPU against the CPU restatement.
+solve   the last timed tick's velocity solve: sweeps, residual, islands still above the tolerance
+        at the cap and their rows, and a histogram of the islands' last-sweep residuals.
 
 Multi-GPU: a single world does not shard (its contacts couple every body), so N ranks run N
 independent replicas (one per GPU, scaling "weak"); no collective touches the data path.
-``--impl reference`` times the CPU reference restatement instead (rank 0 only).
+``--impl reference`` times the CPU restatement alone on the same workload: the full scene settled
+on the CPU, then the same warm-up and timed ticks (rank 0 only).
 """
 import argparse
 import ctypes
@@ -227,42 +233,93 @@ def oracle_path():
     return p
 
 
+def oracle_world(lib, args, threads):
+    """The CPU restatement's world of the benchmark scene (terrain or box drop), all threads."""
+    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies)
+    if args.mode == "residual":
+        w.set_residual_mode(TOL, 4 * ITERS[args.config])
+    lib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.dll.rphys_oracle_set_threads(w.h, threads)
+    return w, dt, nb, desc
+
+
 def run_reference(args):
-    """--impl reference: the CPU restatement of the reference step, all host threads."""
+    """--impl reference: the CPU restatement of the reference step (the reference itself is Rust and
+    cannot be built here) on the same workload as our arm: the full scene, settled on the CPU, then
+    W warm-up and K timed ticks, all host threads."""
     rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
+    if args.config not in ("terrain", "box_drop"):
+        print(json.dumps({"impl": "reference", "unavailable": f"--impl reference covers the terrain and box_drop "
+                                                             f"workloads, not {args.config}"}), flush=True)
+        return
+    args.mode = args.mode or "residual"
     lib = rp.Lib(oracle_path())
-    lib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
     threads = os.cpu_count() or 1
-    ticks = max(1, args.steps)
-    value, sample = cpu_sample_with(lib, ticks, threads)
-    print(json.dumps({"impl": "reference", "metric": METRIC, "value": value, "unit": "body-ticks/s",
-                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-                      "scaling": "weak", "dtype": "f32", "data": "synthetic",
-                      "config": {"workload": args.config, "sample": sample},
+    w, dt, nb, desc = oracle_world(lib, args, threads)
+    t0 = time.perf_counter()
+    w.step_n(dt, args.settle + args.warmup)
+    t_settle = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    w.step_n(dt, args.steps)
+    el = time.perf_counter() - t0
+    value = nb * args.steps / el
+    sample = (f"the whole workload: ticks {args.settle + args.warmup + 1}-{args.settle + args.warmup + args.steps} "
+              f"after {args.settle + args.warmup} settle and warm-up ticks on the CPU ({t_settle:.0f} s), "
+              f"{threads} threads, islands solved in parallel")
+    print(json.dumps({"impl": "reference", "metric": metric_name(args.config), "value": value, "unit": "body-ticks/s",
+                      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": el * 1000.0 / args.steps, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                      "config": run_config(args, desc, world_size),
                       "cpu_baseline": {"value": value, "unit": "body-ticks/s", "cores": threads, "kind": "port",
                                        "sample": sample},
                       "e2e": {"value": value, "unit": "body-ticks/s", "h2d_bytes_per_step": 0,
                               "d2h_bytes_per_step": 0}}), flush=True)
 
 
-def cpu_sample_with(lib, ticks, threads, settle=240):
-    n = int(round(100_000 * (50.0 / 400.0) ** 2))
-    w = lib.world(n + 16, n + 16)
-    dt, nb = scenes.terrain(rp, w, n_bodies=n, hf_n=64, area=50.0)
-    w.set_residual_mode(TOL, 80)
-    lib.dll.rphys_oracle_set_threads(w.h, threads)
-    w.step_n(dt, settle)
-    t0 = time.perf_counter()
-    w.step_n(dt, ticks)
-    el = time.perf_counter() - t0
-    return nb * ticks / el, (f"{nb}-body 50x50 m patch of the 100k-body terrain workload (same density and shape "
-                             f"mix, 64^2 heightfield), ticks {settle + 1}-{settle + ticks}, residual mode, "
-                             f"{threads} threads")
+def cpu_sample_from_state(olib, args, blob, gpu_world, dt, ticks, threads):
+    """The CPU baseline on the benchmark's own state: a CPU-restatement world of the same scene loads
+    the GPU world's state blob taken at the timed region's start and steps `ticks` ticks (timed);
+    the GPU world, restored to the same snapshot by the caller, steps the same ticks. Returns the
+    CPU throughput, the sample's description and whether every tick's hash and the final body
+    states agreed."""
+    import numpy as np
+    w, _, nb, _ = oracle_world(olib, args, threads)
+    w.state_import(blob)
+    same = w.hash() == gpu_world.hash()
+    hs = []
+    el = 0.0
+    for _ in range(ticks):
+        t0 = time.perf_counter()
+        w.step_n(dt, 1)
+        el += time.perf_counter() - t0
+        hs.append(w.hash())
+    for k in range(ticks):
+        gpu_world.step_n(dt, 1)
+        same = same and gpu_world.hash() == hs[k]
+    same = same and np.array_equal(w.body_states().view(np.uint32), gpu_world.body_states().view(np.uint32))
+    first = args.settle + args.warmup + 1
+    sample = (f"the benchmark's own {nb}-body state at its timed region's start (loaded from the GPU world's state "
+              f"blob), ticks {first}-{first + ticks - 1}, {threads} threads, islands solved in parallel")
+    w.close()
+    return nb * ticks / el, sample, same
 
 
-METRIC = "body-ticks/s at PGS residual <=1e-4"
+def metric_name(config):
+    """The headline metric: throughput with every solve island sweeping until its residual is
+    <= 1e-4 m/s or the sweep cap (4x the configuration's iteration count) stops it."""
+    return f"body-ticks/s at PGS residual <=1e-4 or {4 * ITERS[config]} sweeps per island"
+
+
+def run_config(args, desc, world_size):
+    """The workload's configuration, identical in both arms' lines (measured values live elsewhere)."""
+    return {"workload": desc, "settle_ticks": args.settle, "warmup_ticks": args.warmup, "mode": args.mode,
+            "tolerance": TOL if args.mode == "residual" else None,
+            "max_sweeps": 4 * ITERS[args.config] if args.mode == "residual" else ITERS[args.config],
+            "parallelism": f"replicas{world_size}", "l2": "inputs larger than L2 (126 MB)"}
 
 
 def main():
@@ -281,6 +338,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--bodies", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-ticks", type=int, default=3, help="ticks of the CPU sample (and of the parity check)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -326,6 +384,8 @@ def main():
     # the e2e and profiled passes replay exactly the timed ticks from this snapshot (the restore is
     # bit-exact, so all three passes see the same contacts, islands and sweeps)
     snap = w.snapshot()
+    # the same state as a host blob, for the CPU restatement's sample of the same ticks
+    blob = w.state_export() if args.config in ("terrain", "box_drop") and w.num_players() == 0 else None
     launches0 = lib.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
@@ -358,8 +418,11 @@ def main():
         w.step(dt)
         w.c("rphys_ext_get_body_states", 0, nb, host.ctypes.data_as(ctypes.c_void_p))
     e2e_s = time.perf_counter() - t0
-    e2e = {"value": nb * e2e_ticks / e2e_s, "unit": "body-ticks/s", "h2d_bytes_per_step": 0,
-           "d2h_bytes_per_step": 64 * nb}
+    e2e = {"value": nb * e2e_ticks / e2e_s, "unit": "body-ticks/s", "h2d_bytes_per_step": 20,
+           "d2h_bytes_per_step": 52 * nb,
+           "note": "each tick one rphys_world_step_ex call whose input is its 20-byte RPhysStepParams (the world "
+                   "state lives in the library between calls, as behind the reference's FFI), then "
+                   "rphys_ext_get_body_states reads every body's pos, rot, lin, ang (52 B) back to host memory"}
 
     # roofline: the stage with the most device time, in a separate profiled pass
     w.restore(snap)
@@ -394,13 +457,18 @@ def main():
         roof.update({"achieved": None, "frac": None, "ms_per_launch": stage_ms / max(1, stage_calls)})
     stages = {k: round(v[0] / max(1, v[1]), 4) for k, v in prof.items() if v[1]}
 
-    cpu = None
-    if rank == 0 and world_size == 1 and not args.no_cpu_baseline and args.config == "terrain":
+    cpu, parity = None, None
+    if rank == 0 and world_size == 1 and not args.no_cpu_baseline and blob is not None:
+        # the CPU restatement on the benchmark's own state: timed (cpu_baseline), and every tick's
+        # hash and the final body state compared with the GPU's replay of the same ticks (parity)
         olib = rp.Lib(oracle_path())
-        olib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
         threads = os.cpu_count() or 1
-        v, sample = cpu_sample_with(olib, 10, threads)
+        w.restore_exact(snap)
+        v, sample, same = cpu_sample_from_state(olib, args, blob, w, dt, args.cpu_ticks, threads)
         cpu = {"value": v, "unit": "body-ticks/s", "cores": threads, "kind": "port", "sample": sample}
+        parity = {"bit_exact": bool(same), "ticks": args.cpu_ticks,
+                  "checked": "tick hash every tick and all body states after the last, GPU vs CPU restatement "
+                             "from the same state"}
 
     learned = None
     if learned_on and learn_f:
@@ -488,20 +556,21 @@ def main():
                                              "one 256-thread block per ray over every collider")
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "body-ticks/s", "n_gpus": world_size, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": desc, "settle_ticks": args.settle, "mode": args.mode, "tolerance": TOL,
-                           "parallelism": f"replicas{world_size}", "l2": "inputs larger than L2" if nb > 50000 else
-                           "working set within L2", "sweeps_last_tick": st["sweeps"],
-                           "residual_last_tick": st["residual"], "rows_last_tick": st["rows_scheduled"],
-                           "contacts_last_tick": st["contacts"], "islands_last_tick": st["islands"],
-                           "levels_last_tick": st["levels"], "islands_capped_last_tick": st["islands_capped"],
-                           "row_sweeps_last_tick": st["row_sweeps"],
-                           "solve_groups_last_tick": {"shared_memory": st["groups_shared"],
-                                                      "global_memory": st["groups_global"],
-                                                      "max_rows": st["max_group_rows"],
-                                                      "max_bodies": st["max_group_bodies"]}},
+        rows, capped = st["rows_scheduled"], st["rows_capped"]
+        solve = {"sweeps": st["sweeps"], "residual": st["residual"], "rows": rows, "contacts": st["contacts"],
+                 "islands": st["islands"], "levels": st["levels"], "islands_capped": st["islands_capped"],
+                 "rows_in_capped_islands": capped,
+                 "rows_converged_frac": (rows - capped) / rows if rows else None,
+                 "island_residual_hist": dict(zip(["<=1e-4", "<=1e-3", "<=1e-2", "<=1e-1", "<=1", ">1"],
+                                                  st["res_hist"])),
+                 "row_sweeps": st["row_sweeps"],
+                 "solve_groups": {"shared_memory": st["groups_shared"], "global_memory": st["groups_global"],
+                                  "max_rows": st["max_group_rows"], "max_bodies": st["max_group_bodies"]},
+                 "note": "the last timed tick's velocity solve"}
+        line = {"metric": metric_name(args.config), "value": value, "unit": "body-ticks/s", "n_gpus": world_size,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": run_config(args, desc, world_size), "solve": solve, "parity": parity,
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "stage_ms": stages}
         if rollback is not None:

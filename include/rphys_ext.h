@@ -88,6 +88,10 @@ typedef struct RPhysStepStats {
     uint32_t groups_shared, groups_global, max_group_rows, max_group_bodies;
     uint32_t islands_capped; /* residual mode: solve islands still above the tolerance at the sweep cap */
     uint32_t pred_used;      /* rows whose warm start came from the learned prediction */
+    uint32_t rows_capped;    /* residual mode: rows of the islands counted in islands_capped */
+    /* solve islands by the residual of their last sweep (m/s): <= 1e-4, <= 1e-3, <= 1e-2, <= 1e-1,
+     * <= 1, above 1 */
+    uint32_t res_hist[6];
 } RPhysStepStats;
 RPhysResult rphys_ext_get_stats(const RPhysWorld* world, RPhysStepStats* out);
 
@@ -297,6 +301,26 @@ RPhysResult rphys_ext_raycast_batch(const RPhysWorld* world, const RPhysRayQuery
  * ray, and a ray starting inside a solid hits at fraction 0 with normal -dir. */
 RPhysResult rphys_ext_raycast_exact_batch(const RPhysWorld* world, const RPhysRayQuery* queries, uint32_t n,
                                           RPhysRayHit* out);
+
+/* The world's dynamic state as one flat little-endian byte blob (no counterpart in the
+ * reference, whose World clone, crates/riftphys-world/src/world/world.rs:912-961, stays inside one
+ * process). It holds every stored bit a tick reads that the world's set-up does not fix: the tick,
+ * epoch and rng state; per body its pose, velocities and last linear velocity; the sleep state at
+ * the world's capacity; the contact and joint warm-start caches. Importing it into a world built
+ * with the same bodies, joints and settings (in this library or in any library with this ABI, a CPU
+ * world included) makes that world's next ticks bit-identical to the exporter's. Layout: a 48-byte
+ * header ("RPS1", version 1, tick, epoch, rng as u64; bodies, capacity, warm entries, joints as u32),
+ * 64 bytes per body (pos xyz, rot xyzw, lin xyz, ang xyz, last linear velocity xyz as f32), one
+ * alive byte per body, one awake byte per capacity slot, then one u16 sleep counter per slot,
+ * 44 bytes per warm entry (key: body a, body b or 0xFFFFFFFF, ordinals a and b as u32; anchor xyz,
+ * normal impulse, friction impulse xyz as f32), 164 bytes per joint (cached row count u32 with
+ * 0xFFFFFFFF for none, 32 row tags u8, 32 impulses f32). With out NULL, *out_bytes receives the size;
+ * a buffer below it gives RPHYS_ERR_CAPACITY. Worlds with players have no blob (RPHYS_ERR_BAD_ARG). */
+RPhysResult rphys_ext_state_export(const RPhysWorld* world, uint8_t* out, uint64_t out_cap, uint64_t* out_bytes);
+/* Loads a blob of rphys_ext_state_export. RPHYS_ERR_BAD_ARG, with nothing changed, when its body
+ * count, capacity, joint count or live bodies differ from this world's, or its size does not match
+ * its counts. */
+RPhysResult rphys_ext_state_import(RPhysWorld* world, const uint8_t* in, uint64_t bytes);
 
 /* rphys_world_get_step_hash without any device allocation (no counterpart in the reference, whose
  * hash runs on the CPU). For hosts that hash every tick from a thread that must not allocate:

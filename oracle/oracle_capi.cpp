@@ -648,6 +648,132 @@ RPhysResult rphys_ext_snapshot_restore_exact(RPhysWorld* W, const RPhysWorldSnap
   w.restore_carried_state(s->s.carried);
   return RPHYS_OK;
 }
+// The state blob of rphys_ext_state_export (layout in rphys_ext.h): the same fields the device
+// library writes, from the World's own containers.
+static constexpr uint32_t kStateMagic = 0x31535052u;  // "RPS1"
+static uint64_t state_size(const World& w) {
+  uint64_t nb = w.num_bodies(), cap = w.awake.size() > nb ? w.awake.size() : nb, nw = 0;
+  for (const auto& kv : w.warm) nw += kv.second.size();
+  return 48 + 65 * nb + 3 * cap + 44 * nw + 164 * (uint64_t)w.joints.size();
+}
+RPhysResult rphys_ext_state_export(const RPhysWorld* Wc, uint8_t* out, uint64_t out_cap, uint64_t* out_bytes) {
+  clear_err();
+  if (!Wc || !out_bytes) return fail(RPHYS_ERR_NULL, "rphys_ext_state_export: null arg");
+  *out_bytes = 0;
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  std::lock_guard<std::mutex> g(W->mu);
+  const World& w = W->w;
+  if (!w.players.empty()) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_export: a world with players has no state blob");
+  const uint64_t n = state_size(w);
+  *out_bytes = n;
+  if (!out) return RPHYS_OK;
+  if (out_cap < n) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_state_export: buffer smaller than the state");
+  const uint32_t nb = w.num_bodies(), cap = (uint32_t)(w.awake.size() > nb ? w.awake.size() : nb);
+  uint32_t nw = 0;
+  for (const auto& kv : w.warm) nw += (uint32_t)kv.second.size();
+  uint8_t* p = out;
+  auto put = [&](const void* v, size_t b) { std::memcpy(p, v, b); p += b; };
+  const uint32_t hdr[2] = {kStateMagic, 1u};
+  put(hdr, 8); put(&w.tick, 8); put(&w.epoch, 8); put(&w.rng, 8);
+  const uint32_t cnt[4] = {nb, cap, nw, (uint32_t)w.joints.size()};
+  put(cnt, 16);
+  for (uint32_t i = 0; i < nb; ++i) {
+    const V3 ll = i < w.last_lin_vel.size() ? w.last_lin_vel[i] : V3{0, 0, 0};
+    const float v[16] = {w.pos[i].x, w.pos[i].y, w.pos[i].z, w.rot[i].x, w.rot[i].y, w.rot[i].z, w.rot[i].w, w.lin[i].x,
+                         w.lin[i].y, w.lin[i].z, w.ang[i].x, w.ang[i].y, w.ang[i].z, ll.x, ll.y, ll.z};
+    put(v, 64);
+  }
+  for (uint32_t i = 0; i < nb; ++i) put(&w.alive[i], 1);
+  for (uint32_t i = 0; i < cap; ++i) { uint8_t a = i < w.awake.size() ? w.awake[i] : 1; put(&a, 1); }
+  for (uint32_t i = 0; i < cap; ++i) { uint16_t t = i < w.sleep_ticks.size() ? w.sleep_ticks[i] : 0; put(&t, 2); }
+  for (const auto& kv : w.warm) {
+    const uint32_t key[4] = {std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), std::get<3>(kv.first)};
+    for (const WarmContact& c : kv.second) {
+      put(key, 16);
+      const float v[7] = {c.la.x, c.la.y, c.la.z, c.jn, c.jt.x, c.jt.y, c.jt.z};
+      put(v, 28);
+    }
+  }
+  for (uint32_t j = 0; j < (uint32_t)w.joints.size(); ++j) {
+    uint8_t rec[164];
+    std::memset(rec, 0, sizeof(rec));
+    uint32_t c = 0xFFFFFFFFu;
+    auto it = w.warm_joints.find(j);
+    if (it != w.warm_joints.end()) {
+      if (it->second.size() > 32) return fail(RPHYS_ERR_INTERNAL, "rphys_ext_state_export: joint with more than 32 cached rows");
+      c = (uint32_t)it->second.size();
+      for (uint32_t k = 0; k < c; ++k) {
+        rec[4 + k] = it->second[k].first;
+        std::memcpy(rec + 36 + 4 * k, &it->second[k].second, 4);
+      }
+    }
+    std::memcpy(rec, &c, 4);
+    put(rec, 164);
+  }
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_state_import(RPhysWorld* W, const uint8_t* in, uint64_t bytes) {
+  clear_err();
+  if (!W || !in) return fail(RPHYS_ERR_NULL, "rphys_ext_state_import: null arg");
+  std::lock_guard<std::mutex> g(W->mu);
+  World& w = W->w;
+  if (bytes < 48) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_import: state blob shorter than its header");
+  uint32_t hdr[2], cnt[4];
+  uint64_t tick, epoch, rng;
+  std::memcpy(hdr, in, 8);
+  if (hdr[0] != kStateMagic || hdr[1] != 1u) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_import: not a version 1 state blob");
+  std::memcpy(&tick, in + 8, 8); std::memcpy(&epoch, in + 16, 8); std::memcpy(&rng, in + 24, 8);
+  std::memcpy(cnt, in + 32, 16);
+  const uint32_t nb = w.num_bodies(), cap = (uint32_t)(w.awake.size() > nb ? w.awake.size() : nb);
+  const uint32_t nj = (uint32_t)w.joints.size(), nw = cnt[2];
+  if (cnt[0] != nb || cnt[1] != cap || cnt[3] != nj)
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_import: state blob of another world");
+  if (bytes != 48 + 65ull * nb + 3ull * cap + 44ull * nw + 164ull * nj)
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_import: state blob size does not match its counts");
+  if (!w.players.empty()) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_import: a world with players takes no state blob");
+  const uint8_t* p = in + 48 + 64ull * nb;
+  for (uint32_t i = 0; i < nb; ++i)
+    if (p[i] != w.alive[i]) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_import: state blob's live bodies differ from this world's");
+  p = in + 48;
+  if (w.last_lin_vel.size() < nb) w.last_lin_vel.resize(nb, V3{0, 0, 0});
+  for (uint32_t i = 0; i < nb; ++i, p += 64) {
+    float v[16];
+    std::memcpy(v, p, 64);
+    w.pos[i] = V3{v[0], v[1], v[2]}; w.rot[i] = Q4{v[3], v[4], v[5], v[6]};
+    w.lin[i] = V3{v[7], v[8], v[9]}; w.ang[i] = V3{v[10], v[11], v[12]};
+    w.last_lin_vel[i] = V3{v[13], v[14], v[15]};
+  }
+  p += nb;
+  w.awake.resize(cap); w.sleep_ticks.resize(cap);
+  for (uint32_t i = 0; i < cap; ++i) w.awake[i] = p[i];
+  p += cap;
+  for (uint32_t i = 0; i < cap; ++i) std::memcpy(&w.sleep_ticks[i], p + 2 * i, 2);
+  p += 2ull * cap;
+  w.warm.clear();
+  for (uint32_t e = 0; e < nw; ++e, p += 44) {
+    uint32_t key[4];
+    float v[7];
+    std::memcpy(key, p, 16);
+    std::memcpy(v, p + 16, 28);
+    w.warm[WarmKey{key[0], key[1], key[2], key[3]}].push_back(WarmContact{V3{v[0], v[1], v[2]}, v[3], V3{v[4], v[5], v[6]}});
+  }
+  w.warm_joints.clear();
+  for (uint32_t j = 0; j < nj; ++j, p += 164) {
+    uint32_t c;
+    std::memcpy(&c, p, 4);
+    if (c == 0xFFFFFFFFu) continue;
+    WarmJointRows rows;
+    for (uint32_t k = 0; k < c && k < 32; ++k) {
+      float l;
+      std::memcpy(&l, p + 36 + 4 * k, 4);
+      rows.emplace_back(p[4 + k], l);
+    }
+    w.warm_joints[j] = rows;
+  }
+  w.tick = tick; w.epoch = epoch; w.rng = rng;
+  w.update_colliders_aabb();
+  return RPHYS_OK;
+}
 void rphys_world_snapshot_free(RPhysWorldSnapshot* s) { delete s; }
 
 // ---------------------------------------------------------------- extensions
@@ -915,6 +1041,8 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
   o->row_sweeps = s.row_sweeps; o->rows_scheduled = s.rows_scheduled;
   o->islands_capped = s.islands_capped;
   o->pred_used = s.pred_used;
+  o->rows_capped = s.rows_capped;
+  for (int k = 0; k < 6; ++k) o->res_hist[k] = s.res_hist[k];
   uint32_t we = 0;
   for (auto& kv : W->w.warm) we += (uint32_t)kv.second.size();
   o->warm_entries = we;

@@ -29,6 +29,16 @@ static const float kWarmTol = 0.01f;       // WARM_MATCH_TOL (solver.rs:13)
 static const float kCell = 2.5f;           // GridBroadphase::new(2.5) (world.rs:419)
 
 static const Q4 kQId{0, 0, 0, 1};
+// Residual histogram bin of an island's last-sweep residual (m/s): <= 1e-4, 1e-3, 1e-2, 1e-1, 1,
+// above 1 or NaN (a statistic of this restatement's residual mode; the reference has none).
+static uint32_t res_bin(float r) {
+  if (r <= 1.0e-4f) return 0u;
+  if (r <= 1.0e-3f) return 1u;
+  if (r <= 1.0e-2f) return 2u;
+  if (r <= 1.0e-1f) return 3u;
+  if (r <= 1.0f) return 4u;
+  return 5u;
+}
 
 // ------------------------------------------------------------------ materials
 // props() core table (riftphys-materials/src/materials.rs:97-110), ordinals 0..13.
@@ -1986,7 +1996,7 @@ void World::step(float dt) {
         if (isl_of_root[r] == 0xFFFFFFFFu) isl_of_root[r] = n_sisl++;
         row_isl[e] = isl_of_root[r];
       }
-    std::vector<float> row_res(nent, 0.0f), isl_res(n_sisl), isl_last(n_sisl, 0.0f);
+    std::vector<float> row_res(nent, 0.0f), isl_last(n_sisl, 0.0f);
     std::vector<uint32_t> isl_sweeps(n_sisl, 0), isl_rows(n_sisl, 0);
     std::vector<uint8_t> isl_done(n_sisl, 0);
     for (auto& b : batches)
@@ -2030,37 +2040,41 @@ void World::step(float dt) {
     };
     const bool residual_mode = res_tol > 0.0f;
     const uint32_t max_sweeps = residual_mode ? (res_max > 0 ? res_max : iters_v) : iters_v;
-    uint32_t active = n_sisl;
-    for (uint32_t it = 0; it < max_sweeps && active > 0; ++it) {
-      for (auto& b : batches) {
-#ifdef _OPENMP
-        if (threads > 1 && b.size() >= 64) {
-#pragma omp parallel for num_threads(threads)
-          for (long q = 0; q < (long)b.size(); ++q) {
-            uint32_t e = b[q];
-            if (isl_done[row_isl[e]] || (e < njr && jrows[e].idx)) continue;
-            row_res[e] = 0.0f;
-            solve_ent(e, &row_res[e]);
-          }
-        } else
-#endif
-          for (uint32_t e : b) {
-            if (isl_done[row_isl[e]] || (e < njr && jrows[e].idx)) continue;
-            row_res[e] = 0.0f;
-            solve_ent(e, &row_res[e]);
-          }
-      }
-      std::fill(isl_res.begin(), isl_res.end(), 0.0f);
+    // Each solve island sweeps on its own: its rows in batch order (the serial order restricted to
+    // the island), until its residual stop or the cap. Islands move disjoint bodies, so solving
+    // them one after another, or on several threads at once, gives the bits of the batch-by-batch
+    // sweep over all islands.
+    std::vector<uint32_t> isl_first(n_sisl + 1, 0), isl_list(nent);
+    for (uint32_t i = 0; i < n_sisl; ++i) isl_first[i + 1] = isl_first[i] + isl_rows[i];
+    {
+      std::vector<uint32_t> fill(isl_first.begin(), isl_first.end() - 1);
       for (auto& b : batches)
-        for (uint32_t e : b)
-          if (!isl_done[row_isl[e]]) isl_res[row_isl[e]] = rmax(isl_res[row_isl[e]], row_res[e]);
-      for (uint32_t i = 0; i < n_sisl; ++i) {
-        if (isl_done[i]) continue;
-        isl_sweeps[i] = it + 1;
-        isl_last[i] = isl_res[i];
-        if (residual_mode && isl_res[i] <= res_tol) { isl_done[i] = 1; active--; }
-      }
+        for (uint32_t e : b) isl_list[fill[row_isl[e]]++] = e;
     }
+    auto solve_island = [&](uint32_t i) {
+      const uint32_t* L = isl_list.data() + isl_first[i];
+      const uint32_t n = isl_first[i + 1] - isl_first[i];
+      for (uint32_t it = 0; it < max_sweeps; ++it) {
+        for (uint32_t q = 0; q < n; ++q) {
+          uint32_t e = L[q];
+          if (e < njr && jrows[e].idx) continue;
+          row_res[e] = 0.0f;
+          solve_ent(e, &row_res[e]);
+        }
+        float r = 0.0f;
+        for (uint32_t q = 0; q < n; ++q) r = rmax(r, row_res[L[q]]);
+        isl_sweeps[i] = it + 1;
+        isl_last[i] = r;
+        if (residual_mode && r <= res_tol) { isl_done[i] = 1; break; }
+      }
+    };
+#ifdef _OPENMP
+    if (threads > 1) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+      for (long i = 0; i < (long)n_sisl; ++i) solve_island((uint32_t)i);
+    } else
+#endif
+      for (uint32_t i = 0; i < n_sisl; ++i) solve_island(i);
     stats.sweeps = 0;
     stats.residual = 0.0f;
     stats.rows_scheduled = 0;
@@ -2070,7 +2084,8 @@ void World::step(float dt) {
       stats.residual = rmax(stats.residual, isl_last[i]);
       stats.rows_scheduled += isl_rows[i];
       stats.row_sweeps += isl_rows[i] * isl_sweeps[i];
-      if (residual_mode && !isl_done[i]) stats.islands_capped++;
+      if (residual_mode && !isl_done[i]) { stats.islands_capped++; stats.rows_capped += isl_rows[i]; }
+      stats.res_hist[res_bin(isl_last[i])]++;
     }
     // joints solved this tick replace their rows; the rest keep theirs (:946-952); distance rows
     // are not kept

@@ -105,6 +105,8 @@ struct Stats {
   uint32_t sweeps = 0, bounce_rows = 0, row_sweeps = 0, rows_scheduled = 0;
   uint32_t islands_capped = 0;  // residual mode: solve islands still above the tolerance at the cap
   uint32_t pred_used = 0;       // rows started from an offered prediction
+  uint32_t rows_capped = 0;     // residual mode: rows of the islands counted in islands_capped
+  uint32_t res_hist[6] = {0, 0, 0, 0, 0, 0};  // solve islands by last-sweep residual (res_bin)
   float residual = 0;
 };
 

@@ -203,7 +203,8 @@ class StepStats(Structure):
                                         "sweeps", "bounce_rows", "warm_entries", "sleeping", "error_flags")] + \
                [("residual", c_float), ("row_sweeps", c_uint32), ("rows_scheduled", c_uint32)] + \
                [(n, c_uint32) for n in ("groups_shared", "groups_global", "max_group_rows", "max_group_bodies",
-                                        "islands_capped", "pred_used")]
+                                        "islands_capped", "pred_used", "rows_capped")] + \
+               [("res_hist", c_uint32 * 6)]
 
 
 class ContactRecord(Structure):
@@ -299,6 +300,8 @@ ABI = [
     ("rphys_ext_set_joint_axis", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_uint32, c_float]),
     ("rphys_ext_set_joint_drive", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, POINTER(JointDrive)]),
     ("rphys_ext_set_joint_damping", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_float, c_float]),
+    ("rphys_ext_state_export", c_uint32, [c_void_p, c_void_p, c_uint64, POINTER(c_uint64)]),
+    ("rphys_ext_state_import", c_uint32, [c_void_p, c_void_p, c_uint64]),
 ]
 
 
@@ -452,6 +455,19 @@ class World:
 
     def restore_exact(self, snap):
         self.c("rphys_ext_snapshot_restore_exact", c_void_p(snap))
+
+    def state_export(self):
+        """rphys_ext_state_export: the world's dynamic state as bytes (loads into a world of either
+        library built with the same bodies, joints and settings)."""
+        n = c_uint64(0)
+        self.c("rphys_ext_state_export", None, 0, byref(n))
+        buf = ctypes.create_string_buffer(max(1, n.value))
+        self.c("rphys_ext_state_export", buf, n.value, byref(n))
+        return buf.raw[: n.value]
+
+    def state_import(self, blob):
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        self.c("rphys_ext_state_import", buf, len(blob))
 
     def free_snapshot(self, snap):
         self.lib.dll.rphys_world_snapshot_free(c_void_p(snap))
@@ -696,7 +712,9 @@ class World:
     def stats(self):
         s = StepStats()
         self.c("rphys_ext_get_stats", byref(s))
-        return {f: getattr(s, f) for f, _ in StepStats._fields_}
+        out = {f: getattr(s, f) for f, _ in StepStats._fields_}
+        out["res_hist"] = list(out["res_hist"])
+        return out
 
     def pairs(self):
         import numpy as np

@@ -670,6 +670,35 @@ RPhysResult rphys_ext_snapshot_restore_exact(RPhysWorld* W, const RPhysWorldSnap
     return (RPhysResult)RPHYS_OK;
   });
 }
+RPhysResult rphys_ext_state_export(const RPhysWorld* Wc, uint8_t* out, uint64_t out_cap, uint64_t* out_bytes) {
+  clear_err();
+  if (!Wc || !out_bytes) return fail(RPHYS_ERR_NULL, "rphys_ext_state_export: null arg");
+  *out_bytes = 0;
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  return guard("rphys_ext_state_export", [&]() {
+    LOCK;
+    if (W->w->num_players()) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_state_export: a world with players has no state blob");
+    uint64_t n = W->w->state_bytes();
+    *out_bytes = n;
+    if (!out) return (RPhysResult)RPHYS_OK;
+    if (out_cap < n) return fail(RPHYS_ERR_CAPACITY, "rphys_ext_state_export: buffer smaller than the state");
+    W->w->state_export(out);
+    return (RPhysResult)RPHYS_OK;
+  });
+}
+RPhysResult rphys_ext_state_import(RPhysWorld* W, const uint8_t* in, uint64_t bytes) {
+  clear_err();
+  if (!W || !in) return fail(RPHYS_ERR_NULL, "rphys_ext_state_import: null arg");
+  return guard("rphys_ext_state_import", [&]() {
+    LOCK;
+    try {
+      W->w->state_import(in, bytes);
+    } catch (const std::invalid_argument& e) {
+      return fail(RPHYS_ERR_BAD_ARG, std::string("rphys_ext_state_import: ") + e.what());
+    }
+    return (RPhysResult)RPHYS_OK;
+  });
+}
 void rphys_world_snapshot_free(RPhysWorldSnapshot* s) {
   if (!s) return;
   try { WorldGpu::snapshot_free(s->s); } catch (...) {}
@@ -1011,6 +1040,8 @@ RPhysResult rphys_ext_get_stats(const RPhysWorld* Wc, RPhysStepStats* o) {
     o->max_group_rows = s.max_group_rows; o->max_group_bodies = s.max_group_bodies;
     o->islands_capped = s.islands_capped;
     o->pred_used = s.pred_used;
+    o->rows_capped = s.rows_capped;
+    for (int k = 0; k < 6; ++k) o->res_hist[k] = s.res_hist[k];
     return (RPhysResult)RPHYS_OK;
   });
 }

@@ -49,8 +49,20 @@ enum : int {
   STAT_MAX_GROUP_BODIES = 13,
   STAT_ISLANDS_CAPPED = 14,
   STAT_PRED_USED = 15,   // rows that started from the learned prediction
-  STAT_COUNT = 16
+  STAT_ROWS_CAPPED = 16, // residual mode: rows of the islands still above the tolerance at the cap
+  STAT_RES_HIST = 17,    // 6 slots: solve islands by their last sweep's residual (res_bin)
+  STAT_COUNT = 23
 };
+// The residual histogram's bin of an island's last-sweep residual r (m/s): <= 1e-4, 1e-3, 1e-2,
+// 1e-1, 1, and above 1 (or NaN). The CPU restatement bins with the same f32 comparisons.
+__host__ __device__ inline uint32_t res_bin(float r) {
+  if (r <= 1.0e-4f) return 0u;
+  if (r <= 1.0e-3f) return 1u;
+  if (r <= 1.0e-2f) return 2u;
+  if (r <= 1.0e-1f) return 3u;
+  if (r <= 1.0f) return 4u;
+  return 5u;
+}
 
 
 

@@ -550,10 +550,15 @@ __global__ void k_vel_solve(uint32_t nisl, uint32_t nc, Sched S, RowsV R, Bodies
     if (tol > 0.0f && resid <= tol) break;
   }
   if (lane == 0) {
-    atomicAdd(&stats[STAT_ROWSWEEPS], (S.lvl_start[off + nl] - S.lvl_start[off]) * (uint32_t)it);
+    const uint32_t nrows = S.lvl_start[off + nl] - S.lvl_start[off];
+    atomicAdd(&stats[STAT_ROWSWEEPS], nrows * (uint32_t)it);
     atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
     atomicMax(&stats[STAT_RESID], fbits(resid));
-    if (tol > 0.0f && !(resid <= tol)) atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
+    atomicAdd(&stats[STAT_RES_HIST + res_bin(resid)], 1u);
+    if (tol > 0.0f && !(resid <= tol)) {
+      atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
+      atomicAdd(&stats[STAT_ROWS_CAPPED], nrows);
+    }
   }
 }
 // Shock propagation (solver.rs:964-993): rows in (1e-6 height key, index) order, the lower body
@@ -1668,18 +1673,41 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
     G.lin[b] = W.lin[i];
     G.ang[b] = W.ang[i];
   }
-  uint32_t my_rs = 0;
+  uint32_t my_rs = 0, my_rcap = 0;
   for (uint32_t i = tid; i < nr; i += NT) {
     uint32_t r = S.ord[base + i];
     acc_jn[r] = W.jn[i];
     acc_jt[r] = W.jt[i];
-    my_rs += W.isl_sw[W.rows[i].flags >> 16];
+    const uint32_t li = W.rows[i].flags >> 16;
+    my_rs += W.isl_sw[li];
+    if (tol > 0.0f && !W.isl_done[li]) my_rcap++;
   }
   uint32_t my_sw = 0, my_res = 0, my_cap = 0;
+  uint32_t h0 = 0, h1 = 0, h2 = 0, h3 = 0, h4 = 0, h5 = 0;
   for (uint32_t i = tid; i < nisl; i += NT) {
     my_sw = max(my_sw, W.isl_sw[i]);
     my_res = max(my_res, W.isl_last[i]);
     if (tol > 0.0f && !W.isl_done[i]) my_cap++;
+    switch (res_bin(__uint_as_float(W.isl_last[i]))) {
+      case 0: h0++; break;
+      case 1: h1++; break;
+      case 2: h2++; break;
+      case 3: h3++; break;
+      case 4: h4++; break;
+      default: h5++; break;
+    }
+  }
+  {
+    const uint32_t hs[6] = {__reduce_add_sync(0xffffffffu, h0), __reduce_add_sync(0xffffffffu, h1),
+                            __reduce_add_sync(0xffffffffu, h2), __reduce_add_sync(0xffffffffu, h3),
+                            __reduce_add_sync(0xffffffffu, h4), __reduce_add_sync(0xffffffffu, h5)};
+    const uint32_t rc = __reduce_add_sync(0xffffffffu, my_rcap);
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k)
+        if (hs[k]) atomicAdd(&stats[STAT_RES_HIST + k], hs[k]);
+      if (rc) atomicAdd(&stats[STAT_ROWS_CAPPED], rc);
+    }
   }
   my_rs = __reduce_add_sync(0xffffffffu, my_rs);
   my_cap = __reduce_add_sync(0xffffffffu, my_cap);
@@ -1912,7 +1940,11 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
           atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
           atomicMax(&stats[STAT_RESID], rb);
           atomicAdd(&stats[STAT_ROWSWEEPS], (lvl[nl] - lvl[0]) * (uint32_t)it);
-          if (tol > 0.0f && !(__uint_as_float(rb) <= tol)) atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
+          atomicAdd(&stats[STAT_RES_HIST + res_bin(__uint_as_float(rb))], 1u);
+          if (tol > 0.0f && !(__uint_as_float(rb) <= tol)) {
+            atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
+            atomicAdd(&stats[STAT_ROWS_CAPPED], lvl[nl] - lvl[0]);
+          }
         }
       }
       __syncthreads();

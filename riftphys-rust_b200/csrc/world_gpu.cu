@@ -540,6 +540,8 @@ const StepStatsHost& WorldGpu::stats() {
     st_.max_group_bodies = h[STAT_MAX_GROUP_BODIES];
     st_.islands_capped = h[STAT_ISLANDS_CAPPED];
     st_.pred_used = h[STAT_PRED_USED];
+    st_.rows_capped = h[STAT_ROWS_CAPPED];
+    for (int k = 0; k < 6; ++k) st_.res_hist[k] = h[STAT_RES_HIST + k];
     stats_dirty_ = false;
   }
   st_.warm_entries = n_warm;
@@ -570,6 +572,136 @@ void WorldGpu::get_contacts(std::vector<ContactOut>& out) {
     c.n[0] = nn[k].x; c.n[1] = nn[k].y; c.n[2] = nn[k].z; c.impulse = nn[k].w;
     c.level = lv[k];
   }
+}
+
+// ------------------------------------------------------------------ state blob
+// Layout (little-endian): header of 48 bytes (magic "RPS1", version 1, tick, epoch, rng as u64,
+// bodies, capacity, warm entries, joints as u32); per body 16 f32 (pos xyz, rot xyzw, lin xyz,
+// ang xyz, last linear velocity xyz); per body its alive byte; per capacity slot the awake byte,
+// then the sleep counter as u16; per warm entry its key (4 x u32) and la xyz, jn, jt xyz (7 f32);
+// per joint its cached row count (u32, 0xFFFFFFFF: none), 32 row tags (u8) and 32 impulses (f32).
+static constexpr uint32_t kStateMagic = 0x31535052u;  // "RPS1"
+static constexpr uint64_t kStateHead = 48, kStateBody = 64, kStateWarm = 44, kStateJoint = 4 + 32 + 128;
+static_assert(kJointRows == 32, "state blob: 32 cached rows per joint");
+uint64_t WorldGpu::state_bytes() {
+  uint64_t cap = cap_b_ > nb_ ? cap_b_ : nb_;
+  return kStateHead + (kStateBody + 1) * nb_ + 3 * cap + kStateWarm * n_warm + kStateJoint * (uint64_t)num_joints();
+}
+void WorldGpu::state_export(uint8_t* out) {
+  upload_joints();
+  const uint32_t cap = cap_b_ > nb_ ? cap_b_ : nb_, nj = num_joints();
+  std::vector<float4> hp(nb_), hr(nb_), hl(nb_), ha(nb_), hll(nb_);
+  std::vector<uint8_t> aw(cap);
+  std::vector<uint16_t> tk(cap);
+  std::vector<uint4> wk(n_warm);
+  std::vector<float4> wa(n_warm), wb(n_warm);
+  std::vector<uint32_t> jn(nj);
+  std::vector<uint8_t> jt((size_t)kJointRows * nj);
+  std::vector<float> jl((size_t)kJointRows * nj);
+  auto get = [&](void* d, const void* s, size_t b) { if (b) RP_CUDA(cudaMemcpyAsync(d, s, b, cudaMemcpyDeviceToHost, stream_)); };
+  get(hp.data(), pos.p, 16ull * nb_); get(hr.data(), rot.p, 16ull * nb_); get(hl.data(), lin.p, 16ull * nb_);
+  get(ha.data(), ang.p, 16ull * nb_); get(hll.data(), last_lin.p, 16ull * nb_);
+  get(aw.data(), awake.p, cap); get(tk.data(), sleep_ticks.p, 2ull * cap);
+  get(wk.data(), warm_key.p, 16ull * n_warm); get(wa.data(), warm_a.p, 16ull * n_warm); get(wb.data(), warm_b.p, 16ull * n_warm);
+  if (nj) {
+    get(jn.data(), jw_n.p, 4ull * nj);
+    get(jt.data(), jw_tag.p, (size_t)kJointRows * nj);
+    get(jl.data(), jw_lam.p, 4ull * kJointRows * nj);
+  }
+  RP_CUDA(cudaStreamSynchronize(stream_));
+  uint8_t* p = out;
+  auto put = [&](const void* v, size_t b) { std::memcpy(p, v, b); p += b; };
+  const uint32_t hdr[2] = {kStateMagic, 1u};
+  put(hdr, 8); put(&tick_, 8); put(&epoch_, 8); put(&rng_, 8);
+  const uint32_t cnt[4] = {nb_, cap, n_warm, nj};
+  put(cnt, 16);
+  for (uint32_t i = 0; i < nb_; ++i) {
+    const float v[16] = {hp[i].x, hp[i].y, hp[i].z, hr[i].x, hr[i].y, hr[i].z, hr[i].w, hl[i].x,
+                         hl[i].y, hl[i].z, ha[i].x, ha[i].y, ha[i].z, hll[i].x, hll[i].y, hll[i].z};
+    put(v, 64);
+  }
+  put(h_alive_.data(), nb_);
+  put(aw.data(), cap);
+  put(tk.data(), 2ull * cap);
+  for (uint32_t e = 0; e < n_warm; ++e) {
+    put(&wk[e], 16);
+    const float v[7] = {wa[e].x, wa[e].y, wa[e].z, wa[e].w, wb[e].x, wb[e].y, wb[e].z};
+    put(v, 28);
+  }
+  for (uint32_t j = 0; j < nj; ++j) {
+    put(&jn[j], 4);
+    put(&jt[(size_t)kJointRows * j], kJointRows);
+    put(&jl[(size_t)kJointRows * j], 4 * kJointRows);
+  }
+}
+void WorldGpu::state_import(const uint8_t* in, uint64_t bytes) {
+  if (bytes < kStateHead) throw std::invalid_argument("state blob shorter than its header");
+  uint32_t hdr[2];
+  std::memcpy(hdr, in, 8);
+  if (hdr[0] != kStateMagic || hdr[1] != 1u) throw std::invalid_argument("not a version 1 state blob");
+  uint64_t tick, epoch, rng;
+  std::memcpy(&tick, in + 8, 8); std::memcpy(&epoch, in + 16, 8); std::memcpy(&rng, in + 24, 8);
+  uint32_t cnt[4];
+  std::memcpy(cnt, in + 32, 16);
+  const uint32_t cap = cap_b_ > nb_ ? cap_b_ : nb_;
+  upload_joints();
+  const uint32_t nj = num_joints(), nw = cnt[2];
+  if (cnt[0] != nb_ || cnt[1] != cap || cnt[3] != nj)
+    throw std::invalid_argument("state blob of another world: bodies " + std::to_string(cnt[0]) + ", capacity " +
+                                std::to_string(cnt[1]) + ", joints " + std::to_string(cnt[3]) + "; this world has " +
+                                std::to_string(nb_) + ", " + std::to_string(cap) + ", " + std::to_string(nj));
+  const uint64_t need = kStateHead + (kStateBody + 1) * (uint64_t)nb_ + 3ull * cap + kStateWarm * (uint64_t)nw +
+                        kStateJoint * (uint64_t)nj;
+  if (bytes != need) throw std::invalid_argument("state blob size does not match its counts");
+  if (!h_players_.empty()) throw std::invalid_argument("a world with players takes no state blob");
+  const uint8_t* p = in + kStateHead;
+  std::vector<float4> hp(nb_), hr(nb_), hl(nb_), ha(nb_), hll(nb_);
+  for (uint32_t i = 0; i < nb_; ++i, p += 64) {
+    float v[16];
+    std::memcpy(v, p, 64);
+    hp[i] = make_float4(v[0], v[1], v[2], 0.0f); hr[i] = make_float4(v[3], v[4], v[5], v[6]);
+    hl[i] = make_float4(v[7], v[8], v[9], 0.0f); ha[i] = make_float4(v[10], v[11], v[12], 0.0f);
+    hll[i] = make_float4(v[13], v[14], v[15], 0.0f);
+  }
+  if (std::memcmp(p, h_alive_.data(), nb_) != 0) throw std::invalid_argument("state blob's live bodies differ from this world's");
+  p += nb_;
+  const uint8_t* aw = p; p += cap;
+  const uint8_t* tk = p; p += 2ull * cap;
+  std::vector<uint4> wk(nw);
+  std::vector<float4> wa(nw), wb(nw);
+  for (uint32_t e = 0; e < nw; ++e, p += 44) {
+    std::memcpy(&wk[e], p, 16);
+    float v[7];
+    std::memcpy(v, p + 16, 28);
+    wa[e] = make_float4(v[0], v[1], v[2], v[3]);
+    wb[e] = make_float4(v[4], v[5], v[6], 0.0f);
+  }
+  std::vector<uint32_t> jn(nj);
+  std::vector<uint8_t> jt((size_t)kJointRows * nj);
+  std::vector<float> jl((size_t)kJointRows * nj);
+  for (uint32_t j = 0; j < nj; ++j) {
+    std::memcpy(&jn[j], p, 4);
+    std::memcpy(&jt[(size_t)kJointRows * j], p + 4, kJointRows);
+    std::memcpy(&jl[(size_t)kJointRows * j], p + 4 + kJointRows, 4 * kJointRows);
+    p += kStateJoint;
+  }
+  // the w lanes the device keeps (a body's pos.w / lin.w / ang.w) are untouched by the tick's
+  // arithmetic and zero in every world; the blob restores the rest
+  tick_ = tick; epoch_ = epoch; rng_ = rng;
+  warm_key.ensure(nw + 1); warm_a.ensure(nw + 1); warm_b.ensure(nw + 1);
+  auto put = [&](void* d, const void* s, size_t b) { if (b) RP_CUDA(cudaMemcpyAsync(d, s, b, cudaMemcpyHostToDevice, stream_)); };
+  put(pos.p, hp.data(), 16ull * nb_); put(rot.p, hr.data(), 16ull * nb_); put(lin.p, hl.data(), 16ull * nb_);
+  put(ang.p, ha.data(), 16ull * nb_); put(last_lin.p, hll.data(), 16ull * nb_);
+  put(awake.p, aw, cap); put(sleep_ticks.p, tk, 2ull * cap);
+  put(warm_key.p, wk.data(), 16ull * nw); put(warm_a.p, wa.data(), 16ull * nw); put(warm_b.p, wb.data(), 16ull * nw);
+  n_warm = nw;
+  if (nj) {
+    put(jw_n.p, jn.data(), 4ull * nj);
+    put(jw_tag.p, jt.data(), (size_t)kJointRows * nj);
+    put(jw_lam.p, jl.data(), 4ull * kJointRows * nj);
+  }
+  RP_CUDA(cudaStreamSynchronize(stream_));
+  stats_dirty_ = true;
 }
 
 // ------------------------------------------------------------------ rollback

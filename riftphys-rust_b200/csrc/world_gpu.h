@@ -33,6 +33,7 @@ struct StepStatsHost {
   uint32_t row_sweeps = 0, rows_scheduled = 0;
   uint32_t groups_shared = 0, groups_global = 0, max_group_rows = 0, max_group_bodies = 0;
   uint32_t islands_capped = 0, pred_used = 0;
+  uint32_t rows_capped = 0, res_hist[6] = {0, 0, 0, 0, 0, 0};
 };
 
 struct PairPropsHost { float mu_s, mu_k, restitution, stribeck_v, stiffness; };
@@ -197,6 +198,12 @@ class WorldGpu {
   bool players_dev_newer_ = false;
   DBuf<PlayerGpu> players_d;
   DBuf<uint32_t> player_of_d;                // per body: its controller's index, or 0xFFFFFFFF
+
+  // ---- the dynamic state as one host byte blob (layout in rphys_ext.h, rphys_ext_state_export)
+  uint64_t state_bytes();
+  void state_export(uint8_t* out);
+  // throws std::invalid_argument when the blob does not fit this world's bodies and joints
+  void state_import(const uint8_t* in, uint64_t bytes);
 
   // ---- rollback
   SnapshotGpu* snapshot_create();

@@ -42,7 +42,8 @@ def run_pair(oracle, gpu, build, ticks, check_every=1):
         assert wo.hash() == wg.hash(), f"tick {t}: tick hash differs"
         sto, stg = wo.stats(), wg.stats()
         for k in ("pairs", "contacts", "islands", "levels", "max_batch", "warm_matched", "warm_entries", "sleeping",
-                  "bounce_rows", "sweeps", "row_sweeps", "rows_scheduled", "islands_capped", "residual"):
+                  "bounce_rows", "sweeps", "row_sweeps", "rows_scheduled", "islands_capped", "residual", "rows_capped",
+                  "res_hist"):
             assert sto[k] == stg[k], f"tick {t}: stat {k} {sto[k]} vs {stg[k]}"
     return wo, wg
 
@@ -54,7 +55,7 @@ def test_box_drop_small(oracle, gpu):
 
 def test_box_drop_1000(oracle, gpu):
     build = {"cap": (1024, 1024), "fn": lambda rp_, w: scenes.box_drop(rp_, w, n_side=10)}
-    run_pair(oracle, gpu, build, 300, check_every=10)
+    run_pair(oracle, gpu, build, 300, check_every=1)
 
 
 def test_terrain_small(oracle, gpu):
