@@ -1125,6 +1125,26 @@ RPhysResult rphys_oracle_set_threads(RPhysWorld* W, int threads) {
   W->w.threads = threads < 1 ? 1 : threads;
   return RPHYS_OK;
 }
+// Oracle-only diagnostics: keep the worst solve island of each tick (rows and residual history).
+RPhysResult rphys_oracle_diag_worst(RPhysWorld* W, int on) {
+  if (!W) return RPHYS_ERR_NULL;
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.diag_worst = on != 0;
+  return RPHYS_OK;
+}
+// Copies the last tick's worst island: up to cap_rows rows of 5 floats (body a, body b as bits,
+// m_n, jn, the row's residual in the last sweep), up to cap_hist residuals.
+RPhysResult rphys_oracle_diag_read(RPhysWorld* W, float* rows, uint32_t cap_rows, float* hist, uint32_t cap_hist,
+                                   uint32_t* n_rows, uint32_t* n_hist) {
+  if (!W || !n_rows || !n_hist) return RPHYS_ERR_NULL;
+  std::lock_guard<std::mutex> g(W->mu);
+  const World& w = W->w;
+  *n_rows = (uint32_t)(w.diag_rows.size() / 5);
+  *n_hist = (uint32_t)w.diag_hist.size();
+  for (uint32_t k = 0; rows && k < 5 * std::min(cap_rows, *n_rows); ++k) rows[k] = w.diag_rows[k];
+  for (uint32_t k = 0; hist && k < std::min(cap_hist, *n_hist); ++k) hist[k] = w.diag_hist[k];
+  return RPHYS_OK;
+}
 // Oracle-only: BLAKE3 of a byte buffer (known-answer tests).
 void rphys_oracle_blake3(const uint8_t* data, size_t n, uint8_t out[32]);
 

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstring>
 #include <cstdio>
 #include <numeric>
 #include <unordered_map>
@@ -2051,6 +2052,7 @@ void World::step(float dt) {
       for (auto& b : batches)
         for (uint32_t e : b) isl_list[fill[row_isl[e]]++] = e;
     }
+    std::vector<std::vector<float>> isl_hist(diag_worst ? n_sisl : 0);
     auto solve_island = [&](uint32_t i) {
       const uint32_t* L = isl_list.data() + isl_first[i];
       const uint32_t n = isl_first[i + 1] - isl_first[i];
@@ -2065,6 +2067,7 @@ void World::step(float dt) {
         for (uint32_t q = 0; q < n; ++q) r = rmax(r, row_res[L[q]]);
         isl_sweeps[i] = it + 1;
         isl_last[i] = r;
+        if (diag_worst) isl_hist[i].push_back(r);
         if (residual_mode && r <= res_tol) { isl_done[i] = 1; break; }
       }
     };
@@ -2075,6 +2078,25 @@ void World::step(float dt) {
     } else
 #endif
       for (uint32_t i = 0; i < n_sisl; ++i) solve_island(i);
+    if (diag_worst) {
+      diag_rows.clear();
+      diag_hist.clear();
+      uint32_t worst = 0;
+      for (uint32_t i = 1; i < n_sisl; ++i)
+        if (isl_last[i] > isl_last[worst]) worst = i;
+      if (n_sisl) {
+        diag_hist = isl_hist[worst];
+        for (uint32_t q = isl_first[worst]; q < isl_first[worst + 1]; ++q) {
+          uint32_t e = isl_list[q];
+          uint32_t a = 0xFFFFFFFFu, bb = 0xFFFFFFFFu;
+          float mn = 0.0f, jn = 0.0f;
+          if (e >= njr) { const CC& cs = cons[e - njr]; a = cs.ai; bb = cs.terrain ? 0xFFFFFFFFu : cs.bi; mn = cs.m_n; jn = acc_jn[e - njr]; }
+          float fa, fb;
+          std::memcpy(&fa, &a, 4); std::memcpy(&fb, &bb, 4);
+          diag_rows.insert(diag_rows.end(), {fa, fb, mn, jn, row_res[e]});
+        }
+      }
+    }
     stats.sweeps = 0;
     stats.residual = 0.0f;
     stats.rows_scheduled = 0;

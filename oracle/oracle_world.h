@@ -148,6 +148,12 @@ struct World {
   std::vector<float> next_pred;
   uint32_t res_max = 0;
   int threads = 1;  // >1: narrowphase and level batches on OpenMP (order-preserving)
+  // Diagnostics of the residual stop (test infrastructure only): when on, the velocity solve keeps,
+  // for the island with the largest last-sweep residual, its rows (bodies, m_n, jn, residual)
+  // and its residual after every sweep.
+  bool diag_worst = false;
+  std::vector<float> diag_rows;   // 5 per row: body a, body b (as float bits), m_n, jn, last residual
+  std::vector<float> diag_hist;   // residual per sweep
 
   explicit World(uint32_t capacity);
   uint32_t num_bodies() const { return (uint32_t)pos.size(); }
