@@ -339,6 +339,7 @@ def main():
     ap.add_argument("--bodies", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-ticks", type=int, default=3, help="ticks of the CPU sample (and of the parity check)")
+    ap.add_argument("--coloured", type=int, default=1, help="also replay the timed ticks in coloured order (1/0)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -385,7 +386,7 @@ def main():
     # bit-exact, so all three passes see the same contacts, islands and sweeps)
     snap = w.snapshot()
     # the same state as a host blob, for the CPU restatement's sample of the same ticks
-    blob = w.state_export() if args.config in ("terrain", "box_drop") and w.num_players() == 0 else None
+    blob = w.state_export() if args.config in ("terrain", "box_drop") else None
     launches0 = lib.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
@@ -469,6 +470,41 @@ def main():
         parity = {"bit_exact": bool(same), "ticks": args.cpu_ticks,
                   "checked": "tick hash every tick and all body states after the last, GPU vs CPU restatement "
                              "from the same state"}
+
+    coloured = None
+    if args.config in ("terrain", "box_drop", "batch") and args.coloured:
+        # the same timed ticks replayed in coloured order (rphys_ext_set_solve_order): steps per sweep,
+        # device time, and the first tick's divergence from the serial order's (same state)
+        import numpy as np
+        w.restore_exact(snap)
+        w.step_n(dt, 1)
+        ser1 = w.body_states()
+        w.restore_exact(snap)
+        w.set_coloured(True)
+        w.step_n(dt, 1)
+        col1 = w.body_states()
+        w.restore_exact(snap)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        c0.record(stream)
+        w.step_n(dt, args.steps)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        cms = c0.elapsed_time(c1)
+        cs = w.stats()
+        w.set_coloured(False)
+
+        def rel(a, b):
+            return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+        coloured = {"value": nb * args.steps / (cms / 1000.0), "unit": "body-ticks/s", "ms_per_step": cms / args.steps,
+                    "levels_last_tick": cs["levels"], "levels_last_tick_serial": st["levels"],
+                    "sweeps_last_tick": cs["sweeps"], "row_sweeps_last_tick": cs["row_sweeps"],
+                    "islands_capped_last_tick": cs["islands_capped"],
+                    "first_tick_rel_divergence": {"pos": rel(col1[:, 0:3], ser1[:, 0:3]),
+                                                  "lin": rel(col1[:, 7:10], ser1[:, 7:10]),
+                                                  "ang": rel(col1[:, 10:13], ser1[:, 10:13])},
+                    "note": "same timed ticks replayed from the snapshot in coloured order; divergence: relative L2 "
+                            "difference of one tick from the same state, coloured vs serial"}
 
     learned = None
     if learned_on and learn_f:
@@ -577,6 +613,8 @@ def main():
             line["rollback"] = rollback
         if learned is not None:
             line["learned_warm_start"] = learned
+        if coloured is not None:
+            line["coloured_order"] = coloured
         if wire is not None:
             line["wire_snapshot"] = wire
         print(json.dumps(line), flush=True)

@@ -60,6 +60,19 @@ RPhysResult rphys_ext_set_heightfield_f32(RPhysWorld* world, uint32_t nx, uint32
  * m/s) is <= tolerance, at most max_sweeps sweeps. */
 RPhysResult rphys_ext_set_residual_mode(RPhysWorld* world, float tolerance, uint32_t max_sweeps);
 
+/* Order of the order-dependent contact passes (warm-start application, velocity sweeps, ballistic
+ * test, position projection). RPHYS_ORDER_SERIAL (default): the reference's serial order, through
+ * its level schedule (crates/riftphys-world/src/world/solver.rs:621-642), bit for bit.
+ * RPHYS_ORDER_COLOURED (an extension; the reference has no such order): each solve island is
+ * coloured by first fit in level order -- a row takes the smallest colour no already coloured row
+ * writing one of its bodies holds, at most 128 per body (an island needing more keeps its levels) --
+ * and the passes run colour by colour. Fewer, wider steps than the levels; the Gauss-Seidel updates
+ * are reordered, so results differ from the serial order's (they match the CPU restatement's
+ * coloured order bit for bit). Worlds with joints keep the serial order. */
+#define RPHYS_ORDER_SERIAL   0u
+#define RPHYS_ORDER_COLOURED 1u
+RPhysResult rphys_ext_set_solve_order(RPhysWorld* world, uint32_t order);
+
 /* Runs n ticks of dt (each one World::step) with a single completion wait at the end. */
 RPhysResult rphys_ext_step_n(RPhysWorld* world, float dt, uint32_t n);
 

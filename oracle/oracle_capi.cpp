@@ -846,6 +846,14 @@ RPhysResult rphys_ext_set_residual_mode(RPhysWorld* W, float tol, uint32_t max_s
   W->w.res_tol = tol; W->w.res_max = max_sweeps;
   return RPHYS_OK;
 }
+RPhysResult rphys_ext_set_solve_order(RPhysWorld* W, uint32_t order) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_solve_order: world is null");
+  if (order > RPHYS_ORDER_COLOURED) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_solve_order: unknown order");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->w.coloured = order == RPHYS_ORDER_COLOURED;
+  return RPHYS_OK;
+}
 RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_t n, uint32_t* out_first) {
   clear_err();
   if (out_first) *out_first = 0;

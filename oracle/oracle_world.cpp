@@ -1759,6 +1759,10 @@ void World::step(float dt) {
   std::vector<CC> cons;
   std::vector<std::vector<uint32_t>> batches;
   std::vector<uint32_t> level;
+  // the contacts in the order the order-dependent contact passes visit them (warm-start
+  // application, ballistic test, position projection): contact order, or in coloured mode the
+  // scheduled contacts colour by colour, then the rest
+  std::vector<uint32_t> pass_order, pass_rank;
   if (n_islands > 0) {
     // --- solve_islands_parallel (solver.rs:477-1271)
     const float beta = 0.05f, slop = 0.005f, margin = kMargin;
@@ -1868,9 +1872,89 @@ void World::step(float dt) {
         if (tb) bl[b] = t + 1;
       }
     }
+    // Coloured order (an extension; worlds without joints). Each solve island -- rows joined
+    // through the bodies they write -- is coloured by first fit in level order: walking the levels,
+    // a row takes the smallest colour that no already coloured row writing one of its bodies holds
+    // (128 colours per body at most). Rows of one colour then share no written body. An island
+    // with a row that finds no free colour keeps its levels, and so does an island of more than
+    // 32 rows whose colours are no fewer than its levels. Every pass that follows the level
+    // schedule in the serial order then visits the rows colour by colour (within a colour in
+    // (level, serial) order, which changes nothing: the rows of a colour are independent), so the
+    // Gauss-Seidel updates are reordered and the results are no longer the reference's bits.
+    if (coloured && njr == 0 && !batches.empty()) {
+      std::vector<uint32_t> root(count);
+      std::iota(root.begin(), root.end(), 0u);
+      auto find = [&](uint32_t x) {
+        while (root[x] != x) { root[x] = root[root[x]]; x = root[x]; }
+        return x;
+      };
+      for (auto& b : batches)
+        for (uint32_t e : b) {
+          uint32_t a, bb; bool ta, tb;
+          ent(e, &a, &bb, &ta, &tb);
+          if (ta && tb) {
+            uint32_t ra = find(a), rb = find(bb);
+            if (ra != rb) root[ra < rb ? rb : ra] = ra < rb ? ra : rb;
+          }
+        }
+      std::vector<uint64_t> mask(2 * (size_t)count, 0ull);
+      std::vector<uint32_t> colour(nent, 0xFFFFFFFFu);
+      std::vector<uint8_t> over(count, 0);
+      for (auto& b : batches)
+        for (uint32_t e : b) {
+          uint32_t a, bb; bool ta, tb;
+          ent(e, &a, &bb, &ta, &tb);
+          uint64_t m0 = 0, m1 = 0;
+          if (ta) { m0 |= mask[2 * a]; m1 |= mask[2 * a + 1]; }
+          if (tb) { m0 |= mask[2 * bb]; m1 |= mask[2 * bb + 1]; }
+          uint32_t c = 0xFFFFFFFFu;
+          if (~m0) c = (uint32_t)__builtin_ctzll(~m0);
+          else if (~m1) c = 64u + (uint32_t)__builtin_ctzll(~m1);
+          colour[e] = c;
+          if (c == 0xFFFFFFFFu) { over[find(ta ? a : bb)] = 1; continue; }
+          const uint64_t bit = 1ull << (c & 63u);
+          if (ta) mask[2 * a + (c >> 6)] |= bit;
+          if (tb) mask[2 * bb + (c >> 6)] |= bit;
+        }
+      // an island of more than 32 rows (the size the device solves as a group alone) that needs no
+      // fewer colours than levels keeps its levels too
+      std::vector<uint32_t> nrow(count, 0), ncol(count, 0), nlev(count, 0);
+      for (uint32_t L = 0; L < (uint32_t)batches.size(); ++L)
+        for (uint32_t e : batches[L]) {
+          uint32_t a, bb; bool ta, tb;
+          ent(e, &a, &bb, &ta, &tb);
+          uint32_t r = find(ta ? a : bb);
+          nrow[r]++;
+          nlev[r] = std::max(nlev[r], L + 1);
+          if (colour[e] != 0xFFFFFFFFu) ncol[r] = std::max(ncol[r], colour[e] + 1);
+        }
+      for (uint32_t r = 0; r < count; ++r)
+        if (nrow[r] > 32u && ncol[r] >= nlev[r]) over[r] = 1;
+      std::vector<std::vector<uint32_t>> cb;
+      for (uint32_t L = 0; L < (uint32_t)batches.size(); ++L)
+        for (uint32_t e : batches[L]) {
+          uint32_t a, bb; bool ta, tb;
+          ent(e, &a, &bb, &ta, &tb);
+          uint32_t key = over[find(ta ? a : bb)] ? L : colour[e];
+          if (key >= cb.size()) cb.resize(key + 1);
+          cb[key].push_back(e);
+          ent_level[e] = key;
+        }
+      batches.swap(cb);
+    }
     stats.levels = (uint32_t)batches.size();
     for (auto& b : batches) stats.max_batch = std::max<uint32_t>(stats.max_batch, (uint32_t)b.size());
     for (uint32_t k = 0; k < nc; ++k) levels_out[k] = ent_level[njr + k];
+    pass_order.clear();
+    pass_rank.assign(nc, 0xFFFFFFFFu);
+    if (coloured && njr == 0) {
+      for (auto& b : batches)
+        for (uint32_t e : b) { pass_rank[e] = (uint32_t)pass_order.size(); pass_order.push_back(e); }
+      for (uint32_t k = 0; k < nc; ++k)
+        if (pass_rank[k] == 0xFFFFFFFFu) { pass_rank[k] = (uint32_t)pass_order.size(); pass_order.push_back(k); }
+    } else {
+      for (uint32_t k = 0; k < nc; ++k) { pass_rank[k] = k; pass_order.push_back(k); }
+    }
     // warm start, joints (:699-712): serial in joint order, clamped to each row's bounds; distance
     // rows start cold (:704-705)
     for (uint32_t jk = 0; jk < (uint32_t)joints.size(); ++jk) {
@@ -1946,7 +2030,7 @@ void World::step(float dt) {
         if (!cs.terrain) { lin[cs.bi] = lb; ang[cs.bi] = ab; }
         return e;
       };
-      for (uint32_t k = 0; k < nc; ++k) {
+      for (uint32_t k : pass_order) {
         const CC& cs = cons[k];
         if (cs.soft) continue;
         const bool hp = preds && next_pred[4 * (size_t)k + 3] != 0.0f;
@@ -2189,7 +2273,8 @@ void World::step(float dt) {
   for (auto& jt : joints) { constrained[jt.a] = 1; constrained[jt.b] = 1; }
   std::vector<uint8_t> ballistic(count);
   for (uint32_t i = 0; i < count; ++i) ballistic[i] = !constrained[i] || (!jointed[i] && !contact_loaded[i]);
-  for (auto& c : contacts) {
+  for (uint32_t ci = 0; ci < nc; ++ci) {
+    const Contact& c = contacts[pass_order.size() == nc ? pass_order[ci] : ci];
     uint32_t a = colliders[c.a_collider].body;
     bool hb = c.b_collider != kTerrain;
     uint32_t b = hb ? colliders[c.b_collider].body : 0;
@@ -2290,6 +2375,8 @@ void World::step(float dt) {
   auto project = [&](bool shock) {
     std::vector<uint32_t> ord(pcs.size());
     std::iota(ord.begin(), ord.end(), 0u);
+    if (!shock && coloured && pass_rank.size() == nc)  // coloured order: the passes' rank of each contact
+      std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) { return pass_rank[pcs[x].src] < pass_rank[pcs[y].src]; });
     if (shock) {
       std::vector<int64_t> hk(pcs.size());
       for (size_t x = 0; x < pcs.size(); ++x)

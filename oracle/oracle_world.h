@@ -143,6 +143,9 @@ struct World {
   std::vector<uint32_t> last_levels;  // per last_frame_contacts entry
   Stats stats;
   float res_tol = 0.0f;
+  // Solve order (an extension): false, the reference's serial order (its level schedule); true,
+  // coloured order for worlds without joints (see the tick's colouring step).
+  bool coloured = false;
   // predictions offered to the next tick's warm start, 4 floats per contact in contact order
   // (normal, friction 1, friction 2 in kImpulseUnit x m_n; 1 when offered), consumed by step()
   std::vector<float> next_pred;

@@ -302,6 +302,7 @@ ABI = [
     ("rphys_ext_set_joint_damping", c_uint32, [c_void_p, c_uint32, c_uint32, c_uint32, c_float, c_float]),
     ("rphys_ext_state_export", c_uint32, [c_void_p, c_void_p, c_uint64, POINTER(c_uint64)]),
     ("rphys_ext_state_import", c_uint32, [c_void_p, c_void_p, c_uint64]),
+    ("rphys_ext_set_solve_order", c_uint32, [c_void_p, c_uint32]),
 ]
 
 
@@ -702,6 +703,10 @@ class World:
         assert h.size == nx * nz
         self.c("rphys_ext_set_heightfield_f32", nx, nz, c_float(cell_x), c_float(cell_z), c_float(origin_x),
                c_float(origin_z), h.ctypes.data_as(c_void_p), material)
+
+    def set_coloured(self, on=True):
+        """rphys_ext_set_solve_order: coloured order (on) or the reference's serial order."""
+        self.c("rphys_ext_set_solve_order", 1 if on else 0)
 
     def set_residual_mode(self, tol, max_sweeps):
         self.c("rphys_ext_set_residual_mode", c_float(tol), max_sweeps)

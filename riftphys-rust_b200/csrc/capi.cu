@@ -1013,6 +1013,14 @@ RPhysResult rphys_ext_set_residual_mode(RPhysWorld* W, float tol, uint32_t max_s
   W->w->set_residual_mode(tol, max_sweeps);
   return RPHYS_OK;
 }
+RPhysResult rphys_ext_set_solve_order(RPhysWorld* W, uint32_t order) {
+  clear_err();
+  if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_set_solve_order: world is null");
+  if (order > RPHYS_ORDER_COLOURED) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_solve_order: unknown order");
+  LOCK;
+  W->w->set_coloured(order == RPHYS_ORDER_COLOURED);
+  return RPHYS_OK;
+}
 RPhysResult rphys_ext_step_n(RPhysWorld* W, float dt, uint32_t n) {
   clear_err();
   if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_step_n: world is null");

@@ -446,6 +446,65 @@ __global__ void k_level_relax(uint32_t nisl, const uint32_t* __restrict__ isl_st
   for (int o = 16; o > 0; o >>= 1) { uint32_t t = __shfl_xor_sync(0xffffffffu, mx, o); if (t > mx) mx = t; }
   if (lane == 0) nlev[warp] = mx;
 }
+// Coloured order (worlds without joints): one warp per group walks its levels in order, and each
+// row of a level takes the smallest colour that no already coloured row writing one of its bodies
+// holds (first fit; 128 colours per body, bits in col_mask). The rows of one level share no written
+// body, so the warp colours them at once, and the result is the sequential first fit in level
+// order. A group where some row finds no free colour keeps its levels (flag over), and so does a
+// group of one island (g >= g_small: more than GROUP_ROWS rows) whose colours are no fewer than its
+// levels. Output: the (group, colour) key of every schedule position and the group's step count.
+__global__ void k_colour_levels(uint32_t ng, uint32_t g_small, const uint32_t* __restrict__ ord, const uint32_t* __restrict__ lvl_off,
+                                const uint32_t* __restrict__ lvl_start, const uint32_t* __restrict__ nlev,
+                                const uint2* __restrict__ ab, const uint32_t* __restrict__ flags, uint4* mask,
+                                unsigned long long* key_out, uint32_t* ncol) {
+  const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  if (g >= ng) return;
+  const uint32_t off = lvl_off[g], nl = nlev[g];
+  bool over = false;
+  uint32_t mx = 0;
+  for (uint32_t L = 0; L < nl; ++L) {
+    const uint32_t s1 = lvl_start[off + L + 1];
+    for (uint32_t s = lvl_start[off + L] + lane; s < s1; s += 32u) {
+      const uint32_t r = ord[s], f = flags[r];
+      const uint2 x = ab[r];
+      const bool ta = (f & RF_TA) != 0, tb = (f & RF_TB) != 0;
+      uint4 m = make_uint4(0u, 0u, 0u, 0u), ma = m, mb = m;
+      if (ta) ma = mask[x.x];
+      if (tb) mb = mask[x.y];
+      m = make_uint4(ma.x | mb.x, ma.y | mb.y, ma.z | mb.z, ma.w | mb.w);
+      uint32_t c = 0xFFFFFFFFu;
+      if (~m.x) c = __ffs(~m.x) - 1;
+      else if (~m.y) c = 32u + __ffs(~m.y) - 1;
+      else if (~m.z) c = 64u + __ffs(~m.z) - 1;
+      else if (~m.w) c = 96u + __ffs(~m.w) - 1;
+      if (c == 0xFFFFFFFFu) {
+        over = true;
+      } else {
+        const uint32_t bit = 1u << (c & 31u), w = c >> 5;
+        if (ta) { (&ma.x)[w] |= bit; mask[x.x] = ma; }
+        if (tb) { (&mb.x)[w] |= bit; mask[x.y] = mb; }
+        if (c + 1u > mx) mx = c + 1u;
+      }
+      key_out[s] = ((unsigned long long)g << 32) | c;
+    }
+    __syncwarp();  // this level's colours reach the masks before the next level reads them
+  }
+  over = __any_sync(0xffffffffu, over);
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (g >= g_small && mx >= nl) over = true;
+  if (over) {
+    for (uint32_t L = 0; L < nl; ++L)
+      for (uint32_t s = lvl_start[off + L] + lane; s < lvl_start[off + L + 1]; s += 32u)
+        key_out[s] = ((unsigned long long)g << 32) | L;
+  }
+  if (lane == 0) ncol[g] = over ? nl : mx;
+}
+__global__ void k_row_key_level(uint32_t n, const uint32_t* __restrict__ ord, const unsigned long long* __restrict__ keys,
+                                uint32_t* row_level) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) row_level[ord[s]] = (uint32_t)keys[s];
+}
 __global__ void k_plus1(uint32_t n, const uint32_t* __restrict__ a, uint32_t* b) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = a[i] + 1;
@@ -2081,6 +2140,32 @@ __global__ void k_joint_first_order(uint32_t n, uint32_t nc, uint32_t njr, const
   fl[i] = root[r] != 0xFFFFFFFFu ? 1 : 0;
 }
 // ------------------------------------------------------------------ host driver
+// Replaces a built level schedule (ord sorted by (group, level), level starts, level counts, the
+// level histogram and each row's level) by the coloured one (k_colour_levels): rows sorted by
+// (group, colour), stable, so a colour's rows keep their (level, serial) order.
+static void colour_schedule(WorldGpu::Scratch& S, uint32_t nsched, uint32_t ng, uint32_t g_small, uint32_t nb, const uint32_t* g_start,
+                            const uint32_t* g_cnt, DBuf<uint32_t>& ord, DBuf<uint32_t>& lvl_off, DBuf<uint32_t>& lvl_start,
+                            DBuf<uint32_t>& nlev, uint32_t* hist, uint32_t* row_level, cudaStream_t st) {
+  if (!nsched || !ng) return;
+  S.col_mask.ensure(nb + 1);
+  S.col_nlev.ensure(ng + 1);
+  S.col_ord.ensure(nsched + 1);
+  S.key64.ensure(nsched + 1); S.key64b.ensure(nsched + 1);
+  RP_CUDA(cudaMemsetAsync(S.col_mask.p, 0, sizeof(uint4) * (size_t)(nb + 1), st));
+  k_colour_levels<<<nblk(ng * 32, 128), 128, 0, st>>>(ng, g_small, ord.p, lvl_off.p, lvl_start.p, nlev.p, S.r_ab.p, S.r_flags.p,
+                                                      S.col_mask.p, S.key64.p, S.col_nlev.p); RP_COUNT_LAUNCH(1);
+  sort_pairs_u64(S, S.key64.p, S.key64b.p, ord.p, S.col_ord.p, nsched, 0, 64, st);
+  RP_CUDA(cudaMemcpyAsync(ord.p, S.col_ord.p, sizeof(uint32_t) * (size_t)nsched, cudaMemcpyDeviceToDevice, st));
+  RP_CUDA(cudaMemcpyAsync(nlev.p, S.col_nlev.p, sizeof(uint32_t) * (size_t)ng, cudaMemcpyDeviceToDevice, st));
+  S.lv_np1.ensure(ng + 1);
+  k_plus1<<<nblk(ng), T, 0, st>>>(ng, nlev.p, S.lv_np1.p); RP_COUNT_LAUNCH(1);
+  uint32_t total = exclusive_scan_total(S, S.lv_np1.p, lvl_off.p, ng, st);
+  lvl_start.ensure(total + 1);
+  if (hist) RP_CUDA(cudaMemsetAsync(hist, 0, sizeof(uint32_t) * (size_t)(nsched + 1), st));
+  k_level_starts<<<nblk(nsched), T, 0, st>>>(nsched, S.key64b.p, lvl_off.p, nlev.p, g_start, g_cnt, lvl_start.p, hist);
+  RP_COUNT_LAUNCH(1);
+  if (row_level) { k_row_key_level<<<nblk(nsched), T, 0, st>>>(nsched, ord.p, S.key64b.p, row_level); RP_COUNT_LAUNCH(1); }
+}
 // units: R.t1 of the rows when a joint's rows form one schedule unit (the velocity schedule), else null.
 static void build_schedule(WorldGpu::Scratch& S, uint32_t* W_err, uint32_t nsched, uint32_t nisl, const uint32_t* ord_in,
                            const uint32_t* isl_start, const uint32_t* isl_cnt, uint32_t* ord_out, DBuf<uint32_t>& lvl_off,
@@ -2276,6 +2361,11 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       RP_CUDA(cudaMemsetAsync(S.lvl_hist.p, 0, sizeof(uint32_t) * (nsched + 1), st));
       build_schedule(S, stats + STAT_ERR, nsched, ng, S.tmp32.p, S.g_start.p, S.g_cnt.p, S.ord_main.p, S.lvl_off, S.lvl_start,
                      S.nlev, S.lvl_hist.p, S.row_level.p, st, njr ? S.r_t1.p : nullptr);
+      // coloured order (worlds without joints): every pass on the main schedule -- warm start,
+      // sweeps, ballistic test, position projection -- then runs colour by colour
+      if (W.coloured_ && njr == 0)
+        colour_schedule(S, nsched, ng, g_small, nb, S.g_start.p, S.g_cnt.p, S.ord_main, S.lvl_off, S.lvl_start, S.nlev,
+                        S.lvl_hist.p, S.row_level.p, st);
       // ---- the bodies each group moves, with their index inside the group
       S.body_grp.ensure(nb + 1); S.gb_tmp.ensure(nb + 1); S.gb_key.ensure(nb + 1); S.gb_key2.ensure(nb + 1);
       S.gb_list.ensure(nb + 1); S.gb_start.ensure(ng + 1); S.gb_cnt.ensure(ng + 1); S.body_local.ensure(nb + 1);

@@ -90,6 +90,9 @@ class WorldGpu {
   void set_solver_iterations(uint32_t v, uint32_t p) { iters_v_ = v < 1 ? 1 : v; iters_p_ = p < 1 ? 1 : p; }
   void set_gravity(f3 g) { gravity_ = g; }
   void set_residual_mode(float tol, uint32_t max_sweeps) { res_tol_ = tol; res_max_ = max_sweeps; }
+  // Solve order: false, the reference's serial order (exact); true, coloured (worlds without joints)
+  void set_coloured(bool on) { coloured_ = on; }
+  bool coloured_ = false;
   void set_heightfield(uint32_t nx, uint32_t nz, float sx, float sz, float ox, float oz,
                        const std::vector<float>& q6_heights, float min_y, float max_y, uint32_t mat);
   void clear_heightfield();
