@@ -24,8 +24,10 @@ parity  those ticks' hashes and the final body states, GPU against the CPU resta
 solve   the last timed tick's velocity solve: sweeps, residual, islands still above the tolerance
         at the cap and their rows, and a histogram of the islands' last-sweep residuals.
 
-Multi-GPU: a single world does not shard (its contacts couple every body), so N ranks run N
-independent replicas (one per GPU, scaling "weak"); no collective touches the data path.
+Multi-GPU: a single world does not shard (its contacts couple every body), so for the terrain and
+box-drop workloads N ranks run N independent replicas (one per GPU, scaling "weak"). ``--config
+batch`` splits one world table across the ranks (contiguous world ranges, riftphys-rust_b200/shards.py)
+and gathers the per-world hashes once per rollback window; no collective touches the ticks.
 ``--impl reference`` times the CPU restatement alone on the same workload: the full scene settled
 on the CPU, then the same warm-up and timed ticks (rank 0 only).
 """
@@ -56,6 +58,7 @@ def _import_pkg():
 
 rp = _import_pkg()
 import riftphys_rust_b200.scenes as scenes  # noqa: E402
+import riftphys_rust_b200.shards as shards  # noqa: E402
 
 TOL = 1.0e-4
 # algorithmic bytes per unit of each stage (counted once per required HBM read or write)
@@ -69,18 +72,21 @@ BYTES = {
 ITERS = {"terrain": 20, "box_drop": 8, "batch": 16, "ragdolls": 24}
 
 
-def build_scene(lib, config, n_bodies=None, area=None, hf_n=None, worlds=4096, rank=0):
+def build_scene(lib, config, n_bodies=None, area=None, hf_n=None, worlds=4096, rank=0, world_size=1):
     if config == "batch":
-        # each rank steps its own set of worlds (the world table sharded across GPUs, no exchange)
-        descs = [scenes.batch_world_descs(rp, k, seed=3 + rank) for k in range(worlds)]
+        # one world table from one seed; this rank steps its contiguous range of it (no exchange
+        # during the ticks; the hashes are gathered at the rollback window's end)
+        lo, hi = shards.world_range(rank, world_size, worlds)
+        descs = [scenes.batch_world_descs(rp, k, seed=3) for k in range(lo, hi)]
         total = sum(len(d) for d in descs)
         w = lib.world(total + 16, total + 16)
         dt = scenes.batch_setup(w)
         for d in descs:
             w.add_world(d)
-        return w, dt, total, (f"batch: {worlds} independent worlds stepped together ({total:,} bodies), body counts "
-                              "log-uniform in [16, 4096], alternately square box pyramids and random box piles "
-                              "(half-extents U[0.25, 0.75] m, 1000 kg/m^3) on 50x0.5x50 ground boxes, dt 1/60, 16 iters")
+        return w, dt, total, (f"batch: {worlds} independent worlds stepped together (worlds {lo}-{hi - 1} on this "
+                              f"rank, {total:,} bodies), body counts log-uniform in [16, 4096], alternately square box "
+                              "pyramids and random box piles (half-extents U[0.25, 0.75] m, 1000 kg/m^3) on 50x0.5x50 "
+                              "ground boxes, dt 1/60, 16 iters")
     if config == "ragdolls":
         # worlds of 5 ragdolls each (15 capsules, 14 ball / hinge joints with limits), all on the same
         # 128^2 heightfield; the worlds' joints added in world order in one call
@@ -357,7 +363,8 @@ def main():
     if args.config == "model":
         return run_model(args, lib, torch)
     worlds = args.worlds or (2000 if args.config == "ragdolls" else 4096)
-    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, worlds=worlds, rank=rank)
+    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, worlds=worlds, rank=rank,
+                                  world_size=world_size)
     args.mode = args.mode or ("fixed" if args.config == "ragdolls" else "residual")
     if args.mode == "residual":
         w.set_residual_mode(TOL, 4 * ITERS[args.config])
@@ -545,9 +552,10 @@ def main():
     if args.config in ("batch", "ragdolls"):
         # the rollback workload: back to the snapshot, re-simulate 8 ticks twice from it (the first
         # pass and the replay), the replay timed on the device; every world's hash must match
+        # (ragdoll worlds stay per rank; batch worlds are one table: its hashes gathered over ranks)
         w.restore_exact(snap)
         w.step_n(dt, 8)
-        h_first = w.world_hashes()
+        local_first = w.world_hashes()
         w.restore_exact(snap)
         r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -555,8 +563,13 @@ def main():
         w.step_n(dt, 8)
         r1.record(stream)
         torch.cuda.synchronize()
-        h_again = w.world_hashes()
-        rollback = {"ticks": 8, "ms": r0.elapsed_time(r1), "worlds": w.num_worlds(),
+        local_again = w.world_hashes()
+        if args.config == "batch":
+            h_first = shards.gather_world_hashes(local_first, worlds, dist, "cuda")
+            h_again = shards.gather_world_hashes(local_again, worlds, dist, "cuda")
+        else:
+            h_first, h_again = local_first, local_again
+        rollback = {"ticks": 8, "ms": r0.elapsed_time(r1), "worlds": len(h_first),
                     "hashes_match": h_first == h_again}
 
     # the riftnet wire snapshot of the final state (riftphys-riftnet/src/wire.rs): packed on the
