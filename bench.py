@@ -59,6 +59,7 @@ def _import_pkg():
 rp = _import_pkg()
 import riftphys_rust_b200.scenes as scenes  # noqa: E402
 import riftphys_rust_b200.shards as shards  # noqa: E402
+import riftphys_rust_b200.autotune as autotune  # noqa: E402
 
 TOL = 1.0e-4
 # algorithmic bytes per unit of each stage (counted once per required HBM read or write)
@@ -346,6 +347,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-ticks", type=int, default=3, help="ticks of the CPU sample (and of the parity check)")
     ap.add_argument("--coloured", type=int, default=1, help="also replay the timed ticks in coloured order (1/0)")
+    ap.add_argument("--autotune", type=int, default=0, help="time every velocity-solve launch shape first (1/0)")
+    ap.add_argument("--tuning-out", default=autotune.TABLE, help="where --autotune records its table")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -374,12 +377,13 @@ def main():
     learned_on = args.learned and args.config == "terrain"
     if args.settle:
         if learned_on and args.settle > 60:
-            # the learned warm start's training rows: every 10th of the last 60 settle ticks
+            # the learned warm start's training rows: every row of every 3rd of the last 60 settle
+            # ticks (about 8M rows of this workload), with the impulses the plain solver converged to
             w.step_n(dt, args.settle - 60)
             w.set_feature_logging(True)
             for k in range(60):
                 w.step_n(dt, 1)
-                if k % 10 == 9:
+                if k % 3 == 2:
                     f, t = w.row_features()
                     learn_f.append(f); learn_t.append(t)
             w.set_feature_logging(False)
@@ -392,6 +396,16 @@ def main():
     # the e2e and profiled passes replay exactly the timed ticks from this snapshot (the restore is
     # bit-exact, so all three passes see the same contacts, islands and sweeps)
     snap = w.snapshot()
+    tuning_note = None
+    if args.autotune:
+        # time every launch shape on this state (same bits for all), record the table, keep the best
+        best, rows = autotune.tune(w, dt, snap, 5, torch, stream)
+        autotune.record(args.tuning_out, args.config, best, rows,
+                        f"{desc}; 5 ticks from the state after {args.settle + args.warmup} ticks, per shape")
+        tuning_note = "autotuned in this run"
+        print(f"[bench] autotune: best {best}; all same bits: {all(r['same_bits'] for r in rows)}", file=sys.stderr)
+    else:
+        tuning_note = "recorded table" if autotune.apply(w, args.config) else "compiled defaults"
     # the same state as a host blob, for the CPU restatement's sample of the same ticks
     blob = w.state_export() if args.config in ("terrain", "box_drop") else None
     launches0 = lib.launch_count()
@@ -515,38 +529,52 @@ def main():
 
     learned = None
     if learned_on and learn_f:
-        # train on the settle rows (new contacts, targets clipped to +-20 units), then replay the
-        # timed ticks with the model offering starts to the rows the previous tick has nothing for
+        # train on the settle rows (targets clipped to +-20 units: the rows of infeasible contact
+        # sets carry impulses thousands of units large), then replay the timed ticks with the model
+        # offering a start to every row (each row keeps the prediction only where it starts better
+        # than the previous tick's impulse) and, separately, only to rows the cache has nothing for
         import numpy as np
-        F, T = np.concatenate(learn_f), np.concatenate(learn_t)
-        cold = F[:, 22] == 0
-        F, T = F[cold], np.clip(T[cold], -20.0, 20.0)
+        F, T = np.concatenate(learn_f), np.clip(np.concatenate(learn_t), -20.0, 20.0)
+        del learn_f, learn_t
         model = lib.model(seed=2)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        loss = model.train(F, T, epochs=3, batch=2048, lr=1e-3)
+        epochs = 2
+        loss = model.train(F, T, epochs=epochs, batch=4096, lr=1e-3)
         t_train = time.perf_counter() - t0
-        w.restore_exact(snap)
         w.set_warm_model(model)
-        w.set_warm_policy(True)
-        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        l0.record(stream)
-        rs = pu = 0
-        for _ in range(args.steps):
-            w.step_n(dt, 1)
-            s_ = w.stats()
-            rs += s_["row_sweeps"]
-            pu += s_["pred_used"]
-        l1.record(stream)
-        torch.cuda.synchronize()
-        lms = l0.elapsed_time(l1)
+        runs = {}
+        for policy, cold in (("all_rows", False), ("cold_rows", True)):
+            w.set_warm_policy(cold)
+            w.restore_exact(snap)
+            l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            l0.record(stream)
+            w.step_n(dt, args.steps)
+            l1.record(stream)
+            torch.cuda.synchronize()
+            lms = l0.elapsed_time(l1)
+            # the same ticks again, stats read after each (row updates, starts taken) and staged
+            w.restore_exact(snap)
+            w.profile(True)
+            rs = pu = capped = 0
+            for _ in range(args.steps):
+                w.step_n(dt, 1)
+                s_ = w.stats()
+                rs += s_["row_sweeps"]; pu += s_["pred_used"]; capped += s_["rows_capped"]
+            lprof = w.profile_read()
+            w.profile(False)
+            runs[policy] = {"value": nb * args.steps / (lms / 1000.0), "ms_per_step": lms / args.steps,
+                            "row_updates": rs, "rows_in_capped_islands": capped,
+                            "rows_started_from_prediction": pu,
+                            "stage_ms": {k: round(v[0] / max(1, v[1]), 4) for k, v in lprof.items()
+                                         if k in ("warm_match", "vel_solve")}}
         w.set_warm_model(None)
-        learned = {"value": nb * args.steps / (lms / 1000.0), "unit": "body-ticks/s", "ms_per_step": lms / args.steps,
-                   "row_updates": rs, "row_updates_previous_tick_start": units["row_sweeps"],
-                   "rows_started_from_prediction": pu, "train_rows": int(len(F)), "train_epochs": 3,
-                   "train_seconds": t_train, "train_loss": loss,
-                   "note": "same timed ticks replayed from the snapshot; per-tick stats read between ticks"}
+        learned = dict(runs["all_rows"], unit="body-ticks/s", policies=runs,
+                       row_updates_previous_tick_start=units["row_sweeps"], train_rows=int(len(F)),
+                       train_epochs=epochs, train_seconds=t_train, train_loss=loss,
+                       note="same timed ticks replayed from the snapshot; value and ms from a replay with no host "
+                            "reads, row counts from a second replay with stats read after each tick")
 
     rollback = None
     if args.config in ("batch", "ragdolls"):
@@ -621,7 +649,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": run_config(args, desc, world_size), "solve": solve, "parity": parity,
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-                "gpu_launches": launches, "stage_ms": stages}
+                "gpu_launches": launches, "stage_ms": stages,
+                "tuning": dict(w.tuning(), source=tuning_note)}
         if rollback is not None:
             line["rollback"] = rollback
         if learned is not None:

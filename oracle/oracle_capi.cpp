@@ -25,6 +25,7 @@ struct RPhysWorld {
   std::mutex mu;
   World w;
   uint32_t bodies_created = 0, colliders_created = 0, max_bodies, max_colliders;
+  RPhysTuning tuning{32, 64, 128};
   RPhysWorld(uint32_t mb, uint32_t mc) : w(mb), max_bodies(mb), max_colliders(mc) {}
 };
 struct RPhysWorldSnapshot { Snapshot s; std::vector<World::Player> players; };  // lib.rs:1696-1702
@@ -852,6 +853,23 @@ RPhysResult rphys_ext_set_solve_order(RPhysWorld* W, uint32_t order) {
   if (order > RPHYS_ORDER_COLOURED) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_solve_order: unknown order");
   std::lock_guard<std::mutex> g(W->mu);
   W->w.coloured = order == RPHYS_ORDER_COLOURED;
+  return RPHYS_OK;
+}
+// Launch shapes mean nothing on the CPU: checked like the CUDA library's, stored and returned.
+RPhysResult rphys_ext_set_tuning(RPhysWorld* W, const RPhysTuning* t) {
+  clear_err();
+  if (!W || !t) return fail(RPHYS_ERR_NULL, "rphys_ext_set_tuning: null arg");
+  auto in = [](uint32_t v, uint32_t a, uint32_t b, uint32_t c) { return v == a || v == b || v == c; };
+  if (!(in(t->group_rows, 8, 16, 32) && in(t->packed_threads, 32, 64, 128) && in(t->island_threads, 64, 128, 256)))
+    return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_tuning: unsupported launch shape");
+  std::lock_guard<std::mutex> g(W->mu);
+  W->tuning = *t;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_tuning(const RPhysWorld* Wc, RPhysTuning* out) {
+  clear_err();
+  if (!Wc || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_get_tuning: null arg");
+  *out = Wc->tuning;
   return RPHYS_OK;
 }
 RPhysResult rphys_ext_add_joints(RPhysWorld* W, const RPhysJointDesc* d, uint32_t n, uint32_t* out_first) {

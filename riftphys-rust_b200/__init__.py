@@ -207,6 +207,10 @@ class StepStats(Structure):
                [("res_hist", c_uint32 * 6)]
 
 
+class Tuning(Structure):
+    _fields_ = [("group_rows", c_uint32), ("packed_threads", c_uint32), ("island_threads", c_uint32)]
+
+
 class ContactRecord(Structure):
     _fields_ = [("a_collider", c_uint32), ("b_collider", c_uint32), ("point", Vec3), ("normal", Vec3),
                 ("depth", c_float), ("impulse", c_float), ("level", c_uint32), ("pad", c_uint32)]
@@ -303,6 +307,8 @@ ABI = [
     ("rphys_ext_state_export", c_uint32, [c_void_p, c_void_p, c_uint64, POINTER(c_uint64)]),
     ("rphys_ext_state_import", c_uint32, [c_void_p, c_void_p, c_uint64]),
     ("rphys_ext_set_solve_order", c_uint32, [c_void_p, c_uint32]),
+    ("rphys_ext_set_tuning", c_uint32, [c_void_p, POINTER(Tuning)]),
+    ("rphys_ext_get_tuning", c_uint32, [c_void_p, POINTER(Tuning)]),
 ]
 
 
@@ -703,6 +709,15 @@ class World:
         assert h.size == nx * nz
         self.c("rphys_ext_set_heightfield_f32", nx, nz, c_float(cell_x), c_float(cell_z), c_float(origin_x),
                c_float(origin_z), h.ctypes.data_as(c_void_p), material)
+
+    def set_tuning(self, group_rows, packed_threads, island_threads):
+        """rphys_ext_set_tuning: the velocity solve's launch shapes (no result bit changes)."""
+        self.c("rphys_ext_set_tuning", byref(Tuning(group_rows, packed_threads, island_threads)))
+
+    def tuning(self):
+        t = Tuning()
+        self.c("rphys_ext_get_tuning", byref(t))
+        return {"group_rows": t.group_rows, "packed_threads": t.packed_threads, "island_threads": t.island_threads}
 
     def set_coloured(self, on=True):
         """rphys_ext_set_solve_order: coloured order (on) or the reference's serial order."""

@@ -1021,6 +1021,28 @@ RPhysResult rphys_ext_set_solve_order(RPhysWorld* W, uint32_t order) {
   W->w->set_coloured(order == RPHYS_ORDER_COLOURED);
   return RPHYS_OK;
 }
+static bool tuning_ok(const RPhysTuning& t) {
+  auto in = [](uint32_t v, uint32_t a, uint32_t b, uint32_t c) { return v == a || v == b || v == c; };
+  return in(t.group_rows, 8, 16, 32) && in(t.packed_threads, 32, 64, 128) && in(t.island_threads, 64, 128, 256);
+}
+RPhysResult rphys_ext_set_tuning(RPhysWorld* W, const RPhysTuning* t) {
+  clear_err();
+  if (!W || !t) return fail(RPHYS_ERR_NULL, "rphys_ext_set_tuning: null arg");
+  if (!tuning_ok(*t)) return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_tuning: unsupported launch shape");
+  LOCK;
+  W->w->tuning_.group_rows = t->group_rows;
+  W->w->tuning_.packed_threads = t->packed_threads;
+  W->w->tuning_.island_threads = t->island_threads;
+  return RPHYS_OK;
+}
+RPhysResult rphys_ext_get_tuning(const RPhysWorld* Wc, RPhysTuning* out) {
+  clear_err();
+  if (!Wc || !out) return fail(RPHYS_ERR_NULL, "rphys_ext_get_tuning: null arg");
+  RPhysWorld* W = const_cast<RPhysWorld*>(Wc);
+  LOCK;
+  *out = RPhysTuning{W->w->tuning_.group_rows, W->w->tuning_.packed_threads, W->w->tuning_.island_threads};
+  return RPHYS_OK;
+}
 RPhysResult rphys_ext_step_n(RPhysWorld* W, float dt, uint32_t n) {
   clear_err();
   if (!W) return fail(RPHYS_ERR_NULL, "rphys_ext_step_n: world is null");

@@ -451,8 +451,9 @@ __global__ void k_level_relax(uint32_t nisl, const uint32_t* __restrict__ isl_st
 // holds (first fit; 128 colours per body, bits in col_mask). The rows of one level share no written
 // body, so the warp colours them at once, and the result is the sequential first fit in level
 // order. A group where some row finds no free colour keeps its levels (flag over), and so does a
-// group of one island (g >= g_small: more than GROUP_ROWS rows) whose colours are no fewer than its
-// levels. Output: the (group, colour) key of every schedule position and the group's step count.
+// group of one island (g >= g_small) whose colours are no fewer than its
+// levels if it has more than 32 rows. Output: the (group, colour) key of every schedule position and
+// the group's step count.
 __global__ void k_colour_levels(uint32_t ng, uint32_t g_small, const uint32_t* __restrict__ ord, const uint32_t* __restrict__ lvl_off,
                                 const uint32_t* __restrict__ lvl_start, const uint32_t* __restrict__ nlev,
                                 const uint2* __restrict__ ab, const uint32_t* __restrict__ flags, uint4* mask,
@@ -492,7 +493,7 @@ __global__ void k_colour_levels(uint32_t ng, uint32_t g_small, const uint32_t* _
   }
   over = __any_sync(0xffffffffu, over);
   for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (g >= g_small && mx >= nl) over = true;
+  if (g >= g_small && lvl_start[off + nl] - lvl_start[off] > 32u && mx >= nl) over = true;
   if (over) {
     for (uint32_t L = 0; L < nl; ++L)
       for (uint32_t s = lvl_start[off + L] + lane; s < lvl_start[off + L + 1]; s += 32u)
@@ -1059,9 +1060,8 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
 // of it on chip; 0, a bigger island, by one CTA with its body velocities on chip and its rows
 // streamed through a cp.async double buffer; 2, an island beyond that, by one warp over global
 // memory.
-#ifndef GROUP_ROWS
-#define GROUP_ROWS 32u
-#endif
+// (the row count GROUP_ROWS is a tuning knob, WorldGpu::Tuning::group_rows: 8, 16 or 32)
+#define GROUP_ROWS_MAX 32u
 // big islands (classes 20..22): bodies and level starts held in shared memory, rows per staged
 // chunk (= threads per CTA) -- sized per bucket so that smaller ones share an SM
 #define BIG_BUCKETS 3
@@ -1069,8 +1069,8 @@ __constant__ uint32_t c_big_bodies[BIG_BUCKETS] = {1024u, 2048u, 4500u};
 __constant__ uint32_t c_big_levels[BIG_BUCKETS] = {2048u, 4096u, 4096u};
 static const uint32_t kBigBodies[BIG_BUCKETS] = {1024u, 2048u, 4500u};
 static const uint32_t kBigLevels[BIG_BUCKETS] = {2048u, 4096u, 4096u};
-#define WG_ROWS (2u * GROUP_ROWS)  // rows a packed group can hold
-#define WG_BODIES (2u * WG_ROWS)   // bodies those rows can move
+#define WG_ROWS(gr) (2u * (gr))    // rows a packed group of group_rows gr can hold
+#define WG_BODIES(gr) (4u * (gr))  // bodies those rows can move
 // single islands solved with everything on chip, by size bucket (class 10 + bucket): rows and
 // bodies held. An island moves at most rows + 1 bodies, so the smaller buckets hold that many;
 // the largest one (1152 rows, 768 bodies: 225.8 KB) is sized to the per-block limit.
@@ -1079,18 +1079,20 @@ __constant__ uint32_t c_island_rows[ISLAND_BUCKETS] = {128u, 256u, 384u, 512u, 7
 __constant__ uint32_t c_island_bodies[ISLAND_BUCKETS] = {129u, 257u, 385u, 513u, 769u, 768u};
 static const uint32_t kIslandRows[ISLAND_BUCKETS] = {128u, 256u, 384u, 512u, 768u, 1152u};
 static const uint32_t kIslandBodies[ISLAND_BUCKETS] = {129u, 257u, 385u, 513u, 769u, 768u};
-__global__ void k_group_flags(uint32_t nisl, const uint32_t* __restrict__ isl_cnt, uint32_t* small_rows, uint32_t* big) {
+__global__ void k_group_flags(uint32_t nisl, uint32_t group_rows, const uint32_t* __restrict__ isl_cnt, uint32_t* small_rows,
+                              uint32_t* big) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nisl) return;
-  bool small = isl_cnt[i] <= GROUP_ROWS;
+  bool small = isl_cnt[i] <= group_rows;
   small_rows[i] = small ? isl_cnt[i] : 0u;
   big[i] = small ? 0u : 1u;
 }
-__global__ void k_group_of_isl(uint32_t nisl, const uint32_t* __restrict__ isl_cnt, const uint32_t* __restrict__ small_pre,
-                               const uint32_t* __restrict__ big_pre, uint32_t g_small, uint32_t* g_of_isl) {
+__global__ void k_group_of_isl(uint32_t nisl, uint32_t group_rows, const uint32_t* __restrict__ isl_cnt,
+                               const uint32_t* __restrict__ small_pre, const uint32_t* __restrict__ big_pre, uint32_t g_small,
+                               uint32_t* g_of_isl) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nisl) return;
-  g_of_isl[i] = isl_cnt[i] <= GROUP_ROWS ? small_pre[i] / GROUP_ROWS : g_small + big_pre[i];
+  g_of_isl[i] = isl_cnt[i] <= group_rows ? small_pre[i] / group_rows : g_small + big_pre[i];
 }
 // group key of each position of the island-sorted row order (island id = run index)
 __global__ void k_group_keys(uint32_t n, const uint32_t* __restrict__ run_flag, const uint32_t* __restrict__ run_pre,
@@ -1608,10 +1610,8 @@ __host__ __device__ inline OnchipLayout onchip_layout(uint32_t RC, uint32_t BC, 
   L.bytes = o;
   return L;
 }
-#ifndef ONCHIP_T_PACKED
-#define ONCHIP_T_PACKED 64   // threads of a packed-group block (levels of up to 63 rows in one pass)
-#endif
-#define ONCHIP_T_ISLAND 128  // threads of a single-island block (wide first levels of terrain piles)
+// threads of a packed-group block (32, 64 or 128) and of a single-island block (64, 128 or 256) are
+// tuning knobs (WorldGpu::Tuning); each value has its own instantiation below
 template <bool MULTI, int NT>
 __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32_t g0, uint32_t ng,
                                                          const uint32_t* __restrict__ glist, uint32_t want_class,
@@ -2330,12 +2330,14 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       // ---- solve groups: small islands packed by the prefix sum of their rows, big ones alone
       S.g_small_rows.ensure(nisl + 1); S.g_small_pre.ensure(nisl + 1); S.g_big.ensure(nisl + 1);
       S.g_big_pre.ensure(nisl + 1); S.g_of_isl.ensure(nisl + 1);
-      k_group_flags<<<nblk(nisl), T, 0, st>>>(nisl, S.isl_cnt.p, S.g_small_rows.p, S.g_big.p); RP_COUNT_LAUNCH(1);
+      const uint32_t group_rows = W.tuning_.group_rows;
+      k_group_flags<<<nblk(nisl), T, 0, st>>>(nisl, group_rows, S.isl_cnt.p, S.g_small_rows.p, S.g_big.p); RP_COUNT_LAUNCH(1);
       uint32_t small_total = exclusive_scan_total(S, S.g_small_rows.p, S.g_small_pre.p, nisl, st);
       uint32_t nbig = exclusive_scan_total(S, S.g_big.p, S.g_big_pre.p, nisl, st);
-      g_small = small_total ? (small_total - 1) / GROUP_ROWS + 1 : 0;
+      g_small = small_total ? (small_total - 1) / group_rows + 1 : 0;
       ng = g_small + nbig;
-      k_group_of_isl<<<nblk(nisl), T, 0, st>>>(nisl, S.isl_cnt.p, S.g_small_pre.p, S.g_big_pre.p, g_small, S.g_of_isl.p); RP_COUNT_LAUNCH(1);
+      k_group_of_isl<<<nblk(nisl), T, 0, st>>>(nisl, group_rows, S.isl_cnt.p, S.g_small_pre.p, S.g_big_pre.p, g_small,
+                                                S.g_of_isl.p); RP_COUNT_LAUNCH(1);
       S.g_key.ensure(nsched + 1); S.g_key2.ensure(nsched + 1);
       k_group_keys<<<nblk(nsched), T, 0, st>>>(nsched, S.woff.p, S.wpos.p, S.g_of_isl.p, S.g_key.p); RP_COUNT_LAUNCH(1);
       int gbits = 1;
@@ -2436,7 +2438,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     }
     if (learned) {
       S.pred3.ensure(3 * (size_t)nc + 3); S.pred_used.ensure(nc + 1);
-      W.model_->predict(nc, S.feat.p, S.pred3.p, true, st);
+      W.model_->predict_async(nc, S.feat.p, S.pred3.p, stats + STAT_ERR, st);  // no host wait mid-tick
     }
     W.pred_valid_ = learned;
     P.end(PH_WARM_MATCH, st);
@@ -2459,7 +2461,9 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                                                  learned ? S.pred_used.p : nullptr, W.pred_cold_only_ ? 1u : 0u, SR); RP_COUNT_LAUNCH(1);
       const float tol = resid_mode ? W.res_tol_ : 0.0f;
       // dynamic shared memory above the 48 KB default, opted into once per device
-      const OnchipLayout lay_packed = onchip_layout(WG_ROWS, WG_BODIES, WG_ROWS);
+      const uint32_t gr = W.tuning_.group_rows;
+      const OnchipLayout lay_packed = onchip_layout(WG_ROWS(gr), WG_BODIES(gr), WG_ROWS(gr));
+      const OnchipLayout lay_packed_max = onchip_layout(WG_ROWS(GROUP_ROWS_MAX), WG_BODIES(GROUP_ROWS_MAX), WG_ROWS(GROUP_ROWS_MAX));
       const OnchipLayout lay_top = onchip_layout(kIslandRows[ISLAND_BUCKETS - 1], kIslandBodies[ISLAND_BUCKETS - 1], 1u);
       static std::atomic<unsigned long long> smem_attr{0};
       int dev = 0;
@@ -2469,10 +2473,10 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                                      (int)big_smem<128>(kBigBodies[2], kBigLevels[2])));
         RP_CUDA(cudaFuncSetAttribute(k_vel_solve_big<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)big_smem<64>(kBigBodies[1], kBigLevels[1])));
-        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_onchip<false, ONCHIP_T_ISLAND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)lay_top.bytes));
-        RP_CUDA(cudaFuncSetAttribute(k_vel_solve_onchip<true, ONCHIP_T_PACKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)lay_packed.bytes));
+        for (auto f : {k_vel_solve_onchip<false, 64>, k_vel_solve_onchip<false, 128>, k_vel_solve_onchip<false, 256>})
+          RP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay_top.bytes));
+        for (auto f : {k_vel_solve_onchip<true, 32>, k_vel_solve_onchip<true, 64>, k_vel_solve_onchip<true, 128>})
+          RP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay_packed_max.bytes));
         smem_attr.fetch_or(1ull << (dev & 63));
       }
       // single islands (classes 10..15, few blocks, long) run on the side streams, one bucket per
@@ -2490,7 +2494,9 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           if (!n) continue;
           if (top < 0) { top = b; P.begin(PH_VEL_ISLAND, sb); }
           OnchipLayout lay = onchip_layout(kIslandRows[b], kIslandBodies[b], 1u);
-          k_vel_solve_onchip<false, ONCHIP_T_ISLAND><<<n, ONCHIP_T_ISLAND, lay.bytes, sb>>>(
+          auto kern = W.tuning_.island_threads == 64 ? k_vel_solve_onchip<false, 64>
+                    : W.tuning_.island_threads == 256 ? k_vel_solve_onchip<false, 256> : k_vel_solve_onchip<false, 128>;
+          kern<<<n, W.tuning_.island_threads, lay.bytes, sb>>>(
               lay, 0u, n, lst(10 + b), 10u + (uint32_t)b, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
               S.g_nisl.p, SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
           if (b == top) P.end(PH_VEL_ISLAND, sb);
@@ -2498,7 +2504,9 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       }
       P.begin(PH_VEL_PACKED, st);
       if (g_small > 0) {
-        k_vel_solve_onchip<true, ONCHIP_T_PACKED><<<g_small, ONCHIP_T_PACKED, lay_packed.bytes, st>>>(
+        auto kern = W.tuning_.packed_threads == 32 ? k_vel_solve_onchip<true, 32>
+                  : W.tuning_.packed_threads == 128 ? k_vel_solve_onchip<true, 128> : k_vel_solve_onchip<true, 64>;
+        kern<<<g_small, W.tuning_.packed_threads, lay_packed.bytes, st>>>(
             lay_packed, 0u, g_small, nullptr, 3u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
             W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
       }

@@ -208,6 +208,134 @@ void tc_gemm(uint32_t M, uint32_t N, uint32_t K, const __nv_bfloat16* A, uint32_
   wm_count(1);
 }
 
+// ------------------------------------------------------------------ fused inference
+// The whole forward pass in one kernel: a persistent CTA of 128 threads keeps the four bf16 weight
+// matrices in shared memory (core-matrix layout, staged once), and for each tile of 128 rows converts
+// the rows' 24 f32 features to bf16, then per layer issues the MMAs into one 128-column TMEM
+// accumulator and runs the epilogue -- thread t reads row t's columns (tcgen05.ld), adds the bias,
+// applies SiLU and writes the bf16 activation into shared memory as the next layer's A operand.
+// The last layer writes the three outputs. Every product and rounding is the one the layer-by-layer
+// path (forward) makes, so the outputs are the same bits. Waits are bounded: a timeout sets
+// RPHYS_STATERR_WAIT_TIMEOUT in *err and the CTA stops.
+namespace fused {
+constexpr uint32_t kIn = 24, kInPad = 32, kH = 128;
+// byte offset of element (r, k) of a [rows x K] operand in the no-swizzle K-major layout
+__device__ __forceinline__ uint32_t core_off(uint32_t r, uint32_t k, uint32_t K) {
+  return (r / 8u) * (K / 8u) * 128u + (k / 8u) * 128u + (r % 8u) * 16u + (k % 8u) * 2u;
+}
+struct Smem {
+  __nv_bfloat16 w1[kH * kInPad], w2[kH * kH], w3[kH * kH], w4[16 * kH];
+  __nv_bfloat16 x[128 * kInPad], a[128 * kH];
+  float b[3 * kH + 16];
+  uint64_t mbar;
+  uint32_t tmem;
+};
+}  // namespace fused
+__global__ void __launch_bounds__(128) k_mlp_fused(uint32_t n, const float* __restrict__ feats,
+                                                   const __nv_bfloat16* __restrict__ wb, const float* __restrict__ w32,
+                                                   float* out3, uint32_t* err, uint32_t oW1, uint32_t oW2, uint32_t oW3,
+                                                   uint32_t oW4, uint32_t oB1, uint32_t oB2, uint32_t oB3, uint32_t oB4) {
+  using namespace fused;
+  extern __shared__ __align__(1024) unsigned char mf_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(mf_raw);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)), "r"(kH));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) mbar_init(&sm.mbar, 1);
+  // weights into the core-matrix layout, one 16-byte piece (8 bf16 of one row) per step
+  auto stage = [&](__nv_bfloat16* dst, const __nv_bfloat16* src, uint32_t rows, uint32_t K) {
+    for (uint32_t p = tid; p < rows * (K / 8u); p += 128u) {
+      uint32_t r = p / (K / 8u), j = p % (K / 8u);
+      *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(dst) + core_off(r, 8u * j, K)) =
+          *reinterpret_cast<const uint4*>(src + (size_t)r * K + 8u * j);
+    }
+  };
+  stage(sm.w1, wb + oW1, kH, kInPad);
+  stage(sm.w2, wb + oW2, kH, kH);
+  stage(sm.w3, wb + oW3, kH, kH);
+  stage(sm.w4, wb + oW4, 16, kH);
+  for (uint32_t i = tid; i < kH; i += 128u) {
+    sm.b[i] = w32[oB1 + i]; sm.b[kH + i] = w32[oB2 + i]; sm.b[2 * kH + i] = w32[oB3 + i];
+  }
+  if (tid < 16) sm.b[3 * kH + tid] = w32[oB4 + tid];
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem;
+  uint32_t phase = 0;
+  bool ok = true;
+  // one layer: D[128 x N] = A[128 x K] . W^T, then wait for it
+  auto layer = [&](const __nv_bfloat16* A, const __nv_bfloat16* W, uint32_t N, uint32_t K) {
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+      const uint32_t a0 = smem_u32(A), b0 = smem_u32(W), sbo = (K / 8u) * 128u, idesc = umma_idesc(128u, N);
+      for (uint32_t ks = 0; ks < K / 16u; ++ks)
+        umma_bf16(tmem, umma_desc(a0 + ks * 256u, 128u, sbo), umma_desc(b0 + ks * 256u, 128u, sbo), idesc, ks ? 1u : 0u);
+      umma_commit(&sm.mbar);
+    }
+    const bool waited = mbar_wait(&sm.mbar, phase);
+    phase ^= 1u;
+    tc_fence_after();
+    return __syncthreads_and(waited) != 0;
+  };
+  const uint32_t tiles = (n + 127u) / 128u;
+  for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+    const uint32_t row = tile * 128u + tid;  // thread t: row t of the tile (TMEM lane t)
+    // features: f32 -> bf16, inputs 24..31 zero, rows past n zero
+    for (uint32_t j = 0; j < kInPad / 8u; ++j) {
+      __align__(16) __nv_bfloat16 v[8];
+      for (uint32_t q = 0; q < 8u; ++q) {
+        uint32_t k = 8u * j + q;
+        v[q] = __float2bfloat16(row < n && k < kIn ? feats[(size_t)row * kIn + k] : 0.0f);
+      }
+      *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(sm.x) + core_off(tid, 8u * j, kInPad)) =
+          *reinterpret_cast<const uint4*>(v);
+    }
+    const __nv_bfloat16* Ws[3] = {sm.w1, sm.w2, sm.w3};
+    for (int L = 0; L < 3 && ok; ++L) {
+      ok = layer(L == 0 ? sm.x : sm.a, Ws[L], kH, L == 0 ? kInPad : kH);
+      if (!ok) break;
+      // epilogue: bias + SiLU -> bf16 activation (the next layer's A operand, row t)
+      for (uint32_t c = 0; c < kH; c += 16u) {
+        float v[16];
+        tmem_ld16(tmem + ((warp * 32u) << 16) + c, v);
+        __align__(16) __nv_bfloat16 h[16];
+        for (int k = 0; k < 16; ++k) {
+          float z = v[k] + sm.b[L * kH + c + k];
+          h[k] = __float2bfloat16(z / (1.0f + expf(-z)));
+        }
+        unsigned char* base = reinterpret_cast<unsigned char*>(sm.a);
+        *reinterpret_cast<uint4*>(base + core_off(tid, c, kH)) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(base + core_off(tid, c + 8u, kH)) = *reinterpret_cast<const uint4*>(h + 8);
+      }
+      tc_fence_before();  // the TMEM reads are done before the next layer's MMAs overwrite the columns
+    }
+    if (!ok) break;
+    ok = layer(sm.a, sm.w4, 16u, kH);
+    if (!ok) break;
+    float v[16];
+    tmem_ld16(tmem + ((warp * 32u) << 16), v);
+    if (row < n)
+      for (int k = 0; k < 3; ++k) out3[(size_t)row * 3 + k] = v[k] + sm.b[3 * kH + k];
+    tc_fence_before();
+    __syncthreads();  // the accumulator is read before the next tile's MMAs
+    tc_fence_after();
+  }
+  if (!ok && tid == 0) {
+    atomicOr(err, 4u);  // RPHYS_STATERR_WAIT_TIMEOUT
+    mbar_wait(&sm.mbar, phase ^ 1u);  // an MMA still in flight gets one more bounded chance
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kH));
+}
+
 // ------------------------------------------------------------------ elementwise pieces
 __device__ __forceinline__ float silu(float z) { return z / (1.0f + expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
@@ -376,20 +504,39 @@ WarmModel::Acts WarmModel::acts(uint32_t M, int base) {
   return a;
 }
 
-// Predictions for n rows of f32 features (24 each, host or device pointer given by on_device).
+// The fused forward pass (k_mlp_fused) over n rows of device features into device out3, queued on
+// st with nothing waited for; a timed-out wait ORs RPHYS_STATERR_WAIT_TIMEOUT into *err.
+void WarmModel::predict_async(uint32_t n, const float* feats, float* out3, uint32_t* err, cudaStream_t st) {
+  if (!n) return;
+  static int attr_dev = -1;
+  int dev = 0;
+  WM_CUDA(cudaGetDevice(&dev));
+  if (attr_dev != dev) {
+    WM_CUDA(cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(fused::Smem)));
+    attr_dev = dev;
+  }
+  int sms = 148;
+  WM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const uint32_t tiles = (n + 127) / 128;
+  const uint32_t grid = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;  // one persistent CTA per SM
+  k_mlp_fused<<<grid, 128, sizeof(fused::Smem), st>>>(n, feats, wb_, w_, out3, err, kW1, kW2, kW3, kW4, kB1, kB2, kB3, kB4);
+  wm_count(1);
+}
+// Predictions for n rows of f32 features (24 each, host or device pointer given by on_device),
+// returned when they are done.
 void WarmModel::predict(uint32_t n, const float* feats, float* out3, bool on_device, cudaStream_t st) {
   if (!st) st = st_;
-  uint32_t M = (n + 127) / 128 * 128;
-  if (M == 0) return;
-  float* F = (float*)buf(0, 4 * (size_t)M * kInPad);
-  __nv_bfloat16* X = (__nv_bfloat16*)buf(1, 2 * (size_t)M * kInPad);
-  float* Y = (float*)buf(2, 4 * (size_t)M * 16);
-  WM_CUDA(cudaMemsetAsync(F, 0, 4 * (size_t)M * kInPad, st));
-  WM_CUDA(cudaMemcpy2DAsync(F, 4 * kInPad, feats, 4 * kIn, 4 * kIn, n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-  k_f32_to_bf16<<<blocks((size_t)M * kInPad), 256, 0, st>>>((size_t)M * kInPad, F, X); wm_count(1);
-  Acts a = acts(M, 8);
-  forward(M, X, Y, st, &a);
-  WM_CUDA(cudaMemcpy2DAsync(out3, 12, Y, 64, 12, n, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  if (n == 0) return;
+  const float* F = feats;
+  float* O = out3;
+  if (!on_device) {
+    float* f = (float*)buf(0, 4 * (size_t)n * kIn);
+    WM_CUDA(cudaMemcpyAsync(f, feats, 4 * (size_t)n * kIn, cudaMemcpyHostToDevice, st));
+    F = f;
+    O = (float*)buf(2, 12 * (size_t)n);
+  }
+  predict_async(n, F, O, err_, st);
+  if (!on_device) WM_CUDA(cudaMemcpyAsync(out3, O, 12 * (size_t)n, cudaMemcpyDeviceToHost, st));
   WM_CUDA(cudaStreamSynchronize(st));
   check_err();
 }

@@ -26,6 +26,8 @@ class WarmModel {
   explicit WarmModel(uint64_t seed);
   ~WarmModel();
   void predict(uint32_t n, const float* feats, float* out3, bool on_device, cudaStream_t st = nullptr);
+  // the same predictions from device features into device memory, queued on st without waiting
+  void predict_async(uint32_t n, const float* feats, float* out3, uint32_t* err, cudaStream_t st);
   float gradients(uint32_t n, const float* feats, const float* targets, bool on_device);
   float train(uint32_t n, const float* feats, const float* targets, uint32_t epochs, uint32_t batch, float lr);
   void get_weights(float* out);

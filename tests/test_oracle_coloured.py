@@ -71,3 +71,16 @@ def test_set_solve_order_rejects_unknown(oracle):
         assert e.code == rp.RPHYS_ERR_BAD_ARG
     else:
         raise AssertionError("order 7 accepted")
+
+
+def test_tuning_is_stored_and_checked(oracle):
+    w, _ = _terrain(oracle, False, n=10)
+    assert w.tuning() == {"group_rows": 32, "packed_threads": 64, "island_threads": 128}
+    w.set_tuning(16, 128, 256)
+    assert w.tuning() == {"group_rows": 16, "packed_threads": 128, "island_threads": 256}
+    try:
+        w.set_tuning(32, 48, 128)
+    except rp.RPhysError as e:
+        assert e.code == rp.RPHYS_ERR_BAD_ARG
+    else:
+        raise AssertionError("packed_threads 48 accepted")
