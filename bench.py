@@ -124,8 +124,8 @@ def build_scene(lib, config, n_bodies=None, area=None, hf_n=None, worlds=4096, r
     n_bodies = n_bodies or 100_000
     w = lib.world(n_bodies + 16, n_bodies + 16)
     dt, n = scenes.terrain(rp, w, n_bodies=n_bodies, hf_n=hf_n or 512, area=area or 400.0)
-    return w, dt, n, (f"terrain: {n} bodies (40% spheres, 30% capsules, 30% boxes, 1000 kg/m^3) on a "
-                      f"{hf_n or 512}^2 heightfield at 1 m spacing, dt 1/60, 20 iters")
+    return w, dt, n, (f"terrain: {n} bodies (40% spheres, 30% capsules, 30% boxes, 1000 kg/m^3) starting in a "
+                      f"{area or 400.0:g} m square over a {hf_n or 512}^2 heightfield at 1 m spacing, dt 1/60, 20 iters")
 
 
 class ClockSampler:
@@ -242,7 +242,7 @@ def oracle_path():
 
 def oracle_world(lib, args, threads):
     """The CPU restatement's world of the benchmark scene (terrain or box drop), all threads."""
-    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies)
+    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, area=args.area)
     if args.mode == "residual":
         w.set_residual_mode(TOL, 4 * ITERS[args.config])
     lib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
@@ -344,6 +344,9 @@ def main():
                          "(default for ragdolls, whose articulations stay above 1e-4 for most islands)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--bodies", type=int, default=None)
+    ap.add_argument("--area", type=float, default=None,
+                    help="terrain: side of the square the bodies start in (default 400 m; the workload's density "
+                         "for n bodies is 400 * sqrt(n / 100000))")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-ticks", type=int, default=3, help="ticks of the CPU sample (and of the parity check)")
     ap.add_argument("--coloured", type=int, default=1, help="also replay the timed ticks in coloured order (1/0)")
@@ -366,7 +369,7 @@ def main():
     if args.config == "model":
         return run_model(args, lib, torch)
     worlds = args.worlds or (2000 if args.config == "ragdolls" else 4096)
-    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, worlds=worlds, rank=rank,
+    w, dt, nb, desc = build_scene(lib, args.config, n_bodies=args.bodies, area=args.area, worlds=worlds, rank=rank,
                                   world_size=world_size)
     args.mode = args.mode or ("fixed" if args.config == "ragdolls" else "residual")
     if args.mode == "residual":

@@ -501,6 +501,11 @@ __global__ void k_colour_levels(uint32_t ng, uint32_t g_small, const uint32_t* _
   }
   if (lane == 0) ncol[g] = over ? nl : mx;
 }
+// The residual histogram over the solve islands from each island's last-sweep residual (bits).
+__global__ void k_res_hist(uint32_t nisl, const uint32_t* __restrict__ isl_final, uint32_t* stats) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nisl) atomicAdd(&stats[STAT_RES_HIST + res_bin(__uint_as_float(isl_final[i]))], 1u);
+}
 __global__ void k_row_key_level(uint32_t n, const uint32_t* __restrict__ ord, const unsigned long long* __restrict__ keys,
                                 uint32_t* row_level) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -566,7 +571,8 @@ __device__ __forceinline__ float warp_max(float v) {
 __global__ void k_vel_solve(uint32_t nisl, uint32_t nc, Sched S, RowsV R, BodiesV B, float* acc_jn, float2* acc_jt,
                             const int* __restrict__ wm_idx, const float4* __restrict__ wa, const float4* __restrict__ wb,
                             int iters, float tol, uint32_t* stats, const uint32_t* __restrict__ g_class,
-                            const uint32_t* __restrict__ glist) {
+                            const uint32_t* __restrict__ glist, const uint32_t* __restrict__ row_islid,
+                            uint32_t* isl_final) {
   uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (wi >= nisl) return;
@@ -614,7 +620,7 @@ __global__ void k_vel_solve(uint32_t nisl, uint32_t nc, Sched S, RowsV R, Bodies
     atomicAdd(&stats[STAT_ROWSWEEPS], nrows * (uint32_t)it);
     atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
     atomicMax(&stats[STAT_RESID], fbits(resid));
-    atomicAdd(&stats[STAT_RES_HIST + res_bin(resid)], 1u);
+    isl_final[row_islid[S.ord[S.lvl_start[off]]]] = fbits(resid);  // the group is one island
     if (tol > 0.0f && !(resid <= tol)) {
       atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
       atomicAdd(&stats[STAT_ROWS_CAPPED], nrows);
@@ -1622,7 +1628,8 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
                                                          const uint32_t* __restrict__ g_nisl, Sched S, SRowsV R,
                                                          BodiesV G, const float4* __restrict__ wa,
                                                          const float4* __restrict__ wb, float* acc_jn, float2* acc_jt,
-                                                         int iters, float tol, uint32_t* stats) {
+                                                         int iters, float tol, uint32_t* stats,
+                                                         const uint32_t* __restrict__ row_islid, uint32_t* isl_final) {
   if (glist && blockIdx.x >= ng) return;
   uint32_t g = glist ? glist[blockIdx.x] : g0 + blockIdx.x;
   if (!glist && g >= ng) return;
@@ -1737,36 +1744,20 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
     uint32_t r = S.ord[base + i];
     acc_jn[r] = W.jn[i];
     acc_jt[r] = W.jt[i];
-    const uint32_t li = W.rows[i].flags >> 16;
+    const uint32_t li = MULTI ? W.rows[i].flags >> 16 : 0u;
     my_rs += W.isl_sw[li];
     if (tol > 0.0f && !W.isl_done[li]) my_rcap++;
+    isl_final[row_islid[r]] = W.isl_last[li];  // every row of an island writes the same value
   }
   uint32_t my_sw = 0, my_res = 0, my_cap = 0;
-  uint32_t h0 = 0, h1 = 0, h2 = 0, h3 = 0, h4 = 0, h5 = 0;
   for (uint32_t i = tid; i < nisl; i += NT) {
     my_sw = max(my_sw, W.isl_sw[i]);
     my_res = max(my_res, W.isl_last[i]);
     if (tol > 0.0f && !W.isl_done[i]) my_cap++;
-    switch (res_bin(__uint_as_float(W.isl_last[i]))) {
-      case 0: h0++; break;
-      case 1: h1++; break;
-      case 2: h2++; break;
-      case 3: h3++; break;
-      case 4: h4++; break;
-      default: h5++; break;
-    }
   }
   {
-    const uint32_t hs[6] = {__reduce_add_sync(0xffffffffu, h0), __reduce_add_sync(0xffffffffu, h1),
-                            __reduce_add_sync(0xffffffffu, h2), __reduce_add_sync(0xffffffffu, h3),
-                            __reduce_add_sync(0xffffffffu, h4), __reduce_add_sync(0xffffffffu, h5)};
     const uint32_t rc = __reduce_add_sync(0xffffffffu, my_rcap);
-    if (lane == 0) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k)
-        if (hs[k]) atomicAdd(&stats[STAT_RES_HIST + k], hs[k]);
-      if (rc) atomicAdd(&stats[STAT_ROWS_CAPPED], rc);
-    }
+    if (lane == 0 && rc) atomicAdd(&stats[STAT_ROWS_CAPPED], rc);
   }
   my_rs = __reduce_add_sync(0xffffffffu, my_rs);
   my_cap = __reduce_add_sync(0xffffffffu, my_cap);
@@ -1896,7 +1887,8 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
                                                            const float4* __restrict__ X, float4* J, BodiesV G,
                                                            const float4* __restrict__ wa, const float4* __restrict__ wb,
                                                            float* acc_jn, float2* acc_jt, int iters, float tol,
-                                                           uint32_t* stats) {
+                                                           uint32_t* stats, const uint32_t* __restrict__ row_islid,
+                                                           uint32_t* isl_final) {
   if (blockIdx.x >= n_listed) return;
   const uint32_t g = glist[blockIdx.x];
   if (g_class[g] != want_class) return;
@@ -1999,7 +1991,7 @@ __global__ void __launch_bounds__(CH) k_vel_solve_big(uint32_t BC, uint32_t LC, 
           atomicMax(&stats[STAT_SWEEPS], (uint32_t)it);
           atomicMax(&stats[STAT_RESID], rb);
           atomicAdd(&stats[STAT_ROWSWEEPS], (lvl[nl] - lvl[0]) * (uint32_t)it);
-          atomicAdd(&stats[STAT_RES_HIST + res_bin(__uint_as_float(rb))], 1u);
+          isl_final[row_islid[S.ord[lvl[0]]]] = rb;  // the group is one island
           if (tol > 0.0f && !(__uint_as_float(rb) <= tol)) {
             atomicAdd(&stats[STAT_ISLANDS_CAPPED], 1u);
             atomicAdd(&stats[STAT_ROWS_CAPPED], lvl[nl] - lvl[0]);
@@ -2460,6 +2452,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                                                  learned ? S.pred3.p : nullptr, S.row_isl2.p, S.g_class.p,
                                                  learned ? S.pred_used.p : nullptr, W.pred_cold_only_ ? 1u : 0u, SR); RP_COUNT_LAUNCH(1);
       const float tol = resid_mode ? W.res_tol_ : 0.0f;
+      S.isl_final.ensure(nisl + 1);
       // dynamic shared memory above the 48 KB default, opted into once per device
       const uint32_t gr = W.tuning_.group_rows;
       const OnchipLayout lay_packed = onchip_layout(WG_ROWS(gr), WG_BODIES(gr), WG_ROWS(gr));
@@ -2498,7 +2491,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                     : W.tuning_.island_threads == 256 ? k_vel_solve_onchip<false, 256> : k_vel_solve_onchip<false, 128>;
           kern<<<n, W.tuning_.island_threads, lay.bytes, sb>>>(
               lay, 0u, n, lst(10 + b), 10u + (uint32_t)b, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
-              S.g_nisl.p, SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+              S.g_nisl.p, SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats, S.row_islid.p,
+              S.isl_final.p); RP_COUNT_LAUNCH(1);
           if (b == top) P.end(PH_VEL_ISLAND, sb);
         }
       }
@@ -2508,7 +2502,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                   : W.tuning_.packed_threads == 128 ? k_vel_solve_onchip<true, 128> : k_vel_solve_onchip<true, 64>;
         kern<<<g_small, W.tuning_.packed_threads, lay_packed.bytes, st>>>(
             lay_packed, 0u, g_small, nullptr, 3u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.g_nisl.p, SM, SR, B,
-            W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats); RP_COUNT_LAUNCH(1);
+            W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats, S.row_islid.p, S.isl_final.p);
+        RP_COUNT_LAUNCH(1);
       }
       P.end(PH_VEL_PACKED, st);
       P.begin(PH_VEL_BIG, st);
@@ -2526,18 +2521,20 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           if (b == BIG_BUCKETS - 1)
             k_vel_solve_big<128><<<n, 128, big_smem<128>(kBigBodies[b], kBigLevels[b]), st>>>(
                 kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
-                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats);
+                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats,
+                S.row_islid.p, S.isl_final.p);
           else
             k_vel_solve_big<64><<<n, 64, big_smem<64>(kBigBodies[b], kBigLevels[b]), st>>>(
                 kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
-                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats);
+                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats,
+                S.row_islid.p, S.isl_final.p);
           RP_COUNT_LAUNCH(1);
         }
       }
       if (cls_n[2]) {
         k_vel_solve<<<nblk(cls_n[2] * 32, 128), 128, 0, st>>>(cls_n[2], nc, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
                                                                W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
-                                                               lst(2)); RP_COUNT_LAUNCH(1);
+                                                               lst(2), S.row_islid.p, S.isl_final.p); RP_COUNT_LAUNCH(1);
       }
       P.end(PH_VEL_BIG, st);
       if (big) {
@@ -2546,6 +2543,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           RP_CUDA(cudaStreamWaitEvent(st, W.ev_join_[k], 0));
         }
       }
+      // every solve island's last-sweep residual, written by its rows, binned once
+      k_res_hist<<<nblk(nisl), T, 0, st>>>(nisl, S.isl_final.p, stats); RP_COUNT_LAUNCH(1);
     }
     P.end(PH_VEL_SOLVE, st);
     joints_store_warm(W, R, nc, S.acc_jn.p, st);
