@@ -315,6 +315,66 @@ def cpu_sample_from_state(olib, args, blob, gpu_world, dt, ticks, threads):
     return nb * ticks / el, sample, same
 
 
+def batched_record(lib, torch, n_worlds, settle=30, ticks=10, every=32):
+    """The batched-worlds workload (n_worlds worlds of 16-4096 boxes, residual <= 1e-4 or 64 sweeps)
+    stepped as one device batch, against the plain path -- each world its own RPhysWorld stepped by
+    its own calls, as the reference steps one World per call -- on every `every`-th world (the worlds'
+    sizes are independent draws, so the sample has the table's size distribution). Both from tick 0:
+    `settle` ticks untimed, then `ticks` timed; the batch on the device clock, the plain worlds on the
+    host clock around each world's completed ticks (its launches and waits are its cost). Plus the
+    8-tick rollback window of the batch: restore, re-simulate, every world's hash compared."""
+    tol, cap = TOL, 4 * ITERS["batch"]
+    descs = [scenes.batch_world_descs(rp, k, seed=3) for k in range(n_worlds)]
+    total = sum(len(d) for d in descs)
+    b = lib.world(total + 16, total + 16)
+    dt = scenes.batch_setup(b)
+    for d in descs:
+        b.add_world(d)
+    b.set_residual_mode(tol, cap)
+    b.step_n(dt, settle)
+    snap = b.snapshot()
+    stream = torch.cuda.ExternalStream(b.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.step_n(dt, ticks)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    bms = e0.elapsed_time(e1)
+    sb = b.stats()
+    h_first = b.world_hashes()
+    b.restore_exact(snap)
+    b.step_n(dt, ticks)
+    rollback_ok = b.world_hashes() == h_first
+    b.free_snapshot(snap)
+    b.close()
+    plain_s, plain_bodies, sample = 0.0, 0, list(range(0, n_worlds, every))
+    for k in sample:
+        d = descs[k]
+        w = lib.world(len(d), len(d))
+        scenes.batch_setup(w)
+        w.add_bodies_array(d)
+        w.set_residual_mode(tol, cap)
+        w.step_n(dt, settle)
+        t0 = time.perf_counter()
+        w.step_n(dt, ticks)
+        plain_s += time.perf_counter() - t0
+        plain_bodies += len(d)
+        w.close()
+    batched_v = total * ticks / (bms / 1000.0)
+    plain_v = plain_bodies * ticks / plain_s
+    return {"workload": f"{n_worlds} worlds, {total:,} boxes, ticks {settle + 1}-{settle + ticks} from rest, residual "
+                        f"<=1e-4 or {cap} sweeps per island, previous-tick warm start",
+            "batched": {"value": batched_v, "unit": "body-ticks/s", "ms_per_tick": bms / ticks,
+                        "levels_last_tick": sb["levels"], "sweeps_last_tick": sb["sweeps"],
+                        "islands_capped_last_tick": sb["islands_capped"]},
+            "plain": {"value": plain_v, "unit": "body-ticks/s", "worlds": len(sample), "bodies": plain_bodies,
+                      "s_per_tick_all_sampled_worlds": plain_s / ticks,
+                      "note": "one RPhysWorld per world stepped through rphys_ext_step_n, host-timed"},
+            "batched_over_plain": batched_v / plain_v,
+            "rollback_window": {"ticks": ticks, "hashes_match": rollback_ok}}
+
+
 def metric_name(config):
     """The headline metric: throughput with every solve island sweeping until its residual is
     <= 1e-4 m/s or the sweep cap (4x the configuration's iteration count) stops it."""
@@ -351,6 +411,9 @@ def main():
     ap.add_argument("--cpu-ticks", type=int, default=3, help="ticks of the CPU sample (and of the parity check)")
     ap.add_argument("--coloured", type=int, default=1, help="also replay the timed ticks in coloured order (1/0)")
     ap.add_argument("--autotune", type=int, default=0, help="time every velocity-solve launch shape first (1/0)")
+    ap.add_argument("--batched", type=int, default=1,
+                    help="terrain: also measure the batched-worlds workload against stepping its worlds one by one")
+    ap.add_argument("--batched-worlds", type=int, default=4096)
     ap.add_argument("--tuning-out", default=autotune.TABLE, help="where --autotune records its table")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -478,6 +541,14 @@ def main():
         achieved = bytes_per_launch / (stage_ms / stage_calls / 1000.0) / 1e9
         roof.update({"achieved": achieved, "frac": achieved / peak, "bytes_per_launch": bytes_per_launch,
                      "ms_per_launch": stage_ms / stage_calls})
+    if stage == "vel_solve" and stage_calls:
+        # the bound that holds: the serial chain of the deepest island, sweeps x its levels dependent
+        # row updates (a level step: one row update plus a block barrier)
+        chain = st["sweeps"] * st["levels"]
+        roof["latency"] = {"level_steps_last_tick": chain, "ms_per_launch": stage_ms / stage_calls,
+                           "ns_per_level_step": stage_ms / stage_calls * 1e6 / chain if chain else None,
+                           "note": "vel_solve time over the deepest island's chain (sweeps x levels of the last "
+                                   "timed tick); the kernel is latency-bound, not HBM-bound"}
     else:
         roof.update({"achieved": None, "frac": None, "ms_per_launch": stage_ms / max(1, stage_calls)})
     stages = {k: round(v[0] / max(1, v[1]), 4) for k, v in prof.items() if v[1]}
@@ -605,6 +676,10 @@ def main():
 
     # the riftnet wire snapshot of the final state (riftphys-riftnet/src/wire.rs): packed on the
     # device and copied to the host, as a server does every tick; host-timed over a few calls
+    batched = None
+    if args.config == "terrain" and args.batched and rank == 0 and world_size == 1:
+        batched = batched_record(lib, torch, args.batched_worlds)
+
     wire = None
     if args.config == "terrain":
         import time as _time
@@ -654,6 +729,8 @@ def main():
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "stage_ms": stages,
                 "tuning": dict(w.tuning(), source=tuning_note)}
+        if batched is not None:
+            line["batched"] = batched
         if rollback is not None:
             line["rollback"] = rollback
         if learned is not None:

@@ -802,9 +802,12 @@ RPhysResult rphys_ext_batch_get_hashes(const RPhysWorld* Wc, uint32_t first, uin
     LOCK;
     uint32_t nw = W->w->batched() ? W->w->num_worlds() : 1u;
     if ((uint64_t)first + count > nw) return fail(RPHYS_ERR_INVALID_ID, "rphys_ext_batch_get_hashes: world range out of bounds");
-    for (uint32_t k = 0; k < count; ++k) {
-      if (W->w->batched()) W->w->step_hash_world(first + k, out[k].bytes);
-      else W->w->step_hash(out[k].bytes);
+    static_assert(sizeof(RPhysHash32) == 32, "RPhysHash32: 32 bytes");
+    if (W->w->batched()) {
+      // every requested world's digest from one pass of kernels over the world table
+      W->w->step_hash_worlds(first, count, reinterpret_cast<uint8_t*>(out));
+    } else {
+      for (uint32_t k = 0; k < count; ++k) W->w->step_hash(out[k].bytes);
     }
     return (RPhysResult)RPHYS_OK;
   });

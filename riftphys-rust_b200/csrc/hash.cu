@@ -553,3 +553,308 @@ void WorldGpu::step_hash_noalloc(uint8_t out32[32]) {
 }
 
 }  // namespace rp
+
+namespace rp {
+// ------------------------------------------------------------------ every world of a batch at once
+// The digests step_hash_world gives, for worlds [first, first + count), from kernels that walk the
+// world table: per world its body range, warm-cache range (binary search on the sorted keys), key
+// and joint-entry counts (differences of prefix sums over the whole cache), stream length and
+// chunk count (k_wh_meta); then, per slice of worlds whose streams fit the scratch, every world's
+// stream written at its chunk offset by one thread per record, one thread per 1 KiB chunk over all
+// the slice's worlds (k_wh_chunks), and one block per world merging its parent tree (k_wh_tree).
+struct WhMeta {
+  uint32_t b0, nb, wlo, nw, g0, nkeys, j0, njw, jo0, jbytes, jcount, nch;
+  unsigned long long len;
+};
+__global__ void k_wh_meta(uint32_t nwld, uint32_t w0, const uint32_t* __restrict__ wbs, uint32_t nb_total,
+                          const uint4* __restrict__ wk, uint32_t n_warm, const uint32_t* __restrict__ gflag,
+                          const uint32_t* __restrict__ gpre, const uint32_t* __restrict__ jrange,
+                          const uint32_t* __restrict__ jsz, const uint32_t* __restrict__ joff,
+                          const uint32_t* __restrict__ jhas, const uint32_t* __restrict__ jpos, WhMeta* meta) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nwld) return;
+  uint32_t w = w0 + k;
+  WhMeta m;
+  m.b0 = wbs[w];
+  uint32_t b1 = wbs[w + 1] < nb_total ? wbs[w + 1] : nb_total;
+  m.nb = b1 - m.b0;
+  auto lower = [&](uint32_t b) {
+    uint32_t lo = 0, hi = n_warm;
+    while (lo < hi) { uint32_t md = (lo + hi) >> 1; if (wk[md].x < b) lo = md + 1; else hi = md; }
+    return lo;
+  };
+  m.wlo = lower(m.b0);
+  uint32_t whi = lower(b1);
+  m.nw = whi - m.wlo;
+  m.g0 = m.nw ? gpre[m.wlo] : 0u;
+  m.nkeys = m.nw ? (gpre[whi - 1] + gflag[whi - 1]) - gpre[m.wlo] : 0u;
+  m.j0 = jrange[2 * w];
+  m.njw = jrange[2 * w + 1] - m.j0;
+  m.jo0 = m.njw ? joff[m.j0] : 0u;
+  m.jbytes = m.njw ? (joff[m.j0 + m.njw - 1] + jsz[m.j0 + m.njw - 1]) - m.jo0 : 0u;
+  m.jcount = m.njw ? (jpos[m.j0 + m.njw - 1] + jhas[m.j0 + m.njw - 1]) - jpos[m.j0] : 0u;
+  const unsigned long long cap = m.nb;
+  m.len = 48ull + 56ull * m.nb + 8 + 20ull * m.nkeys + 28ull * m.nw + 8 + 8 + m.jbytes + 8 + 8 + 12ull * m.nb + 8 + cap +
+          8 + 2ull * cap;
+  m.nch = (uint32_t)((m.len + 1023) / 1024);
+  meta[w] = m;
+}
+__device__ __forceinline__ uint32_t wh_world_of(const unsigned long long* __restrict__ ch0, uint32_t lo, uint32_t hi,
+                                                unsigned long long c) {  // last world of [lo, hi) starting at or before c
+  while (hi - lo > 1) { uint32_t md = (lo + hi) >> 1; if (ch0[md] <= c) lo = md; else hi = md; }
+  return lo;
+}
+// the fixed parts of every world's stream: header, section counts
+__global__ void k_wh_head(uint32_t w0, uint32_t nwld, const WhMeta* __restrict__ meta,
+                          const unsigned long long* __restrict__ ch0, unsigned long long epoch, unsigned long long rng,
+                          uint8_t* buf) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nwld) return;
+  const WhMeta m = meta[w0 + k];
+  uint8_t* p = buf + (ch0[k] - ch0[0]) * 1024ull;
+  const uint8_t empty[32] = {0xaf, 0x13, 0x49, 0xb9, 0xf5, 0xf9, 0xa1, 0xa6, 0xa0, 0x40, 0x4d, 0xea, 0x36, 0xdc, 0xc9, 0x49,
+                             0x9b, 0xcb, 0x25, 0xc9, 0xad, 0xc1, 0x12, 0xb7, 0xcc, 0x9a, 0x93, 0xca, 0xe4, 0x1f, 0x32, 0x62};
+  put64(p, epoch);
+  put64(p + 8, rng);
+  for (int i = 0; i < 32; ++i) p[16 + i] = empty[i];
+  const unsigned long long off_warm = 48ull + 56ull * m.nb;
+  put64(p + off_warm, m.nkeys);
+  const unsigned long long off_joints = off_warm + 8 + 20ull * m.nkeys + 28ull * m.nw + 8;
+  put64(p + off_joints, m.jcount);
+}
+// body records and the carried tail of each world (0-based ids; capacity = the world's body count)
+__global__ void k_wh_bodies(uint32_t w0, uint32_t nwld, uint32_t bfirst, uint32_t nbod, const uint32_t* __restrict__ wbs,
+                            const WhMeta* __restrict__ meta, const unsigned long long* __restrict__ ch0,
+                            const float4* __restrict__ pos, const float4* __restrict__ rot, const float4* __restrict__ lin,
+                            const float4* __restrict__ ang, const float4* __restrict__ last,
+                            const uint8_t* __restrict__ awake, const uint16_t* __restrict__ ticks, uint8_t* buf) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nbod) return;
+  const uint32_t i = bfirst + t;
+  uint32_t lo = 0, hi = nwld;  // the world holding body i
+  while (hi - lo > 1) { uint32_t md = (lo + hi) >> 1; if (wbs[w0 + md] <= i) lo = md; else hi = md; }
+  const WhMeta m = meta[w0 + lo];
+  uint8_t* s = buf + (ch0[lo] - ch0[0]) * 1024ull;
+  const uint32_t li = i - m.b0;
+  uint8_t* p = s + 48 + 56ull * li;
+  float4 a = pos[i], q = rot[i], l = lin[i], w = ang[i];
+  put32(p, li);
+  put32(p + 4, canon_bits(a.x)); put32(p + 8, canon_bits(a.y)); put32(p + 12, canon_bits(a.z));
+  put32(p + 16, canon_bits(q.x)); put32(p + 20, canon_bits(q.y)); put32(p + 24, canon_bits(q.z)); put32(p + 28, canon_bits(q.w));
+  put32(p + 32, canon_bits(l.x)); put32(p + 36, canon_bits(l.y)); put32(p + 40, canon_bits(l.z));
+  put32(p + 44, canon_bits(w.x)); put32(p + 48, canon_bits(w.y)); put32(p + 52, canon_bits(w.z));
+  // tail: [u64 nb][12 nb][u64 cap][cap][u64 cap][2 cap]
+  uint8_t* tl = s + 48ull + 56ull * m.nb + 8 + 20ull * m.nkeys + 28ull * m.nw + 8 + 8 + m.jbytes + 8;
+  if (li == 0) put64(tl, m.nb);
+  float4 v = last[i];
+  put32(tl + 8 + 12ull * li, canon_bits(v.x)); put32(tl + 12 + 12ull * li, canon_bits(v.y));
+  put32(tl + 16 + 12ull * li, canon_bits(v.z));
+  uint8_t* aw = tl + 8 + 12ull * m.nb;
+  if (li == 0) put64(aw, m.nb);
+  aw[8 + li] = awake[i];
+  uint8_t* tk = aw + 8 + m.nb;
+  if (li == 0) put64(tk, m.nb);
+  uint16_t tv = ticks[i];
+  tk[8 + 2 * li] = (uint8_t)tv;
+  tk[9 + 2 * li] = (uint8_t)(tv >> 8);
+}
+// warm-cache entries [efirst, efirst + n) of the slice: key headers and entries, ids 0-based
+__global__ void k_wh_warm(uint32_t w0, uint32_t nwld, uint32_t efirst, uint32_t n, const uint32_t* __restrict__ wbs,
+                          const WhMeta* __restrict__ meta, const unsigned long long* __restrict__ ch0,
+                          const uint4* __restrict__ wk, const float4* __restrict__ wa, const float4* __restrict__ wb,
+                          const uint32_t* __restrict__ gflag, const uint32_t* __restrict__ gpre, uint32_t n_warm, uint8_t* buf) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t e = efirst + t;
+  const uint4 key = wk[e];
+  uint32_t lo = 0, hi = nwld;  // the world of the key's first body
+  while (hi - lo > 1) { uint32_t md = (lo + hi) >> 1; if (wbs[w0 + md] <= key.x) lo = md; else hi = md; }
+  const WhMeta m = meta[w0 + lo];
+  uint8_t* out = buf + (ch0[lo] - ch0[0]) * 1024ull + 48ull + 56ull * m.nb + 8;
+  const uint32_t le = e - m.wlo, g = gpre[e] + gflag[e] - 1 - m.g0;
+  if (gflag[e]) {
+    uint32_t cnt = 1;
+    while (e + cnt < n_warm && !gflag[e + cnt]) cnt++;
+    uint8_t* h = out + 20ull * g + 28ull * le;
+    put32(h, key.x - m.b0); put32(h + 4, key.y == 0xFFFFFFFFu ? key.y : key.y - m.b0);
+    put32(h + 8, key.z); put32(h + 12, key.w); put32(h + 16, cnt);
+  }
+  uint8_t* p = out + 20ull * (g + 1) + 28ull * le;
+  float4 a = wa[e], b = wb[e];
+  put32(p, canon_bits(a.x)); put32(p + 4, canon_bits(a.y)); put32(p + 8, canon_bits(a.z)); put32(p + 12, canon_bits(a.w));
+  put32(p + 16, canon_bits(b.x)); put32(p + 20, canon_bits(b.y)); put32(p + 24, canon_bits(b.z));
+}
+// joint-cache entries of joints [jfirst, jfirst + n) of the slice, joint ids 0-based per world
+__global__ void k_wh_joints(uint32_t w0, uint32_t nwld, uint32_t jfirst, uint32_t n, const uint32_t* __restrict__ jrange,
+                            const WhMeta* __restrict__ meta, const unsigned long long* __restrict__ ch0,
+                            const uint32_t* __restrict__ jw_n,
+                            const uint8_t* __restrict__ tag, const float* __restrict__ lam,
+                            const uint32_t* __restrict__ joff, uint8_t* buf) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t j = jfirst + t;
+  const uint32_t c = jw_n[j];
+  if (c == 0xFFFFFFFFu) return;
+  uint32_t lo = 0, hi = nwld;  // the last world whose joint range starts at or before j (empty ones come first)
+  while (hi - lo > 1) { uint32_t md = (lo + hi) >> 1; if (jrange[2 * (w0 + md)] <= j) lo = md; else hi = md; }
+  const WhMeta m = meta[w0 + lo];
+  uint8_t* p = buf + (ch0[lo] - ch0[0]) * 1024ull + 48ull + 56ull * m.nb + 8 + 20ull * m.nkeys + 28ull * m.nw + 8 + 8 +
+               (joff[j] - m.jo0);
+  put32(p, j - m.j0);
+  put32(p + 4, c);
+  for (uint32_t k = 0; k < c; ++k) {
+    p[8 + 5 * k] = tag[kJointRows * (size_t)j + k];
+    put32(p + 9 + 5 * k, canon_bits(lam[kJointRows * (size_t)j + k]));
+  }
+}
+// one thread per 1 KiB chunk of the slice's streams: chaining values, or the root of a one-chunk world
+__global__ void k_wh_chunks(uint32_t w0, uint32_t nwld, unsigned long long nchunks, const WhMeta* __restrict__ meta,
+                            const unsigned long long* __restrict__ ch0, const uint8_t* __restrict__ buf, uint32_t* cvs,
+                            uint32_t* roots) {
+  unsigned long long gc = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gc >= nchunks) return;
+  const unsigned long long c_abs = ch0[0] + gc;
+  const uint32_t k = wh_world_of(ch0, 0, nwld, c_abs);
+  const WhMeta m = meta[w0 + k];
+  const unsigned long long c = c_abs - ch0[k];
+  const unsigned long long base = c * 1024ull;
+  const unsigned long long clen = m.len - base < 1024ull ? m.len - base : 1024ull;
+  const uint32_t nblocks = clen == 0 ? 1u : (uint32_t)((clen + 63) / 64);
+  const uint8_t* data = buf + (ch0[k] - ch0[0]) * 1024ull + base;
+  uint32_t cv[8];
+  for (int i = 0; i < 8; ++i) cv[i] = c_iv[i];
+  for (uint32_t b = 0; b < nblocks; ++b) {
+    uint32_t blk[16];
+    const uint32_t* wds = reinterpret_cast<const uint32_t*>(data + 64ull * b);
+    for (int i = 0; i < 16; ++i) blk[i] = wds[i];
+    uint32_t blen = b + 1 == nblocks ? (uint32_t)(clen - 64ull * b) : 64u;
+    uint32_t flags = (b == 0 ? CHUNK_START : 0u) | (b + 1 == nblocks ? CHUNK_END : 0u);
+    if (m.nch == 1 && b + 1 == nblocks) flags |= ROOT;
+    uint32_t o[8];
+    b3_compress(cv, blk, c, blen, flags, o);
+    for (int i = 0; i < 8; ++i) cv[i] = o[i];
+  }
+  uint32_t* dst = m.nch == 1 ? roots + 8ull * k : cvs + 8ull * (c_abs - ch0[0]);
+  for (int i = 0; i < 8; ++i) dst[i] = cv[i];
+}
+// one block per world of the slice: its parent tree, level by level (left-complete: an odd last
+// node moves up unchanged), ping-ponging between the chunk values and a second buffer
+__global__ void k_wh_tree(uint32_t w0, const WhMeta* __restrict__ meta, const unsigned long long* __restrict__ ch0,
+                          uint32_t* cvs, uint32_t* cvs2, uint32_t* roots) {
+  const uint32_t k = blockIdx.x;
+  const WhMeta m = meta[w0 + k];
+  if (m.nch <= 1) return;
+  uint32_t* a = cvs + 8ull * (ch0[k] - ch0[0]);
+  uint32_t* b = cvs2 + 8ull * (ch0[k] - ch0[0]);
+  uint32_t n = m.nch;
+  while (n > 1) {
+    const uint32_t n_out = (n + 1) / 2;
+    for (uint32_t t = threadIdx.x; t < n_out; t += blockDim.x) {
+      if (2 * t + 1 < n) {
+        uint32_t blk[16], cv[8], o[8];
+        for (int i = 0; i < 8; ++i) { blk[i] = a[16 * t + i]; blk[8 + i] = a[16 * t + 8 + i]; cv[i] = c_iv[i]; }
+        b3_compress(cv, blk, 0, 64, PARENT | (n == 2 ? ROOT : 0u), o);
+        uint32_t* dst = n == 2 ? roots + 8ull * k : b + 8 * t;
+        for (int i = 0; i < 8; ++i) dst[i] = o[i];
+      } else {
+        for (int i = 0; i < 8; ++i) b[8 * t + i] = a[16 * t + i];
+      }
+    }
+    __syncthreads();
+    uint32_t* tmp = a; a = b; b = tmp;
+    n = n_out;
+  }
+}
+
+void WorldGpu::step_hash_worlds(uint32_t first, uint32_t count, uint8_t* out) {
+  if (!count) return;
+  upload_joints();
+  upload_worlds();
+  Scratch& S = *s_;
+  cudaStream_t st = stream_;
+  const int T = 256;
+  const uint32_t nwt = num_worlds(), nj = num_joints();
+  // the world table (body starts + end) and each world's joint id range, from the host mirrors
+  std::vector<uint32_t> wbs(nwt + 1), jr(2 * (size_t)nwt);
+  for (uint32_t w = 0; w < nwt; ++w) wbs[w] = h_wb_start_[w];
+  wbs[nwt] = nb_;
+  auto first_at = [&](uint32_t b) {
+    uint32_t lo = 0, hi = nj;
+    while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (h_joints_[m].a < b) lo = m + 1; else hi = m; }
+    return lo;
+  };
+  for (uint32_t w = 0; w < nwt; ++w) { jr[2 * w] = first_at(wbs[w]); jr[2 * w + 1] = first_at(wbs[w + 1]); }
+  static_assert(sizeof(WhMeta) == 56, "WhMeta: 7 eight-byte words");
+  S.wh_wbs.ensure(nwt + 1); S.wh_jr.ensure(2 * (size_t)nwt + 2); S.wh_meta.ensure(7 * (size_t)nwt + 7);
+  RP_CUDA(cudaMemcpyAsync(S.wh_wbs.p, wbs.data(), 4 * wbs.size(), cudaMemcpyHostToDevice, st));
+  RP_CUDA(cudaMemcpyAsync(S.wh_jr.p, jr.data(), 4 * jr.size(), cudaMemcpyHostToDevice, st));
+  // key groups of the whole warm cache and the joint entries' sizes, as prefix sums
+  S.woff.ensure(n_warm + 1); S.wpos.ensure(n_warm + 1);
+  if (n_warm) {
+    k_h_warm_flags<<<(n_warm + T - 1) / T, T, 0, st>>>(n_warm, warm_key.p, S.woff.p); RP_COUNT_LAUNCH(1);
+    exclusive_scan_total(S, S.woff.p, S.wpos.p, n_warm, st);
+  }
+  S.jh_sz.ensure(nj + 1); S.jh_off.ensure(nj + 1); S.jh_has.ensure(nj + 1); S.jh_pos.ensure(nj + 1);
+  if (nj) {
+    k_hj_sizes<<<(nj + T - 1) / T, T, 0, st>>>(nj, jw_n.p, S.jh_sz.p, S.jh_has.p); RP_COUNT_LAUNCH(1);
+    exclusive_scan_total(S, S.jh_sz.p, S.jh_off.p, nj, st);
+    exclusive_scan_total(S, S.jh_has.p, S.jh_pos.p, nj, st);
+  }
+  WhMeta* meta = reinterpret_cast<WhMeta*>(S.wh_meta.p);
+  k_wh_meta<<<(count + T - 1) / T, T, 0, st>>>(count, first, S.wh_wbs.p, nb_, warm_key.p, n_warm, S.woff.p, S.wpos.p,
+                                                S.wh_jr.p, S.jh_sz.p, S.jh_off.p, S.jh_has.p, S.jh_pos.p, meta);
+  RP_COUNT_LAUNCH(1);
+  std::vector<WhMeta> hm(count);
+  RP_CUDA(cudaMemcpyAsync(hm.data(), meta + first, sizeof(WhMeta) * count, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaStreamSynchronize(st));
+  // slices of worlds whose streams fit 64 MiB (a world larger than that is a slice alone)
+  const unsigned long long budget = 64ull << 10;  // chunks
+  S.wh_roots.ensure(8 * (size_t)count + 8);
+  uint32_t w = 0;
+  while (w < count) {
+    uint32_t e = w;
+    unsigned long long chunks = 0;
+    std::vector<unsigned long long> ch0;
+    while (e < count && (e == w || chunks + hm[e].nch <= budget)) { ch0.push_back(chunks); chunks += hm[e].nch; e++; }
+    const uint32_t nwl = e - w;
+    ch0.push_back(chunks);
+    S.wh_ch0.ensure(ch0.size());
+    S.hbuf.ensure((size_t)chunks * 1024 + 64);
+    S.hcv.ensure(16 * (size_t)chunks + 16);
+    RP_CUDA(cudaMemcpyAsync(S.wh_ch0.p, ch0.data(), 8 * ch0.size(), cudaMemcpyHostToDevice, st));
+    RP_CUDA(cudaMemsetAsync(S.hbuf.p, 0, (size_t)chunks * 1024 + 64, st));
+    const uint32_t wg = first + w;
+    k_wh_head<<<(nwl + T - 1) / T, T, 0, st>>>(wg, nwl, meta, S.wh_ch0.p, epoch_, rng_, S.hbuf.p); RP_COUNT_LAUNCH(1);
+    const uint32_t bfirst = hm[w].b0, nbod = hm[e - 1].b0 + hm[e - 1].nb - bfirst;
+    if (nbod) {
+      k_wh_bodies<<<(nbod + T - 1) / T, T, 0, st>>>(wg, nwl, bfirst, nbod, S.wh_wbs.p, meta, S.wh_ch0.p, pos.p, rot.p, lin.p,
+                                                    ang.p, last_lin.p, awake.p, sleep_ticks.p, S.hbuf.p);
+      RP_COUNT_LAUNCH(1);
+    }
+    const uint32_t efirst = hm[w].wlo, nent = hm[e - 1].wlo + hm[e - 1].nw - efirst;
+    if (nent) {
+      k_wh_warm<<<(nent + T - 1) / T, T, 0, st>>>(wg, nwl, efirst, nent, S.wh_wbs.p, meta, S.wh_ch0.p, warm_key.p, warm_a.p,
+                                                  warm_b.p, S.woff.p, S.wpos.p, n_warm, S.hbuf.p);
+      RP_COUNT_LAUNCH(1);
+    }
+    const uint32_t jfirst = hm[w].j0, njs = hm[e - 1].j0 + hm[e - 1].njw - jfirst;
+    if (njs) {
+      k_wh_joints<<<(njs + T - 1) / T, T, 0, st>>>(wg, nwl, jfirst, njs, S.wh_jr.p, meta, S.wh_ch0.p, jw_n.p,
+                                                   jw_tag.p, jw_lam.p, S.jh_off.p, S.hbuf.p);
+      RP_COUNT_LAUNCH(1);
+    }
+    k_wh_chunks<<<(unsigned)((chunks + 127) / 128), 128, 0, st>>>(wg, nwl, chunks, meta, S.wh_ch0.p, S.hbuf.p, S.hcv.p,
+                                                                  S.wh_roots.p + 8ull * w);
+    RP_COUNT_LAUNCH(1);
+    k_wh_tree<<<nwl, 128, 0, st>>>(wg, meta, S.wh_ch0.p, S.hcv.p, S.hcv.p + 8 * (size_t)chunks + 8, S.wh_roots.p + 8ull * w);
+    RP_COUNT_LAUNCH(1);
+    w = e;
+  }
+  std::vector<uint32_t> r(8 * (size_t)count);
+  RP_CUDA(cudaMemcpyAsync(r.data(), S.wh_roots.p, 32 * (size_t)count, cudaMemcpyDeviceToHost, st));
+  RP_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t k = 0; k < count; ++k)
+    for (int i = 0; i < 8; ++i)
+      for (int b = 0; b < 4; ++b) out[32 * (size_t)k + 4 * i + b] = (uint8_t)(r[8 * (size_t)k + i] >> (8 * b));
+}
+}  // namespace rp

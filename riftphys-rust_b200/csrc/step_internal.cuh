@@ -180,7 +180,9 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> lv_key, lv_key2, lv_val, lv_val2, lv_pred, lv_level, lv_np1, lv_lead;  // parallel level schedule
   DBuf<uint4> col_mask;                                                        // coloured order: colours per body
   DBuf<uint32_t> col_nlev, col_ord;
-  DBuf<uint32_t> isl_final;                                                    // per solve island: last residual (bits)
+  DBuf<uint32_t> isl_final;
+  DBuf<unsigned long long> wh_meta, wh_ch0;                                    // per-world hashes of a batch
+  DBuf<uint32_t> wh_wbs, wh_jr, wh_roots;                                                    // per solve island: last residual (bits)
   DBuf<uint32_t> row_islid, row_lisl, li_flag, li_pre, g_nisl;                 // islands inside solve groups
   DBuf<uint32_t> pp_rows, pp_key, pp_gs, pp_gc, ord_pp, lvl_off_pp, lvl_start_pp, nlev_pp;  // position pass (joints)
   DBuf<uint32_t> cls_cnt, cls_list;                                            // solve groups by class

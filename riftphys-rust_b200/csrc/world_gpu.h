@@ -121,6 +121,8 @@ class WorldGpu {
   uint32_t num_worlds() const { return (uint32_t)h_wb_start_.size(); }
   bool batched() const { return batch_; }
   void step_hash_world(uint32_t w, uint8_t out[32]);    // that world's own digest
+  // the digests of worlds [first, first + count), 32 bytes each, from kernels over the world table
+  void step_hash_worlds(uint32_t first, uint32_t count, uint8_t* out);
   std::vector<uint32_t> h_wb_start_, h_wc_start_;       // first body / collider of each world
   bool batch_ = false, worlds_dirty_ = false;
   DBuf<uint32_t> col_world, world_col_start;           // per collider; per world (+ end)
