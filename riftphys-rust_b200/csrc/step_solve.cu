@@ -1616,7 +1616,7 @@ __host__ __device__ inline OnchipLayout onchip_layout(uint32_t RC, uint32_t BC, 
   L.bytes = o;
   return L;
 }
-// threads of a packed-group block (32, 64 or 128) and of a single-island block (64, 128 or 256) are
+// threads of a packed-group block (32, 64 or 128) and of a single-island block (32 to 256) are
 // tuning knobs (WorldGpu::Tuning); each value has its own instantiation below
 template <bool MULTI, int NT>
 __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32_t g0, uint32_t ng,
@@ -2466,7 +2466,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                                      (int)big_smem<128>(kBigBodies[2], kBigLevels[2])));
         RP_CUDA(cudaFuncSetAttribute(k_vel_solve_big<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)big_smem<64>(kBigBodies[1], kBigLevels[1])));
-        for (auto f : {k_vel_solve_onchip<false, 64>, k_vel_solve_onchip<false, 128>, k_vel_solve_onchip<false, 256>})
+        for (auto f : {k_vel_solve_onchip<false, 32>, k_vel_solve_onchip<false, 64>, k_vel_solve_onchip<false, 128>,
+                       k_vel_solve_onchip<false, 256>})
           RP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay_top.bytes));
         for (auto f : {k_vel_solve_onchip<true, 32>, k_vel_solve_onchip<true, 64>, k_vel_solve_onchip<true, 128>})
           RP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay_packed_max.bytes));
@@ -2487,8 +2488,10 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           if (!n) continue;
           if (top < 0) { top = b; P.begin(PH_VEL_ISLAND, sb); }
           OnchipLayout lay = onchip_layout(kIslandRows[b], kIslandBodies[b], 1u);
-          auto kern = W.tuning_.island_threads == 64 ? k_vel_solve_onchip<false, 64>
-                    : W.tuning_.island_threads == 256 ? k_vel_solve_onchip<false, 256> : k_vel_solve_onchip<false, 128>;
+          auto kern = W.tuning_.island_threads == 32    ? k_vel_solve_onchip<false, 32>
+                      : W.tuning_.island_threads == 64  ? k_vel_solve_onchip<false, 64>
+                      : W.tuning_.island_threads == 256 ? k_vel_solve_onchip<false, 256>
+                                                        : k_vel_solve_onchip<false, 128>;
           kern<<<n, W.tuning_.island_threads, lay.bytes, sb>>>(
               lay, 0u, n, lst(10 + b), 10u + (uint32_t)b, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
               S.g_nisl.p, SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats, S.row_islid.p,

@@ -95,7 +95,7 @@ class WorldGpu {
   bool coloured_ = false;
   // Launch shapes of the velocity solve (none changes a result bit: islands are independent and the
   // rows of a level are): rows up to which islands are packed into shared groups (8, 16, 32), threads
-  // of a packed-group block (32, 64, 128) and of a single-island block (64, 128, 256). Defaults are
+  // of a packed-group block (32, 64, 128) and of a single-island block (32, 64, 128, 256). Defaults are
   // the autotuner's choice for the terrain workload.
   struct Tuning { uint32_t group_rows = 32, packed_threads = 64, island_threads = 128; };
   Tuning tuning_;
