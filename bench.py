@@ -470,6 +470,7 @@ def main():
                         f"{desc}; 5 ticks from the state after {args.settle + args.warmup} ticks, per shape")
         tuning_note = "autotuned in this run"
         print(f"[bench] autotune: best {best}; all same bits: {all(r['same_bits'] for r in rows)}", file=sys.stderr)
+        w.restore_exact(snap)  # the tuner stepped on from the snapshot: back to it
     else:
         tuning_note = "recorded table" if autotune.apply(w, args.config) else "compiled defaults"
     # the same state as a host blob, for the CPU restatement's sample of the same ticks

@@ -138,9 +138,6 @@ static const double kTwoOverPi = 0x1.45f306dc9c883p-1;
 static const double kPio2_1 = 0x1.921fb54400000p+0;
 static const double kPio2_2 = 0x1.0b4611a600000p-34;
 static const double kPio2_3 = 0x1.3198a2e037073p-69;
-static const double kInvLn2 = 0x1.71547652b82fep+0;
-static const double kLn2Hi = 0x1.62e42fef00000p-1;
-static const double kLn2Lo = 0x1.473de6af278edp-34;
 
 // Taylor series of sin and cos about 0, |r| <= pi/4 (+ reduction slack): terms through r^19 / r^18.
 static inline double sin_poly(double r) {
@@ -187,31 +184,33 @@ static inline void sincosf_rp(float xf, float* s, float* c) {
   }
   *s = (float)sv; *c = (float)cv;
 }
-// exp of an f32, rounded once to f32.
+// exp of an f32, rounded once to f32: x = (32 m + j) ln2/32 + r with |r| <= ln2/64, e^x = 2^m 2^(j/32) e^r;
+// 2^(j/32) the double nearest it (computed with 80-digit decimal arithmetic), e^r - 1 by its
+// Taylor series through r^5 (error below 3e-15).
+static const double kExp2_32[32] = {
+  0x1.0000000000000p+0, 0x1.059b0d3158574p+0, 0x1.0b5586cf9890fp+0, 0x1.11301d0125b51p+0,
+  0x1.172b83c7d517bp+0, 0x1.1d4873168b9aap+0, 0x1.2387a6e756238p+0, 0x1.29e9df51fdee1p+0,
+  0x1.306fe0a31b715p+0, 0x1.371a7373aa9cbp+0, 0x1.3dea64c123422p+0, 0x1.44e086061892dp+0,
+  0x1.4bfdad5362a27p+0, 0x1.5342b569d4f82p+0, 0x1.5ab07dd485429p+0, 0x1.6247eb03a5585p+0,
+  0x1.6a09e667f3bcdp+0, 0x1.71f75e8ec5f74p+0, 0x1.7a11473eb0187p+0, 0x1.82589994cce13p+0,
+  0x1.8ace5422aa0dbp+0, 0x1.93737b0cdc5e5p+0, 0x1.9c49182a3f090p+0, 0x1.a5503b23e255dp+0,
+  0x1.ae89f995ad3adp+0, 0x1.b7f76f2fb5e47p+0, 0x1.c199bdd85529cp+0, 0x1.cb720dcef9069p+0,
+  0x1.d5818dcfba487p+0, 0x1.dfc97337b9b5fp+0, 0x1.ea4afa2a490dap+0, 0x1.f50765b6e4540p+0
+};
 static inline float expf_rp(float xf) {
   double x = (double)xf;
   if (std::isnan(x)) return NAN;
   if (x > 89.0) return INFINITY;
   if (x < -104.0) return 0.0f;
-  double k = std::floor(x * kInvLn2 + 0.5);
-  double r = (x - k * kLn2Hi) - k * kLn2Lo;
-  // Taylor series of e^r through r^14, |r| <= 0.35
-  double p = 1.0 / 87178291200.0;                    // 1/14!
-  p = p * r + 1.0 / 6227020800.0;                    // 1/13!
-  p = p * r + 1.0 / 479001600.0;                     // 1/12!
-  p = p * r + 1.0 / 39916800.0;                      // 1/11!
-  p = p * r + 1.0 / 3628800.0;                       // 1/10!
-  p = p * r + 1.0 / 362880.0;                        // 1/9!
-  p = p * r + 1.0 / 40320.0;                         // 1/8!
-  p = p * r + 1.0 / 5040.0;                          // 1/7!
-  p = p * r + 1.0 / 720.0;                           // 1/6!
-  p = p * r + 1.0 / 120.0;                           // 1/5!
-  p = p * r + 1.0 / 24.0;                            // 1/4!
-  p = p * r + 1.0 / 6.0;                             // 1/3!
-  p = p * r + 0.5;                                   // 1/2!
-  p = p * r + 1.0;
-  p = p * r + 1.0;
-  return (float)std::ldexp(p, (int)k);
+  double k = std::floor(x * 0x1.71547652b82fep+5 + 0.5);               // 32 / ln2
+  double r = (x - k * 0x1.62e42fef00000p-6) - k * 0x1.473de6af278edp-39;  // ln2/32, split
+  long long ki = (long long)k;
+  int j = (int)(ki & 31), m = (int)((ki - j) / 32);
+  double r2 = r * r;
+  double q = r + (r2 * (0.5 + r * (1.0 / 6.0)) + (r2 * r2) * (1.0 / 24.0 + r * (1.0 / 120.0)));
+  double t = kExp2_32[j];
+  double p = t + t * q;
+  return (float)std::ldexp(p, m);
 }
 
 // Quat::from_axis_angle(axis, angle): (axis sin(angle/2), cos(angle/2))

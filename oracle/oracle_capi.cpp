@@ -25,7 +25,7 @@ struct RPhysWorld {
   std::mutex mu;
   World w;
   uint32_t bodies_created = 0, colliders_created = 0, max_bodies, max_colliders;
-  RPhysTuning tuning{32, 64, 128};
+  RPhysTuning tuning{32, 32, 64};
   RPhysWorld(uint32_t mb, uint32_t mc) : w(mb), max_bodies(mb), max_colliders(mc) {}
 };
 struct RPhysWorldSnapshot { Snapshot s; std::vector<World::Player> players; };  // lib.rs:1696-1702

@@ -137,9 +137,6 @@ RP_HD m3 world_inertia(q4 q, const m3& il) { m3 r = mfrom_quat(q); return mmul(m
 #define RP_PIO2_1 0x1.921fb54400000p+0
 #define RP_PIO2_2 0x1.0b4611a600000p-34
 #define RP_PIO2_3 0x1.3198a2e037073p-69
-#define RP_INV_LN2 0x1.71547652b82fep+0
-#define RP_LN2_HI 0x1.62e42fef00000p-1
-#define RP_LN2_LO 0x1.473de6af278edp-34
 
 RP_HD double rp_sin_poly(double r) {
   double r2 = r * r;
@@ -185,33 +182,47 @@ RP_HD void sincos_rp(float xf, float* s, float* c) {
 // Unit of the learned warm start's impulses: a row's effective mass times 9.81 m/s^2 / 60 Hz (the
 // impulse that holds the row's mass against gravity for one tick), written as one f32 constant.
 constexpr float kImpulseUnit = 0.1635f;
+// exp: x = (32 m + j) ln2/32 + r with |r| <= ln2/64, so e^x = 2^m 2^(j/32) e^r; 2^(j/32) from the
+// table below (each entry the double nearest 2^(j/32), computed with 80-digit decimal arithmetic),
+// e^r - 1 from its Taylor series through r^5 (error below 3e-15), evaluated in double and rounded
+// once to f32. Over every seventh f32 in [-104, 0] it returns the bits of the degree-14 series on
+// |r| <= ln2/2 that it replaced, with a shorter dependent chain (the friction law calls it once per
+// row update).
+#define RP_EXP2_32_TABLE { \
+  0x1.0000000000000p+0, 0x1.059b0d3158574p+0, 0x1.0b5586cf9890fp+0, 0x1.11301d0125b51p+0, \
+  0x1.172b83c7d517bp+0, 0x1.1d4873168b9aap+0, 0x1.2387a6e756238p+0, 0x1.29e9df51fdee1p+0, \
+  0x1.306fe0a31b715p+0, 0x1.371a7373aa9cbp+0, 0x1.3dea64c123422p+0, 0x1.44e086061892dp+0, \
+  0x1.4bfdad5362a27p+0, 0x1.5342b569d4f82p+0, 0x1.5ab07dd485429p+0, 0x1.6247eb03a5585p+0, \
+  0x1.6a09e667f3bcdp+0, 0x1.71f75e8ec5f74p+0, 0x1.7a11473eb0187p+0, 0x1.82589994cce13p+0, \
+  0x1.8ace5422aa0dbp+0, 0x1.93737b0cdc5e5p+0, 0x1.9c49182a3f090p+0, 0x1.a5503b23e255dp+0, \
+  0x1.ae89f995ad3adp+0, 0x1.b7f76f2fb5e47p+0, 0x1.c199bdd85529cp+0, 0x1.cb720dcef9069p+0, \
+  0x1.d5818dcfba487p+0, 0x1.dfc97337b9b5fp+0, 0x1.ea4afa2a490dap+0, 0x1.f50765b6e4540p+0 }
+#ifdef __CUDA_ARCH__
+static __device__ const double rp_exp2_32[32] = RP_EXP2_32_TABLE;
+#else
+static const double rp_exp2_32[32] = RP_EXP2_32_TABLE;
+#endif
+#define RP_32_OVER_LN2 0x1.71547652b82fep+5
+#define RP_LN2_32_HI 0x1.62e42fef00000p-6  // ln2/32 split: k * HI is exact for |k| < 2^20
+#define RP_LN2_32_LO 0x1.473de6af278edp-39
 RP_HD float exp_rp(float xf) {
   double x = (double)xf;
   if (isnan(x)) return NAN;
   if (x > 89.0) return INFINITY;
   if (x < -104.0) return 0.0f;
-  double k = floor(x * RP_INV_LN2 + 0.5);
-  double r = (x - k * RP_LN2_HI) - k * RP_LN2_LO;
-  double p = 1.0 / 87178291200.0;
-  p = p * r + 1.0 / 6227020800.0;
-  p = p * r + 1.0 / 479001600.0;
-  p = p * r + 1.0 / 39916800.0;
-  p = p * r + 1.0 / 3628800.0;
-  p = p * r + 1.0 / 362880.0;
-  p = p * r + 1.0 / 40320.0;
-  p = p * r + 1.0 / 5040.0;
-  p = p * r + 1.0 / 720.0;
-  p = p * r + 1.0 / 120.0;
-  p = p * r + 1.0 / 24.0;
-  p = p * r + 1.0 / 6.0;
-  p = p * r + 0.5;
-  p = p * r + 1.0;
-  p = p * r + 1.0;
-  // p * 2^k is exact (k in [-150, 128] keeps 2^k a normal double): the same value ldexp gives
-  long long eb = (long long)((int)k + 1023) << 52;
-  double two_k;
-  memcpy(&two_k, &eb, 8);
-  return (float)(p * two_k);
+  double k = floor(x * RP_32_OVER_LN2 + 0.5);
+  double r = (x - k * RP_LN2_32_HI) - k * RP_LN2_32_LO;
+  long long ki = (long long)k;
+  int j = (int)(ki & 31), m = (int)((ki - j) / 32);
+  double r2 = r * r;
+  double q = r + (r2 * (0.5 + r * (1.0 / 6.0)) + (r2 * r2) * (1.0 / 24.0 + r * (1.0 / 120.0)));
+  double t = rp_exp2_32[j];
+  double p = t + t * q;
+  // p * 2^m is exact (m in [-150, 128] keeps 2^m a normal double): the value ldexp gives
+  long long eb = (long long)(m + 1023) << 52;
+  double two_m;
+  memcpy(&two_m, &eb, 8);
+  return (float)(p * two_m);
 }
 // atan of a non-negative double: 1/x for x > 1, two half-angle reductions
 // t -> t / (1 + sqrt(1 + t^2)) to |t| <= tan(pi/16), the Taylor series through t^27, times 4.
