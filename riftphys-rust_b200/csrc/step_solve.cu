@@ -1671,9 +1671,17 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
   for (uint32_t i = tid; i < nisl; i += NT) { W.isl_res[i] = 0u; W.isl_last[i] = 0u; W.isl_sw[i] = 0u; W.isl_done[i] = 0; }
   __syncthreads();
   SBodies B{W.lin, W.ang, W.Iw, W.im};
+  // Between two levels of at most 32 rows only the first warp works and a warp barrier orders its
+  // shared-memory writes; a block barrier is taken only where a wider level begins or ends (every
+  // warp takes the same barriers: the condition depends on the level sizes alone).
+  auto wide = [&](uint32_t L) { return L < nl && W.lvl[L + 1] - W.lvl[L] > 32u; };
+  auto level_sync = [&](uint32_t L) {
+    if (NT == 32 || wide(L) || wide(L + 1)) __syncthreads();
+    else __syncwarp();
+  };
   uint32_t n_pred = 0;
   for (uint32_t L = 0; L < nl; ++L) {
-    for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1]; i += NT) {
+    for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1] && (wid == 0 || wide(L)); i += NT) {
       int e = R.wm[base + i];
       float4 p = R.pred[base + i];
       const SRow& r = W.rows[i];
@@ -1684,13 +1692,14 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
                             e >= 0 ? wa[e] : make_float4(0, 0, 0, 0), e >= 0 ? wb[e] : make_float4(0, 0, 0, 0), p,
                             W.jn[i], W.jt[i]);
     }
-    __syncthreads();
+    level_sync(L);
   }
+  __syncthreads();
   if (n_pred) atomicAdd(&stats[STAT_PRED_USED], n_pred);
   int it = 0;
   while (it < iters) {
     for (uint32_t L = 0; L < nl; ++L) {
-      for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1]; i += NT) {
+      for (uint32_t i = W.lvl[L] + tid; i < W.lvl[L + 1] && (wid == 0 || wide(L)); i += NT) {
         const SRow& r = W.rows[i];
         if (MULTI && W.isl_done[r.flags >> 16]) continue;
         if (r.flags & RF_JOINT) {  // a joint is one unit: its first row runs all its rows in order
@@ -1700,8 +1709,9 @@ __global__ void __launch_bounds__(NT) k_vel_solve_onchip(OnchipLayout Lo, uint32
         }
         pgs_row_reg(B, r, i, W.jn, W.jt, W.dres);
       }
-      __syncthreads();
+      level_sync(L);
     }
+    __syncthreads();
     // the sweep's residual per island, off the level chain (non-negative floats: integer max)
     if (!MULTI) {
       uint32_t m = 0;
