@@ -723,10 +723,14 @@ def main():
                  "solve_groups": {"shared_memory": st["groups_shared"], "global_memory": st["groups_global"],
                                   "max_rows": st["max_group_rows"], "max_bodies": st["max_group_bodies"]},
                  "note": "the last timed tick's velocity solve"}
+        rows_total = units["pos_row_sweeps"] / ITERS[args.config]  # rows present, summed over the K ticks
+        rates = {"constraint_rows_per_s": rows_total / (ms / 1000.0), "row_updates_per_s": units["row_sweeps"] / (ms / 1000.0),
+                 "note": "rows present per tick and velocity row updates run, summed over the timed ticks (from the "
+                         "profiled replay of the same ticks) over the timed span"}
         line = {"metric": metric_name(args.config), "value": value, "unit": "body-ticks/s", "n_gpus": world_size,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": run_config(args, desc, world_size), "solve": solve, "parity": parity,
+                "config": run_config(args, desc, world_size), "solve": solve, "rates": rates, "parity": parity,
                 "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "stage_ms": stages,
                 "tuning": dict(w.tuning(), source=tuning_note)}
