@@ -71,6 +71,11 @@ BYTES = {
 
 
 ITERS = {"terrain": 20, "box_drop": 8, "batch": 16, "ragdolls": 24}
+# DRAM bytes the velocity-solve kernels read and write per scheduled row and tick, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum over the vel_solve kernels of 2 timed ticks of the
+# terrain workload at 20,000 bodies: 48.8 MB over 175,676 rows; profiles/vel_solve_dram_terrain20k.md):
+# the one-time staging of rows and bodies into shared memory, which grows with the rows
+TRAFFIC_PER_ROW = {"vel_solve": 278.0}
 
 
 def build_scene(lib, config, n_bodies=None, area=None, hf_n=None, worlds=4096, rank=0, world_size=1):
@@ -542,6 +547,10 @@ def main():
         achieved = bytes_per_launch / (stage_ms / stage_calls / 1000.0) / 1e9
         roof.update({"achieved": achieved, "frac": achieved / peak, "bytes_per_launch": bytes_per_launch,
                      "ms_per_launch": stage_ms / stage_calls})
+    if stage in TRAFFIC_PER_ROW and stage_calls:
+        roof["traffic"] = TRAFFIC_PER_ROW[stage] * (units["pos_row_sweeps"] / ITERS[args.config]) / stage_calls
+        roof["traffic_source"] = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the vel_solve kernels at 20,000 "
+                                  "bodies, scaled by this run's rows (profiles/vel_solve_dram_terrain20k.md)")
     if stage == "vel_solve" and stage_calls:
         # the bound that holds: the serial chain of the deepest island, sweeps x its levels dependent
         # row updates (a level step: one row update plus a block barrier)

@@ -1084,6 +1084,7 @@ static const uint32_t kBigLevels[BIG_BUCKETS] = {2048u, 4096u, 4096u};
 __constant__ uint32_t c_island_rows[ISLAND_BUCKETS] = {128u, 256u, 384u, 512u, 768u, 1152u};
 __constant__ uint32_t c_island_bodies[ISLAND_BUCKETS] = {129u, 257u, 385u, 513u, 769u, 768u};
 static const uint32_t kIslandRows[ISLAND_BUCKETS] = {128u, 256u, 384u, 512u, 768u, 1152u};
+static_assert(ISLAND_BUCKETS + 1 <= WorldGpu::kAux, "a side stream per island bucket and one for the big islands");
 static const uint32_t kIslandBodies[ISLAND_BUCKETS] = {129u, 257u, 385u, 513u, 769u, 768u};
 __global__ void k_group_flags(uint32_t nisl, uint32_t group_rows, const uint32_t* __restrict__ isl_cnt, uint32_t* small_rows,
                               uint32_t* big) {
@@ -2483,17 +2484,48 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           RP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lay_packed_max.bytes));
         smem_attr.fetch_or(1ull << (dev & 63));
       }
-      // single islands (classes 10..15, few blocks, long) run on the side streams, one bucket per
-      // stream, largest first, while the packed groups and the biggest islands run here; no two
-      // groups share a body
+      // Groups share no body, so every class runs concurrently: the big islands (one long block
+      // each) on their own highest-priority side stream, launched first; the single-island buckets
+      // (classes 10..15, few long blocks) one per side stream, largest first; the many short packed
+      // groups on the tick's stream. Side streams fork from the tick's stream and join it after.
       const bool big = ng > g_small;
       auto lst = [&](int c) { return S.cls_list.p + (size_t)c * ng; };
       if (big) {
         RP_CUDA(cudaEventRecord(W.ev_fork_, st));
+        for (int k = 0; k < WorldGpu::kAux; ++k) RP_CUDA(cudaStreamWaitEvent(W.aux_[k], W.ev_fork_, 0));
+        cudaStream_t sg = W.aux_[WorldGpu::kAux - 1];
+        P.begin(PH_VEL_BIG, sg);
+        // big islands: per-row inverse inertias for the staged stream, then one CTA each, per bucket
+        uint32_t nbig = cls_n[20] + cls_n[21] + cls_n[22];
+        if (nbig) {
+          S.big_x.ensure(7 * (size_t)nsched + 7); S.big_j.ensure(nsched + 1);
+          k_big_rows_x<<<nblk(nsched), T, 0, sg>>>(nsched, S.ord_main.p, S.row_isl2.p, S.g_class.p, R, B, SR, S.big_x.p,
+                                                   S.big_j.p); RP_COUNT_LAUNCH(1);
+        }
+        for (int b = BIG_BUCKETS - 1; b >= 0; --b) {
+          uint32_t n = cls_n[20 + b];
+          if (!n) continue;
+          if (b == BIG_BUCKETS - 1)
+            k_vel_solve_big<128><<<n, 128, big_smem<128>(kBigBodies[b], kBigLevels[b]), sg>>>(
+                kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
+                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats,
+                S.row_islid.p, S.isl_final.p);
+          else
+            k_vel_solve_big<64><<<n, 64, big_smem<64>(kBigBodies[b], kBigLevels[b]), sg>>>(
+                kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
+                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats,
+                S.row_islid.p, S.isl_final.p);
+          RP_COUNT_LAUNCH(1);
+        }
+        if (cls_n[2]) {  // islands beyond the big buckets: a warp each over global memory
+          k_vel_solve<<<nblk(cls_n[2] * 32, 128), 128, 0, sg>>>(cls_n[2], nc, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
+                                                                 W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
+                                                                 lst(2), S.row_islid.p, S.isl_final.p); RP_COUNT_LAUNCH(1);
+        }
+        P.end(PH_VEL_BIG, sg);
         int top = -1;  // the largest non-empty bucket, timed as "vel_solve.island"
         for (int b = ISLAND_BUCKETS - 1; b >= 0; --b) {
           cudaStream_t sb = W.aux_[b];
-          RP_CUDA(cudaStreamWaitEvent(sb, W.ev_fork_, 0));
           uint32_t n = cls_n[10 + b];
           if (!n) continue;
           if (top < 0) { top = b; P.begin(PH_VEL_ISLAND, sb); }
@@ -2519,39 +2551,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
         RP_COUNT_LAUNCH(1);
       }
       P.end(PH_VEL_PACKED, st);
-      P.begin(PH_VEL_BIG, st);
-      {
-        // big islands: per-row inverse inertias for the staged stream, then one CTA each, per bucket
-        uint32_t nbig = cls_n[20] + cls_n[21] + cls_n[22];
-        if (nbig) {
-          S.big_x.ensure(7 * (size_t)nsched + 7); S.big_j.ensure(nsched + 1);
-          k_big_rows_x<<<nblk(nsched), T, 0, st>>>(nsched, S.ord_main.p, S.row_isl2.p, S.g_class.p, R, B, SR, S.big_x.p,
-                                                   S.big_j.p); RP_COUNT_LAUNCH(1);
-        }
-        for (int b = BIG_BUCKETS - 1; b >= 0; --b) {
-          uint32_t n = cls_n[20 + b];
-          if (!n) continue;
-          if (b == BIG_BUCKETS - 1)
-            k_vel_solve_big<128><<<n, 128, big_smem<128>(kBigBodies[b], kBigLevels[b]), st>>>(
-                kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
-                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats,
-                S.row_islid.p, S.isl_final.p);
-          else
-            k_vel_solve_big<64><<<n, 64, big_smem<64>(kBigBodies[b], kBigLevels[b]), st>>>(
-                kBigBodies[b], kBigLevels[b], 20u + (uint32_t)b, n, lst(20 + b), S.g_class.p, S.gb_start.p, S.gb_cnt.p,
-                S.gb_list.p, SM, SR, S.big_x.p, S.big_j.p, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats,
-                S.row_islid.p, S.isl_final.p);
-          RP_COUNT_LAUNCH(1);
-        }
-      }
-      if (cls_n[2]) {
-        k_vel_solve<<<nblk(cls_n[2] * 32, 128), 128, 0, st>>>(cls_n[2], nc, SM, R, B, S.acc_jn.p, S.acc_jt.p, S.wm_idx.p,
-                                                               W.warm_a.p, W.warm_b.p, iters, tol, stats, S.g_class.p,
-                                                               lst(2), S.row_islid.p, S.isl_final.p); RP_COUNT_LAUNCH(1);
-      }
-      P.end(PH_VEL_BIG, st);
       if (big) {
-        for (int k = 0; k < ISLAND_BUCKETS; ++k) {
+        for (int k = 0; k < WorldGpu::kAux; ++k) {
           RP_CUDA(cudaEventRecord(W.ev_join_[k], W.aux_[k]));
           RP_CUDA(cudaStreamWaitEvent(st, W.ev_join_[k], 0));
         }

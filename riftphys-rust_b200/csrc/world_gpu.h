@@ -231,7 +231,7 @@ class WorldGpu {
   void get_row_features(std::vector<float>& feats, std::vector<float>& targets);
   void get_row_predictions(std::vector<float>& pred4);
   // side streams the velocity solve forks onto (independent solve groups run concurrently)
-  static constexpr int kAux = 6;
+  static constexpr int kAux = 7;  // one per single-island size bucket, one for the big islands
   cudaStream_t aux_[kAux] = {};
   cudaEvent_t ev_fork_ = nullptr, ev_join_[kAux] = {};
   // per-stage CUDA-event timing (totals since the last reset)
