@@ -239,6 +239,7 @@ struct StepCtx {
   float dt;
   f3 g, up;
   uint32_t np = 0, nc = 0, nisl = 0, nref_isl = 0, nsched = 0;
+  uint32_t g_small = 0;  // solve groups [0, g_small) are packed groups of small islands
   HFView hf{nullptr, 0, 0, 1, 1, 0, 0, 0, 0};
   uint32_t hf_mat = 4;
 };

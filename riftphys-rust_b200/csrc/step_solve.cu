@@ -866,37 +866,35 @@ __global__ void k_pos_anchors(uint32_t nc, RowsV R, const float4* __restrict__ c
   lb[k] = f4(qrot(qconj(asq(orig_rot[b])), xyz(c_pt[k]) - xyz(orig_pos[b])));
 }
 // One projection of contact k (step.rs:457-496).
-__device__ __forceinline__ void project_one(const BodiesV& B, const RowsV& R, uint32_t k, bool shock, f3 up,
-                                            const float4* __restrict__ c_pt, const float4* __restrict__ c_n,
-                                            const float4* __restrict__ lbv, float4* split_l, float4* split_a) {
-  uint2 x = R.ab[k];
-  uint32_t f = R.flags[k];
-  bool hb = !(f & RF_TERRAIN);
-  uint32_t a = x.x, b = x.y;
-  bool am = B.inv_mass[a] > 0.0f && B.awake[a];
-  bool bm = hb && B.inv_mass[b] > 0.0f && B.awake[b];
+// The projection of one contact (step.rs:447-497) on an accessor of the bodies' state: pose, inverse
+// mass and inertia, whether the body moves (dynamic and awake), the split accumulators. The same
+// operations in the same order whatever the accessor, so the global-memory and the shared-memory
+// passes give the same bits.
+template <class Acc>
+__device__ __forceinline__ void project_core(Acc& A, uint32_t a, uint32_t b, bool hb, bool shock, f3 up, f3 n,
+                                             float4 cp, f3 la, f3 lb) {
+  bool am = A.movable(a);
+  bool bm = hb && A.movable(b);
   if (shock && am && bm) {
-    float ha = dot(xyz(B.pos[a]), up), hbb = dot(xyz(B.pos[b]), up);
+    float ha = dot(A.pos(a), up), hbb = dot(A.pos(b), up);
     if (ha < hbb) am = false; else bm = false;
   }
-  f3 n = xyz(c_n[k]);
-  float4 cp = c_pt[k];
   float pen0 = cp.w - 0.05f;
-  f3 pa_pos = xyz(B.pos[a]); q4 pa_rot = asq(B.rot[a]);
-  f3 wa = pa_pos + qrot(pa_rot, xyz(R.la[k]));
+  f3 pa_pos = A.pos(a); q4 pa_rot = A.rot(a);
+  f3 wa = pa_pos + qrot(pa_rot, la);
   f3 pb_pos = mk3(0, 0, 0); q4 pb_rot = qident();
   f3 wb;
-  if (hb) { pb_pos = xyz(B.pos[b]); pb_rot = asq(B.rot[b]); wb = pb_pos + qrot(pb_rot, xyz(lbv[k])); }
+  if (hb) { pb_pos = A.pos(b); pb_rot = A.rot(b); wb = pb_pos + qrot(pb_rot, lb); }
   else wb = xyz(cp);
   float pen = pen0 - dot(wb - wa, n);
   float err = pen - 0.005f;
   if (err <= 0.0f) return;
   f3 ra = wa - pa_pos;
   f3 rb = hb ? wb - pb_pos : mk3(0, 0, 0);
-  float ima = am ? B.inv_mass[a] : 0.0f;
-  m3 iia = am ? world_inertia(pa_rot, ld_m3(B.inv_I, a)) : mzero();
-  float imb = (hb && bm) ? B.inv_mass[b] : 0.0f;
-  m3 iib = (hb && bm) ? world_inertia(pb_rot, ld_m3(B.inv_I, b)) : mzero();
+  float ima = am ? A.inv_mass(a) : 0.0f;
+  m3 iia = am ? world_inertia(pa_rot, A.inv_I(a)) : mzero();
+  float imb = (hb && bm) ? A.inv_mass(b) : 0.0f;
+  m3 iib = (hb && bm) ? world_inertia(pb_rot, A.inv_I(b)) : mzero();
   f3 ca = cross(ra, n), cb = cross(rb, n);
   float w = ((ima + imb) + dot(ca, mvec(iia, ca))) + dot(cb, mvec(iib, cb));
   if (w <= 1.0e-9f) return;
@@ -904,19 +902,167 @@ __device__ __forceinline__ void project_one(const BodiesV& B, const RowsV& R, ui
   // move_body (step.rs:484-491)
   auto move_body = [&](uint32_t id, f3 ppos, q4 prot, float im, const m3& ii, f3 r, f3 j) {
     f3 dth = mvec(ii, cross(r, j));
-    float4 sl = split_l[id], sa = split_a[id];
-    split_l[id] = f4(xyz(sl) + j * im);
-    split_a[id] = f4(xyz(sa) + dth);
+    A.split_add(id, j * im, dth);
     q4 dq = qscale(qmul(mkq(dth.x, dth.y, dth.z, 0.0f), prot), 0.5f);
     q4 nr = qnormalize(mkq(prot.x + dq.x, prot.y + dq.y, prot.z + dq.z, prot.w + dq.w));
     f3 np = ppos + j * im;
-    float4 P = B.pos[id];
-    if (vfin(np)) B.pos[id] = f4(fin_v(np), P.w);
-    if (qfin(nr)) B.rot[id] = f4q(fin_q(nr));
+    if (vfin(np)) A.set_pos(id, fin_v(np));
+    if (qfin(nr)) A.set_rot(id, fin_q(nr));
   };
   if (am) move_body(a, pa_pos, pa_rot, ima, iia, ra, (-n) * lambda);
   if (hb && bm) move_body(b, pb_pos, pb_rot, imb, iib, rb, n * lambda);
 }
+// Body state in global memory (bodies by their world index).
+struct PosAccGlobal {
+  const BodiesV& B;
+  float4* split_l;
+  float4* split_a;
+  __device__ bool movable(uint32_t i) const { return B.inv_mass[i] > 0.0f && B.awake[i]; }
+  __device__ f3 pos(uint32_t i) const { return xyz(B.pos[i]); }
+  __device__ q4 rot(uint32_t i) const { return asq(B.rot[i]); }
+  __device__ float inv_mass(uint32_t i) const { return B.inv_mass[i]; }
+  __device__ m3 inv_I(uint32_t i) const { return ld_m3(B.inv_I, i); }
+  __device__ void split_add(uint32_t i, f3 dl, f3 da) {
+    float4 sl = split_l[i], sa = split_a[i];
+    split_l[i] = f4(xyz(sl) + dl);
+    split_a[i] = f4(xyz(sa) + da);
+  }
+  __device__ void set_pos(uint32_t i, f3 p) { float4 P = B.pos[i]; B.pos[i] = f4(p, P.w); }
+  __device__ void set_rot(uint32_t i, q4 q) { B.rot[i] = f4q(q); }
+};
+__device__ __forceinline__ void project_one(const BodiesV& B, const RowsV& R, uint32_t k, bool shock, f3 up,
+                                            const float4* __restrict__ c_pt, const float4* __restrict__ c_n,
+                                            const float4* __restrict__ lbv, float4* split_l, float4* split_a) {
+  uint2 x = R.ab[k];
+  uint32_t f = R.flags[k];
+  bool hb = !(f & RF_TERRAIN);
+  PosAccGlobal A{B, split_l, split_a};
+  project_core(A, x.x, x.y, hb, shock, up, xyz(c_n[k]), c_pt[k], xyz(R.la[k]), hb ? xyz(lbv[k]) : mk3(0, 0, 0));
+}
+// ---- the position pass with its groups on chip (worlds without joints): a block per solve group
+// (the packed groups and the single islands the velocity solve keeps on chip) holds its bodies'
+// poses, inverse masses and inertias and split accumulators in shared memory, and its rows' body
+// indices, anchors, normals and contact points, for all the iterations; bodies a row reads but
+// cannot move (static, asleep, or the terrain) are read from global memory, which nothing writes
+// during the pass. Same projections, same order (project_core), so the same bits as
+// k_pos_iterations.
+struct PosLayout {
+  uint32_t RC, BC;
+  uint32_t o_pos, o_rot, o_sl, o_sa, o_iI, o_im, o_mov, o_ab, o_la, o_lb, o_n, o_cp, o_lvl, bytes;
+};
+__host__ __device__ inline PosLayout pos_layout(uint32_t RC, uint32_t BC) {
+  PosLayout L;
+  L.RC = RC; L.BC = BC;
+  uint32_t o = 0;
+  auto take = [&](uint32_t bytes) { uint32_t a = o; o = (o + bytes + 15u) & ~15u; return a; };
+  L.o_pos = take(16u * BC); L.o_rot = take(16u * BC); L.o_sl = take(16u * BC); L.o_sa = take(16u * BC);
+  L.o_iI = take(36u * BC); L.o_im = take(4u * BC); L.o_mov = take(BC);
+  L.o_ab = take(8u * RC); L.o_la = take(16u * RC); L.o_lb = take(16u * RC); L.o_n = take(16u * RC); L.o_cp = take(16u * RC);
+  L.o_lvl = take(4u * (RC + 1u));
+  L.bytes = o;
+  return L;
+}
+// A body index of a row: its index in the group, or 0x80000000 | its world index when the row
+// only reads it.
+struct PosAccShared {
+  float4 *s_pos, *s_rot, *s_sl, *s_sa;
+  const float* s_iI;
+  const float* s_im;
+  const uint8_t* s_mov;
+  const BodiesV& G;
+  __device__ static bool local(uint32_t i) { return !(i & 0x80000000u); }
+  __device__ bool movable(uint32_t i) const {
+    const uint32_t g = i & 0x7FFFFFFFu;
+    return local(i) ? s_mov[i] != 0 : (G.inv_mass[g] > 0.0f && G.awake[g]);
+  }
+  __device__ f3 pos(uint32_t i) const { return local(i) ? xyz(s_pos[i]) : xyz(G.pos[i & 0x7FFFFFFFu]); }
+  __device__ q4 rot(uint32_t i) const { return local(i) ? asq(s_rot[i]) : asq(G.rot[i & 0x7FFFFFFFu]); }
+  __device__ float inv_mass(uint32_t i) const { return local(i) ? s_im[i] : G.inv_mass[i & 0x7FFFFFFFu]; }
+  __device__ m3 inv_I(uint32_t i) const { return local(i) ? ld_m3(s_iI, i) : ld_m3(G.inv_I, i & 0x7FFFFFFFu); }
+  __device__ void split_add(uint32_t i, f3 dl, f3 da) {  // only a body the group moves
+    s_sl[i] = f4(xyz(s_sl[i]) + dl);
+    s_sa[i] = f4(xyz(s_sa[i]) + da);
+  }
+  __device__ void set_pos(uint32_t i, f3 p) { s_pos[i] = f4(p, s_pos[i].w); }
+  __device__ void set_rot(uint32_t i, q4 q) { s_rot[i] = f4q(q); }
+};
+template <int NT>
+__global__ void __launch_bounds__(NT) k_pos_onchip(PosLayout Lo, uint32_t n_listed, const uint32_t* __restrict__ glist,
+                                                   uint32_t want_class, const uint32_t* __restrict__ g_class,
+                                                   const uint32_t* __restrict__ gb_start, const uint32_t* __restrict__ gb_cnt,
+                                                   const uint32_t* __restrict__ gb_list, const uint32_t* __restrict__ body_grp,
+                                                   const uint32_t* __restrict__ body_local, Sched S, RowsV R, BodiesV G,
+                                                   int iters, f3 up, const float4* __restrict__ c_pt,
+                                                   const float4* __restrict__ c_n, const float4* __restrict__ lbv,
+                                                   float4* split_l, float4* split_a, uint32_t* stats) {
+  if (glist && blockIdx.x >= n_listed) return;
+  const uint32_t g = glist ? glist[blockIdx.x] : blockIdx.x;
+  if (!glist && g >= n_listed) return;
+  if (g_class[g] != want_class) return;
+  extern __shared__ float4 pos_raw[];
+  unsigned char* sb = reinterpret_cast<unsigned char*>(pos_raw);
+  float4* pos = reinterpret_cast<float4*>(sb + Lo.o_pos);
+  float4* rot = reinterpret_cast<float4*>(sb + Lo.o_rot);
+  float4* sl = reinterpret_cast<float4*>(sb + Lo.o_sl);
+  float4* sa = reinterpret_cast<float4*>(sb + Lo.o_sa);
+  float* iI = reinterpret_cast<float*>(sb + Lo.o_iI);
+  float* im = reinterpret_cast<float*>(sb + Lo.o_im);
+  uint8_t* mov = sb + Lo.o_mov;
+  uint2* ab = reinterpret_cast<uint2*>(sb + Lo.o_ab);
+  float4* la = reinterpret_cast<float4*>(sb + Lo.o_la);
+  float4* lb = reinterpret_cast<float4*>(sb + Lo.o_lb);
+  float4* nn = reinterpret_cast<float4*>(sb + Lo.o_n);
+  float4* cp = reinterpret_cast<float4*>(sb + Lo.o_cp);
+  uint32_t* lvl = reinterpret_cast<uint32_t*>(sb + Lo.o_lvl);
+  const uint32_t tid = threadIdx.x, wid = tid >> 5;
+  const uint32_t nbg = gb_cnt[g], b0 = gb_start[g];
+  const uint32_t off = S.lvl_off[g], nl = S.nlev[g];
+  const uint32_t base = S.lvl_start[off], nr = S.lvl_start[off + nl] - base;
+  if (nbg > Lo.BC || nr > Lo.RC || nl > Lo.RC) {  // not reached: the class was chosen by these sizes
+    if (tid == 0) atomicOr(&stats[STAT_ERR], 2u);
+    return;
+  }
+  for (uint32_t i = tid; i < nbg; i += NT) {
+    const uint32_t b = gb_list[b0 + i];
+    pos[i] = G.pos[b]; rot[i] = G.rot[b]; sl[i] = split_l[b]; sa[i] = split_a[b];
+    for (int k = 0; k < 9; ++k) iI[9 * i + k] = G.inv_I[9 * (size_t)b + k];
+    im[i] = G.inv_mass[b];
+    mov[i] = (G.inv_mass[b] > 0.0f && G.awake[b]) ? 1 : 0;
+  }
+  for (uint32_t i = tid; i < nr; i += NT) {
+    const uint32_t k = S.ord[base + i];
+    const uint2 x = R.ab[k];
+    const bool hb = !(R.flags[k] & RF_TERRAIN);
+    const uint32_t a = body_grp[x.x] == g ? body_local[x.x] : (0x80000000u | x.x);
+    const uint32_t b = !hb ? 0xFFFFFFFFu : (body_grp[x.y] == g ? body_local[x.y] : (0x80000000u | x.y));
+    ab[i] = make_uint2(a, b);
+    la[i] = R.la[k];
+    lb[i] = hb ? lbv[k] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    nn[i] = c_n[k];
+    cp[i] = c_pt[k];
+  }
+  for (uint32_t L = tid; L <= nl; L += NT) lvl[L] = S.lvl_start[off + L] - base;
+  __syncthreads();
+  PosAccShared A{pos, rot, sl, sa, iI, im, mov, G};
+  auto wide = [&](uint32_t L) { return L < nl && lvl[L + 1] - lvl[L] > 32u; };
+  for (int it = 0; it < iters; ++it) {
+    for (uint32_t L = 0; L < nl; ++L) {
+      for (uint32_t i = lvl[L] + tid; i < lvl[L + 1] && (wid == 0 || wide(L)); i += NT) {
+        const uint2 x = ab[i];
+        const bool hb = x.y != 0xFFFFFFFFu;
+        project_core(A, x.x, x.y, hb, false, up, xyz(nn[i]), cp[i], xyz(la[i]), xyz(lb[i]));
+      }
+      if (NT == 32 || wide(L) || wide(L + 1)) __syncthreads();
+      else __syncwarp();
+    }
+    __syncthreads();
+  }
+  for (uint32_t i = tid; i < nbg; i += NT) {
+    const uint32_t b = gb_list[b0 + i];
+    G.pos[b] = pos[i]; G.rot[b] = rot[i]; split_l[b] = sl[i]; split_a[b] = sa[i];
+  }
+}
+
 // Position sweeps (step.rs:301-308): each joint's solve (bodies.rs:422-471, SHAKE directions from the
 // step's start poses spos / srot) rides on its first velocity row, which the schedule places before
 // every later row touching its bodies -- the reference's joints-then-contacts order; joints between
@@ -2361,6 +2507,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       k_local_isl<<<nblk(nsched), T, 0, st>>>(nsched, S.tmp32.p, S.g_key2.p, S.g_start.p, S.g_cnt.p, S.li_flag.p, S.li_pre.p,
                                               S.row_lisl.p, S.g_nisl.p); RP_COUNT_LAUNCH(1);
       ctx.nisl = ng;
+      ctx.g_small = g_small;
       // ---- main schedule (row order within each group)
       S.lvl_hist.ensure(nsched + 1);
       RP_CUDA(cudaMemsetAsync(S.lvl_hist.p, 0, sizeof(uint32_t) * (nsched + 1), st));
@@ -2680,8 +2827,55 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       pos_launch(std::integral_constant<int, 4>{}, cls_n[10], S.cls_list.p + 10 * (size_t)ngr, 0u);
       pos_launch(std::integral_constant<int, 8>{}, cls_n[11], S.cls_list.p + 11 * (size_t)ngr, 0u);
       pos_launch(std::integral_constant<int, 32>{}, ngr, nullptr, (1u << 10) | (1u << 11));
-    } else {
-      pos_launch(std::integral_constant<int, 32>{}, ngr, nullptr, 0u);
+    } else if (ngr) {
+      // no joints: the groups the velocity solve keeps on chip run the pass on chip as well (the
+      // single-island buckets on the side streams, the packed groups here); the big and
+      // global-memory islands keep the warp kernel, on the big islands' side stream
+      static std::atomic<unsigned long long> pos_attr{0};
+      int dev = 0;
+      RP_CUDA(cudaGetDevice(&dev));
+      const PosLayout top = pos_layout(kIslandRows[ISLAND_BUCKETS - 1], kIslandBodies[ISLAND_BUCKETS - 1]);
+      if (!((pos_attr.load() >> (dev & 63)) & 1ull)) {
+        for (auto f : {k_pos_onchip<32>, k_pos_onchip<64>, k_pos_onchip<128>, k_pos_onchip<256>})
+          RP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)top.bytes));
+        pos_attr.fetch_or(1ull << (dev & 63));
+      }
+      auto onchip = [&](uint32_t threads) {
+        return threads == 32 ? k_pos_onchip<32> : threads == 64 ? k_pos_onchip<64>
+             : threads == 128 ? k_pos_onchip<128> : k_pos_onchip<256>;
+      };
+      const uint32_t g_small = ctx.g_small;
+      RP_CUDA(cudaEventRecord(W.ev_fork_, st));
+      for (int k = 0; k < WorldGpu::kAux; ++k) RP_CUDA(cudaStreamWaitEvent(W.aux_[k], W.ev_fork_, 0));
+      {
+        cudaStream_t sg = W.aux_[WorldGpu::kAux - 1];
+        const uint32_t skip = (1u << 3) | (0x3Fu << 10);  // classes run on chip
+        const uint32_t warps = ngr;
+        k_pos_iterations<32><<<nblk(warps * 32, 128), 128, 0, sg>>>(
+            ngr, nullptr, skip, S.g_class.p, nc, SPP, R, B, (int)W.iters_p_, 0, ctx.up, S.c_pt.p, S.c_n.p, S.pc_lb.p,
+            S.split_l.p, S.split_a.p, W.joints_d.p, W.jlam.p, S.orig_pos.p, S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
+      }
+      for (int b = ISLAND_BUCKETS - 1; b >= 0; --b) {
+        const uint32_t n = cls_n[10 + b];
+        if (!n) continue;
+        const PosLayout lay = pos_layout(kIslandRows[b], kIslandBodies[b]);
+        onchip(W.tuning_.island_threads)<<<n, W.tuning_.island_threads, lay.bytes, W.aux_[b]>>>(
+            lay, n, S.cls_list.p + (size_t)(10 + b) * ngr, 10u + (uint32_t)b, S.g_class.p, S.gb_start.p, S.gb_cnt.p,
+            S.gb_list.p, S.body_grp.p, S.body_local.p, SPP, R, B, (int)W.iters_p_, ctx.up, S.c_pt.p, S.c_n.p, S.pc_lb.p,
+            S.split_l.p, S.split_a.p, stats); RP_COUNT_LAUNCH(1);
+      }
+      if (g_small) {
+        const uint32_t gr = W.tuning_.group_rows;
+        const PosLayout lay = pos_layout(WG_ROWS(gr), WG_BODIES(gr));
+        onchip(W.tuning_.packed_threads)<<<g_small, W.tuning_.packed_threads, lay.bytes, st>>>(
+            lay, g_small, nullptr, 3u, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p, S.body_grp.p, S.body_local.p,
+            SPP, R, B, (int)W.iters_p_, ctx.up, S.c_pt.p, S.c_n.p, S.pc_lb.p, S.split_l.p, S.split_a.p, stats);
+        RP_COUNT_LAUNCH(1);
+      }
+      for (int k = 0; k < WorldGpu::kAux; ++k) {
+        RP_CUDA(cudaEventRecord(W.ev_join_[k], W.aux_[k]));
+        RP_CUDA(cudaStreamWaitEvent(st, W.ev_join_[k], 0));
+      }
     }
     P.end(PH_POS_ITER, st);
     P.begin(PH_POS_SHOCK, st);
