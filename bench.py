@@ -347,7 +347,9 @@ def batched_record(lib, torch, n_worlds, settle=30, ticks=10, every=32):
     torch.cuda.synchronize()
     bms = e0.elapsed_time(e1)
     sb = b.stats()
+    t0 = time.perf_counter()
     h_first = b.world_hashes()
+    hash_ms = (time.perf_counter() - t0) * 1000.0
     b.restore_exact(snap)
     b.step_n(dt, ticks)
     rollback_ok = b.world_hashes() == h_first
@@ -377,7 +379,10 @@ def batched_record(lib, torch, n_worlds, settle=30, ticks=10, every=32):
                       "s_per_tick_all_sampled_worlds": plain_s / ticks,
                       "note": "one RPhysWorld per world stepped through rphys_ext_step_n, host-timed"},
             "batched_over_plain": batched_v / plain_v,
-            "rollback_window": {"ticks": ticks, "hashes_match": rollback_ok}}
+            "rollback_window": {"ticks": ticks, "hashes_match": rollback_ok,
+                                "all_world_hashes_ms": hash_ms,
+                                "note": "every world's tick hash in one rphys_ext_batch_get_hashes call (kernels over the "
+                                        "world table), host-timed"}}
 
 
 def metric_name(config):
