@@ -78,18 +78,24 @@ def test_trained_model_against_previous_tick_warm_start(gpu):
         w.restore_exact(snap)
         w.set_warm_model(m if mode == "learned" else None)
         w.set_warm_policy(True)
-        tot = used = 0
+        tot = used = conv = 0
         for _ in range(40):
             w.step(dt)
             st = w.stats()
             tot += st["row_sweeps"]
             used += st["pred_used"]
-        sweeps[mode] = (tot, used)
+            conv += st["row_sweeps"] - 80 * st["rows_capped"]  # updates of the islands that converged
+        sweeps[mode] = (tot, used, conv)
     w.set_warm_model(None)
     w.free_snapshot(snap)
     gain = 1.0 - sweeps["learned"][0] / sweeps["previous-tick"][0]
-    print(f"row updates over 40 ticks: {sweeps}; gain {100 * gain:.2f}%")
+    gain_conv = 1.0 - sweeps["learned"][2] / max(1, sweeps["previous-tick"][2])
+    print(f"row updates over 40 ticks (total, from prediction, in converged islands): {sweeps}; gain {100 * gain:.2f}% "
+          f"overall, {100 * gain_conv:.2f}% in the islands that converge")
     assert sweeps["learned"][1] > 0
-    # the per-row fallback keeps a prediction only where it starts the row better; the measured gain
-    # on this workload is about +0.5%, so the check is that it costs no more than 2%
+    # What the trained network gains, measured: nothing that matters. About +0.5% fewer row updates
+    # on this scene; on the 100k-body bench state +0.2% with this policy. The sweeps go to islands
+    # whose contact sets are infeasible and run to the cap whatever their start. In the islands that
+    # converge, the previous tick's impulse is already a close start. The per-row fallback keeps a
+    # prediction only where it starts the row better, so the check is that it costs no more than 2%.
     assert gain > -0.02, sweeps
