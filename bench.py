@@ -508,20 +508,21 @@ def main():
 
     # e2e: the drop-in C-ABI call with the tick's state read back to host memory every tick
     import numpy as np
-    host = np.empty((nb, 13), dtype=np.float32)
+    host = torch.empty((nb, 13), dtype=torch.float32, pin_memory=True)  # page-locked: the fast D2H path
     e2e_ticks = args.steps
-    w.restore(snap)
+    w.restore_exact(snap)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_ticks):
         w.step(dt)
-        w.c("rphys_ext_get_body_states", 0, nb, host.ctypes.data_as(ctypes.c_void_p))
+        w.c("rphys_ext_get_body_states", 0, nb, ctypes.c_void_p(host.data_ptr()))
     e2e_s = time.perf_counter() - t0
     e2e = {"value": nb * e2e_ticks / e2e_s, "unit": "body-ticks/s", "h2d_bytes_per_step": 20,
            "d2h_bytes_per_step": 52 * nb,
            "note": "each tick one rphys_world_step_ex call whose input is its 20-byte RPhysStepParams (the world "
                    "state lives in the library between calls, as behind the reference's FFI), then "
-                   "rphys_ext_get_body_states reads every body's pos, rot, lin, ang (52 B) back to host memory"}
+                   "rphys_ext_get_body_states reads every body's pos, rot, lin, ang (52 B) back into pinned host "
+                   "memory"}
 
     # roofline: the stage with the most device time, in a separate profiled pass
     w.restore(snap)
