@@ -269,7 +269,7 @@ def run_reference(args):
         return
     args.mode = args.mode or "residual"
     lib = rp.Lib(oracle_path())
-    threads = os.cpu_count() or 1
+    threads = args.cpu_threads or os.cpu_count() or 1
     w, dt, nb, desc = oracle_world(lib, args, threads)
     t0 = time.perf_counter()
     w.step_n(dt, args.settle + args.warmup)
@@ -320,14 +320,16 @@ def cpu_sample_from_state(olib, args, blob, gpu_world, dt, ticks, threads):
     return nb * ticks / el, sample, same
 
 
-def batched_record(lib, torch, n_worlds, settle=30, ticks=10, every=32):
+def batched_record(lib, torch, n_worlds, settle=30, ticks=10, every=32, cpu_every=128, cpu_threads=1):
     """The batched-worlds workload (n_worlds worlds of 16-4096 boxes, residual <= 1e-4 or 64 sweeps)
     stepped as one device batch, against the plain path -- each world its own RPhysWorld stepped by
     its own calls, as the reference steps one World per call -- on every `every`-th world (the worlds'
     sizes are independent draws, so the sample has the table's size distribution). Both from tick 0:
     `settle` ticks untimed, then `ticks` timed; the batch on the device clock, the plain worlds on the
     host clock around each world's completed ticks (its launches and waits are its cost). Plus the
-    8-tick rollback window of the batch: restore, re-simulate, every world's hash compared."""
+    8-tick rollback window of the batch: restore, re-simulate, every world's hash compared. Plus the
+    CPU restatement on every `cpu_every`-th world, stepped the same ticks (host-timed over the timed
+    ticks) with each world's final hash compared with the batch's hash of that world."""
     tol, cap = TOL, 4 * ITERS["batch"]
     descs = [scenes.batch_world_descs(rp, k, seed=3) for k in range(n_worlds)]
     total = sum(len(d) for d in descs)
@@ -368,6 +370,23 @@ def batched_record(lib, torch, n_worlds, settle=30, ticks=10, every=32):
         plain_s += time.perf_counter() - t0
         plain_bodies += len(d)
         w.close()
+    cpu_s, cpu_bodies, cpu_same, cpu_sample = 0.0, 0, True, list(range(0, n_worlds, cpu_every))
+    olib = rp.Lib(oracle_path())
+    olib.dll.rphys_oracle_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    for k in cpu_sample:
+        d = descs[k]
+        o = olib.world(len(d), len(d))
+        scenes.batch_setup(o)
+        o.add_bodies_array(d)
+        o.set_residual_mode(tol, cap)
+        olib.dll.rphys_oracle_set_threads(o.h, cpu_threads)
+        o.step_n(dt, settle)
+        t0 = time.perf_counter()
+        o.step_n(dt, ticks)
+        cpu_s += time.perf_counter() - t0
+        cpu_bodies += len(d)
+        cpu_same = cpu_same and o.hash() == h_first[k]
+        o.close()
     batched_v = total * ticks / (bms / 1000.0)
     plain_v = plain_bodies * ticks / plain_s
     return {"workload": f"{n_worlds} worlds, {total:,} boxes, ticks {settle + 1}-{settle + ticks} from rest, residual "
@@ -379,6 +398,10 @@ def batched_record(lib, torch, n_worlds, settle=30, ticks=10, every=32):
                       "s_per_tick_all_sampled_worlds": plain_s / ticks,
                       "note": "one RPhysWorld per world stepped through rphys_ext_step_n, host-timed"},
             "batched_over_plain": batched_v / plain_v,
+            "cpu": {"value": cpu_bodies * ticks / cpu_s, "unit": "body-ticks/s", "cores": cpu_threads, "kind": "port",
+                    "worlds": len(cpu_sample), "bodies": cpu_bodies, "hashes_match_batch": cpu_same,
+                    "note": f"the CPU restatement stepping every {cpu_every}th world alone, host-timed over the "
+                            f"timed ticks; each world's hash after them compared with the batch's"},
             "rollback_window": {"ticks": ticks, "hashes_match": rollback_ok,
                                 "all_world_hashes_ms": hash_ms,
                                 "note": "every world's tick hash in one rphys_ext_batch_get_hashes call (kernels over the "
@@ -419,6 +442,7 @@ def main():
                          "for n bodies is 400 * sqrt(n / 100000))")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-ticks", type=int, default=3, help="ticks of the CPU sample (and of the parity check)")
+    ap.add_argument("--cpu-threads", type=int, default=0, help="threads of the CPU restatement (0: all host threads)")
     ap.add_argument("--coloured", type=int, default=1, help="also replay the timed ticks in coloured order (1/0)")
     ap.add_argument("--autotune", type=int, default=0, help="time every velocity-solve launch shape first (1/0)")
     ap.add_argument("--batched", type=int, default=1,
@@ -574,10 +598,15 @@ def main():
         # the CPU restatement on the benchmark's own state: timed (cpu_baseline), and every tick's
         # hash and the final body state compared with the GPU's replay of the same ticks (parity)
         olib = rp.Lib(oracle_path())
-        threads = os.cpu_count() or 1
+        threads = args.cpu_threads or os.cpu_count() or 1
         w.restore_exact(snap)
         v, sample, same = cpu_sample_from_state(olib, args, blob, w, dt, args.cpu_ticks, threads)
         cpu = {"value": v, "unit": "body-ticks/s", "cores": threads, "kind": "port", "sample": sample}
+        if threads > 1:
+            # the first of those ticks again on one thread (the reference's single-core figure)
+            w.restore_exact(snap)
+            v1, _, same1 = cpu_sample_from_state(olib, args, blob, w, dt, 1, 1)
+            cpu["one_thread"] = {"value": v1, "ticks": 1, "same_bits": bool(same1)}
         parity = {"bit_exact": bool(same), "ticks": args.cpu_ticks,
                   "checked": "tick hash every tick and all body states after the last, GPU vs CPU restatement "
                              "from the same state"}
@@ -694,7 +723,7 @@ def main():
     # device and copied to the host, as a server does every tick; host-timed over a few calls
     batched = None
     if args.config == "terrain" and args.batched and rank == 0 and world_size == 1:
-        batched = batched_record(lib, torch, args.batched_worlds)
+        batched = batched_record(lib, torch, args.batched_worlds, cpu_threads=args.cpu_threads or os.cpu_count() or 1)
 
     wire = None
     if args.config == "terrain":

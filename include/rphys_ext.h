@@ -75,7 +75,7 @@ RPhysResult rphys_ext_set_solve_order(RPhysWorld* world, uint32_t order);
 
 /* Launch shapes of the velocity solve (an extension; no reference counterpart). None changes a
  * result bit: islands are independent, and so are the rows of one level or colour. group_rows:
- * islands of at most this many rows are packed into shared solve groups (8, 16 or 32); packed_threads:
+ * islands of at most this many rows are packed into shared solve groups (8, 16, 32, 64 or 128); packed_threads:
  * threads of a packed group's block (32, 64 or 128); island_threads: threads of a single island's
  * block (32, 64, 128 or 256). Defaults are the autotuner's choice for the terrain workload (bench.py
  * --autotune, recorded in riftphys-rust_b200/tuning.json). Other values give RPHYS_ERR_BAD_ARG. The

@@ -25,7 +25,7 @@ struct RPhysWorld {
   std::mutex mu;
   World w;
   uint32_t bodies_created = 0, colliders_created = 0, max_bodies, max_colliders;
-  RPhysTuning tuning{32, 32, 64};
+  RPhysTuning tuning{64, 32, 128};
   RPhysWorld(uint32_t mb, uint32_t mc) : w(mb), max_bodies(mb), max_colliders(mc) {}
 };
 struct RPhysWorldSnapshot { Snapshot s; std::vector<World::Player> players; };  // lib.rs:1696-1702
@@ -860,7 +860,7 @@ RPhysResult rphys_ext_set_tuning(RPhysWorld* W, const RPhysTuning* t) {
   clear_err();
   if (!W || !t) return fail(RPHYS_ERR_NULL, "rphys_ext_set_tuning: null arg");
   auto in = [](uint32_t v, uint32_t a, uint32_t b, uint32_t c) { return v == a || v == b || v == c; };
-  if (!(in(t->group_rows, 8, 16, 32) && in(t->packed_threads, 32, 64, 128) &&
+  if (!((in(t->group_rows, 8, 16, 32) || in(t->group_rows, 64, 128, 128)) && in(t->packed_threads, 32, 64, 128) &&
         (t->island_threads == 32 || in(t->island_threads, 64, 128, 256))))
     return fail(RPHYS_ERR_BAD_ARG, "rphys_ext_set_tuning: unsupported launch shape");
   std::lock_guard<std::mutex> g(W->mu);

@@ -9,7 +9,7 @@ import itertools
 import json
 import os
 
-GRID = {"group_rows": (8, 16, 32), "packed_threads": (32, 64, 128), "island_threads": (32, 64, 128, 256)}
+GRID = {"group_rows": (8, 16, 32, 64, 128), "packed_threads": (32, 64, 128), "island_threads": (32, 64, 128, 256)}
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning.json")
 
 

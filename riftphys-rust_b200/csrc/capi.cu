@@ -1026,7 +1026,7 @@ RPhysResult rphys_ext_set_solve_order(RPhysWorld* W, uint32_t order) {
 }
 static bool tuning_ok(const RPhysTuning& t) {
   auto in = [](uint32_t v, uint32_t a, uint32_t b, uint32_t c) { return v == a || v == b || v == c; };
-  return in(t.group_rows, 8, 16, 32) && in(t.packed_threads, 32, 64, 128) &&
+  return (in(t.group_rows, 8, 16, 32) || in(t.group_rows, 64, 128, 128)) && in(t.packed_threads, 32, 64, 128) &&
          (t.island_threads == 32 || in(t.island_threads, 64, 128, 256));
 }
 RPhysResult rphys_ext_set_tuning(RPhysWorld* W, const RPhysTuning* t) {

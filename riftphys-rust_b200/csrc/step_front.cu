@@ -290,13 +290,13 @@ __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* a, uint32_t 
   while (lo < hi) { uint32_t mid = (lo + hi) >> 1; if (a[mid] <= v) lo = mid + 1; else hi = mid; }
   return lo;
 }
-template <bool EMIT>
+// Each item's points go to its 8 fixed slots (2 triangles x at most 4 points), its count to cnt;
+// k_terrain_gather then packs them in item order, so the triangle tests run once.
 __global__ void k_terrain_items(uint32_t nitems, int ncol, HFView hf, const uint32_t* __restrict__ cell_off,
                                 const int4* __restrict__ win, const uint32_t* __restrict__ cbody,
                                 const uint32_t* __restrict__ ckind, const float4* __restrict__ cdims,
                                 const float4* __restrict__ pos, const float4* __restrict__ rot,
-                                const float* __restrict__ sweep, uint32_t* cnt, const uint32_t* __restrict__ cand_off,
-                                float4* cand_p, float4* cand_n) {
+                                const float* __restrict__ sweep, uint32_t* cnt, float4* slot_p, float4* slot_n) {
   uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
   if (it >= nitems) return;
   uint32_t ci = upper_bound_u32(cell_off, (uint32_t)ncol, it) - 1;  // cell_off: exclusive scan of cell counts
@@ -309,20 +309,30 @@ __global__ void k_terrain_items(uint32_t nitems, int ncol, HFView hf, const uint
   Shape sh; sh.kind = ckind[ci]; sh.a = d.x; sh.b = d.y; sh.c = d.z;
   Iso x; x.pos = xyz(pos[b]); x.rot = asq(rot[b]);
   float cd = sweep[ci];
-  uint32_t n = 0, o = EMIT ? cand_off[it] : 0;
+  uint32_t n = 0;
+  const size_t o = 8 * (size_t)it;
   for (int tri = 0; tri < 2; ++tri) {
     Tri t = hf_tri(hf, gx, gz, tri);
     Manifold m;
     if (!collide_tri(sh, x, t, cd, &m)) continue;
     for (int k = 0; k < m.len; ++k) {
-      if (EMIT) {
-        cand_p[o + n] = f4(m.pts[k].position, (m.pts[k].penetration - cd) + 0.05f);
-        cand_n[o + n] = f4(m.pts[k].normal);
-      }
+      slot_p[o + n] = f4(m.pts[k].position, (m.pts[k].penetration - cd) + 0.05f);
+      slot_n[o + n] = f4(m.pts[k].normal);
       n++;
     }
   }
-  if (!EMIT) cnt[it] = n;
+  cnt[it] = n;
+}
+__global__ void k_terrain_gather(uint32_t nitems, const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ cand_off,
+                                 const float4* __restrict__ slot_p, const float4* __restrict__ slot_n, float4* cand_p,
+                                 float4* cand_n) {
+  uint32_t it = blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= nitems) return;
+  const uint32_t n = cnt[it], o = cand_off[it];
+  for (uint32_t k = 0; k < n; ++k) {
+    cand_p[o + k] = slot_p[8 * (size_t)it + k];
+    cand_n[o + k] = slot_n[8 * (size_t)it + k];
+  }
 }
 __global__ void k_terrain_cull(int ncol, const uint32_t* __restrict__ ckind, const uint32_t* __restrict__ cell_off,
                                const uint32_t* __restrict__ ncell, const uint32_t* __restrict__ cand_off, uint32_t nitems,
@@ -547,17 +557,17 @@ void run_front(WorldGpu& W, StepCtx& ctx) {
     uint32_t nitems = exclusive_scan_total(S, S.t_ncell.p, S.t_celloff.p, ncol, st);
     uint32_t ncand = 0;
     S.t_icnt.ensure(nitems + 1); S.t_ioff.ensure(nitems + 1);
+    S.t_sp.ensure(8 * (size_t)nitems + 8); S.t_sn.ensure(8 * (size_t)nitems + 8);
     if (nitems > 0) {
-      k_terrain_items<false><<<(nitems + 127) / 128, 128, 0, st>>>(nitems, ncol, ctx.hf, S.t_celloff.p, S.t_win.p, W.col_body.p,
-                                                                  W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, S.sweep.p,
-                                                                  S.t_icnt.p, nullptr, nullptr, nullptr); RP_COUNT_LAUNCH(1);
+      k_terrain_items<<<(nitems + 127) / 128, 128, 0, st>>>(nitems, ncol, ctx.hf, S.t_celloff.p, S.t_win.p, W.col_body.p,
+                                                           W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, S.sweep.p,
+                                                           S.t_icnt.p, S.t_sp.p, S.t_sn.p); RP_COUNT_LAUNCH(1);
       ncand = exclusive_scan_total(S, S.t_icnt.p, S.t_ioff.p, nitems, st);
     }
     S.t_cp.ensure(ncand + 1); S.t_cn.ensure(ncand + 1);
     if (ncand > 0) {
-      k_terrain_items<true><<<(nitems + 127) / 128, 128, 0, st>>>(nitems, ncol, ctx.hf, S.t_celloff.p, S.t_win.p, W.col_body.p,
-                                                                 W.col_kind.p, W.col_dims.p, W.pos.p, W.rot.p, S.sweep.p,
-                                                                 nullptr, S.t_ioff.p, S.t_cp.p, S.t_cn.p); RP_COUNT_LAUNCH(1);
+      k_terrain_gather<<<(nitems + 255) / 256, 256, 0, st>>>(nitems, S.t_icnt.p, S.t_ioff.p, S.t_sp.p, S.t_sn.p, S.t_cp.p,
+                                                            S.t_cn.p); RP_COUNT_LAUNCH(1);
     }
     k_terrain_cull<<<(ncol + 127) / 128, 128, 0, st>>>(ncol, W.col_kind.p, S.t_celloff.p, S.t_ncell.p, S.t_ioff.p, nitems,
                                                       ncand, S.t_cp.p, S.t_cn.p, S.t_pt.p, S.t_n.p, S.t_cnt.p); RP_COUNT_LAUNCH(1);

@@ -71,13 +71,16 @@ enum Phase : int {
   PH_FORCES = 0, PH_AABB, PH_BROAD, PH_NARROW, PH_TERRAIN, PH_CONTACTS, PH_ISLANDS, PH_ROWS, PH_SCHED,
   PH_WARM_MATCH, PH_VEL_SOLVE, PH_WARM_CACHE, PH_VEL_SHOCK, PH_BALLISTIC, PH_INTEGRATE, PH_POS_ITER,
   PH_POS_SHOCK, PH_STAGE6,
-  // parts of vel_solve (nested inside it; named "vel_solve.*")
-  PH_VEL_PACKED, PH_VEL_ISLAND, PH_VEL_BIG, PH_COUNT
+  // parts of vel_solve (nested inside it; named "vel_solve.*"): the rows' staging before the
+  // classes fork, the packed groups, the big islands, and each single-island bucket on its stream
+  PH_VEL_PREP, PH_VEL_PACKED, PH_VEL_BIG, PH_VEL_ISL0, PH_VEL_ISL1, PH_VEL_ISL2, PH_VEL_ISL3, PH_VEL_ISL4,
+  PH_VEL_ISL5, PH_COUNT
 };
 static const char* const kPhaseNames[PH_COUNT] = {
     "forces", "aabb_sweep", "broadphase", "narrow_pairs", "terrain", "contacts", "islands", "rows", "schedule",
     "warm_match", "vel_solve", "warm_cache", "vel_shock", "ballistic", "integrate", "pos_iter", "pos_shock", "stage6",
-    "vel_solve.packed", "vel_solve.island", "vel_solve.big"};
+    "vel_solve.prep", "vel_solve.packed", "vel_solve.big", "vel_solve.island128", "vel_solve.island256",
+    "vel_solve.island384", "vel_solve.island512", "vel_solve.island768", "vel_solve.island1152"};
 
 struct Profiler {
   bool on = false;
@@ -159,7 +162,7 @@ struct WorldGpu::Scratch {
   DBuf<uint32_t> p_cnt, t_cnt, pstart, bcnt, boff;
   DBuf<int4> t_win;
   DBuf<uint32_t> t_ncell, t_celloff, t_icnt, t_ioff;
-  DBuf<float4> t_cp, t_cn;
+  DBuf<float4> t_cp, t_cn, t_sp, t_sn;  // terrain points: packed, and 8 slots per (collider, cell) item
   // contacts
   DBuf<uint32_t> c_a, c_b;
   DBuf<float4> c_pt, c_n;  // c_pt.w = depth, c_n.w = impulse
@@ -208,7 +211,7 @@ struct WorldGpu::Scratch {
   DBuf<float4> pred_used, s_pred;
   // solve groups (islands packed for one CTA each) and their shared-memory residents
   DBuf<uint32_t> g_small_rows, g_small_pre, g_big, g_big_pre, g_of_isl, g_key, g_key2, g_start, g_cnt, g_class,
-      body_grp, gb_key, gb_key2, gb_list, gb_tmp, gb_start, gb_cnt, body_local;
+      g_iota, g_perm, g_sz_sorted, g_pre_sorted, body_grp, gb_key, gb_key2, gb_list, gb_tmp, gb_start, gb_cnt, body_local;
   // rows in schedule order (coalesced per level) for the shared-memory solve
   DBuf<uint2> s_loc;                      // local body index of A / B (0xFFFFFFFF: cannot move)
   DBuf<uint32_t> s_flags;

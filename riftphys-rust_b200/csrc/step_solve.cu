@@ -1203,8 +1203,8 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
 }
 
 // ------------------------------------------------------------------ solve groups
-// Small islands (at most GROUP_ROWS rows) are packed, in island order, into groups of about
-// GROUP_ROWS rows (by the prefix sum of their row counts, so a group holds at most
+// Small islands (at most GROUP_ROWS rows) are packed, in order of their row counts, into groups of
+// about GROUP_ROWS rows (by the prefix sum of their row counts, so a group holds at most
 // 2 * GROUP_ROWS - 1 rows and twice that many bodies); bigger islands form a group alone.
 // Islands are independent, so any interleaving of their rows is a valid serial order: a group
 // is scheduled and solved exactly like one island. Classes: 3, a packed group, and 10..15, an
@@ -1212,8 +1212,8 @@ __global__ void k_count_sleeping(uint32_t n, const uint8_t* __restrict__ awake, 
 // of it on chip; 0, a bigger island, by one CTA with its body velocities on chip and its rows
 // streamed through a cp.async double buffer; 2, an island beyond that, by one warp over global
 // memory.
-// (the row count GROUP_ROWS is a tuning knob, WorldGpu::Tuning::group_rows: 8, 16 or 32)
-#define GROUP_ROWS_MAX 32u
+// (the row count GROUP_ROWS is a tuning knob, WorldGpu::Tuning::group_rows: 8, 16, 32, 64 or 128)
+#define GROUP_ROWS_MAX 128u
 // big islands (classes 20..22): bodies and level starts held in shared memory, rows per staged
 // chunk (= threads per CTA) -- sized per bucket so that smaller ones share an SM
 #define BIG_BUCKETS 3
@@ -2481,7 +2481,16 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       S.g_big_pre.ensure(nisl + 1); S.g_of_isl.ensure(nisl + 1);
       const uint32_t group_rows = W.tuning_.group_rows;
       k_group_flags<<<nblk(nisl), T, 0, st>>>(nisl, group_rows, S.isl_cnt.p, S.g_small_rows.p, S.g_big.p); RP_COUNT_LAUNCH(1);
-      uint32_t small_total = exclusive_scan_total(S, S.g_small_rows.p, S.g_small_pre.p, nisl, st);
+      // small islands are packed in order of their row count (island order among equal counts), so
+      // a group holds islands of about one size: a small island is mostly a chain of rows on one
+      // body, so its levels are about its rows, and a group's levels are its deepest island's
+      S.g_iota.ensure(nisl + 1); S.g_perm.ensure(nisl + 1); S.g_sz_sorted.ensure(nisl + 1); S.g_pre_sorted.ensure(nisl + 1);
+      k_iota<<<nblk(nisl), T, 0, st>>>(nisl, S.g_iota.p); RP_COUNT_LAUNCH(1);
+      int sbits = 1;
+      while ((1u << sbits) <= group_rows) sbits++;
+      sort_pairs_u32(S, S.g_small_rows.p, S.g_sz_sorted.p, S.g_iota.p, S.g_perm.p, nisl, 0, sbits, st);
+      uint32_t small_total = exclusive_scan_total(S, S.g_sz_sorted.p, S.g_pre_sorted.p, nisl, st);
+      k_scatter_u32<<<nblk(nisl), T, 0, st>>>(nisl, S.g_perm.p, S.g_pre_sorted.p, S.g_small_pre.p); RP_COUNT_LAUNCH(1);
       uint32_t nbig = exclusive_scan_total(S, S.g_big.p, S.g_big_pre.p, nisl, st);
       g_small = small_total ? (small_total - 1) / group_rows + 1 : 0;
       ng = g_small + nbig;
@@ -2593,6 +2602,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
     W.pred_valid_ = learned;
     P.end(PH_WARM_MATCH, st);
     P.begin(PH_VEL_SOLVE, st);
+    P.begin(PH_VEL_PREP, st);
     // ---- warm application + velocity sweeps
     const bool resid_mode = W.res_tol_ > 0.0f;
     int iters = (int)(resid_mode ? (W.res_max_ > 0 ? W.res_max_ : W.iters_v_) : W.iters_v_);
@@ -2637,6 +2647,8 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       // groups on the tick's stream. Side streams fork from the tick's stream and join it after.
       const bool big = ng > g_small;
       auto lst = [&](int c) { return S.cls_list.p + (size_t)c * ng; };
+      static_assert(PH_VEL_ISL5 - PH_VEL_ISL0 + 1 == ISLAND_BUCKETS, "a profile phase per island bucket");
+      P.end(PH_VEL_PREP, st);
       if (big) {
         RP_CUDA(cudaEventRecord(W.ev_fork_, st));
         for (int k = 0; k < WorldGpu::kAux; ++k) RP_CUDA(cudaStreamWaitEvent(W.aux_[k], W.ev_fork_, 0));
@@ -2670,12 +2682,11 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
                                                                  lst(2), S.row_islid.p, S.isl_final.p); RP_COUNT_LAUNCH(1);
         }
         P.end(PH_VEL_BIG, sg);
-        int top = -1;  // the largest non-empty bucket, timed as "vel_solve.island"
         for (int b = ISLAND_BUCKETS - 1; b >= 0; --b) {
           cudaStream_t sb = W.aux_[b];
           uint32_t n = cls_n[10 + b];
           if (!n) continue;
-          if (top < 0) { top = b; P.begin(PH_VEL_ISLAND, sb); }
+          P.begin(PH_VEL_ISL0 + b, sb);
           OnchipLayout lay = onchip_layout(kIslandRows[b], kIslandBodies[b], 1u);
           auto kern = W.tuning_.island_threads == 32    ? k_vel_solve_onchip<false, 32>
                       : W.tuning_.island_threads == 64  ? k_vel_solve_onchip<false, 64>
@@ -2685,7 +2696,7 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
               lay, 0u, n, lst(10 + b), 10u + (uint32_t)b, S.g_class.p, S.gb_start.p, S.gb_cnt.p, S.gb_list.p,
               S.g_nisl.p, SM, SR, B, W.warm_a.p, W.warm_b.p, S.acc_jn.p, S.acc_jt.p, iters, tol, stats, S.row_islid.p,
               S.isl_final.p); RP_COUNT_LAUNCH(1);
-          if (b == top) P.end(PH_VEL_ISLAND, sb);
+          P.end(PH_VEL_ISL0 + b, sb);
         }
       }
       P.begin(PH_VEL_PACKED, st);

@@ -97,7 +97,7 @@ class WorldGpu {
   // rows of a level are): rows up to which islands are packed into shared groups (8, 16, 32), threads
   // of a packed-group block (32, 64, 128) and of a single-island block (32, 64, 128, 256). Defaults are
   // the autotuner's choice for the terrain workload.
-  struct Tuning { uint32_t group_rows = 32, packed_threads = 32, island_threads = 64; };
+  struct Tuning { uint32_t group_rows = 64, packed_threads = 32, island_threads = 128; };
   Tuning tuning_;
   void set_heightfield(uint32_t nx, uint32_t nz, float sx, float sz, float ox, float oz,
                        const std::vector<float>& q6_heights, float min_y, float max_y, uint32_t mat);

@@ -7,7 +7,7 @@ from conftest import rp, scenes
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(32, 32, 64), (8, 32, 32), (16, 128, 256), (32, 64, 128)]
+SHAPES = [(64, 32, 128), (32, 32, 64), (8, 32, 32), (16, 128, 256), (32, 64, 128), (64, 32, 32), (64, 128, 64), (128, 32, 128)]
 
 
 def _terrain_hashes(gpu, shape):
@@ -35,4 +35,4 @@ def test_unsupported_shape_is_refused(gpu):
     with pytest.raises(rp.RPhysError) as e:
         w.set_tuning(12, 64, 128)
     assert e.value.code == rp.RPHYS_ERR_BAD_ARG
-    assert w.tuning() == {"group_rows": 32, "packed_threads": 32, "island_threads": 64}  # the tuned defaults
+    assert w.tuning() == {"group_rows": 64, "packed_threads": 32, "island_threads": 128}  # the tuned defaults

@@ -75,7 +75,7 @@ def test_set_solve_order_rejects_unknown(oracle):
 
 def test_tuning_is_stored_and_checked(oracle):
     w, _ = _terrain(oracle, False, n=10)
-    assert w.tuning() == {"group_rows": 32, "packed_threads": 32, "island_threads": 64}
+    assert w.tuning() == {"group_rows": 64, "packed_threads": 32, "island_threads": 128}
     w.set_tuning(16, 128, 256)
     assert w.tuning() == {"group_rows": 16, "packed_threads": 128, "island_threads": 256}
     try:
