@@ -210,9 +210,20 @@ __device__ __forceinline__ void contact_impulse(const BodiesV& B, const Row& r, 
   if (r.inv_b > 0.0f) body_impulse(B, r.bi, j, cross(r.rb, j));
 }
 #include "bounce.cuh"
+// The friction law mu_k + (mu_s - mu_k) * exp(-(slip / sv)^2). Where mu_s == mu_k and slip / sv is
+// a number, exp's value lies in [0, 1], so (mu_s - mu_k) * exp(...) has the bits of
+// (mu_s - mu_k) * 0 (+0, or NaN for infinite coefficients): the law is evaluated without the
+// division and the exp, with the same result.
+__device__ __forceinline__ bool ratio_is_nan(float a, float b) {
+  return isnan(a) || isnan(b) || (a == 0.0f && b == 0.0f) || (isinf(a) && isinf(b));
+}
+__device__ __forceinline__ float mu_law(float mu_s, float mu_k, float sv, float slip) {
+  if (mu_s == mu_k && !ratio_is_nan(slip, sv)) return mu_k + (mu_s - mu_k) * 0.0f;
+  float t = slip / sv;
+  return mu_k + (mu_s - mu_k) * exp_rp(-(t * t));
+}
 __device__ __forceinline__ float mu_dynamic(const Row& r, float slip) {  // solver.rs:429-431
-  float t = slip / r.sv;
-  return r.mu_k + (r.mu_s - r.mu_k) * exp_rp(-(t * t));
+  return mu_law(r.mu_s, r.mu_k, r.sv, slip);
 }
 // Warm start of one matched row (solver.rs:749-760)
 __device__ __forceinline__ void warm_apply(const BodiesV& B, const Row& r, uint32_t k, float4 ea, float4 eb,
@@ -1419,10 +1430,7 @@ __device__ __forceinline__ void contact_impulse_s(const SBodies& B, const SRow& 
   if (r.inv_a > 0.0f) { f3 nj = -j; body_impulse_s(B, r.la, nj, cross(r.ra, nj)); }
   if (r.inv_b > 0.0f) body_impulse_s(B, r.lb, j, cross(r.rb, j));
 }
-__device__ __forceinline__ float mu_dynamic_s(const SRow& r, float slip) {
-  float t = slip / r.sv;
-  return r.mu_k + (r.mu_s - r.mu_k) * exp_rp(-(t * t));
-}
+__device__ __forceinline__ float mu_dynamic_s(const SRow& r, float slip) { return mu_law(r.mu_s, r.mu_k, r.sv, slip); }
 __device__ __forceinline__ void warm_apply_s(const SBodies& B, const SRow& r, uint32_t s, float4 ea, float4 eb,
                                              float* jn_arr, float2* jt_arr) {
   float jn = ea.w;
@@ -1469,6 +1477,16 @@ __device__ __forceinline__ void impulse_reg(f3& lin, f3& ang, float im, const m3
   if (im > 0.0f && vfin(j)) lin = fin_v(lin + j * im);
   if (im > 0.0f && vfin(tau)) ang = fin_v(ang + mvec(Iw, tau));
 }
+// impulse_reg on side `on` of a row, with its conditions as selects instead of branches: the new
+// velocities are computed unconditionally and kept where impulse_reg would write them (the same
+// expressions, so the same bits), so the two sides of a row interleave on one dependent chain
+__device__ __forceinline__ f3 sel3(bool c, f3 a, f3 b) { return mk3(c ? a.x : b.x, c ? a.y : b.y, c ? a.z : b.z); }
+__device__ __forceinline__ void impulse_sel(f3& lin, f3& ang, bool on, float im, const m3& Iw, f3 j, f3 tau) {
+  const bool mv = on && im > 0.0f;
+  const f3 nl = fin_v(lin + j * im), na = fin_v(ang + mvec(Iw, tau));
+  lin = sel3(mv && vfin(j), nl, lin);
+  ang = sel3(mv && vfin(tau), na, ang);
+}
 __device__ __forceinline__ m3 load_iw(const float* q) {
   return mcols(mk3(q[0], q[1], q[2]), mk3(q[3], q[4], q[5]), mk3(q[6], q[7], q[8]));
 }
@@ -1479,12 +1497,14 @@ __device__ __forceinline__ void joint_apply_reg(f3& la, f3& aa, f3& lb, f3& ab, 
                                                 float ima, float imb, float lam) {
   f3 p = r.n * lam;
   const bool ia = r.inv_a > 0.0f, ib = r.inv_b > 0.0f;
-  if (r.flags & RF_JANG) {
-    if (ia) { f3 t = -p; if (ima > 0.0f && vfin(t)) aa = fin_v(aa + mvec(qa, t)); }
-    if (ib && imb > 0.0f && vfin(p)) ab = fin_v(ab + mvec(qb, p));
+  const f3 np = -p;
+  if (r.flags & RF_JANG) {  // selects, as impulse_sel
+    const f3 na = fin_v(aa + mvec(qa, np)), nb = fin_v(ab + mvec(qb, p));
+    aa = sel3(ia && ima > 0.0f && vfin(np), na, aa);
+    ab = sel3(ib && imb > 0.0f && vfin(p), nb, ab);
   } else {
-    if (ia) { f3 nj = -p; impulse_reg(la, aa, ima, qa, nj, cross(r.ra, nj)); }
-    if (ib) impulse_reg(lb, ab, imb, qb, p, cross(r.rb, p));
+    impulse_sel(la, aa, ia, ima, qa, np, cross(r.ra, np));
+    impulse_sel(lb, ab, ib, imb, qb, p, cross(r.rb, p));
   }
 }
 // The original distance row (solver.rs:793-817) on register copies of the two linear velocities
@@ -1603,8 +1623,9 @@ __device__ __forceinline__ void pgs_row_core(float4* lin, float4* ang, const SRo
     return vb - va;
   };
   auto apply = [&](f3 j) {
-    if (ia) { f3 nj = -j; impulse_reg(la, aa, ima, qa, nj, cross(r.ra, nj)); }
-    if (ib) impulse_reg(lb, ab, imb, qb, j, cross(r.rb, j));
+    const f3 nj = -j;
+    impulse_sel(la, aa, ia, ima, qa, nj, cross(r.ra, nj));
+    impulse_sel(lb, ab, ib, imb, qb, j, cross(r.rb, j));
   };
   float v_rel_n = dot(rel(), r.n);
   float jn_raw = (r.bias - v_rel_n) * r.m_n;
@@ -1649,8 +1670,9 @@ __device__ __forceinline__ void warm_core(float4* lin, float4* ang, const SRow& 
   f3 t = clamp_length_max(mk3(dot(jt, r.t1), dot(jt, r.t2), 0.0f), mu * jn);
   jt_acc = make_float2(t.x, t.y);
   imp = imp + ((r.t1 * t.x) + (r.t2 * t.y));
-  if (ia) { f3 nj = -imp; impulse_reg(la, aa, ima, qa, nj, cross(r.ra, nj)); }
-  if (ib) impulse_reg(lb, ab, imb, qb, imp, cross(r.rb, imp));
+  const f3 nimp = -imp;
+  impulse_sel(la, aa, ia, ima, qa, nimp, cross(r.ra, nimp));
+  impulse_sel(lb, ab, ib, imb, qb, imp, cross(r.rb, imp));
   if (ia) { lin[r.la] = f4(la, LA.w); ang[r.la] = f4(aa, AA.w); }
   if (ib) { lin[r.lb] = f4(lb, LB.w); ang[r.lb] = f4(ab, AB.w); }
 }
@@ -2650,10 +2672,14 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
       static_assert(PH_VEL_ISL5 - PH_VEL_ISL0 + 1 == ISLAND_BUCKETS, "a profile phase per island bucket");
       P.end(PH_VEL_PREP, st);
       if (big) {
+        // every class's timer starts here, on the tick's stream, and stops on the class's own
+        // stream: each reads as the time from the fork to that class's end
+        P.begin(PH_VEL_BIG, st);
+        for (int b = 0; b < ISLAND_BUCKETS; ++b)
+          if (cls_n[10 + b]) P.begin(PH_VEL_ISL0 + b, st);
         RP_CUDA(cudaEventRecord(W.ev_fork_, st));
         for (int k = 0; k < WorldGpu::kAux; ++k) RP_CUDA(cudaStreamWaitEvent(W.aux_[k], W.ev_fork_, 0));
         cudaStream_t sg = W.aux_[WorldGpu::kAux - 1];
-        P.begin(PH_VEL_BIG, sg);
         // big islands: per-row inverse inertias for the staged stream, then one CTA each, per bucket
         uint32_t nbig = cls_n[20] + cls_n[21] + cls_n[22];
         if (nbig) {
@@ -2686,7 +2712,6 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           cudaStream_t sb = W.aux_[b];
           uint32_t n = cls_n[10 + b];
           if (!n) continue;
-          P.begin(PH_VEL_ISL0 + b, sb);
           OnchipLayout lay = onchip_layout(kIslandRows[b], kIslandBodies[b], 1u);
           auto kern = W.tuning_.island_threads == 32    ? k_vel_solve_onchip<false, 32>
                       : W.tuning_.island_threads == 64  ? k_vel_solve_onchip<false, 64>
