@@ -2859,10 +2859,13 @@ void run_solve(WorldGpu& W, StepCtx& ctx) {
           S.split_a.p, W.joints_d.p, W.jlam.p, S.orig_pos.p, S.orig_rot.p, ctx.dt); RP_COUNT_LAUNCH(1);
     };
     if (npp) {
-      // jointed islands of up to 128 / 256 rows (a ragdoll or two): 4 / 8 lanes each
-      pos_launch(std::integral_constant<int, 4>{}, cls_n[10], S.cls_list.p + 10 * (size_t)ngr, 0u);
-      pos_launch(std::integral_constant<int, 8>{}, cls_n[11], S.cls_list.p + 11 * (size_t)ngr, 0u);
-      pos_launch(std::integral_constant<int, 32>{}, ngr, nullptr, (1u << 10) | (1u << 11));
+      // jointed islands of up to 128 / 256 rows (a ragdoll or two): 2 / 4 lanes each, the rest 8.
+      // The pass is bound by the instructions a warp issues: more islands per warp put more of its
+      // lanes to work per instruction (ragdolls: 2 / 4 / 8 lanes 21 ms, 4 / 8 / 32 lanes 27 ms,
+      // 32 lanes for every island 58 ms; lane counts change no result bit)
+      pos_launch(std::integral_constant<int, 2>{}, cls_n[10], S.cls_list.p + 10 * (size_t)ngr, 0u);
+      pos_launch(std::integral_constant<int, 4>{}, cls_n[11], S.cls_list.p + 11 * (size_t)ngr, 0u);
+      pos_launch(std::integral_constant<int, 8>{}, ngr, nullptr, (1u << 10) | (1u << 11));
     } else if (ngr) {
       // no joints: the groups the velocity solve keeps on chip run the pass on chip as well (the
       // single-island buckets on the side streams, the packed groups here); the big and
