@@ -17,12 +17,16 @@ e2e     the same metric through the C ABI's rphys_world_step_ex with the tick's 
 roofline  the stage with the most device time in a profiled replay of the same K ticks (CUDA events
         around each stage on the world's stream): its algorithmic bytes per launch / its mean
         duration, against the measured HBM copy bandwidth in MEASURED_PEAKS.json.
-cpu_baseline  the CPU restatement of the reference step (C++, OpenMP, all host threads) on the
-        benchmark's own state: it loads the GPU world's state blob from the timed region's start
-        and steps --cpu-ticks ticks of the full workload.
+cpu_baseline  the CPU restatement of the reference step (C++, OpenMP, all host threads or
+        --cpu-threads) on the benchmark's own state: it loads the GPU world's state blob from the
+        timed region's start and steps --cpu-ticks ticks of the full workload; ``one_thread``: the
+        first of those ticks again on one thread.
 parity  those ticks' hashes and the final body states, GPU against the CPU restatement.
 solve   the last timed tick's velocity solve: sweeps, residual, islands still above the tolerance
         at the cap and their rows, and a histogram of the islands' last-sweep residuals.
+batched (terrain) the 4,096-world batch stepped as one device world against the same worlds
+        stepped one by one through their own RPhysWorld, and against the CPU restatement on every
+        128th world (whose hashes must equal the batch's), plus the rollback window.
 
 Multi-GPU: a single world does not shard (its contacts couple every body), so for the terrain and
 box-drop workloads N ranks run N independent replicas (one per GPU, scaling "weak"). ``--config

@@ -84,3 +84,23 @@ def test_tuning_is_stored_and_checked(oracle):
         assert e.code == rp.RPHYS_ERR_BAD_ARG
     else:
         raise AssertionError("packed_threads 48 accepted")
+
+
+def test_tuning_accepts_the_tuner_grid_and_nothing_else(oracle):
+    """Every launch shape the autotuner times is accepted by the C ABI's check (the CPU restatement
+    applies the same check as the CUDA library), and shapes outside the grid are refused."""
+    import itertools
+    import riftphys_rust_b200.autotune as autotune
+    w, _ = _terrain(oracle, False, n=10)
+    for gr, pt, it in itertools.product(autotune.GRID["group_rows"], autotune.GRID["packed_threads"],
+                                        autotune.GRID["island_threads"]):
+        w.set_tuning(gr, pt, it)
+        assert w.tuning() == {"group_rows": gr, "packed_threads": pt, "island_threads": it}
+    for bad in [(12, 32, 32), (256, 32, 32), (0, 32, 32), (64, 256, 32), (64, 32, 512), (64, 32, 16)]:
+        try:
+            w.set_tuning(*bad)
+        except rp.RPhysError as e:
+            assert e.code == rp.RPHYS_ERR_BAD_ARG
+        else:
+            raise AssertionError(f"shape {bad} accepted")
+    assert w.tuning() == {"group_rows": 128, "packed_threads": 128, "island_threads": 256}  # the last accepted one
